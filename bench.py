@@ -1,0 +1,466 @@
+"""Benchmark of the wavefront path-tracing loop (one JSON line on rank 0).
+
+Workload (N=1): the instanced PBR scene — 64 instances of a 16,384-triangle
+sphere, a 2-triangle ground and 1,024 emissive triangles (1,049,602
+triangles) — at 1920x1080, 4 spp, 8 bounces, ReSTIR DI with 32 candidates,
+1 temporal and 1 spatial pass (5 neighbours, radius 30 px).  A step renders
+one frame.  Metric: Mrays/s (camera + extension + shadow rays per second).
+
+* ``value``: device time of the frame (CUDA events on the renderer's stream),
+  scene resident, output into a device buffer; L2 flushed between steps.
+* ``e2e``: the same frames through ``render_frame`` (host output array,
+  per-step device->host image copy), timed by the host clock.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  average event-timed launch duration, against MEASURED_PEAKS.json.
+* ``cpu_baseline``: the oracle restatement of CpuReferenceRenderer on a
+  bounded sample of the same scene, all host cores.
+
+``--impl reference`` times that CPU reference alone (rank 0).
+For N > 1 (torchrun), every rank renders its own frames (weak scaling, no
+data-path collective); the step time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+from pathlib import Path
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+METRIC = "Mrays/s, 1M-tri 1080p; served p50/p99 latency vs plain path, same B200"
+WIDTH, HEIGHT, SPP, BOUNCES = 1920, 1080, 4, 8
+WORKLOAD = ("instanced PBR scene: 64 x 16,384-tri spheres + 2-tri ground + 1,024 emissive tris "
+            "(1,049,602 tris), 1920x1080, 4 spp, 8 bounces, GGX+NEE, ReSTIR DI 32 candidates + "
+            "1 temporal + 1 spatial (5 neighbours, r=30 px)")
+
+# Algorithmic bytes per work unit of each stage (fixed figures, independent of
+# the layout): ray 32 B, hit 20 B, path 36 B, material 32 B, shading triangle
+# 72 B, shadow ray 44 B.
+BYTES_PER_UNIT = {
+    "raygen": 68.0,          # write ray 32 + path 36 per camera ray
+    "trace_closest": 52.0,   # read ray 32, write hit 20 per ray
+    "shade_hit": 304.0,      # read 32+20+36+32+36+36, write 36+32+44 per surface hit
+    "shade_miss": 124.0,     # read ray 32 + hit 20 + path 36, write path 36
+    "trace_shadow": 68.0,    # read shadow ray 44, read+write radiance 12+12
+    "accumulate": 44.0,      # read radiance 12, read+write pixel 16+16
+    "restir": 408.0,         # ray+hit 52, reservoir write 32, history read 32; spatial: ray+hit 52,
+                             # 6 reservoir reads 192, write 32, selected sample 16
+    "resolve": 40.0,         # read 24 B fixed-point sums, write 16 B pixel
+}
+
+
+def _peaks():
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU reference sample (oracle restatement of CpuReferenceRenderer)
+# ---------------------------------------------------------------------------
+_CPU_STATE = {}
+
+
+def _cpu_worker_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["MKL_NUM_THREADS"] = "1"
+    from ordinarylight_b200 import scenes
+
+    scene, camera = scenes.instanced_spheres()
+    _CPU_STATE["triangles"] = scene.triangles()
+    _CPU_STATE["camera"] = camera
+
+
+def _cpu_tile(args):
+    """Closest-hit rays of one tile of the workload's first bounce, traced by
+    the oracle's brute-force intersector (path_tracer.py:154-176)."""
+    tile, size = args
+    from oracle import reference_path_tracer as ref
+
+    tris = _CPU_STATE["triangles"][0]
+    camera = _CPU_STATE["camera"]
+    rng = np.random.default_rng(1000 + tile)
+    o, d = ref.camera_rays(camera, WIDTH, HEIGHT, rng)
+    tiles_x = WIDTH // size
+    tx, ty = tile % tiles_x, (tile // tiles_x) % (HEIGHT // size)
+    sel = ((np.arange(HEIGHT)[:, None] // size == ty) & (np.arange(WIDTH)[None, :] // size == tx)).reshape(-1)
+    counter = ref.RayCounter()
+    t0 = time.perf_counter()
+    ref.intersect(o[sel], d[sel], tris, counter)
+    return counter.rays, time.perf_counter() - t0
+
+
+class CpuReference:
+    """Pool of spawn workers, each holding the workload's triangle soup."""
+
+    def __init__(self, processes=None, tile=8):
+        import multiprocessing as mp
+
+        self.processes = processes or os.cpu_count() or 1
+        self.tile = tile
+        self.pool = mp.get_context("spawn").Pool(self.processes, initializer=_cpu_worker_init)
+        self.step = 0
+
+    def run_step(self):
+        jobs = [(self.step * self.processes + k, self.tile) for k in range(self.processes)]
+        self.step += 1
+        results = self.pool.map(_cpu_tile, jobs)
+        rays = sum(r for r, _ in results)
+        seconds = max(s for _, s in results)
+        return rays, seconds
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self, steps):
+        return (f"first bounce (camera rays) of {self.processes} {self.tile}x{self.tile}-pixel tiles per step at "
+                f"1 spp, {steps} step(s), brute-force intersection over all 1,049,602 triangles as the CPU "
+                "reference does; one process per core, slowest process timed")
+
+
+def cpu_reference_measure(steps, processes=None):
+    ref = CpuReference(processes)
+    try:
+        total_rays, total_s = 0, 0.0
+        for _ in range(steps):
+            rays, secs = ref.run_step()
+            total_rays += rays
+            total_s += secs
+        return total_rays / total_s / 1e6, ref.processes, ref.describe(steps)
+    finally:
+        ref.close()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = str(index)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", self.index, "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the CUDA arm
+# ---------------------------------------------------------------------------
+def _make_renderer(device):
+    from ordinarylight_b200 import CudaWavefrontRenderer
+
+    return CudaWavefrontRenderer(device=device, samples_per_pixel=SPP, max_bounces=BOUNCES, restir=True,
+                                 restir_candidates=32, restir_temporal=True, restir_spatial=1,
+                                 restir_neighbours=5, restir_radius=30.0)
+
+
+def _profile(renderer):
+    from ordinarylight_b200 import _native
+    import ctypes
+
+    count = ctypes.c_uint32()
+    lib = renderer._lib
+    _native.check(lib, renderer._ctx, lib.olc_frame_profile(renderer._ctx, None, 0, ctypes.byref(count)))
+    records = (_native.OlcLaunchRecord * count.value)()
+    _native.check(lib, renderer._ctx, lib.olc_frame_profile(renderer._ctx, records, count.value,
+                                                            ctypes.byref(count)))
+    return [(_native.STAGE_NAMES[r.stage], r.bounce, int(r.items), int(r.misses), float(r.ms)) for r in records]
+
+
+def _launch_bytes(stage, items, misses):
+    if stage == "shade":
+        return BYTES_PER_UNIT["shade_hit"] * (items - misses) + BYTES_PER_UNIT["shade_miss"] * misses
+    return BYTES_PER_UNIT[stage] * items
+
+
+def _traffic_from_profiles(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = REPO / "profiles" / f"{kernel}_traffic.txt"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch_full_workload:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, rank, world, device_index):
+    import torch
+
+    from ordinarylight_b200 import _native, scenes
+
+    torch.cuda.set_device(device_index)
+    scene, camera = scenes.instanced_spheres()
+    renderer = _make_renderer(device_index)
+    out = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, device=f"cuda:{device_index}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device_index}")
+    import ctypes
+
+    handle = ctypes.c_void_p()
+    _native.check(renderer._lib, renderer._ctx, renderer._lib.olc_stream(renderer._ctx, ctypes.byref(handle)))
+    stream = torch.cuda.ExternalStream(handle.value, device=f"cuda:{device_index}")
+    frame0 = 1000 * rank
+    # warm-up (also builds the BVH and captures nothing: ReSTIR frames run uncaptured)
+    for k in range(args.warmup):
+        renderer.render_frame_into(scene, camera, WIDTH, HEIGHT, out, frame_index=frame0 + k)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    clocks = ClockSampler(device_index)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    rays = 0
+    stage_ms, stage_bytes, stage_launches = {}, {}, {}
+    launches = 0
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))  # evict L2 between timed steps
+            starts[k].record(stream)
+        renderer.render_frame_into(scene, camera, WIDTH, HEIGHT, out, frame_index=frame0 + args.warmup + k)
+        with torch.cuda.stream(stream):
+            ends[k].record(stream)
+        rays += renderer.last_timings["rays"]
+        for stage, _b, items, misses, ms in _profile(renderer):
+            stage_ms[stage] = stage_ms.get(stage, 0.0) + ms
+            stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, items, misses)
+            stage_launches[stage] = stage_launches.get(stage, 0) + 1
+            launches += 2 if stage == "restir" else 1
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{device_index}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        r = torch.tensor([float(rays)], dtype=torch.float64, device=f"cuda:{device_index}")
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        rays_all = float(r.item())
+    else:
+        rays_all = float(rays)
+    value = rays_all / (total_ms * 1e3)
+
+    # end to end through the public API: host output, per-step host clock
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_rays = 0
+    for k in range(e2e_steps):
+        img = renderer.render_frame(scene, camera, WIDTH, HEIGHT, frame_index=frame0 + 500 + k)
+        e2e_rays += renderer.last_timings["rays"]
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{device_index}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=f"cuda:{device_index}")
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        e2e_rays = float(r.item())
+    e2e = e2e_rays / e2e_s / 1e6
+    finite = bool(np.all(np.isfinite(img)))
+    timings = dict(renderer.last_timings)
+
+    # dominant kernel roofline
+    peak, peak_kind = _peaks()
+    dominant = max(stage_ms, key=stage_ms.get)
+    per_launch_bytes = stage_bytes[dominant] / stage_launches[dominant]
+    per_launch_ms = stage_ms[dominant] / stage_launches[dominant]
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    stages = {name: {"ms_per_step": stage_ms[name] / args.steps,
+                     "share": stage_ms[name] / sum(stage_ms.values()),
+                     "achieved_gbs": stage_bytes[name] / (stage_ms[name] * 1e-3) / 1e9 if stage_ms[name] else 0.0}
+              for name in stage_ms}
+    renderer.close()
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded scene generators, ordinarylight_b200/scenes.py)",
+        "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_bounces": BOUNCES,
+                   "triangles": 1049602, "parallelism": f"replicas x{world} (independent frames per GPU)",
+                   "l2": "256 MiB buffer written between timed steps (L2 flush); per-frame queues 1.7 GB"},
+        "rays_per_step": rays_all / args.steps,
+        "mrays_closest_hit": None,
+        "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 64 + 112,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 1600, "steps": e2e_steps, "finite": finite},
+        "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": _traffic_from_profiles(dominant),
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
+        "stages": stages,
+        "gpu_launches": launches,
+        "clocks": clock_info,
+        "last_frame": {k: timings[k] for k in ("camera_rays", "extension_rays", "shadow_rays", "gpu_ms",
+                                               "restir_history_used", "traversal_errors", "queue_overflow")},
+    }
+    cr = timings["camera_rays"] + timings["extension_rays"]
+    line["mrays_closest_hit"] = cr * args.steps / (total_ms * 1e3) if world == 1 else None
+    return line
+
+
+def run_reference_arm(args):
+    steps = args.steps
+    ref = CpuReference(args.cpu_processes)
+    try:
+        for _ in range(args.warmup):
+            ref.run_step()
+        total_rays, total_s = 0, 0.0
+        for _ in range(steps):
+            rays, secs = ref.run_step()
+            total_rays += rays
+            total_s += secs
+    finally:
+        ref.close()
+    value = total_rays / total_s / 1e6
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "Mrays/s",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_s * 1e3 / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded scene generators, ordinarylight_b200/scenes.py)",
+        "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_bounces": BOUNCES,
+                   "triangles": 1049602, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": ref.processes, "kind": "port",
+                         "sample": ref.describe(steps)},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--cpu-steps", type=int, default=1)
+    p.add_argument("--cpu-processes", type=int, default=None)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference_arm(args)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+    try:
+        line = run_ours(args, rank, world, local)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            value, cores, sample = cpu_reference_measure(args.cpu_steps, args.cpu_processes)
+            line["cpu_baseline"] = {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                                    "sample": sample}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

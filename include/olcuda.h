@@ -1,0 +1,337 @@
+/*
+ * olcuda.h — C ABI of the B200 wavefront path tracer (libolcuda.so).
+ *
+ * Every entry point returns an int status (OLC_OK == 0).  On failure the
+ * message is available from olc_last_error(ctx) (or olc_last_error(NULL)
+ * for failures that happen before a context exists).  The Python layer maps
+ * the codes to the exception types the reference renderer raises:
+ *   OLC_ERR_VALUE   -> ValueError    (bad sizes / sample counts,
+ *                                      ordinarylight/targets/vulkan/api.py:1267-1272,
+ *                                      ordinarylight/renderers/reference/cpu.py:15-21)
+ *   OLC_ERR_TYPE    -> TypeError
+ *   OLC_ERR_CLOSED  -> RuntimeError  (closed renderer, cpu.py:60-62)
+ *   OLC_ERR_RUNTIME / OLC_ERR_CUDA / OLC_ERR_MEMORY / OLC_ERR_TIMEOUT
+ *                   -> RuntimeError / MemoryError
+ *
+ * Bulk arrays are plain pointers plus sizes.  Arguments documented as
+ * "host" are read on the host; arguments documented as "device" must be
+ * device pointers on the context's GPU (for example torch.Tensor.data_ptr()).
+ * No entry point takes or returns framework (torch) types.
+ */
+#ifndef OLCUDA_H
+#define OLCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OLC_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define OLC_API __attribute__((visibility("default")))
+#else
+#define OLC_API
+#endif
+
+enum olc_status {
+  OLC_OK = 0,
+  OLC_ERR_VALUE = 1,
+  OLC_ERR_TYPE = 2,
+  OLC_ERR_RUNTIME = 3,
+  OLC_ERR_CUDA = 4,
+  OLC_ERR_MEMORY = 5,
+  OLC_ERR_CLOSED = 6,
+  OLC_ERR_TIMEOUT = 7
+};
+
+/* Transport modes. */
+enum olc_mode {
+  /* GGX/Lambert BSDF, next-event estimation with power-heuristic MIS,
+   * Russian roulette; the reference GPU wavefront's estimator
+   * (ordinarylight/shaders/wavefront_shade.comp:262-596). */
+  OLC_MODE_PRODUCTION = 0,
+  /* The CPU reference's estimator: pure Lambert (albedo = base_color),
+   * emission on every hit, CPU sky gradient, no NEE/RR, origin offset
+   * 1e-4 along the facing normal and t_min 1e-4
+   * (ordinarylight/renderers/reference/path_tracer.py:31-95). */
+  OLC_MODE_REFERENCE_COMPATIBLE = 1
+};
+
+/* Camera projections (ordinarylight/cameras/). */
+enum olc_projection {
+  OLC_PROJECTION_PERSPECTIVE = 0,
+  OLC_PROJECTION_ORTHOGRAPHIC = 1,
+  OLC_PROJECTION_PANORAMIC = 2
+};
+
+/* Analytic light types; the codes of Scene.analytic_light_data
+ * (ordinarylight/scene/_core.py:2578-2632). */
+enum olc_light_type {
+  OLC_LIGHT_POINT = 0,
+  OLC_LIGHT_DIRECTIONAL = 1,
+  OLC_LIGHT_SPOT = 2
+};
+
+/* Environment kinds: none (analytic sky of the mode), constant colour, or an
+ * equirectangular float32 RGB image (path_tracer.py:185-202). */
+enum olc_environment_kind {
+  OLC_ENV_NONE = 0,
+  OLC_ENV_CONSTANT = 1,
+  OLC_ENV_EQUIRECT = 2
+};
+
+typedef struct olc_context olc_context;
+
+/* Renderer configuration.  Mirrors ReferenceConfig
+ * (ordinarylight/renderers/reference/cpu.py:9-21) plus the wavefront knobs of
+ * RendererConfig (ordinarylight/targets/vulkan/api.py:27-717). */
+typedef struct olc_config {
+  int32_t device;               /* CUDA ordinal */
+  uint32_t mode;                /* enum olc_mode */
+  uint32_t max_bounces;         /* 1..64 */
+  uint32_t seed;                /* added to frame_index, as cpu.py:64 does */
+  uint32_t russian_roulette_start;   /* 0 disables RR (production mode) */
+  float russian_roulette_min_survival;
+  uint32_t restir;              /* 1 enables ReSTIR DI at the primary hit */
+  uint32_t restir_candidates;   /* initial RIS candidates (1..64) */
+  uint32_t restir_temporal;     /* temporal reuse passes (0/1) */
+  uint32_t restir_spatial;      /* spatial reuse passes (0..2) */
+  uint32_t restir_neighbours;   /* spatial neighbours per pass */
+  float restir_radius;          /* spatial radius in pixels */
+  uint32_t restir_max_history;  /* temporal M cap, multiple of the candidates */
+  uint32_t block_size;          /* threads per block for the queue kernels */
+  uint32_t stack_depth;         /* shared-memory traversal stack: 16, 24, 32 */
+  uint32_t chunk_paths;         /* paths resident per wavefront chunk; 0 = auto */
+  uint32_t use_graphs;          /* capture the bounce loop as a CUDA graph */
+  uint32_t reserved[8];
+} olc_config;
+
+/* Scene description: host arrays, copied at upload.  Geometry follows the
+ * reference's instancing model: one bottom-level structure per MeshResource
+ * (ordinarylight/targets/vulkan/scene.py:1493-1530), one instance per visible
+ * Mesh in Scene.visible_meshes order (scene/_core.py:1029). */
+typedef struct olc_scene_desc {
+  /* bottom level: meshes in object space */
+  uint32_t num_meshes;
+  const uint32_t* mesh_vertex_offset;    /* [num_meshes + 1] */
+  const uint32_t* mesh_triangle_offset;  /* [num_meshes + 1] */
+  const float* vertices;                 /* [total_vertices * 3] */
+  const float* normals;                  /* [total_vertices * 3] */
+  const uint32_t* indices;               /* [total_triangles * 3], mesh-local */
+  /* top level */
+  uint32_t num_instances;
+  const float* instance_object_to_world; /* [num_instances * 12], row-major 3x4 */
+  const uint32_t* instance_mesh;         /* [num_instances] */
+  const uint32_t* instance_material;     /* [num_instances] */
+  const uint32_t* instance_id;           /* [num_instances] Mesh.id */
+  const uint32_t* instance_primitive_offset; /* [num_instances] packed base */
+  /* materials: 16 floats each:
+   * base_color.rgb, roughness, emission.rgb, metallic, emission_two_sided,
+   * material_id (as float bits), 6 reserved */
+  uint32_t num_materials;
+  const float* materials;
+  /* emissive triangles, 20 floats each, the layout of
+   * Scene.emissive_triangle_data (scene/_core.py:2637-2691):
+   * a.xyz,0  b.xyz,0  c.xyz,0  emission.rgb,area  cdf,pdf,two_sided,0 */
+  uint32_t num_emitters;
+  const float* emitters;
+  float emissive_weight;                 /* Scene.emissive_light_weight */
+  /* analytic lights, 16 floats each, Scene.analytic_light_data layout:
+   * position.xyz,type  direction.xyz,range  color.rgb,intensity  cos_inner,cos_outer,0,0 */
+  uint32_t num_lights;
+  const float* lights;
+  /* environment */
+  uint32_t environment_kind;             /* enum olc_environment_kind */
+  float environment_color[3];            /* colour * intensity */
+  float environment_rotation;
+  uint32_t environment_width, environment_height;
+  const float* environment_image;        /* [h * w * 3] float32 */
+  /* heterogeneous medium (one dense grid in a unit box; 0 = none) */
+  uint32_t volume_present;
+  uint32_t volume_dims[3];               /* nx, ny, nz */
+  const float* volume_density;           /* [nz * ny * nx] */
+  float volume_world_to_box[12];         /* row-major 3x4 world -> [0,1]^3 */
+  float volume_sigma_t_scale;
+  float volume_albedo;
+  float volume_max_density;
+  uint32_t reserved[7];
+} olc_scene_desc;
+
+/* Camera basis computed by the caller in float32 exactly as the reference's
+ * ReferencePathTracer._camera_rays does (path_tracer.py:110-151). */
+typedef struct olc_camera {
+  float position[3];
+  float forward[3];
+  float right[3];
+  float up[3];
+  float half_height;       /* tan(fov/2) or ortho half size */
+  float horizontal_half;   /* panoramic: half horizontal angle (radians) */
+  float vertical_half;     /* panoramic: half vertical angle (radians) */
+  uint32_t projection;     /* enum olc_projection */
+} olc_camera;
+
+/* Per-frame statistics (host). */
+typedef struct olc_render_stats {
+  uint64_t camera_rays;
+  uint64_t extension_rays;   /* closest-hit rays after the camera rays */
+  uint64_t shadow_rays;
+  uint64_t overflow;         /* queue overflows (paths terminated) */
+  uint64_t traversal_errors; /* stack overflows (0 on a healthy run) */
+  float gpu_ms;              /* CUDA-event time of the device work */
+  float raygen_ms, trace_ms, shade_ms, shadow_ms, restir_ms, accumulate_ms;
+  uint32_t chunks;
+  uint32_t restir_history_used;
+  uint32_t reserved[6];
+} olc_render_stats;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Create a context on cfg->device.  Replaces the construction of the
+ * reference's GPU engine (_VulkanGlobalIlluminationEngine,
+ * ordinarylight/targets/vulkan/api.py:844). */
+OLC_API int olc_create(const olc_config* cfg, olc_context** out);
+
+/* Release all device memory; ctx becomes invalid (RendererProtocol.close,
+ * ordinarylight/renderers/base.py:69-71). */
+OLC_API int olc_destroy(olc_context* ctx);
+
+/* Last error message of ctx, or of the calling thread when ctx is NULL. */
+OLC_API const char* olc_last_error(const olc_context* ctx);
+
+/* Library ABI version (OLC_ABI_VERSION). */
+OLC_API int olc_abi_version(void);
+
+/* Update the mutable knobs of a live context (Renderer.reconfigure,
+ * ordinarylight/renderer/_core.py:386-413). */
+OLC_API int olc_reconfigure(olc_context* ctx, const olc_config* cfg);
+
+/* ---- scene residency ------------------------------------------------- */
+
+/* Upload a scene and build its two-level LBVH on the device
+ * (replaces VulkanSceneUploader._build_scene,
+ * ordinarylight/targets/vulkan/scene.py:1322-1560, and upload_window_scene,
+ * ordinarylight/targets/vulkan/core.py:4574-4634).  Transactional: on
+ * failure the previously resident scene stays resident. */
+OLC_API int olc_upload_scene(olc_context* ctx, const olc_scene_desc* scene);
+
+/* Device bytes held by the resident scene (for HBM admission). */
+OLC_API int olc_scene_bytes(const olc_context* ctx, uint64_t* bytes);
+
+/* ---- rendering ------------------------------------------------------- */
+
+/* Render width x height at spp samples for frame_index into out_rgba
+ * ((height, width, 4) float32, linear HDR, channel 3 = 0 like the CPU
+ * reference).  out_is_device selects a device or host destination.
+ * Replaces render_wavefront_outputs (ordinarylight/targets/vulkan/api.py:1252-1451)
+ * behind RendererProtocol.render_frame (ordinarylight/renderers/base.py:56-67). */
+OLC_API int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width,
+               uint32_t height, uint32_t spp, uint32_t frame_index,
+               float* out_rgba, int out_is_device, olc_render_stats* stats);
+
+/* Optional per-pixel products of the first sample's primary hit
+ * (render_products, ordinarylight/renderer/_core.py:768-777).  Each pointer
+ * may be NULL; all are host arrays of height*width entries (normal: *3).
+ * Valid after olc_render with the same size. */
+OLC_API int olc_read_products(olc_context* ctx, uint32_t width, uint32_t height,
+                      float* depth, float* normal, uint32_t* instance_id,
+                      uint32_t* material_id, uint32_t* primitive_id);
+
+/* Forget temporal history (Renderer.reset_sequence ->
+ * reset_output_history, ordinarylight/renderer/_core.py:339-351, :447-451). */
+OLC_API int olc_reset_history(olc_context* ctx);
+
+/* Device timeline of the last olc_render: one record per kernel launch in
+ * launch order, timed with CUDA events on the context's stream (the
+ * per-stage timestamps of the reference's wavefront executor,
+ * ordinarylight/targets/vulkan/core.py:2679-3116, "generate",
+ * "intersect_shade.{b}", "resolve").  items = work units of the launch
+ * (camera rays, rays, hits+misses, shadow rays, path samples, pixels);
+ * misses = rays of the launch's bounce that left the scene. */
+enum olc_stage {
+  OLC_STAGE_RAYGEN = 0,
+  OLC_STAGE_TRACE = 1,
+  OLC_STAGE_RESTIR = 2,
+  OLC_STAGE_SHADE = 3,
+  OLC_STAGE_SHADOW = 4,
+  OLC_STAGE_ACCUMULATE = 5,
+  OLC_STAGE_RESOLVE = 6
+};
+typedef struct olc_launch_record {
+  uint32_t stage;
+  uint32_t bounce;
+  uint32_t chunk;
+  uint32_t misses;
+  uint64_t items;
+  float ms;
+  uint32_t reserved;
+} olc_launch_record;
+OLC_API int olc_frame_profile(const olc_context* ctx, olc_launch_record* records, uint32_t capacity,
+                              uint32_t* count);
+
+/* The CUDA stream (cudaStream_t) the context launches on, for callers that
+ * time or order work against it. */
+OLC_API int olc_stream(const olc_context* ctx, void** stream);
+
+/* ---- tracing primitives (parity and tests) --------------------------- */
+
+/* Closest hit of n world-space rays against the resident scene.  Device
+ * arrays: origins/directions [n*3] float32; outputs instance_id (Mesh.id,
+ * 0xffffffff on miss), primitive (packed triangle index as in
+ * Scene.triangles(), -1 on miss), t (inf on miss).  t_min applies strictly
+ * (t > t_min).  Equal-t ties resolve to the lowest packed index, the rule of
+ * ReferencePathTracer._intersect (path_tracer.py:154-176). */
+OLC_API int olc_trace_closest(olc_context* ctx, uint32_t n, const float* origins,
+                      const float* directions, float t_min,
+                      uint32_t* instance_id, int32_t* primitive, float* t,
+                      float* barycentrics);
+
+/* Occlusion of n rays on (t_min, t_max[i]): occluded[i] = 1 if any hit. */
+OLC_API int olc_trace_occluded(olc_context* ctx, uint32_t n, const float* origins,
+                       const float* directions, float t_min,
+                       const float* t_max, uint8_t* occluded);
+
+/* Camera rays of one sample (device outputs origins/directions [w*h*3]) using
+ * the renderer's counter-based jitter; jitter_override (host, may be NULL)
+ * replaces the random jitter with a fixed (jx, jy) for every pixel. */
+OLC_API int olc_camera_rays(olc_context* ctx, const olc_camera* camera, uint32_t width,
+                    uint32_t height, uint32_t sample, uint32_t frame_index,
+                    const float* jitter_override, float* origins,
+                    float* directions);
+
+/* ---- LBVH building blocks (exposed for bit-exact tests) --------------- */
+
+/* 30-bit Morton codes of the AABB centres of n triangles (device arrays:
+ * tri_vertices [n*9] float32 as a,b,c; codes [n]). */
+OLC_API int olc_morton_codes(olc_context* ctx, uint32_t n, const float* tri_vertices,
+                     uint32_t* codes);
+
+/* Stable LSD radix sort of (key, value) pairs on the low key_bits bits.
+ * Device arrays; in place (keys/values are overwritten with the sorted
+ * sequence).  Ties keep input order, matching numpy.argsort(kind="stable"). */
+OLC_API int olc_radix_sort_pairs(olc_context* ctx, uint32_t n, uint32_t key_bits,
+                         uint32_t* keys, uint32_t* values);
+
+/* Statistics of the resident acceleration structure (host outputs). */
+typedef struct olc_bvh_info {
+  uint32_t blas_count;
+  uint32_t blas_nodes;
+  uint32_t tlas_nodes;
+  uint32_t triangles;
+  uint32_t max_depth;
+  uint32_t reserved[3];
+  double build_ms;
+} olc_bvh_info;
+OLC_API int olc_bvh_info_get(const olc_context* ctx, olc_bvh_info* info);
+
+/* Verify the resident BVH: every triangle reachable once and every child box
+ * inside its parent.  bad (host) receives the number of violations. */
+OLC_API int olc_bvh_validate(olc_context* ctx, uint64_t* bad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OLCUDA_H */

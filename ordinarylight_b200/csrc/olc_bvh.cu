@@ -1,0 +1,623 @@
+// Device LBVH construction: 30-bit Morton codes, a stable LSD radix sort,
+// Karras' parallel hierarchy emission, bottom-up boxes, leaf collapse and a
+// node layout of two child boxes per 64-byte node.
+//
+// Replaces the driver-built hardware BLAS/TLAS of the reference
+// (VulkanSceneUploader._build_scene, ordinarylight/targets/vulkan/scene.py:1484-1560):
+// one BLAS per mesh resource, one TLAS over instances.
+//
+// Bit-exactness: the Morton quantisation uses only correctly rounded float
+// operations without contraction (__fadd_rn/__fsub_rn/__fmul_rn/__fdiv_rn),
+// so the codes equal a float32 host computation of the same formula, and the
+// radix sort is stable, so the permutation equals
+// numpy.argsort(codes, kind="stable").
+#include <algorithm>
+
+#include "olc_internal.h"
+
+namespace olc {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+OLC_D uint32_t f2ord(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+OLC_D float ord2f(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+OLC_HD uint32_t expand_bits10(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_triangle_boxes(const float* __restrict__ vertices, const uint32_t* __restrict__ indices,
+                                 uint32_t nt, float4* lo, float4* hi, float4* centers) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  uint32_t i0 = indices[3 * i + 0], i1 = indices[3 * i + 1], i2 = indices[3 * i + 2];
+  float3 a = f3(vertices[3 * i0 + 0], vertices[3 * i0 + 1], vertices[3 * i0 + 2]);
+  float3 b = f3(vertices[3 * i1 + 0], vertices[3 * i1 + 1], vertices[3 * i1 + 2]);
+  float3 c = f3(vertices[3 * i2 + 0], vertices[3 * i2 + 1], vertices[3 * i2 + 2]);
+  float3 l = fminf3(fminf3(a, b), c), h = fmaxf3(fmaxf3(a, b), c);
+  lo[i] = make_float4(l.x, l.y, l.z, 0.0f);
+  hi[i] = make_float4(h.x, h.y, h.z, 0.0f);
+  centers[i] = make_float4(__fmul_rn(__fadd_rn(l.x, h.x), 0.5f), __fmul_rn(__fadd_rn(l.y, h.y), 0.5f),
+                           __fmul_rn(__fadd_rn(l.z, h.z), 0.5f), 0.0f);
+}
+
+__global__ void k_triangle_boxes_flat(const float* __restrict__ tri, uint32_t nt, float4* lo, float4* hi,
+                                      float4* centers) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt) return;
+  const float* p = tri + 9ull * i;
+  float3 a = f3(p[0], p[1], p[2]), b = f3(p[3], p[4], p[5]), c = f3(p[6], p[7], p[8]);
+  float3 l = fminf3(fminf3(a, b), c), h = fmaxf3(fmaxf3(a, b), c);
+  lo[i] = make_float4(l.x, l.y, l.z, 0.0f);
+  hi[i] = make_float4(h.x, h.y, h.z, 0.0f);
+  centers[i] = make_float4(__fmul_rn(__fadd_rn(l.x, h.x), 0.5f), __fmul_rn(__fadd_rn(l.y, h.y), 0.5f),
+                           __fmul_rn(__fadd_rn(l.z, h.z), 0.5f), 0.0f);
+}
+
+__global__ void k_init_bounds(uint32_t* b) {
+  if (threadIdx.x < 3) b[threadIdx.x] = 0xffffffffu;   // min
+  else if (threadIdx.x < 6) b[threadIdx.x] = 0u;       // max
+}
+
+__global__ void k_center_bounds(const float4* __restrict__ centers, uint32_t n, uint32_t* bounds) {
+  __shared__ uint32_t s[6];
+  if (threadIdx.x < 3) s[threadIdx.x] = 0xffffffffu;
+  else if (threadIdx.x < 6) s[threadIdx.x] = 0u;
+  __syncthreads();
+  uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 c = centers[i];
+    uint32_t o[3] = {f2ord(c.x), f2ord(c.y), f2ord(c.z)};
+    for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], o[k]); mx[k] = max(mx[k], o[k]); }
+  }
+  for (int k = 0; k < 3; ++k) { atomicMin(&s[k], mn[k]); atomicMax(&s[3 + k], mx[k]); }
+  __syncthreads();
+  if (threadIdx.x < 3) atomicMin(&bounds[threadIdx.x], s[threadIdx.x]);
+  else if (threadIdx.x < 6) atomicMax(&bounds[threadIdx.x], s[threadIdx.x]);
+}
+
+__global__ void k_morton(const float4* __restrict__ centers, uint32_t n, const uint32_t* __restrict__ bounds,
+                         uint32_t* codes, uint32_t* vals) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float lo[3], inv[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = ord2f(bounds[k]);
+    float ext = __fsub_rn(ord2f(bounds[3 + k]), lo[k]);
+    inv[k] = ext > 0.0f ? __fdiv_rn(1.0f, ext) : 0.0f;
+  }
+  float4 c = centers[i];
+  float cc[3] = {c.x, c.y, c.z};
+  uint32_t q[3];
+  for (int k = 0; k < 3; ++k) {
+    float v = __fmul_rn(__fmul_rn(__fsub_rn(cc[k], lo[k]), inv[k]), 1024.0f);
+    v = fminf(fmaxf(v, 0.0f), 1023.0f);
+    q[k] = (uint32_t)v;
+  }
+  codes[i] = (expand_bits10(q[0]) << 2) | (expand_bits10(q[1]) << 1) | expand_bits10(q[2]);
+  if (vals) vals[i] = i;
+}
+
+// ---- radix sort ----------------------------------------------------------
+constexpr int kRsWarps = 8;
+constexpr int kRsRounds = 8;
+constexpr int kRsTile = kRsWarps * kRsRounds * 32;  // 2048 items per block
+
+__global__ void k_rs_hist(const uint32_t* __restrict__ keys, uint32_t n, uint32_t shift, uint32_t* hist,
+                          uint32_t nblocks) {
+  __shared__ uint32_t cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t base = blockIdx.x * kRsTile;
+  for (uint32_t i = threadIdx.x; i < (uint32_t)kRsTile; i += blockDim.x) {
+    uint32_t idx = base + i;
+    if (idx < n) atomicAdd(&cnt[(keys[idx] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Exclusive scan of hist[0..len) by one block of 1024 threads.
+__global__ void k_exclusive_scan_1block(uint32_t* data, uint32_t len) {
+  __shared__ uint32_t sums[1024];
+  uint32_t per = (len + blockDim.x - 1) / blockDim.x;
+  uint32_t begin = threadIdx.x * per;
+  uint32_t end = min(begin + per, len);
+  uint32_t local = 0;
+  for (uint32_t i = begin; i < end; ++i) local += data[i];
+  sums[threadIdx.x] = local;
+  __syncthreads();
+  for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+    uint32_t v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0u;
+    __syncthreads();
+    sums[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = sums[threadIdx.x] - local;
+  for (uint32_t i = begin; i < end; ++i) {
+    uint32_t v = data[i];
+    data[i] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_rs_scatter(const uint32_t* __restrict__ keys_in,
+                                                    const uint32_t* __restrict__ vals_in, uint32_t* keys_out,
+                                                    uint32_t* vals_out, uint32_t n, uint32_t shift,
+                                                    const uint32_t* __restrict__ hist, uint32_t nblocks) {
+  __shared__ uint32_t whist[kRsWarps][256];
+  __shared__ uint32_t boff[256];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  for (uint32_t i = threadIdx.x; i < (uint32_t)(kRsWarps * 256); i += blockDim.x) (&whist[0][0])[i] = 0u;
+  __syncthreads();
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint32_t k[kRsRounds], v[kRsRounds], dig[kRsRounds], rank[kRsRounds];
+  const uint32_t base = blockIdx.x * kRsTile + warp * (kRsRounds * 32);
+#pragma unroll
+  for (int r = 0; r < kRsRounds; ++r) {
+    uint32_t idx = base + r * 32 + lane;
+    bool valid = idx < n;
+    k[r] = valid ? keys_in[idx] : 0u;
+    v[r] = valid ? vals_in[idx] : 0u;
+    uint32_t d = valid ? ((k[r] >> shift) & 255u) : 256u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t leader = __ffs(peers) - 1u;
+    uint32_t prior = valid ? whist[warp][d] : 0u;
+    __syncwarp();
+    if (valid && lane == leader) whist[warp][d] = prior + __popc(peers);
+    __syncwarp();
+    dig[r] = d;
+    rank[r] = prior + __popc(peers & lanemask_lt);
+  }
+  __syncthreads();
+  {
+    uint32_t d = threadIdx.x;  // blockDim == 256: one digit per thread
+    uint32_t run = 0;
+    for (int w = 0; w < kRsWarps; ++w) {
+      uint32_t t = whist[w][d];
+      whist[w][d] = run;
+      run += t;
+    }
+    boff[d] = hist[d * nblocks + blockIdx.x];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kRsRounds; ++r) {
+    if (dig[r] < 256u) {
+      uint32_t dst = boff[dig[r]] + whist[warp][dig[r]] + rank[r];
+      keys_out[dst] = k[r];
+      vals_out[dst] = v[r];
+    }
+  }
+}
+
+// ---- Karras hierarchy ----------------------------------------------------
+OLC_D int lbvh_delta(const uint32_t* codes, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = codes[i], b = codes[j];
+  if (a == b) return 32 + __clz((uint32_t)(i ^ j));
+  return __clz(a ^ b);
+}
+
+__global__ void k_karras(const uint32_t* __restrict__ codes, int n, int* left, int* right, int* first, int* last,
+                         int* parent, int* leaf_parent) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (lbvh_delta(codes, n, i, i + 1) - lbvh_delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = lbvh_delta(codes, n, i, i - d);
+  int lmax = 2;
+  while (lbvh_delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (lbvh_delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = lbvh_delta(codes, n, i, j);
+  int s = 0, t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (lbvh_delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  int gamma = i + s * d + min(d, 0);
+  int lo = min(i, j), hi = max(i, j);
+  // child encoding: >= 0 internal, < 0 leaf (~index)
+  int lc = (lo == gamma) ? ~gamma : gamma;
+  int rc = (hi == gamma + 1) ? ~(gamma + 1) : (gamma + 1);
+  left[i] = lc;
+  right[i] = rc;
+  first[i] = lo;
+  last[i] = hi;
+  if (lc < 0) leaf_parent[~lc] = i; else parent[lc] = i;
+  if (rc < 0) leaf_parent[~rc] = i; else parent[rc] = i;
+  if (i == 0) parent[0] = -1;
+}
+
+__global__ void k_gather_sorted_boxes(const uint32_t* __restrict__ order, uint32_t n, const float4* lo,
+                                      const float4* hi, float4* slo, float4* shi) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t o = order[i];
+  slo[i] = lo[o];
+  shi[i] = hi[o];
+}
+
+OLC_D float4 ld_cg(const float4* p) { return __ldcg(p); }
+
+__global__ void k_bottom_up(int n, const int* __restrict__ left, const int* __restrict__ right,
+                            const int* __restrict__ parent, const int* __restrict__ leaf_parent,
+                            const float4* __restrict__ leaf_lo, const float4* __restrict__ leaf_hi, float4* node_lo,
+                            float4* node_hi, uint32_t* flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int p = leaf_parent[i];
+  while (p >= 0) {
+    __threadfence();
+    uint32_t old = atomicAdd(&flags[p], 1u);
+    if (old == 0u) return;
+    __threadfence();
+    int lc = left[p], rc = right[p];
+    float4 llo = lc < 0 ? leaf_lo[~lc] : ld_cg(node_lo + lc);
+    float4 lhi = lc < 0 ? leaf_hi[~lc] : ld_cg(node_hi + lc);
+    float4 rlo = rc < 0 ? leaf_lo[~rc] : ld_cg(node_lo + rc);
+    float4 rhi = rc < 0 ? leaf_hi[~rc] : ld_cg(node_hi + rc);
+    node_lo[p] = make_float4(fminf(llo.x, rlo.x), fminf(llo.y, rlo.y), fminf(llo.z, rlo.z), 0.0f);
+    node_hi[p] = make_float4(fmaxf(lhi.x, rhi.x), fmaxf(lhi.y, rhi.y), fmaxf(lhi.z, rhi.z), 0.0f);
+    p = parent[p];
+  }
+}
+
+// Emit final nodes.  blas: leaves reference slot ranges (collapse subtrees of
+// at most leaf_max leaves); tlas: leaves reference instance indices.
+__global__ void k_emit_nodes(int n, const int* __restrict__ left, const int* __restrict__ right,
+                             const int* __restrict__ first, const int* __restrict__ last,
+                             const float4* __restrict__ leaf_lo, const float4* __restrict__ leaf_hi,
+                             const float4* __restrict__ node_lo, const float4* __restrict__ node_hi,
+                             const uint32_t* __restrict__ sorted_vals, int is_tlas, uint32_t leaf_max,
+                             BvhNode* nodes, uint32_t node_base, uint32_t slot_base) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int ch[2] = {left[i], right[i]};
+  float4 lo[2], hi[2];
+  int ref[2];
+  for (int s = 0; s < 2; ++s) {
+    int c = ch[s];
+    if (c < 0) {
+      int leaf = ~c;
+      lo[s] = leaf_lo[leaf];
+      hi[s] = leaf_hi[leaf];
+      ref[s] = is_tlas ? olc_make_leaf(sorted_vals[leaf], 1u) : olc_make_leaf(slot_base + (uint32_t)leaf, 1u);
+    } else {
+      lo[s] = node_lo[c];
+      hi[s] = node_hi[c];
+      uint32_t size = (uint32_t)(last[c] - first[c] + 1);
+      if (!is_tlas && size <= leaf_max) ref[s] = olc_make_leaf(slot_base + (uint32_t)first[c], size);
+      else ref[s] = (int)(node_base + (uint32_t)c);
+    }
+  }
+  BvhNode nd;
+  nd.a = make_float4(lo[0].x, hi[0].x, lo[0].y, hi[0].y);
+  nd.b = make_float4(lo[1].x, hi[1].x, lo[1].y, hi[1].y);
+  nd.c = make_float4(lo[0].z, hi[0].z, lo[1].z, hi[1].z);
+  nd.d = make_int4(ref[0], ref[1], 0, 0);
+  nodes[node_base + i] = nd;
+}
+
+// A structure with a single primitive: one node, child 1 empty.
+__global__ void k_single_leaf_node(const float4* lo, const float4* hi, int is_tlas, const uint32_t* sorted_vals,
+                                   BvhNode* nodes, uint32_t node_base, uint32_t slot_base, uint32_t n) {
+  BvhNode nd;
+  if (n == 0) {
+    const float inf = CUDART_INF_F;
+    nd.a = make_float4(inf, -inf, inf, -inf);
+    nd.b = nd.a;
+    nd.c = make_float4(inf, -inf, inf, -inf);
+    nd.d = make_int4(OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, 0, 0);
+  } else {
+    const float inf = CUDART_INF_F;
+    nd.a = make_float4(lo[0].x, hi[0].x, lo[0].y, hi[0].y);
+    nd.b = make_float4(inf, -inf, inf, -inf);
+    nd.c = make_float4(lo[0].z, hi[0].z, inf, -inf);
+    nd.d = make_int4(is_tlas ? olc_make_leaf(sorted_vals[0], 1u) : olc_make_leaf(slot_base, 1u),
+                     OLC_EMPTY_CHILD, 0, 0);
+  }
+  nodes[node_base] = nd;
+}
+
+__global__ void k_reorder_triangles(const uint32_t* __restrict__ order, uint32_t nt,
+                                    const float* __restrict__ vertices, const float* __restrict__ normals,
+                                    const uint32_t* __restrict__ indices, float4* tri_verts,
+                                    float4* tri_normals, uint32_t* tri_index, uint32_t slot_base) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nt) return;
+  uint32_t t = order[s];
+  uint32_t dst = slot_base + s;
+  for (int k = 0; k < 3; ++k) {
+    uint32_t vi = indices[3 * t + k];
+    tri_verts[3ull * dst + k] = make_float4(vertices[3 * vi + 0], vertices[3 * vi + 1], vertices[3 * vi + 2], 0.0f);
+    tri_normals[3ull * dst + k] = make_float4(normals[3 * vi + 0], normals[3 * vi + 1], normals[3 * vi + 2], 0.0f);
+  }
+  tri_index[dst] = t;
+}
+
+__global__ void k_instance_boxes(const InstanceRec* __restrict__ inst, const float* __restrict__ o2w, uint32_t n,
+                                 const BvhNode* __restrict__ nodes, float4* lo, float4* hi, float4* centers) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BvhNode r = nodes[inst[i].blas_root];
+  float3 blo = f3(fminf(r.a.x, r.b.x), fminf(r.a.z, r.b.z), fminf(r.c.x, r.c.z));
+  float3 bhi = f3(fmaxf(r.a.y, r.b.y), fmaxf(r.a.w, r.b.w), fmaxf(r.c.y, r.c.w));
+  Affine m;
+  const float* p = o2w + 12ull * i;
+  m.r0 = make_float4(p[0], p[1], p[2], p[3]);
+  m.r1 = make_float4(p[4], p[5], p[6], p[7]);
+  m.r2 = make_float4(p[8], p[9], p[10], p[11]);
+  float3 wl = f3(CUDART_INF_F, CUDART_INF_F, CUDART_INF_F), wh = -wl;
+  for (int c = 0; c < 8; ++c) {
+    float3 q = f3((c & 1) ? bhi.x : blo.x, (c & 2) ? bhi.y : blo.y, (c & 4) ? bhi.z : blo.z);
+    float3 w = xform_point(m, q);
+    wl = fminf3(wl, w);
+    wh = fmaxf3(wh, w);
+  }
+  // Pad by a relative epsilon: the transformed ray of the traversal is not
+  // bit-identical to the forward transform of the corners.
+  float mag = fmaxf(fmaxf(max3(fmaxf3(wh, -wl)), max3(wh - wl)), 1e-3f);
+  float3 pad = f3(mag, mag, mag) * 1e-5f;
+  wl = wl - pad;
+  wh = wh + pad;
+  lo[i] = make_float4(wl.x, wl.y, wl.z, 0.0f);
+  hi[i] = make_float4(wh.x, wh.y, wh.z, 0.0f);
+  centers[i] = make_float4(__fmul_rn(__fadd_rn(wl.x, wh.x), 0.5f), __fmul_rn(__fadd_rn(wl.y, wh.y), 0.5f),
+                           __fmul_rn(__fadd_rn(wl.z, wh.z), 0.5f), 0.0f);
+}
+
+inline uint32_t blocks_for(uint64_t n, int threads = kThreads) { return (uint32_t)((n + threads - 1) / threads); }
+
+// Common tail of a BLAS/TLAS build after boxes and centres exist.
+uint32_t build_hierarchy(uint32_t n, BuildScratch& sc, int is_tlas, uint32_t leaf_max, BvhNode* nodes,
+                         uint32_t node_base, uint32_t slot_base, cudaStream_t stream) {
+  if (n <= 1) {
+    if (n == 1) {
+      // sorted order is the identity
+      uint32_t zero = 0;
+      OLC_CUDA(cudaMemcpyAsync(sc.vals.as<uint32_t>(), &zero, sizeof(zero), cudaMemcpyHostToDevice, stream));
+    }
+    k_single_leaf_node<<<1, 1, 0, stream>>>(sc.boxes_lo.as<float4>(), sc.boxes_hi.as<float4>(), is_tlas,
+                                            sc.vals.as<uint32_t>(), nodes, node_base, slot_base, n);
+    OLC_LAUNCH_CHECK("k_single_leaf_node");
+    OLC_CUDA(cudaStreamSynchronize(stream));
+    return node_base;
+  }
+  uint32_t* bounds = sc.bounds.as<uint32_t>();
+  morton_codes(sc.centers.as<float4>(), n, bounds, nullptr, stream);
+  k_morton<<<blocks_for(n), kThreads, 0, stream>>>(sc.centers.as<float4>(), n, bounds, sc.keys.as<uint32_t>(),
+                                                     sc.vals.as<uint32_t>());
+  OLC_LAUNCH_CHECK("k_morton");
+  radix_sort_pairs(sc.keys.as<uint32_t>(), sc.vals.as<uint32_t>(), sc.keys_alt.as<uint32_t>(),
+                   sc.vals_alt.as<uint32_t>(), sc.hist.as<uint32_t>(), n, 30, stream);
+  k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(sc.keys.as<uint32_t>(), (int)n, sc.left.as<int>(),
+                                                         sc.right.as<int>(), sc.first.as<int>(), sc.last.as<int>(),
+                                                         sc.parent.as<int>(), sc.leaf_parent.as<int>());
+  OLC_LAUNCH_CHECK("k_karras");
+  k_gather_sorted_boxes<<<blocks_for(n), kThreads, 0, stream>>>(sc.vals.as<uint32_t>(), n, sc.boxes_lo.as<float4>(),
+                                                                  sc.boxes_hi.as<float4>(), sc.sorted_lo.as<float4>(),
+                                                                  sc.sorted_hi.as<float4>());
+  OLC_LAUNCH_CHECK("k_gather_sorted_boxes");
+  OLC_CUDA(cudaMemsetAsync(sc.flags.get(), 0, sizeof(uint32_t) * (n - 1), stream));
+  k_bottom_up<<<blocks_for(n), kThreads, 0, stream>>>((int)n, sc.left.as<int>(), sc.right.as<int>(),
+                                                        sc.parent.as<int>(), sc.leaf_parent.as<int>(),
+                                                        sc.sorted_lo.as<float4>(), sc.sorted_hi.as<float4>(),
+                                                        sc.node_lo.as<float4>(), sc.node_hi.as<float4>(),
+                                                        sc.flags.as<uint32_t>());
+  OLC_LAUNCH_CHECK("k_bottom_up");
+  k_emit_nodes<<<blocks_for(n - 1), kThreads, 0, stream>>>(
+      (int)n, sc.left.as<int>(), sc.right.as<int>(), sc.first.as<int>(), sc.last.as<int>(),
+      sc.sorted_lo.as<float4>(), sc.sorted_hi.as<float4>(), sc.node_lo.as<float4>(), sc.node_hi.as<float4>(),
+      sc.vals.as<uint32_t>(), is_tlas, leaf_max, nodes, node_base, slot_base);
+  OLC_LAUNCH_CHECK("k_emit_nodes");
+  return node_base;  // Karras root is internal node 0
+}
+
+}  // namespace
+
+void BuildScratch::ensure(size_t n) {
+  if (n <= capacity) return;
+  size_t c = std::max<size_t>(n, 1024);
+  boxes_lo.allocate(c * 16);
+  boxes_hi.allocate(c * 16);
+  centers.allocate(c * 16);
+  bounds.allocate(64);
+  keys.allocate(c * 4);
+  vals.allocate(c * 4);
+  keys_alt.allocate(c * 4);
+  vals_alt.allocate(c * 4);
+  hist.allocate(radix_sort_hist_words((uint32_t)c) * 4);
+  sorted_lo.allocate(c * 16);
+  sorted_hi.allocate(c * 16);
+  left.allocate(c * 4);
+  right.allocate(c * 4);
+  first.allocate(c * 4);
+  last.allocate(c * 4);
+  parent.allocate(c * 4);
+  leaf_parent.allocate(c * 4);
+  flags.allocate(c * 4);
+  node_lo.allocate(c * 16);
+  node_hi.allocate(c * 16);
+  capacity = c;
+}
+
+size_t radix_sort_hist_words(uint32_t n) {
+  uint32_t nblocks = (n + kRsTile - 1) / kRsTile;
+  return (size_t)256 * std::max<uint32_t>(nblocks, 1u);
+}
+
+void morton_codes(const float4* centers, uint32_t n, uint32_t* bounds, uint32_t* codes, cudaStream_t stream) {
+  k_init_bounds<<<1, 32, 0, stream>>>(bounds);
+  OLC_LAUNCH_CHECK("k_init_bounds");
+  uint32_t grid = std::min<uint32_t>(blocks_for(n), 148u * 8u);
+  k_center_bounds<<<std::max<uint32_t>(grid, 1u), kThreads, 0, stream>>>(centers, n, bounds);
+  OLC_LAUNCH_CHECK("k_center_bounds");
+  if (codes) {
+    k_morton<<<blocks_for(n), kThreads, 0, stream>>>(centers, n, bounds, codes, nullptr);
+    OLC_LAUNCH_CHECK("k_morton");
+  }
+}
+
+void triangle_centers_flat(const float* tri, uint32_t n, float4* lo, float4* hi, float4* centers,
+                           cudaStream_t stream) {
+  k_triangle_boxes_flat<<<blocks_for(n), kThreads, 0, stream>>>(tri, n, lo, hi, centers);
+  OLC_LAUNCH_CHECK("k_triangle_boxes_flat");
+}
+
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, uint32_t* hist,
+                      uint32_t n, uint32_t key_bits, cudaStream_t stream) {
+  if (n <= 1) return;
+  uint32_t nblocks = (n + kRsTile - 1) / kRsTile;
+  uint32_t passes = (key_bits + 7) / 8;
+  uint32_t* kin = keys;
+  uint32_t* vin = vals;
+  uint32_t* kout = keys_alt;
+  uint32_t* vout = vals_alt;
+  for (uint32_t p = 0; p < passes; ++p) {
+    uint32_t shift = 8 * p;
+    k_rs_hist<<<nblocks, 256, 0, stream>>>(kin, n, shift, hist, nblocks);
+    OLC_LAUNCH_CHECK("k_rs_hist");
+    k_exclusive_scan_1block<<<1, 1024, 0, stream>>>(hist, 256 * nblocks);
+    OLC_LAUNCH_CHECK("k_exclusive_scan_1block");
+    k_rs_scatter<<<nblocks, 256, 0, stream>>>(kin, vin, kout, vout, n, shift, hist, nblocks);
+    OLC_LAUNCH_CHECK("k_rs_scatter");
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  if (kin != keys) {
+    OLC_CUDA(cudaMemcpyAsync(keys, kin, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream));
+    OLC_CUDA(cudaMemcpyAsync(vals, vin, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream));
+  }
+}
+
+uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_t node_base, float4* tri_verts,
+                    float4* tri_normals, uint32_t* tri_index, uint32_t slot_base, uint32_t leaf_max,
+                    cudaStream_t stream) {
+  uint32_t n = d.num_triangles;
+  sc.ensure(std::max<uint32_t>(n, 1u));
+  if (n > 0) {
+    k_triangle_boxes<<<blocks_for(n), kThreads, 0, stream>>>(d.vertices, d.indices, n, sc.boxes_lo.as<float4>(),
+                                                               sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
+    OLC_LAUNCH_CHECK("k_triangle_boxes");
+  }
+  uint32_t root = build_hierarchy(n, sc, 0, leaf_max, nodes, node_base, slot_base, stream);
+  if (n > 0) {
+    k_reorder_triangles<<<blocks_for(n), kThreads, 0, stream>>>(sc.vals.as<uint32_t>(), n, d.vertices, d.normals,
+                                                                  d.indices, tri_verts, tri_normals, tri_index,
+                                                                  slot_base);
+    OLC_LAUNCH_CHECK("k_reorder_triangles");
+  }
+  return root;
+}
+
+uint32_t build_tlas(const InstanceRec* instances, const float* o2w, uint32_t n, const BvhNode* nodes_in,
+                    BuildScratch& sc, BvhNode* nodes, uint32_t node_base, cudaStream_t stream) {
+  sc.ensure(std::max<uint32_t>(n, 1u));
+  if (n > 0) {
+    k_instance_boxes<<<blocks_for(n), kThreads, 0, stream>>>(instances, o2w, n, nodes_in, sc.boxes_lo.as<float4>(),
+                                                               sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
+    OLC_LAUNCH_CHECK("k_instance_boxes");
+  }
+  return build_hierarchy(n, sc, 1, 1, nodes, node_base, 0, stream);
+}
+
+// ---- validation ----------------------------------------------------------
+namespace {
+// Walk every BLAS subtree from each instance root; count how often each slot
+// is reached and whether child boxes nest (within float slack).
+__global__ void k_validate(SceneView s, uint32_t num_instances, uint32_t* slot_hits, unsigned long long* bad,
+                           const uint8_t* seen_blas_first) {
+  uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
+  if (inst >= num_instances) return;
+  if (!seen_blas_first[inst]) return;  // one walker per distinct BLAS
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = (int)s.instances[inst].blas_root;
+  while (sp > 0) {
+    int node = stack[--sp];
+    if (node >= 0) {
+      BvhNode nd = s.nodes[node];
+      int ch[2] = {nd.d.x, nd.d.y};
+      for (int c = 0; c < 2; ++c) {
+        if (ch[c] == OLC_EMPTY_CHILD) continue;
+        if (ch[c] >= 0) {
+          BvhNode cn = s.nodes[ch[c]];
+          // child's own children boxes must lie inside the box stored for it
+          float lx = c == 0 ? nd.a.x : nd.b.x, hx = c == 0 ? nd.a.y : nd.b.y;
+          float ly = c == 0 ? nd.a.z : nd.b.z, hy = c == 0 ? nd.a.w : nd.b.w;
+          float lz = c == 0 ? nd.c.x : nd.c.z, hz = c == 0 ? nd.c.y : nd.c.w;
+          for (int g = 0; g < 2; ++g) {
+            int gc = g == 0 ? cn.d.x : cn.d.y;
+            if (gc == OLC_EMPTY_CHILD) continue;
+            float glx = g == 0 ? cn.a.x : cn.b.x, ghx = g == 0 ? cn.a.y : cn.b.y;
+            float gly = g == 0 ? cn.a.z : cn.b.z, ghy = g == 0 ? cn.a.w : cn.b.w;
+            float glz = g == 0 ? cn.c.x : cn.c.z, ghz = g == 0 ? cn.c.y : cn.c.w;
+            if (glx < lx || gly < ly || glz < lz || ghx > hx || ghy > hy || ghz > hz) atomicAdd(bad, 1ull);
+          }
+          if (sp < 128) stack[sp++] = ch[c]; else atomicAdd(bad, 1ull);
+        } else {
+          uint32_t f = olc_leaf_first(ch[c]), cnt = olc_leaf_count(ch[c]);
+          for (uint32_t k = 0; k < cnt; ++k) atomicAdd(&slot_hits[f + k], 1u);
+        }
+      }
+    }
+  }
+}
+__global__ void k_count_bad_slots(const uint32_t* slot_hits, uint32_t n, unsigned long long* bad) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && slot_hits[i] != 1u) atomicAdd(bad, 1ull);
+}
+}  // namespace
+
+uint64_t validate_bvh(const SceneView& s, uint32_t total_slots, uint32_t num_instances,
+                      const uint32_t* /*blas_slot_begin*/, const uint32_t* /*blas_slot_end*/, cudaStream_t stream) {
+  // mark the first instance of every distinct BLAS root on the host
+  std::vector<InstanceRec> inst(num_instances);
+  if (num_instances)
+    OLC_CUDA(cudaMemcpyAsync(inst.data(), s.instances, sizeof(InstanceRec) * num_instances, cudaMemcpyDeviceToHost,
+                             stream));
+  OLC_CUDA(cudaStreamSynchronize(stream));
+  std::vector<uint8_t> first(num_instances, 0);
+  std::vector<uint32_t> roots;
+  for (uint32_t i = 0; i < num_instances; ++i) {
+    if (std::find(roots.begin(), roots.end(), inst[i].blas_root) == roots.end()) {
+      roots.push_back(inst[i].blas_root);
+      first[i] = 1;
+    }
+  }
+  DeviceBuffer hits(std::max<size_t>(total_slots, 1) * 4), bad(8), seen(std::max<size_t>(num_instances, 1));
+  OLC_CUDA(cudaMemsetAsync(hits.get(), 0, std::max<size_t>(total_slots, 1) * 4, stream));
+  OLC_CUDA(cudaMemsetAsync(bad.get(), 0, 8, stream));
+  if (num_instances)
+    OLC_CUDA(cudaMemcpyAsync(seen.get(), first.data(), num_instances, cudaMemcpyHostToDevice, stream));
+  if (num_instances) {
+    k_validate<<<blocks_for(num_instances, 64), 64, 0, stream>>>(s, num_instances, hits.as<uint32_t>(),
+                                                                 bad.as<unsigned long long>(), seen.as<uint8_t>());
+    OLC_LAUNCH_CHECK("k_validate");
+  }
+  if (total_slots) {
+    k_count_bad_slots<<<blocks_for(total_slots), kThreads, 0, stream>>>(hits.as<uint32_t>(), total_slots,
+                                                                          bad.as<unsigned long long>());
+    OLC_LAUNCH_CHECK("k_count_bad_slots");
+  }
+  unsigned long long h = 0;
+  OLC_CUDA(cudaMemcpyAsync(&h, bad.get(), 8, cudaMemcpyDeviceToHost, stream));
+  OLC_CUDA(cudaStreamSynchronize(stream));
+  return h;
+}
+
+}  // namespace olc

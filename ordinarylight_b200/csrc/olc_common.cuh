@@ -1,0 +1,278 @@
+// Shared device definitions: vector math, the counter-based sampling
+// sequence, and the HBM layouts of the resident scene and wavefront queues.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#define OLC_HD __host__ __device__ __forceinline__
+#define OLC_D __device__ __forceinline__
+
+// ---------------------------------------------------------------------------
+// float3 helpers
+// ---------------------------------------------------------------------------
+OLC_HD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+OLC_HD float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+OLC_HD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+OLC_HD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+OLC_HD float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+OLC_HD float3 operator*(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+OLC_HD float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+OLC_HD float3 operator*(float s, float3 a) { return f3(a.x * s, a.y * s, a.z * s); }
+OLC_HD float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+OLC_HD float3& operator+=(float3& a, float3 b) { a = a + b; return a; }
+OLC_HD float3& operator*=(float3& a, float3 b) { a = a * b; return a; }
+OLC_HD float3& operator*=(float3& a, float s) { a = a * s; return a; }
+OLC_HD float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+OLC_HD float3 cross(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+OLC_HD float length(float3 a) { return sqrtf(dot(a, a)); }
+OLC_HD float3 normalize(float3 a) {
+  float l = sqrtf(dot(a, a));
+  return l > 0.0f ? a * (1.0f / l) : a;
+}
+OLC_HD float3 fminf3(float3 a, float3 b) { return f3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+OLC_HD float3 fmaxf3(float3 a, float3 b) { return f3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+OLC_HD float max3(float3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+OLC_HD float get(float3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+OLC_HD float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+OLC_HD float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+OLC_HD float3 lerp3(float3 a, float3 b, float t) { return a + (b - a) * t; }
+
+// Affine 3x4 row-major transform.
+struct Affine {
+  float4 r0, r1, r2;
+};
+OLC_HD float3 xform_point(const Affine& m, float3 p) {
+  return f3(m.r0.x * p.x + m.r0.y * p.y + m.r0.z * p.z + m.r0.w,
+            m.r1.x * p.x + m.r1.y * p.y + m.r1.z * p.z + m.r1.w,
+            m.r2.x * p.x + m.r2.y * p.y + m.r2.z * p.z + m.r2.w);
+}
+OLC_HD float3 xform_vector(const Affine& m, float3 v) {
+  return f3(m.r0.x * v.x + m.r0.y * v.y + m.r0.z * v.z,
+            m.r1.x * v.x + m.r1.y * v.y + m.r1.z * v.z,
+            m.r2.x * v.x + m.r2.y * v.y + m.r2.z * v.z);
+}
+// Normal transform by the inverse transpose: given W = world->object,
+// n_world = W^T n_object.
+OLC_HD float3 xform_normal_by_inverse(const Affine& w2o, float3 n) {
+  return f3(w2o.r0.x * n.x + w2o.r1.x * n.y + w2o.r2.x * n.z,
+            w2o.r0.y * n.x + w2o.r1.y * n.y + w2o.r2.y * n.z,
+            w2o.r0.z * n.x + w2o.r1.z * n.y + w2o.r2.z * n.z);
+}
+
+// ---------------------------------------------------------------------------
+// Counter-based sampling sequence.
+//
+// The mixing function is the 32-bit integer hash the reference wavefront uses
+// for its per-path seed (waveHash, ordinarylight/shaders/wavefront_generate.comp:71-79:
+// xor-shift 16, multiply 0x7feb352d, xor-shift 15, multiply 0x846ca68b,
+// xor-shift 16 — C. Wellons' published "lowbias32"), and the per-draw
+// generator is the PCG-RXS-M-XS 32-bit step of randomFloat
+// (ordinarylight/shaders/transport_v1/sampling.glsl:16-22; M. O'Neill, PCG).
+// Unlike the reference, the stream is re-keyed for every bounce from
+// (pixel, sample, bounce, frame), so a path's random numbers never depend on
+// how many numbers an earlier bounce consumed or on which queue slot or
+// launch processed it.
+// ---------------------------------------------------------------------------
+OLC_HD uint32_t olc_hash(uint32_t v) {
+  v ^= v >> 16;
+  v *= 0x7feb352du;
+  v ^= v >> 15;
+  v *= 0x846ca68bu;
+  v ^= v >> 16;
+  return v;
+}
+
+// Seed of (pixel, sample, frame).  The reference combines
+// H(H(pixel ^ H(frame) ^ H(sample + 1))) (wavefront_generate.comp:113-116),
+// whose xor makes (frame f, sample s) and (frame s + 1, sample f - 1) share a
+// stream (for example every pixel of frame 1 sample 0 equals frame 2
+// sample 1... and pixel 0 of frame 1 sample 0 gets jitter 0).  Nesting the
+// pixel/frame hash before mixing in the sample removes that symmetry:
+// H(H(pixel ^ H(frame)) ^ H(sample + 1)).
+OLC_HD uint32_t olc_path_seed(uint32_t pixel, uint32_t sample, uint32_t frame) {
+  return olc_hash(olc_hash(pixel ^ olc_hash(frame)) ^ olc_hash(sample + 1u));
+}
+
+// Stream state of one bounce of one path.
+OLC_HD uint32_t olc_bounce_state(uint32_t path_seed, uint32_t bounce) {
+  return olc_hash(path_seed ^ olc_hash(bounce * 0x9e3779b9u + 0x632be5abu));
+}
+
+// One PCG-RXS-M-XS step; returns a float in [0, 1).
+OLC_HD float olc_rand(uint32_t& state) {
+  state = state * 747796405u + 2891336453u;
+  uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+  word = (word >> 22u) ^ word;
+  return (float)word * (1.0f / 4294967296.0f);
+}
+
+// Camera jitter of (pixel, sample, frame): two hash steps of the path seed,
+// the reference raygen's jitter draws (wavefront_generate.comp:117-121).
+OLC_HD float2 olc_camera_jitter(uint32_t pixel, uint32_t sample, uint32_t frame) {
+  uint32_t s = olc_path_seed(pixel, sample, frame);
+  s = olc_hash(s);
+  float jx = (float)s * (1.0f / 4294967296.0f);
+  s = olc_hash(s);
+  float jy = (float)s * (1.0f / 4294967296.0f);
+  return make_float2(jx, jy);
+}
+
+// ---------------------------------------------------------------------------
+// Resident scene layout in HBM.
+// ---------------------------------------------------------------------------
+// BVH2 node, 64 bytes, four 16-byte loads: both child boxes are stored in the
+// parent so one node fetch tests two children.
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, -, -)   child >= 0: node index; child < 0: leaf
+struct __align__(16) BvhNode {
+  float4 a, b, c;
+  int4 d;
+};
+// Leaf reference: ~((first << 3) | (count - 1)), count in 1..8.
+#define OLC_LEAF_MAX 8
+OLC_HD int olc_make_leaf(uint32_t first, uint32_t count) { return ~(int)((first << 3) | (count - 1u)); }
+OLC_HD uint32_t olc_leaf_first(int ref) { return ((uint32_t)(~ref)) >> 3; }
+OLC_HD uint32_t olc_leaf_count(int ref) { return (((uint32_t)(~ref)) & 7u) + 1u; }
+#define OLC_EMPTY_CHILD ((int)0x80000000)
+
+// Instance record, 112 bytes: world->object 3x4 and identity/offsets (the
+// 64 bytes traversal reads), then object->world 3x4 for shading.
+struct __align__(16) InstanceRec {
+  float4 w2o0, w2o1, w2o2;
+  uint32_t blas_root;      // node index of the instance's BLAS root
+  uint32_t material;       // material table index
+  uint32_t prim_offset;    // packed triangle base (Scene.triangles order)
+  uint32_t instance_id;    // Mesh.id
+  float4 o2w0, o2w1, o2w2;
+};
+
+// Material record, 32 bytes.
+struct __align__(16) MaterialRec {
+  float4 base_rough;       // base_color.rgb, roughness
+  float4 emit_metal;       // emission.rgb, metallic
+};
+struct __align__(16) MaterialAux {
+  uint32_t two_sided;
+  uint32_t material_id;
+  uint32_t pad0, pad1;
+};
+
+// Emitter record (area light), 80 bytes like Scene.emissive_triangle_data.
+struct __align__(16) EmitterRec {
+  float4 a, b, c;
+  float4 emission_area;    // emission.rgb, area
+  float4 dist;             // cdf, pdf, two_sided, 0
+};
+
+struct __align__(16) LightRec {
+  float4 position_type;
+  float4 direction_range;
+  float4 color_intensity;
+  float4 spot;
+};
+
+struct SceneView {
+  const BvhNode* nodes;          // BLAS and TLAS nodes, one pool
+  const float4* tri_verts;       // 3 float4 per triangle slot (object space)
+  const float4* tri_normals;     // 3 float4 per triangle slot (object space)
+  const uint32_t* tri_index;     // slot -> mesh-local triangle index
+  const InstanceRec* instances;
+  const MaterialRec* materials;
+  const MaterialAux* material_aux;
+  const EmitterRec* emitters;
+  const LightRec* lights;
+  const float* env_image;        // equirect RGB
+  const float* volume;           // density grid
+  uint32_t tlas_root;
+  uint32_t num_instances;
+  uint32_t num_emitters;
+  uint32_t num_lights;
+  float emissive_weight;
+  uint32_t env_kind;
+  float3 env_color;
+  float env_rotation;
+  uint32_t env_w, env_h;
+  uint32_t volume_present;
+  uint32_t vol_nx, vol_ny, vol_nz;
+  Affine vol_world_to_box;
+  float vol_sigma_t_scale;
+  float vol_albedo;
+  float vol_max_density;
+};
+
+// ---------------------------------------------------------------------------
+// Wavefront queues (structure of arrays, 16-byte elements).
+// ---------------------------------------------------------------------------
+struct RayQueue {
+  float4* origin_tmin;     // origin.xyz, t_min
+  float4* dir_tmax;        // direction.xyz, t_max
+  uint32_t* path;          // path slot
+};
+
+struct HitBuf {
+  float4* tuv_slot;        // t, u, v, triangle slot bits (t < 0: miss)
+  uint32_t* instance;      // instance index
+};
+
+struct ShadowQueue {
+  float4* origin_tmax;     // origin.xyz, t_max
+  float4* dir_path;        // direction.xyz, path slot bits
+  float4* contrib;         // unoccluded contribution rgb
+};
+
+struct PathState {
+  float4* throughput;      // rgb, previous BSDF pdf
+  float4* radiance;        // rgb, unused
+  uint4* meta;             // pixel, sample, bounce | flags << 8, job
+};
+
+#define OLC_PATH_FLAG_PREV_NEE 1u     // the previous vertex sampled area lights
+#define OLC_PATH_FLAG_PREV_RESTIR 2u  // area lights of the previous vertex came from ReSTIR
+
+// Fixed-point scale of the per-pixel radiance accumulator.  Sums of
+// non-negative samples in unsigned 64-bit fixed point are independent of the
+// order of the atomic additions, so every launch shape, chunking and batch
+// mix produces the same bits.
+#define OLC_ACCUM_SHIFT 28
+#define OLC_ACCUM_SCALE 268435456.0f
+#define OLC_SAMPLE_CLAMP 1.0e7f
+
+// Per-frame parameters, read by every wavefront kernel from device memory so
+// a captured graph can be replayed for a new frame after one copy.
+struct FrameParams {
+  float4 cam_pos;          // xyz, x scale (aspect*half_height | half horizontal angle)
+  float4 cam_forward;      // xyz, y scale (half_height | half vertical angle)
+  float4 cam_right;        // xyz, 0
+  float4 cam_up;           // xyz, 0
+  uint32_t projection;
+  uint32_t width, height;
+  uint32_t spp;
+  uint32_t frame;          // seed + frame_index
+  uint32_t npix;
+  uint32_t max_bounces;
+  uint32_t mode;
+  uint32_t rr_start;
+  float rr_min_survival;
+  uint32_t restir;
+  uint32_t pad;
+};
+
+// Work counters kept in device memory, zeroed once per chunk.
+#define OLC_MAX_BOUNCES 64
+struct Counters {
+  uint32_t queue_count[OLC_MAX_BOUNCES + 2];    // rays in the queue of each bounce
+  uint32_t shadow_count[OLC_MAX_BOUNCES + 2];   // shadow rays emitted at each bounce
+  uint32_t closest_cursor[OLC_MAX_BOUNCES + 2]; // persistent closest-hit work cursor
+  uint32_t shadow_cursor[OLC_MAX_BOUNCES + 2];  // persistent any-hit work cursor
+  uint32_t miss_count[OLC_MAX_BOUNCES + 2];     // rays of each bounce that left the scene
+  uint32_t overflow;
+  uint32_t traversal_errors;
+  uint32_t nan_samples;
+  uint32_t pad;
+};

@@ -1,0 +1,118 @@
+// Host-side internals shared by the translation units of libolcuda.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "olc_common.cuh"
+
+namespace olc {
+
+// Error carrying an olc_status code across the C++ layers; the C ABI
+// converts it into a return code plus last-error string.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int code = (e == cudaErrorMemoryAllocation) ? 5 /*OLC_ERR_MEMORY*/ : 4 /*OLC_ERR_CUDA*/;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+#define OLC_CUDA(call) ::olc::check_cuda((call), #call)
+#define OLC_LAUNCH_CHECK(name) ::olc::check_cuda(cudaGetLastError(), name)
+
+// Owning device allocation.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t bytes) { allocate(bytes); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) { o.ptr_ = nullptr; o.bytes_ = 0; }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    if (this != &o) { release(); ptr_ = o.ptr_; bytes_ = o.bytes_; o.ptr_ = nullptr; o.bytes_ = 0; }
+    return *this;
+  }
+  void allocate(size_t bytes) {
+    release();
+    if (bytes == 0) return;
+    OLC_CUDA(cudaMalloc(&ptr_, bytes));
+    bytes_ = bytes;
+  }
+  // Grow-only reallocation (contents are not preserved).
+  void ensure(size_t bytes) { if (bytes > bytes_) allocate(bytes); }
+  void release() {
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(ptr_); }
+  void* get() const { return ptr_; }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// ---- LBVH construction (olc_bvh.cu) --------------------------------------
+
+// Scratch for one LBVH build of up to n primitives.
+struct BuildScratch {
+  DeviceBuffer boxes_lo, boxes_hi;   // float4 per primitive (unsorted)
+  DeviceBuffer centers;              // float4 per primitive
+  DeviceBuffer bounds;               // 6 ordered uints
+  DeviceBuffer keys, vals, keys_alt, vals_alt, hist;
+  DeviceBuffer sorted_lo, sorted_hi; // float4 per leaf in sorted order
+  DeviceBuffer left, right, first, last, parent, leaf_parent, flags;
+  DeviceBuffer node_lo, node_hi;     // float4 per internal node
+  size_t capacity = 0;
+  void ensure(size_t n);
+};
+
+// Compute 30-bit Morton codes of box centres (exposed for tests too).
+void morton_codes(const float4* centers, uint32_t n, uint32_t* bounds_scratch, uint32_t* codes,
+                  cudaStream_t stream);
+// Centres of triangle AABBs from a flat [n*9] array (tests).
+void triangle_centers_flat(const float* tri, uint32_t n, float4* lo, float4* hi, float4* centers,
+                           cudaStream_t stream);
+// Stable LSD radix sort of pairs; result lands in keys/vals.
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                      uint32_t* hist, uint32_t n, uint32_t key_bits, cudaStream_t stream);
+size_t radix_sort_hist_words(uint32_t n);
+
+struct BlasDesc {
+  const float* vertices;      // device [nv*3]
+  const float* normals;       // device [nv*3]
+  const uint32_t* indices;    // device [nt*3]
+  uint32_t num_vertices;
+  uint32_t num_triangles;
+};
+
+// Build one BLAS.  Writes nodes at nodes[node_base ...] and triangle data at
+// slot range [slot_base, slot_base + nt).  Returns the root node index.
+uint32_t build_blas(const BlasDesc& d, BuildScratch& scratch, BvhNode* nodes, uint32_t node_base,
+                    float4* tri_verts, float4* tri_normals, uint32_t* tri_index, uint32_t slot_base,
+                    uint32_t leaf_max, cudaStream_t stream);
+inline uint32_t blas_node_count(uint32_t nt) { return nt > 1 ? nt - 1 : 1; }
+
+// Build the TLAS over instances (world boxes computed from BLAS roots).
+uint32_t build_tlas(const InstanceRec* instances, const float* object_to_world, uint32_t n,
+                    const BvhNode* nodes_in, BuildScratch& scratch, BvhNode* nodes,
+                    uint32_t node_base, cudaStream_t stream);
+
+// Count structural violations of the resident BVH.
+uint64_t validate_bvh(const SceneView& s, uint32_t total_slots, uint32_t num_instances,
+                      const uint32_t* blas_slot_begin, const uint32_t* blas_slot_end,
+                      cudaStream_t stream);
+
+}  // namespace olc

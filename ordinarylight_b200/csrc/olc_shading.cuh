@@ -1,0 +1,191 @@
+// Shading math: environment/sky, the GGX + Lambert BSDF, emitter sampling.
+//
+// Production BSDF = the reference's isotropic PBR helpers
+// (ordinarylight_pbr_cosine_hemisphere / _evaluate / _pdf /
+// _sample_half_vector / _reflect / _weight / _specular_probability,
+// ordinarylight/shaders/ordinaryshade_primary.glsl:506-609):
+//   f0 = mix(0.04, base, metallic); F = Schlick(f0, v.h);
+//   D = GGX with alpha = max(roughness^2, 0.0009); G = Smith G1(n.v) G1(n.l);
+//   f = (1 - F)(1 - metallic) base / pi + F D G / (4 n.v n.l);
+//   specular lobe probability = clamp(max(f0), 0.1, 0.9);
+//   pdf = mix(n.l / pi, D n.h / (4 v.h), p_spec).
+// Reference-compatible BSDF = the CPU tracer's Lambert: throughput *= albedo,
+// cosine-distributed direction (path_tracer.py:84-87, :205-211).
+#pragma once
+
+#include "olc_common.cuh"
+
+#define OLC_PI 3.14159265358979f
+
+// CPU reference sky (path_tracer.py:201-202).
+OLC_D float3 cpu_sky(float3 d) {
+  float blend = clampf(0.5f * (d.y + 1.0f), 0.0f, 1.0f);
+  return f3(0.8f, 0.8f, 0.8f) * (1.0f - blend) + f3(0.2f, 0.4f, 0.9f) * blend;
+}
+
+// Reference GPU analytic sky (ordinaryshade_primary.glsl:703-707).
+OLC_D float3 gpu_sky(float3 d) {
+  float sky = fmaxf(d.y, 0.0f);
+  return lerp3(f3(0.018f, 0.022f, 0.032f), f3(0.32f, 0.46f, 0.72f), sky);
+}
+
+// Environment radiance (constant or equirectangular nearest lookup as in
+// ReferencePathTracer._sky, path_tracer.py:185-200); kind NONE falls back to
+// the mode's analytic sky.
+OLC_D float3 environment_radiance(const SceneView& s, float3 d, bool cpu_mode) {
+  if (s.env_kind == 0u) return cpu_mode ? cpu_sky(d) : gpu_sky(d);
+  if (s.env_kind == 1u) return s.env_color;
+  float lon = atan2f(d.z, d.x) + s.env_rotation;
+  float u = lon / (2.0f * OLC_PI) + 0.5f;
+  u = u - floorf(u);
+  float v = acosf(clampf(d.y, -1.0f, 1.0f)) / OLC_PI;
+  uint32_t x = min((uint32_t)(u * (float)s.env_w), s.env_w - 1u);
+  uint32_t y = min((uint32_t)(v * (float)s.env_h), s.env_h - 1u);
+  const float* p = s.env_image + 3ull * ((uint64_t)y * s.env_w + x);
+  return f3(p[0], p[1], p[2]) * s.env_color;
+}
+
+OLC_D void tangent_frame(float3 n, float3& t, float3& b) {
+  t = (fabsf(n.z) < 0.999f) ? cross(n, f3(0.0f, 0.0f, 1.0f)) : cross(n, f3(0.0f, 1.0f, 0.0f));
+  t = normalize(t);
+  b = cross(n, t);
+}
+
+OLC_D float3 cosine_hemisphere(float3 n, float u, float v) {
+  float r = sqrtf(u);
+  float phi = 2.0f * OLC_PI * v;
+  float3 t, b;
+  tangent_frame(n, t, b);
+  float sp, cp;
+  __sincosf(phi, &sp, &cp);
+  return normalize(t * (r * cp) + b * (r * sp) + n * sqrtf(fmaxf(0.0f, 1.0f - u)));
+}
+
+OLC_D float ggx_alpha2(float roughness) {
+  float a = fmaxf(roughness * roughness, 0.0009f);
+  return a * a;
+}
+OLC_D float ggx_d(float nh, float a2) {
+  float den = nh * nh * (a2 - 1.0f) + 1.0f;
+  return a2 / fmaxf(OLC_PI * den * den, 1e-6f);
+}
+OLC_D float ggx_g1(float nd, float a2) {
+  return 2.0f * nd / fmaxf(nd + sqrtf(a2 + (1.0f - a2) * nd * nd), 1e-6f);
+}
+
+struct SurfaceMat {
+  float3 base;
+  float roughness;
+  float3 emission;
+  float metallic;
+  uint32_t two_sided;
+};
+
+OLC_D float spec_probability(const SurfaceMat& m) {
+  float3 f0 = lerp3(f3(0.04f, 0.04f, 0.04f), m.base, m.metallic);
+  return clampf(max3(f0), 0.1f, 0.9f);
+}
+
+OLC_D float3 pbr_eval(const SurfaceMat& m, float3 n, float3 view, float3 out) {
+  float nv = fmaxf(dot(n, view), 0.0f);
+  float nl = fmaxf(dot(n, out), 0.0f);
+  if (nv <= 0.0f || nl <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
+  float3 h = normalize(view + out);
+  float nh = fmaxf(dot(n, h), 0.0f);
+  float vh = fmaxf(dot(view, h), 0.0f);
+  float3 f0 = lerp3(f3(0.04f, 0.04f, 0.04f), m.base, m.metallic);
+  float w = 1.0f - clampf(vh, 0.0f, 1.0f);
+  float w5 = w * w * w * w * w;
+  float3 F = f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * w5;
+  float a2 = ggx_alpha2(m.roughness);
+  float D = ggx_d(nh, a2);
+  float G = ggx_g1(nv, a2) * ggx_g1(nl, a2);
+  float3 spec = F * (D * G / fmaxf(4.0f * nv * nl, 1e-6f));
+  float3 diff = (f3(1.0f, 1.0f, 1.0f) - F) * m.base * ((1.0f - m.metallic) / OLC_PI);
+  return diff + spec;
+}
+
+OLC_D float pbr_pdf(const SurfaceMat& m, float3 n, float3 view, float3 out) {
+  float nl = fmaxf(dot(n, out), 0.0f);
+  if (nl <= 0.0f) return 0.0f;
+  float3 h = normalize(view + out);
+  float nh = fmaxf(dot(n, h), 0.0f);
+  float vh = fmaxf(dot(view, h), 1e-6f);
+  float a2 = ggx_alpha2(m.roughness);
+  float spec_pdf = ggx_d(nh, a2) * nh / (4.0f * vh);
+  float diff_pdf = nl / OLC_PI;
+  float p = spec_probability(m);
+  return diff_pdf + (spec_pdf - diff_pdf) * p;
+}
+
+OLC_D float3 sample_half_vector(float3 n, float roughness, float u, float v) {
+  float a2 = ggx_alpha2(roughness);
+  float phi = 2.0f * OLC_PI * v;
+  float c = sqrtf((1.0f - u) / fmaxf(1.0f + (a2 - 1.0f) * u, 1e-6f));
+  float sn = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+  float3 t, b;
+  tangent_frame(n, t, b);
+  float sp, cp;
+  __sincosf(phi, &sp, &cp);
+  return normalize(t * (sn * cp) + b * (sn * sp) + n * c);
+}
+
+// samplePbr (transport_v1/lighting.glsl:226-246): lobe choice, direction,
+// pdf and weight = f cos / pdf.
+OLC_D void pbr_sample(const SurfaceMat& m, float3 n, float3 incoming, uint32_t& rng, float3& out, float3& weight,
+                      float& pdf) {
+  float3 view = -incoming;
+  float p = spec_probability(m);
+  bool specular = olc_rand(rng) < p;
+  float u = olc_rand(rng), v = olc_rand(rng);
+  out = cosine_hemisphere(n, u, v);
+  if (specular) {
+    float3 h = sample_half_vector(n, m.roughness, u, v);
+    out = incoming - h * (2.0f * dot(h, incoming));
+  }
+  if (dot(n, out) <= 0.0f) {
+    float u2 = olc_rand(rng), v2 = olc_rand(rng);
+    out = cosine_hemisphere(n, u2, v2);
+  }
+  out = normalize(out);
+  pdf = fmaxf(pbr_pdf(m, n, view, out), 1e-6f);
+  float3 f = pbr_eval(m, n, view, out);
+  weight = f * (fmaxf(dot(n, out), 0.0f) / pdf);
+}
+
+OLC_D float power_heuristic(float a, float b) {
+  float a2 = a * a, b2 = b * b;
+  return a2 / fmaxf(a2 + b2, 1e-6f);
+}
+
+OLC_D SurfaceMat load_material(const SceneView& s, uint32_t mi) {
+  MaterialRec r = s.materials[mi];
+  SurfaceMat m;
+  m.base = f3(r.base_rough);
+  m.roughness = r.base_rough.w;
+  m.emission = f3(r.emit_metal);
+  m.metallic = r.emit_metal.w;
+  m.two_sided = s.material_aux[mi].two_sided;
+  return m;
+}
+
+// Emitter selection by binary search of the power CDF
+// (sampleAreaLightTechnique, transport_v1/lighting.glsl:356-377).
+OLC_D uint32_t select_emitter(const SceneView& s, float selector) {
+  uint32_t lo = 0, hi = s.num_emitters - 1u;
+  for (int step = 0; step < 32 && lo < hi; ++step) {
+    uint32_t mid = lo + (hi - lo) / 2u;
+    if (selector <= __ldg(&s.emitters[mid].dist.x)) hi = mid; else lo = mid + 1u;
+  }
+  return lo;
+}
+
+OLC_D float3 emitter_point(const EmitterRec& e, float root_u, float v) {
+  return f3(e.a) * (1.0f - root_u) + f3(e.b) * (root_u * (1.0f - v)) + f3(e.c) * (root_u * v);
+}
+
+OLC_D float emitter_cosine(const EmitterRec& e, float3 dir) {
+  float3 ln = normalize(cross(f3(e.b) - f3(e.a), f3(e.c) - f3(e.a)));
+  float c = dot(ln, -dir);
+  return e.dist.z > 0.5f ? fabsf(c) : fmaxf(c, 0.0f);
+}

@@ -1,0 +1,252 @@
+// Software two-level BVH traversal: closest hit and any hit.
+//
+// Replaces the hardware ray queries of the reference wavefront
+// (nativeTraceSurface, ordinarylight/shaders/wavefront_intersect.comp:96-235;
+// nativeOccluded in ordinarylight/shaders/transport_v1/lighting.glsl).
+// * TLAS and BLAS nodes share one node pool; a TLAS leaf is one instance.
+//   Entering an instance transforms the ray to object space (t is preserved
+//   because the direction is not renormalised) and pushes a marker that
+//   restores the world ray when the instance's subtree is exhausted.
+// * The traversal stack lives in shared memory (STACK entries per thread,
+//   entry k of thread t at k * blockDim.x + t, so a warp's pushes hit 32
+//   distinct banks); deeper entries spill to a bounded local array.  A push
+//   beyond both is counted as a traversal error instead of writing out of
+//   bounds.
+// * Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013):
+//   the edge functions are evaluated without FMA contraction so that an edge
+//   shared by two triangles gets exactly negated values, with a double
+//   precision re-evaluation when an edge function is exactly zero.
+// * Closest-hit ties (equal t) resolve to the lowest packed triangle index,
+//   the rule of ReferencePathTracer._intersect (strict "<" over triangles in
+//   packed order, ordinarylight/renderers/reference/path_tracer.py:159-175),
+//   which also makes the result independent of traversal order.
+#pragma once
+
+#include "olc_common.cuh"
+
+#define OLC_SPILL 96
+#define OLC_MARKER 0x7fffffff
+
+struct TraceRay {
+  float3 o, d;
+  float3 inv, oinv;
+  int kx, ky, kz;
+  float sx, sy, sz;
+};
+
+OLC_D void setup_ray(TraceRay& r, float3 o, float3 d) {
+  r.o = o;
+  r.d = d;
+  float dx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
+  float dy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
+  float dz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
+  r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dz);
+  r.oinv = f3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  float dkz = get(d, kz);
+  if (dkz < 0.0f) { int t = kx; kx = ky; ky = t; }
+  r.kx = kx; r.ky = ky; r.kz = kz;
+  r.sx = get(d, kx) / dkz;
+  r.sy = get(d, ky) / dkz;
+  r.sz = 1.0f / dkz;
+}
+
+// Watertight ray/triangle test.  Returns true with t, b1 (weight of v1),
+// b2 (weight of v2) when the ray hits with t_min < t <= t_max.
+OLC_D bool intersect_triangle(const TraceRay& r, float3 v0, float3 v1, float3 v2,
+                              float t_min, float t_max, float& t_out, float& b1, float& b2) {
+  float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+  float Akz = get(A, r.kz), Bkz = get(B, r.kz), Ckz = get(C, r.kz);
+  float Ax = __fmaf_rn(-r.sx, Akz, get(A, r.kx));
+  float Ay = __fmaf_rn(-r.sy, Akz, get(A, r.ky));
+  float Bx = __fmaf_rn(-r.sx, Bkz, get(B, r.kx));
+  float By = __fmaf_rn(-r.sy, Bkz, get(B, r.ky));
+  float Cx = __fmaf_rn(-r.sx, Ckz, get(C, r.kx));
+  float Cy = __fmaf_rn(-r.sy, Ckz, get(C, r.ky));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    double CxBy = (double)Cx * (double)By, CyBx = (double)Cy * (double)Bx;
+    U = (float)(CxBy - CyBx);
+    double AxCy = (double)Ax * (double)Cy, AyCx = (double)Ay * (double)Cx;
+    V = (float)(AxCy - AyCx);
+    double BxAy = (double)Bx * (double)Ay, ByAx = (double)By * (double)Ax;
+    W = (float)(BxAy - ByAx);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = U + V + W;
+  if (det == 0.0f) return false;
+  float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
+  float T = U * Az + V * Bz + W * Cz;
+  float t = __fdiv_rn(T, det);
+  if (!(t > t_min) || !(t <= t_max)) return false;
+  float rcp = 1.0f / det;
+  t_out = t;
+  b1 = V * rcp;
+  b2 = W * rcp;
+  return true;
+}
+
+struct HitResult {
+  float t, u, v;
+  uint32_t slot;       // triangle slot (BVH order)
+  uint32_t instance;   // instance index (0xffffffff: miss)
+  uint32_t packed;     // packed triangle index (tie-break key)
+};
+
+template <int STACK>
+struct TraversalStack {
+  int* smem;           // this thread's column in the shared stack
+  int stride;
+  int sp;
+  int spill[OLC_SPILL];
+
+  OLC_D void init(int* base, int tid, int threads) { smem = base + tid; stride = threads; sp = 0; }
+  OLC_D bool push(int v, uint32_t& err) {
+    if (sp < STACK) { smem[sp * stride] = v; ++sp; return true; }
+    if (sp < STACK + OLC_SPILL) { spill[sp - STACK] = v; ++sp; return true; }
+    err = 1u;
+    return false;
+  }
+  OLC_D int pop() {
+    --sp;
+    return sp < STACK ? smem[sp * stride] : spill[sp - STACK];
+  }
+};
+
+OLC_D void load_instance_w2o(const InstanceRec* inst, uint32_t i, Affine& w2o, uint32_t& root,
+                             uint32_t& prim_offset) {
+  const float4* p = reinterpret_cast<const float4*>(inst + i);
+  w2o.r0 = __ldg(p + 0);
+  w2o.r1 = __ldg(p + 1);
+  w2o.r2 = __ldg(p + 2);
+  uint4 m = __ldg(reinterpret_cast<const uint4*>(p + 3));
+  root = m.x;
+  prim_offset = m.z;
+}
+
+// Intersect both child boxes of a node with the current ray.
+OLC_D void node_boxes(const BvhNode* nodes, int node, const TraceRay& r, float t_min, float t_max,
+                      bool& hit0, bool& hit1, float& near0, float& near1, int& c0, int& c1) {
+  const float4* p = reinterpret_cast<const float4*>(nodes + node);
+  float4 a = __ldg(p + 0);
+  float4 b = __ldg(p + 1);
+  float4 c = __ldg(p + 2);
+  int4 d = __ldg(reinterpret_cast<const int4*>(p + 3));
+  const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
+  const float ox = r.oinv.x, oy = r.oinv.y, oz = r.oinv.z;
+  float l0x = __fmaf_rn(a.x, ix, -ox), h0x = __fmaf_rn(a.y, ix, -ox);
+  float l0y = __fmaf_rn(a.z, iy, -oy), h0y = __fmaf_rn(a.w, iy, -oy);
+  float l0z = __fmaf_rn(c.x, iz, -oz), h0z = __fmaf_rn(c.y, iz, -oz);
+  float l1x = __fmaf_rn(b.x, ix, -ox), h1x = __fmaf_rn(b.y, ix, -ox);
+  float l1y = __fmaf_rn(b.z, iy, -oy), h1y = __fmaf_rn(b.w, iy, -oy);
+  float l1z = __fmaf_rn(c.z, iz, -oz), h1z = __fmaf_rn(c.w, iz, -oz);
+  float n0 = fmaxf(fmaxf(fminf(l0x, h0x), fminf(l0y, h0y)), fmaxf(fminf(l0z, h0z), t_min));
+  float f0 = fminf(fminf(fmaxf(l0x, h0x), fmaxf(l0y, h0y)), fminf(fmaxf(l0z, h0z), t_max));
+  float n1 = fmaxf(fmaxf(fminf(l1x, h1x), fminf(l1y, h1y)), fmaxf(fminf(l1z, h1z), t_min));
+  float f1 = fminf(fminf(fmaxf(l1x, h1x), fmaxf(l1y, h1y)), fminf(fmaxf(l1z, h1z), t_max));
+  // Conservative far bound (robust traversal, Ize 2013): a few ulps of slack
+  // so rounding in the slab test never culls a box the ray touches.
+  c0 = d.x;
+  c1 = d.y;
+  hit0 = (n0 <= f0 * 1.0000004f) && (c0 != OLC_EMPTY_CHILD);
+  hit1 = (n1 <= f1 * 1.0000004f) && (c1 != OLC_EMPTY_CHILD);
+  near0 = n0;
+  near1 = n1;
+}
+
+// Traverse the two-level structure.  ANY_HIT stops at the first hit in
+// (t_min, t_max).  Returns true on a hit.
+template <int STACK, bool ANY_HIT>
+OLC_D bool olc_traverse(const SceneView& s, float3 wo, float3 wd, float t_min, float t_max,
+                        HitResult& hit, int* smem_base, uint32_t& err) {
+  TraversalStack<STACK> st;
+  st.init(smem_base, threadIdx.x, blockDim.x);
+  TraceRay ray;
+  setup_ray(ray, wo, wd);
+  hit.t = t_max;
+  hit.instance = 0xffffffffu;
+  hit.slot = 0;
+  hit.u = hit.v = 0.0f;
+  hit.packed = 0xffffffffu;
+  bool found = false;
+  int level = 0;
+  uint32_t cur_inst = 0, cur_prim_offset = 0;
+  int node = (int)s.tlas_root;
+  while (true) {
+    if (node >= 0 && node != OLC_MARKER) {
+      bool h0, h1;
+      float n0, n1;
+      int c0, c1;
+      node_boxes(s.nodes, node, ray, t_min, hit.t, h0, h1, n0, n1, c0, c1);
+      if (h0 && h1) {
+        int near_c = (n0 <= n1) ? c0 : c1;
+        int far_c = (n0 <= n1) ? c1 : c0;
+        st.push(far_c, err);
+        node = near_c;
+        continue;
+      }
+      if (h0) { node = c0; continue; }
+      if (h1) { node = c1; continue; }
+    } else if (node != OLC_MARKER) {
+      uint32_t first = olc_leaf_first(node);
+      uint32_t count = olc_leaf_count(node);
+      if (level == 0) {
+        // instance leaf (TLAS leaves hold one instance)
+        Affine w2o;
+        uint32_t root;
+        load_instance_w2o(s.instances, first, w2o, root, cur_prim_offset);
+        cur_inst = first;
+        float3 oo = xform_point(w2o, wo);
+        float3 od = xform_vector(w2o, wd);
+        setup_ray(ray, oo, od);
+        level = 1;
+        if (st.push(OLC_MARKER, err)) {
+          node = (int)root;
+          continue;
+        }
+        level = 0;
+        setup_ray(ray, wo, wd);
+      } else {
+        for (uint32_t k = 0; k < count; ++k) {
+          uint32_t slot = first + k;
+          const float4* tv = s.tri_verts + 3u * slot;
+          float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
+          float t, b1, b2;
+          if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
+            if (ANY_HIT) {
+              hit.t = t;
+              hit.instance = cur_inst;
+              hit.slot = slot;
+              return true;
+            }
+            uint32_t packed = cur_prim_offset + __ldg(s.tri_index + slot);
+            if (t < hit.t || packed < hit.packed) {
+              hit.t = t;
+              hit.u = b1;
+              hit.v = b2;
+              hit.slot = slot;
+              hit.instance = cur_inst;
+              hit.packed = packed;
+              found = true;
+            }
+          }
+        }
+      }
+    }
+    // pop
+    if (st.sp == 0) break;
+    node = st.pop();
+    if (node == OLC_MARKER) {
+      level = 0;
+      setup_ray(ray, wo, wd);
+      if (st.sp == 0) break;
+      node = st.pop();
+    }
+  }
+  return found;
+}

@@ -1,0 +1,598 @@
+// Wavefront path-tracing stages: camera raygen, closest-hit and any-hit
+// traversal, shading with NEE and warp-aggregated queue compaction, and the
+// fixed-point HDR accumulation.
+//
+// Stage map against the reference wavefront (ordinarylight/shaders/):
+//   k_raygen         wavefront_generate.comp:86-167 (+ path init)
+//   k_trace_closest  wavefront_intersect.comp:317-356 (software traversal)
+//   k_shade          wavefront_shade.comp:262-596
+//   k_trace_shadow   nativeOccluded in transport_v1/lighting.glsl
+//   k_accumulate     wavefront_resolve.comp:45-54 plus the host float64
+//                    accumulation of api.py:1404-1422, moved on device
+// Queue counts never leave the device: persistent kernels read them, so the
+// whole bounce loop can be captured once as a CUDA graph.
+#include "olc_internal.h"
+#include "olc_shading.cuh"
+#include "olc_trace.cuh"
+#include "olc_wavefront.h"
+
+namespace olc {
+
+namespace {
+
+OLC_D uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated slot reservation: one atomic per warp for all lanes that
+// want a slot (reserveOutputIndex, wavefront_shade.comp:199-213).  Must be
+// called by all 32 lanes.
+OLC_D uint32_t warp_reserve(uint32_t* counter, bool want) {
+  uint32_t ballot = __ballot_sync(0xffffffffu, want);
+  if (ballot == 0u) return 0xffffffffu;
+  uint32_t leader = __ffs(ballot) - 1u;
+  uint32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(counter, __popc(ballot));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return want ? base + __popc(ballot & ((1u << lane_id()) - 1u)) : 0xffffffffu;
+}
+
+__global__ void k_raygen(const FrameParams* __restrict__ fp_ptr, uint64_t chunk_begin, uint32_t chunk_count,
+                         RayQueue q, PathState ps, Counters* cnt, float t_min) {
+  const FrameParams fp = *fp_ptr;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < chunk_count; i += gridDim.x * blockDim.x) {
+    uint64_t linear = chunk_begin + i;
+    uint32_t sample = (uint32_t)(linear / fp.npix);
+    uint32_t pixel = (uint32_t)(linear - (uint64_t)sample * fp.npix);
+    float3 o, d;
+    camera_ray(fp, pixel, sample, nullptr, o, d);
+    q.origin_tmin[i] = make_float4(o.x, o.y, o.z, t_min);
+    q.dir_tmax[i] = make_float4(d.x, d.y, d.z, CUDART_INF_F);
+    q.path[i] = i;
+    ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ps.meta[i] = make_uint4(pixel, sample, 0u, 0u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = chunk_count;
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
+                                                       uint32_t bounce) {
+  extern __shared__ int smem_stack[];
+  const uint32_t n = cnt->queue_count[bounce];
+  uint32_t err = 0;
+  while (true) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(&cnt->closest_cursor[bounce], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint32_t i = base + lane_id();
+    if (i < n) {
+      float4 ot = q.origin_tmin[i];
+      float4 dt = q.dir_tmax[i];
+      HitResult hr;
+      bool hit = olc_traverse<STACK, false>(s, f3(ot), f3(dt), ot.w, dt.w, hr, smem_stack, err);
+      h.tuv_slot[i] = hit ? make_float4(hr.t, hr.u, hr.v, __uint_as_float(hr.slot))
+                          : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+      h.instance[i] = hit ? hr.instance : 0xffffffffu;
+    }
+  }
+  if (err) atomicAdd(&cnt->traversal_errors, 1u);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
+                                                      uint32_t bounce) {
+  extern __shared__ int smem_stack[];
+  const uint32_t n = cnt->shadow_count[bounce];
+  uint32_t err = 0;
+  while (true) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(&cnt->shadow_cursor[bounce], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint32_t i = base + lane_id();
+    if (i < n) {
+      float4 ot = sq.origin_tmax[i];
+      float4 dp = sq.dir_path[i];
+      HitResult hr;
+      bool occluded = olc_traverse<STACK, true>(s, f3(ot), f3(dp), 0.001f, ot.w, hr, smem_stack, err);
+      if (!occluded) {
+        uint32_t path = __float_as_uint(dp.w);
+        float4 c = sq.contrib[i];
+        float4 r = ps.radiance[path];
+        ps.radiance[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
+      }
+    }
+  }
+  if (err) atomicAdd(&cnt->traversal_errors, 1u);
+}
+
+// Products of the first sample's primary hit (render_products).
+struct Products {
+  float* depth;
+  float4* normal;
+  uint32_t* instance_id;
+  uint32_t* material_id;
+  uint32_t* primitive_id;
+};
+
+struct ShadeArgs {
+  const FrameParams* fp;
+  SceneView s;
+  RayQueue qin;
+  HitBuf hits;
+  RayQueue qout;
+  ShadowQueue sq;
+  PathState ps;
+  Counters* cnt;
+  uint32_t bounce;
+  uint32_t capacity;
+  Products prod;
+  const uint4* restir;   // per-path selected light sample (bounce 0), or null
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
+  const FrameParams& fp = *a.fp;
+  const SceneView& s = a.s;
+  const uint32_t bounce = a.bounce;
+  const uint32_t n = a.cnt->queue_count[bounce];
+  const bool cpu_mode = (MODE == 1);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t i = base + lane_id();
+    const bool valid = i < n;
+    bool want_next = false, want_shadow = false, is_miss = false;
+    float3 next_o = f3(0, 0, 0), next_d = f3(0, 0, 0);
+    float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), sh_c = f3(0, 0, 0);
+    float sh_tmax = 0.0f;
+    uint32_t path = 0;
+    if (valid) {
+      path = a.qin.path[i];
+      float4 ot = a.qin.origin_tmin[i];
+      float4 dt = a.qin.dir_tmax[i];
+      float4 hit = a.hits.tuv_slot[i];
+      float4 tp4 = a.ps.throughput[path];
+      float4 rad4 = a.ps.radiance[path];
+      uint4 meta = a.ps.meta[path];
+      float3 tp = f3(tp4), rad = f3(rad4);
+      const float3 o = f3(ot), d = f3(dt);
+      const uint32_t flags = meta.z >> 8;
+      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), bounce);
+      uint32_t new_flags = 0;
+      float new_pdf = 0.0f;
+      if (hit.x < 0.0f) {
+        is_miss = true;
+        // miss: environment (no environment NEE, so BSDF sampling carries it
+        // with MIS weight 1)
+        rad += tp * environment_radiance(s, d, cpu_mode);
+        if (bounce == 0 && meta.y == 0 && a.prod.depth) {
+          a.prod.depth[meta.x] = CUDART_INF_F;
+          a.prod.normal[meta.x] = make_float4(0, 0, 0, 0);
+          a.prod.instance_id[meta.x] = 0xffffffffu;
+          a.prod.material_id[meta.x] = 0xffffffffu;
+          a.prod.primitive_id[meta.x] = 0xffffffffu;
+        }
+      } else {
+        const float t = hit.x, bu = hit.y, bv = hit.z;
+        const uint32_t slot = __float_as_uint(hit.w);
+        const uint32_t inst = a.hits.instance[i];
+        const InstanceRec& ir = s.instances[inst];
+        Affine o2w{ir.o2w0, ir.o2w1, ir.o2w2};
+        Affine w2o{ir.w2o0, ir.w2o1, ir.w2o2};
+        const float4* tv = s.tri_verts + 3u * slot;
+        float3 v0 = xform_point(o2w, f3(tv[0])), v1 = xform_point(o2w, f3(tv[1])), v2 = xform_point(o2w, f3(tv[2]));
+        float3 e1 = v1 - v0, e2 = v2 - v0;
+        float3 gcross = cross(e1, e2);
+        float3 ng = normalize(gcross);
+        float3 p = o + d * t;
+        SurfaceMat m = load_material(s, ir.material);
+        if (bounce == 0 && meta.y == 0 && a.prod.depth) {
+          a.prod.depth[meta.x] = t;
+          float3 fn = dot(ng, d) > 0.0f ? -ng : ng;
+          a.prod.normal[meta.x] = make_float4(fn.x, fn.y, fn.z, 0.0f);
+          a.prod.instance_id[meta.x] = ir.instance_id;
+          a.prod.material_id[meta.x] = s.material_aux[ir.material].material_id;
+          a.prod.primitive_id[meta.x] = ir.prim_offset + s.tri_index[slot];
+        }
+        if (MODE == 1) {
+          // CPU reference transport (path_tracer.py:74-87)
+          float3 nrm = dot(ng, d) > 0.0f ? -ng : ng;
+          rad += tp * m.emission;
+          tp *= m.base;
+          if (bounce + 1u < fp.max_bounces) {
+            float u1 = olc_rand(rng), u2 = olc_rand(rng);
+            next_o = p + nrm * 1e-4f;
+            next_d = cosine_hemisphere(nrm, u1, u2);
+            want_next = true;
+          }
+        } else {
+          // shading normal: interpolated vertex normals in world space
+          const float4* tn = s.tri_normals + 3u * slot;
+          float w0 = 1.0f - bu - bv;
+          float3 nobj = f3(tn[0]) * w0 + f3(tn[1]) * bu + f3(tn[2]) * bv;
+          float3 ns = normalize(xform_normal_by_inverse(w2o, nobj));
+          if (!(dot(ns, ns) > 0.5f)) ns = ng;
+          if (dot(ns, ng) < 0.0f) ns = -ns;
+          const bool entering = dot(d, ng) < 0.0f;
+          const float3 nrm = entering ? ns : -ns;
+          // emission with power-heuristic MIS against the previous BSDF pdf
+          // (wavefront_shade.comp:412-433)
+          if ((entering || m.two_sided) && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f)) {
+            float mis = 1.0f;
+            if (flags & OLC_PATH_FLAG_PREV_RESTIR) {
+              mis = 0.0f;  // the primary vertex's area lighting came from ReSTIR
+            } else if ((flags & OLC_PATH_FLAG_PREV_NEE) && s.num_emitters > 0u) {
+              float area = 0.5f * length(gcross);
+              float lc_raw = dot(ng, -d);
+              float lc = m.two_sided ? fabsf(lc_raw) : fmaxf(lc_raw, 0.0f);
+              float sel = area * luminance(m.emission) / fmaxf(s.emissive_weight, 1e-6f);
+              float p_area = s.num_lights > 0u ? 0.5f : 1.0f;
+              float light_pdf = sel * t * t / fmaxf(lc * area, 1e-6f) * p_area;
+              mis = power_heuristic(tp4.w, light_pdf);
+            }
+            rad += tp * m.emission * mis;
+          }
+          const uint32_t next_bounce = bounce + 1u;
+          if (next_bounce < fp.max_bounces) {
+            const float3 view = -d;
+            bool did_area_nee = false, did_restir = false;
+            // ---- next-event estimation: one shadow ray per path per bounce
+            if (bounce == 0u && a.restir != nullptr && s.num_emitters > 0u) {
+              uint4 rs = a.restir[path];
+              did_restir = true;
+              float Wr = __uint_as_float(rs.z);
+              if (rs.x != 0xffffffffu && Wr > 0.0f) {
+                const EmitterRec e = s.emitters[rs.x];
+                float2 bary = __half22float2(*reinterpret_cast<const __half2*>(&rs.y));
+                float3 lp = f3(e.a) * fmaxf(1.0f - bary.x - bary.y, 0.0f) + f3(e.b) * bary.x + f3(e.c) * bary.y;
+                float3 off = lp - p;
+                float dist2 = dot(off, off);
+                float dist = sqrtf(dist2);
+                float3 ldir = off / fmaxf(dist, 1e-6f);
+                float sc = fmaxf(dot(nrm, ldir), 0.0f);
+                float lc = emitter_cosine(e, ldir);
+                if (sc > 0.0f && lc > 1e-6f) {
+                  float3 f = pbr_eval(m, nrm, view, ldir);
+                  float G = lc / fmaxf(dist2, 1e-12f);
+                  float3 c = tp * f * f3(e.emission_area) * (sc * G * Wr);
+                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
+                    sh_o = p + nrm * 0.002f;
+                    sh_d = ldir;
+                    sh_tmax = fmaxf(dist - 0.004f, 0.001f);
+                    sh_c = c;
+                    want_shadow = true;
+                  }
+                }
+              }
+            } else if (s.num_emitters > 0u || s.num_lights > 0u) {
+              float p_area = s.num_emitters > 0u ? (s.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
+              float choose = olc_rand(rng);
+              if (choose < p_area) {
+                did_area_nee = true;
+                // area light (sampleAreaLightTechnique, lighting.glsl:341-403)
+                float sel = olc_rand(rng);
+                uint32_t li = select_emitter(s, sel);
+                const EmitterRec e = s.emitters[li];
+                float ru = sqrtf(olc_rand(rng));
+                float rv = olc_rand(rng);
+                float3 lp = emitter_point(e, ru, rv);
+                float3 off = lp - p;
+                float dist2 = dot(off, off);
+                float dist = sqrtf(dist2);
+                float3 ldir = off / fmaxf(dist, 1e-6f);
+                float sc = fmaxf(dot(nrm, ldir), 0.0f);
+                float lc = emitter_cosine(e, ldir);
+                if (sc > 0.0f && lc > 1e-6f) {
+                  float eff_pdf = e.dist.y * dist2 / fmaxf(lc * e.emission_area.w, 1e-6f) * p_area;
+                  float bsdf_pdf = pbr_pdf(m, nrm, view, ldir);
+                  float mis = power_heuristic(eff_pdf, bsdf_pdf);
+                  float3 f = pbr_eval(m, nrm, view, ldir);
+                  float3 c = tp * f * f3(e.emission_area) * (sc * mis / fmaxf(eff_pdf, 1e-6f));
+                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
+                    sh_o = p + nrm * 0.002f;
+                    sh_d = ldir;
+                    sh_tmax = fmaxf(dist - 0.004f, 0.001f);
+                    sh_c = c;
+                    want_shadow = true;
+                  }
+                }
+              } else if (s.num_lights > 0u) {
+                // analytic light (samplePointLights, lighting.glsl:260-312)
+                float pick = olc_rand(rng);
+                uint32_t li = min((uint32_t)(pick * (float)s.num_lights), s.num_lights - 1u);
+                float p_sel = (1.0f - p_area) / (float)s.num_lights;
+                const LightRec L = s.lights[li];
+                int type = (int)(L.position_type.w + 0.5f);
+                float3 ldir;
+                float dist2 = 1.0f, dist = 1e4f;
+                if (type == 1) {
+                  ldir = -normalize(f3(L.direction_range));
+                } else {
+                  float3 off = f3(L.position_type) - p;
+                  dist2 = fmaxf(dot(off, off), 1e-6f);
+                  dist = sqrtf(dist2);
+                  ldir = off / dist;
+                }
+                bool in_range = !(type != 1 && L.direction_range.w > 0.0f && dist > L.direction_range.w);
+                float atten = type == 1 ? 1.0f : 1.0f / dist2;
+                if (type == 2) {
+                  float cone = dot(normalize(f3(L.direction_range)), -ldir);
+                  float x = clampf((cone - L.spot.y) / (L.spot.x - L.spot.y), 0.0f, 1.0f);
+                  atten *= x * x * (3.0f - 2.0f * x);
+                }
+                float sc = fmaxf(dot(nrm, ldir), 0.0f);
+                if (in_range && atten > 0.0f && sc > 0.0f) {
+                  float3 f = pbr_eval(m, nrm, view, ldir);
+                  float3 c = tp * f * f3(L.color_intensity) * (L.color_intensity.w * atten * sc / p_sel);
+                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
+                    sh_o = p + nrm * 0.002f;
+                    sh_d = ldir;
+                    sh_tmax = type == 1 ? 1e4f : fmaxf(dist - 0.004f, 0.001f);
+                    sh_c = c;
+                    want_shadow = true;
+                  }
+                }
+              }
+            }
+            // ---- BSDF sample
+            float3 wdir, weight;
+            float pdf;
+            pbr_sample(m, nrm, d, rng, wdir, weight, pdf);
+            tp *= weight;
+            new_pdf = pdf;
+            if (did_restir) new_flags |= OLC_PATH_FLAG_PREV_RESTIR;
+            else if (s.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
+            (void)did_area_nee;
+            bool alive = max3(tp) >= 1e-4f;
+            // Russian roulette (wavefront_shade.comp:569-580)
+            if (alive && fp.rr_start > 0u && next_bounce >= fp.rr_start) {
+              float survival = clampf(max3(tp), fp.rr_min_survival, 0.95f);
+              if (olc_rand(rng) >= survival) alive = false;
+              else tp = tp * (1.0f / survival);
+            }
+            if (alive) {
+              next_o = p + wdir * 0.002f;
+              next_d = wdir;
+              want_next = true;
+            }
+          }
+        }
+      }
+      a.ps.throughput[path] = make_float4(tp.x, tp.y, tp.z, new_pdf);
+      a.ps.radiance[path] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+      a.ps.meta[path] = make_uint4(meta.x, meta.y, (bounce + 1u) | (new_flags << 8), meta.w);
+    }
+    // miss statistics (per-bounce hit/miss split of the shade roofline)
+    {
+      uint32_t ballot = __ballot_sync(0xffffffffu, is_miss);
+      if (ballot && lane_id() == (uint32_t)(__ffs(ballot) - 1)) atomicAdd(&a.cnt->miss_count[bounce], __popc(ballot));
+    }
+    // compaction of the next queue and the shadow queue
+    uint32_t slot = warp_reserve(&a.cnt->queue_count[bounce + 1u], want_next);
+    if (want_next) {
+      if (slot < a.capacity) {
+        a.qout.origin_tmin[slot] = make_float4(next_o.x, next_o.y, next_o.z, cpu_mode ? 1e-4f : 0.001f);
+        a.qout.dir_tmax[slot] = make_float4(next_d.x, next_d.y, next_d.z, CUDART_INF_F);
+        a.qout.path[slot] = path;
+      } else {
+        atomicAdd(&a.cnt->overflow, 1u);
+      }
+    }
+    uint32_t sslot = warp_reserve(&a.cnt->shadow_count[bounce], want_shadow);
+    if (want_shadow) {
+      if (sslot < a.capacity) {
+        a.sq.origin_tmax[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
+        a.sq.dir_path[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(path));
+        a.sq.contrib[sslot] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+      } else {
+        atomicAdd(&a.cnt->overflow, 1u);
+      }
+    }
+  }
+}
+
+OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
+  if (!(v == v)) {  // NaN
+    atomicAdd(nan_counter, 1u);
+    return 0ull;
+  }
+  v = fminf(fmaxf(v, 0.0f), OLC_SAMPLE_CLAMP);
+  return __float2ull_rn(v * OLC_ACCUM_SCALE);
+}
+
+__global__ void k_accumulate(PathState ps, uint32_t chunk_count, unsigned long long* accum, Counters* cnt) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < chunk_count; i += gridDim.x * blockDim.x) {
+    float4 r = ps.radiance[i];
+    uint32_t pixel = ps.meta[i].x;
+    unsigned long long* dst = accum + 3ull * pixel;
+    atomicAdd(dst + 0, to_fixed(r.x, &cnt->nan_samples));
+    atomicAdd(dst + 1, to_fixed(r.y, &cnt->nan_samples));
+    atomicAdd(dst + 2, to_fixed(r.z, &cnt->nan_samples));
+  }
+}
+
+__global__ void k_resolve(const unsigned long long* __restrict__ accum, uint32_t npix, uint32_t spp, float4* out) {
+  const double scale = 1.0 / ((double)OLC_ACCUM_SCALE * (double)spp);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    const unsigned long long* a = accum + 3ull * p;
+    out[p] = make_float4((float)((double)a[0] * scale), (float)((double)a[1] * scale), (float)((double)a[2] * scale),
+                         0.0f);
+  }
+}
+
+__global__ void k_camera_rays(const FrameParams* __restrict__ fp_ptr, uint32_t sample, float2 jitter_override,
+                              int use_override, float* origins, float* dirs) {
+  const FrameParams fp = *fp_ptr;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < fp.npix; p += gridDim.x * blockDim.x) {
+    float3 o, d;
+    camera_ray(fp, p, sample, use_override ? &jitter_override : nullptr, o, d);
+    origins[3ull * p + 0] = o.x;
+    origins[3ull * p + 1] = o.y;
+    origins[3ull * p + 2] = o.z;
+    dirs[3ull * p + 0] = d.x;
+    dirs[3ull * p + 1] = d.y;
+    dirs[3ull * p + 2] = d.z;
+  }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace_rays(SceneView s, uint32_t n, const float* __restrict__ origins,
+                                                    const float* __restrict__ dirs, float t_min, uint32_t* inst_id,
+                                                    int32_t* prim, float* tout, float* bary, Counters* cnt) {
+  extern __shared__ int smem_stack[];
+  uint32_t err = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float3 o = f3(origins[3ull * i], origins[3ull * i + 1], origins[3ull * i + 2]);
+    float3 d = f3(dirs[3ull * i], dirs[3ull * i + 1], dirs[3ull * i + 2]);
+    HitResult hr;
+    bool hit = olc_traverse<STACK, false>(s, o, d, t_min, CUDART_INF_F, hr, smem_stack, err);
+    if (inst_id) inst_id[i] = hit ? s.instances[hr.instance].instance_id : 0xffffffffu;
+    if (prim) prim[i] = hit ? (int32_t)hr.packed : -1;
+    if (tout) tout[i] = hit ? hr.t : CUDART_INF_F;
+    if (bary) {
+      bary[2ull * i] = hit ? hr.u : 0.0f;
+      bary[2ull * i + 1] = hit ? hr.v : 0.0f;
+    }
+  }
+  if (err) atomicAdd(&cnt->traversal_errors, 1u);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_occluded_rays(SceneView s, uint32_t n, const float* __restrict__ origins,
+                                                       const float* __restrict__ dirs, float t_min,
+                                                       const float* __restrict__ t_max, uint8_t* occ, Counters* cnt) {
+  extern __shared__ int smem_stack[];
+  uint32_t err = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float3 o = f3(origins[3ull * i], origins[3ull * i + 1], origins[3ull * i + 2]);
+    float3 d = f3(dirs[3ull * i], dirs[3ull * i + 1], dirs[3ull * i + 2]);
+    HitResult hr;
+    occ[i] = olc_traverse<STACK, true>(s, o, d, t_min, t_max[i], hr, smem_stack, err) ? 1 : 0;
+  }
+  if (err) atomicAdd(&cnt->traversal_errors, 1u);
+}
+
+constexpr int kTraceThreads = 128;
+
+template <class F>
+void dispatch_stack(uint32_t depth, F&& f) {
+  if (depth <= 16) f(std::integral_constant<int, 16>{});
+  else if (depth <= 24) f(std::integral_constant<int, 24>{});
+  else f(std::integral_constant<int, 32>{});
+}
+
+inline size_t stack_bytes(uint32_t depth) {
+  uint32_t d = depth <= 16 ? 16 : (depth <= 24 ? 24 : 32);
+  return (size_t)d * kTraceThreads * sizeof(int);
+}
+
+}  // namespace
+
+void launch_raygen(const LaunchShape& ls, const FrameParams* fp, uint64_t chunk_begin, uint32_t chunk_count,
+                   const RayQueue& q, const PathState& ps, Counters* cnt, float t_min, cudaStream_t stream) {
+  k_raygen<<<ls.grid_simple, ls.block, 0, stream>>>(fp, chunk_begin, chunk_count, q, ps, cnt, t_min);
+  OLC_LAUNCH_CHECK("k_raygen");
+}
+
+void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
+                          Counters* cnt, uint32_t bounce, cudaStream_t stream) {
+  dispatch_stack(ls.stack_depth, [&](auto depth) {
+    constexpr int D = decltype(depth)::value;
+    k_trace_closest<D><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
+  });
+  OLC_LAUNCH_CHECK("k_trace_closest");
+}
+
+void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const ShadowQueue& sq, const PathState& ps,
+                         Counters* cnt, uint32_t bounce, cudaStream_t stream) {
+  dispatch_stack(ls.stack_depth, [&](auto depth) {
+    constexpr int D = decltype(depth)::value;
+    k_trace_shadow<D><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
+  });
+  OLC_LAUNCH_CHECK("k_trace_shadow");
+}
+
+void launch_shade(const LaunchShape& ls, uint32_t mode, const FrameParams* fp, const SceneView& s,
+                  const RayQueue& qin, const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq,
+                  const PathState& ps, Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod,
+                  const uint4* restir, cudaStream_t stream) {
+  ShadeArgs a;
+  a.fp = fp;
+  a.s = s;
+  a.qin = qin;
+  a.hits = hits;
+  a.qout = qout;
+  a.sq = sq;
+  a.ps = ps;
+  a.cnt = cnt;
+  a.bounce = bounce;
+  a.capacity = capacity;
+  a.prod.depth = prod.depth;
+  a.prod.normal = prod.normal;
+  a.prod.instance_id = prod.instance_id;
+  a.prod.material_id = prod.material_id;
+  a.prod.primitive_id = prod.primitive_id;
+  a.restir = restir;
+  if (mode == 1) k_shade<1><<<ls.grid_shade, 128, 0, stream>>>(a);
+  else k_shade<0><<<ls.grid_shade, 128, 0, stream>>>(a);
+  OLC_LAUNCH_CHECK("k_shade");
+}
+
+void launch_accumulate(const LaunchShape& ls, const PathState& ps, uint32_t chunk_count, unsigned long long* accum,
+                       Counters* cnt, cudaStream_t stream) {
+  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(ps, chunk_count, accum, cnt);
+  OLC_LAUNCH_CHECK("k_accumulate");
+}
+
+void launch_resolve(const LaunchShape& ls, const unsigned long long* accum, uint32_t npix, uint32_t spp,
+                    float4* out, cudaStream_t stream) {
+  k_resolve<<<ls.grid_simple, ls.block, 0, stream>>>(accum, npix, spp, out);
+  OLC_LAUNCH_CHECK("k_resolve");
+}
+
+void launch_camera_rays(const LaunchShape& ls, const FrameParams* fp, uint32_t sample, const float* jitter,
+                        float* origins, float* dirs, cudaStream_t stream) {
+  float2 j = make_float2(0.5f, 0.5f);
+  if (jitter) j = make_float2(jitter[0], jitter[1]);
+  k_camera_rays<<<ls.grid_simple, ls.block, 0, stream>>>(fp, sample, j, jitter ? 1 : 0, origins, dirs);
+  OLC_LAUNCH_CHECK("k_camera_rays");
+}
+
+void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins, const float* dirs,
+                       float t_min, uint32_t* inst_id, int32_t* prim, float* t, float* bary, Counters* cnt,
+                       cudaStream_t stream) {
+  dispatch_stack(ls.stack_depth, [&](auto depth) {
+    constexpr int D = decltype(depth)::value;
+    uint32_t grid = std::max<uint32_t>(1u, std::min<uint32_t>((n + kTraceThreads - 1) / kTraceThreads, ls.grid_trace));
+    k_trace_rays<D><<<grid, kTraceThreads, stack_bytes(D), stream>>>(s, n, origins, dirs, t_min, inst_id, prim, t,
+                                                                      bary, cnt);
+  });
+  OLC_LAUNCH_CHECK("k_trace_rays");
+}
+
+void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins,
+                          const float* dirs, float t_min, const float* t_max, uint8_t* occ, Counters* cnt,
+                          cudaStream_t stream) {
+  dispatch_stack(ls.stack_depth, [&](auto depth) {
+    constexpr int D = decltype(depth)::value;
+    uint32_t grid = std::max<uint32_t>(1u, std::min<uint32_t>((n + kTraceThreads - 1) / kTraceThreads, ls.grid_trace));
+    k_occluded_rays<D><<<grid, kTraceThreads, stack_bytes(D), stream>>>(s, n, origins, dirs, t_min, t_max, occ, cnt);
+  });
+  OLC_LAUNCH_CHECK("k_occluded_rays");
+}
+
+void configure_trace_kernels() {
+  // Opt every traversal instantiation into the shared-memory carve-out it
+  // needs (default limit is 48 KB per block; ours stay below it, but the
+  // preferred carve-out lets more blocks share one SM).
+  auto prefer = [](const void* fn) { cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100); };
+  prefer((const void*)k_trace_closest<16>);
+  prefer((const void*)k_trace_closest<24>);
+  prefer((const void*)k_trace_closest<32>);
+  prefer((const void*)k_trace_shadow<16>);
+  prefer((const void*)k_trace_shadow<24>);
+  prefer((const void*)k_trace_shadow<32>);
+}
+
+}  // namespace olc

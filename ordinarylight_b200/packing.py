@@ -1,0 +1,311 @@
+"""Scene and camera packing for the C ABI.
+
+Works on any object with the reference's scene surface (``visible_meshes``,
+mesh ``vertices``/``indices``/``normals``/``transform``/``material``/
+``resource``/``id``, ``lights``, ``environment``, ``visible_volumes``), so the
+reference's ``ordinarylight.Scene`` and this package's mirror both pack.
+
+Geometry stays indexed in object space: one bottom-level mesh per distinct
+``MeshResource`` (or per resource-less ``Mesh``), one instance per visible
+mesh with triangles, in ``visible_meshes`` order.  The instance's packed
+primitive base is the running triangle count in that order, so the
+device-reported primitive index equals the index into ``Scene.triangles()``
+(ordinarylight/scene/_core.py:2732-2753) that the CPU reference reports.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+import math
+
+import numpy as np
+
+from . import _native
+
+_LUMINANCE = np.array((0.2126, 0.7152, 0.0722), np.float64)
+
+
+@dataclass
+class PackedScene:
+    mesh_vertex_offset: np.ndarray
+    mesh_triangle_offset: np.ndarray
+    vertices: np.ndarray
+    normals: np.ndarray
+    indices: np.ndarray
+    instance_object_to_world: np.ndarray
+    instance_mesh: np.ndarray
+    instance_material: np.ndarray
+    instance_id: np.ndarray
+    instance_primitive_offset: np.ndarray
+    materials: np.ndarray
+    emitters: np.ndarray
+    emissive_weight: float
+    lights: np.ndarray
+    environment_kind: int
+    environment_color: tuple
+    environment_rotation: float
+    environment_image: np.ndarray | None
+    volume: dict | None
+    total_triangles: int
+
+    def descriptor(self) -> _native.OlcSceneDesc:
+        d = _native.OlcSceneDesc()
+        f32, u32 = _native.c_float, _native.c_uint32
+        d.num_meshes = len(self.mesh_vertex_offset) - 1
+        d.mesh_vertex_offset = _native.typed_ptr(self.mesh_vertex_offset, u32)
+        d.mesh_triangle_offset = _native.typed_ptr(self.mesh_triangle_offset, u32)
+        d.vertices = _native.typed_ptr(self.vertices, f32)
+        d.normals = _native.typed_ptr(self.normals, f32)
+        d.indices = _native.typed_ptr(self.indices, u32)
+        d.num_instances = len(self.instance_mesh)
+        d.instance_object_to_world = _native.typed_ptr(self.instance_object_to_world, f32)
+        d.instance_mesh = _native.typed_ptr(self.instance_mesh, u32)
+        d.instance_material = _native.typed_ptr(self.instance_material, u32)
+        d.instance_id = _native.typed_ptr(self.instance_id, u32)
+        d.instance_primitive_offset = _native.typed_ptr(self.instance_primitive_offset, u32)
+        d.num_materials = len(self.materials)
+        d.materials = _native.typed_ptr(self.materials, f32)
+        d.num_emitters = len(self.emitters)
+        d.emitters = _native.typed_ptr(self.emitters if len(self.emitters) else None, f32)
+        d.emissive_weight = float(self.emissive_weight)
+        d.num_lights = len(self.lights)
+        d.lights = _native.typed_ptr(self.lights if len(self.lights) else None, f32)
+        d.environment_kind = self.environment_kind
+        for k in range(3):
+            d.environment_color[k] = float(self.environment_color[k])
+        d.environment_rotation = float(self.environment_rotation)
+        if self.environment_image is not None:
+            d.environment_height, d.environment_width = self.environment_image.shape[:2]
+            d.environment_image = _native.typed_ptr(self.environment_image, f32)
+        if self.volume is not None:
+            v = self.volume
+            d.volume_present = 1
+            nz, ny, nx = v["density"].shape
+            d.volume_dims[0], d.volume_dims[1], d.volume_dims[2] = nx, ny, nz
+            d.volume_density = _native.typed_ptr(v["density"], f32)
+            for k in range(12):
+                d.volume_world_to_box[k] = float(v["world_to_box"].reshape(-1)[k])
+            d.volume_sigma_t_scale = float(v["sigma_t_scale"])
+            d.volume_albedo = float(v["albedo"])
+            d.volume_max_density = float(v["max_density"])
+        return d
+
+
+def _material_record(material, material_id: int) -> np.ndarray:
+    rec = np.zeros(16, np.float32)
+    rec[0:3] = np.asarray(material.base_color, np.float32)
+    rec[3] = float(getattr(material, "roughness", 1.0))
+    rec[4:7] = np.asarray(material.emission, np.float32)
+    rec[7] = float(getattr(material, "metallic", 0.0))
+    rec[8] = 1.0 if getattr(material, "emission_two_sided", False) else 0.0
+    rec[9] = np.array([material_id], np.uint32).view(np.float32)[0]
+    return rec
+
+
+def emitter_records(scene):
+    """Emissive triangles with a power CDF: the records and probabilities of
+    Scene.emissive_triangle_data (scene/_core.py:2637-2691), computed with
+    array operations.  Returns (records [n, 20] float32, total weight)."""
+    chunks, weights, sided = [], [], []
+    for mesh in scene.visible_meshes:
+        emission = np.asarray(mesh.material.emission, np.float32)
+        if not np.any(emission > 0.0) or not len(mesh.indices):
+            continue
+        tris = mesh.world_vertices[mesh.indices]
+        area = 0.5 * np.linalg.norm(np.cross(tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0]), axis=1)
+        keep = area > 1e-12
+        if not np.any(keep):
+            continue
+        tris, area = tris[keep], area[keep]
+        rec = np.zeros((len(tris), 20), np.float32)
+        rec[:, 0:3] = tris[:, 0]
+        rec[:, 4:7] = tris[:, 1]
+        rec[:, 8:11] = tris[:, 2]
+        rec[:, 12:15] = emission
+        rec[:, 15] = area
+        chunks.append(rec)
+        weights.append(area.astype(np.float64) * float(np.dot(emission.astype(np.float64), _LUMINANCE)))
+        sided.append(np.full(len(tris), 1.0 if getattr(mesh.material, "emission_two_sided", False) else 0.0,
+                             np.float32))
+    if not chunks:
+        return np.zeros((0, 20), np.float32), 0.0
+    rec = np.concatenate(chunks)
+    w = np.concatenate(weights)
+    total = float(w.sum())
+    prob = w / total if total > 0.0 else np.full(len(w), 1.0 / len(w))
+    cdf = np.cumsum(prob)
+    cdf[-1] = 1.0
+    rec[:, 16] = cdf.astype(np.float32)
+    rec[:, 17] = prob.astype(np.float32)
+    rec[:, 18] = np.concatenate(sided)
+    return rec, float(scene.emissive_light_weight) if hasattr(scene, "emissive_light_weight") else total
+
+
+def light_records(scene) -> np.ndarray:
+    """Analytic lights in the layout of Scene.analytic_light_data
+    (scene/_core.py:2578-2632), without the environment record."""
+    records = []
+    for light in getattr(scene, "lights", ()):
+        name = type(light).__name__
+        rec = np.zeros((4, 4), np.float32)
+        rec[2, :3] = np.asarray(light.color, np.float32)
+        rec[2, 3] = float(light.intensity)
+        if name == "PointLight":
+            rec[0, :3] = np.asarray(light.position, np.float32)
+            rec[0, 3] = 0.0
+            rec[1, 3] = float(light.range or 0.0)
+        elif name == "DirectionalLight":
+            direction = np.asarray(light.direction, np.float32)
+            rec[0, 3] = 1.0
+            rec[1, :3] = direction / np.linalg.norm(direction)
+        elif name == "SpotLight":
+            direction = np.asarray(light.direction, np.float32)
+            rec[0, :3] = np.asarray(light.position, np.float32)
+            rec[0, 3] = 2.0
+            rec[1, :3] = direction / np.linalg.norm(direction)
+            rec[1, 3] = float(light.range or 0.0)
+            rec[3, 0] = math.cos(light.inner_cone_angle)
+            rec[3, 1] = math.cos(light.outer_cone_angle)
+        else:
+            raise TypeError(f"unsupported light type {name}")
+        records.append(rec.reshape(-1))
+    if not records:
+        return np.zeros((0, 16), np.float32)
+    return np.ascontiguousarray(np.stack(records), np.float32)
+
+
+def _volume_record(scene):
+    volumes = tuple(getattr(scene, "visible_volumes", ()))
+    if not volumes:
+        return None
+    if len(volumes) > 1:
+        raise RuntimeError("the CUDA renderer supports one visible volume per scene")
+    vol = volumes[0]
+    density = np.ascontiguousarray(getattr(vol, "data", None), np.float32)
+    if density.ndim != 3:
+        raise RuntimeError("volume data must be a dense 3D grid")
+    material = getattr(vol, "material", None)
+    sigma = float(getattr(material, "sigma_t_scale", getattr(material, "density_scale", 1.0)))
+    albedo = float(getattr(material, "albedo", 0.9)) if material is not None else 0.9
+    w2b = np.linalg.inv(np.asarray(vol.transform.matrix, np.float64))[:3, :4].astype(np.float32)
+    return {"density": density, "world_to_box": w2b, "sigma_t_scale": sigma, "albedo": albedo,
+            "max_density": float(density.max()) if density.size else 0.0}
+
+
+def pack_scene(scene) -> PackedScene:
+    """Flatten a scene into the arrays of olc_scene_desc."""
+    mesh_index = {}
+    vertices, normals, indices = [], [], []
+    v_off, t_off = [0], [0]
+    inst_xf, inst_mesh, inst_mat, inst_id, inst_prim = [], [], [], [], []
+    materials, material_index = [], {}
+    prim = 0
+    material_id = getattr(scene, "material_id", None)
+    for mesh in scene.visible_meshes:
+        count = len(mesh.indices)
+        if count == 0:
+            continue
+        key = id(mesh.resource) if getattr(mesh, "resource", None) is not None else id(mesh)
+        if key not in mesh_index:
+            mesh_index[key] = len(v_off) - 1
+            verts = np.ascontiguousarray(mesh.vertices, np.float32).reshape(-1, 3)
+            vertices.append(verts)
+            n = getattr(mesh, "normals", None)
+            normals.append(np.ascontiguousarray(n if n is not None else np.zeros_like(verts), np.float32))
+            indices.append(np.ascontiguousarray(mesh.indices, np.uint32).reshape(-1, 3))
+            v_off.append(v_off[-1] + len(verts))
+            t_off.append(t_off[-1] + len(mesh.indices))
+        mat = mesh.material
+        if id(mat) not in material_index:
+            mid = 0
+            if callable(material_id):
+                try:
+                    mid = int(material_id(mat))
+                except KeyError:
+                    mid = 0
+            material_index[id(mat)] = len(materials)
+            materials.append(_material_record(mat, mid))
+        inst_xf.append(np.asarray(mesh.transform.matrix, np.float32)[:3, :4].reshape(-1))
+        inst_mesh.append(mesh_index[id(mesh.resource) if getattr(mesh, "resource", None) is not None else id(mesh)])
+        inst_mat.append(material_index[id(mat)])
+        inst_id.append(int(mesh.id) if mesh.id is not None else 0)
+        inst_prim.append(prim)
+        prim += count
+    emitters, weight = emitter_records(scene)
+    env = getattr(scene, "environment", None)
+    env_kind, env_color, env_rot, env_img = _native.ENV_NONE, (0.0, 0.0, 0.0), 0.0, None
+    if env is not None:
+        env_color = tuple(float(c) * float(env.intensity) for c in env.color)
+        env_rot = float(env.rotation)
+        if getattr(env, "image", None) is not None:
+            env_kind = _native.ENV_EQUIRECT
+            env_img = np.ascontiguousarray(np.asarray(env.image, np.float32)[..., :3])
+        else:
+            env_kind = _native.ENV_CONSTANT
+
+    def stack(parts, dtype, shape):
+        return np.ascontiguousarray(np.concatenate(parts), dtype) if parts else np.zeros(shape, dtype)
+
+    return PackedScene(
+        mesh_vertex_offset=np.asarray(v_off, np.uint32),
+        mesh_triangle_offset=np.asarray(t_off, np.uint32),
+        vertices=stack(vertices, np.float32, (0, 3)),
+        normals=stack(normals, np.float32, (0, 3)),
+        indices=stack(indices, np.uint32, (0, 3)),
+        instance_object_to_world=np.ascontiguousarray(np.asarray(inst_xf, np.float32).reshape(-1, 12)),
+        instance_mesh=np.asarray(inst_mesh, np.uint32),
+        instance_material=np.asarray(inst_mat, np.uint32),
+        instance_id=np.asarray(inst_id, np.uint32),
+        instance_primitive_offset=np.asarray(inst_prim, np.uint32),
+        materials=np.ascontiguousarray(np.asarray(materials, np.float32).reshape(-1, 16)),
+        emitters=np.ascontiguousarray(emitters),
+        emissive_weight=weight,
+        lights=light_records(scene),
+        environment_kind=env_kind,
+        environment_color=env_color,
+        environment_rotation=env_rot,
+        environment_image=env_img,
+        volume=_volume_record(scene),
+        total_triangles=prim,
+    )
+
+
+def camera_kind(camera) -> int:
+    name = type(camera).__name__
+    if name == "PanoramicCamera" or hasattr(camera, "horizontal_fov_degrees"):
+        return _native.PROJECTION_PANORAMIC
+    if name == "OrthographicCamera" or hasattr(camera, "vertical_size"):
+        return _native.PROJECTION_ORTHOGRAPHIC
+    return _native.PROJECTION_PERSPECTIVE
+
+
+def camera_basis(camera):
+    """Camera frame in float32, computed as ReferencePathTracer._camera_rays
+    does (path_tracer.py:110-116)."""
+    position = np.asarray(camera.position, dtype=np.float32)
+    forward = np.asarray(camera.target, dtype=np.float32) - position
+    forward /= np.linalg.norm(forward)
+    right = np.cross(forward, np.asarray(camera.up, dtype=np.float32))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, forward)
+    return position, forward, right, up
+
+
+def pack_camera(camera) -> _native.OlcCamera:
+    position, forward, right, up = camera_basis(camera)
+    cam = _native.OlcCamera()
+    for k in range(3):
+        cam.position[k] = float(position[k])
+        cam.forward[k] = float(forward[k])
+        cam.right[k] = float(right[k])
+        cam.up[k] = float(up[k])
+    kind = camera_kind(camera)
+    cam.projection = kind
+    if kind == _native.PROJECTION_PANORAMIC:
+        cam.horizontal_half = math.radians(camera.horizontal_fov_degrees) * 0.5
+        cam.vertical_half = math.radians(camera.vertical_fov_degrees) * 0.5
+    elif kind == _native.PROJECTION_ORTHOGRAPHIC:
+        cam.half_height = float(camera.vertical_size) * 0.5
+    else:
+        cam.half_height = math.tan(math.radians(camera.vertical_fov_degrees) / 2.0)
+    return cam

@@ -1,0 +1,395 @@
+"""``renderers.cuda``: the B200 wavefront path tracer behind RendererProtocol.
+
+A drop-in ``RendererImplementation`` for OrdinaryLight's renderer facade:
+``ol.Renderer(implementation=CudaWavefrontRenderer(...))`` (or the
+``renderer_preference="cuda"`` route of :func:`ordinarylight_b200.Renderer`)
+renders ``(height, width, 4)`` float32 linear HDR through hand-written sm_100a
+kernels in ``libolcuda.so``.  It replaces the Vulkan GI engine's offscreen
+path (``_VulkanGlobalIlluminationEngine.render_frame`` ->
+``render_wavefront_outputs``, ordinarylight/targets/vulkan/api.py:1233-1451)
+and matches the contract of ``CpuReferenceRenderer``
+(ordinarylight/renderers/reference/cpu.py:24-75):
+
+* ``render_frame(scene, camera, w, h, *, samples=None, frame_index=0)``;
+  the seed of a frame is ``config.seed + frame_index`` and identical
+  (scene, camera, size, samples, frame_index) give identical bytes;
+* ``ValueError`` for invalid sizes and sample counts, ``RuntimeError`` after
+  ``close()`` (which is idempotent);
+* ``last_timings`` with ``total_ms``/``gpu_ms`` (read by RenderStatistics,
+  ordinarylight/renderer/_core.py:43-96) plus ray counts and Mrays/s.
+
+``mode="reference_compatible"`` reproduces the CPU reference's estimator
+(Lambert, emission on every hit, CPU sky, no NEE) for parity; the default
+``mode="production"`` is the GPU wavefront's GGX/Lambert transport with
+next-event estimation, MIS, Russian roulette and optional ReSTIR DI.
+"""
+
+from __future__ import annotations
+
+from dataclasses import asdict, dataclass, fields, replace
+import ctypes
+import time
+
+import numpy as np
+
+from .. import _native
+from ..packing import pack_camera, pack_scene
+from .base import RendererImplementation, RendererImplementationInfo
+
+_MODES = {"production": _native.MODE_PRODUCTION, "reference_compatible": _native.MODE_REFERENCE_COMPATIBLE}
+_PRODUCTS = ("color", "depth", "normal", "instance_id", "object_id", "material_id")
+
+
+@dataclass(frozen=True)
+class CudaRendererConfig:
+    """Frozen renderer configuration: ReferenceConfig's fields
+    (cpu.py:9-21) plus the wavefront knobs."""
+
+    samples_per_pixel: int = 1
+    max_bounces: int = 3
+    seed: int = 1
+    mode: str = "production"
+    device: int = 0
+    russian_roulette_start: int = 3
+    russian_roulette_min_survival: float = 0.1
+    restir: bool = False
+    restir_candidates: int = 32
+    restir_temporal: bool = True
+    restir_spatial: int = 1
+    restir_neighbours: int = 5
+    restir_radius: float = 30.0
+    restir_max_history: int = 20
+    block_size: int = 256
+    stack_depth: int = 24
+    chunk_paths: int = 0
+    use_graphs: bool = True
+
+    def __post_init__(self):
+        if not 1 <= int(self.samples_per_pixel) <= 65536:
+            raise ValueError("samples_per_pixel must be between 1 and 65536")
+        if not 1 <= int(self.max_bounces) <= 64:
+            raise ValueError("max_bounces must be between 1 and 64")
+        if int(self.seed) < 0:
+            raise ValueError("seed cannot be negative")
+        if self.mode not in _MODES:
+            raise ValueError(f"mode must be one of {tuple(_MODES)}")
+        if int(self.device) < 0:
+            raise ValueError("device cannot be negative")
+        if not 0 <= int(self.russian_roulette_start) <= 64:
+            raise ValueError("russian_roulette_start must be between 0 and 64")
+        if not 0.0 <= float(self.russian_roulette_min_survival) <= 1.0:
+            raise ValueError("russian_roulette_min_survival must be between 0 and 1")
+        if not 1 <= int(self.restir_candidates) <= 64:
+            raise ValueError("restir_candidates must be between 1 and 64")
+        if not 0 <= int(self.restir_spatial) <= 4:
+            raise ValueError("restir_spatial must be between 0 and 4")
+        if not 0 <= int(self.restir_neighbours) <= 16:
+            raise ValueError("restir_neighbours must be between 0 and 16")
+        if not float(self.restir_radius) > 0.0:
+            raise ValueError("restir_radius must be positive")
+        if int(self.stack_depth) not in (16, 24, 32):
+            raise ValueError("stack_depth must be 16, 24 or 32")
+        if int(self.block_size) % 32 or not 64 <= int(self.block_size) <= 1024:
+            raise ValueError("block_size must be a multiple of 32 in [64, 1024]")
+        if int(self.chunk_paths) < 0:
+            raise ValueError("chunk_paths cannot be negative")
+
+    def native(self) -> _native.OlcConfig:
+        c = _native.OlcConfig()
+        c.device = int(self.device)
+        c.mode = _MODES[self.mode]
+        c.max_bounces = int(self.max_bounces)
+        c.seed = int(self.seed) & 0xFFFFFFFF
+        c.russian_roulette_start = int(self.russian_roulette_start)
+        c.russian_roulette_min_survival = float(self.russian_roulette_min_survival)
+        c.restir = int(bool(self.restir))
+        c.restir_candidates = int(self.restir_candidates)
+        c.restir_temporal = int(bool(self.restir_temporal))
+        c.restir_spatial = int(self.restir_spatial)
+        c.restir_neighbours = int(self.restir_neighbours)
+        c.restir_radius = float(self.restir_radius)
+        c.restir_max_history = int(self.restir_max_history)
+        c.block_size = int(self.block_size)
+        c.stack_depth = int(self.stack_depth)
+        c.chunk_paths = int(self.chunk_paths)
+        c.use_graphs = int(bool(self.use_graphs))
+        return c
+
+
+class CudaWavefrontRenderer(RendererImplementation):
+    """Wavefront path tracer on one CUDA device (sm_100a kernels)."""
+
+    available_outputs = _PRODUCTS
+    implementation = RendererImplementationInfo(name="cuda-wavefront", family="global_illumination",
+                                                graphics_api="cuda")
+
+    def __init__(self, config: CudaRendererConfig | None = None, **options):
+        if config is not None and options:
+            raise TypeError("pass config or renderer options, not both")
+        self.config = config or CudaRendererConfig(**options)
+        if not isinstance(self.config, CudaRendererConfig):
+            raise TypeError("config must be a CudaRendererConfig")
+        self._lib = _native.load()
+        handle = ctypes.c_void_p()
+        _native.check(self._lib, None, self._lib.olc_create(ctypes.byref(self.config.native()),
+                                                             ctypes.byref(handle)))
+        self._ctx = handle
+        self._closed = False
+        self._scene_key = None
+        self._packed = None
+        self.last_timings = {}
+        self.device = f"cuda:{self.config.device}"
+
+    # -- identity / capabilities --------------------------------------------
+    @property
+    def capabilities(self):
+        return {
+            "renderer": "cuda-wavefront",
+            "outputs": self.available_outputs,
+            "features": frozenset({"offscreen_rendering", "instancing", "next_event_estimation",
+                                   "restir_di", "deterministic_sequences", "resident_scenes"}),
+            "limits": {"max_bounces": 64, "max_samples_per_pixel": 65536},
+            "device": self.device,
+        }
+
+    def _require_open(self):
+        if self._closed:
+            raise RuntimeError("cuda renderer is closed")
+
+    # -- scene residency -------------------------------------------------------
+    def _ensure_scene(self, scene, force=False):
+        key = (id(scene), getattr(scene, "revision", None))
+        if not force and key == self._scene_key:
+            return 0.0
+        t0 = time.perf_counter()
+        packed = pack_scene(scene)
+        desc = packed.descriptor()
+        _native.check(self._lib, self._ctx, self._lib.olc_upload_scene(self._ctx, ctypes.byref(desc)))
+        self._packed = packed
+        self._scene_key = key
+        return (time.perf_counter() - t0) * 1e3
+
+    def replace_scene(self, scene) -> None:
+        """Make ``scene`` resident (ResidentSceneRendererProtocol,
+        ordinarylight/renderers/base.py:106-112).  On failure the previous
+        scene stays resident."""
+        self._require_open()
+        self._ensure_scene(scene, force=True)
+        self.reset_output_history()
+
+    def scene_bytes(self) -> int:
+        value = ctypes.c_uint64()
+        _native.check(self._lib, self._ctx, self._lib.olc_scene_bytes(self._ctx, ctypes.byref(value)))
+        return int(value.value)
+
+    # -- rendering -----------------------------------------------------------
+    def _render(self, scene, camera, width, height, samples, frame_index, out_ptr, out_is_device):
+        width, height = int(width), int(height)
+        if width <= 0 or height <= 0:
+            raise ValueError("width and height must be positive")
+        spp = self.config.samples_per_pixel if samples is None else int(samples)
+        if not 1 <= spp <= 65536:
+            raise ValueError("samples must be between 1 and 65536")
+        frame_index = int(frame_index)
+        if frame_index < 0:
+            raise ValueError("frame_index cannot be negative")
+        t0 = time.perf_counter()
+        upload_ms = self._ensure_scene(scene)
+        cam = pack_camera(camera)
+        stats = _native.OlcRenderStats()
+        status = self._lib.olc_render(self._ctx, ctypes.byref(cam), width, height, spp, frame_index & 0xFFFFFFFF,
+                                      out_ptr, int(out_is_device), ctypes.byref(stats))
+        _native.check(self._lib, self._ctx, status)
+        total_ms = (time.perf_counter() - t0) * 1e3
+        rays = stats.camera_rays + stats.extension_rays + stats.shadow_rays
+        gpu_ms = float(stats.gpu_ms)
+        self.last_timings = {
+            "total_ms": total_ms,
+            "gpu_ms": gpu_ms,
+            "scene_upload_ms": upload_ms,
+            "camera_rays": int(stats.camera_rays),
+            "extension_rays": int(stats.extension_rays),
+            "shadow_rays": int(stats.shadow_rays),
+            "rays": int(rays),
+            "closest_hit_rays": int(stats.camera_rays + stats.extension_rays),
+            "mrays_per_s": rays / (gpu_ms * 1e3) if gpu_ms > 0 else 0.0,
+            "queue_overflow": int(stats.overflow),
+            "traversal_errors": int(stats.traversal_errors),
+            "chunks": int(stats.chunks),
+            "restir_history_used": bool(stats.restir_history_used),
+            "samples_per_pixel": spp,
+        }
+        if stats.traversal_errors:
+            raise RuntimeError(f"{stats.traversal_errors} traversal stack overflows")
+
+    def render_frame(self, scene, camera, width, height, *, samples=None, frame_index=0):
+        """Render one linear-HDR frame as a (height, width, 4) float32 array."""
+        self._require_open()
+        width, height = int(width), int(height)
+        if width <= 0 or height <= 0:
+            raise ValueError("width and height must be positive")
+        out = np.empty((height, width, 4), np.float32)
+        self._render(scene, camera, width, height, samples, frame_index, _native.ptr(out), False)
+        return out
+
+    render_wavefront = render_frame
+
+    def render_frame_into(self, scene, camera, width, height, out, *, samples=None, frame_index=0):
+        """Render into a caller-owned buffer: a host numpy array or a device
+        tensor (anything with ``data_ptr()``) of height*width*4 float32."""
+        self._require_open()
+        on_device = hasattr(out, "data_ptr") and getattr(out, "is_cuda", False)
+        if hasattr(out, "numel"):
+            count = out.numel()
+        else:
+            count = out.size
+            if out.dtype != np.float32 or not out.flags.c_contiguous:
+                raise TypeError("out must be a contiguous float32 array")
+        if count != int(width) * int(height) * 4:
+            raise ValueError("out must hold height*width*4 float32 values")
+        self._render(scene, camera, width, height, samples, frame_index, _native.ptr(out), on_device)
+        return out
+
+    def render_products(self, scene, camera, width, height, *, outputs, samples=None, frame_index=0):
+        """Named products (ProductRendererProtocol, base.py:74-90): ``color``
+        plus the first sample's primary-hit ``depth``, ``normal``,
+        ``instance_id``/``object_id`` and ``material_id`` (shapes of
+        ordinarylight/renderer/_core.py:768-777)."""
+        self._require_open()
+        requested = (outputs,) if isinstance(outputs, str) else tuple(outputs)
+        unknown = [name for name in requested if name not in self.available_outputs]
+        if unknown:
+            raise ValueError(f"unsupported render outputs {tuple(unknown)}")
+        color = self.render_frame(scene, camera, width, height, samples=samples, frame_index=frame_index)
+        h, w = int(height), int(width)
+        depth = np.empty((h, w), np.float32)
+        normal = np.empty((h, w, 3), np.float32)
+        inst = np.empty((h, w), np.uint32)
+        mat = np.empty((h, w), np.uint32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_products(
+            self._ctx, w, h, _native.ptr(depth), _native.ptr(normal), _native.ptr(inst), _native.ptr(mat), None))
+        table = {"color": color, "depth": depth, "normal": normal, "instance_id": inst, "object_id": inst.copy(),
+                 "material_id": mat}
+        return {name: table[name] for name in requested}
+
+    def primitive_ids(self, width, height):
+        """Packed primitive index of the last render's first-sample primary hits."""
+        prim = np.empty((int(height), int(width)), np.uint32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_products(
+            self._ctx, int(width), int(height), None, None, None, None, _native.ptr(prim)))
+        return prim
+
+    # -- tracing primitives ---------------------------------------------------
+    def trace_closest(self, scene, origins, directions, t_min=1e-4):
+        """Closest hits of host rays: (instance_id uint32, primitive int32,
+        t float32, barycentrics (n, 2) float32)."""
+        import torch
+
+        self._require_open()
+        self._ensure_scene(scene)
+        o = torch.as_tensor(np.ascontiguousarray(origins, np.float32).reshape(-1, 3), device=self.device)
+        d = torch.as_tensor(np.ascontiguousarray(directions, np.float32).reshape(-1, 3), device=self.device)
+        n = o.shape[0]
+        inst = torch.empty(n, dtype=torch.int32, device=self.device)
+        prim = torch.empty(n, dtype=torch.int32, device=self.device)
+        t = torch.empty(n, dtype=torch.float32, device=self.device)
+        bary = torch.empty((n, 2), dtype=torch.float32, device=self.device)
+        torch.cuda.synchronize(self.device)
+        _native.check(self._lib, self._ctx, self._lib.olc_trace_closest(
+            self._ctx, n, _native.ptr(o), _native.ptr(d), float(t_min), _native.ptr(inst), _native.ptr(prim),
+            _native.ptr(t), _native.ptr(bary)))
+        return (inst.cpu().numpy().view(np.uint32), prim.cpu().numpy(), t.cpu().numpy(), bary.cpu().numpy())
+
+    def trace_occluded(self, scene, origins, directions, t_max, t_min=1e-3):
+        import torch
+
+        self._require_open()
+        self._ensure_scene(scene)
+        o = torch.as_tensor(np.ascontiguousarray(origins, np.float32).reshape(-1, 3), device=self.device)
+        d = torch.as_tensor(np.ascontiguousarray(directions, np.float32).reshape(-1, 3), device=self.device)
+        tm = torch.as_tensor(np.ascontiguousarray(t_max, np.float32).reshape(-1), device=self.device)
+        occ = torch.empty(o.shape[0], dtype=torch.uint8, device=self.device)
+        torch.cuda.synchronize(self.device)
+        _native.check(self._lib, self._ctx, self._lib.olc_trace_occluded(
+            self._ctx, o.shape[0], _native.ptr(o), _native.ptr(d), float(t_min), _native.ptr(tm), _native.ptr(occ)))
+        return occ.cpu().numpy().astype(bool)
+
+    def camera_rays(self, camera, width, height, *, sample=0, frame_index=0, jitter=None):
+        """Device camera rays of one sample (the raygen kernel's model)."""
+        import torch
+
+        self._require_open()
+        n = int(width) * int(height)
+        o = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        d = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        j = None if jitter is None else np.ascontiguousarray(jitter, np.float32)
+        cam = pack_camera(camera)
+        _native.check(self._lib, self._ctx, self._lib.olc_camera_rays(
+            self._ctx, ctypes.byref(cam), int(width), int(height), int(sample), int(frame_index),
+            _native.ptr(j), _native.ptr(o), _native.ptr(d)))
+        return o.cpu().numpy(), d.cpu().numpy()
+
+    def bvh_info(self):
+        info = _native.OlcBvhInfo()
+        _native.check(self._lib, self._ctx, self._lib.olc_bvh_info_get(self._ctx, ctypes.byref(info)))
+        return {"blas_count": info.blas_count, "blas_nodes": info.blas_nodes, "tlas_nodes": info.tlas_nodes,
+                "triangles": info.triangles, "build_ms": info.build_ms}
+
+    def validate_bvh(self, scene) -> int:
+        self._require_open()
+        self._ensure_scene(scene)
+        bad = ctypes.c_uint64()
+        _native.check(self._lib, self._ctx, self._lib.olc_bvh_validate(self._ctx, ctypes.byref(bad)))
+        return int(bad.value)
+
+    # -- sequencing / configuration ----------------------------------------------
+    def reset_output_history(self):
+        """Forget temporal (ReSTIR) history; called by Renderer.reset_sequence
+        (ordinarylight/renderer/_core.py:339-351)."""
+        self._require_open()
+        _native.check(self._lib, self._ctx, self._lib.olc_reset_history(self._ctx))
+
+    reset_accumulation = reset_output_history
+
+    def reconfigure(self, **changes):
+        """Apply configuration changes in place (Renderer.reconfigure,
+        ordinarylight/renderer/_core.py:386-413)."""
+        self._require_open()
+        names = {f.name for f in fields(CudaRendererConfig)}
+        unknown = set(changes) - names
+        if unknown:
+            raise RuntimeError(f"unsupported settings {sorted(unknown)} require renderer recreation")
+        if "device" in changes and int(changes["device"]) != self.config.device:
+            raise RuntimeError("changing the device requires renderer recreation")
+        config = replace(self.config, **changes)
+        _native.check(self._lib, self._ctx, self._lib.olc_reconfigure(self._ctx, ctypes.byref(config.native())))
+        self.config = config
+        return config
+
+    def close(self):
+        if self._closed:
+            return
+        self._closed = True
+        ctx, self._ctx = self._ctx, None
+        if ctx:
+            self._lib.olc_destroy(ctx)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        self._require_open()
+        return self
+
+    def __exit__(self, *_exc):
+        self.close()
+
+
+def config_dict(config: CudaRendererConfig) -> dict:
+    return asdict(config)
+
+
+__all__ = ["CudaRendererConfig", "CudaWavefrontRenderer"]

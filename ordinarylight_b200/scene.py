@@ -1,0 +1,675 @@
+"""Host scene model: the subset of OrdinaryLight's backend-neutral scene API
+that the wavefront path consumes.
+
+The CUDA renderer reads scenes structurally (``visible_meshes``, each mesh's
+``vertices``/``indices``/``normals``/``transform``/``material``/``resource``/
+``id``, ``lights``, ``environment``, ``visible_volumes``, ``revision``), so it
+accepts the reference's own ``ordinarylight.Scene`` unchanged.  This module
+supplies the same names and semantics for environments without the reference
+package installed:
+
+* ``Transform``   ordinarylight/scene/_core.py:50-114
+* ``Material``    ordinarylight/scene/_core.py:431-553 (parameters the
+                  wavefront path shades with; the rest are accepted and kept)
+* ``Mesh`` / ``MeshResource`` / ``Instance``  :556-815
+* ``Scene``       :943-3093 (mesh/instance/light/environment/volume
+                  membership, stable ids, revision counters, packing helpers)
+* cameras         ordinarylight/cameras/*.py
+* lights          ordinarylight/lights/*.py
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+import math
+from types import MappingProxyType
+
+import numpy as np
+
+__all__ = [
+    "Transform", "Material", "Mesh", "MeshResource", "Instance", "Scene",
+    "Volume", "VolumeMaterial",
+    "PerspectiveCamera", "OrthographicCamera", "PanoramicCamera",
+    "PointLight", "DirectionalLight", "SpotLight", "EnvironmentLight",
+    "CAMERA_TYPES", "LIGHT_TYPES",
+]
+
+_LUMINANCE = (0.2126, 0.7152, 0.0722)
+
+
+def _vec3(value, name):
+    result = np.asarray(value, dtype=np.float32)
+    if result.shape != (3,):
+        raise ValueError(f"{name} must contain exactly three values")
+    if not np.all(np.isfinite(result)):
+        raise ValueError(f"{name} must be finite")
+    return result
+
+
+# ---------------------------------------------------------------------------
+# cameras (ordinarylight/cameras/)
+# ---------------------------------------------------------------------------
+def _validate_look_at(position, target, up):
+    p, t, u = _vec3(position, "position"), _vec3(target, "target"), _vec3(up, "up")
+    forward = t - p
+    if float(np.linalg.norm(forward)) < 1e-8:
+        raise ValueError("camera position and target must differ")
+    if float(np.linalg.norm(np.cross(forward, u))) < 1e-8:
+        raise ValueError("camera up vector must not be parallel to the view direction")
+
+
+@dataclass(frozen=True)
+class PerspectiveCamera:
+    """Pinhole camera (ordinarylight/cameras/perspective_camera.py:8-20)."""
+
+    position: tuple
+    target: tuple
+    up: tuple = (0.0, 1.0, 0.0)
+    vertical_fov_degrees: float = 45.0
+
+    def __post_init__(self):
+        _validate_look_at(self.position, self.target, self.up)
+        if not 1.0 <= self.vertical_fov_degrees < 179.0:
+            raise ValueError("vertical_fov_degrees must be in [1, 179)")
+
+
+@dataclass(frozen=True)
+class OrthographicCamera:
+    """Parallel projection (ordinarylight/cameras/orthographic_camera.py)."""
+
+    position: tuple
+    target: tuple
+    up: tuple = (0.0, 1.0, 0.0)
+    vertical_size: float = 2.0
+
+    def __post_init__(self):
+        _validate_look_at(self.position, self.target, self.up)
+        if not np.isfinite(self.vertical_size) or self.vertical_size <= 0.0:
+            raise ValueError("vertical_size must be finite and positive")
+
+    @property
+    def vertical_fov_degrees(self):
+        return 90.0
+
+
+@dataclass(frozen=True)
+class PanoramicCamera:
+    """Equirectangular camera (ordinarylight/cameras/panoramic_camera.py)."""
+
+    position: tuple
+    target: tuple
+    up: tuple = (0.0, 1.0, 0.0)
+    horizontal_fov_degrees: float = 360.0
+    vertical_fov_degrees: float = 180.0
+
+    def __post_init__(self):
+        _validate_look_at(self.position, self.target, self.up)
+        if not 1.0 <= self.horizontal_fov_degrees <= 360.0:
+            raise ValueError("horizontal_fov_degrees must be in [1, 360]")
+        if not 1.0 <= self.vertical_fov_degrees <= 180.0:
+            raise ValueError("vertical_fov_degrees must be in [1, 180]")
+
+
+CAMERA_TYPES = (PerspectiveCamera, OrthographicCamera, PanoramicCamera)
+
+
+# ---------------------------------------------------------------------------
+# lights (ordinarylight/lights/)
+# ---------------------------------------------------------------------------
+def _validate_color_intensity(color, intensity):
+    c = _vec3(color, "color")
+    if np.any(c < 0.0):
+        raise ValueError("color components cannot be negative")
+    if not math.isfinite(intensity) or intensity < 0.0:
+        raise ValueError("intensity must be finite and non-negative")
+
+
+@dataclass
+class PointLight:
+    position: tuple
+    color: tuple = (1.0, 1.0, 1.0)
+    intensity: float = 1.0
+    range: float | None = None
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        _vec3(self.position, "position")
+        _validate_color_intensity(self.color, self.intensity)
+        if self.range is not None and not (self.range > 0.0):
+            raise ValueError("range must be positive")
+
+
+@dataclass
+class DirectionalLight:
+    direction: tuple
+    color: tuple = (1.0, 1.0, 1.0)
+    intensity: float = 1.0
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        if float(np.linalg.norm(_vec3(self.direction, "direction"))) < 1e-8:
+            raise ValueError("direction cannot be zero")
+        _validate_color_intensity(self.color, self.intensity)
+
+
+@dataclass
+class SpotLight:
+    position: tuple
+    direction: tuple
+    color: tuple = (1.0, 1.0, 1.0)
+    intensity: float = 1.0
+    inner_cone_angle: float = 0.0
+    outer_cone_angle: float = math.pi / 4.0
+    range: float | None = None
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        _vec3(self.position, "position")
+        if float(np.linalg.norm(_vec3(self.direction, "direction"))) < 1e-8:
+            raise ValueError("direction cannot be zero")
+        _validate_color_intensity(self.color, self.intensity)
+        if not 0.0 <= self.inner_cone_angle <= self.outer_cone_angle:
+            raise ValueError("inner_cone_angle must be in [0, outer_cone_angle]")
+        if not 0.0 < self.outer_cone_angle <= math.pi / 2.0:
+            raise ValueError("outer_cone_angle must be in (0, pi/2]")
+
+
+@dataclass(frozen=True)
+class EnvironmentLight:
+    """Constant or equirectangular environment (lights/environment_light.py)."""
+
+    image: np.ndarray | None = field(default=None, compare=False, repr=False)
+    color: tuple = (1.0, 1.0, 1.0)
+    intensity: float = 1.0
+    rotation: float = 0.0
+
+    def __post_init__(self):
+        _validate_color_intensity(self.color, self.intensity)
+        if not math.isfinite(self.rotation):
+            raise ValueError("environment rotation must be finite")
+        if self.image is None:
+            return
+        image = np.array(self.image, dtype=np.float32, copy=True, order="C")
+        if image.ndim != 3 or image.shape[2] not in (3, 4) or min(image.shape[:2]) < 1:
+            raise ValueError("environment image must have shape (height, width, 3 or 4)")
+        image = np.ascontiguousarray(image[..., :3])
+        if not np.all(np.isfinite(image)) or np.any(image < 0.0):
+            raise ValueError("environment image radiance must be finite and non-negative")
+        image.flags.writeable = False
+        object.__setattr__(self, "image", image)
+
+
+LIGHT_TYPES = (PointLight, DirectionalLight, SpotLight)
+
+
+# ---------------------------------------------------------------------------
+# geometry
+# ---------------------------------------------------------------------------
+@dataclass(frozen=True)
+class Transform:
+    """Immutable affine object-to-world transform (scene/_core.py:50-114)."""
+
+    matrix: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32), compare=False, repr=False)
+
+    def __post_init__(self):
+        m = np.array(self.matrix, dtype=np.float32, copy=True)
+        if m.shape != (4, 4):
+            raise ValueError("transform matrix must have shape (4, 4)")
+        if not np.all(np.isfinite(m)):
+            raise ValueError("transform matrix must contain finite values")
+        if not np.allclose(m[3], (0.0, 0.0, 0.0, 1.0), atol=1e-6):
+            raise ValueError("transform matrix must be affine")
+        if abs(float(np.linalg.det(m[:3, :3]))) < 1e-10:
+            raise ValueError("transform linear component must be invertible")
+        m.setflags(write=False)
+        object.__setattr__(self, "matrix", m)
+
+    @classmethod
+    def translation(cls, offset):
+        m = np.eye(4, dtype=np.float32)
+        m[:3, 3] = _vec3(offset, "translation")
+        return cls(m)
+
+    @classmethod
+    def scale(cls, factors):
+        v = np.asarray(factors, dtype=np.float32)
+        if v.ndim == 0:
+            v = np.repeat(v, 3)
+        m = np.eye(4, dtype=np.float32)
+        m[:3, :3] = np.diag(_vec3(v, "scale"))
+        return cls(m)
+
+    @classmethod
+    def rotation(cls, axis, angle_radians):
+        """Rotation about ``axis`` (Rodrigues' formula)."""
+        a = _vec3(axis, "rotation axis").astype(np.float64)
+        n = float(np.linalg.norm(a))
+        if n < 1e-8:
+            raise ValueError("rotation axis cannot be zero")
+        a /= n
+        k = np.array([[0.0, -a[2], a[1]], [a[2], 0.0, -a[0]], [-a[1], a[0], 0.0]])
+        r = np.eye(3) + math.sin(angle_radians) * k + (1.0 - math.cos(angle_radians)) * (k @ k)
+        m = np.eye(4, dtype=np.float32)
+        m[:3, :3] = r
+        return cls(m)
+
+    def __matmul__(self, other):
+        if not isinstance(other, Transform):
+            return NotImplemented
+        return Transform(self.matrix @ other.matrix)
+
+
+@dataclass(frozen=True)
+class Material:
+    """PBR material (scene/_core.py:431-553)."""
+
+    base_color: tuple = (0.8, 0.8, 0.8)
+    emission: tuple = (0.0, 0.0, 0.0)
+    metallic: float = 0.0
+    roughness: float = 1.0
+    transmission: float = 0.0
+    ior: float = 1.5
+    opacity: float = 1.0
+    emission_two_sided: bool = False
+
+    def __post_init__(self):
+        color = _vec3(self.base_color, "base_color")
+        emission = _vec3(self.emission, "emission")
+        if np.any(color < 0.0) or np.any(color > 1.0):
+            raise ValueError("base_color components must be between zero and one")
+        if np.any(emission < 0.0):
+            raise ValueError("emission components cannot be negative")
+        for name in ("metallic", "roughness", "transmission", "opacity"):
+            if not 0.0 <= getattr(self, name) <= 1.0:
+                raise ValueError(f"{name} must be between zero and one")
+        if self.ior <= 0.0:
+            raise ValueError("ior must be positive")
+        if not isinstance(self.emission_two_sided, bool):
+            raise TypeError("emission_two_sided must be a bool")
+
+
+def _generate_normals(vertices, indices):
+    """Area-weighted vertex normals with identical positions welded, the
+    convention of Mesh._generate_normals (scene/_core.py:716-738)."""
+    normals = np.zeros_like(vertices)
+    if len(indices):
+        tri = vertices[indices]
+        face = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+        for corner in range(3):
+            np.add.at(normals, indices[:, corner], face)
+    _unique, groups = np.unique(vertices, axis=0, return_inverse=True)
+    groups = groups.reshape(-1)
+    welded = np.zeros((len(_unique), 3), dtype=np.float32)
+    np.add.at(welded, groups, normals)
+    normals = welded[groups]
+    lengths = np.linalg.norm(normals, axis=1)
+    missing = lengths < 1e-8
+    normals[~missing] /= lengths[~missing, None]
+    normals[missing] = (0.0, 1.0, 0.0)
+    return np.ascontiguousarray(normals, dtype=np.float32)
+
+
+@dataclass
+class Mesh:
+    """Placed triangle geometry (scene/_core.py:556-715)."""
+
+    vertices: np.ndarray
+    indices: np.ndarray
+    material: Material = field(default_factory=Material)
+    normals: np.ndarray | None = None
+    transform: Transform = field(default_factory=Transform)
+    resource: "MeshResource | None" = field(default=None, repr=False)
+    visible: bool = True
+    name: str | None = None
+    metadata: dict = field(default_factory=dict, repr=False)
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        if not isinstance(self.visible, bool):
+            raise TypeError("visible must be a bool")
+        if not isinstance(self.transform, Transform):
+            self.transform = Transform(self.transform)
+        self.metadata = MappingProxyType(dict(self.metadata))
+        if self.resource is not None:
+            self.vertices = self.resource.vertices
+            self.indices = self.resource.indices
+            self.normals = self.resource.normals
+            return
+        self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float32)
+        self.indices = np.ascontiguousarray(self.indices, dtype=np.uint32)
+        if self.vertices.ndim != 2 or self.vertices.shape[1] != 3:
+            raise ValueError("vertices must have shape (vertex_count, 3)")
+        if self.indices.ndim != 2 or self.indices.shape[1] != 3:
+            raise ValueError("indices must have shape (triangle_count, 3)")
+        if self.indices.size and int(self.indices.max()) >= len(self.vertices):
+            raise ValueError("an index refers to a vertex that does not exist")
+        if self.normals is None:
+            self.normals = _generate_normals(self.vertices, self.indices)
+        else:
+            n = np.ascontiguousarray(self.normals, dtype=np.float32)
+            if n.shape != self.vertices.shape:
+                raise ValueError("normals must have the same shape as vertices")
+            lengths = np.linalg.norm(n, axis=1)
+            if np.any(lengths < 1e-8):
+                raise ValueError("normals cannot contain zero vectors")
+            self.normals = n / lengths[:, None]
+
+    @property
+    def world_vertices(self):
+        linear = self.transform.matrix[:3, :3]
+        translation = self.transform.matrix[:3, 3]
+        return np.ascontiguousarray(self.vertices @ linear.T + translation, dtype=np.float32)
+
+    @property
+    def world_normals(self):
+        normal_matrix = np.linalg.inv(self.transform.matrix[:3, :3]).T
+        result = self.normals @ normal_matrix.T
+        result /= np.linalg.norm(result, axis=1, keepdims=True)
+        return np.ascontiguousarray(result, dtype=np.float32)
+
+
+@dataclass
+class MeshResource:
+    """Reusable object-space geometry shared by instances (scene/_core.py:776-810)."""
+
+    vertices: np.ndarray
+    indices: np.ndarray
+    material: Material = field(default_factory=Material)
+    normals: np.ndarray | None = None
+    name: str | None = None
+    metadata: dict = field(default_factory=dict, repr=False)
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        checked = Mesh(self.vertices, self.indices, self.material, normals=self.normals)
+        self.vertices = checked.vertices
+        self.indices = checked.indices
+        self.normals = checked.normals
+        self.vertices.flags.writeable = False
+        self.indices.flags.writeable = False
+        self.normals.flags.writeable = False
+
+
+class Instance(Mesh):
+    """A placed occurrence of a MeshResource."""
+
+
+@dataclass
+class VolumeMaterial:
+    """Participating-medium parameters of a dense density grid."""
+
+    sigma_t_scale: float = 1.0
+    albedo: float = 0.9
+
+    def __post_init__(self):
+        if not (self.sigma_t_scale >= 0.0 and math.isfinite(self.sigma_t_scale)):
+            raise ValueError("sigma_t_scale must be finite and non-negative")
+        if not 0.0 <= self.albedo <= 1.0:
+            raise ValueError("albedo must be between zero and one")
+
+
+@dataclass
+class Volume:
+    """Dense density grid (z, y, x) filling the unit box [0,1]^3 under
+    ``transform`` (scene/_core.py:249-400)."""
+
+    data: np.ndarray
+    material: VolumeMaterial = field(default_factory=VolumeMaterial)
+    transform: Transform = field(default_factory=Transform)
+    visible: bool = True
+    name: str | None = None
+    id: int | None = field(default=None, init=False)
+
+    def __post_init__(self):
+        d = np.ascontiguousarray(self.data, dtype=np.float32)
+        if d.ndim != 3 or min(d.shape) < 1:
+            raise ValueError("volume data must be a non-empty 3D array")
+        if not np.all(np.isfinite(d)) or np.any(d < 0.0):
+            raise ValueError("volume densities must be finite and non-negative")
+        d.flags.writeable = False
+        self.data = d
+        if not isinstance(self.transform, Transform):
+            self.transform = Transform(self.transform)
+
+
+class Scene:
+    """Scene container with stable ids and revision counters
+    (scene/_core.py:943-3093)."""
+
+    def __init__(self, meshes=(), lights=(), mesh_resources=(), volumes=(), environment=None, metadata=None):
+        self.meshes = []
+        self.lights = []
+        self.mesh_resources = []
+        self.volumes = []
+        self.environment = None
+        self.metadata = dict(metadata or {})
+        self._revision = 0
+        self._geometry_revision = 0
+        self._shading_revision = 0
+        self._transform_revision = 0
+        self._next_resource_id = 1
+        self._next_mesh_resource_id = 1
+        self._next_material_id = 1
+        self._material_ids = {}
+        for resource in mesh_resources:
+            self._attach_mesh_resource(resource)
+            self.mesh_resources.append(resource)
+        for mesh in meshes:
+            if not isinstance(mesh, Mesh):
+                raise TypeError("scene resources must be mesh or light objects")
+            self._attach(mesh)
+            self._register_material(mesh.material)
+            self.meshes.append(mesh)
+        for light in lights:
+            self.add_light(light)
+        for volume in volumes:
+            self._attach(volume)
+            self.volumes.append(volume)
+        if environment is not None:
+            self.set_environment(environment)
+
+    # -- identity and revisions -------------------------------------------
+    @property
+    def revision(self):
+        return self._revision
+
+    @property
+    def geometry_revision(self):
+        return self._geometry_revision
+
+    @property
+    def shading_revision(self):
+        return self._shading_revision
+
+    @property
+    def transform_revision(self):
+        return self._transform_revision
+
+    def _changed(self, *, geometry=False, shading=False, transform=False):
+        self._revision += 1
+        self._geometry_revision += int(geometry)
+        self._shading_revision += int(shading)
+        self._transform_revision += int(transform)
+
+    def _attach(self, resource):
+        if resource.id is not None:
+            raise ValueError("a scene resource cannot belong to multiple scenes")
+        resource.id = self._next_resource_id
+        self._next_resource_id += 1
+
+    def _attach_mesh_resource(self, resource):
+        if resource.id is not None:
+            raise ValueError("a mesh resource cannot belong to multiple scenes")
+        resource.id = self._next_mesh_resource_id
+        self._next_mesh_resource_id += 1
+
+    def _register_material(self, material):
+        existing = self._material_ids.get(id(material))
+        if existing is not None and existing[0] is material:
+            return existing[1]
+        material_id = self._next_material_id
+        self._next_material_id += 1
+        self._material_ids[id(material)] = (material, material_id)
+        return material_id
+
+    def material_id(self, material):
+        existing = self._material_ids.get(id(material))
+        if existing is None or existing[0] is not material:
+            raise KeyError("material is not attached to this scene")
+        return existing[1]
+
+    # -- membership -------------------------------------------------------
+    @property
+    def instances(self):
+        return tuple(self.meshes)
+
+    @property
+    def visible_meshes(self):
+        return tuple(mesh for mesh in self.meshes if mesh.visible)
+
+    @property
+    def visible_volumes(self):
+        return tuple(volume for volume in self.volumes if volume.visible)
+
+    def create_mesh(self, vertices, indices, material=None, *, normals=None, name=None, metadata=None):
+        resource = MeshResource(vertices, indices, material or Material(), normals=normals, name=name,
+                                metadata={} if metadata is None else metadata)
+        self._attach_mesh_resource(resource)
+        self.mesh_resources.append(resource)
+        return resource
+
+    create_mesh_resource = create_mesh
+
+    def add_mesh(self, vertices, indices, material=None, *, normals=None, transform=None, name=None,
+                 metadata=None):
+        resource = self.create_mesh(vertices, indices, material, normals=normals, name=name, metadata=metadata)
+        return self.add_instance(resource, transform=transform, name=name, metadata=metadata)
+
+    def _resolve_resource(self, resource):
+        for candidate in self.mesh_resources:
+            if candidate is resource or candidate.id == resource:
+                return candidate
+        raise KeyError("mesh resource is not part of this scene")
+
+    def add_instance(self, resource, *, transform=None, material=None, visible=True, name=None, metadata=None):
+        resource = self._resolve_resource(resource)
+        instance = Instance(resource.vertices, resource.indices,
+                            resource.material if material is None else material,
+                            transform=Transform() if transform is None else transform,
+                            resource=resource, visible=visible, name=name,
+                            metadata={} if metadata is None else metadata)
+        self._attach(instance)
+        self._register_material(instance.material)
+        self.meshes.append(instance)
+        self._changed(geometry=True, shading=True)
+        return instance
+
+    def add_instances(self, resource, transforms, *, materials=None, visible=True, names=None):
+        resource = self._resolve_resource(resource)
+        transforms = [t if isinstance(t, Transform) else Transform(t) for t in transforms]
+        count = len(transforms)
+        if materials is None:
+            materials = [resource.material] * count
+        elif isinstance(materials, Material):
+            materials = [materials] * count
+        else:
+            materials = list(materials)
+            if len(materials) != count:
+                raise ValueError(f"expected {count} materials, got {len(materials)}")
+        names = [names] * count if names is None or isinstance(names, str) else list(names)
+        created = []
+        for transform, material, name in zip(transforms, materials, names):
+            instance = Instance(resource.vertices, resource.indices, material, transform=transform,
+                                resource=resource, visible=visible, name=name)
+            self._attach(instance)
+            self._register_material(material)
+            self.meshes.append(instance)
+            created.append(instance)
+        if created:
+            self._changed(geometry=True, shading=True)
+        return tuple(created)
+
+    def update_instance(self, instance, *, transform=None, material=None, visible=None):
+        if transform is not None:
+            instance.transform = transform if isinstance(transform, Transform) else Transform(transform)
+        if material is not None:
+            instance.material = material
+            self._register_material(material)
+        if visible is not None:
+            instance.visible = bool(visible)
+        self._changed(geometry=visible is not None, shading=material is not None, transform=transform is not None)
+        return instance
+
+    def add_light(self, light):
+        if not isinstance(light, LIGHT_TYPES):
+            raise TypeError("light must be a PointLight, DirectionalLight, or SpotLight")
+        self._attach(light)
+        self.lights.append(light)
+        self._changed(shading=True)
+        return light
+
+    def add_point_light(self, position, color=(1.0, 1.0, 1.0), intensity=1.0, *, range=None):
+        return self.add_light(PointLight(position, color, intensity, range))
+
+    def add_directional_light(self, direction, color=(1.0, 1.0, 1.0), intensity=1.0):
+        return self.add_light(DirectionalLight(direction, color, intensity))
+
+    def set_environment(self, environment=None, **parameters):
+        if environment is not None and parameters:
+            raise TypeError("pass an EnvironmentLight or keyword parameters, not both")
+        if parameters:
+            environment = EnvironmentLight(**parameters)
+        if environment is not None and not isinstance(environment, EnvironmentLight):
+            raise TypeError("environment must be an EnvironmentLight or None")
+        if environment is self.environment:
+            return environment
+        self.environment = environment
+        self._changed(shading=True)
+        return environment
+
+    def add_volume(self, data, material=None, *, transform=None, name=None):
+        volume = Volume(data, material or VolumeMaterial(), Transform() if transform is None else transform,
+                        name=name)
+        self._attach(volume)
+        self.volumes.append(volume)
+        self._changed(geometry=True, shading=True)
+        return volume
+
+    # -- packing helpers (same layouts as the reference) -----------------
+    def triangles(self):
+        """World-space triangle soup, colours and emissions in packed order
+        (Scene.triangles, scene/_core.py:2732-2753)."""
+        tris, colors, emissions = [], [], []
+        for mesh in self.visible_meshes:
+            t = mesh.world_vertices[mesh.indices]
+            tris.append(t)
+            colors.extend([mesh.material.base_color] * len(t))
+            emissions.extend([mesh.material.emission] * len(t))
+        if not tris:
+            return (np.empty((0, 3, 3), np.float32), np.empty((0, 3), np.float32), np.empty((0, 3), np.float32))
+        return (np.concatenate(tris), np.asarray(colors, dtype=np.float32).reshape(-1, 3),
+                np.asarray(emissions, dtype=np.float32).reshape(-1, 3))
+
+    def triangle_instance_ids(self):
+        values = [np.full(len(m.indices), m.id, np.uint32) for m in self.visible_meshes if len(m.indices)]
+        return np.concatenate(values) if values else np.empty(0, np.uint32)
+
+    @property
+    def emissive_light_weight(self):
+        total = 0.0
+        for mesh in self.visible_meshes:
+            lum = float(np.dot(np.asarray(mesh.material.emission, np.float64), _LUMINANCE))
+            if lum <= 0.0:
+                continue
+            t = mesh.world_vertices[mesh.indices]
+            areas = 0.5 * np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1)
+            total += float(areas[areas > 1e-12].sum()) * lum
+        return total
+
+    @property
+    def bounds(self):
+        tris = self.triangles()[0]
+        if not len(tris):
+            return None
+        flat = tris.reshape(-1, 3)
+        return flat.min(axis=0), flat.max(axis=0)

@@ -1,0 +1,94 @@
+"""GPU rendering: the HDR contract, determinism across launch shapes, and
+statistical parity of the reference-compatible mode with the reference's
+CpuReferenceRenderer (golden converged image of the closed-box room)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import reference_path_tracer as ref
+from ordinarylight_b200 import CudaWavefrontRenderer, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def image_error_metrics(reference, candidate):
+    """Relative RMSE as the reference defines it
+    (ordinarylight/validation/_core.py:249-263)."""
+    reference = np.asarray(reference, np.float64)[..., :3]
+    candidate = np.asarray(candidate, np.float64)[..., :3]
+    diff = candidate - reference
+    rmse = float(np.sqrt(np.mean(diff * diff)))
+    scale = float(np.sqrt(np.mean(reference * reference)))
+    return {"rmse": rmse, "relative_rmse": rmse / max(scale, 1e-8), "mae": float(np.mean(np.abs(diff)))}
+
+
+@pytest.fixture(scope="module")
+def compat(native_library, cuda_device):
+    r = CudaWavefrontRenderer(mode="reference_compatible", max_bounces=4, samples_per_pixel=16, seed=1)
+    yield r
+    r.close()
+
+
+def test_hdr_contract_and_repeatability(compat):
+    scene, camera = scenes.box_room()
+    a = compat.render_frame(scene, camera, 64, 48)
+    b = compat.render_frame(scene, camera, 64, 48)
+    assert a.shape == (48, 64, 4) and a.dtype == np.float32
+    assert np.all(np.isfinite(a)) and float(a[..., :3].max()) > 0.0
+    assert np.all(a[..., 3] == 0.0)
+    assert a.tobytes() == b.tobytes()
+    c = compat.render_frame(scene, camera, 64, 48, frame_index=1)
+    assert a.tobytes() != c.tobytes()
+    t = compat.last_timings
+    assert t["camera_rays"] == 64 * 48 * 16 and t["traversal_errors"] == 0 and t["queue_overflow"] == 0
+    assert t["gpu_ms"] > 0 and t["total_ms"] >= t["gpu_ms"] * 0.5
+
+
+def test_invalid_arguments_raise_like_the_reference(compat):
+    scene, camera = scenes.box_room()
+    with pytest.raises(ValueError):
+        compat.render_frame(scene, camera, 0, 4)
+    with pytest.raises(ValueError):
+        compat.render_frame(scene, camera, 4, 4, samples=0)
+    r = CudaWavefrontRenderer(mode="reference_compatible")
+    r.close()
+    r.close()
+    with pytest.raises(RuntimeError):
+        r.render_frame(scene, camera, 4, 4)
+
+
+def test_chunking_and_graphs_do_not_change_a_bit(native_library, cuda_device):
+    scene, camera = scenes.box_room()
+    images = []
+    for chunk, graphs in ((0, True), (0, False), (4096, True), (1000, False)):
+        with CudaWavefrontRenderer(mode="reference_compatible", max_bounces=4, samples_per_pixel=8,
+                                   chunk_paths=chunk, use_graphs=graphs) as r:
+            images.append(r.render_frame(scene, camera, 48, 40, frame_index=2))
+    for other in images[1:]:
+        assert other.tobytes() == images[0].tobytes()
+
+
+def test_production_mode_renders_instanced_scene(native_library, cuda_device):
+    scene, camera = scenes.instanced_spheres(seed=5, instances=8, segments=32, bands=17, emitters=64)
+    with CudaWavefrontRenderer(max_bounces=6, samples_per_pixel=4) as r:
+        img = r.render_frame(scene, camera, 96, 64)
+        again = r.render_frame(scene, camera, 96, 64)
+        t = r.last_timings
+    assert np.all(np.isfinite(img)) and float(img[..., :3].mean()) > 0.0
+    assert img.tobytes() == again.tobytes()
+    assert t["shadow_rays"] > 0 and t["extension_rays"] > 0 and t["traversal_errors"] == 0
+
+
+def test_reference_compatible_matches_oracle_statistically_small(compat):
+    """Small scene, both sides live: image means agree within 3 standard errors."""
+    scene, camera = scenes.box_room()
+    w, h = 32, 24
+    cpu = [ref.render_frame(scene, camera, w, h, samples=16, max_bounces=4, seed=1, frame_index=k)[..., :3]
+           for k in range(8)]
+    gpu = [compat.render_frame(scene, camera, w, h, samples=16, frame_index=k)[..., :3] for k in range(8)]
+    cm = np.array([c.mean(axis=(0, 1)) for c in cpu])
+    gm = np.array([g.mean(axis=(0, 1)) for g in gpu])
+    se = np.sqrt(cm.var(axis=0, ddof=1) / len(cm) + gm.var(axis=0, ddof=1) / len(gm))
+    assert np.all(np.abs(cm.mean(axis=0) - gm.mean(axis=0)) <= 3.0 * se + 1e-6)
