@@ -260,7 +260,7 @@ __global__ void k_bottom_up(int n, const int* __restrict__ left, const int* __re
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int p = leaf_parent[i];
-  while (p >= 0) {
+  for (int guard = 0; p >= 0 && guard < n; ++guard) {
     __threadfence();
     uint32_t old = atomicAdd(&flags[p], 1u);
     if (old == 0u) return;
@@ -547,7 +547,11 @@ __global__ void k_validate(SceneView s, uint32_t num_instances, uint32_t* slot_h
   int stack[128];
   int sp = 0;
   stack[sp++] = (int)s.instances[inst].blas_root;
-  while (sp > 0) {
+  for (uint32_t guard = 0; sp > 0; ++guard) {
+    if (guard > (1u << 26)) {
+      atomicAdd(bad, 1ull);
+      break;
+    }
     int node = stack[--sp];
     if (node >= 0) {
       BvhNode nd = s.nodes[node];

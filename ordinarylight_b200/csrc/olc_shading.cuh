@@ -61,6 +61,24 @@ OLC_D float3 cosine_hemisphere(float3 n, float u, float v) {
   return normalize(t * (r * cp) + b * (r * sp) + n * sqrtf(fmaxf(0.0f, 1.0f - u)));
 }
 
+// The CPU reference's bounce direction: normalize(n + s) with s uniform on
+// the unit sphere and flipped into n's hemisphere
+// (ReferencePathTracer._cosine_hemisphere, path_tracer.py:205-211).  The flip
+// makes this distribution more concentrated around n than a cosine lobe
+// (normalize(n + s) is cosine-distributed only for s on the whole sphere),
+// while the reference still weights the bounce by the albedo alone;
+// reference-compatible mode reproduces the reference's estimator exactly in
+// distribution, so it uses the same construction.
+OLC_D float3 reference_bounce_direction(float3 n, float u, float v) {
+  float z = 1.0f - 2.0f * u;
+  float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  float sp, cp;
+  __sincosf(2.0f * OLC_PI * v, &sp, &cp);
+  float3 s = f3(r * cp, r * sp, z);
+  if (dot(s, n) < 0.0f) s = -s;
+  return normalize(n + s);
+}
+
 OLC_D float ggx_alpha2(float roughness) {
   float a = fmaxf(roughness * roughness, 0.0009f);
   return a * a;

@@ -26,6 +26,7 @@
 
 #define OLC_SPILL 96
 #define OLC_MARKER 0x7fffffff
+#define OLC_TRAVERSAL_BUDGET (1u << 22)
 
 struct TraceRay {
   float3 o, d;
@@ -177,7 +178,14 @@ OLC_D bool olc_traverse(const SceneView& s, float3 wo, float3 wd, float t_min, f
   int level = 0;
   uint32_t cur_inst = 0, cur_prim_offset = 0;
   int node = (int)s.tlas_root;
+  // A well-formed tree is acyclic and finite; the cap only guarantees the
+  // loop ends (and reports an error) should the structure ever be corrupt.
+  uint32_t budget = OLC_TRAVERSAL_BUDGET;
   while (true) {
+    if (--budget == 0u) {
+      err = 1u;
+      break;
+    }
     if (node >= 0 && node != OLC_MARKER) {
       bool h0, h1;
       float n0, n1;

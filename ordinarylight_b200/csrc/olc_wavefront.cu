@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
           if (bounce + 1u < fp.max_bounces) {
             float u1 = olc_rand(rng), u2 = olc_rand(rng);
             next_o = p + nrm * 1e-4f;
-            next_d = cosine_hemisphere(nrm, u1, u2);
+            next_d = reference_bounce_direction(nrm, u1, u2);
             want_next = true;
           }
         } else {

@@ -92,3 +92,35 @@ def test_reference_compatible_matches_oracle_statistically_small(compat):
     gm = np.array([g.mean(axis=(0, 1)) for g in gpu])
     se = np.sqrt(cm.var(axis=0, ddof=1) / len(cm) + gm.var(axis=0, ddof=1) / len(gm))
     assert np.all(np.abs(cm.mean(axis=0) - gm.mean(axis=0)) <= 3.0 * se + 1e-6)
+
+
+def test_converged_parity_with_reference_renderer(compat, golden):
+    """Config-1 room at 256x256, 4 bounces: the GPU's reference-compatible
+    mode against the reference CpuReferenceRenderer's own 1024-spp image.
+
+    * per-image mean radiance (each channel) within 3 standard errors;
+    * relative RMSE (image_error_metrics, validation/_core.py:249-263) of the
+      per-pixel images below 1% once the Monte Carlo noise of both sides is
+      removed (E[rmse^2] = bias^2 + sem_cpu^2 + sem_gpu^2, sems estimated from
+      independent batches); the raw figure must be consistent with that noise.
+    """
+    data = golden("config1_converged.npz")
+    ref_mean = data["mean"].astype(np.float64)
+    ref_sem = data["sem"].astype(np.float64)
+    ref_batches = data["batch_means"]
+    scene, camera = scenes.box_room()
+    batches = np.stack([compat.render_frame(scene, camera, 256, 256, samples=256, frame_index=100 + k)[..., :3]
+                        for k in range(16)]).astype(np.float64)
+    gpu_mean = batches.mean(axis=0)
+    gpu_sem = batches.std(axis=0, ddof=1) / np.sqrt(len(batches))
+    gpu_img = batches.reshape(len(batches), -1, 3).mean(axis=1)
+    se = np.sqrt(ref_batches.var(axis=0, ddof=1) / len(ref_batches) + gpu_img.var(axis=0, ddof=1) / len(gpu_img))
+    diff = np.abs(ref_batches.mean(axis=0) - gpu_img.mean(axis=0))
+    assert np.all(diff <= 3.0 * se), f"image means differ by {diff} (3 SE = {3 * se})"
+    raw = image_error_metrics(ref_mean, gpu_mean)
+    scale = float(np.sqrt(np.mean(ref_mean ** 2)))
+    noise = float(np.sqrt(np.mean(ref_sem ** 2 + gpu_sem ** 2)))
+    bias = float(np.sqrt(max(raw["rmse"] ** 2 - noise ** 2, 0.0)))
+    assert bias / scale < 0.01, f"noise-corrected relative RMSE {bias / scale:.4f} (raw {raw['relative_rmse']:.4f}, " \
+                                f"noise {noise / scale:.4f})"
+    assert raw["relative_rmse"] < 1.25 * noise / scale + 0.01
