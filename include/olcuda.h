@@ -106,7 +106,12 @@ typedef struct olc_config {
   uint32_t stack_depth;         /* shared-memory traversal stack: 16, 24, 32 */
   uint32_t chunk_paths;         /* paths resident per wavefront chunk; 0 = auto */
   uint32_t use_graphs;          /* capture the bounce loop as a CUDA graph */
-  uint32_t reserved[8];
+  uint32_t flatten_instances;   /* bake instances of meshes with <= 64 triangles
+                                   into world-space triangles of the TLAS */
+  uint32_t trace_scheduler;     /* 0: persistent lanes refilled from the queue
+                                   as rays finish; 1: warps take 32 rays at a
+                                   time and run them to completion */
+  uint32_t reserved[6];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the

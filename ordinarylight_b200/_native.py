@@ -43,7 +43,8 @@ class OlcConfig(ctypes.Structure):
         ("restir", c_uint32), ("restir_candidates", c_uint32), ("restir_temporal", c_uint32),
         ("restir_spatial", c_uint32), ("restir_neighbours", c_uint32), ("restir_radius", c_float),
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
-        ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("reserved", c_uint32 * 8),
+        ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
+        ("trace_scheduler", c_uint32), ("reserved", c_uint32 * 6),
     ]
 
 

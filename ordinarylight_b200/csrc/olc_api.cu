@@ -30,8 +30,14 @@ namespace {
 
 thread_local std::string g_thread_error;
 
+// Instances of meshes with at most this many triangles are baked into one
+// world-space mesh at upload, up to kFlattenMaxTotal baked triangles.
+constexpr uint32_t kFlattenMaxTriangles = 64;
+constexpr uint64_t kFlattenMaxTotal = 1ull << 24;
+
 struct ScenePack {
-  DeviceBuffer nodes, tri_verts, tri_normals, tri_index, instances, o2w, materials, material_aux, emitters, lights,
+  DeviceBuffer nodes, tri_verts, tri_normals, tri_index, instances, o2w, materials, material_aux, emitters,
+      emitter_alias, lights,
       env_image, volume;
   SceneView view{};
   uint32_t total_triangles = 0;
@@ -39,6 +45,9 @@ struct ScenePack {
   uint64_t bytes = 0;
   double build_ms = 0.0;
   bool valid = false;
+  DeviceBuffer tri_owner;
+  std::vector<BlasRange> blas_ranges;
+  uint32_t flattened_instances = 0, tlas_instances = 0;
 };
 
 struct TimelineEntry {
@@ -111,6 +120,7 @@ void validate_config(const olc_config& c) {
   if (c.max_bounces < 1 || c.max_bounces > OLC_MAX_BOUNCES)
     throw Error(OLC_ERR_VALUE, "max_bounces must be between 1 and 64");
   if (c.mode > 1) throw Error(OLC_ERR_VALUE, "mode must be 0 (production) or 1 (reference_compatible)");
+  if (c.trace_scheduler > 1) throw Error(OLC_ERR_VALUE, "trace_scheduler must be 0 (refill) or 1 (batch)");
   if (c.restir && (c.restir_candidates < 1 || c.restir_candidates > 64))
     throw Error(OLC_ERR_VALUE, "restir_candidates must be between 1 and 64");
   if (c.restir_spatial > 4) throw Error(OLC_ERR_VALUE, "restir_spatial must be between 0 and 4");
@@ -126,6 +136,7 @@ void validate_config(const olc_config& c) {
 void apply_launch_shape(olc_context* ctx) {
   ctx->ls.block = ctx->cfg.block_size ? ctx->cfg.block_size : 256;
   ctx->ls.stack_depth = ctx->cfg.stack_depth ? ctx->cfg.stack_depth : 24;
+  ctx->ls.scheduler = ctx->cfg.trace_scheduler;
   ctx->ls.grid_simple = ctx->sm_count * 8;
   ctx->ls.grid_shade = ctx->sm_count * 12;
   ctx->ls.grid_trace = ctx->sm_count * 12;
@@ -193,6 +204,55 @@ void upload(DeviceBuffer& buf, const T* host, size_t count, cudaStream_t stream,
   bytes += b;
 }
 
+// Emitter records for sampling from the reference layout (a, b, c, emission +
+// area, cdf/pdf/two-sided; Scene.emissive_triangle_data), plus a Vose alias
+// table over the pdfs (M. D. Vose, "A linear algorithm for generating random
+// numbers with a given distribution", IEEE TSE 1991).
+void build_emitters(const olc_scene_desc* d, std::vector<EmitterRec>& em, std::vector<AliasEntry>& alias) {
+  const uint32_t n = d->num_emitters;
+  em.resize(n);
+  alias.resize(n);
+  if (n == 0) return;
+  if (!d->emitters) throw Error(OLC_ERR_VALUE, "emitter records are required");
+  std::vector<double> p(n);
+  double total = 0.0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* r = d->emitters + 20ull * i;
+    float3 a = make_float3(r[0], r[1], r[2]), b = make_float3(r[4], r[5], r[6]), c = make_float3(r[8], r[9], r[10]);
+    float3 e1 = b - a, e2 = c - a;
+    float3 nrm = normalize(cross(e1, e2));
+    float pdf = r[17];
+    if (!(pdf >= 0.0f) || !std::isfinite(pdf)) throw Error(OLC_ERR_VALUE, "emitter pdf must be finite and >= 0");
+    em[i].a_pdf = make_float4(a.x, a.y, a.z, pdf);
+    em[i].e1_area = make_float4(e1.x, e1.y, e1.z, r[15]);
+    em[i].e2_sided = make_float4(e2.x, e2.y, e2.z, r[18] > 0.5f ? 1.0f : 0.0f);
+    em[i].normal = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+    em[i].emission = make_float4(r[12], r[13], r[14], 0.0f);
+    p[i] = pdf;
+    total += pdf;
+  }
+  if (!(total > 0.0)) throw Error(OLC_ERR_VALUE, "emitter pdfs sum to zero");
+  std::vector<double> scaled(n);
+  std::vector<uint32_t> small, large;
+  for (uint32_t i = 0; i < n; ++i) {
+    scaled[i] = p[i] / total * n;
+    (scaled[i] < 1.0 ? small : large).push_back(i);
+  }
+  while (!small.empty() && !large.empty()) {
+    uint32_t s = small.back(), l = large.back();
+    small.pop_back();
+    alias[s].threshold = (float)scaled[s];
+    alias[s].alias = l;
+    scaled[l] = (scaled[l] + scaled[s]) - 1.0;
+    if (scaled[l] < 1.0) {
+      large.pop_back();
+      small.push_back(l);
+    }
+  }
+  for (uint32_t i : large) alias[i] = AliasEntry{1.0f, i};
+  for (uint32_t i : small) alias[i] = AliasEntry{1.0f, i};
+}
+
 void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
   auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = ctx->stream;
@@ -221,59 +281,169 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
   upload(dn, d->normals, 3ull * total_v, st, bytes);
   upload(di, d->indices, 3ull * total_t, st, bytes);
   bytes = 0;
-  // node pool: BLAS nodes then TLAS nodes
-  std::vector<uint32_t> node_base(nm), blas_root(nm);
+  // ---- instance flattening: instances of meshes with at most
+  // kFlattenMaxTriangles triangles are baked into one world-space mesh.
+  auto mesh_tris = [&](uint32_t m) { return d->mesh_triangle_offset[m + 1] - d->mesh_triangle_offset[m]; };
+  std::vector<uint8_t> flat(ni, 0);
+  uint64_t flat_tris = 0;
+  uint32_t flat_count = 0;
+  for (uint32_t i = 0; i < ni; ++i) {
+    uint32_t nt = mesh_tris(d->instance_mesh[i]);
+    if (nt > 0 && nt <= kFlattenMaxTriangles) {
+      flat[i] = 1;
+      flat_tris += nt;
+      ++flat_count;
+    }
+  }
+  if (!ctx->cfg.flatten_instances || flat_count < 2 || flat_tris > kFlattenMaxTotal) {
+    std::fill(flat.begin(), flat.end(), 0);
+    flat_tris = 0;
+    flat_count = 0;
+  }
+  const bool flattening = flat_count > 0;
+  // internal instance order: TLAS members (instances kept as instances, then
+  // the flattened mesh's identity instance), then the flattened originals.
+  std::vector<uint32_t> order;
+  for (uint32_t i = 0; i < ni; ++i)
+    if (!flat[i]) order.push_back(i);
+  const uint32_t pseudo = (uint32_t)order.size();
+  const uint32_t tlas_members = pseudo + (flattening ? 1u : 0u);
+  std::vector<uint32_t> internal_of(ni);
+  for (uint32_t k = 0; k < pseudo; ++k) internal_of[order[k]] = k;
+  {
+    uint32_t k = tlas_members;
+    for (uint32_t i = 0; i < ni; ++i)
+      if (flat[i]) internal_of[i] = k++;
+  }
+  const uint32_t n_records = tlas_members + flat_count;
+  // meshes that still need their own BLAS
+  std::vector<uint8_t> mesh_used(nm, 0);
+  for (uint32_t k = 0; k < pseudo; ++k) mesh_used[d->instance_mesh[order[k]]] = 1;
+  // node pool: BLAS nodes, the flattened mesh, then TLAS nodes
+  std::vector<uint32_t> node_base(nm), blas_root(nm, 0);
   uint32_t nodes_total = 0;
   for (uint32_t m = 0; m < nm; ++m) {
     node_base[m] = nodes_total;
-    nodes_total += blas_node_count(d->mesh_triangle_offset[m + 1] - d->mesh_triangle_offset[m]);
+    if (mesh_used[m]) nodes_total += blas_node_count(mesh_tris(m));
   }
   uint32_t tlas_base = nodes_total;
-  uint32_t tlas_nodes = ni > 1 ? ni - 1 : 1;
+  const uint64_t tlas_prims = (uint64_t)pseudo + flat_tris;  // instances + direct triangles
+  uint32_t tlas_nodes = tlas_prims > 1 ? (uint32_t)(tlas_prims - 1) : 1;
   nodes_total += tlas_nodes;
+  const uint64_t total_slots = (uint64_t)total_t + flat_tris;
+  if (total_slots >= (1ull << 28)) throw Error(OLC_ERR_VALUE, "scene exceeds 2^28 triangles");
   sp.nodes.allocate((size_t)nodes_total * sizeof(BvhNode));
-  sp.tri_verts.allocate(std::max<size_t>(total_t, 1) * 3 * sizeof(float4));
-  sp.tri_normals.allocate(std::max<size_t>(total_t, 1) * 3 * sizeof(float4));
-  sp.tri_index.allocate(std::max<size_t>(total_t, 1) * sizeof(uint32_t));
-  bytes += sp.nodes.bytes() + sp.tri_verts.bytes() + sp.tri_normals.bytes() + sp.tri_index.bytes();
+  sp.tri_verts.allocate(std::max<size_t>(total_slots, 1) * 3 * sizeof(float4));
+  sp.tri_normals.allocate(std::max<size_t>(total_slots, 1) * 3 * sizeof(float4));
+  sp.tri_index.allocate(std::max<size_t>(total_slots, 1) * sizeof(uint32_t));
+  sp.tri_owner.allocate(std::max<size_t>(total_slots, 1) * sizeof(uint32_t));
+  OLC_CUDA(cudaMemsetAsync(sp.tri_owner.get(), 0, sp.tri_owner.bytes(), st));
+  bytes += sp.nodes.bytes() + sp.tri_verts.bytes() + sp.tri_normals.bytes() + sp.tri_index.bytes() +
+           sp.tri_owner.bytes();
+  sp.blas_ranges.clear();
   for (uint32_t m = 0; m < nm; ++m) {
+    if (!mesh_used[m]) continue;
     BlasDesc bd;
     uint32_t v0 = d->mesh_vertex_offset[m], t0i = d->mesh_triangle_offset[m];
     bd.vertices = dv.as<float>() + 3ull * v0;
     bd.normals = dn.as<float>() + 3ull * v0;
     bd.indices = di.as<uint32_t>() + 3ull * t0i;
     bd.num_vertices = d->mesh_vertex_offset[m + 1] - v0;
-    bd.num_triangles = d->mesh_triangle_offset[m + 1] - t0i;
+    bd.num_triangles = mesh_tris(m);
     blas_root[m] = build_blas(bd, ctx->scratch, sp.nodes.as<BvhNode>(), node_base[m], sp.tri_verts.as<float4>(),
                               sp.tri_normals.as<float4>(), sp.tri_index.as<uint32_t>(), t0i, 4, st);
+    sp.blas_ranges.push_back({blas_root[m], t0i, t0i + bd.num_triangles});
   }
-  // instances
-  std::vector<InstanceRec> inst(ni);
-  std::vector<float> o2w(12ull * std::max<uint32_t>(ni, 1));
-  for (uint32_t i = 0; i < ni; ++i) {
-    const float* m = d->instance_object_to_world + 12ull * i;
-    for (int k = 0; k < 12; ++k) {
-      if (!std::isfinite(m[k])) throw Error(OLC_ERR_VALUE, "instance transform must be finite");
-      o2w[12ull * i + k] = m[k];
-    }
+  // instance records (internal order)
+  std::vector<InstanceRec> inst(n_records);
+  std::vector<float> o2w(12ull * std::max<uint32_t>(tlas_members, 1), 0.0f);
+  auto fill_record = [&](InstanceRec& r, const float* m) {
     float w2o[12];
     invert_affine(m, w2o);
-    InstanceRec& r = inst[i];
     r.w2o0 = make_float4(w2o[0], w2o[1], w2o[2], w2o[3]);
     r.w2o1 = make_float4(w2o[4], w2o[5], w2o[6], w2o[7]);
     r.w2o2 = make_float4(w2o[8], w2o[9], w2o[10], w2o[11]);
     r.o2w0 = make_float4(m[0], m[1], m[2], m[3]);
     r.o2w1 = make_float4(m[4], m[5], m[6], m[7]);
     r.o2w2 = make_float4(m[8], m[9], m[10], m[11]);
+    r.flags = 0;
+    r.pad[0] = r.pad[1] = r.pad[2] = 0;
+  };
+  for (uint32_t i = 0; i < ni; ++i) {
+    const float* m = d->instance_object_to_world + 12ull * i;
+    for (int k = 0; k < 12; ++k)
+      if (!std::isfinite(m[k])) throw Error(OLC_ERR_VALUE, "instance transform must be finite");
+    const uint32_t k = internal_of[i];
+    InstanceRec& r = inst[k];
+    fill_record(r, m);
     r.blas_root = blas_root[d->instance_mesh[i]];
     r.material = d->instance_material[i];
     r.prim_offset = d->instance_primitive_offset[i];
     r.instance_id = d->instance_id[i];
+    if (k < tlas_members)
+      for (int c = 0; c < 12; ++c) o2w[12ull * k + c] = m[c];
   }
-  upload(sp.instances, inst.data(), ni, st, bytes);
-  upload(sp.o2w, o2w.data(), 12ull * ni, st, bytes);
-  uint32_t tlas_root = build_tlas(sp.instances.as<InstanceRec>(), sp.o2w.as<float>(), ni, sp.nodes.as<BvhNode>(),
-                                  ctx->scratch, sp.nodes.as<BvhNode>(), tlas_base, st);
+  if (flattening) {
+    // world-space triangles of the flattened instances, in packed order,
+    // written straight into their slots; the TLAS references them directly
+    std::vector<float4> fv(3ull * flat_tris), fn(3ull * flat_tris);
+    std::vector<uint32_t> fpacked(flat_tris), fowner(flat_tris);
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < ni; ++i) {
+      if (!flat[i]) continue;
+      const InstanceRec& r = inst[internal_of[i]];
+      Affine mo{r.o2w0, r.o2w1, r.o2w2}, mw{r.w2o0, r.w2o1, r.w2o2};
+      const uint32_t m = d->instance_mesh[i];
+      const uint32_t v0 = d->mesh_vertex_offset[m];
+      for (uint32_t lt = 0; lt < mesh_tris(m); ++lt, ++t) {
+        for (int c = 0; c < 3; ++c) {
+          uint32_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
+          float3 p = xform_point(mo, make_float3(d->vertices[3ull * vi], d->vertices[3ull * vi + 1],
+                                                 d->vertices[3ull * vi + 2]));
+          float3 nn = normalize(xform_normal_by_inverse(
+              mw, make_float3(d->normals[3ull * vi], d->normals[3ull * vi + 1], d->normals[3ull * vi + 2])));
+          fv[3 * t + c] = make_float4(p.x, p.y, p.z, 0.0f);
+          fn[3 * t + c] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+        }
+        fpacked[t] = r.prim_offset + lt;
+        fowner[t] = internal_of[i];
+      }
+    }
+    OLC_CUDA(cudaMemcpyAsync(sp.tri_verts.as<float4>() + 3ull * total_t, fv.data(), fv.size() * sizeof(float4),
+                             cudaMemcpyHostToDevice, st));
+    OLC_CUDA(cudaMemcpyAsync(sp.tri_normals.as<float4>() + 3ull * total_t, fn.data(), fn.size() * sizeof(float4),
+                             cudaMemcpyHostToDevice, st));
+    OLC_CUDA(cudaMemcpyAsync(sp.tri_index.as<uint32_t>() + total_t, fpacked.data(), fpacked.size() * 4,
+                             cudaMemcpyHostToDevice, st));
+    OLC_CUDA(cudaMemcpyAsync(sp.tri_owner.as<uint32_t>() + total_t, fowner.data(), fowner.size() * 4,
+                             cudaMemcpyHostToDevice, st));
+    OLC_CUDA(cudaStreamSynchronize(st));  // the host staging vectors go out of scope
+    // identity record that hits on direct triangles report as their instance
+    const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    InstanceRec& r = inst[pseudo];
+    fill_record(r, identity);
+    r.blas_root = 0;
+    r.material = 0;
+    r.prim_offset = 0;
+    r.instance_id = 0xffffffffu;
+    r.flags = OLC_INSTANCE_FLATTENED;
+  }
+  upload(sp.instances, inst.data(), n_records, st, bytes);
+  upload(sp.o2w, o2w.data(), 12ull * std::max<uint32_t>(pseudo, 1), st, bytes);
+  std::vector<uint2> ranges(std::max<uint32_t>(pseudo, 1));
+  for (uint32_t k = 0; k < pseudo; ++k) {
+    const uint32_t m = d->instance_mesh[order[k]];
+    ranges[k] = make_uint2(d->mesh_triangle_offset[m], d->mesh_triangle_offset[m + 1]);
+  }
+  DeviceBuffer dranges;
+  uint64_t scratch_bytes = 0;
+  upload(dranges, ranges.data(), pseudo, st, scratch_bytes);
+  uint32_t tlas_root = build_tlas(sp.o2w.as<float>(), dranges.as<uint2>(), pseudo, sp.tri_verts.as<float4>(),
+                                  sp.tri_verts.as<float4>() + 3ull * total_t, (uint32_t)flat_tris, ctx->scratch,
+                                  sp.nodes.as<BvhNode>(), tlas_base, st);
+  OLC_CUDA(cudaStreamSynchronize(st));  // dranges goes out of scope
+  sp.flattened_instances = flat_count;
+  sp.tlas_instances = tlas_members;
   // materials
   std::vector<MaterialRec> mats(d->num_materials);
   std::vector<MaterialAux> aux(d->num_materials);
@@ -289,7 +459,13 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
   }
   upload(sp.materials, mats.data(), mats.size(), st, bytes);
   upload(sp.material_aux, aux.data(), aux.size(), st, bytes);
-  upload(sp.emitters, reinterpret_cast<const EmitterRec*>(d->emitters), d->num_emitters, st, bytes);
+  {
+    std::vector<EmitterRec> em;
+    std::vector<AliasEntry> alias;
+    build_emitters(d, em, alias);
+    upload(sp.emitters, em.data(), em.size(), st, bytes);
+    upload(sp.emitter_alias, alias.data(), alias.size(), st, bytes);
+  }
   upload(sp.lights, reinterpret_cast<const LightRec*>(d->lights), d->num_lights, st, bytes);
   size_t env_count = d->environment_kind == OLC_ENV_EQUIRECT ? 3ull * d->environment_width * d->environment_height : 0;
   if (d->environment_kind == OLC_ENV_EQUIRECT && (!d->environment_image || env_count == 0))
@@ -303,15 +479,20 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
   v.tri_verts = sp.tri_verts.as<float4>();
   v.tri_normals = sp.tri_normals.as<float4>();
   v.tri_index = sp.tri_index.as<uint32_t>();
+  v.tri_owner = sp.tri_owner.as<uint32_t>();
   v.instances = sp.instances.as<InstanceRec>();
   v.materials = sp.materials.as<MaterialRec>();
   v.material_aux = sp.material_aux.as<MaterialAux>();
   v.emitters = sp.emitters.as<EmitterRec>();
+  v.emitter_alias = sp.emitter_alias.as<AliasEntry>();
   v.lights = sp.lights.as<LightRec>();
   v.env_image = sp.env_image.as<float>();
   v.volume = sp.volume.as<float>();
   v.tlas_root = tlas_root;
-  v.num_instances = ni;
+  v.num_instances = tlas_members;
+  v.tlas_instances = pseudo;
+  v.flat_slot_base = total_t;
+  v.flat_instance = pseudo;
   v.num_emitters = d->num_emitters;
   v.num_lights = d->num_lights;
   v.emissive_weight = d->emissive_weight;
@@ -827,8 +1008,7 @@ int olc_bvh_validate(olc_context* ctx, uint64_t* bad) {
   if (!ctx || !bad) return fail(ctx, OLC_ERR_VALUE, "context and output are required");
   return guarded(ctx, [&] {
     if (!ctx->scene.valid) throw Error(OLC_ERR_RUNTIME, "no scene is resident");
-    *bad = validate_bvh(ctx->scene.view, ctx->scene.total_triangles, ctx->scene.view.num_instances, nullptr,
-                        nullptr, ctx->stream);
+    *bad = validate_bvh(ctx->scene.view, ctx->scene.blas_ranges, ctx->stream);
   });
 }
 

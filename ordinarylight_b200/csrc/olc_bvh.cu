@@ -349,27 +349,60 @@ __global__ void k_reorder_triangles(const uint32_t* __restrict__ order, uint32_t
   tri_index[dst] = t;
 }
 
-__global__ void k_instance_boxes(const InstanceRec* __restrict__ inst, const float* __restrict__ o2w, uint32_t n,
-                                 const BvhNode* __restrict__ nodes, float4* lo, float4* hi, float4* centers) {
+// Boxes of world-space triangles that the TLAS references directly.
+__global__ void k_flat_triangle_boxes(const float4* __restrict__ verts, uint32_t n, float4* lo, float4* hi,
+                                      float4* centers) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  BvhNode r = nodes[inst[i].blas_root];
-  float3 blo = f3(fminf(r.a.x, r.b.x), fminf(r.a.z, r.b.z), fminf(r.c.x, r.c.z));
-  float3 bhi = f3(fmaxf(r.a.y, r.b.y), fmaxf(r.a.w, r.b.w), fmaxf(r.c.y, r.c.w));
+  float3 a = f3(verts[3ull * i]), b = f3(verts[3ull * i + 1]), c = f3(verts[3ull * i + 2]);
+  float3 l = fminf3(fminf3(a, b), c), h = fmaxf3(fmaxf3(a, b), c);
+  lo[i] = make_float4(l.x, l.y, l.z, 0.0f);
+  hi[i] = make_float4(h.x, h.y, h.z, 0.0f);
+  centers[i] = make_float4(__fmul_rn(__fadd_rn(l.x, h.x), 0.5f), __fmul_rn(__fadd_rn(l.y, h.y), 0.5f),
+                           __fmul_rn(__fadd_rn(l.z, h.z), 0.5f), 0.0f);
+}
+
+// Tight world box of each instance: the bounds of its BLAS's vertices after
+// the object-to-world transform (a rotated object-space box can be up to
+// sqrt(3) wider per axis than the object it holds).  One block per instance.
+__global__ void __launch_bounds__(256) k_instance_boxes(const float* __restrict__ o2w, uint32_t n,
+                                                        const uint2* __restrict__ slot_ranges,
+                                                        const float4* __restrict__ tri_verts, float4* lo, float4* hi,
+                                                        float4* centers) {
+  __shared__ float red[6][256];
+  const uint32_t i = blockIdx.x;
+  if (i >= n) return;
   Affine m;
   const float* p = o2w + 12ull * i;
   m.r0 = make_float4(p[0], p[1], p[2], p[3]);
   m.r1 = make_float4(p[4], p[5], p[6], p[7]);
   m.r2 = make_float4(p[8], p[9], p[10], p[11]);
+  const uint2 range = slot_ranges[i];
   float3 wl = f3(CUDART_INF_F, CUDART_INF_F, CUDART_INF_F), wh = -wl;
-  for (int c = 0; c < 8; ++c) {
-    float3 q = f3((c & 1) ? bhi.x : blo.x, (c & 2) ? bhi.y : blo.y, (c & 4) ? bhi.z : blo.z);
-    float3 w = xform_point(m, q);
+  for (uint64_t v = 3ull * range.x + threadIdx.x; v < 3ull * range.y; v += blockDim.x) {
+    float3 w = xform_point(m, f3(tri_verts[v]));
     wl = fminf3(wl, w);
     wh = fmaxf3(wh, w);
   }
-  // Pad by a relative epsilon: the transformed ray of the traversal is not
-  // bit-identical to the forward transform of the corners.
+  red[0][threadIdx.x] = wl.x;
+  red[1][threadIdx.x] = wl.y;
+  red[2][threadIdx.x] = wl.z;
+  red[3][threadIdx.x] = wh.x;
+  red[4][threadIdx.x] = wh.y;
+  red[5][threadIdx.x] = wh.z;
+  __syncthreads();
+  for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = fminf(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+      for (int k = 3; k < 6; ++k) red[k][threadIdx.x] = fmaxf(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  wl = f3(red[0][0], red[1][0], red[2][0]);
+  wh = f3(red[3][0], red[4][0], red[5][0]);
+  // Pad by a relative epsilon: the traversal transforms the ray, not the
+  // vertices, so its hit points are not bit-identical to these.
   float mag = fmaxf(fmaxf(max3(fmaxf3(wh, -wl)), max3(wh - wl)), 1e-3f);
   float3 pad = f3(mag, mag, mag) * 1e-5f;
   wl = wl - pad;
@@ -524,104 +557,96 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
   return root;
 }
 
-uint32_t build_tlas(const InstanceRec* instances, const float* o2w, uint32_t n, const BvhNode* nodes_in,
-                    BuildScratch& sc, BvhNode* nodes, uint32_t node_base, cudaStream_t stream) {
-  sc.ensure(std::max<uint32_t>(n, 1u));
+uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, const float4* tri_verts,
+                    const float4* flat_verts, uint32_t n_flat, BuildScratch& sc, BvhNode* nodes, uint32_t node_base,
+                    cudaStream_t stream) {
+  const uint32_t total = n + n_flat;
+  sc.ensure(std::max<uint32_t>(total, 1u));
   if (n > 0) {
-    k_instance_boxes<<<blocks_for(n), kThreads, 0, stream>>>(instances, o2w, n, nodes_in, sc.boxes_lo.as<float4>(),
-                                                               sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
+    k_instance_boxes<<<n, 256, 0, stream>>>(o2w, n, slot_ranges, tri_verts, sc.boxes_lo.as<float4>(),
+                                            sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
     OLC_LAUNCH_CHECK("k_instance_boxes");
   }
-  return build_hierarchy(n, sc, 1, 1, nodes, node_base, 0, stream);
+  if (n_flat > 0) {
+    k_flat_triangle_boxes<<<blocks_for(n_flat), kThreads, 0, stream>>>(
+        flat_verts, n_flat, sc.boxes_lo.as<float4>() + n, sc.boxes_hi.as<float4>() + n, sc.centers.as<float4>() + n);
+    OLC_LAUNCH_CHECK("k_flat_triangle_boxes");
+  }
+  return build_hierarchy(total, sc, 1, 1, nodes, node_base, 0, stream);
 }
 
 // ---- validation ----------------------------------------------------------
 namespace {
-// Walk every BLAS subtree from each instance root; count how often each slot
-// is reached and whether child boxes nest (within float slack).
-__global__ void k_validate(SceneView s, uint32_t num_instances, uint32_t* slot_hits, unsigned long long* bad,
-                           const uint8_t* seen_blas_first) {
-  uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
-  if (inst >= num_instances) return;
-  if (!seen_blas_first[inst]) return;  // one walker per distinct BLAS
+// Walk each built BLAS from its root; count how often each slot is reached,
+// leaves outside the BLAS's own slot range, and child boxes that do not lie
+// inside the box stored for them in the parent.
+__global__ void k_validate(SceneView s, const BlasRange* ranges, uint32_t count, uint32_t* slot_hits,
+                           unsigned long long* bad) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= count) return;
+  const BlasRange r = ranges[b];
   int stack[128];
   int sp = 0;
-  stack[sp++] = (int)s.instances[inst].blas_root;
+  stack[sp++] = (int)r.root;
   for (uint32_t guard = 0; sp > 0; ++guard) {
     if (guard > (1u << 26)) {
       atomicAdd(bad, 1ull);
       break;
     }
     int node = stack[--sp];
-    if (node >= 0) {
-      BvhNode nd = s.nodes[node];
-      int ch[2] = {nd.d.x, nd.d.y};
-      for (int c = 0; c < 2; ++c) {
-        if (ch[c] == OLC_EMPTY_CHILD) continue;
-        if (ch[c] >= 0) {
-          BvhNode cn = s.nodes[ch[c]];
-          // child's own children boxes must lie inside the box stored for it
-          float lx = c == 0 ? nd.a.x : nd.b.x, hx = c == 0 ? nd.a.y : nd.b.y;
-          float ly = c == 0 ? nd.a.z : nd.b.z, hy = c == 0 ? nd.a.w : nd.b.w;
-          float lz = c == 0 ? nd.c.x : nd.c.z, hz = c == 0 ? nd.c.y : nd.c.w;
-          for (int g = 0; g < 2; ++g) {
-            int gc = g == 0 ? cn.d.x : cn.d.y;
-            if (gc == OLC_EMPTY_CHILD) continue;
-            float glx = g == 0 ? cn.a.x : cn.b.x, ghx = g == 0 ? cn.a.y : cn.b.y;
-            float gly = g == 0 ? cn.a.z : cn.b.z, ghy = g == 0 ? cn.a.w : cn.b.w;
-            float glz = g == 0 ? cn.c.x : cn.c.z, ghz = g == 0 ? cn.c.y : cn.c.w;
-            if (glx < lx || gly < ly || glz < lz || ghx > hx || ghy > hy || ghz > hz) atomicAdd(bad, 1ull);
-          }
-          if (sp < 128) stack[sp++] = ch[c]; else atomicAdd(bad, 1ull);
-        } else {
-          uint32_t f = olc_leaf_first(ch[c]), cnt = olc_leaf_count(ch[c]);
-          for (uint32_t k = 0; k < cnt; ++k) atomicAdd(&slot_hits[f + k], 1u);
+    if (node < 0) continue;
+    BvhNode nd = s.nodes[node];
+    int ch[2] = {nd.d.x, nd.d.y};
+    for (int c = 0; c < 2; ++c) {
+      if (ch[c] == OLC_EMPTY_CHILD) continue;
+      if (ch[c] >= 0) {
+        BvhNode cn = s.nodes[ch[c]];
+        float lx = c == 0 ? nd.a.x : nd.b.x, hx = c == 0 ? nd.a.y : nd.b.y;
+        float ly = c == 0 ? nd.a.z : nd.b.z, hy = c == 0 ? nd.a.w : nd.b.w;
+        float lz = c == 0 ? nd.c.x : nd.c.z, hz = c == 0 ? nd.c.y : nd.c.w;
+        for (int g = 0; g < 2; ++g) {
+          int gc = g == 0 ? cn.d.x : cn.d.y;
+          if (gc == OLC_EMPTY_CHILD) continue;
+          float glx = g == 0 ? cn.a.x : cn.b.x, ghx = g == 0 ? cn.a.y : cn.b.y;
+          float gly = g == 0 ? cn.a.z : cn.b.z, ghy = g == 0 ? cn.a.w : cn.b.w;
+          float glz = g == 0 ? cn.c.x : cn.c.z, ghz = g == 0 ? cn.c.y : cn.c.w;
+          if (glx < lx || gly < ly || glz < lz || ghx > hx || ghy > hy || ghz > hz) atomicAdd(bad, 1ull);
+        }
+        if (sp < 128) stack[sp++] = ch[c]; else atomicAdd(bad, 1ull);
+      } else {
+        uint32_t f = olc_leaf_first(ch[c]), cnt = olc_leaf_count(ch[c]);
+        for (uint32_t k = 0; k < cnt; ++k) {
+          if (f + k < r.slot_begin || f + k >= r.slot_end) atomicAdd(bad, 1ull);
+          else atomicAdd(&slot_hits[f + k], 1u);
         }
       }
     }
   }
 }
-__global__ void k_count_bad_slots(const uint32_t* slot_hits, uint32_t n, unsigned long long* bad) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && slot_hits[i] != 1u) atomicAdd(bad, 1ull);
-}
 }  // namespace
 
-uint64_t validate_bvh(const SceneView& s, uint32_t total_slots, uint32_t num_instances,
-                      const uint32_t* /*blas_slot_begin*/, const uint32_t* /*blas_slot_end*/, cudaStream_t stream) {
-  // mark the first instance of every distinct BLAS root on the host
-  std::vector<InstanceRec> inst(num_instances);
-  if (num_instances)
-    OLC_CUDA(cudaMemcpyAsync(inst.data(), s.instances, sizeof(InstanceRec) * num_instances, cudaMemcpyDeviceToHost,
-                             stream));
-  OLC_CUDA(cudaStreamSynchronize(stream));
-  std::vector<uint8_t> first(num_instances, 0);
-  std::vector<uint32_t> roots;
-  for (uint32_t i = 0; i < num_instances; ++i) {
-    if (std::find(roots.begin(), roots.end(), inst[i].blas_root) == roots.end()) {
-      roots.push_back(inst[i].blas_root);
-      first[i] = 1;
-    }
-  }
-  DeviceBuffer hits(std::max<size_t>(total_slots, 1) * 4), bad(8), seen(std::max<size_t>(num_instances, 1));
-  OLC_CUDA(cudaMemsetAsync(hits.get(), 0, std::max<size_t>(total_slots, 1) * 4, stream));
+uint64_t validate_bvh(const SceneView& s, const std::vector<BlasRange>& blas, cudaStream_t stream) {
+  uint32_t slots = 0;
+  for (const BlasRange& r : blas) slots = std::max(slots, r.slot_end);
+  DeviceBuffer hits(std::max<size_t>(slots, 1) * 4), bad(8), ranges(std::max<size_t>(blas.size(), 1) * sizeof(BlasRange));
+  OLC_CUDA(cudaMemsetAsync(hits.get(), 0, std::max<size_t>(slots, 1) * 4, stream));
   OLC_CUDA(cudaMemsetAsync(bad.get(), 0, 8, stream));
-  if (num_instances)
-    OLC_CUDA(cudaMemcpyAsync(seen.get(), first.data(), num_instances, cudaMemcpyHostToDevice, stream));
-  if (num_instances) {
-    k_validate<<<blocks_for(num_instances, 64), 64, 0, stream>>>(s, num_instances, hits.as<uint32_t>(),
-                                                                 bad.as<unsigned long long>(), seen.as<uint8_t>());
+  if (!blas.empty()) {
+    OLC_CUDA(cudaMemcpyAsync(ranges.get(), blas.data(), blas.size() * sizeof(BlasRange), cudaMemcpyHostToDevice,
+                             stream));
+    k_validate<<<blocks_for(blas.size(), 64), 64, 0, stream>>>(s, ranges.as<BlasRange>(), (uint32_t)blas.size(),
+                                                               hits.as<uint32_t>(), bad.as<unsigned long long>());
     OLC_LAUNCH_CHECK("k_validate");
   }
-  if (total_slots) {
-    k_count_bad_slots<<<blocks_for(total_slots), kThreads, 0, stream>>>(hits.as<uint32_t>(), total_slots,
-                                                                          bad.as<unsigned long long>());
-    OLC_LAUNCH_CHECK("k_count_bad_slots");
-  }
-  unsigned long long h = 0;
-  OLC_CUDA(cudaMemcpyAsync(&h, bad.get(), 8, cudaMemcpyDeviceToHost, stream));
+  std::vector<uint32_t> h(std::max<size_t>(slots, 1));
+  unsigned long long nbad = 0;
+  OLC_CUDA(cudaMemcpyAsync(h.data(), hits.get(), h.size() * 4, cudaMemcpyDeviceToHost, stream));
+  OLC_CUDA(cudaMemcpyAsync(&nbad, bad.get(), 8, cudaMemcpyDeviceToHost, stream));
   OLC_CUDA(cudaStreamSynchronize(stream));
-  return h;
+  for (const BlasRange& r : blas)
+    for (uint32_t i = r.slot_begin; i < r.slot_end; ++i)
+      if (h[i] != 1u) ++nbad;
+  return nbad;
 }
 
 }  // namespace olc

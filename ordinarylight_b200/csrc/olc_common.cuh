@@ -141,8 +141,17 @@ OLC_HD uint32_t olc_leaf_first(int ref) { return ((uint32_t)(~ref)) >> 3; }
 OLC_HD uint32_t olc_leaf_count(int ref) { return (((uint32_t)(~ref)) & 7u) + 1u; }
 #define OLC_EMPTY_CHILD ((int)0x80000000)
 
-// Instance record, 112 bytes: world->object 3x4 and identity/offsets (the
-// 64 bytes traversal reads), then object->world 3x4 for shading.
+// Instance record, 128 bytes: world->object 3x4 and identity/offsets (the
+// 64 bytes traversal reads), then object->world 3x4 for shading, then flags.
+//
+// Instances of very small meshes (the 1,024 one-triangle emitters of the
+// instanced benchmark scene, the walls of the box room) are baked at upload
+// into world-space triangles that the TLAS references directly, so a ray
+// reaching such an object needs no transform and no second hierarchy.  Hits
+// on them report one identity record flagged OLC_INSTANCE_FLATTENED; for
+// their slots tri_index holds the packed triangle index itself and tri_owner
+// the record of the original instance (material, Mesh.id).
+#define OLC_INSTANCE_FLATTENED 1u
 struct __align__(16) InstanceRec {
   float4 w2o0, w2o1, w2o2;
   uint32_t blas_root;      // node index of the instance's BLAS root
@@ -150,6 +159,8 @@ struct __align__(16) InstanceRec {
   uint32_t prim_offset;    // packed triangle base (Scene.triangles order)
   uint32_t instance_id;    // Mesh.id
   float4 o2w0, o2w1, o2w2;
+  uint32_t flags;          // OLC_INSTANCE_FLATTENED
+  uint32_t pad[3];
 };
 
 // Material record, 32 bytes.
@@ -163,11 +174,25 @@ struct __align__(16) MaterialAux {
   uint32_t pad0, pad1;
 };
 
-// Emitter record (area light), 80 bytes like Scene.emissive_triangle_data.
+// Emitter record (area light), 80 bytes: the reference's emissive-triangle
+// records (Scene.emissive_triangle_data, scene/_core.py:2637-2691:
+// vertices, emission, area, power pdf, two-sided flag) re-expressed at upload
+// for sampling — vertex a, both edges and the unit normal precomputed, so a
+// candidate costs no cross product or normalisation.
 struct __align__(16) EmitterRec {
-  float4 a, b, c;
-  float4 emission_area;    // emission.rgb, area
-  float4 dist;             // cdf, pdf, two_sided, 0
+  float4 a_pdf;            // a.xyz, selection probability
+  float4 e1_area;          // b - a, area
+  float4 e2_sided;         // c - a, two-sided flag (0/1)
+  float4 normal;           // unit normal of cross(e1, e2), 0
+  float4 emission;         // rgb, 0
+};
+
+// Walker/Vose alias table entry over the emitter power distribution: O(1)
+// selection with the same probabilities as the reference's CDF binary
+// search (transport_v1/lighting.glsl:356-377).
+struct __align__(8) AliasEntry {
+  float threshold;
+  uint32_t alias;
 };
 
 struct __align__(16) LightRec {
@@ -177,19 +202,31 @@ struct __align__(16) LightRec {
   float4 spot;
 };
 
+struct SceneView;
+// The instance that owns a hit's material and identity: the hit instance
+// itself, or for the flattened mesh the original instance of the triangle.
+OLC_D uint32_t owner_instance(const InstanceRec* instances, const uint32_t* tri_owner, uint32_t inst, uint32_t slot) {
+  return (instances[inst].flags & OLC_INSTANCE_FLATTENED) ? tri_owner[slot] : inst;
+}
+
 struct SceneView {
   const BvhNode* nodes;          // BLAS and TLAS nodes, one pool
   const float4* tri_verts;       // 3 float4 per triangle slot (object space)
   const float4* tri_normals;     // 3 float4 per triangle slot (object space)
-  const uint32_t* tri_index;     // slot -> mesh-local triangle index
+  const uint32_t* tri_index;     // slot -> mesh-local triangle index (packed index in the flattened mesh)
+  const uint32_t* tri_owner;     // slot -> original instance (flattened mesh only)
   const InstanceRec* instances;
   const MaterialRec* materials;
   const MaterialAux* material_aux;
   const EmitterRec* emitters;
+  const AliasEntry* emitter_alias;
   const LightRec* lights;
   const float* env_image;        // equirect RGB
   const float* volume;           // density grid
   uint32_t tlas_root;
+  uint32_t tlas_instances;       // TLAS leaf payloads below this are instances
+  uint32_t flat_slot_base;       // ... the rest are world-space triangle slots from here
+  uint32_t flat_instance;        // identity record reported for direct triangles
   uint32_t num_instances;
   uint32_t num_emitters;
   uint32_t num_lights;

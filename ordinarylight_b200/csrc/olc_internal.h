@@ -105,14 +105,22 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& scratch, BvhNode* nodes, ui
                     uint32_t leaf_max, cudaStream_t stream);
 inline uint32_t blas_node_count(uint32_t nt) { return nt > 1 ? nt - 1 : 1; }
 
-// Build the TLAS over instances (world boxes computed from BLAS roots).
-uint32_t build_tlas(const InstanceRec* instances, const float* object_to_world, uint32_t n,
-                    const BvhNode* nodes_in, BuildScratch& scratch, BvhNode* nodes,
+// Build the TLAS over n instances (world boxes computed from BLAS roots) and
+// n_flat world-space triangles referenced directly (flat_verts: 3 float4 per
+// triangle).  Leaf payload p < n is instance p, p >= n is flat triangle p - n.
+// slot_ranges[i] = triangle slot range of instance i's BLAS (its world box is
+// the transformed bounds of those vertices).
+uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint32_t n, const float4* tri_verts,
+                    const float4* flat_verts, uint32_t n_flat, BuildScratch& scratch, BvhNode* nodes,
                     uint32_t node_base, cudaStream_t stream);
 
-// Count structural violations of the resident BVH.
-uint64_t validate_bvh(const SceneView& s, uint32_t total_slots, uint32_t num_instances,
-                      const uint32_t* blas_slot_begin, const uint32_t* blas_slot_end,
-                      cudaStream_t stream);
+// One built bottom-level structure: its root node and triangle slot range.
+struct BlasRange {
+  uint32_t root, slot_begin, slot_end;
+};
+
+// Count structural violations of the resident BVH: every slot of every built
+// BLAS reached exactly once from its root, child boxes inside parent boxes.
+uint64_t validate_bvh(const SceneView& s, const std::vector<BlasRange>& blas, cudaStream_t stream);
 
 }  // namespace olc

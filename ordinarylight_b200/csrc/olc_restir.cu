@@ -14,9 +14,15 @@
 //
 // Storage: two uint4 words per reservoir,
 //   w0 = (light index, barycentrics as half2, w_sum, M)
-//   w1 = (p_hat of the selected sample, primary depth, octahedral normal, valid)
+//   w1 = (p_hat of the selected sample, primary depth, octahedral normal, stamp)
 // indexed by sample stream * npix + pixel, so a stream's history survives
-// chunking and batching.
+// chunking and batching.  A reservoir is valid only when its stamp equals the
+// stamp of the frame that should have written it, so pixels whose primary ray
+// missed never need clearing.
+//
+// Only primary rays that hit take part: a compaction pass lists them first,
+// so the candidate loop runs with full warps even when much of the image is
+// sky.
 #include <cuda_fp16.h>
 
 #include "olc_restir.h"
@@ -27,6 +33,8 @@ namespace olc {
 namespace {
 
 constexpr uint32_t kRestirStream = 0x52455354u;  // stream key offset of the reuse passes
+
+OLC_D uint32_t lane() { return threadIdx.x & 31u; }
 
 OLC_D uint32_t oct_encode(float3 n) {
   float s = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
@@ -54,9 +62,42 @@ OLC_D float3 oct_decode(uint32_t v) {
   return normalize(f3(x, y, z));
 }
 
+// BSDF of one surface with the light-independent terms hoisted
+// (preparePrimaryPbr, transport_v1/lighting.glsl:116-133): every candidate
+// then costs only the half-vector terms.
+struct PreparedBsdf {
+  float3 n, view, f0, diffuse;
+  float nv, a2, g1v;
+};
+
+OLC_D PreparedBsdf prepare_bsdf(const SurfaceMat& m, float3 n, float3 view) {
+  PreparedBsdf b;
+  b.n = n;
+  b.view = view;
+  b.nv = fmaxf(dot(n, view), 0.0f);
+  b.f0 = lerp3(f3(0.04f, 0.04f, 0.04f), m.base, m.metallic);
+  b.diffuse = m.base * ((1.0f - m.metallic) / OLC_PI);
+  b.a2 = ggx_alpha2(m.roughness);
+  b.g1v = ggx_g1(b.nv, b.a2);
+  return b;
+}
+
+OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
+  float3 h = normalize(b.view + l);
+  float nh = fmaxf(dot(b.n, h), 0.0f);
+  float vh = fmaxf(dot(b.view, h), 0.0f);
+  float w = 1.0f - clampf(vh, 0.0f, 1.0f);
+  float w5 = w * w * w * w * w;
+  float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
+  float D = ggx_d(nh, b.a2);
+  float G = b.g1v * ggx_g1(nl, b.a2);
+  float3 spec = F * (D * G / fmaxf(4.0f * b.nv * nl, 1e-6f));
+  return (f3(1.0f, 1.0f, 1.0f) - F) * b.diffuse + spec;
+}
+
 struct Surface {
-  float3 p, n, view;
-  SurfaceMat m;
+  float3 p;
+  PreparedBsdf bsdf;
   float depth;
   bool valid;
 };
@@ -69,9 +110,7 @@ struct Res {
   float target;
 };
 
-OLC_D float2 unpack_bary(uint32_t b) {
-  return __half22float2(*reinterpret_cast<const __half2*>(&b));
-}
+OLC_D float2 unpack_bary(uint32_t b) { return __half22float2(*reinterpret_cast<const __half2*>(&b)); }
 OLC_D uint32_t pack_bary(float b1, float b2) {
   __half2 h = __floats2half2_rn(b1, b2);
   return *reinterpret_cast<uint32_t*>(&h);
@@ -79,33 +118,30 @@ OLC_D uint32_t pack_bary(float b1, float b2) {
 
 // Unshadowed target of light sample (light, bary) at surface s.
 OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary) {
-  const EmitterRec e = sc.emitters[light];
+  const EmitterRec e = load_emitter(sc, light);
   float2 b = unpack_bary(bary);
-  float3 lp = f3(e.a) * fmaxf(1.0f - b.x - b.y, 0.0f) + f3(e.b) * b.x + f3(e.c) * b.y;
-  float3 off = lp - s.p;
+  float3 off = emitter_point(e, b.x, b.y) - s.p;
   float d2 = dot(off, off);
   if (!(d2 > 1e-12f)) return 0.0f;
-  float dist = sqrtf(d2);
-  float3 l = off / dist;
-  float cs = dot(s.n, l);
-  if (cs <= 0.0f) return 0.0f;
+  float inv = rsqrtf(d2);
+  float3 l = off * inv;
+  float cs = dot(s.bsdf.n, l);
+  if (cs <= 0.0f || s.bsdf.nv <= 0.0f) return 0.0f;
   float cl = emitter_cosine(e, l);
   if (cl <= 1e-6f) return 0.0f;
-  float3 f = pbr_eval(s.m, s.n, s.view, l);
-  float t = luminance(f * f3(e.emission_area)) * cs * cl / d2;
+  float3 f = prepared_eval(s.bsdf, l, cs);
+  float t = luminance(f * f3(e.emission)) * cs * cl / d2;
   return (t == t && t < 3.0e38f) ? fmaxf(t, 0.0f) : 0.0f;
 }
 
-OLC_D bool res_update(Res& r, uint32_t light, uint32_t bary, float target, float w, uint32_t m, float u) {
+OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float w, uint32_t m, float u) {
   r.M += m;
   r.w_sum += w;
-  bool sel = w > 0.0f && (r.light == 0xffffffffu || u * r.w_sum < w);
-  if (sel) {
+  if (w > 0.0f && (r.light == 0xffffffffu || u * r.w_sum < w)) {
     r.light = light;
     r.bary = bary;
     r.target = target;
   }
-  return sel;
 }
 
 OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i) {
@@ -130,28 +166,25 @@ OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBu
   if (!(dot(ns, ns) > 0.5f)) ns = ng;
   if (dot(ns, ng) < 0.0f) ns = -ns;
   const bool entering = dot(d, ng) < 0.0f;
-  su.n = entering ? ns : -ns;
   su.p = f3(ot) + d * hit.x;
-  su.view = -d;
-  su.m = load_material(s, ir.material);
+  const uint32_t owner = owner_instance(s.instances, s.tri_owner, h.instance[i], slot);
+  su.bsdf = prepare_bsdf(load_material(s, s.instances[owner].material), entering ? ns : -ns, -d);
   su.depth = hit.x;
   su.valid = true;
   return su;
 }
 
 OLC_D bool similar(const Surface& s, uint32_t w1_normal, float depth) {
-  float3 n = oct_decode(w1_normal);
-  if (dot(n, s.n) < 0.9f) return false;
+  if (dot(oct_decode(w1_normal), s.bsdf.n) < 0.9f) return false;
   return fabsf(depth - s.depth) <= 0.1f * s.depth;
 }
 
-OLC_D void store_res(uint4* w0, uint4* w1, uint64_t g, const Res& r, const Surface& s) {
+OLC_D void store_res(uint4* w0, uint4* w1, uint64_t g, const Res& r, const Surface& s, uint32_t stamp) {
   w0[g] = make_uint4(r.light, r.bary, __float_as_uint(r.w_sum), r.M);
-  w1[g] = make_uint4(__float_as_uint(r.target), __float_as_uint(s.valid ? s.depth : -1.0f),
-                     s.valid ? oct_encode(s.n) : 0u, s.valid ? 1u : 0u);
+  w1[g] = make_uint4(__float_as_uint(r.target), __float_as_uint(s.depth), oct_encode(s.bsdf.n), stamp);
 }
 
-OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, uint32_t& nrm, bool& valid) {
+OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, uint32_t& nrm, uint32_t& stamp) {
   uint4 a = w0[g], b = w1[g];
   Res r;
   r.light = a.x;
@@ -161,7 +194,7 @@ OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, u
   r.target = __uint_as_float(b.x);
   depth = __uint_as_float(b.y);
   nrm = b.z;
-  valid = b.w != 0u;
+  stamp = b.w;
   return r;
 }
 
@@ -173,9 +206,11 @@ struct RestirArgs {
   PathState ps;
   uint64_t chunk_begin;
   uint32_t chunk_count;
-  uint32_t npix;
+  const uint32_t* hit_list;
+  const uint32_t* hit_count;
   uint32_t candidates;
-  uint32_t use_history;
+  uint32_t history_stamp;   // stamp of the previous frame's final reservoirs (0: none)
+  uint32_t stamp;           // this frame's stamp
   uint32_t history_cap;     // M cap of the temporal history
   uint32_t neighbours;
   float radius;
@@ -190,81 +225,99 @@ struct RestirArgs {
   uint32_t finalize;
 };
 
+// List the chunk's primary rays that hit something (warp-aggregated append;
+// the list order does not affect any result).
+__global__ void k_restir_compact(HitBuf h, uint32_t n, uint32_t* list, uint32_t* count) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    uint32_t i = base + lane();
+    bool hit = i < n && h.tuv_slot[i].x >= 0.0f;
+    uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+    if (ballot == 0u) continue;
+    uint32_t leader = __ffs(ballot) - 1u;
+    uint32_t off = 0;
+    if (lane() == leader) off = atomicAdd(count, __popc(ballot));
+    off = __shfl_sync(0xffffffffu, off, leader);
+    if (hit) list[off + __popc(ballot & ((1u << lane()) - 1u))] = i;
+  }
+}
+
 __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
   const FrameParams& fp = *a.fp;
   const SceneView& s = a.s;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.chunk_count; i += gridDim.x * blockDim.x) {
-    uint4 meta = a.ps.meta[i];
+  const uint32_t n = *a.hit_count;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t i = a.hit_list[k];
+    const uint4 meta = a.ps.meta[i];
     const uint64_t g = a.chunk_begin + i;
-    Surface su = primary_surface(s, a.q, a.h, i);
+    const Surface su = primary_surface(s, a.q, a.h, i);
     Res r{0xffffffffu, 0u, 0.0f, 0u, 0.0f};
-    if (su.valid) {
-      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), kRestirStream);
-      for (uint32_t c = 0; c < a.candidates; ++c) {
-        float sel = olc_rand(rng);
-        uint32_t li = select_emitter(s, sel);
-        float ru = sqrtf(olc_rand(rng));
-        float rv = olc_rand(rng);
-        uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
-        float t = target_of(s, su, li, bary);
-        const EmitterRec& e = s.emitters[li];
-        float p_src = e.dist.y / fmaxf(e.emission_area.w, 1e-12f);
-        float w = p_src > 0.0f ? t / p_src : 0.0f;
-        res_update(r, li, bary, t, w, 1u, olc_rand(rng));
-      }
-      // temporal reuse
-      if (a.use_history) {
-        float pd;
-        uint32_t pn;
-        bool pv;
-        Res prev = load_res(a.hist0, a.hist1, g, pd, pn, pv);
-        if (pv && prev.light != 0xffffffffu && prev.M > 0u && prev.target > 0.0f && similar(su, pn, pd)) {
-          uint32_t m = min(prev.M, a.history_cap);
-          float wsum = prev.w_sum * ((float)m / (float)prev.M);
-          float t = target_of(s, su, prev.light, prev.bary);
-          float w = t * wsum / prev.target;
-          res_update(r, prev.light, prev.bary, t, w, m, olc_rand(rng));
-        }
+    uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), kRestirStream);
+    for (uint32_t c = 0; c < a.candidates; ++c) {
+      uint32_t li = select_emitter(s, olc_rand(rng));
+      float ru = sqrtf(olc_rand(rng));
+      float rv = olc_rand(rng);
+      uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
+      float t = target_of(s, su, li, bary);
+      const float4 ap = __ldg(&s.emitters[li].a_pdf);
+      const float area = __ldg(&s.emitters[li].e1_area.w);
+      float p_src = ap.w / fmaxf(area, 1e-12f);
+      float w = p_src > 0.0f ? t / p_src : 0.0f;
+      res_update(r, li, bary, t, w, 1u, olc_rand(rng));
+    }
+    // temporal reuse
+    if (a.history_stamp) {
+      float pd;
+      uint32_t pn, pstamp;
+      Res prev = load_res(a.hist0, a.hist1, g, pd, pn, pstamp);
+      if (pstamp == a.history_stamp && prev.light != 0xffffffffu && prev.M > 0u && prev.target > 0.0f &&
+          similar(su, pn, pd)) {
+        uint32_t m = min(prev.M, a.history_cap);
+        float wsum = prev.w_sum * ((float)m / (float)prev.M);
+        float t = target_of(s, su, prev.light, prev.bary);
+        res_update(r, prev.light, prev.bary, t, t * wsum / prev.target, m, olc_rand(rng));
       }
     }
-    store_res(a.out0, a.out1, g, r, su);
+    store_res(a.out0, a.out1, g, r, su, a.stamp);
   }
 }
 
 __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
   const FrameParams& fp = *a.fp;
   const SceneView& s = a.s;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.chunk_count; i += gridDim.x * blockDim.x) {
-    uint4 meta = a.ps.meta[i];
+  const uint32_t n = *a.hit_count;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t i = a.hit_list[k];
+    const uint4 meta = a.ps.meta[i];
     const uint64_t g = a.chunk_begin + i;
     const uint64_t stream_base = g - meta.x;  // stream * npix
-    Surface su = primary_surface(s, a.q, a.h, i);
+    const Surface su = primary_surface(s, a.q, a.h, i);
     float d0;
-    uint32_t n0;
-    bool v0;
-    Res r = load_res(a.in0, a.in1, g, d0, n0, v0);
-    if (su.valid && a.neighbours > 0u) {
+    uint32_t n0, st0;
+    Res r = load_res(a.in0, a.in1, g, d0, n0, st0);
+    if (a.neighbours > 0u) {
       uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), kRestirStream + 1u + a.pass);
       const int px = (int)(meta.x % fp.width), py = (int)(meta.x / fp.width);
-      for (uint32_t k = 0; k < a.neighbours; ++k) {
+      for (uint32_t j = 0; j < a.neighbours; ++j) {
         float rr = a.radius * sqrtf(olc_rand(rng));
         float th = 2.0f * OLC_PI * olc_rand(rng);
         float u = olc_rand(rng);
-        int qx = px + __float2int_rn(rr * cosf(th));
-        int qy = py + __float2int_rn(rr * sinf(th));
+        float sn, cs;
+        __sincosf(th, &sn, &cs);
+        int qx = px + __float2int_rn(rr * cs);
+        int qy = py + __float2int_rn(rr * sn);
         if (qx < 0 || qy < 0 || qx >= (int)fp.width || qy >= (int)fp.height || (qx == px && qy == py)) continue;
         uint64_t gq = stream_base + (uint64_t)qy * fp.width + (uint64_t)qx;
         float dq;
-        uint32_t nq;
-        bool vq;
-        Res nb = load_res(a.in0, a.in1, gq, dq, nq, vq);
-        if (!vq || nb.light == 0xffffffffu || nb.M == 0u || !(nb.target > 0.0f) || !similar(su, nq, dq)) continue;
+        uint32_t nq, sq;
+        Res nb = load_res(a.in0, a.in1, gq, dq, nq, sq);
+        if (sq != a.stamp || nb.light == 0xffffffffu || nb.M == 0u || !(nb.target > 0.0f) || !similar(su, nq, dq))
+          continue;
         float t = target_of(s, su, nb.light, nb.bary);
-        float w = t * nb.w_sum / nb.target;
-        res_update(r, nb.light, nb.bary, t, w, nb.M, u);
+        res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u);
       }
     }
-    store_res(a.out0, a.out1, g, r, su);
+    store_res(a.out0, a.out1, g, r, su, a.stamp);
     if (a.finalize) {
       float W = (r.light != 0xffffffffu && r.M > 0u && r.target > 0.0f) ? r.w_sum / ((float)r.M * r.target) : 0.0f;
       if (!(W == W) || W > 3.0e38f) W = 0.0f;
@@ -285,16 +338,18 @@ void restir_prepare(RestirState& st, const olc_config& cfg, uint32_t w, uint32_t
     st.res_b1.allocate(n * 16);
     st.hist0.allocate(n * 16);
     st.hist1.allocate(n * 16);
+    // stamps start at 1; zero-filled buffers are never valid
+    for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, n * 16));
     st.reservoirs = n;
     st.history_valid = false;
   }
   if (slots > st.slots) {
     st.selected.allocate((size_t)slots * 16);
+    st.hit_list.allocate((size_t)slots * 4);
     st.slots = slots;
   }
-  auto same = [](const float4& x, const float4& y) {
-    return x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w;
-  };
+  if (!st.hit_count.get()) st.hit_count.allocate(16);
+  auto same = [](const float4& x, const float4& y) { return x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w; };
   bool camera_same = same(cam.cam_pos, st.hist_camera.cam_pos) && same(cam.cam_forward, st.hist_camera.cam_forward) &&
                      same(cam.cam_right, st.hist_camera.cam_right) && same(cam.cam_up, st.hist_camera.cam_up) &&
                      cam.projection == st.hist_camera.projection;
@@ -305,11 +360,13 @@ void restir_prepare(RestirState& st, const olc_config& cfg, uint32_t w, uint32_t
   st.cur_spp = spp;
   st.cur_frame = frame_index;
   st.hist_camera = cam;
+  st.prev_stamp = st.stamp;
+  st.stamp = st.stamp + 1u == 0u ? 1u : st.stamp + 1u;
 }
 
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
                         const FrameParams* fp, const RayQueue& q, const HitBuf& hits, const PathState& ps,
-                        Counters* /*cnt*/, uint64_t chunk_begin, uint32_t chunk_count, uint32_t npix,
+                        Counters* /*cnt*/, uint64_t chunk_begin, uint32_t chunk_count, uint32_t /*npix*/,
                         cudaStream_t stream) {
   RestirArgs a{};
   a.fp = fp;
@@ -319,9 +376,11 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.ps = ps;
   a.chunk_begin = chunk_begin;
   a.chunk_count = chunk_count;
-  a.npix = npix;
+  a.hit_list = st.hit_list.as<uint32_t>();
+  a.hit_count = st.hit_count.as<uint32_t>();
   a.candidates = cfg.restir_candidates;
-  a.use_history = st.history_used ? 1u : 0u;
+  a.history_stamp = st.history_used ? st.prev_stamp : 0u;
+  a.stamp = st.stamp;
   a.history_cap = std::max<uint32_t>(1u, cfg.restir_max_history ? cfg.restir_max_history : 20u) * cfg.restir_candidates;
   a.neighbours = cfg.restir_neighbours;
   a.radius = cfg.restir_radius > 0.0f ? cfg.restir_radius : 30.0f;
@@ -330,7 +389,11 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.selected = st.selected.as<uint4>();
   a.out0 = st.res_a0.as<uint4>();
   a.out1 = st.res_a1.as<uint4>();
-  uint32_t grid = ls.grid_shade;
+  OLC_CUDA(cudaMemsetAsync(st.hit_count.get(), 0, 4, stream));
+  k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hits, chunk_count, st.hit_list.as<uint32_t>(),
+                                                        st.hit_count.as<uint32_t>());
+  OLC_LAUNCH_CHECK("k_restir_compact");
+  const uint32_t grid = ls.grid_shade;
   k_restir_initial<<<grid, 128, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_restir_initial");
   // spatial passes ping-pong A -> B -> A ...; the last pass finalises.
@@ -382,6 +445,8 @@ void restir_release(RestirState& st) {
   st.hist0.release();
   st.hist1.release();
   st.selected.release();
+  st.hit_list.release();
+  st.hit_count.release();
   st.reservoirs = 0;
   st.slots = 0;
   st.history_valid = false;

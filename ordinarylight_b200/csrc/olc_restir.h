@@ -12,8 +12,11 @@ struct RestirState {
   DeviceBuffer res_a0, res_a1;     // current reservoirs (two uint4 words each)
   DeviceBuffer res_b0, res_b1;     // spatial ping-pong
   DeviceBuffer hist0, hist1;       // previous frame's final reservoirs
-  DeviceBuffer gbuf_pos, gbuf_nrm, gbuf_view;  // primary surface per path slot
   DeviceBuffer selected;           // per path slot: light, bary, W
+  DeviceBuffer hit_list;           // path slots whose primary ray hit
+  DeviceBuffer hit_count;
+  uint32_t stamp = 0;              // validity stamp of this frame's reservoirs
+  uint32_t prev_stamp = 0;
   uint64_t reservoirs = 0;         // npix * spp capacity
   uint32_t slots = 0;              // path slot capacity
   // frame continuity of the history

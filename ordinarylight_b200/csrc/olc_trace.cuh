@@ -104,9 +104,14 @@ struct TraversalStack {
   int* smem;           // this thread's column in the shared stack
   int stride;
   int sp;
-  int spill[OLC_SPILL];
+  int* spill;          // this thread's local overflow array (OLC_SPILL entries)
 
-  OLC_D void init(int* base, int tid, int threads) { smem = base + tid; stride = threads; sp = 0; }
+  OLC_D void init(int* base, int tid, int threads, int* spill_area) {
+    smem = base + tid;
+    stride = threads;
+    sp = 0;
+    spill = spill_area;
+  }
   OLC_D bool push(int v, uint32_t& err) {
     if (sp < STACK) { smem[sp * stride] = v; ++sp; return true; }
     if (sp < STACK + OLC_SPILL) { spill[sp - STACK] = v; ++sp; return true; }
@@ -160,101 +165,159 @@ OLC_D void node_boxes(const BvhNode* nodes, int node, const TraceRay& r, float t
   near1 = n1;
 }
 
-// Traverse the two-level structure.  ANY_HIT stops at the first hit in
-// (t_min, t_max).  Returns true on a hit.
+// Resumable traversal of the two-level structure.  ANY_HIT stops at the
+// first hit in (t_min, t_max).  advance() runs at most `iterations` loop
+// iterations (node visits, leaf tests, instance transitions) and returns true
+// once the ray is finished, so a persistent kernel can refill lanes whose rays
+// finished while the other lanes of the warp are still traversing.
 template <int STACK, bool ANY_HIT>
-OLC_D bool olc_traverse(const SceneView& s, float3 wo, float3 wd, float t_min, float t_max,
-                        HitResult& hit, int* smem_base, uint32_t& err) {
-  TraversalStack<STACK> st;
-  st.init(smem_base, threadIdx.x, blockDim.x);
+struct Traversal {
   TraceRay ray;
-  setup_ray(ray, wo, wd);
-  hit.t = t_max;
-  hit.instance = 0xffffffffu;
-  hit.slot = 0;
-  hit.u = hit.v = 0.0f;
-  hit.packed = 0xffffffffu;
-  bool found = false;
-  int level = 0;
-  uint32_t cur_inst = 0, cur_prim_offset = 0;
-  int node = (int)s.tlas_root;
-  // A well-formed tree is acyclic and finite; the cap only guarantees the
-  // loop ends (and reports an error) should the structure ever be corrupt.
-  uint32_t budget = OLC_TRAVERSAL_BUDGET;
-  while (true) {
-    if (--budget == 0u) {
-      err = 1u;
-      break;
-    }
-    if (node >= 0 && node != OLC_MARKER) {
-      bool h0, h1;
-      float n0, n1;
-      int c0, c1;
-      node_boxes(s.nodes, node, ray, t_min, hit.t, h0, h1, n0, n1, c0, c1);
-      if (h0 && h1) {
-        int near_c = (n0 <= n1) ? c0 : c1;
-        int far_c = (n0 <= n1) ? c1 : c0;
-        st.push(far_c, err);
-        node = near_c;
-        continue;
+  float3 wo, wd;
+  float t_min;
+  HitResult hit;
+  int node;
+  int level;
+  uint32_t cur_inst, cur_prim_offset;
+  uint32_t budget;
+  bool found;
+  TraversalStack<STACK> st;
+
+  OLC_D void begin(const SceneView& s, float3 o, float3 d, float tmin, float tmax, int* smem_base,
+                   int* spill_area) {
+    st.init(smem_base, threadIdx.x, blockDim.x, spill_area);
+    wo = o;
+    wd = d;
+    t_min = tmin;
+    setup_ray(ray, o, d);
+    hit.t = tmax;
+    hit.instance = 0xffffffffu;
+    hit.slot = 0;
+    hit.u = hit.v = 0.0f;
+    hit.packed = 0xffffffffu;
+    found = false;
+    level = 0;
+    cur_inst = 0;
+    cur_prim_offset = 0;
+    node = (int)s.tlas_root;
+    // A well-formed tree is acyclic and finite; the budget only guarantees
+    // the loop ends (and reports an error) should the structure be corrupt.
+    budget = OLC_TRAVERSAL_BUDGET;
+  }
+
+  OLC_D bool advance(const SceneView& s, int iterations, uint32_t& err) {
+    for (int it = 0; it < iterations; ++it) {
+      if (--budget == 0u) {
+        err = 1u;
+        return true;
       }
-      if (h0) { node = c0; continue; }
-      if (h1) { node = c1; continue; }
-    } else if (node != OLC_MARKER) {
-      uint32_t first = olc_leaf_first(node);
-      uint32_t count = olc_leaf_count(node);
-      if (level == 0) {
-        // instance leaf (TLAS leaves hold one instance)
-        Affine w2o;
-        uint32_t root;
-        load_instance_w2o(s.instances, first, w2o, root, cur_prim_offset);
-        cur_inst = first;
-        float3 oo = xform_point(w2o, wo);
-        float3 od = xform_vector(w2o, wd);
-        setup_ray(ray, oo, od);
-        level = 1;
-        if (st.push(OLC_MARKER, err)) {
-          node = (int)root;
+      if (node >= 0 && node != OLC_MARKER) {
+        bool h0, h1;
+        float n0, n1;
+        int c0, c1;
+        node_boxes(s.nodes, node, ray, t_min, hit.t, h0, h1, n0, n1, c0, c1);
+        if (h0 && h1) {
+          int near_c = (n0 <= n1) ? c0 : c1;
+          int far_c = (n0 <= n1) ? c1 : c0;
+          st.push(far_c, err);
+          node = near_c;
           continue;
         }
-        level = 0;
-        setup_ray(ray, wo, wd);
-      } else {
-        for (uint32_t k = 0; k < count; ++k) {
-          uint32_t slot = first + k;
+        if (h0) { node = c0; continue; }
+        if (h1) { node = c1; continue; }
+      } else if (node != OLC_MARKER) {
+        uint32_t first = olc_leaf_first(node);
+        uint32_t count = olc_leaf_count(node);
+        if (level == 0 && first >= s.tlas_instances) {
+          // world-space triangle referenced directly by the TLAS
+          const uint32_t slot = s.flat_slot_base + (first - s.tlas_instances);
           const float4* tv = s.tri_verts + 3u * slot;
           float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
           float t, b1, b2;
           if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
             if (ANY_HIT) {
               hit.t = t;
-              hit.instance = cur_inst;
+              hit.instance = s.flat_instance;
               hit.slot = slot;
+              found = true;
               return true;
             }
-            uint32_t packed = cur_prim_offset + __ldg(s.tri_index + slot);
+            uint32_t packed = __ldg(s.tri_index + slot);
             if (t < hit.t || packed < hit.packed) {
               hit.t = t;
               hit.u = b1;
               hit.v = b2;
               hit.slot = slot;
-              hit.instance = cur_inst;
+              hit.instance = s.flat_instance;
               hit.packed = packed;
               found = true;
             }
           }
+        } else if (level == 0) {
+          // instance leaf (TLAS leaves hold one instance)
+          Affine w2o;
+          uint32_t root;
+          load_instance_w2o(s.instances, first, w2o, root, cur_prim_offset);
+          cur_inst = first;
+          setup_ray(ray, xform_point(w2o, wo), xform_vector(w2o, wd));
+          level = 1;
+          if (st.push(OLC_MARKER, err)) {
+            node = (int)root;
+            continue;
+          }
+          level = 0;
+          setup_ray(ray, wo, wd);
+        } else {
+          for (uint32_t k = 0; k < count; ++k) {
+            uint32_t slot = first + k;
+            const float4* tv = s.tri_verts + 3u * slot;
+            float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
+            float t, b1, b2;
+            if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
+              if (ANY_HIT) {
+                hit.t = t;
+                hit.instance = cur_inst;
+                hit.slot = slot;
+                found = true;
+                return true;
+              }
+              uint32_t packed = cur_prim_offset + __ldg(s.tri_index + slot);
+              if (t < hit.t || packed < hit.packed) {
+                hit.t = t;
+                hit.u = b1;
+                hit.v = b2;
+                hit.slot = slot;
+                hit.instance = cur_inst;
+                hit.packed = packed;
+                found = true;
+              }
+            }
+          }
         }
       }
-    }
-    // pop
-    if (st.sp == 0) break;
-    node = st.pop();
-    if (node == OLC_MARKER) {
-      level = 0;
-      setup_ray(ray, wo, wd);
-      if (st.sp == 0) break;
+      // pop
+      if (st.sp == 0) return true;
       node = st.pop();
+      if (node == OLC_MARKER) {
+        level = 0;
+        setup_ray(ray, wo, wd);
+        if (st.sp == 0) return true;
+        node = st.pop();
+      }
     }
+    return false;
   }
-  return found;
+};
+
+// Blocking traversal: the whole ray in one call.  Returns true on a hit.
+template <int STACK, bool ANY_HIT>
+OLC_D bool olc_traverse(const SceneView& s, float3 wo, float3 wd, float t_min, float t_max,
+                        HitResult& hit, int* smem_base, uint32_t& err) {
+  Traversal<STACK, ANY_HIT> tr;
+  int spill[OLC_SPILL];
+  tr.begin(s, wo, wd, t_min, t_max, smem_base, spill);
+  while (!tr.advance(s, 1 << 30, err)) {
+  }
+  hit = tr.hit;
+  return tr.found;
 }

@@ -54,56 +54,117 @@ __global__ void k_raygen(const FrameParams* __restrict__ fp_ptr, uint64_t chunk_
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = chunk_count;
 }
 
-template <int STACK>
+// Persistent traversal (Aila and Laine, "Understanding the Efficiency of Ray
+// Traversal on GPUs", HPG 2009: persistent threads with dynamic fetch).
+// Scheduler 0 (refill): each lane runs its ray for up to 16 loop iterations;
+// lanes whose ray finished are refilled from the queue with one
+// warp-aggregated atomic once at least 8 of them are idle, so SIMD lanes stay
+// busy instead of waiting for the warp's longest ray.  Scheduler 1 (batch): a
+// warp takes 32 rays and runs all of them to completion before fetching more.
+template <int SCHED>
+struct TraceSchedule;
+template <>
+struct TraceSchedule<0> {
+  static constexpr int kSteps = 16;
+  static constexpr uint32_t kRefillLanes = 8;
+};
+template <>
+struct TraceSchedule<1> {
+  static constexpr int kSteps = 1 << 30;
+  static constexpr uint32_t kRefillLanes = 32;
+};
+
+template <int STACK, bool ANY_HIT, int SCHED, class Load, class Store>
+OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, int* smem, Load load, Store store,
+                            uint32_t& err) {
+  constexpr int kTraceSteps = TraceSchedule<SCHED>::kSteps;
+  constexpr uint32_t kRefillLanes = TraceSchedule<SCHED>::kRefillLanes;
+  Traversal<STACK, ANY_HIT> tr;
+  int spill[OLC_SPILL];
+  uint32_t my = 0xffffffffu;
+  bool exhausted = false;
+  const uint32_t lt = (1u << lane_id()) - 1u;
+  while (true) {
+    const bool idle = my == 0xffffffffu;
+    if (!exhausted) {
+      const uint32_t idle_mask = __ballot_sync(0xffffffffu, idle);
+      const uint32_t want = __popc(idle_mask);
+      if (want >= kRefillLanes || idle_mask == 0xffffffffu) {
+        const uint32_t leader = __ffs(idle_mask) - 1u;
+        uint32_t base = 0;
+        if (lane_id() == leader) base = atomicAdd(cursor, want);
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (idle) {
+          const uint32_t cand = base + __popc(idle_mask & lt);
+          if (cand < n) {
+            my = cand;
+            float3 o, d;
+            float tmin, tmax;
+            load(my, o, d, tmin, tmax);
+            tr.begin(s, o, d, tmin, tmax, smem, spill);
+          }
+        }
+        if (base + want >= n) exhausted = true;
+      }
+    }
+    if (__ballot_sync(0xffffffffu, my != 0xffffffffu) == 0u) break;
+    if (my != 0xffffffffu && tr.advance(s, kTraceSteps, err)) {
+      store(my, tr);
+      my = 0xffffffffu;
+    }
+  }
+}
+
+template <int STACK, int SCHED>
 __global__ void __launch_bounds__(128) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
                                                        uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->queue_count[bounce];
   uint32_t err = 0;
-  while (true) {
-    uint32_t base = 0;
-    if (lane_id() == 0) base = atomicAdd(&cnt->closest_cursor[bounce], 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    uint32_t i = base + lane_id();
-    if (i < n) {
-      float4 ot = q.origin_tmin[i];
-      float4 dt = q.dir_tmax[i];
-      HitResult hr;
-      bool hit = olc_traverse<STACK, false>(s, f3(ot), f3(dt), ot.w, dt.w, hr, smem_stack, err);
-      h.tuv_slot[i] = hit ? make_float4(hr.t, hr.u, hr.v, __uint_as_float(hr.slot))
-                          : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
-      h.instance[i] = hit ? hr.instance : 0xffffffffu;
-    }
-  }
+  persistent_trace<STACK, false, SCHED>(
+      s, n, &cnt->closest_cursor[bounce], smem_stack,
+      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax) {
+        float4 ot = q.origin_tmin[i];
+        float4 dt = q.dir_tmax[i];
+        o = f3(ot);
+        d = f3(dt);
+        tmin = ot.w;
+        tmax = dt.w;
+      },
+      [&](uint32_t i, const Traversal<STACK, false>& tr) {
+        h.tuv_slot[i] = tr.found ? make_float4(tr.hit.t, tr.hit.u, tr.hit.v, __uint_as_float(tr.hit.slot))
+                                 : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+        h.instance[i] = tr.found ? tr.hit.instance : 0xffffffffu;
+      },
+      err);
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
 
-template <int STACK>
+template <int STACK, int SCHED>
 __global__ void __launch_bounds__(128) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
                                                       uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->shadow_count[bounce];
   uint32_t err = 0;
-  while (true) {
-    uint32_t base = 0;
-    if (lane_id() == 0) base = atomicAdd(&cnt->shadow_cursor[bounce], 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    uint32_t i = base + lane_id();
-    if (i < n) {
-      float4 ot = sq.origin_tmax[i];
-      float4 dp = sq.dir_path[i];
-      HitResult hr;
-      bool occluded = olc_traverse<STACK, true>(s, f3(ot), f3(dp), 0.001f, ot.w, hr, smem_stack, err);
-      if (!occluded) {
-        uint32_t path = __float_as_uint(dp.w);
-        float4 c = sq.contrib[i];
-        float4 r = ps.radiance[path];
-        ps.radiance[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
-      }
-    }
-  }
+  persistent_trace<STACK, true, SCHED>(
+      s, n, &cnt->shadow_cursor[bounce], smem_stack,
+      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax) {
+        float4 ot = sq.origin_tmax[i];
+        float4 dp = sq.dir_path[i];
+        o = f3(ot);
+        d = f3(dp);
+        tmin = 0.001f;
+        tmax = ot.w;
+      },
+      [&](uint32_t i, const Traversal<STACK, true>& tr) {
+        if (!tr.found) {
+          uint32_t path = __float_as_uint(sq.dir_path[i].w);
+          float4 c = sq.contrib[i];
+          float4 r = ps.radiance[path];
+          ps.radiance[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
+        }
+      },
+      err);
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
 
@@ -186,13 +247,14 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
         float3 gcross = cross(e1, e2);
         float3 ng = normalize(gcross);
         float3 p = o + d * t;
-        SurfaceMat m = load_material(s, ir.material);
+        const InstanceRec& orec = s.instances[owner_instance(s.instances, s.tri_owner, inst, slot)];
+        SurfaceMat m = load_material(s, orec.material);
         if (bounce == 0 && meta.y == 0 && a.prod.depth) {
           a.prod.depth[meta.x] = t;
           float3 fn = dot(ng, d) > 0.0f ? -ng : ng;
           a.prod.normal[meta.x] = make_float4(fn.x, fn.y, fn.z, 0.0f);
-          a.prod.instance_id[meta.x] = ir.instance_id;
-          a.prod.material_id[meta.x] = s.material_aux[ir.material].material_id;
+          a.prod.instance_id[meta.x] = orec.instance_id;
+          a.prod.material_id[meta.x] = s.material_aux[orec.material].material_id;
           a.prod.primitive_id[meta.x] = ir.prim_offset + s.tri_index[slot];
         }
         if (MODE == 1) {
@@ -243,9 +305,9 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
               did_restir = true;
               float Wr = __uint_as_float(rs.z);
               if (rs.x != 0xffffffffu && Wr > 0.0f) {
-                const EmitterRec e = s.emitters[rs.x];
+                const EmitterRec e = load_emitter(s, rs.x);
                 float2 bary = __half22float2(*reinterpret_cast<const __half2*>(&rs.y));
-                float3 lp = f3(e.a) * fmaxf(1.0f - bary.x - bary.y, 0.0f) + f3(e.b) * bary.x + f3(e.c) * bary.y;
+                float3 lp = emitter_point(e, bary.x, bary.y);
                 float3 off = lp - p;
                 float dist2 = dot(off, off);
                 float dist = sqrtf(dist2);
@@ -255,7 +317,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                 if (sc > 0.0f && lc > 1e-6f) {
                   float3 f = pbr_eval(m, nrm, view, ldir);
                   float G = lc / fmaxf(dist2, 1e-12f);
-                  float3 c = tp * f * f3(e.emission_area) * (sc * G * Wr);
+                  float3 c = tp * f * f3(e.emission) * (sc * G * Wr);
                   if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
                     sh_o = p + nrm * 0.002f;
                     sh_d = ldir;
@@ -273,10 +335,10 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                 // area light (sampleAreaLightTechnique, lighting.glsl:341-403)
                 float sel = olc_rand(rng);
                 uint32_t li = select_emitter(s, sel);
-                const EmitterRec e = s.emitters[li];
+                const EmitterRec e = load_emitter(s, li);
                 float ru = sqrtf(olc_rand(rng));
                 float rv = olc_rand(rng);
-                float3 lp = emitter_point(e, ru, rv);
+                float3 lp = emitter_point(e, ru * (1.0f - rv), ru * rv);
                 float3 off = lp - p;
                 float dist2 = dot(off, off);
                 float dist = sqrtf(dist2);
@@ -284,11 +346,11 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                 float sc = fmaxf(dot(nrm, ldir), 0.0f);
                 float lc = emitter_cosine(e, ldir);
                 if (sc > 0.0f && lc > 1e-6f) {
-                  float eff_pdf = e.dist.y * dist2 / fmaxf(lc * e.emission_area.w, 1e-6f) * p_area;
+                  float eff_pdf = e.a_pdf.w * dist2 / fmaxf(lc * e.e1_area.w, 1e-6f) * p_area;
                   float bsdf_pdf = pbr_pdf(m, nrm, view, ldir);
                   float mis = power_heuristic(eff_pdf, bsdf_pdf);
                   float3 f = pbr_eval(m, nrm, view, ldir);
-                  float3 c = tp * f * f3(e.emission_area) * (sc * mis / fmaxf(eff_pdf, 1e-6f));
+                  float3 c = tp * f * f3(e.emission) * (sc * mis / fmaxf(eff_pdf, 1e-6f));
                   if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
                     sh_o = p + nrm * 0.002f;
                     sh_d = ldir;
@@ -447,7 +509,9 @@ __global__ void __launch_bounds__(128) k_trace_rays(SceneView s, uint32_t n, con
     float3 d = f3(dirs[3ull * i], dirs[3ull * i + 1], dirs[3ull * i + 2]);
     HitResult hr;
     bool hit = olc_traverse<STACK, false>(s, o, d, t_min, CUDART_INF_F, hr, smem_stack, err);
-    if (inst_id) inst_id[i] = hit ? s.instances[hr.instance].instance_id : 0xffffffffu;
+    if (inst_id)
+      inst_id[i] = hit ? s.instances[owner_instance(s.instances, s.tri_owner, hr.instance, hr.slot)].instance_id
+                       : 0xffffffffu;
     if (prim) prim[i] = hit ? (int32_t)hr.packed : -1;
     if (tout) tout[i] = hit ? hr.t : CUDART_INF_F;
     if (bary) {
@@ -499,7 +563,10 @@ void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQu
                           Counters* cnt, uint32_t bounce, cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
-    k_trace_closest<D><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
+    if (ls.scheduler == 1)
+      k_trace_closest<D, 1><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
+    else
+      k_trace_closest<D, 0><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
   });
   OLC_LAUNCH_CHECK("k_trace_closest");
 }
@@ -508,7 +575,10 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
                          Counters* cnt, uint32_t bounce, cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
-    k_trace_shadow<D><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
+    if (ls.scheduler == 1)
+      k_trace_shadow<D, 1><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
+    else
+      k_trace_shadow<D, 0><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
   });
   OLC_LAUNCH_CHECK("k_trace_shadow");
 }
@@ -587,12 +657,18 @@ void configure_trace_kernels() {
   // needs (default limit is 48 KB per block; ours stay below it, but the
   // preferred carve-out lets more blocks share one SM).
   auto prefer = [](const void* fn) { cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100); };
-  prefer((const void*)k_trace_closest<16>);
-  prefer((const void*)k_trace_closest<24>);
-  prefer((const void*)k_trace_closest<32>);
-  prefer((const void*)k_trace_shadow<16>);
-  prefer((const void*)k_trace_shadow<24>);
-  prefer((const void*)k_trace_shadow<32>);
+  prefer((const void*)k_trace_closest<16, 0>);
+  prefer((const void*)k_trace_closest<24, 0>);
+  prefer((const void*)k_trace_closest<32, 0>);
+  prefer((const void*)k_trace_shadow<16, 0>);
+  prefer((const void*)k_trace_shadow<24, 0>);
+  prefer((const void*)k_trace_shadow<32, 0>);
+  prefer((const void*)k_trace_closest<16, 1>);
+  prefer((const void*)k_trace_closest<24, 1>);
+  prefer((const void*)k_trace_closest<32, 1>);
+  prefer((const void*)k_trace_shadow<16, 1>);
+  prefer((const void*)k_trace_shadow<24, 1>);
+  prefer((const void*)k_trace_shadow<32, 1>);
 }
 
 }  // namespace olc

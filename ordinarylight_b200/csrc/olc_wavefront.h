@@ -48,6 +48,7 @@ struct LaunchShape {
   uint32_t grid_trace = 148 * 8;
   uint32_t grid_shade = 148 * 8;
   uint32_t stack_depth = 24;
+  uint32_t scheduler = 0;      // traversal scheduling (olc_config.trace_scheduler)
 };
 
 struct ProductPtrs {

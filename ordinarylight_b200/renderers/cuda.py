@@ -63,6 +63,8 @@ class CudaRendererConfig:
     stack_depth: int = 24
     chunk_paths: int = 0
     use_graphs: bool = True
+    flatten_instances: bool = True
+    trace_scheduler: str = "refill"
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -93,6 +95,8 @@ class CudaRendererConfig:
             raise ValueError("block_size must be a multiple of 32 in [64, 1024]")
         if int(self.chunk_paths) < 0:
             raise ValueError("chunk_paths cannot be negative")
+        if self.trace_scheduler not in ("refill", "batch"):
+            raise ValueError("trace_scheduler must be 'refill' or 'batch'")
 
     def native(self) -> _native.OlcConfig:
         c = _native.OlcConfig()
@@ -113,6 +117,8 @@ class CudaRendererConfig:
         c.stack_depth = int(self.stack_depth)
         c.chunk_paths = int(self.chunk_paths)
         c.use_graphs = int(bool(self.use_graphs))
+        c.flatten_instances = int(bool(self.flatten_instances))
+        c.trace_scheduler = 0 if self.trace_scheduler == "refill" else 1
         return c
 
 

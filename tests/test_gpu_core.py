@@ -153,3 +153,23 @@ def _basis(camera):
     from ordinarylight_b200.packing import camera_basis
 
     return camera_basis(camera)
+
+
+def test_flattened_small_instances_hit_the_same_primitives(native_library, cuda_device, golden):
+    """Baking small instances into one world-space mesh changes no primary-hit
+    ID (beyond t-ties) and reports the original instance IDs."""
+    from ordinarylight_b200 import CudaWavefrontRenderer
+
+    data = golden("spheres_small.npz")
+    scene, _camera = scenes.instanced_spheres(seed=5, instances=2, segments=16, bands=9, emitters=4, extent=3.0)
+    results = []
+    for flatten in (True, False):
+        with CudaWavefrontRenderer(mode="reference_compatible", flatten_instances=flatten) as r:
+            results.append(r.trace_closest(scene, data["origins"], data["directions"], t_min=1e-4))
+            assert r.validate_bvh(scene) == 0
+    for inst, prim, t, _ in results:
+        mismatches, _ties, tie_ok = _classify(prim, t, data["triangle"], data["t"])
+        assert mismatches == tie_ok
+        ids = scene.triangle_instance_ids()
+        ok = prim >= 0
+        np.testing.assert_array_equal(inst[ok], ids[prim[ok]])
