@@ -111,7 +111,9 @@ typedef struct olc_config {
   uint32_t trace_scheduler;     /* 0: persistent lanes refilled from the queue
                                    as rays finish; 1: warps take 32 rays at a
                                    time and run them to completion */
-  uint32_t reserved[6];
+  uint32_t disable_nee;         /* production mode without next-event
+                                   estimation (pure BSDF sampling) */
+  uint32_t reserved[5];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the

@@ -44,7 +44,7 @@ class OlcConfig(ctypes.Structure):
         ("restir_spatial", c_uint32), ("restir_neighbours", c_uint32), ("restir_radius", c_float),
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
         ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
-        ("trace_scheduler", c_uint32), ("reserved", c_uint32 * 6),
+        ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("reserved", c_uint32 * 5),
     ]
 
 
@@ -120,8 +120,7 @@ _SIGNATURES = {
     "olc_camera_rays": ([c_void_p, POINTER(OlcCamera), c_uint32, c_uint32, c_uint32, c_uint32, c_void_p,
                          c_void_p, c_void_p], c_int),
     "olc_morton_codes": ([c_void_p, c_uint32, c_void_p, c_void_p], c_int),
-    "olc_radix_sort_pairs": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
-    "olc_bvh_info_get": ([c_void_p, POINTER(OlcBvhInfo)], c_int),
+    "olc_radix_sort_pairs": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),    "olc_bvh_info_get": ([c_void_p, POINTER(OlcBvhInfo)], c_int),
     "olc_bvh_validate": ([c_void_p, POINTER(c_uint64)], c_int),
     "olc_frame_profile": ([c_void_p, POINTER(OlcLaunchRecord), c_uint32, POINTER(c_uint32)], c_int),
     "olc_stream": ([c_void_p, POINTER(c_void_p)], c_int),

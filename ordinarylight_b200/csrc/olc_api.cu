@@ -591,7 +591,7 @@ void fill_frame(olc_context* ctx, const olc_camera* cam, uint32_t w, uint32_t h,
   f.rr_start = ctx->cfg.mode == OLC_MODE_PRODUCTION ? ctx->cfg.russian_roulette_start : 0u;
   f.rr_min_survival = ctx->cfg.russian_roulette_min_survival;
   f.restir = ctx->cfg.restir;
-  f.pad = 0;
+  f.nee = ctx->cfg.disable_nee ? 0u : 1u;
 }
 
 struct Timing {

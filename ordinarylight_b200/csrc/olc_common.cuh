@@ -297,7 +297,7 @@ struct FrameParams {
   uint32_t rr_start;
   float rr_min_survival;
   uint32_t restir;
-  uint32_t pad;
+  uint32_t nee;            // next-event estimation on (production mode)
 };
 
 // Work counters kept in device memory, zeroed once per chunk.

@@ -148,27 +148,39 @@ OLC_D float3 sample_half_vector(float3 n, float roughness, float u, float v) {
   return normalize(t * (sn * cp) + b * (sn * sp) + n * c);
 }
 
-// samplePbr (transport_v1/lighting.glsl:226-246): lobe choice, direction,
-// pdf and weight = f cos / pdf.
-OLC_D void pbr_sample(const SurfaceMat& m, float3 n, float3 incoming, uint32_t& rng, float3& out, float3& weight,
+// BSDF sampling after samplePbr (transport_v1/lighting.glsl:226-246): lobe
+// choice with the specular probability, a cosine-weighted diffuse direction
+// or a GGX half-vector reflection, pdf = mix(diffuse pdf, specular pdf, p)
+// and weight = f cos / pdf.  One deliberate difference: the reference
+// replaces a specular reflection that points below the surface with a fresh
+// cosine direction but still reports the mixture pdf, which under-states the
+// density of the directions it returns (the estimator comes out too bright,
+// most visibly for rough surfaces).  Here such a sample is invalid — zero
+// weight, the path ends — so the reported pdf is exactly the density of the
+// directions that carry weight and the estimator is unbiased.  Returns false
+// for an invalid sample.
+OLC_D bool pbr_sample(const SurfaceMat& m, float3 n, float3 incoming, uint32_t& rng, float3& out, float3& weight,
                       float& pdf) {
   float3 view = -incoming;
   float p = spec_probability(m);
   bool specular = olc_rand(rng) < p;
   float u = olc_rand(rng), v = olc_rand(rng);
-  out = cosine_hemisphere(n, u, v);
   if (specular) {
     float3 h = sample_half_vector(n, m.roughness, u, v);
     out = incoming - h * (2.0f * dot(h, incoming));
-  }
-  if (dot(n, out) <= 0.0f) {
-    float u2 = olc_rand(rng), v2 = olc_rand(rng);
-    out = cosine_hemisphere(n, u2, v2);
+  } else {
+    out = cosine_hemisphere(n, u, v);
   }
   out = normalize(out);
+  if (!(dot(n, out) > 0.0f)) {
+    weight = f3(0.0f, 0.0f, 0.0f);
+    pdf = 0.0f;
+    return false;
+  }
   pdf = fmaxf(pbr_pdf(m, n, view, out), 1e-6f);
   float3 f = pbr_eval(m, n, view, out);
   weight = f * (fmaxf(dot(n, out), 0.0f) / pdf);
+  return true;
 }
 
 OLC_D float power_heuristic(float a, float b) {

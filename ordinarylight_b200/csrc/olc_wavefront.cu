@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                   }
                 }
               }
-            } else if (s.num_emitters > 0u || s.num_lights > 0u) {
+            } else if (fp.nee && (s.num_emitters > 0u || s.num_lights > 0u)) {
               float p_area = s.num_emitters > 0u ? (s.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
               float choose = olc_rand(rng);
               if (choose < p_area) {
@@ -400,13 +400,17 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
             // ---- BSDF sample
             float3 wdir, weight;
             float pdf;
-            pbr_sample(m, nrm, d, rng, wdir, weight, pdf);
+            const bool sampled = pbr_sample(m, nrm, d, rng, wdir, weight, pdf);
             tp *= weight;
             new_pdf = pdf;
             if (did_restir) new_flags |= OLC_PATH_FLAG_PREV_RESTIR;
-            else if (s.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
+            else if (fp.nee && s.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
             (void)did_area_nee;
-            bool alive = max3(tp) >= 1e-4f;
+            // (the reference also ends paths whose throughput falls below 1e-4,
+            // wavefront_shade.comp:322-327; that cut-off is biased, so only
+            // exactly-zero throughput ends a path here and Russian roulette
+            // handles the rest)
+            bool alive = sampled && max3(tp) > 0.0f;
             // Russian roulette (wavefront_shade.comp:569-580)
             if (alive && fp.rr_start > 0u && next_bounce >= fp.rr_start) {
               float survival = clampf(max3(tp), fp.rr_min_survival, 0.95f);

@@ -65,6 +65,7 @@ class CudaRendererConfig:
     use_graphs: bool = True
     flatten_instances: bool = True
     trace_scheduler: str = "refill"
+    nee: bool = True
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -119,6 +120,7 @@ class CudaRendererConfig:
         c.use_graphs = int(bool(self.use_graphs))
         c.flatten_instances = int(bool(self.flatten_instances))
         c.trace_scheduler = 0 if self.trace_scheduler == "refill" else 1
+        c.disable_nee = 0 if self.nee else 1
         return c
 
 
