@@ -321,6 +321,22 @@ OLC_API int olc_morton_codes(olc_context* ctx, uint32_t n, const float* tri_vert
 OLC_API int olc_radix_sort_pairs(olc_context* ctx, uint32_t n, uint32_t key_bits,
                          uint32_t* keys, uint32_t* values);
 
+/* Allocation-free variant of olc_radix_sort_pairs, for callers that must not
+ * allocate device memory when they sort: code running while a stream is
+ * captured into a CUDA graph, serving loops held to a fixed memory budget,
+ * and hosts whose device allocator belongs to another runtime.  It needs no
+ * context and calls no allocator: its scratch is one file-scope device array
+ * of the library (about 8.5 MB per device that loads the library, held until
+ * the process exits).  Limit: n <= 1048576 pairs per call (larger n returns
+ * OLC_ERR_VALUE).  Asynchronous on `stream` (a cudaStream_t; NULL is the
+ * default stream); message of a failure from olc_last_error(NULL).  The first
+ * call on a device looks up the array's device address and should come before
+ * any stream capture on that device.  All calls on a device share the array,
+ * so calls whose device work overlaps race: order them on one stream.
+ * This entry point has no counterpart in the reference. */
+OLC_API int olc_radix_sort_pairs_noalloc(uint32_t n, uint32_t key_bits, uint32_t* keys, uint32_t* values,
+                                         void* stream);
+
 /* Statistics of the resident acceleration structure (host outputs). */
 typedef struct olc_bvh_info {
   uint32_t blas_count;

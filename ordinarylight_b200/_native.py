@@ -120,7 +120,9 @@ _SIGNATURES = {
     "olc_camera_rays": ([c_void_p, POINTER(OlcCamera), c_uint32, c_uint32, c_uint32, c_uint32, c_void_p,
                          c_void_p, c_void_p], c_int),
     "olc_morton_codes": ([c_void_p, c_uint32, c_void_p, c_void_p], c_int),
-    "olc_radix_sort_pairs": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),    "olc_bvh_info_get": ([c_void_p, POINTER(OlcBvhInfo)], c_int),
+    "olc_radix_sort_pairs": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
+    "olc_radix_sort_pairs_noalloc": ([c_uint32, c_uint32, c_void_p, c_void_p, c_void_p], c_int),
+    "olc_bvh_info_get": ([c_void_p, POINTER(OlcBvhInfo)], c_int),
     "olc_bvh_validate": ([c_void_p, POINTER(c_uint64)], c_int),
     "olc_frame_profile": ([c_void_p, POINTER(OlcLaunchRecord), c_uint32, POINTER(c_uint32)], c_int),
     "olc_stream": ([c_void_p, POINTER(c_void_p)], c_int),

@@ -672,6 +672,10 @@ uint32_t choose_capacity(olc_context* ctx, uint32_t npix, uint32_t spp) {
 
 }  // namespace
 
+namespace olc {
+void set_thread_error(const std::string& message) { g_thread_error = message; }
+}  // namespace olc
+
 extern "C" {
 
 int olc_abi_version(void) { return OLC_ABI_VERSION; }

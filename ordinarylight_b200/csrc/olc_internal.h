@@ -20,6 +20,9 @@ struct Error : std::runtime_error {
   Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
 };
 
+// Message returned by olc_last_error(NULL) on this thread.
+void set_thread_error(const std::string& message);
+
 inline void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
     int code = (e == cudaErrorMemoryAllocation) ? 5 /*OLC_ERR_MEMORY*/ : 4 /*OLC_ERR_CUDA*/;
