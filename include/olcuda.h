@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OLC_ABI_VERSION 1
+#define OLC_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define OLC_API __attribute__((visibility("default")))
@@ -113,7 +113,9 @@ typedef struct olc_config {
                                    time and run them to completion */
   uint32_t disable_nee;         /* production mode without next-event
                                    estimation (pure BSDF sampling) */
-  uint32_t reserved[5];
+  uint32_t trace_block;         /* threads per block of the traversal and
+                                   shading kernels: 64, 128 or 256; 0 = 128 */
+  uint32_t reserved[4];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the
@@ -226,6 +228,104 @@ OLC_API int olc_upload_scene(olc_context* ctx, const olc_scene_desc* scene);
 
 /* Device bytes held by the resident scene (for HBM admission). */
 OLC_API int olc_scene_bytes(const olc_context* ctx, uint64_t* bytes);
+
+/* ---- scene pool: several resident scenes ------------------------------ */
+
+/* All resident scenes share one device pool (nodes, triangle slots,
+ * instances, materials, emitters, lights), so one wavefront can mix rays of
+ * different scenes.  olc_upload_scene replaces the context's default scene;
+ * olc_add_scene makes an additional scene resident and returns its handle,
+ * the way the reference keeps a scene resident across frames keyed by
+ * Scene.revision (upload_window_scene, ordinarylight/targets/vulkan/core.py:4574-4634;
+ * replace_scene, ordinarylight/targets/vulkan/api.py:913-917).
+ * Transactional: on failure nothing becomes resident. */
+OLC_API int olc_add_scene(olc_context* ctx, const olc_scene_desc* scene, uint32_t* handle);
+
+/* Release a scene added by olc_add_scene.  Its pool ranges are reused by
+ * later scenes.  Queued jobs that render it must have completed. */
+OLC_API int olc_remove_scene(olc_context* ctx, uint32_t handle);
+
+/* Statistics of one resident scene (handle from olc_add_scene). */
+typedef struct olc_scene_stats {
+  uint64_t bytes;            /* device bytes of the scene's data and hierarchy */
+  uint32_t triangles;
+  uint32_t blas_count;
+  uint32_t blas_nodes;
+  uint32_t tlas_nodes;
+  uint32_t flattened_instances;
+  uint32_t reserved;
+  double build_ms;
+} olc_scene_stats;
+OLC_API int olc_scene_stats_get(const olc_context* ctx, uint32_t handle, olc_scene_stats* stats);
+
+/* Device memory of the context, for admission by an HBM budget. */
+typedef struct olc_pool_info {
+  uint32_t resident_scenes;
+  uint32_t queued_jobs;       /* served jobs not yet completed */
+  uint64_t scene_bytes;       /* bytes the resident scenes use */
+  uint64_t pool_bytes;        /* bytes the scene pool has allocated (capacity) */
+  uint64_t wavefront_bytes;   /* queues, path state, reservoirs */
+  uint64_t pixel_bytes;       /* allocated accumulator/output arena */
+  uint64_t pixel_bytes_used;  /* arena bytes held by queued jobs */
+  uint64_t reserved[3];
+} olc_pool_info;
+OLC_API int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info);
+
+/* ---- batched and served rendering ------------------------------------- */
+
+/* One render job.  Its random numbers are keyed exactly as olc_render's
+ * (pixel, sample, bounce, seed + frame_index), so a job renders the same
+ * bits alone, in a batch or among served requests, and the same bits as
+ * olc_render of the same scene, camera, size, samples and frame when that
+ * frame uses no temporal history (first frame or after olc_reset_history). */
+typedef struct olc_job {
+  uint32_t scene;               /* handle from olc_add_scene */
+  uint32_t width, height;
+  uint32_t samples_per_pixel;   /* 1..65536 */
+  uint32_t frame_index;
+  uint32_t max_bounces;         /* 0: the context's max_bounces; else 1..64 */
+  uint32_t reserved[2];
+  olc_camera camera;
+  float* out_rgba;              /* (height, width, 4) float32, host or device */
+  int32_t out_is_device;
+  uint32_t reserved2;
+} olc_job;
+
+/* Render num_jobs jobs as one wavefront: every chunk of paths may hold
+ * paths of several jobs and scenes, sharing the ray queues, and the chunk
+ * sequence is replayed from a CUDA graph when the same mix recurs.  Returns
+ * when every output is written.  Replaces rendering the jobs one at a time
+ * through Renderer.render_async (ordinarylight/renderer/_core.py:614-651,
+ * which serialises submissions on one worker). */
+OLC_API int olc_render_batch(olc_context* ctx, const olc_job* jobs, uint32_t num_jobs,
+                             olc_render_stats* stats);
+
+/* Serving: queue a job (continuous batching).  Validates the job, reserves
+ * its accumulator pixels and returns a ticket; the job's paths join the
+ * shared wavefront at the next olc_serve_step.  job->out_rgba must stay
+ * valid until the ticket is reported complete. */
+OLC_API int olc_submit(olc_context* ctx, const olc_job* job, uint64_t* ticket);
+
+/* Run one chunk (at most chunk_paths paths) drawn from the queued jobs,
+ * shortest remaining work first (a job passed over for 8 steps goes first),
+ * then resolve and copy out the jobs whose last paths were in it.  done (host, capacity done_capacity) receives their tickets
+ * and num_done their count; stats (may be NULL) the chunk's statistics.
+ * Jobs submitted between steps join the next chunk. */
+OLC_API int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity,
+                           uint32_t* num_done, olc_render_stats* stats);
+
+/* Drop a queued job; its partial samples are discarded (RenderJob.cancel,
+ * ordinarylight/renderer/_core.py:614-651). */
+OLC_API int olc_cancel(olc_context* ctx, uint64_t ticket);
+
+/* Tickets of the queued jobs in submission order (tickets may be NULL to
+ * query the count).  After an olc_serve_step failure the jobs of the failed
+ * chunk are no longer queued; this tells the caller which ones remain. */
+OLC_API int olc_queued_jobs(const olc_context* ctx, uint64_t* tickets, uint32_t capacity, uint32_t* count);
+
+/* Device bytes a job needs while queued (accumulator and output pixels),
+ * for admission by an HBM budget. */
+OLC_API int olc_job_bytes(const olc_context* ctx, const olc_job* job, uint64_t* bytes);
 
 /* ---- rendering ------------------------------------------------------- */
 

@@ -44,7 +44,8 @@ class OlcConfig(ctypes.Structure):
         ("restir_spatial", c_uint32), ("restir_neighbours", c_uint32), ("restir_radius", c_float),
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
         ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
-        ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("reserved", c_uint32 * 5),
+        ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("trace_block", c_uint32),
+        ("reserved", c_uint32 * 4),
     ]
 
 
@@ -97,6 +98,29 @@ class OlcLaunchRecord(ctypes.Structure):
     ]
 
 
+class OlcSceneStats(ctypes.Structure):
+    _fields_ = [
+        ("bytes", c_uint64), ("triangles", c_uint32), ("blas_count", c_uint32), ("blas_nodes", c_uint32),
+        ("tlas_nodes", c_uint32), ("flattened_instances", c_uint32), ("reserved", c_uint32), ("build_ms", c_double),
+    ]
+
+
+class OlcPoolInfo(ctypes.Structure):
+    _fields_ = [
+        ("resident_scenes", c_uint32), ("queued_jobs", c_uint32), ("scene_bytes", c_uint64),
+        ("pool_bytes", c_uint64), ("wavefront_bytes", c_uint64), ("pixel_bytes", c_uint64),
+        ("pixel_bytes_used", c_uint64), ("reserved", c_uint64 * 3),
+    ]
+
+
+class OlcJob(ctypes.Structure):
+    _fields_ = [
+        ("scene", c_uint32), ("width", c_uint32), ("height", c_uint32), ("samples_per_pixel", c_uint32),
+        ("frame_index", c_uint32), ("max_bounces", c_uint32), ("reserved", c_uint32 * 2),
+        ("camera", OlcCamera), ("out_rgba", c_void_p), ("out_is_device", c_int32), ("reserved2", c_uint32),
+    ]
+
+
 STAGE_NAMES = ("raygen", "trace_closest", "restir", "shade", "trace_shadow", "accumulate", "resolve")
 
 
@@ -110,6 +134,16 @@ _SIGNATURES = {
     "olc_reconfigure": ([c_void_p, POINTER(OlcConfig)], c_int),
     "olc_upload_scene": ([c_void_p, POINTER(OlcSceneDesc)], c_int),
     "olc_scene_bytes": ([c_void_p, POINTER(c_uint64)], c_int),
+    "olc_add_scene": ([c_void_p, POINTER(OlcSceneDesc), POINTER(c_uint32)], c_int),
+    "olc_remove_scene": ([c_void_p, c_uint32], c_int),
+    "olc_scene_stats_get": ([c_void_p, c_uint32, POINTER(OlcSceneStats)], c_int),
+    "olc_pool_info_get": ([c_void_p, POINTER(OlcPoolInfo)], c_int),
+    "olc_render_batch": ([c_void_p, POINTER(OlcJob), c_uint32, POINTER(OlcRenderStats)], c_int),
+    "olc_submit": ([c_void_p, POINTER(OlcJob), POINTER(c_uint64)], c_int),
+    "olc_serve_step": ([c_void_p, POINTER(c_uint64), c_uint32, POINTER(c_uint32), POINTER(OlcRenderStats)], c_int),
+    "olc_cancel": ([c_void_p, c_uint64], c_int),
+    "olc_queued_jobs": ([c_void_p, POINTER(c_uint64), c_uint32, POINTER(c_uint32)], c_int),
+    "olc_job_bytes": ([c_void_p, POINTER(OlcJob), POINTER(c_uint64)], c_int),
     "olc_render": ([c_void_p, POINTER(OlcCamera), c_uint32, c_uint32, c_uint32, c_uint32, c_void_p, c_int,
                     POINTER(OlcRenderStats)], c_int),
     "olc_read_products": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),

@@ -1,22 +1,33 @@
-// C ABI of libolcuda: context, scene residency, the wavefront frame driver.
+// C ABI of libolcuda: context, the resident scene pool, and the chunked
+// wavefront executor that plain frames, batches and served requests share.
 //
-// A frame is processed as chunks of at most `capacity` paths.  Path linear
-// index = sample * npix + pixel (sample-major), so a chunk that spans whole
-// sample streams keeps every pixel of a stream resident together (ReSTIR's
-// spatial pass needs that).  Per chunk: raygen, then per bounce
-// trace_closest -> [ReSTIR at bounce 0] -> shade -> trace_shadow, then
-// accumulate.  With use_graphs the whole frame is captured once per
-// (width, height, spp) and replayed; per-frame parameters live in device
-// memory and are refreshed by one host->device copy before each replay.
+// Work is organised in jobs (one image of one scene) and chunks (at most
+// `capacity` paths resident at once).  A job's path has the job-local index
+// sample * npix + pixel.  A chunk is a list of segments, each a contiguous
+// run of one job's paths, so one chunk can hold paths of many jobs and
+// scenes.  Segments of ReSTIR jobs hold whole sample streams, because
+// spatial reuse reads the stream's neighbouring pixels.  Per chunk: raygen,
+// then per bounce trace_closest -> [ReSTIR at bounce 0] -> shade ->
+// trace_shadow, then accumulate into the job's pixels in fixed point (order
+// independent), so the bits of a job do not depend on how its paths are
+// chunked or mixed with other jobs.
+//
+// A run is a sequence of chunks planned on the host.  All chunk tables reach
+// the device in one copy, and the run's launches are captured into a CUDA
+// graph keyed by the run's signature (each chunk's bounce count and ReSTIR
+// flag plus every buffer address the launches see); later runs with the same
+// signature replay it.  A plain frame is one run over one job, a batch one
+// run over all its jobs, a serving step one run of one chunk over the queued
+// jobs (continuous batching: jobs submitted between steps join the next
+// chunk).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
-#include <mutex>
 #include <string>
-#include <tuple>
 #include <vector>
 
 #include "olcuda.h"
@@ -30,33 +41,175 @@ namespace {
 
 thread_local std::string g_thread_error;
 
-// Instances of meshes with at most this many triangles are baked into one
-// world-space mesh at upload, up to kFlattenMaxTotal baked triangles.
+// Instances of meshes with at most this many triangles are baked into
+// world-space triangles referenced by the TLAS, up to kFlattenMaxTotal baked
+// triangles per scene.
 constexpr uint32_t kFlattenMaxTriangles = 64;
 constexpr uint64_t kFlattenMaxTotal = 1ull << 24;
+constexpr size_t kMaxGraphs = 16;
+constexpr uint64_t kDefaultChunkPaths = 1ull << 24;
+constexpr uint32_t kNoScene = 0xffffffffu;
+constexpr uint32_t kMaxWaitSteps = 8;
 
-struct ScenePack {
-  DeviceBuffer nodes, tri_verts, tri_normals, tri_index, instances, o2w, materials, material_aux, emitters,
-      emitter_alias, lights,
-      env_image, volume;
-  SceneView view{};
-  uint32_t total_triangles = 0;
-  uint32_t blas_nodes = 0, tlas_nodes = 0, blas_count = 0;
+// First-fit allocator of element ranges in [0, capacity).
+class RangeAllocator {
+ public:
+  bool allocate(uint64_t n, uint64_t& off) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      off = it->first;
+      const uint64_t rest = it->second - n;
+      free_.erase(it);
+      if (rest) free_.emplace(off + n, rest);
+      used_ += n;
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t n) {
+    if (n == 0) return;
+    used_ -= n;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  void grow(uint64_t new_capacity) {
+    if (new_capacity <= capacity_) return;
+    const uint64_t old = capacity_;
+    capacity_ = new_capacity;
+    used_ += new_capacity - old;  // release() below takes it off again
+    release(old, new_capacity - old);
+  }
+  // Free elements at the end of the range (a growth extends them).
+  uint64_t tail_free() const {
+    if (free_.empty()) return 0;
+    auto last = std::prev(free_.end());
+    return last->first + last->second == capacity_ ? last->second : 0;
+  }
+  uint64_t capacity() const { return capacity_; }
+  uint64_t used() const { return used_; }
+
+ private:
+  std::map<uint64_t, uint64_t> free_;  // offset -> size
+  uint64_t capacity_ = 0, used_ = 0;
+};
+
+struct Range {
+  uint64_t off = 0, n = 0;
+};
+
+// Device arrays indexed by one range allocator (for example the four
+// per-slot triangle arrays).  Growing copies the old contents into the new
+// allocation, so indices held by resident scenes and queued jobs stay valid;
+// only base addresses change.
+struct PoolGroup {
+  std::vector<size_t> elem;  // bytes per element of each array
+  std::vector<DeviceBuffer> bufs;
+  RangeAllocator ranges;
+  uint32_t min_capacity = 1024;
+
+  PoolGroup(std::initializer_list<size_t> sizes, uint32_t min_cap) : elem(sizes), bufs(sizes.size()),
+                                                                      min_capacity(min_cap) {}
+
+  Range acquire(uint64_t n, cudaStream_t st) {
+    Range r;
+    r.n = n;
+    if (n == 0) return r;
+    if (ranges.allocate(n, r.off)) return r;
+    const uint64_t cap = ranges.capacity();
+    const uint64_t need = cap + n - ranges.tail_free();
+    const uint64_t new_cap = std::max<uint64_t>({need, cap + cap / 2, (uint64_t)min_capacity});
+    for (size_t k = 0; k < bufs.size(); ++k) {
+      DeviceBuffer nb(new_cap * elem[k]);
+      if (cap)
+        OLC_CUDA(cudaMemcpyAsync(nb.get(), bufs[k].get(), cap * elem[k], cudaMemcpyDeviceToDevice, st));
+      OLC_CUDA(cudaStreamSynchronize(st));
+      bufs[k] = std::move(nb);
+    }
+    ranges.grow(new_cap);
+    if (!ranges.allocate(n, r.off)) throw Error(OLC_ERR_RUNTIME, "pool allocation failed after growth");
+    return r;
+  }
+  void release(Range& r) {
+    ranges.release(r.off, r.n);
+    r = Range{};
+  }
+  template <class T>
+  T* at(size_t k, uint64_t off = 0) const {
+    return reinterpret_cast<T*>(bufs[k].as<char>() + off * elem[k]);
+  }
+  uint64_t range_bytes(const Range& r) const {
+    uint64_t b = 0;
+    for (size_t e : elem) b += r.n * e;
+    return b;
+  }
+  uint64_t bytes() const {
+    uint64_t b = 0;
+    for (const DeviceBuffer& d : bufs) b += d.bytes();
+    return b;
+  }
+};
+
+// One resident scene: its ranges of the pool and its own image and volume.
+struct ResidentScene {
+  Range nodes, slots, instances, materials, emitters, lights;
+  DeviceBuffer env_image, volume;
+  SceneRec rec{};
+  std::vector<BlasRange> blas_ranges;
+  uint32_t triangles = 0, blas_count = 0, blas_nodes = 0, tlas_nodes = 0, flattened = 0;
   uint64_t bytes = 0;
   double build_ms = 0.0;
-  bool valid = false;
-  DeviceBuffer tri_owner;
-  std::vector<BlasRange> blas_ranges;
-  uint32_t flattened_instances = 0, tlas_instances = 0;
+};
+
+// A job waiting for (or in) the wavefront.
+struct QueuedJob {
+  uint64_t ticket = 0;
+  JobRec rec{};              // seg_* filled per segment
+  uint64_t total = 0;        // npix * spp
+  uint64_t issued = 0;       // paths handed to chunks
+  Range pixels;              // accumulator / output arena range
+  float* out = nullptr;
+  bool out_device = false;
+  // ReSTIR reservoirs at job-local indices (reservoir_base 0), where the next
+  // plain frame's temporal pass finds them; otherwise chunk-local ones
+  bool job_local_reservoirs = false;
+  uint32_t waited = 0;       // serving steps that issued none of its paths
+};
+
+struct ChunkPlan {
+  uint32_t count = 0;
+  uint32_t bounces = 0;
+  bool restir = false;
+  std::vector<JobRec> segs;
+};
+
+struct RunPlan {
+  std::vector<ChunkPlan> chunks;
+  std::vector<QueuedJob*> finished;  // jobs whose last paths are in this run
+  uint32_t max_segments = 0;
+  uint32_t max_count = 0;
+  bool restir = false;               // some chunk runs ReSTIR
+  bool chunk_reservoirs = false;     // some ReSTIR segment uses chunk-local reservoirs
 };
 
 struct TimelineEntry {
   uint32_t stage, bounce, chunk;
 };
 
-struct GraphKey {
-  uint32_t w, h, spp;
-  bool operator<(const GraphKey& o) const { return std::tie(w, h, spp) < std::tie(o.w, o.h, o.spp); }
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<TimelineEntry> timeline;
+  uint64_t last_used = 0;
 };
 
 }  // namespace
@@ -68,27 +221,46 @@ struct olc_context {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
   std::string error;
-  ScenePack scene;
   BuildScratch scratch;
   LaunchShape ls;
+  // scene pool
+  PoolGroup nodes{{sizeof(BvhNode)}, 4096};
+  PoolGroup slots{{3 * sizeof(float4), 3 * sizeof(float4), sizeof(uint32_t), sizeof(uint32_t)}, 4096};
+  PoolGroup instances{{sizeof(InstanceRec)}, 256};
+  PoolGroup materials{{sizeof(MaterialRec), sizeof(MaterialAux)}, 64};
+  PoolGroup emitters{{sizeof(EmitterRec), sizeof(AliasEntry)}, 256};
+  PoolGroup lights{{sizeof(LightRec)}, 16};
+  Range identity_instance;
+  std::vector<std::unique_ptr<ResidentScene>> scenes;  // index = handle
+  DeviceBuffer scene_table;                              // SceneRec per handle
+  uint32_t default_scene = kNoScene;
   // wavefront buffers
   uint32_t capacity = 0;
   DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp, ps_rad, ps_meta;
-  DeviceBuffer counters, fp_dev, accum, out_dev;
+  DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim;
-  uint32_t npix_capacity = 0;
-  FrameParams* fp_host = nullptr;     // pinned
+  uint32_t prod_pixels = 0;
+  PoolGroup pixels{{3 * sizeof(unsigned long long), sizeof(float4)}, 1 << 16};
+  // run tables: chunk headers + segments, then the resolve list
+  DeviceBuffer table_dev;
+  char* table_host = nullptr;  // pinned
+  size_t table_bytes = 0;
+  uint32_t seg_capacity = 64;
   Counters* counters_host = nullptr;  // pinned, one per chunk
   uint32_t counters_host_chunks = 0;
   RestirState restir;
-  std::map<GraphKey, cudaGraphExec_t> graphs;
-  std::map<GraphKey, std::vector<TimelineEntry>> graph_timelines;
+  std::map<std::vector<uint64_t>, GraphEntry> graphs;
+  uint64_t graph_clock = 0;
   // device timeline: events[k] .. events[k+1] brackets launch k
   std::vector<cudaEvent_t> tl_events;
   std::vector<TimelineEntry> tl_entries;
   bool capturing = false;
   std::vector<olc_launch_record> last_profile;
+  std::vector<uint32_t> last_chunk_counts;
   uint32_t last_w = 0, last_h = 0;
+  // served jobs in submission order
+  std::deque<std::unique_ptr<QueuedJob>> served;
+  uint64_t next_ticket = 1;
   bool closed = false;
 };
 
@@ -129,23 +301,28 @@ void validate_config(const olc_config& c) {
     throw Error(OLC_ERR_VALUE, "stack_depth must be 16, 24 or 32");
   if (c.block_size != 0 && (c.block_size < 64 || c.block_size > 1024 || (c.block_size & 31u)))
     throw Error(OLC_ERR_VALUE, "block_size must be a multiple of 32 in [64, 1024]");
+  if (c.trace_block != 0 && c.trace_block != 64 && c.trace_block != 128 && c.trace_block != 256)
+    throw Error(OLC_ERR_VALUE, "trace_block must be 64, 128 or 256");
   if (c.russian_roulette_min_survival < 0.0f || c.russian_roulette_min_survival > 1.0f)
     throw Error(OLC_ERR_VALUE, "russian_roulette_min_survival must be in [0, 1]");
 }
 
 void apply_launch_shape(olc_context* ctx) {
   ctx->ls.block = ctx->cfg.block_size ? ctx->cfg.block_size : 256;
+  // traversal and shading: 64, 128 or 256 threads; 1,536 threads per SM of
+  // grid keeps the persistent kernels' work cursors busy on every SM
+  const uint32_t tb = ctx->cfg.trace_block ? ctx->cfg.trace_block : 128;
+  ctx->ls.trace_block = tb;
   ctx->ls.stack_depth = ctx->cfg.stack_depth ? ctx->cfg.stack_depth : 24;
   ctx->ls.scheduler = ctx->cfg.trace_scheduler;
   ctx->ls.grid_simple = ctx->sm_count * 8;
-  ctx->ls.grid_shade = ctx->sm_count * 12;
-  ctx->ls.grid_trace = ctx->sm_count * 12;
+  ctx->ls.grid_shade = ctx->sm_count * (1536 / tb);
+  ctx->ls.grid_trace = ctx->sm_count * (1536 / tb);
 }
 
 void drop_graphs(olc_context* ctx) {
-  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   ctx->graphs.clear();
-  ctx->graph_timelines.clear();
 }
 
 void tl_record(olc_context* ctx, size_t index) {
@@ -204,10 +381,33 @@ void upload(DeviceBuffer& buf, const T* host, size_t count, cudaStream_t stream,
   bytes += b;
 }
 
+template <class T>
+void upload_to(T* dst, const T* host, size_t count, cudaStream_t stream) {
+  if (count) OLC_CUDA(cudaMemcpyAsync(dst, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+}
+
+SceneView pool_view(const olc_context* ctx) {
+  SceneView v{};
+  v.nodes = ctx->nodes.at<BvhNode>(0);
+  v.tri_verts = ctx->slots.at<float4>(0);
+  v.tri_normals = ctx->slots.at<float4>(1);
+  v.tri_index = ctx->slots.at<uint32_t>(2);
+  v.tri_owner = ctx->slots.at<uint32_t>(3);
+  v.instances = ctx->instances.at<InstanceRec>(0);
+  v.materials = ctx->materials.at<MaterialRec>(0);
+  v.material_aux = ctx->materials.at<MaterialAux>(1);
+  v.emitters = ctx->emitters.at<EmitterRec>(0);
+  v.emitter_alias = ctx->emitters.at<AliasEntry>(1);
+  v.lights = ctx->lights.at<LightRec>(0);
+  v.scenes = ctx->scene_table.as<SceneRec>();
+  return v;
+}
+
 // Emitter records for sampling from the reference layout (a, b, c, emission +
 // area, cdf/pdf/two-sided; Scene.emissive_triangle_data), plus a Vose alias
 // table over the pdfs (M. D. Vose, "A linear algorithm for generating random
-// numbers with a given distribution", IEEE TSE 1991).
+// numbers with a given distribution", IEEE TSE 1991).  Alias entries are
+// scene-local indices.
 void build_emitters(const olc_scene_desc* d, std::vector<EmitterRec>& em, std::vector<AliasEntry>& alias) {
   const uint32_t n = d->num_emitters;
   em.resize(n);
@@ -253,14 +453,34 @@ void build_emitters(const olc_scene_desc* d, std::vector<EmitterRec>& em, std::v
   for (uint32_t i : small) alias[i] = AliasEntry{1.0f, i};
 }
 
-void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
-  auto t0 = std::chrono::steady_clock::now();
-  cudaStream_t st = ctx->stream;
+void fill_instance(InstanceRec& r, const float* m) {
+  float w2o[12];
+  invert_affine(m, w2o);
+  r.w2o0 = make_float4(w2o[0], w2o[1], w2o[2], w2o[3]);
+  r.w2o1 = make_float4(w2o[4], w2o[5], w2o[6], w2o[7]);
+  r.w2o2 = make_float4(w2o[8], w2o[9], w2o[10], w2o[11]);
+  r.o2w0 = make_float4(m[0], m[1], m[2], m[3]);
+  r.o2w1 = make_float4(m[4], m[5], m[6], m[7]);
+  r.o2w2 = make_float4(m[8], m[9], m[10], m[11]);
+  r.flags = 0;
+  r.pad[0] = r.pad[1] = r.pad[2] = 0;
+}
+
+void release_scene_ranges(olc_context* ctx, ResidentScene& rs) {
+  ctx->nodes.release(rs.nodes);
+  ctx->slots.release(rs.slots);
+  ctx->instances.release(rs.instances);
+  ctx->materials.release(rs.materials);
+  ctx->emitters.release(rs.emitters);
+  ctx->lights.release(rs.lights);
+}
+
+void check_scene_desc(const olc_scene_desc* d) {
   if (!d) throw Error(OLC_ERR_VALUE, "scene description is null");
   const uint32_t nm = d->num_meshes, ni = d->num_instances;
   if (nm && (!d->mesh_vertex_offset || !d->mesh_triangle_offset))
     throw Error(OLC_ERR_VALUE, "mesh offsets are required");
-  uint32_t total_v = nm ? d->mesh_vertex_offset[nm] : 0, total_t = nm ? d->mesh_triangle_offset[nm] : 0;
+  uint32_t total_t = nm ? d->mesh_triangle_offset[nm] : 0;
   if (total_t >= (1u << 28)) throw Error(OLC_ERR_VALUE, "scene exceeds 2^28 triangles");
   for (uint32_t m = 0; m < nm; ++m) {
     if (d->mesh_vertex_offset[m + 1] < d->mesh_vertex_offset[m] ||
@@ -273,17 +493,27 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
   for (uint32_t i = 0; i < ni; ++i) {
     if (d->instance_mesh[i] >= nm) throw Error(OLC_ERR_VALUE, "instance refers to a missing mesh");
     if (d->instance_material[i] >= d->num_materials) throw Error(OLC_ERR_VALUE, "instance refers to a missing material");
+    const float* m = d->instance_object_to_world + 12ull * i;
+    for (int k = 0; k < 12; ++k)
+      if (!std::isfinite(m[k])) throw Error(OLC_ERR_VALUE, "instance transform must be finite");
   }
-  uint64_t bytes = 0;
-  // geometry staging (device copies of the host arrays)
-  DeviceBuffer dv, dn, di;
-  upload(dv, d->vertices, 3ull * total_v, st, bytes);
-  upload(dn, d->normals, 3ull * total_v, st, bytes);
-  upload(di, d->indices, 3ull * total_t, st, bytes);
-  bytes = 0;
-  // ---- instance flattening: instances of meshes with at most
-  // kFlattenMaxTriangles triangles are baked into one world-space mesh.
+  if (d->environment_kind > OLC_ENV_EQUIRECT) throw Error(OLC_ERR_VALUE, "unknown environment kind");
+  if (d->environment_kind == OLC_ENV_EQUIRECT &&
+      (!d->environment_image || d->environment_width == 0 || d->environment_height == 0))
+    throw Error(OLC_ERR_VALUE, "equirect environment needs an image");
+}
+
+// Build one scene into the pool.  Every range is acquired before any data is
+// written (a growth moves the arrays), and all of them are released again if
+// the build fails.
+void build_scene(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs) {
+  auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t st = ctx->stream;
+  check_scene_desc(d);
+  const uint32_t nm = d->num_meshes, ni = d->num_instances;
+  const uint32_t total_v = nm ? d->mesh_vertex_offset[nm] : 0, total_t = nm ? d->mesh_triangle_offset[nm] : 0;
   auto mesh_tris = [&](uint32_t m) { return d->mesh_triangle_offset[m + 1] - d->mesh_triangle_offset[m]; };
+  // ---- instance flattening
   std::vector<uint8_t> flat(ni, 0);
   uint64_t flat_tris = 0;
   uint32_t flat_count = 0;
@@ -300,275 +530,280 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ScenePack& sp) {
     flat_tris = 0;
     flat_count = 0;
   }
-  const bool flattening = flat_count > 0;
-  // internal instance order: TLAS members (instances kept as instances, then
-  // the flattened mesh's identity instance), then the flattened originals.
+  // scene-local instance order: TLAS members (instances kept as instances),
+  // then the baked originals (their records hold material and Mesh.id)
   std::vector<uint32_t> order;
   for (uint32_t i = 0; i < ni; ++i)
     if (!flat[i]) order.push_back(i);
-  const uint32_t pseudo = (uint32_t)order.size();
-  const uint32_t tlas_members = pseudo + (flattening ? 1u : 0u);
-  std::vector<uint32_t> internal_of(ni);
-  for (uint32_t k = 0; k < pseudo; ++k) internal_of[order[k]] = k;
+  const uint32_t members = (uint32_t)order.size();
+  std::vector<uint32_t> local_of(ni);
+  for (uint32_t k = 0; k < members; ++k) local_of[order[k]] = k;
   {
-    uint32_t k = tlas_members;
+    uint32_t k = members;
     for (uint32_t i = 0; i < ni; ++i)
-      if (flat[i]) internal_of[i] = k++;
+      if (flat[i]) local_of[i] = k++;
   }
-  const uint32_t n_records = tlas_members + flat_count;
-  // meshes that still need their own BLAS
   std::vector<uint8_t> mesh_used(nm, 0);
-  for (uint32_t k = 0; k < pseudo; ++k) mesh_used[d->instance_mesh[order[k]]] = 1;
-  // node pool: BLAS nodes, the flattened mesh, then TLAS nodes
-  std::vector<uint32_t> node_base(nm), blas_root(nm, 0);
-  uint32_t nodes_total = 0;
+  for (uint32_t k = 0; k < members; ++k) mesh_used[d->instance_mesh[order[k]]] = 1;
+  std::vector<uint32_t> node_local(nm, 0), blas_root(nm, 0);
+  uint32_t node_count = 0;
   for (uint32_t m = 0; m < nm; ++m) {
-    node_base[m] = nodes_total;
-    if (mesh_used[m]) nodes_total += blas_node_count(mesh_tris(m));
+    node_local[m] = node_count;
+    if (mesh_used[m]) node_count += blas_node_count(mesh_tris(m));
   }
-  uint32_t tlas_base = nodes_total;
-  const uint64_t tlas_prims = (uint64_t)pseudo + flat_tris;  // instances + direct triangles
-  uint32_t tlas_nodes = tlas_prims > 1 ? (uint32_t)(tlas_prims - 1) : 1;
-  nodes_total += tlas_nodes;
-  const uint64_t total_slots = (uint64_t)total_t + flat_tris;
-  if (total_slots >= (1ull << 28)) throw Error(OLC_ERR_VALUE, "scene exceeds 2^28 triangles");
-  sp.nodes.allocate((size_t)nodes_total * sizeof(BvhNode));
-  sp.tri_verts.allocate(std::max<size_t>(total_slots, 1) * 3 * sizeof(float4));
-  sp.tri_normals.allocate(std::max<size_t>(total_slots, 1) * 3 * sizeof(float4));
-  sp.tri_index.allocate(std::max<size_t>(total_slots, 1) * sizeof(uint32_t));
-  sp.tri_owner.allocate(std::max<size_t>(total_slots, 1) * sizeof(uint32_t));
-  OLC_CUDA(cudaMemsetAsync(sp.tri_owner.get(), 0, sp.tri_owner.bytes(), st));
-  bytes += sp.nodes.bytes() + sp.tri_verts.bytes() + sp.tri_normals.bytes() + sp.tri_index.bytes() +
-           sp.tri_owner.bytes();
-  sp.blas_ranges.clear();
-  for (uint32_t m = 0; m < nm; ++m) {
-    if (!mesh_used[m]) continue;
-    BlasDesc bd;
-    uint32_t v0 = d->mesh_vertex_offset[m], t0i = d->mesh_triangle_offset[m];
-    bd.vertices = dv.as<float>() + 3ull * v0;
-    bd.normals = dn.as<float>() + 3ull * v0;
-    bd.indices = di.as<uint32_t>() + 3ull * t0i;
-    bd.num_vertices = d->mesh_vertex_offset[m + 1] - v0;
-    bd.num_triangles = mesh_tris(m);
-    blas_root[m] = build_blas(bd, ctx->scratch, sp.nodes.as<BvhNode>(), node_base[m], sp.tri_verts.as<float4>(),
-                              sp.tri_normals.as<float4>(), sp.tri_index.as<uint32_t>(), t0i, 4, st);
-    sp.blas_ranges.push_back({blas_root[m], t0i, t0i + bd.num_triangles});
-  }
-  // instance records (internal order)
-  std::vector<InstanceRec> inst(n_records);
-  std::vector<float> o2w(12ull * std::max<uint32_t>(tlas_members, 1), 0.0f);
-  auto fill_record = [&](InstanceRec& r, const float* m) {
-    float w2o[12];
-    invert_affine(m, w2o);
-    r.w2o0 = make_float4(w2o[0], w2o[1], w2o[2], w2o[3]);
-    r.w2o1 = make_float4(w2o[4], w2o[5], w2o[6], w2o[7]);
-    r.w2o2 = make_float4(w2o[8], w2o[9], w2o[10], w2o[11]);
-    r.o2w0 = make_float4(m[0], m[1], m[2], m[3]);
-    r.o2w1 = make_float4(m[4], m[5], m[6], m[7]);
-    r.o2w2 = make_float4(m[8], m[9], m[10], m[11]);
-    r.flags = 0;
-    r.pad[0] = r.pad[1] = r.pad[2] = 0;
-  };
-  for (uint32_t i = 0; i < ni; ++i) {
-    const float* m = d->instance_object_to_world + 12ull * i;
-    for (int k = 0; k < 12; ++k)
-      if (!std::isfinite(m[k])) throw Error(OLC_ERR_VALUE, "instance transform must be finite");
-    const uint32_t k = internal_of[i];
-    InstanceRec& r = inst[k];
-    fill_record(r, m);
-    r.blas_root = blas_root[d->instance_mesh[i]];
-    r.material = d->instance_material[i];
-    r.prim_offset = d->instance_primitive_offset[i];
-    r.instance_id = d->instance_id[i];
-    if (k < tlas_members)
-      for (int c = 0; c < 12; ++c) o2w[12ull * k + c] = m[c];
-  }
-  if (flattening) {
-    // world-space triangles of the flattened instances, in packed order,
-    // written straight into their slots; the TLAS references them directly
+  const uint32_t tlas_local = node_count;
+  const uint64_t tlas_prims = (uint64_t)members + flat_tris;
+  const uint32_t tlas_nodes = tlas_prims > 1 ? (uint32_t)(tlas_prims - 1) : 1;
+  node_count += tlas_nodes;
+  const uint64_t slot_count = (uint64_t)total_t + flat_tris;
+
+  try {
+    // ---- pool ranges (acquire everything first)
+    rs.nodes = ctx->nodes.acquire(node_count, st);
+    rs.slots = ctx->slots.acquire(std::max<uint64_t>(slot_count, 1), st);
+    rs.instances = ctx->instances.acquire(ni, st);
+    rs.materials = ctx->materials.acquire(d->num_materials, st);
+    rs.emitters = ctx->emitters.acquire(d->num_emitters, st);
+    rs.lights = ctx->lights.acquire(d->num_lights, st);
+    if (rs.slots.off + rs.slots.n >= (1ull << 28)) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^28 triangle slots");
+    if (rs.instances.off + rs.instances.n >= (1ull << 28)) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^28 instances");
+    if (rs.nodes.off + rs.nodes.n >= 0x7fffffffull) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^31 nodes");
+    const uint32_t slot0 = (uint32_t)rs.slots.off, inst0 = (uint32_t)rs.instances.off;
+    const uint32_t node0 = (uint32_t)rs.nodes.off, mat0 = (uint32_t)rs.materials.off;
+    const uint32_t flat_slot0 = slot0 + total_t;
+    BvhNode* nodes = ctx->nodes.at<BvhNode>(0);
+    float4* tri_verts = ctx->slots.at<float4>(0);
+    float4* tri_normals = ctx->slots.at<float4>(1);
+    uint32_t* tri_index = ctx->slots.at<uint32_t>(2);
+    uint32_t* tri_owner = ctx->slots.at<uint32_t>(3);
+    OLC_CUDA(cudaMemsetAsync(tri_owner + slot0, 0, rs.slots.n * sizeof(uint32_t), st));
+
+    // ---- geometry staging and BLAS builds
+    uint64_t staging = 0;
+    DeviceBuffer dv, dn, di;
+    upload(dv, d->vertices, 3ull * total_v, st, staging);
+    upload(dn, d->normals, 3ull * total_v, st, staging);
+    upload(di, d->indices, 3ull * total_t, st, staging);
+    rs.blas_ranges.clear();
+    for (uint32_t m = 0; m < nm; ++m) {
+      if (!mesh_used[m]) continue;
+      BlasDesc bd;
+      uint32_t v0 = d->mesh_vertex_offset[m], t0i = d->mesh_triangle_offset[m];
+      bd.vertices = dv.as<float>() + 3ull * v0;
+      bd.normals = dn.as<float>() + 3ull * v0;
+      bd.indices = di.as<uint32_t>() + 3ull * t0i;
+      bd.num_vertices = d->mesh_vertex_offset[m + 1] - v0;
+      bd.num_triangles = mesh_tris(m);
+      blas_root[m] = build_blas(bd, ctx->scratch, nodes, node0 + node_local[m], tri_verts, tri_normals, tri_index,
+                                slot0 + t0i, 4, st);
+      rs.blas_ranges.push_back({blas_root[m], slot0 + t0i, slot0 + t0i + bd.num_triangles});
+    }
+
+    // ---- instance records (global indices)
+    std::vector<InstanceRec> inst(ni);
+    std::vector<float> o2w(12ull * std::max<uint32_t>(members, 1), 0.0f);
+    for (uint32_t i = 0; i < ni; ++i) {
+      const float* m = d->instance_object_to_world + 12ull * i;
+      const uint32_t k = local_of[i];
+      InstanceRec& r = inst[k];
+      fill_instance(r, m);
+      r.blas_root = blas_root[d->instance_mesh[i]];
+      r.material = mat0 + d->instance_material[i];
+      r.prim_offset = d->instance_primitive_offset[i];
+      r.instance_id = d->instance_id[i];
+      if (k < members)
+        for (int c = 0; c < 12; ++c) o2w[12ull * k + c] = m[c];
+    }
+    // world-space triangles of the baked instances, in packed order; the
+    // TLAS references their slots directly and hits report the identity
+    // record, whose tri_owner entries name the original instances
     std::vector<float4> fv(3ull * flat_tris), fn(3ull * flat_tris);
     std::vector<uint32_t> fpacked(flat_tris), fowner(flat_tris);
-    uint64_t t = 0;
-    for (uint32_t i = 0; i < ni; ++i) {
-      if (!flat[i]) continue;
-      const InstanceRec& r = inst[internal_of[i]];
-      Affine mo{r.o2w0, r.o2w1, r.o2w2}, mw{r.w2o0, r.w2o1, r.w2o2};
-      const uint32_t m = d->instance_mesh[i];
-      const uint32_t v0 = d->mesh_vertex_offset[m];
-      for (uint32_t lt = 0; lt < mesh_tris(m); ++lt, ++t) {
-        for (int c = 0; c < 3; ++c) {
-          uint32_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
-          float3 p = xform_point(mo, make_float3(d->vertices[3ull * vi], d->vertices[3ull * vi + 1],
-                                                 d->vertices[3ull * vi + 2]));
-          float3 nn = normalize(xform_normal_by_inverse(
-              mw, make_float3(d->normals[3ull * vi], d->normals[3ull * vi + 1], d->normals[3ull * vi + 2])));
-          fv[3 * t + c] = make_float4(p.x, p.y, p.z, 0.0f);
-          fn[3 * t + c] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+    {
+      uint64_t t = 0;
+      for (uint32_t i = 0; i < ni; ++i) {
+        if (!flat[i]) continue;
+        const InstanceRec& r = inst[local_of[i]];
+        Affine mo{r.o2w0, r.o2w1, r.o2w2}, mw{r.w2o0, r.w2o1, r.w2o2};
+        const uint32_t m = d->instance_mesh[i];
+        const uint32_t v0 = d->mesh_vertex_offset[m];
+        for (uint32_t lt = 0; lt < mesh_tris(m); ++lt, ++t) {
+          for (int c = 0; c < 3; ++c) {
+            uint32_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
+            float3 p = xform_point(mo, make_float3(d->vertices[3ull * vi], d->vertices[3ull * vi + 1],
+                                                   d->vertices[3ull * vi + 2]));
+            float3 nn = normalize(xform_normal_by_inverse(
+                mw, make_float3(d->normals[3ull * vi], d->normals[3ull * vi + 1], d->normals[3ull * vi + 2])));
+            fv[3 * t + c] = make_float4(p.x, p.y, p.z, 0.0f);
+            fn[3 * t + c] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+          }
+          fpacked[t] = r.prim_offset + lt;
+          fowner[t] = inst0 + local_of[i];
         }
-        fpacked[t] = r.prim_offset + lt;
-        fowner[t] = internal_of[i];
       }
     }
-    OLC_CUDA(cudaMemcpyAsync(sp.tri_verts.as<float4>() + 3ull * total_t, fv.data(), fv.size() * sizeof(float4),
-                             cudaMemcpyHostToDevice, st));
-    OLC_CUDA(cudaMemcpyAsync(sp.tri_normals.as<float4>() + 3ull * total_t, fn.data(), fn.size() * sizeof(float4),
-                             cudaMemcpyHostToDevice, st));
-    OLC_CUDA(cudaMemcpyAsync(sp.tri_index.as<uint32_t>() + total_t, fpacked.data(), fpacked.size() * 4,
-                             cudaMemcpyHostToDevice, st));
-    OLC_CUDA(cudaMemcpyAsync(sp.tri_owner.as<uint32_t>() + total_t, fowner.data(), fowner.size() * 4,
-                             cudaMemcpyHostToDevice, st));
-    OLC_CUDA(cudaStreamSynchronize(st));  // the host staging vectors go out of scope
-    // identity record that hits on direct triangles report as their instance
-    const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
-    InstanceRec& r = inst[pseudo];
-    fill_record(r, identity);
-    r.blas_root = 0;
-    r.material = 0;
-    r.prim_offset = 0;
-    r.instance_id = 0xffffffffu;
-    r.flags = OLC_INSTANCE_FLATTENED;
-  }
-  upload(sp.instances, inst.data(), n_records, st, bytes);
-  upload(sp.o2w, o2w.data(), 12ull * std::max<uint32_t>(pseudo, 1), st, bytes);
-  std::vector<uint2> ranges(std::max<uint32_t>(pseudo, 1));
-  for (uint32_t k = 0; k < pseudo; ++k) {
-    const uint32_t m = d->instance_mesh[order[k]];
-    ranges[k] = make_uint2(d->mesh_triangle_offset[m], d->mesh_triangle_offset[m + 1]);
-  }
-  DeviceBuffer dranges;
-  uint64_t scratch_bytes = 0;
-  upload(dranges, ranges.data(), pseudo, st, scratch_bytes);
-  uint32_t tlas_root = build_tlas(sp.o2w.as<float>(), dranges.as<uint2>(), pseudo, sp.tri_verts.as<float4>(),
-                                  sp.tri_verts.as<float4>() + 3ull * total_t, (uint32_t)flat_tris, ctx->scratch,
-                                  sp.nodes.as<BvhNode>(), tlas_base, st);
-  OLC_CUDA(cudaStreamSynchronize(st));  // dranges goes out of scope
-  sp.flattened_instances = flat_count;
-  sp.tlas_instances = tlas_members;
-  // materials
-  std::vector<MaterialRec> mats(d->num_materials);
-  std::vector<MaterialAux> aux(d->num_materials);
-  for (uint32_t k = 0; k < d->num_materials; ++k) {
-    const float* p = d->materials + 16ull * k;
-    mats[k].base_rough = make_float4(p[0], p[1], p[2], p[3]);
-    mats[k].emit_metal = make_float4(p[4], p[5], p[6], p[7]);
-    aux[k].two_sided = p[8] > 0.5f ? 1u : 0u;
-    uint32_t mid;
-    std::memcpy(&mid, &p[9], 4);
-    aux[k].material_id = mid;
-    aux[k].pad0 = aux[k].pad1 = 0;
-  }
-  upload(sp.materials, mats.data(), mats.size(), st, bytes);
-  upload(sp.material_aux, aux.data(), aux.size(), st, bytes);
-  {
+    upload_to(tri_verts + 3ull * flat_slot0, fv.data(), fv.size(), st);
+    upload_to(tri_normals + 3ull * flat_slot0, fn.data(), fn.size(), st);
+    upload_to(tri_index + flat_slot0, fpacked.data(), fpacked.size(), st);
+    upload_to(tri_owner + flat_slot0, fowner.data(), fowner.size(), st);
+    upload_to(ctx->instances.at<InstanceRec>(0, inst0), inst.data(), inst.size(), st);
+
+    // ---- TLAS over the member instances and the baked triangles
+    std::vector<uint2> ranges(std::max<uint32_t>(members, 1));
+    for (uint32_t k = 0; k < members; ++k) {
+      const uint32_t m = d->instance_mesh[order[k]];
+      ranges[k] = make_uint2(slot0 + d->mesh_triangle_offset[m], slot0 + d->mesh_triangle_offset[m + 1]);
+    }
+    DeviceBuffer d_o2w, d_ranges;
+    upload(d_o2w, o2w.data(), o2w.size(), st, staging);
+    upload(d_ranges, ranges.data(), members, st, staging);
+    const uint32_t tlas_root =
+        build_tlas(d_o2w.as<float>(), d_ranges.as<uint2>(), members, inst0, tri_verts, tri_verts + 3ull * flat_slot0,
+                   (uint32_t)flat_tris, flat_slot0, ctx->scratch, nodes, node0 + tlas_local, st);
+
+    // ---- materials, emitters, lights
+    std::vector<MaterialRec> mats(d->num_materials);
+    std::vector<MaterialAux> aux(d->num_materials);
+    for (uint32_t k = 0; k < d->num_materials; ++k) {
+      const float* p = d->materials + 16ull * k;
+      mats[k].base_rough = make_float4(p[0], p[1], p[2], p[3]);
+      mats[k].emit_metal = make_float4(p[4], p[5], p[6], p[7]);
+      aux[k].two_sided = p[8] > 0.5f ? 1u : 0u;
+      uint32_t mid;
+      std::memcpy(&mid, &p[9], 4);
+      aux[k].material_id = mid;
+      aux[k].pad0 = aux[k].pad1 = 0;
+    }
+    upload_to(ctx->materials.at<MaterialRec>(0, mat0), mats.data(), mats.size(), st);
+    upload_to(ctx->materials.at<MaterialAux>(1, mat0), aux.data(), aux.size(), st);
     std::vector<EmitterRec> em;
     std::vector<AliasEntry> alias;
     build_emitters(d, em, alias);
-    upload(sp.emitters, em.data(), em.size(), st, bytes);
-    upload(sp.emitter_alias, alias.data(), alias.size(), st, bytes);
-  }
-  upload(sp.lights, reinterpret_cast<const LightRec*>(d->lights), d->num_lights, st, bytes);
-  size_t env_count = d->environment_kind == OLC_ENV_EQUIRECT ? 3ull * d->environment_width * d->environment_height : 0;
-  if (d->environment_kind == OLC_ENV_EQUIRECT && (!d->environment_image || env_count == 0))
-    throw Error(OLC_ERR_VALUE, "equirect environment needs an image");
-  upload(sp.env_image, d->environment_image, env_count, st, bytes);
-  size_t vol_count = d->volume_present ? (size_t)d->volume_dims[0] * d->volume_dims[1] * d->volume_dims[2] : 0;
-  upload(sp.volume, d->volume_density, vol_count, st, bytes);
+    upload_to(ctx->emitters.at<EmitterRec>(0, rs.emitters.off), em.data(), em.size(), st);
+    upload_to(ctx->emitters.at<AliasEntry>(1, rs.emitters.off), alias.data(), alias.size(), st);
+    if (d->num_lights && !d->lights) throw Error(OLC_ERR_VALUE, "light records are required");
+    upload_to(ctx->lights.at<LightRec>(0, rs.lights.off), reinterpret_cast<const LightRec*>(d->lights),
+              d->num_lights, st);
+    uint64_t own = 0;
+    size_t env_count =
+        d->environment_kind == OLC_ENV_EQUIRECT ? 3ull * d->environment_width * d->environment_height : 0;
+    upload(rs.env_image, d->environment_image, env_count, st, own);
+    size_t vol_count = d->volume_present ? (size_t)d->volume_dims[0] * d->volume_dims[1] * d->volume_dims[2] : 0;
+    if (d->volume_present && (!d->volume_density || vol_count == 0))
+      throw Error(OLC_ERR_VALUE, "a volume needs a density grid");
+    upload(rs.volume, d->volume_density, vol_count, st, own);
+    OLC_CUDA(cudaStreamSynchronize(st));  // host staging vectors go out of scope
 
-  SceneView& v = sp.view;
-  v.nodes = sp.nodes.as<BvhNode>();
-  v.tri_verts = sp.tri_verts.as<float4>();
-  v.tri_normals = sp.tri_normals.as<float4>();
-  v.tri_index = sp.tri_index.as<uint32_t>();
-  v.tri_owner = sp.tri_owner.as<uint32_t>();
-  v.instances = sp.instances.as<InstanceRec>();
-  v.materials = sp.materials.as<MaterialRec>();
-  v.material_aux = sp.material_aux.as<MaterialAux>();
-  v.emitters = sp.emitters.as<EmitterRec>();
-  v.emitter_alias = sp.emitter_alias.as<AliasEntry>();
-  v.lights = sp.lights.as<LightRec>();
-  v.env_image = sp.env_image.as<float>();
-  v.volume = sp.volume.as<float>();
-  v.tlas_root = tlas_root;
-  v.num_instances = tlas_members;
-  v.tlas_instances = pseudo;
-  v.flat_slot_base = total_t;
-  v.flat_instance = pseudo;
-  v.num_emitters = d->num_emitters;
-  v.num_lights = d->num_lights;
-  v.emissive_weight = d->emissive_weight;
-  v.env_kind = d->environment_kind;
-  v.env_color = make_float3(d->environment_color[0], d->environment_color[1], d->environment_color[2]);
-  v.env_rotation = d->environment_rotation;
-  v.env_w = d->environment_width;
-  v.env_h = d->environment_height;
-  v.volume_present = d->volume_present;
-  v.vol_nx = d->volume_dims[0];
-  v.vol_ny = d->volume_dims[1];
-  v.vol_nz = d->volume_dims[2];
-  const float* vb = d->volume_world_to_box;
-  v.vol_world_to_box.r0 = make_float4(vb[0], vb[1], vb[2], vb[3]);
-  v.vol_world_to_box.r1 = make_float4(vb[4], vb[5], vb[6], vb[7]);
-  v.vol_world_to_box.r2 = make_float4(vb[8], vb[9], vb[10], vb[11]);
-  v.vol_sigma_t_scale = d->volume_sigma_t_scale;
-  v.vol_albedo = d->volume_albedo;
-  v.vol_max_density = d->volume_max_density;
-  OLC_CUDA(cudaStreamSynchronize(st));
-  sp.total_triangles = total_t;
-  sp.blas_nodes = tlas_base;
-  sp.tlas_nodes = tlas_nodes;
-  sp.blas_count = nm;
-  sp.bytes = bytes;
-  sp.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  sp.valid = true;
+    SceneRec& v = rs.rec;
+    std::memset(&v, 0, sizeof(v));
+    v.tlas_root = tlas_root;
+    v.emitter_base = (uint32_t)rs.emitters.off;
+    v.num_emitters = d->num_emitters;
+    v.emissive_weight = d->emissive_weight;
+    v.light_base = (uint32_t)rs.lights.off;
+    v.num_lights = d->num_lights;
+    v.env_kind = d->environment_kind;
+    v.env_rotation = d->environment_rotation;
+    v.env_color = make_float4(d->environment_color[0], d->environment_color[1], d->environment_color[2], 0.0f);
+    v.env_image = rs.env_image.as<float>();
+    v.env_w = d->environment_width;
+    v.env_h = d->environment_height;
+    v.volume = rs.volume.as<float>();
+    v.volume_present = d->volume_present;
+    v.vol_nx = d->volume_dims[0];
+    v.vol_ny = d->volume_dims[1];
+    v.vol_nz = d->volume_dims[2];
+    const float* vb = d->volume_world_to_box;
+    v.vol_w2b0 = make_float4(vb[0], vb[1], vb[2], vb[3]);
+    v.vol_w2b1 = make_float4(vb[4], vb[5], vb[6], vb[7]);
+    v.vol_w2b2 = make_float4(vb[8], vb[9], vb[10], vb[11]);
+    v.vol_sigma_t_scale = d->volume_sigma_t_scale;
+    v.vol_albedo = d->volume_albedo;
+    v.vol_max_density = d->volume_max_density;
+
+    rs.triangles = total_t;
+    rs.blas_count = (uint32_t)rs.blas_ranges.size();
+    rs.blas_nodes = tlas_local;
+    rs.tlas_nodes = tlas_nodes;
+    rs.flattened = flat_count;
+    rs.bytes = ctx->nodes.range_bytes(rs.nodes) + ctx->slots.range_bytes(rs.slots) +
+               ctx->instances.range_bytes(rs.instances) + ctx->materials.range_bytes(rs.materials) +
+               ctx->emitters.range_bytes(rs.emitters) + ctx->lights.range_bytes(rs.lights) + own;
+    rs.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    release_scene_ranges(ctx, rs);
+    throw;
+  }
 }
 
-void ensure_wavefront(olc_context* ctx, uint32_t capacity, uint32_t npix) {
-  if (capacity > ctx->capacity) {
-    size_t c = capacity;
-    ctx->q0_o.allocate(c * 16);
-    ctx->q0_d.allocate(c * 16);
-    ctx->q0_p.allocate(c * 4);
-    ctx->q1_o.allocate(c * 16);
-    ctx->q1_d.allocate(c * 16);
-    ctx->q1_p.allocate(c * 4);
-    ctx->hit_tuv.allocate(c * 16);
-    ctx->hit_inst.allocate(c * 4);
-    ctx->sh_o.allocate(c * 16);
-    ctx->sh_d.allocate(c * 16);
-    ctx->sh_c.allocate(c * 16);
-    ctx->ps_tp.allocate(c * 16);
-    ctx->ps_rad.allocate(c * 16);
-    ctx->ps_meta.allocate(c * 16);
-    ctx->capacity = capacity;
-    drop_graphs(ctx);
+// Upload the scene table (one SceneRec per handle).
+void sync_scene_table(olc_context* ctx) {
+  const size_t n = std::max<size_t>(ctx->scenes.size(), 1);
+  std::vector<SceneRec> recs(n);
+  std::memset(recs.data(), 0, n * sizeof(SceneRec));
+  for (size_t i = 0; i < ctx->scenes.size(); ++i)
+    if (ctx->scenes[i]) recs[i] = ctx->scenes[i]->rec;
+  if (ctx->scene_table.bytes() < n * sizeof(SceneRec)) {
+    ctx->scene_table.allocate(std::max<size_t>(n, 16) * sizeof(SceneRec));
   }
-  if (npix > ctx->npix_capacity) {
-    size_t n = npix;
-    ctx->accum.allocate(n * 3 * 8);
-    ctx->out_dev.allocate(n * 16);
-    ctx->prod_depth.allocate(n * 4);
-    ctx->prod_normal.allocate(n * 16);
-    ctx->prod_inst.allocate(n * 4);
-    ctx->prod_mat.allocate(n * 4);
-    ctx->prod_prim.allocate(n * 4);
-    ctx->npix_capacity = npix;
-    drop_graphs(ctx);
-  }
-  if (!ctx->counters.get()) ctx->counters.allocate(sizeof(Counters));
-  if (!ctx->fp_dev.get()) ctx->fp_dev.allocate(sizeof(FrameParams));
+  OLC_CUDA(cudaMemcpyAsync(ctx->scene_table.get(), recs.data(), n * sizeof(SceneRec), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  OLC_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
-void ensure_host_counters(olc_context* ctx, uint32_t chunks) {
-  if (chunks <= ctx->counters_host_chunks) return;
-  if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
-  ctx->counters_host = nullptr;
-  OLC_CUDA(cudaMallocHost(&ctx->counters_host, sizeof(Counters) * chunks));
-  ctx->counters_host_chunks = chunks;
+uint32_t add_scene(olc_context* ctx, const olc_scene_desc* desc) {
+  std::unique_ptr<ResidentScene> rs(new ResidentScene());
+  build_scene(ctx, desc, *rs);
+  uint32_t handle = 0;
+  while (handle < ctx->scenes.size() && ctx->scenes[handle]) ++handle;
+  if (handle == ctx->scenes.size()) ctx->scenes.emplace_back();
+  ctx->scenes[handle] = std::move(rs);
+  sync_scene_table(ctx);
+  drop_graphs(ctx);
+  return handle;
+}
+
+void remove_scene(olc_context* ctx, uint32_t handle) {
+  if (handle >= ctx->scenes.size() || !ctx->scenes[handle]) throw Error(OLC_ERR_VALUE, "unknown scene handle");
+  for (const auto& j : ctx->served)
+    if (j->rec.scene == handle) throw Error(OLC_ERR_RUNTIME, "a queued job still renders this scene");
+  OLC_CUDA(cudaStreamSynchronize(ctx->stream));
+  release_scene_ranges(ctx, *ctx->scenes[handle]);
+  ctx->scenes[handle].reset();
+  if (ctx->default_scene == handle) ctx->default_scene = kNoScene;
+  if (ctx->restir.hist_scene == handle) restir_reset(ctx->restir);
+  sync_scene_table(ctx);
   drop_graphs(ctx);
 }
 
-void fill_frame(olc_context* ctx, const olc_camera* cam, uint32_t w, uint32_t h, uint32_t spp, uint32_t frame_index) {
-  FrameParams& f = *ctx->fp_host;
+const ResidentScene& scene_of(const olc_context* ctx, uint32_t handle) {
+  if (handle >= ctx->scenes.size() || !ctx->scenes[handle]) throw Error(OLC_ERR_VALUE, "unknown scene handle");
+  return *ctx->scenes[handle];
+}
+
+const ResidentScene& default_scene(const olc_context* ctx) {
+  if (ctx->default_scene == kNoScene) throw Error(OLC_ERR_RUNTIME, "no scene is resident; upload a scene first");
+  return *ctx->scenes[ctx->default_scene];
+}
+
+// ---- jobs -----------------------------------------------------------------
+
+void check_camera(const olc_camera* cam) {
+  if (!cam) throw Error(OLC_ERR_VALUE, "camera is required");
+  if (cam->projection > 2) throw Error(OLC_ERR_VALUE, "unknown camera projection");
+}
+
+void check_size(uint32_t w, uint32_t h, uint32_t spp) {
+  if (w == 0 || h == 0) throw Error(OLC_ERR_VALUE, "width and height must be positive");
+  if ((uint64_t)w * h > (1ull << 28)) throw Error(OLC_ERR_VALUE, "image is too large");
+  if (spp < 1 || spp > 65536) throw Error(OLC_ERR_VALUE, "samples must be between 1 and 65536");
+}
+
+JobRec make_job(const olc_context* ctx, const olc_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                uint32_t frame_index, uint32_t max_bounces, uint32_t scene) {
+  JobRec f;
+  std::memset(&f, 0, sizeof(f));
   f.cam_pos = make_float4(cam->position[0], cam->position[1], cam->position[2], 0.0f);
   f.cam_forward = make_float4(cam->forward[0], cam->forward[1], cam->forward[2], 0.0f);
   f.cam_right = make_float4(cam->right[0], cam->right[1], cam->right[2], 0.0f);
@@ -586,88 +821,429 @@ void fill_frame(olc_context* ctx, const olc_camera* cam, uint32_t w, uint32_t h,
   f.spp = spp;
   f.frame = ctx->cfg.seed + frame_index;
   f.npix = w * h;
-  f.max_bounces = ctx->cfg.max_bounces;
+  f.max_bounces = max_bounces ? max_bounces : ctx->cfg.max_bounces;
   f.mode = ctx->cfg.mode;
   f.rr_start = ctx->cfg.mode == OLC_MODE_PRODUCTION ? ctx->cfg.russian_roulette_start : 0u;
   f.rr_min_survival = ctx->cfg.russian_roulette_min_survival;
-  f.restir = ctx->cfg.restir;
   f.nee = ctx->cfg.disable_nee ? 0u : 1u;
+  f.scene = scene;
+  const bool restir = ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION &&
+                      scene < ctx->scenes.size() && ctx->scenes[scene] && ctx->scenes[scene]->rec.num_emitters > 0;
+  f.restir = restir ? 1u : 0u;
+  return f;
 }
 
-struct Timing {
-  bool on = false;
-  cudaEvent_t ev[8] = {};
-  float ms[7] = {};
+// Reserve the job's accumulator pixels and clear them (stream ordered, before
+// any of its chunks).
+void admit_job(olc_context* ctx, QueuedJob& j) {
+  j.pixels = ctx->pixels.acquire(j.rec.npix, ctx->stream);
+  j.rec.pixel_base = j.pixels.off;
+  OLC_CUDA(cudaMemsetAsync(ctx->pixels.at<unsigned long long>(0, j.pixels.off), 0,
+                           (size_t)j.rec.npix * ctx->pixels.elem[0], ctx->stream));
+}
+
+uint64_t plan_capacity(const olc_context* ctx, const std::vector<QueuedJob*>& jobs) {
+  uint64_t cap = ctx->cfg.chunk_paths ? ctx->cfg.chunk_paths : kDefaultChunkPaths;
+  for (const QueuedJob* j : jobs)
+    if (j->rec.restir) cap = std::max<uint64_t>(cap, j->rec.npix);  // a whole stream per ReSTIR segment
+  return std::min<uint64_t>(cap, 0xffffffffull);
+}
+
+// Split the jobs' remaining paths into at most max_chunks chunks of at most
+// cap paths, in job order.  A ReSTIR segment holds whole sample streams; a
+// stream that does not fit leaves room for later jobs' paths.  Chunk-local
+// reservoirs start after the first reservoir_region entries (the job-local
+// reservoirs of a plain frame).
+void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, uint64_t reservoir_region,
+              RunPlan& plan) {
+  for (uint32_t c = 0; c < max_chunks; ++c) {
+    ChunkPlan ch;
+    uint64_t fill = 0;
+    for (QueuedJob* j : jobs) {
+      if (j->issued >= j->total) continue;
+      const uint64_t left = cap - fill;
+      if (left == 0) break;
+      uint64_t take;
+      if (j->rec.restir) {
+        const uint64_t streams = std::min<uint64_t>(left / j->rec.npix, (j->total - j->issued) / j->rec.npix);
+        take = streams * j->rec.npix;
+        if (take == 0) continue;
+      } else {
+        take = std::min<uint64_t>(left, j->total - j->issued);
+      }
+      JobRec seg = j->rec;
+      seg.seg_begin = fill;
+      seg.seg_first = j->issued;
+      if (seg.restir && !j->job_local_reservoirs) {
+        // chunk-local reservoirs: index = reservoir_region + chunk path index
+        seg.reservoir_base = reservoir_region + fill - j->issued;  // modulo 2^64
+        plan.chunk_reservoirs = true;
+      }
+      ch.segs.push_back(seg);
+      ch.bounces = std::max(ch.bounces, seg.max_bounces);
+      ch.restir = ch.restir || seg.restir;
+      fill += take;
+      j->issued += take;
+      if (j->issued == j->total) plan.finished.push_back(j);
+    }
+    if (fill == 0) break;
+    ch.count = (uint32_t)fill;
+    plan.restir = plan.restir || ch.restir;
+    plan.max_segments = std::max<uint32_t>(plan.max_segments, (uint32_t)ch.segs.size());
+    plan.max_count = std::max<uint32_t>(plan.max_count, ch.count);
+    plan.chunks.push_back(std::move(ch));
+  }
+}
+
+void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
+  if (capacity <= ctx->capacity) return;
+  size_t c = capacity;
+  ctx->q0_o.allocate(c * 16);
+  ctx->q0_d.allocate(c * 16);
+  ctx->q0_p.allocate(c * 4);
+  ctx->q1_o.allocate(c * 16);
+  ctx->q1_d.allocate(c * 16);
+  ctx->q1_p.allocate(c * 4);
+  ctx->hit_tuv.allocate(c * 16);
+  ctx->hit_inst.allocate(c * 4);
+  ctx->sh_o.allocate(c * 16);
+  ctx->sh_d.allocate(c * 16);
+  ctx->sh_c.allocate(c * 16);
+  ctx->ps_tp.allocate(c * 16);
+  ctx->ps_rad.allocate(c * 16);
+  ctx->ps_meta.allocate(c * 16);
+  ctx->capacity = capacity;
+  drop_graphs(ctx);
+}
+
+void ensure_products(olc_context* ctx, uint32_t npix) {
+  if (npix <= ctx->prod_pixels) return;
+  size_t n = npix;
+  ctx->prod_depth.allocate(n * 4);
+  ctx->prod_normal.allocate(n * 16);
+  ctx->prod_inst.allocate(n * 4);
+  ctx->prod_mat.allocate(n * 4);
+  ctx->prod_prim.allocate(n * 4);
+  ctx->prod_pixels = npix;
+  drop_graphs(ctx);
+}
+
+size_t chunk_stride(uint32_t seg_capacity) { return sizeof(ChunkHeader) + (size_t)seg_capacity * sizeof(JobRec); }
+
+void ensure_host_counters(olc_context* ctx, uint32_t chunks) {
+  if (chunks <= ctx->counters_host_chunks) return;
+  if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
+  ctx->counters_host = nullptr;
+  ctx->counters_host_chunks = 0;
+  OLC_CUDA(cudaMallocHost(&ctx->counters_host, sizeof(Counters) * chunks));
+  ctx->counters_host_chunks = chunks;
+  drop_graphs(ctx);
+}
+
+void ensure_table(olc_context* ctx, size_t bytes) {
+  if (bytes <= ctx->table_bytes) return;
+  size_t b = std::max<size_t>(bytes, 64 * 1024);
+  ctx->table_dev.allocate(b);
+  if (ctx->table_host) cudaFreeHost(ctx->table_host);
+  ctx->table_host = nullptr;
+  ctx->table_bytes = 0;
+  OLC_CUDA(cudaMallocHost(&ctx->table_host, b));
+  ctx->table_bytes = b;
+  drop_graphs(ctx);
+}
+
+struct RunBuffers {
+  RayQueue qa, qb;
+  HitBuf hb;
+  ShadowQueue sq;
+  PathState ps;
+  ProductPtrs prod;
+  Counters* cnt;
+  unsigned long long* accum;
+  float4* out;
+  const char* table;
+  size_t stride;
+  size_t resolve_offset;
 };
 
-// Record the device work of one frame into ctx->stream.
-void record_frame(olc_context* ctx, uint32_t w, uint32_t h, uint32_t spp, bool products) {
+RunBuffers run_buffers(olc_context* ctx, size_t stride, size_t resolve_offset) {
+  RunBuffers b;
+  b.qa = RayQueue{ctx->q0_o.as<float4>(), ctx->q0_d.as<float4>(), ctx->q0_p.as<uint32_t>()};
+  b.qb = RayQueue{ctx->q1_o.as<float4>(), ctx->q1_d.as<float4>(), ctx->q1_p.as<uint32_t>()};
+  b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
+  b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
+  b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>()};
+  b.prod.depth = ctx->prod_depth.as<float>();
+  b.prod.normal = ctx->prod_normal.as<float4>();
+  b.prod.instance_id = ctx->prod_inst.as<uint32_t>();
+  b.prod.material_id = ctx->prod_mat.as<uint32_t>();
+  b.prod.primitive_id = ctx->prod_prim.as<uint32_t>();
+  b.cnt = ctx->counters.as<Counters>();
+  b.accum = ctx->pixels.at<unsigned long long>(0);
+  b.out = ctx->pixels.at<float4>(1);
+  b.table = ctx->table_dev.as<char>();
+  b.stride = stride;
+  b.resolve_offset = resolve_offset;
+  return b;
+}
+
+// Record the device work of one run into ctx->stream.
+void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
   cudaStream_t st = ctx->stream;
-  const uint32_t npix = w * h;
-  const uint64_t total = (uint64_t)npix * spp;
-  const uint32_t cap = ctx->capacity;
-  const uint32_t chunks = (uint32_t)((total + cap - 1) / cap);
-  const SceneView& s = ctx->scene.view;
-  const FrameParams* fp = ctx->fp_dev.as<FrameParams>();
-  Counters* cnt = ctx->counters.as<Counters>();
-  RayQueue qa{ctx->q0_o.as<float4>(), ctx->q0_d.as<float4>(), ctx->q0_p.as<uint32_t>()};
-  RayQueue qb{ctx->q1_o.as<float4>(), ctx->q1_d.as<float4>(), ctx->q1_p.as<uint32_t>()};
-  HitBuf hb{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
-  ShadowQueue sq{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
-  PathState ps{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>()};
-  ProductPtrs prod;
-  if (products) {
-    prod.depth = ctx->prod_depth.as<float>();
-    prod.normal = ctx->prod_normal.as<float4>();
-    prod.instance_id = ctx->prod_inst.as<uint32_t>();
-    prod.material_id = ctx->prod_mat.as<uint32_t>();
-    prod.primitive_id = ctx->prod_prim.as<uint32_t>();
-  }
-  const float t_min = ctx->cfg.mode == OLC_MODE_REFERENCE_COMPATIBLE ? 1e-4f : 0.001f;
-  OLC_CUDA(cudaMemsetAsync(ctx->accum.get(), 0, (size_t)npix * 3 * 8, st));
+  const SceneView s = pool_view(ctx);
+  const SceneRec* scenes = ctx->scene_table.as<SceneRec>();
   tl_begin(ctx);
-  for (uint32_t c = 0; c < chunks; ++c) {
-    uint64_t begin = (uint64_t)c * cap;
-    uint32_t count = (uint32_t)std::min<uint64_t>(cap, total - begin);
-    OLC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
-    launch_raygen(ctx->ls, fp, begin, count, qa, ps, cnt, t_min, st);
+  for (uint32_t c = 0; c < plan.chunks.size(); ++c) {
+    const ChunkPlan& ch = plan.chunks[c];
+    const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(rb.table + c * rb.stride);
+    const JobRec* jobs = reinterpret_cast<const JobRec*>(rb.table + c * rb.stride + sizeof(ChunkHeader));
+    OLC_CUDA(cudaMemsetAsync(rb.cnt, 0, sizeof(Counters), st));
+    launch_raygen(ctx->ls, hdr, jobs, scenes, rb.qa, rb.ps, rb.cnt, st);
     tl_mark(ctx, OLC_STAGE_RAYGEN, 0, c);
-    RayQueue* qin = &qa;
-    RayQueue* qout = &qb;
-    for (uint32_t b = 0; b < ctx->cfg.max_bounces; ++b) {
-      launch_trace_closest(ctx->ls, s, *qin, hb, cnt, b, st);
+    const RayQueue* qin = &rb.qa;
+    const RayQueue* qout = &rb.qb;
+    for (uint32_t b = 0; b < ch.bounces; ++b) {
+      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, st);
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
-      if (b == 0 && ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION && s.num_emitters > 0) {
-        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, fp, *qin, hb, ps, cnt, begin, count, npix, st);
+      if (b == 0 && ch.restir) {
+        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, st);
         tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
-      launch_shade(ctx->ls, ctx->cfg.mode, fp, s, *qin, hb, *qout, sq, ps, cnt, b, cap,
-                   (products && c == 0) ? prod : ProductPtrs{}, restir, st);
+      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
-      launch_trace_shadow(ctx->ls, s, sq, ps, cnt, b, st);
+      launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, st);
       tl_mark(ctx, OLC_STAGE_SHADOW, b, c);
       std::swap(qin, qout);
     }
-    launch_accumulate(ctx->ls, ps, count, ctx->accum.as<unsigned long long>(), cnt, st);
+    launch_accumulate(ctx->ls, hdr, jobs, rb.ps, rb.accum, rb.cnt, st);
     tl_mark(ctx, OLC_STAGE_ACCUMULATE, 0, c);
-    OLC_CUDA(cudaMemcpyAsync(ctx->counters_host + c, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaMemcpyAsync(ctx->counters_host + c, rb.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
   }
-  launch_resolve(ctx->ls, ctx->accum.as<unsigned long long>(), npix, spp, ctx->out_dev.as<float4>(), st);
+  const uint32_t* num_entries = reinterpret_cast<const uint32_t*>(rb.table + rb.resolve_offset);
+  const ResolveEntry* entries = reinterpret_cast<const ResolveEntry*>(rb.table + rb.resolve_offset + 16);
+  launch_resolve(ctx->ls, entries, num_entries, rb.accum, rb.out, st);
   tl_mark(ctx, OLC_STAGE_RESOLVE, 0, 0);
 }
 
-uint32_t choose_capacity(olc_context* ctx, uint32_t npix, uint32_t spp) {
-  uint64_t total = (uint64_t)npix * spp;
-  uint64_t cap = ctx->cfg.chunk_paths ? ctx->cfg.chunk_paths : (1ull << 24);
-  if (ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION) {
-    // whole sample streams per chunk (spatial reuse reads neighbours)
-    uint64_t streams = std::max<uint64_t>(1, cap / npix);
-    cap = streams * npix;
+// Everything the recorded launches depend on besides the device tables.
+std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
+  std::vector<uint64_t> k;
+  k.push_back(plan.chunks.size());
+  for (const ChunkPlan& c : plan.chunks) k.push_back(((uint64_t)c.bounces << 1) | (c.restir ? 1u : 0u));
+  auto ptr = [&](const void* p) { k.push_back((uint64_t)(uintptr_t)p); };
+  const SceneView s = pool_view(ctx);
+  const void* const* sv = reinterpret_cast<const void* const*>(&s);
+  for (size_t i = 0; i < sizeof(SceneView) / sizeof(void*); ++i) ptr(sv[i]);
+  for (const void* p : std::initializer_list<const void*>{(const void*)rb.qa.origin_tmin, (const void*)rb.qa.dir_root, (const void*)rb.qa.path,
+                        (const void*)rb.qb.origin_tmin, (const void*)rb.qb.dir_root, (const void*)rb.qb.path,
+                        (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
+                        (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
+                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.prod.depth,
+                        (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
+                        (const void*)rb.prod.primitive_id, (const void*)rb.cnt, (const void*)rb.accum,
+                        (const void*)rb.out, (const void*)rb.table, (const void*)ctx->counters_host,
+                        ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_b0.get(),
+                        ctx->restir.res_b1.get(), ctx->restir.hist0.get(), ctx->restir.hist1.get(),
+                        ctx->restir.selected.get(), ctx->restir.hit_list.get(), ctx->restir.hit_count.get()})
+    ptr(p);
+  k.push_back(rb.stride);
+  k.push_back(rb.resolve_offset);
+  k.push_back(ctx->capacity);
+  const LaunchShape& ls = ctx->ls;
+  for (uint32_t v : {ls.block, ls.trace_block, ls.grid_simple, ls.grid_trace, ls.grid_shade, ls.stack_depth,
+                     ls.scheduler})
+    k.push_back(v);
+  const olc_config& c = ctx->cfg;
+  for (uint32_t v : {c.restir_candidates, c.restir_spatial, c.restir_neighbours, c.restir_max_history})
+    k.push_back(v);
+  uint32_t radius;
+  std::memcpy(&radius, &c.restir_radius, 4);
+  k.push_back(radius);
+  return k;
+}
+
+// Launch a run: from a cached graph, a newly captured one, or directly.
+void launch_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
+  cudaStream_t st = ctx->stream;
+  if (!ctx->cfg.use_graphs) {
+    record_run(ctx, plan, rb);
+    return;
   }
-  cap = std::min<uint64_t>(cap, total);
-  if (cap > 0xffffffffull) cap = 0xffffffffull;
-  return (uint32_t)cap;
+  std::vector<uint64_t> key = run_signature(ctx, plan, rb);
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    if (ctx->graphs.size() >= kMaxGraphs) {
+      auto oldest = ctx->graphs.begin();
+      for (auto g = ctx->graphs.begin(); g != ctx->graphs.end(); ++g)
+        if (g->second.last_used < oldest->second.last_used) oldest = g;
+      cudaGraphExecDestroy(oldest->second.exec);
+      ctx->graphs.erase(oldest);
+    }
+    cudaGraph_t g = nullptr;
+    OLC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    ctx->capturing = true;
+    try {
+      record_run(ctx, plan, rb);
+    } catch (...) {
+      ctx->capturing = false;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    ctx->capturing = false;
+    OLC_CUDA(cudaStreamEndCapture(st, &g));
+    cudaGraphExec_t exec;
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    OLC_CUDA(e);
+    GraphEntry ge;
+    ge.exec = exec;
+    ge.timeline = ctx->tl_entries;
+    it = ctx->graphs.emplace(std::move(key), std::move(ge)).first;
+  }
+  it->second.last_used = ++ctx->graph_clock;
+  ctx->tl_entries = it->second.timeline;
+  OLC_CUDA(cudaGraphLaunch(it->second.exec, st));
+}
+
+// Execute a planned run: stage the tables, launch, copy finished outputs,
+// wait, and gather statistics.  The jobs in plan.finished are complete when
+// this returns.
+void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
+  cudaStream_t st = ctx->stream;
+  const uint32_t nchunks = (uint32_t)plan.chunks.size();
+  if (nchunks == 0) throw Error(OLC_ERR_RUNTIME, "a run without paths");
+  if (plan.max_segments > ctx->seg_capacity) {
+    uint32_t s = ctx->seg_capacity;
+    while (s < plan.max_segments) s *= 2;
+    ctx->seg_capacity = s;
+    drop_graphs(ctx);
+  }
+  ensure_wavefront(ctx, std::max<uint32_t>(plan.max_count, 1));
+  ensure_host_counters(ctx, std::max<uint32_t>(nchunks, 1));
+  if (!ctx->counters.get()) ctx->counters.allocate(sizeof(Counters));
+  const size_t stride = chunk_stride(ctx->seg_capacity);
+  const size_t resolve_offset = stride * nchunks;
+  const size_t bytes = resolve_offset + 16 + sizeof(ResolveEntry) * plan.finished.size();
+  ensure_table(ctx, bytes);
+  // host staging of all chunk tables and the resolve list
+  for (uint32_t c = 0; c < nchunks; ++c) {
+    const ChunkPlan& ch = plan.chunks[c];
+    ChunkHeader* h = reinterpret_cast<ChunkHeader*>(ctx->table_host + c * stride);
+    h->count = ch.count;
+    h->num_segments = (uint32_t)ch.segs.size();
+    h->stamp = plan.restir ? ctx->restir.run_first + c : 0u;
+    h->history_first = ctx->restir.hist_first;
+    h->history_last = ctx->restir.hist_last;
+    h->pad[0] = h->pad[1] = h->pad[2] = 0;
+    std::memcpy(ctx->table_host + c * stride + sizeof(ChunkHeader), ch.segs.data(), ch.segs.size() * sizeof(JobRec));
+  }
+  {
+    uint32_t* n = reinterpret_cast<uint32_t*>(ctx->table_host + resolve_offset);
+    n[0] = (uint32_t)plan.finished.size();
+    n[1] = n[2] = n[3] = 0;
+    ResolveEntry* e = reinterpret_cast<ResolveEntry*>(ctx->table_host + resolve_offset + 16);
+    for (size_t k = 0; k < plan.finished.size(); ++k) {
+      e[k].pixel_base = plan.finished[k]->rec.pixel_base;
+      e[k].npix = plan.finished[k]->rec.npix;
+      e[k].spp = plan.finished[k]->rec.spp;
+    }
+  }
+  OLC_CUDA(cudaMemcpyAsync(ctx->table_dev.get(), ctx->table_host, bytes, cudaMemcpyHostToDevice, st));
+  const RunBuffers rb = run_buffers(ctx, stride, resolve_offset);
+  OLC_CUDA(cudaEventRecord(ctx->ev_begin, st));
+  launch_run(ctx, plan, rb);
+  OLC_CUDA(cudaEventRecord(ctx->ev_end, st));
+  for (QueuedJob* j : plan.finished) {
+    if (!j->out) continue;
+    OLC_CUDA(cudaMemcpyAsync(j->out, rb.out + j->rec.pixel_base, (size_t)j->rec.npix * sizeof(float4),
+                             j->out_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  }
+  OLC_CUDA(cudaStreamSynchronize(st));
+
+  // per-launch device timeline
+  ctx->last_profile.clear();
+  ctx->last_chunk_counts.clear();
+  for (const ChunkPlan& ch : plan.chunks) ctx->last_chunk_counts.push_back(ch.count);
+  float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  uint64_t resolved_pixels = 0;
+  for (const QueuedJob* j : plan.finished) resolved_pixels += j->rec.npix;
+  for (size_t k = 0; k < ctx->tl_entries.size(); ++k) {
+    const TimelineEntry& e = ctx->tl_entries[k];
+    olc_launch_record r{};
+    r.stage = e.stage;
+    r.bounce = e.bounce;
+    r.chunk = e.chunk;
+    OLC_CUDA(cudaEventElapsedTime(&r.ms, ctx->tl_events[k], ctx->tl_events[k + 1]));
+    const Counters& kc = ctx->counters_host[std::min<uint32_t>(e.chunk, nchunks - 1)];
+    switch (e.stage) {
+      case OLC_STAGE_RAYGEN: case OLC_STAGE_ACCUMULATE: r.items = plan.chunks[e.chunk].count; break;
+      case OLC_STAGE_TRACE: case OLC_STAGE_SHADE: case OLC_STAGE_RESTIR:
+        r.items = kc.queue_count[e.bounce];
+        r.misses = kc.miss_count[e.bounce];
+        break;
+      case OLC_STAGE_SHADOW: r.items = kc.shadow_count[e.bounce]; break;
+      default: r.items = resolved_pixels; break;
+    }
+    stage_ms[e.stage] += r.ms;
+    ctx->last_profile.push_back(r);
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->raygen_ms = stage_ms[OLC_STAGE_RAYGEN];
+    stats->trace_ms = stage_ms[OLC_STAGE_TRACE];
+    stats->restir_ms = stage_ms[OLC_STAGE_RESTIR];
+    stats->shade_ms = stage_ms[OLC_STAGE_SHADE];
+    stats->shadow_ms = stage_ms[OLC_STAGE_SHADOW];
+    stats->accumulate_ms = stage_ms[OLC_STAGE_ACCUMULATE] + stage_ms[OLC_STAGE_RESOLVE];
+    for (uint32_t c = 0; c < nchunks; ++c) {
+      const Counters& k = ctx->counters_host[c];
+      stats->camera_rays += k.queue_count[0];
+      for (uint32_t b = 1; b < plan.chunks[c].bounces; ++b) stats->extension_rays += k.queue_count[b];
+      for (uint32_t b = 0; b < plan.chunks[c].bounces; ++b) stats->shadow_rays += k.shadow_count[b];
+      stats->overflow += k.overflow;
+      stats->traversal_errors += k.traversal_errors;
+    }
+    OLC_CUDA(cudaEventElapsedTime(&stats->gpu_ms, ctx->ev_begin, ctx->ev_end));
+    stats->chunks = nchunks;
+  }
+}
+
+// Render the given jobs to completion as one run (plain frames and batches).
+void run_to_completion(olc_context* ctx, std::vector<QueuedJob*>& jobs, olc_render_stats* stats) {
+  uint64_t job_local = 0;
+  for (const QueuedJob* j : jobs)
+    if (j->rec.restir && j->job_local_reservoirs) job_local = std::max<uint64_t>(job_local, j->total);
+  RunPlan plan;
+  plan_run(jobs, plan_capacity(ctx, jobs), 0xffffffffu, job_local, plan);
+  if (plan.restir)
+    restir_prepare(ctx->restir, job_local + (plan.chunk_reservoirs ? plan.max_count : 0),
+                   std::max<uint32_t>(plan.max_count, 1), (uint32_t)plan.chunks.size());
+  execute_run(ctx, plan, stats);
+}
+
+void release_job(olc_context* ctx, QueuedJob& j) { ctx->pixels.release(j.pixels); }
+
+// Fill an olc_job into a queued job (validated; not yet admitted).
+void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
+  if (!d) throw Error(OLC_ERR_VALUE, "job is required");
+  check_camera(&d->camera);
+  check_size(d->width, d->height, d->samples_per_pixel);
+  if (d->max_bounces > OLC_MAX_BOUNCES) throw Error(OLC_ERR_VALUE, "max_bounces must be between 1 and 64");
+  scene_of(ctx, d->scene);
+  if (!d->out_rgba) throw Error(OLC_ERR_VALUE, "output pointer is required");
+  q.rec = make_job(ctx, &d->camera, d->width, d->height, d->samples_per_pixel, d->frame_index, d->max_bounces,
+                   d->scene);
+  q.total = (uint64_t)q.rec.npix * q.rec.spp;
+  q.out = d->out_rgba;
+  q.out_device = d->out_is_device != 0;
+}
+
+bool same_camera(const JobRec& a, const JobRec& b) {
+  auto same = [](const float4& x, const float4& y) { return x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w; };
+  return same(a.cam_pos, b.cam_pos) && same(a.cam_forward, b.cam_forward) && same(a.cam_right, b.cam_right) &&
+         same(a.cam_up, b.cam_up) && a.projection == b.projection;
 }
 
 }  // namespace
@@ -703,13 +1279,25 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     OLC_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     OLC_CUDA(cudaEventCreate(&ctx->ev_begin));
     OLC_CUDA(cudaEventCreate(&ctx->ev_end));
-    OLC_CUDA(cudaMallocHost(&ctx->fp_host, sizeof(FrameParams)));
-    std::memset(ctx->fp_host, 0, sizeof(FrameParams));
     configure_trace_kernels();
     apply_launch_shape(ctx.get());
+    // pool record 0: the identity instance that baked triangles report
+    ctx->identity_instance = ctx->instances.acquire(1, ctx->stream);
+    if (ctx->identity_instance.off != OLC_IDENTITY_INSTANCE) throw Error(OLC_ERR_RUNTIME, "instance pool is not empty");
+    InstanceRec id;
+    const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    fill_instance(id, identity);
+    id.blas_root = 0;
+    id.material = 0;
+    id.prim_offset = 0;
+    id.instance_id = 0xffffffffu;
+    id.flags = OLC_INSTANCE_FLATTENED;
+    upload_to(ctx->instances.at<InstanceRec>(0, OLC_IDENTITY_INSTANCE), &id, 1, ctx->stream);
+    sync_scene_table(ctx.get());
   });
   if (rc != OLC_OK) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = nullptr;
     return rc;
   }
   *out = ctx.release();
@@ -722,13 +1310,14 @@ int olc_destroy(olc_context* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graphs(ctx);
   restir_release(ctx->restir);
-  if (ctx->fp_host) cudaFreeHost(ctx->fp_host);
+  if (ctx->table_host) cudaFreeHost(ctx->table_host);
   if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
   for (cudaEvent_t e : ctx->tl_events) cudaEventDestroy(e);
   if (ctx->ev_begin) cudaEventDestroy(ctx->ev_begin);
   if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  cudaStream_t st = ctx->stream;
+  delete ctx;  // device buffers are freed here
+  if (st) cudaStreamDestroy(st);
   return OLC_OK;
 }
 
@@ -737,6 +1326,8 @@ int olc_reconfigure(olc_context* ctx, const olc_config* cfg) {
   return guarded(ctx, [&] {
     validate_config(*cfg);
     if (cfg->device != ctx->cfg.device) throw Error(OLC_ERR_RUNTIME, "changing the device requires a new renderer");
+    if (!ctx->served.empty() && (cfg->mode != ctx->cfg.mode || cfg->restir != ctx->cfg.restir))
+      throw Error(OLC_ERR_RUNTIME, "mode and ReSTIR cannot change while served jobs are queued");
     bool restir_changed = cfg->restir != ctx->cfg.restir || cfg->restir_candidates != ctx->cfg.restir_candidates;
     ctx->cfg = *cfg;
     apply_launch_shape(ctx);
@@ -748,18 +1339,70 @@ int olc_reconfigure(olc_context* ctx, const olc_config* cfg) {
 int olc_upload_scene(olc_context* ctx, const olc_scene_desc* scene) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    ScenePack fresh;
-    build_scene(ctx, scene, fresh);   // throws before touching the resident scene
-    OLC_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->scene = std::move(fresh);
-    drop_graphs(ctx);
+    const uint32_t old = ctx->default_scene;
+    if (old != kNoScene)
+      for (const auto& j : ctx->served)
+        if (j->rec.scene == old) throw Error(OLC_ERR_RUNTIME, "a queued job still renders the current scene");
+    const uint32_t handle = add_scene(ctx, scene);  // throws before touching the resident scene
+    ctx->default_scene = handle;
+    if (old != kNoScene) remove_scene(ctx, old);
     restir_reset(ctx->restir);
   });
 }
 
 int olc_scene_bytes(const olc_context* ctx, uint64_t* bytes) {
   if (!ctx || !bytes) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "context and output are required");
-  *bytes = ctx->scene.bytes;
+  *bytes = ctx->default_scene == kNoScene ? 0 : ctx->scenes[ctx->default_scene]->bytes;
+  return OLC_OK;
+}
+
+int olc_add_scene(olc_context* ctx, const olc_scene_desc* scene, uint32_t* handle) {
+  if (!ctx || !handle) return fail(ctx, OLC_ERR_VALUE, "context and handle output are required");
+  return guarded(ctx, [&] { *handle = add_scene(ctx, scene); });
+}
+
+int olc_remove_scene(olc_context* ctx, uint32_t handle) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] { remove_scene(ctx, handle); });
+}
+
+int olc_scene_stats_get(const olc_context* ctx, uint32_t handle, olc_scene_stats* stats) {
+  if (!ctx || !stats) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "context and output are required");
+  return guarded(const_cast<olc_context*>(ctx), [&] {
+    const ResidentScene& rs = scene_of(ctx, handle);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->bytes = rs.bytes;
+    stats->triangles = rs.triangles;
+    stats->blas_count = rs.blas_count;
+    stats->blas_nodes = rs.blas_nodes;
+    stats->tlas_nodes = rs.tlas_nodes;
+    stats->flattened_instances = rs.flattened;
+    stats->build_ms = rs.build_ms;
+  });
+}
+
+int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
+  if (!ctx || !info) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "context and output are required");
+  std::memset(info, 0, sizeof(*info));
+  for (const auto& s : ctx->scenes)
+    if (s) {
+      ++info->resident_scenes;
+      info->scene_bytes += s->bytes;
+    }
+  info->queued_jobs = (uint32_t)ctx->served.size();
+  info->pool_bytes = ctx->nodes.bytes() + ctx->slots.bytes() + ctx->instances.bytes() + ctx->materials.bytes() +
+                     ctx->emitters.bytes() + ctx->lights.bytes() + ctx->scene_table.bytes();
+  uint64_t wf = 0;
+  for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p,
+                                &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
+                                &ctx->ps_rad, &ctx->ps_meta, &ctx->table_dev, &ctx->prod_depth, &ctx->prod_normal,
+                                &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->restir.res_a0,
+                                &ctx->restir.res_a1, &ctx->restir.res_b0, &ctx->restir.res_b1, &ctx->restir.hist0,
+                                &ctx->restir.hist1, &ctx->restir.selected, &ctx->restir.hit_list})
+    wf += b->bytes();
+  info->wavefront_bytes = wf;
+  info->pixel_bytes = ctx->pixels.bytes();
+  info->pixel_bytes_used = ctx->pixels.ranges.used() * (ctx->pixels.elem[0] + ctx->pixels.elem[1]);
   return OLC_OK;
 }
 
@@ -767,111 +1410,188 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
                uint32_t frame_index, float* out_rgba, int out_is_device, olc_render_stats* stats) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    if (!camera) throw Error(OLC_ERR_VALUE, "camera is required");
-    if (width == 0 || height == 0) throw Error(OLC_ERR_VALUE, "width and height must be positive");
-    if ((uint64_t)width * height > (1ull << 28)) throw Error(OLC_ERR_VALUE, "image is too large");
-    if (spp < 1 || spp > 65536) throw Error(OLC_ERR_VALUE, "samples must be between 1 and 65536");
-    if (camera->projection > 2) throw Error(OLC_ERR_VALUE, "unknown camera projection");
-    if (!ctx->scene.valid) throw Error(OLC_ERR_RUNTIME, "no scene is resident; upload a scene first");
+    check_camera(camera);
+    check_size(width, height, spp);
+    const ResidentScene& rs = default_scene(ctx);
+    (void)rs;
     if (!out_rgba) throw Error(OLC_ERR_VALUE, "output pointer is required");
-    const uint32_t npix = width * height;
-    uint32_t cap = choose_capacity(ctx, npix, spp);
-    ensure_wavefront(ctx, cap, npix);
-    uint64_t total = (uint64_t)npix * spp;
-    uint32_t chunks = (uint32_t)((total + ctx->capacity - 1) / ctx->capacity);
-    ensure_host_counters(ctx, chunks);
-    fill_frame(ctx, camera, width, height, spp, frame_index);
-    if (ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION)
-      restir_prepare(ctx->restir, ctx->cfg, width, height, spp, frame_index, ctx->capacity, *ctx->fp_host);
-    cudaStream_t st = ctx->stream;
-    OLC_CUDA(cudaMemcpyAsync(ctx->fp_dev.get(), ctx->fp_host, sizeof(FrameParams), cudaMemcpyHostToDevice, st));
-    bool products = true;
-    OLC_CUDA(cudaEventRecord(ctx->ev_begin, st));
-    bool use_graph = ctx->cfg.use_graphs != 0 && !(ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION);
-    if (use_graph) {
-      GraphKey key{width, height, spp};
-      auto it = ctx->graphs.find(key);
-      if (it == ctx->graphs.end()) {
-        cudaGraph_t g;
-        OLC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        ctx->capturing = true;
-        try {
-          record_frame(ctx, width, height, spp, products);
-        } catch (...) {
-          ctx->capturing = false;
-          cudaStreamEndCapture(st, &g);
-          if (g) cudaGraphDestroy(g);
-          throw;
-        }
-        ctx->capturing = false;
-        OLC_CUDA(cudaStreamEndCapture(st, &g));
-        cudaGraphExec_t exec;
-        cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
-        cudaGraphDestroy(g);
-        OLC_CUDA(e);
-        it = ctx->graphs.emplace(key, exec).first;
-        ctx->graph_timelines[key] = ctx->tl_entries;
-      }
-      ctx->tl_entries = ctx->graph_timelines[key];
-      OLC_CUDA(cudaGraphLaunch(it->second, st));
-    } else {
-      record_frame(ctx, width, height, spp, products);
+    QueuedJob job;
+    job.rec = make_job(ctx, camera, width, height, spp, frame_index, 0, ctx->default_scene);
+    job.rec.products = 1;
+    job.total = (uint64_t)job.rec.npix * spp;
+    job.out = out_rgba;
+    job.out_device = out_is_device != 0;
+    const bool restir = job.rec.restir != 0;
+    // the frame's reservoirs live at job-local indices, where the next frame's
+    // temporal pass finds them; the history survives only if the reservoir
+    // buffers need not grow for this frame
+    RestirState& rst = ctx->restir;
+    const bool history = restir && ctx->cfg.restir_temporal && rst.history_valid && rst.hist_w == width &&
+                         rst.hist_h == height && rst.hist_spp == spp && rst.hist_frame + 1u == frame_index &&
+                         rst.hist_scene == ctx->default_scene && same_camera(job.rec, rst.hist_camera) &&
+                         job.total <= rst.reservoirs;
+    job.job_local_reservoirs = restir;
+    job.rec.history = history ? 1u : 0u;
+    job.rec.reservoir_base = 0;
+    job.rec.history_base = 0;
+    ensure_products(ctx, job.rec.npix);
+    admit_job(ctx, job);
+    std::vector<QueuedJob*> jobs{&job};
+    try {
+      run_to_completion(ctx, jobs, stats);
+    } catch (...) {
+      release_job(ctx, job);
+      throw;
     }
-    OLC_CUDA(cudaEventRecord(ctx->ev_end, st));
-    if (out_is_device) {
-      OLC_CUDA(cudaMemcpyAsync(out_rgba, ctx->out_dev.get(), (size_t)npix * 16, cudaMemcpyDeviceToDevice, st));
-    } else {
-      OLC_CUDA(cudaMemcpyAsync(out_rgba, ctx->out_dev.get(), (size_t)npix * 16, cudaMemcpyDeviceToHost, st));
-    }
-    OLC_CUDA(cudaStreamSynchronize(st));
+    release_job(ctx, job);
     ctx->last_w = width;
     ctx->last_h = height;
-    if (ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION) restir_finish(ctx->restir);
-    // per-launch device timeline
-    ctx->last_profile.clear();
-    float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (size_t k = 0; k < ctx->tl_entries.size(); ++k) {
-      const TimelineEntry& e = ctx->tl_entries[k];
-      olc_launch_record r{};
-      r.stage = e.stage;
-      r.bounce = e.bounce;
-      r.chunk = e.chunk;
-      OLC_CUDA(cudaEventElapsedTime(&r.ms, ctx->tl_events[k], ctx->tl_events[k + 1]));
-      const Counters& kc = ctx->counters_host[std::min<uint32_t>(e.chunk, chunks - 1)];
-      uint64_t chunk_count = std::min<uint64_t>(ctx->capacity, total - (uint64_t)e.chunk * ctx->capacity);
-      switch (e.stage) {
-        case OLC_STAGE_RAYGEN: case OLC_STAGE_ACCUMULATE: r.items = chunk_count; break;
-        case OLC_STAGE_TRACE: case OLC_STAGE_SHADE: case OLC_STAGE_RESTIR:
-          r.items = kc.queue_count[e.bounce];
-          r.misses = kc.miss_count[e.bounce];
-          break;
-        case OLC_STAGE_SHADOW: r.items = kc.shadow_count[e.bounce]; break;
-        default: r.items = npix; break;
-      }
-      stage_ms[e.stage] += r.ms;
-      ctx->last_profile.push_back(r);
+    if (restir) {
+      restir_finish(rst);
+      rst.history_valid = true;
+      rst.history_used = history;
+      rst.hist_w = width;
+      rst.hist_h = height;
+      rst.hist_spp = spp;
+      rst.hist_frame = frame_index;
+      rst.hist_scene = ctx->default_scene;
+      rst.hist_camera = job.rec;
     }
-    if (stats) {
-      std::memset(stats, 0, sizeof(*stats));
-      stats->raygen_ms = stage_ms[OLC_STAGE_RAYGEN];
-      stats->trace_ms = stage_ms[OLC_STAGE_TRACE];
-      stats->restir_ms = stage_ms[OLC_STAGE_RESTIR];
-      stats->shade_ms = stage_ms[OLC_STAGE_SHADE];
-      stats->shadow_ms = stage_ms[OLC_STAGE_SHADOW];
-      stats->accumulate_ms = stage_ms[OLC_STAGE_ACCUMULATE] + stage_ms[OLC_STAGE_RESOLVE];
-      for (uint32_t c = 0; c < chunks; ++c) {
-        const Counters& k = ctx->counters_host[c];
-        stats->camera_rays += k.queue_count[0];
-        for (uint32_t b = 1; b < ctx->cfg.max_bounces; ++b) stats->extension_rays += k.queue_count[b];
-        for (uint32_t b = 0; b < ctx->cfg.max_bounces; ++b) stats->shadow_rays += k.shadow_count[b];
-        stats->overflow += k.overflow;
-        stats->traversal_errors += k.traversal_errors;
+    if (stats) stats->restir_history_used = (restir && rst.history_used) ? 1u : 0u;
+  });
+}
+
+int olc_render_batch(olc_context* ctx, const olc_job* jobs, uint32_t num_jobs, olc_render_stats* stats) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (num_jobs == 0) {
+      if (stats) std::memset(stats, 0, sizeof(*stats));
+      return;
+    }
+    if (!jobs) throw Error(OLC_ERR_VALUE, "jobs are required");
+    std::vector<QueuedJob> q(num_jobs);
+    for (uint32_t i = 0; i < num_jobs; ++i) job_from_desc(ctx, &jobs[i], q[i]);
+    std::vector<QueuedJob*> ptrs;
+    try {
+      for (QueuedJob& j : q) {
+        admit_job(ctx, j);
+        ptrs.push_back(&j);
       }
-      OLC_CUDA(cudaEventElapsedTime(&stats->gpu_ms, ctx->ev_begin, ctx->ev_end));
-      stats->chunks = chunks;
-      stats->restir_history_used = ctx->restir.history_used ? 1u : 0u;
+      run_to_completion(ctx, ptrs, stats);
+    } catch (...) {
+      for (QueuedJob* j : ptrs) release_job(ctx, *j);
+      throw;
+    }
+    for (QueuedJob* j : ptrs) release_job(ctx, *j);
+  });
+}
+
+int olc_job_bytes(const olc_context* ctx, const olc_job* job, uint64_t* bytes) {
+  if (!ctx || !job || !bytes) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "arguments are required");
+  *bytes = (uint64_t)job->width * job->height * (ctx->pixels.elem[0] + ctx->pixels.elem[1]);
+  return OLC_OK;
+}
+
+int olc_submit(olc_context* ctx, const olc_job* job, uint64_t* ticket) {
+  if (!ctx || !ticket) return fail(ctx, OLC_ERR_VALUE, "context and ticket output are required");
+  return guarded(ctx, [&] {
+    std::unique_ptr<QueuedJob> q(new QueuedJob());
+    job_from_desc(ctx, job, *q);
+    admit_job(ctx, *q);
+    q->ticket = ctx->next_ticket++;
+    *ticket = q->ticket;
+    ctx->served.push_back(std::move(q));
+  });
+}
+
+int olc_cancel(olc_context* ctx, uint64_t ticket) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    for (auto it = ctx->served.begin(); it != ctx->served.end(); ++it) {
+      if ((*it)->ticket != ticket) continue;
+      release_job(ctx, **it);
+      ctx->served.erase(it);
+      return;
+    }
+    throw Error(OLC_ERR_VALUE, "unknown or completed ticket");
+  });
+}
+
+int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uint32_t* num_done,
+                   olc_render_stats* stats) {
+  if (!ctx || !num_done) return fail(ctx, OLC_ERR_VALUE, "context and num_done are required");
+  return guarded(ctx, [&] {
+    *num_done = 0;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (ctx->served.empty()) return;
+    std::vector<QueuedJob*> jobs;
+    std::vector<uint64_t> issued_before;
+    for (auto& j : ctx->served) {
+      jobs.push_back(j.get());
+      issued_before.push_back(j->issued);
+    }
+    // Shortest remaining work first, so small requests finish inside the
+    // chunks of large ones instead of queueing behind them; a job passed
+    // over for kMaxWaitSteps steps goes first.  The order changes no image.
+    std::stable_sort(jobs.begin(), jobs.end(), [](const QueuedJob* a, const QueuedJob* b) {
+      const bool sa = a->waited >= kMaxWaitSteps, sb = b->waited >= kMaxWaitSteps;
+      if (sa != sb) return sa;
+      return a->total - a->issued < b->total - b->issued;
+    });
+    RunPlan plan;
+    plan_run(jobs, plan_capacity(ctx, jobs), 1, 0, plan);
+    if (plan.finished.size() > done_capacity) {
+      for (size_t k = 0; k < jobs.size(); ++k) jobs[k]->issued = issued_before[k];
+      throw Error(OLC_ERR_VALUE, "done_capacity is smaller than the number of jobs this step completes");
+    }
+    if (plan.restir)
+      restir_prepare(ctx->restir, plan.max_count, std::max<uint32_t>(plan.max_count, 1),
+                     (uint32_t)plan.chunks.size());
+    try {
+      execute_run(ctx, plan, stats);
+    } catch (...) {
+      // the chunk's jobs hold partial samples of a failed chunk: drop them
+      size_t k = 0;
+      for (auto it = ctx->served.begin(); it != ctx->served.end(); ++k) {
+        if ((*it)->issued != issued_before[k]) {
+          release_job(ctx, **it);
+          it = ctx->served.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      throw;
+    }
+    for (QueuedJob* j : plan.finished) done[(*num_done)++] = j->ticket;
+    {
+      size_t k = 0;
+      for (auto& j : ctx->served) {
+        j->waited = j->issued == issued_before[k] ? j->waited + 1 : 0;
+        ++k;
+      }
+    }
+    for (auto it = ctx->served.begin(); it != ctx->served.end();) {
+      if ((*it)->issued == (*it)->total) {
+        release_job(ctx, **it);
+        it = ctx->served.erase(it);
+      } else {
+        ++it;
+      }
     }
   });
+}
+
+int olc_queued_jobs(const olc_context* ctx, uint64_t* tickets, uint32_t capacity, uint32_t* count) {
+  if (!ctx || !count) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "context and count are required");
+  *count = (uint32_t)ctx->served.size();
+  if (tickets) {
+    uint32_t n = 0;
+    for (const auto& j : ctx->served) {
+      if (n == capacity) break;
+      tickets[n++] = j->ticket;
+    }
+  }
+  return OLC_OK;
 }
 
 int olc_frame_profile(const olc_context* ctx, olc_launch_record* records, uint32_t capacity, uint32_t* count) {
@@ -894,7 +1614,7 @@ int olc_read_products(olc_context* ctx, uint32_t width, uint32_t height, float* 
                       uint32_t* instance_id, uint32_t* material_id, uint32_t* primitive_id) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    if (width != ctx->last_w || height != ctx->last_h)
+    if (width != ctx->last_w || height != ctx->last_h || ctx->last_w == 0)
       throw Error(OLC_ERR_VALUE, "products are available only for the size of the last render");
     const size_t n = (size_t)width * height;
     cudaStream_t st = ctx->stream;
@@ -926,13 +1646,13 @@ int olc_trace_closest(olc_context* ctx, uint32_t n, const float* origins, const 
                       uint32_t* instance_id, int32_t* primitive, float* t, float* barycentrics) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    if (!ctx->scene.valid) throw Error(OLC_ERR_RUNTIME, "no scene is resident");
+    const ResidentScene& rs = default_scene(ctx);
     if (n == 0) return;
     if (!origins || !directions) throw Error(OLC_ERR_VALUE, "origins and directions are required");
     if (!ctx->counters.get()) ctx->counters.allocate(sizeof(Counters));
     OLC_CUDA(cudaMemsetAsync(ctx->counters.get(), 0, sizeof(Counters), ctx->stream));
-    launch_trace_rays(ctx->ls, ctx->scene.view, n, origins, directions, t_min, instance_id, primitive, t,
-                      barycentrics, ctx->counters.as<Counters>(), ctx->stream);
+    launch_trace_rays(ctx->ls, pool_view(ctx), rs.rec.tlas_root, n, origins, directions, t_min, instance_id,
+                      primitive, t, barycentrics, ctx->counters.as<Counters>(), ctx->stream);
     Counters h;
     OLC_CUDA(cudaMemcpyAsync(&h, ctx->counters.get(), sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
     OLC_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -944,12 +1664,12 @@ int olc_trace_occluded(olc_context* ctx, uint32_t n, const float* origins, const
                        const float* t_max, uint8_t* occluded) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    if (!ctx->scene.valid) throw Error(OLC_ERR_RUNTIME, "no scene is resident");
+    const ResidentScene& rs = default_scene(ctx);
     if (n == 0) return;
     if (!origins || !directions || !t_max || !occluded) throw Error(OLC_ERR_VALUE, "all arrays are required");
     if (!ctx->counters.get()) ctx->counters.allocate(sizeof(Counters));
     OLC_CUDA(cudaMemsetAsync(ctx->counters.get(), 0, sizeof(Counters), ctx->stream));
-    launch_occluded_rays(ctx->ls, ctx->scene.view, n, origins, directions, t_min, t_max, occluded,
+    launch_occluded_rays(ctx->ls, pool_view(ctx), rs.rec.tlas_root, n, origins, directions, t_min, t_max, occluded,
                          ctx->counters.as<Counters>(), ctx->stream);
     OLC_CUDA(cudaStreamSynchronize(ctx->stream));
   });
@@ -959,14 +1679,13 @@ int olc_camera_rays(olc_context* ctx, const olc_camera* camera, uint32_t width, 
                     uint32_t frame_index, const float* jitter_override, float* origins, float* directions) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] {
-    if (!camera || !origins || !directions) throw Error(OLC_ERR_VALUE, "camera and outputs are required");
+    check_camera(camera);
+    if (!origins || !directions) throw Error(OLC_ERR_VALUE, "camera and outputs are required");
     if (width == 0 || height == 0) throw Error(OLC_ERR_VALUE, "width and height must be positive");
-    if (!ctx->fp_dev.get()) ctx->fp_dev.allocate(sizeof(FrameParams));
-    fill_frame(ctx, camera, width, height, 1, frame_index);
-    OLC_CUDA(cudaMemcpyAsync(ctx->fp_dev.get(), ctx->fp_host, sizeof(FrameParams), cudaMemcpyHostToDevice,
-                             ctx->stream));
-    launch_camera_rays(ctx->ls, ctx->fp_dev.as<FrameParams>(), sample, jitter_override, origins, directions,
-                       ctx->stream);
+    if (!ctx->job_dev.get()) ctx->job_dev.allocate(sizeof(JobRec));
+    JobRec job = make_job(ctx, camera, width, height, 1, frame_index, 0, kNoScene);
+    OLC_CUDA(cudaMemcpyAsync(ctx->job_dev.get(), &job, sizeof(JobRec), cudaMemcpyHostToDevice, ctx->stream));
+    launch_camera_rays(ctx->ls, ctx->job_dev.as<JobRec>(), sample, jitter_override, origins, directions, ctx->stream);
     OLC_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
@@ -1000,19 +1719,21 @@ int olc_radix_sort_pairs(olc_context* ctx, uint32_t n, uint32_t key_bits, uint32
 int olc_bvh_info_get(const olc_context* ctx, olc_bvh_info* info) {
   if (!ctx || !info) return fail(const_cast<olc_context*>(ctx), OLC_ERR_VALUE, "context and output are required");
   std::memset(info, 0, sizeof(*info));
-  info->blas_count = ctx->scene.blas_count;
-  info->blas_nodes = ctx->scene.blas_nodes;
-  info->tlas_nodes = ctx->scene.tlas_nodes;
-  info->triangles = ctx->scene.total_triangles;
-  info->build_ms = ctx->scene.build_ms;
+  if (ctx->default_scene == kNoScene) return OLC_OK;
+  const ResidentScene& rs = *ctx->scenes[ctx->default_scene];
+  info->blas_count = rs.blas_count;
+  info->blas_nodes = rs.blas_nodes;
+  info->tlas_nodes = rs.tlas_nodes;
+  info->triangles = rs.triangles;
+  info->build_ms = rs.build_ms;
   return OLC_OK;
 }
 
 int olc_bvh_validate(olc_context* ctx, uint64_t* bad) {
   if (!ctx || !bad) return fail(ctx, OLC_ERR_VALUE, "context and output are required");
   return guarded(ctx, [&] {
-    if (!ctx->scene.valid) throw Error(OLC_ERR_RUNTIME, "no scene is resident");
-    *bad = validate_bvh(ctx->scene.view, ctx->scene.blas_ranges, ctx->stream);
+    const ResidentScene& rs = default_scene(ctx);
+    *bad = validate_bvh(pool_view(ctx), rs.blas_ranges, ctx->stream);
   });
 }
 

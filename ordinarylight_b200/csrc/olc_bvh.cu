@@ -276,14 +276,25 @@ __global__ void k_bottom_up(int n, const int* __restrict__ left, const int* __re
   }
 }
 
+// TLAS leaf of build primitive p: primitives [0, n_inst) are instances
+// (global instance index inst_base + p), the rest baked world-space triangles
+// (global slot flat_base + p - n_inst).
+struct TlasRefs {
+  uint32_t n_inst = 0, inst_base = 0, flat_base = 0;
+};
+OLC_D int tlas_leaf(const TlasRefs& r, uint32_t p) {
+  return p < r.n_inst ? olc_make_leaf(r.inst_base + p, OLC_TLAS_LEAF_INSTANCE)
+                      : olc_make_leaf(r.flat_base + (p - r.n_inst), OLC_TLAS_LEAF_TRIANGLE);
+}
+
 // Emit final nodes.  blas: leaves reference slot ranges (collapse subtrees of
-// at most leaf_max leaves); tlas: leaves reference instance indices.
+// at most leaf_max leaves); tlas: one instance or baked triangle per leaf.
 __global__ void k_emit_nodes(int n, const int* __restrict__ left, const int* __restrict__ right,
                              const int* __restrict__ first, const int* __restrict__ last,
                              const float4* __restrict__ leaf_lo, const float4* __restrict__ leaf_hi,
                              const float4* __restrict__ node_lo, const float4* __restrict__ node_hi,
-                             const uint32_t* __restrict__ sorted_vals, int is_tlas, uint32_t leaf_max,
-                             BvhNode* nodes, uint32_t node_base, uint32_t slot_base) {
+                             const uint32_t* __restrict__ sorted_vals, int is_tlas, TlasRefs tr,
+                             uint32_t leaf_max, BvhNode* nodes, uint32_t node_base, uint32_t slot_base) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   int ch[2] = {left[i], right[i]};
@@ -295,7 +306,7 @@ __global__ void k_emit_nodes(int n, const int* __restrict__ left, const int* __r
       int leaf = ~c;
       lo[s] = leaf_lo[leaf];
       hi[s] = leaf_hi[leaf];
-      ref[s] = is_tlas ? olc_make_leaf(sorted_vals[leaf], 1u) : olc_make_leaf(slot_base + (uint32_t)leaf, 1u);
+      ref[s] = is_tlas ? tlas_leaf(tr, sorted_vals[leaf]) : olc_make_leaf(slot_base + (uint32_t)leaf, 1u);
     } else {
       lo[s] = node_lo[c];
       hi[s] = node_hi[c];
@@ -313,8 +324,9 @@ __global__ void k_emit_nodes(int n, const int* __restrict__ left, const int* __r
 }
 
 // A structure with a single primitive: one node, child 1 empty.
-__global__ void k_single_leaf_node(const float4* lo, const float4* hi, int is_tlas, const uint32_t* sorted_vals,
-                                   BvhNode* nodes, uint32_t node_base, uint32_t slot_base, uint32_t n) {
+__global__ void k_single_leaf_node(const float4* lo, const float4* hi, int is_tlas, TlasRefs tr,
+                                   const uint32_t* sorted_vals, BvhNode* nodes, uint32_t node_base,
+                                   uint32_t slot_base, uint32_t n) {
   BvhNode nd;
   if (n == 0) {
     const float inf = CUDART_INF_F;
@@ -327,7 +339,7 @@ __global__ void k_single_leaf_node(const float4* lo, const float4* hi, int is_tl
     nd.a = make_float4(lo[0].x, hi[0].x, lo[0].y, hi[0].y);
     nd.b = make_float4(inf, -inf, inf, -inf);
     nd.c = make_float4(lo[0].z, hi[0].z, inf, -inf);
-    nd.d = make_int4(is_tlas ? olc_make_leaf(sorted_vals[0], 1u) : olc_make_leaf(slot_base, 1u),
+    nd.d = make_int4(is_tlas ? tlas_leaf(tr, sorted_vals[0]) : olc_make_leaf(slot_base, 1u),
                      OLC_EMPTY_CHILD, 0, 0);
   }
   nodes[node_base] = nd;
@@ -416,15 +428,15 @@ __global__ void __launch_bounds__(256) k_instance_boxes(const float* __restrict_
 inline uint32_t blocks_for(uint64_t n, int threads = kThreads) { return (uint32_t)((n + threads - 1) / threads); }
 
 // Common tail of a BLAS/TLAS build after boxes and centres exist.
-uint32_t build_hierarchy(uint32_t n, BuildScratch& sc, int is_tlas, uint32_t leaf_max, BvhNode* nodes,
-                         uint32_t node_base, uint32_t slot_base, cudaStream_t stream) {
+uint32_t build_hierarchy(uint32_t n, BuildScratch& sc, int is_tlas, const TlasRefs& tr, uint32_t leaf_max,
+                         BvhNode* nodes, uint32_t node_base, uint32_t slot_base, cudaStream_t stream) {
   if (n <= 1) {
     if (n == 1) {
       // sorted order is the identity
       uint32_t zero = 0;
       OLC_CUDA(cudaMemcpyAsync(sc.vals.as<uint32_t>(), &zero, sizeof(zero), cudaMemcpyHostToDevice, stream));
     }
-    k_single_leaf_node<<<1, 1, 0, stream>>>(sc.boxes_lo.as<float4>(), sc.boxes_hi.as<float4>(), is_tlas,
+    k_single_leaf_node<<<1, 1, 0, stream>>>(sc.boxes_lo.as<float4>(), sc.boxes_hi.as<float4>(), is_tlas, tr,
                                             sc.vals.as<uint32_t>(), nodes, node_base, slot_base, n);
     OLC_LAUNCH_CHECK("k_single_leaf_node");
     OLC_CUDA(cudaStreamSynchronize(stream));
@@ -455,7 +467,7 @@ uint32_t build_hierarchy(uint32_t n, BuildScratch& sc, int is_tlas, uint32_t lea
   k_emit_nodes<<<blocks_for(n - 1), kThreads, 0, stream>>>(
       (int)n, sc.left.as<int>(), sc.right.as<int>(), sc.first.as<int>(), sc.last.as<int>(),
       sc.sorted_lo.as<float4>(), sc.sorted_hi.as<float4>(), sc.node_lo.as<float4>(), sc.node_hi.as<float4>(),
-      sc.vals.as<uint32_t>(), is_tlas, leaf_max, nodes, node_base, slot_base);
+      sc.vals.as<uint32_t>(), is_tlas, tr, leaf_max, nodes, node_base, slot_base);
   OLC_LAUNCH_CHECK("k_emit_nodes");
   return node_base;  // Karras root is internal node 0
 }
@@ -547,7 +559,7 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
                                                                sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
     OLC_LAUNCH_CHECK("k_triangle_boxes");
   }
-  uint32_t root = build_hierarchy(n, sc, 0, leaf_max, nodes, node_base, slot_base, stream);
+  uint32_t root = build_hierarchy(n, sc, 0, TlasRefs{}, leaf_max, nodes, node_base, slot_base, stream);
   if (n > 0) {
     k_reorder_triangles<<<blocks_for(n), kThreads, 0, stream>>>(sc.vals.as<uint32_t>(), n, d.vertices, d.normals,
                                                                   d.indices, tri_verts, tri_normals, tri_index,
@@ -557,9 +569,9 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
   return root;
 }
 
-uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, const float4* tri_verts,
-                    const float4* flat_verts, uint32_t n_flat, BuildScratch& sc, BvhNode* nodes, uint32_t node_base,
-                    cudaStream_t stream) {
+uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint32_t instance_base,
+                    const float4* tri_verts, const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base,
+                    BuildScratch& sc, BvhNode* nodes, uint32_t node_base, cudaStream_t stream) {
   const uint32_t total = n + n_flat;
   sc.ensure(std::max<uint32_t>(total, 1u));
   if (n > 0) {
@@ -572,7 +584,11 @@ uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, cons
         flat_verts, n_flat, sc.boxes_lo.as<float4>() + n, sc.boxes_hi.as<float4>() + n, sc.centers.as<float4>() + n);
     OLC_LAUNCH_CHECK("k_flat_triangle_boxes");
   }
-  return build_hierarchy(total, sc, 1, 1, nodes, node_base, 0, stream);
+  TlasRefs tr;
+  tr.n_inst = n;
+  tr.inst_base = instance_base;
+  tr.flat_base = flat_slot_base;
+  return build_hierarchy(total, sc, 1, tr, 1, nodes, node_base, 0, stream);
 }
 
 // ---- validation ----------------------------------------------------------

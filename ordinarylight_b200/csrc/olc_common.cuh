@@ -202,45 +202,62 @@ struct __align__(16) LightRec {
   float4 spot;
 };
 
-struct SceneView;
 // The instance that owns a hit's material and identity: the hit instance
-// itself, or for the flattened mesh the original instance of the triangle.
+// itself, or for a baked world-space triangle the original instance.
 OLC_D uint32_t owner_instance(const InstanceRec* instances, const uint32_t* tri_owner, uint32_t inst, uint32_t slot) {
   return (instances[inst].flags & OLC_INSTANCE_FLATTENED) ? tri_owner[slot] : inst;
 }
 
+// Pool record 0 is an identity transform flagged OLC_INSTANCE_FLATTENED:
+// hits on baked world-space triangles report it as their instance.
+#define OLC_IDENTITY_INSTANCE 0u
+
+// TLAS leaf kinds (the leaf's count field): an instance (first = global
+// instance record) or a baked world-space triangle (first = global slot).
+#define OLC_TLAS_LEAF_INSTANCE 1u
+#define OLC_TLAS_LEAF_TRIANGLE 2u
+
+// One resident scene of the pool: its TLAS root and its lighting.  Emitter
+// indices of the alias table are scene-local (add emitter_base).
+struct __align__(16) SceneRec {
+  uint32_t tlas_root;
+  uint32_t emitter_base;
+  uint32_t num_emitters;
+  float emissive_weight;       // Scene.emissive_light_weight
+  uint32_t light_base;
+  uint32_t num_lights;
+  uint32_t env_kind;           // olc_environment_kind
+  float env_rotation;
+  float4 env_color;            // colour * intensity
+  const float* env_image;      // equirect RGB
+  uint32_t env_w, env_h;
+  const float* volume;         // density grid (z, y, x)
+  uint32_t volume_present;
+  uint32_t vol_nx, vol_ny, vol_nz;
+  float4 vol_w2b0, vol_w2b1, vol_w2b2;   // world -> unit box
+  float vol_sigma_t_scale;
+  float vol_albedo;
+  float vol_max_density;
+  uint32_t pad;
+};
+
+// Device view of the scene pool shared by every resident scene: all BLAS and
+// TLAS nodes, triangle slots, instances, materials, emitters and lights of
+// all scenes live in one set of arrays, so a wavefront may mix rays of
+// different scenes and each ray needs only its scene's TLAS root.
 struct SceneView {
-  const BvhNode* nodes;          // BLAS and TLAS nodes, one pool
+  const BvhNode* nodes;          // BLAS and TLAS nodes
   const float4* tri_verts;       // 3 float4 per triangle slot (object space)
   const float4* tri_normals;     // 3 float4 per triangle slot (object space)
-  const uint32_t* tri_index;     // slot -> mesh-local triangle index (packed index in the flattened mesh)
-  const uint32_t* tri_owner;     // slot -> original instance (flattened mesh only)
+  const uint32_t* tri_index;     // slot -> mesh-local triangle index (packed index for baked triangles)
+  const uint32_t* tri_owner;     // slot -> original instance (baked triangles only)
   const InstanceRec* instances;
   const MaterialRec* materials;
   const MaterialAux* material_aux;
   const EmitterRec* emitters;
   const AliasEntry* emitter_alias;
   const LightRec* lights;
-  const float* env_image;        // equirect RGB
-  const float* volume;           // density grid
-  uint32_t tlas_root;
-  uint32_t tlas_instances;       // TLAS leaf payloads below this are instances
-  uint32_t flat_slot_base;       // ... the rest are world-space triangle slots from here
-  uint32_t flat_instance;        // identity record reported for direct triangles
-  uint32_t num_instances;
-  uint32_t num_emitters;
-  uint32_t num_lights;
-  float emissive_weight;
-  uint32_t env_kind;
-  float3 env_color;
-  float env_rotation;
-  uint32_t env_w, env_h;
-  uint32_t volume_present;
-  uint32_t vol_nx, vol_ny, vol_nz;
-  Affine vol_world_to_box;
-  float vol_sigma_t_scale;
-  float vol_albedo;
-  float vol_max_density;
+  const SceneRec* scenes;
 };
 
 // ---------------------------------------------------------------------------
@@ -248,7 +265,7 @@ struct SceneView {
 // ---------------------------------------------------------------------------
 struct RayQueue {
   float4* origin_tmin;     // origin.xyz, t_min
-  float4* dir_tmax;        // direction.xyz, t_max
+  float4* dir_root;        // direction.xyz, TLAS root of the ray's scene (bits); t_max is infinite
   uint32_t* path;          // path slot
 };
 
@@ -260,7 +277,7 @@ struct HitBuf {
 struct ShadowQueue {
   float4* origin_tmax;     // origin.xyz, t_max
   float4* dir_path;        // direction.xyz, path slot bits
-  float4* contrib;         // unoccluded contribution rgb
+  float4* contrib_root;    // unoccluded contribution rgb, TLAS root (bits)
 };
 
 struct PathState {
@@ -280,9 +297,13 @@ struct PathState {
 #define OLC_ACCUM_SCALE 268435456.0f
 #define OLC_SAMPLE_CLAMP 1.0e7f
 
-// Per-frame parameters, read by every wavefront kernel from device memory so
-// a captured graph can be replayed for a new frame after one copy.
-struct FrameParams {
+// One segment of a render job inside a chunk: the job's camera, image,
+// samples, transport knobs and scene, plus where this segment's paths sit in
+// the chunk and where the job's pixels and reservoirs live.  Every wavefront
+// kernel reads its paths' records from device memory, so a plain frame is a
+// chunk sequence over one job, batches and served requests mix many, and a
+// captured graph replays for new cameras and mixes after one table copy.
+struct __align__(16) JobRec {
   float4 cam_pos;          // xyz, x scale (aspect*half_height | half horizontal angle)
   float4 cam_forward;      // xyz, y scale (half_height | half vertical angle)
   float4 cam_right;        // xyz, 0
@@ -293,11 +314,45 @@ struct FrameParams {
   uint32_t frame;          // seed + frame_index
   uint32_t npix;
   uint32_t max_bounces;
-  uint32_t mode;
+  uint32_t mode;           // olc_mode
   uint32_t rr_start;
   float rr_min_survival;
-  uint32_t restir;
-  uint32_t nee;            // next-event estimation on (production mode)
+  uint32_t restir;         // ReSTIR DI at the primary vertex
+  uint32_t nee;            // next-event estimation (production mode)
+  uint32_t scene;          // SceneRec index
+  uint32_t history;        // ReSTIR temporal history valid for this job
+  uint32_t products;       // write first-sample primary-hit products
+  uint32_t pad;
+  unsigned long long seg_begin;       // chunk-local index of the segment's first path
+  unsigned long long seg_first;       // job-local index (sample * npix + pixel) of that path
+  unsigned long long pixel_base;      // first pixel of the job in the accumulator and outputs
+  unsigned long long reservoir_base;  // reservoir of (sample, pixel) = base + sample * npix + pixel (mod 2^64)
+  unsigned long long history_base;    // first reservoir of its temporal history
+};
+
+// Header of one chunk's table in device memory, followed by num_segments
+// JobRec entries ordered by seg_begin.  The kernels read the path count from
+// here rather than from launch parameters, so one captured graph serves every
+// chunk with the same bounce count.
+//
+// ReSTIR reservoirs carry the stamp of the chunk that wrote them; stamps grow
+// by one per chunk, so a reservoir is this chunk's only if its stamp equals
+// `stamp`, and the previous plain frame's (its chunks' stamps form a range)
+// only if its stamp lies in [history_first, history_last].
+struct __align__(16) ChunkHeader {
+  uint32_t count;          // paths in the chunk
+  uint32_t num_segments;
+  uint32_t stamp;          // ReSTIR validity stamp of this chunk
+  uint32_t history_first;  // stamps of the temporal history's reservoirs
+  uint32_t history_last;
+  uint32_t pad[3];
+};
+
+// Jobs whose last paths finished in a run: resolved from the accumulator.
+struct __align__(16) ResolveEntry {
+  unsigned long long pixel_base;
+  uint32_t npix;
+  uint32_t spp;
 };
 
 // Work counters kept in device memory, zeroed once per chunk.

@@ -110,12 +110,14 @@ inline uint32_t blas_node_count(uint32_t nt) { return nt > 1 ? nt - 1 : 1; }
 
 // Build the TLAS over n instances (world boxes computed from BLAS roots) and
 // n_flat world-space triangles referenced directly (flat_verts: 3 float4 per
-// triangle).  Leaf payload p < n is instance p, p >= n is flat triangle p - n.
-// slot_ranges[i] = triangle slot range of instance i's BLAS (its world box is
-// the transformed bounds of those vertices).
-uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint32_t n, const float4* tri_verts,
-                    const float4* flat_verts, uint32_t n_flat, BuildScratch& scratch, BvhNode* nodes,
-                    uint32_t node_base, cudaStream_t stream);
+// triangle, the same data as pool slots [flat_slot_base, +n_flat)).  Build
+// primitive p < n becomes an instance leaf of global instance
+// instance_base + p; p >= n a triangle leaf of global slot
+// flat_slot_base + p - n.  slot_ranges[i] = triangle slot range of instance
+// i's BLAS (its world box is the transformed bounds of those vertices).
+uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint32_t n, uint32_t instance_base,
+                    const float4* tri_verts, const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base,
+                    BuildScratch& scratch, BvhNode* nodes, uint32_t node_base, cudaStream_t stream);
 
 // One built bottom-level structure: its root node and triangle slot range.
 struct BlasRange {

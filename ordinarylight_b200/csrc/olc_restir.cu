@@ -15,10 +15,10 @@
 // Storage: two uint4 words per reservoir,
 //   w0 = (light index, barycentrics as half2, w_sum, M)
 //   w1 = (p_hat of the selected sample, primary depth, octahedral normal, stamp)
-// indexed by sample stream * npix + pixel, so a stream's history survives
-// chunking and batching.  A reservoir is valid only when its stamp equals the
-// stamp of the frame that should have written it, so pixels whose primary ray
-// missed never need clearing.
+// indexed by the job's reservoir base + sample stream * npix + pixel, so a
+// stream's reservoirs survive chunking and batching.  A reservoir is valid
+// only when its stamp equals the stamp of the wavefront that should have
+// written it, so pixels whose primary ray missed never need clearing.
 //
 // Only primary rays that hit take part: a compaction pass lists them first,
 // so the candidate loop runs with full warps even when much of the image is
@@ -99,7 +99,6 @@ struct Surface {
   float3 p;
   PreparedBsdf bsdf;
   float depth;
-  bool valid;
 };
 
 struct Res {
@@ -144,16 +143,16 @@ OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float
   }
 }
 
+// Primary surface of path slot i (its ray hit: only listed hits get here).
 OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i) {
   Surface su;
-  su.valid = false;
-  float4 hit = h.tuv_slot[i];
-  if (hit.x < 0.0f) return su;
-  float4 dt = q.dir_tmax[i];
-  float4 ot = q.origin_tmin[i];
-  const float3 d = f3(dt);
+  const float4 hit = h.tuv_slot[i];
+  const float4 dr = q.dir_root[i];
+  const float4 ot = q.origin_tmin[i];
+  const float3 d = f3(dr);
   const uint32_t slot = __float_as_uint(hit.w);
-  const InstanceRec& ir = s.instances[h.instance[i]];
+  const uint32_t inst = h.instance[i];
+  const InstanceRec& ir = s.instances[inst];
   Affine o2w{ir.o2w0, ir.o2w1, ir.o2w2};
   Affine w2o{ir.w2o0, ir.w2o1, ir.w2o2};
   const float4* tv = s.tri_verts + 3u * slot;
@@ -167,10 +166,9 @@ OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBu
   if (dot(ns, ng) < 0.0f) ns = -ns;
   const bool entering = dot(d, ng) < 0.0f;
   su.p = f3(ot) + d * hit.x;
-  const uint32_t owner = owner_instance(s.instances, s.tri_owner, h.instance[i], slot);
+  const uint32_t owner = owner_instance(s.instances, s.tri_owner, inst, slot);
   su.bsdf = prepare_bsdf(load_material(s, s.instances[owner].material), entering ? ns : -ns, -d);
   su.depth = hit.x;
-  su.valid = true;
   return su;
 }
 
@@ -198,19 +196,21 @@ OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, u
   return r;
 }
 
+// Reservoir index of (job, sample stream, pixel).
+OLC_D uint64_t reservoir_index(const JobRec& job, uint32_t sample, uint32_t pixel) {
+  return job.reservoir_base + (uint64_t)sample * job.npix + pixel;
+}
+
 struct RestirArgs {
-  const FrameParams* fp;
+  const ChunkHeader* hdr;
+  const JobRec* jobs;
   SceneView s;
   RayQueue q;
   HitBuf h;
   PathState ps;
-  uint64_t chunk_begin;
-  uint32_t chunk_count;
   const uint32_t* hit_list;
   const uint32_t* hit_count;
   uint32_t candidates;
-  uint32_t history_stamp;   // stamp of the previous frame's final reservoirs (0: none)
-  uint32_t stamp;           // this frame's stamp
   uint32_t history_cap;     // M cap of the temporal history
   uint32_t neighbours;
   float radius;
@@ -225,36 +225,40 @@ struct RestirArgs {
   uint32_t finalize;
 };
 
-// List the chunk's primary rays that hit something (warp-aggregated append;
-// the list order does not affect any result).
-__global__ void k_restir_compact(HitBuf h, uint32_t n, uint32_t* list, uint32_t* count) {
+// List the chunk's primary rays that hit something and belong to ReSTIR
+// jobs (warp-aggregated append; the list order does not affect any result).
+__global__ void k_restir_compact(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, HitBuf h,
+                                 PathState ps, uint32_t* list, uint32_t* count) {
+  const uint32_t n = hdr->count;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
     uint32_t i = base + lane();
-    bool hit = i < n && h.tuv_slot[i].x >= 0.0f;
-    uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+    bool take = i < n && h.tuv_slot[i].x >= 0.0f && jobs[ps.meta[i].w].restir;
+    uint32_t ballot = __ballot_sync(0xffffffffu, take);
     if (ballot == 0u) continue;
     uint32_t leader = __ffs(ballot) - 1u;
     uint32_t off = 0;
     if (lane() == leader) off = atomicAdd(count, __popc(ballot));
     off = __shfl_sync(0xffffffffu, off, leader);
-    if (hit) list[off + __popc(ballot & ((1u << lane()) - 1u))] = i;
+    if (take) list[off + __popc(ballot & ((1u << lane()) - 1u))] = i;
   }
 }
 
 __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
-  const FrameParams& fp = *a.fp;
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const uint32_t i = a.hit_list[k];
     const uint4 meta = a.ps.meta[i];
-    const uint64_t g = a.chunk_begin + i;
+    const JobRec& job = a.jobs[meta.w];
+    const SceneRec& sc = s.scenes[job.scene];
+    const uint64_t g = reservoir_index(job, meta.y, meta.x);
     const Surface su = primary_surface(s, a.q, a.h, i);
+    const uint32_t stamp = a.hdr->stamp;
     Res r{0xffffffffu, 0u, 0.0f, 0u, 0.0f};
-    uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), kRestirStream);
+    uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream);
     for (uint32_t c = 0; c < a.candidates; ++c) {
-      uint32_t li = select_emitter(s, olc_rand(rng));
+      uint32_t li = select_emitter(s, sc, olc_rand(rng));
       float ru = sqrtf(olc_rand(rng));
       float rv = olc_rand(rng);
       uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
@@ -266,11 +270,12 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
       res_update(r, li, bary, t, w, 1u, olc_rand(rng));
     }
     // temporal reuse
-    if (a.history_stamp) {
+    if (job.history) {
       float pd;
       uint32_t pn, pstamp;
-      Res prev = load_res(a.hist0, a.hist1, g, pd, pn, pstamp);
-      if (pstamp == a.history_stamp && prev.light != 0xffffffffu && prev.M > 0u && prev.target > 0.0f &&
+      const uint64_t gh = job.history_base + (uint64_t)meta.y * job.npix + meta.x;
+      Res prev = load_res(a.hist0, a.hist1, gh, pd, pn, pstamp);
+      if (pstamp != 0u && pstamp >= a.hdr->history_first && pstamp <= a.hdr->history_last && prev.light != 0xffffffffu && prev.M > 0u && prev.target > 0.0f &&
           similar(su, pn, pd)) {
         uint32_t m = min(prev.M, a.history_cap);
         float wsum = prev.w_sum * ((float)m / (float)prev.M);
@@ -278,26 +283,27 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
         res_update(r, prev.light, prev.bary, t, t * wsum / prev.target, m, olc_rand(rng));
       }
     }
-    store_res(a.out0, a.out1, g, r, su, a.stamp);
+    store_res(a.out0, a.out1, g, r, su, stamp);
   }
 }
 
 __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
-  const FrameParams& fp = *a.fp;
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const uint32_t i = a.hit_list[k];
     const uint4 meta = a.ps.meta[i];
-    const uint64_t g = a.chunk_begin + i;
-    const uint64_t stream_base = g - meta.x;  // stream * npix
+    const JobRec& job = a.jobs[meta.w];
+    const uint64_t g = reservoir_index(job, meta.y, meta.x);
+    const uint64_t stream_base = g - meta.x;
     const Surface su = primary_surface(s, a.q, a.h, i);
+    const uint32_t stamp = a.hdr->stamp;
     float d0;
     uint32_t n0, st0;
     Res r = load_res(a.in0, a.in1, g, d0, n0, st0);
     if (a.neighbours > 0u) {
-      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), kRestirStream + 1u + a.pass);
-      const int px = (int)(meta.x % fp.width), py = (int)(meta.x / fp.width);
+      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 1u + a.pass);
+      const int px = (int)(meta.x % job.width), py = (int)(meta.x / job.width);
       for (uint32_t j = 0; j < a.neighbours; ++j) {
         float rr = a.radius * sqrtf(olc_rand(rng));
         float th = 2.0f * OLC_PI * olc_rand(rng);
@@ -306,18 +312,18 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
         __sincosf(th, &sn, &cs);
         int qx = px + __float2int_rn(rr * cs);
         int qy = py + __float2int_rn(rr * sn);
-        if (qx < 0 || qy < 0 || qx >= (int)fp.width || qy >= (int)fp.height || (qx == px && qy == py)) continue;
-        uint64_t gq = stream_base + (uint64_t)qy * fp.width + (uint64_t)qx;
+        if (qx < 0 || qy < 0 || qx >= (int)job.width || qy >= (int)job.height || (qx == px && qy == py)) continue;
+        uint64_t gq = stream_base + (uint64_t)qy * job.width + (uint64_t)qx;
         float dq;
         uint32_t nq, sq;
         Res nb = load_res(a.in0, a.in1, gq, dq, nq, sq);
-        if (sq != a.stamp || nb.light == 0xffffffffu || nb.M == 0u || !(nb.target > 0.0f) || !similar(su, nq, dq))
+        if (sq != stamp || nb.light == 0xffffffffu || nb.M == 0u || !(nb.target > 0.0f) || !similar(su, nq, dq))
           continue;
         float t = target_of(s, su, nb.light, nb.bary);
         res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u);
       }
     }
-    store_res(a.out0, a.out1, g, r, su, a.stamp);
+    store_res(a.out0, a.out1, g, r, su, stamp);
     if (a.finalize) {
       float W = (r.light != 0xffffffffu && r.M > 0u && r.target > 0.0f) ? r.w_sum / ((float)r.M * r.target) : 0.0f;
       if (!(W == W) || W > 3.0e38f) W = 0.0f;
@@ -328,19 +334,18 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
 
 }  // namespace
 
-void restir_prepare(RestirState& st, const olc_config& cfg, uint32_t w, uint32_t h, uint32_t spp,
-                    uint32_t frame_index, uint32_t slots, const FrameParams& cam) {
-  uint64_t n = (uint64_t)w * h * spp;
-  if (n > st.reservoirs) {
-    st.res_a0.allocate(n * 16);
-    st.res_a1.allocate(n * 16);
-    st.res_b0.allocate(n * 16);
-    st.res_b1.allocate(n * 16);
-    st.hist0.allocate(n * 16);
-    st.hist1.allocate(n * 16);
-    // stamps start at 1; zero-filled buffers are never valid
-    for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, n * 16));
-    st.reservoirs = n;
+void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks) {
+  if (reservoirs > st.reservoirs) {
+    // the history survives only if its buffers are kept
+    st.res_a0.allocate(reservoirs * 16);
+    st.res_a1.allocate(reservoirs * 16);
+    st.res_b0.allocate(reservoirs * 16);
+    st.res_b1.allocate(reservoirs * 16);
+    st.hist0.allocate(reservoirs * 16);
+    st.hist1.allocate(reservoirs * 16);
+    // stamps start at 1: zero-filled reservoirs are never valid
+    for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, reservoirs * 16));
+    st.reservoirs = reservoirs;
     st.history_valid = false;
   }
   if (slots > st.slots) {
@@ -349,38 +354,31 @@ void restir_prepare(RestirState& st, const olc_config& cfg, uint32_t w, uint32_t
     st.slots = slots;
   }
   if (!st.hit_count.get()) st.hit_count.allocate(16);
-  auto same = [](const float4& x, const float4& y) { return x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w; };
-  bool camera_same = same(cam.cam_pos, st.hist_camera.cam_pos) && same(cam.cam_forward, st.hist_camera.cam_forward) &&
-                     same(cam.cam_right, st.hist_camera.cam_right) && same(cam.cam_up, st.hist_camera.cam_up) &&
-                     cam.projection == st.hist_camera.projection;
-  st.history_used = cfg.restir_temporal && st.history_valid && st.hist_w == w && st.hist_h == h &&
-                    st.hist_spp == spp && st.hist_frame + 1u == frame_index && camera_same;
-  st.cur_w = w;
-  st.cur_h = h;
-  st.cur_spp = spp;
-  st.cur_frame = frame_index;
-  st.hist_camera = cam;
-  st.prev_stamp = st.stamp;
-  st.stamp = st.stamp + 1u == 0u ? 1u : st.stamp + 1u;
+  if ((uint64_t)st.next_stamp + chunks >= 0xffffffffull) {
+    // stamps would wrap: clear every stored stamp and start again at 1
+    for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, st.reservoirs * 16));
+    st.next_stamp = 1;
+    st.history_valid = false;
+    st.hist_first = st.hist_last = 0;
+  }
+  st.run_first = st.next_stamp;
+  st.run_last = st.next_stamp + chunks - 1u;
+  st.next_stamp += chunks;
 }
 
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
-                        const FrameParams* fp, const RayQueue& q, const HitBuf& hits, const PathState& ps,
-                        Counters* /*cnt*/, uint64_t chunk_begin, uint32_t chunk_count, uint32_t /*npix*/,
-                        cudaStream_t stream) {
+                        const ChunkHeader* hdr, const JobRec* jobs, const RayQueue& q, const HitBuf& hits,
+                        const PathState& ps, cudaStream_t stream) {
   RestirArgs a{};
-  a.fp = fp;
+  a.hdr = hdr;
+  a.jobs = jobs;
   a.s = s;
   a.q = q;
   a.h = hits;
   a.ps = ps;
-  a.chunk_begin = chunk_begin;
-  a.chunk_count = chunk_count;
   a.hit_list = st.hit_list.as<uint32_t>();
   a.hit_count = st.hit_count.as<uint32_t>();
   a.candidates = cfg.restir_candidates;
-  a.history_stamp = st.history_used ? st.prev_stamp : 0u;
-  a.stamp = st.stamp;
   a.history_cap = std::max<uint32_t>(1u, cfg.restir_max_history ? cfg.restir_max_history : 20u) * cfg.restir_candidates;
   a.neighbours = cfg.restir_neighbours;
   a.radius = cfg.restir_radius > 0.0f ? cfg.restir_radius : 30.0f;
@@ -390,7 +388,7 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.out0 = st.res_a0.as<uint4>();
   a.out1 = st.res_a1.as<uint4>();
   OLC_CUDA(cudaMemsetAsync(st.hit_count.get(), 0, 4, stream));
-  k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hits, chunk_count, st.hit_list.as<uint32_t>(),
+  k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, hits, ps, st.hit_list.as<uint32_t>(),
                                                         st.hit_count.as<uint32_t>());
   OLC_LAUNCH_CHECK("k_restir_compact");
   const uint32_t grid = ls.grid_shade;
@@ -418,6 +416,8 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
 
 void restir_finish(RestirState& st) {
   // the final reservoirs become the next frame's temporal history
+  st.hist_first = st.run_first;
+  st.hist_last = st.run_last;
   if (st.final_in_b) {
     std::swap(st.hist0, st.res_b0);
     std::swap(st.hist1, st.res_b1);
@@ -425,11 +425,6 @@ void restir_finish(RestirState& st) {
     std::swap(st.hist0, st.res_a0);
     std::swap(st.hist1, st.res_a1);
   }
-  st.history_valid = true;
-  st.hist_w = st.cur_w;
-  st.hist_h = st.cur_h;
-  st.hist_spp = st.cur_spp;
-  st.hist_frame = st.cur_frame;
 }
 
 void restir_reset(RestirState& st) {

@@ -7,38 +7,40 @@
 
 namespace olc {
 
-// Reservoir storage of one frame and the previous frame's history.
+// Reservoir storage of one wavefront and the previous plain frame's history.
 struct RestirState {
   DeviceBuffer res_a0, res_a1;     // current reservoirs (two uint4 words each)
   DeviceBuffer res_b0, res_b1;     // spatial ping-pong
   DeviceBuffer hist0, hist1;       // previous frame's final reservoirs
   DeviceBuffer selected;           // per path slot: light, bary, W
-  DeviceBuffer hit_list;           // path slots whose primary ray hit
+  DeviceBuffer hit_list;           // path slots whose primary ray hit (ReSTIR jobs only)
   DeviceBuffer hit_count;
-  uint32_t stamp = 0;              // validity stamp of this frame's reservoirs
-  uint32_t prev_stamp = 0;
-  uint64_t reservoirs = 0;         // npix * spp capacity
+  uint64_t reservoirs = 0;         // reservoir capacity (pixel-samples of ReSTIR jobs)
   uint32_t slots = 0;              // path slot capacity
-  // frame continuity of the history
+  uint32_t next_stamp = 1;         // stamp of the next chunk (0 never marks a valid reservoir)
+  uint32_t run_first = 0, run_last = 0;    // stamps of this run's chunks
+  uint32_t hist_first = 0, hist_last = 0;  // stamps of the history's chunks (set by restir_finish)
+  bool final_in_b = false;
+  // continuity key of the history (a plain frame: one job)
   bool history_valid = false;
   bool history_used = false;
-  uint32_t hist_w = 0, hist_h = 0, hist_spp = 0, hist_frame = 0;
-  FrameParams hist_camera{};
-  uint32_t cur_w = 0, cur_h = 0, cur_spp = 0, cur_frame = 0;
-  bool final_in_b = false;
+  uint32_t hist_w = 0, hist_h = 0, hist_spp = 0, hist_frame = 0, hist_scene = 0;
+  JobRec hist_camera{};
 };
 
-// Size buffers and decide whether last frame's reservoirs are a valid
-// temporal history for (w, h, spp, frame_index, camera).
-void restir_prepare(RestirState& st, const olc_config& cfg, uint32_t w, uint32_t h, uint32_t spp,
-                    uint32_t frame_index, uint32_t slots, const FrameParams& camera);
-// Run initial RIS + temporal + spatial reuse for one chunk; returns the
-// per-path-slot selected sample buffer consumed by k_shade at bounce 0.
+// Size buffers for `reservoirs` pixel-samples and `slots` path slots, and
+// reserve one stamp per chunk of the run (chunk c of the run gets
+// st.run_first + c; the caller stores it and the history's stamp range in
+// each chunk header).
+void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks);
+// Run initial RIS (+ temporal for jobs with history) + spatial reuse for one
+// chunk; returns the per-path-slot selected sample buffer consumed by k_shade
+// at bounce 0.  Every host-side input is a pointer or a configuration value,
+// so the launches can be captured in a graph and replayed.
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
-                        const FrameParams* fp, const RayQueue& q, const HitBuf& hits, const PathState& ps,
-                        Counters* cnt, uint64_t chunk_begin, uint32_t chunk_count, uint32_t npix,
-                        cudaStream_t stream);
-// Promote this frame's final reservoirs to history.
+                        const ChunkHeader* hdr, const JobRec* jobs, const RayQueue& q, const HitBuf& hits,
+                        const PathState& ps, cudaStream_t stream);
+// Promote this wavefront's final reservoirs to history (plain frames only).
 void restir_finish(RestirState& st);
 void restir_reset(RestirState& st);
 void restir_release(RestirState& st);

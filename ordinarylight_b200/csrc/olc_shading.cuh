@@ -32,9 +32,9 @@ OLC_D float3 gpu_sky(float3 d) {
 // Environment radiance (constant or equirectangular nearest lookup as in
 // ReferencePathTracer._sky, path_tracer.py:185-200); kind NONE falls back to
 // the mode's analytic sky.
-OLC_D float3 environment_radiance(const SceneView& s, float3 d, bool cpu_mode) {
+OLC_D float3 environment_radiance(const SceneRec& s, float3 d, bool cpu_mode) {
   if (s.env_kind == 0u) return cpu_mode ? cpu_sky(d) : gpu_sky(d);
-  if (s.env_kind == 1u) return s.env_color;
+  if (s.env_kind == 1u) return f3(s.env_color);
   float lon = atan2f(d.z, d.x) + s.env_rotation;
   float u = lon / (2.0f * OLC_PI) + 0.5f;
   u = u - floorf(u);
@@ -42,7 +42,7 @@ OLC_D float3 environment_radiance(const SceneView& s, float3 d, bool cpu_mode) {
   uint32_t x = min((uint32_t)(u * (float)s.env_w), s.env_w - 1u);
   uint32_t y = min((uint32_t)(v * (float)s.env_h), s.env_h - 1u);
   const float* p = s.env_image + 3ull * ((uint64_t)y * s.env_w + x);
-  return f3(p[0], p[1], p[2]) * s.env_color;
+  return f3(p[0], p[1], p[2]) * f3(s.env_color);
 }
 
 OLC_D void tangent_frame(float3 n, float3& t, float3& b) {
@@ -202,12 +202,13 @@ OLC_D SurfaceMat load_material(const SceneView& s, uint32_t mi) {
 // Emitter selection with the probabilities of the power CDF
 // (sampleAreaLightTechnique, transport_v1/lighting.glsl:356-377) through an
 // alias table: one 8-byte load instead of a dependent binary search.
-OLC_D uint32_t select_emitter(const SceneView& s, float u) {
-  float scaled = u * (float)s.num_emitters;
-  uint32_t i = min((uint32_t)scaled, s.num_emitters - 1u);
+// Returns the global emitter index (scene base + scene-local index).
+OLC_D uint32_t select_emitter(const SceneView& s, const SceneRec& sc, float u) {
+  float scaled = u * (float)sc.num_emitters;
+  uint32_t i = min((uint32_t)scaled, sc.num_emitters - 1u);
   float frac = scaled - (float)i;
-  AliasEntry e = s.emitter_alias[i];
-  return frac < e.threshold ? i : e.alias;
+  AliasEntry e = s.emitter_alias[sc.emitter_base + i];
+  return sc.emitter_base + (frac < e.threshold ? i : e.alias);
 }
 
 OLC_D EmitterRec load_emitter(const SceneView& s, uint32_t i) {

@@ -183,8 +183,8 @@ struct Traversal {
   bool found;
   TraversalStack<STACK> st;
 
-  OLC_D void begin(const SceneView& s, float3 o, float3 d, float tmin, float tmax, int* smem_base,
-                   int* spill_area) {
+  OLC_D void begin(const SceneView& s, float3 o, float3 d, float tmin, float tmax, uint32_t tlas_root,
+                   int* smem_base, int* spill_area) {
     st.init(smem_base, threadIdx.x, blockDim.x, spill_area);
     wo = o;
     wd = d;
@@ -199,7 +199,7 @@ struct Traversal {
     level = 0;
     cur_inst = 0;
     cur_prim_offset = 0;
-    node = (int)s.tlas_root;
+    node = (int)tlas_root;
     // A well-formed tree is acyclic and finite; the budget only guarantees
     // the loop ends (and reports an error) should the structure be corrupt.
     budget = OLC_TRAVERSAL_BUDGET;
@@ -228,16 +228,16 @@ struct Traversal {
       } else if (node != OLC_MARKER) {
         uint32_t first = olc_leaf_first(node);
         uint32_t count = olc_leaf_count(node);
-        if (level == 0 && first >= s.tlas_instances) {
-          // world-space triangle referenced directly by the TLAS
-          const uint32_t slot = s.flat_slot_base + (first - s.tlas_instances);
+        if (level == 0 && count == OLC_TLAS_LEAF_TRIANGLE) {
+          // baked world-space triangle referenced directly by the TLAS
+          const uint32_t slot = first;
           const float4* tv = s.tri_verts + 3u * slot;
           float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
           float t, b1, b2;
           if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
             if (ANY_HIT) {
               hit.t = t;
-              hit.instance = s.flat_instance;
+              hit.instance = OLC_IDENTITY_INSTANCE;
               hit.slot = slot;
               found = true;
               return true;
@@ -248,7 +248,7 @@ struct Traversal {
               hit.u = b1;
               hit.v = b2;
               hit.slot = slot;
-              hit.instance = s.flat_instance;
+              hit.instance = OLC_IDENTITY_INSTANCE;
               hit.packed = packed;
               found = true;
             }
@@ -311,11 +311,11 @@ struct Traversal {
 
 // Blocking traversal: the whole ray in one call.  Returns true on a hit.
 template <int STACK, bool ANY_HIT>
-OLC_D bool olc_traverse(const SceneView& s, float3 wo, float3 wd, float t_min, float t_max,
+OLC_D bool olc_traverse(const SceneView& s, uint32_t tlas_root, float3 wo, float3 wd, float t_min, float t_max,
                         HitResult& hit, int* smem_base, uint32_t& err) {
   Traversal<STACK, ANY_HIT> tr;
   int spill[OLC_SPILL];
-  tr.begin(s, wo, wd, t_min, t_max, smem_base, spill);
+  tr.begin(s, wo, wd, t_min, t_max, tlas_root, smem_base, spill);
   while (!tr.advance(s, 1 << 30, err)) {
   }
   hit = tr.hit;

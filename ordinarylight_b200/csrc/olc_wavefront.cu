@@ -9,8 +9,11 @@
 //   k_trace_shadow   nativeOccluded in transport_v1/lighting.glsl
 //   k_accumulate     wavefront_resolve.comp:45-54 plus the host float64
 //                    accumulation of api.py:1404-1422, moved on device
-// Queue counts never leave the device: persistent kernels read them, so the
-// whole bounce loop can be captured once as a CUDA graph.
+//   k_resolve        colour = sum / spp, alpha 0 (path_tracer.py:89-95)
+// Every kernel serves a wavefront of one or many jobs (JobRec): a path's job
+// is in its state, a queued ray carries its scene's TLAS root.  Queue counts
+// never leave the device: persistent kernels read them, so the bounce loop
+// can be captured once as a CUDA graph.
 #include "olc_internal.h"
 #include "olc_shading.cuh"
 #include "olc_trace.cuh"
@@ -35,23 +38,38 @@ OLC_D uint32_t warp_reserve(uint32_t* counter, bool want) {
   return want ? base + __popc(ballot & ((1u << lane_id()) - 1u)) : 0xffffffffu;
 }
 
-__global__ void k_raygen(const FrameParams* __restrict__ fp_ptr, uint64_t chunk_begin, uint32_t chunk_count,
-                         RayQueue q, PathState ps, Counters* cnt, float t_min) {
-  const FrameParams fp = *fp_ptr;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < chunk_count; i += gridDim.x * blockDim.x) {
-    uint64_t linear = chunk_begin + i;
-    uint32_t sample = (uint32_t)(linear / fp.npix);
-    uint32_t pixel = (uint32_t)(linear - (uint64_t)sample * fp.npix);
+// Segment owning chunk-local path index g (segments are ordered by seg_begin).
+OLC_D uint32_t segment_of_path(const JobRec* jobs, uint32_t num_segments, uint64_t g) {
+  uint32_t lo = 0, hi = num_segments - 1u;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1u) >> 1;
+    if (jobs[mid].seg_begin <= g) lo = mid; else hi = mid - 1u;
+  }
+  return lo;
+}
+
+OLC_D float job_t_min(const JobRec& j) { return j.mode == 1u ? 1e-4f : 0.001f; }
+
+__global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs,
+                         const SceneRec* __restrict__ scenes, RayQueue q, PathState ps, Counters* cnt) {
+  const uint32_t count = hdr->count;
+  const uint32_t num_segments = hdr->num_segments;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t j = segment_of_path(jobs, num_segments, i);
+    const JobRec& job = jobs[j];
+    const uint64_t local = job.seg_first + (i - job.seg_begin);
+    const uint32_t sample = (uint32_t)(local / job.npix);
+    const uint32_t pixel = (uint32_t)(local - (uint64_t)sample * job.npix);
     float3 o, d;
-    camera_ray(fp, pixel, sample, nullptr, o, d);
-    q.origin_tmin[i] = make_float4(o.x, o.y, o.z, t_min);
-    q.dir_tmax[i] = make_float4(d.x, d.y, d.z, CUDART_INF_F);
+    camera_ray(job, pixel, sample, nullptr, o, d);
+    q.origin_tmin[i] = make_float4(o.x, o.y, o.z, job_t_min(job));
+    q.dir_root[i] = make_float4(d.x, d.y, d.z, __uint_as_float(scenes[job.scene].tlas_root));
     q.path[i] = i;
     ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ps.meta[i] = make_uint4(pixel, sample, 0u, 0u);
+    ps.meta[i] = make_uint4(pixel, sample, 0u, j);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = chunk_count;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = count;
 }
 
 // Persistent traversal (Aila and Laine, "Understanding the Efficiency of Ray
@@ -100,8 +118,9 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
             my = cand;
             float3 o, d;
             float tmin, tmax;
-            load(my, o, d, tmin, tmax);
-            tr.begin(s, o, d, tmin, tmax, smem, spill);
+            uint32_t root;
+            load(my, o, d, tmin, tmax, root);
+            tr.begin(s, o, d, tmin, tmax, root, smem, spill);
           }
         }
         if (base + want >= n) exhausted = true;
@@ -116,20 +135,21 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
 }
 
 template <int STACK, int SCHED>
-__global__ void __launch_bounds__(128) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
+__global__ void __launch_bounds__(256) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
                                                        uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->queue_count[bounce];
   uint32_t err = 0;
   persistent_trace<STACK, false, SCHED>(
       s, n, &cnt->closest_cursor[bounce], smem_stack,
-      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax) {
+      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& root) {
         float4 ot = q.origin_tmin[i];
-        float4 dt = q.dir_tmax[i];
+        float4 dr = q.dir_root[i];
         o = f3(ot);
-        d = f3(dt);
+        d = f3(dr);
         tmin = ot.w;
-        tmax = dt.w;
+        tmax = CUDART_INF_F;
+        root = __float_as_uint(dr.w);
       },
       [&](uint32_t i, const Traversal<STACK, false>& tr) {
         h.tuv_slot[i] = tr.found ? make_float4(tr.hit.t, tr.hit.u, tr.hit.v, __uint_as_float(tr.hit.slot))
@@ -141,25 +161,26 @@ __global__ void __launch_bounds__(128) k_trace_closest(SceneView s, RayQueue q, 
 }
 
 template <int STACK, int SCHED>
-__global__ void __launch_bounds__(128) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
+__global__ void __launch_bounds__(256) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
                                                       uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->shadow_count[bounce];
   uint32_t err = 0;
   persistent_trace<STACK, true, SCHED>(
       s, n, &cnt->shadow_cursor[bounce], smem_stack,
-      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax) {
+      [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& root) {
         float4 ot = sq.origin_tmax[i];
         float4 dp = sq.dir_path[i];
         o = f3(ot);
         d = f3(dp);
         tmin = 0.001f;
         tmax = ot.w;
+        root = __float_as_uint(sq.contrib_root[i].w);
       },
       [&](uint32_t i, const Traversal<STACK, true>& tr) {
         if (!tr.found) {
           uint32_t path = __float_as_uint(sq.dir_path[i].w);
-          float4 c = sq.contrib[i];
+          float4 c = sq.contrib_root[i];
           float4 r = ps.radiance[path];
           ps.radiance[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
         }
@@ -168,17 +189,8 @@ __global__ void __launch_bounds__(128) k_trace_shadow(SceneView s, ShadowQueue s
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
 
-// Products of the first sample's primary hit (render_products).
-struct Products {
-  float* depth;
-  float4* normal;
-  uint32_t* instance_id;
-  uint32_t* material_id;
-  uint32_t* primitive_id;
-};
-
 struct ShadeArgs {
-  const FrameParams* fp;
+  const JobRec* jobs;
   SceneView s;
   RayQueue qin;
   HitBuf hits;
@@ -188,17 +200,14 @@ struct ShadeArgs {
   Counters* cnt;
   uint32_t bounce;
   uint32_t capacity;
-  Products prod;
+  ProductPtrs prod;
   const uint4* restir;   // per-path selected light sample (bounce 0), or null
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
-  const FrameParams& fp = *a.fp;
+__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
   const uint32_t n = a.cnt->queue_count[bounce];
-  const bool cpu_mode = (MODE == 1);
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
     const uint32_t i = base + lane_id();
@@ -206,33 +215,40 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
     bool want_next = false, want_shadow = false, is_miss = false;
     float3 next_o = f3(0, 0, 0), next_d = f3(0, 0, 0);
     float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), sh_c = f3(0, 0, 0);
-    float sh_tmax = 0.0f;
-    uint32_t path = 0;
+    float sh_tmax = 0.0f, next_tmin = 0.0f;
+    uint32_t path = 0, root = 0;
     if (valid) {
       path = a.qin.path[i];
-      float4 ot = a.qin.origin_tmin[i];
-      float4 dt = a.qin.dir_tmax[i];
-      float4 hit = a.hits.tuv_slot[i];
-      float4 tp4 = a.ps.throughput[path];
-      float4 rad4 = a.ps.radiance[path];
-      uint4 meta = a.ps.meta[path];
+      const float4 ot = a.qin.origin_tmin[i];
+      const float4 dr = a.qin.dir_root[i];
+      const float4 hit = a.hits.tuv_slot[i];
+      const float4 tp4 = a.ps.throughput[path];
+      const float4 rad4 = a.ps.radiance[path];
+      const uint4 meta = a.ps.meta[path];
+      const JobRec& job = a.jobs[meta.w];
+      const SceneRec& sc = s.scenes[job.scene];
+      const bool cpu_mode = job.mode == 1u;
+      root = __float_as_uint(dr.w);
+      next_tmin = job_t_min(job);
       float3 tp = f3(tp4), rad = f3(rad4);
-      const float3 o = f3(ot), d = f3(dt);
+      const float3 o = f3(ot), d = f3(dr);
       const uint32_t flags = meta.z >> 8;
-      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, fp.frame), bounce);
+      const uint32_t out_pixel = meta.x;  // products belong to one plain frame's job
+      const bool write_products = job.products && bounce == 0u && meta.y == 0u && a.prod.depth;
+      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), bounce);
       uint32_t new_flags = 0;
       float new_pdf = 0.0f;
       if (hit.x < 0.0f) {
         is_miss = true;
         // miss: environment (no environment NEE, so BSDF sampling carries it
         // with MIS weight 1)
-        rad += tp * environment_radiance(s, d, cpu_mode);
-        if (bounce == 0 && meta.y == 0 && a.prod.depth) {
-          a.prod.depth[meta.x] = CUDART_INF_F;
-          a.prod.normal[meta.x] = make_float4(0, 0, 0, 0);
-          a.prod.instance_id[meta.x] = 0xffffffffu;
-          a.prod.material_id[meta.x] = 0xffffffffu;
-          a.prod.primitive_id[meta.x] = 0xffffffffu;
+        rad += tp * environment_radiance(sc, d, cpu_mode);
+        if (write_products) {
+          a.prod.depth[out_pixel] = CUDART_INF_F;
+          a.prod.normal[out_pixel] = make_float4(0, 0, 0, 0);
+          a.prod.instance_id[out_pixel] = 0xffffffffu;
+          a.prod.material_id[out_pixel] = 0xffffffffu;
+          a.prod.primitive_id[out_pixel] = 0xffffffffu;
         }
       } else {
         const float t = hit.x, bu = hit.y, bv = hit.z;
@@ -249,20 +265,20 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
         float3 p = o + d * t;
         const InstanceRec& orec = s.instances[owner_instance(s.instances, s.tri_owner, inst, slot)];
         SurfaceMat m = load_material(s, orec.material);
-        if (bounce == 0 && meta.y == 0 && a.prod.depth) {
-          a.prod.depth[meta.x] = t;
+        if (write_products) {
+          a.prod.depth[out_pixel] = t;
           float3 fn = dot(ng, d) > 0.0f ? -ng : ng;
-          a.prod.normal[meta.x] = make_float4(fn.x, fn.y, fn.z, 0.0f);
-          a.prod.instance_id[meta.x] = orec.instance_id;
-          a.prod.material_id[meta.x] = s.material_aux[orec.material].material_id;
-          a.prod.primitive_id[meta.x] = ir.prim_offset + s.tri_index[slot];
+          a.prod.normal[out_pixel] = make_float4(fn.x, fn.y, fn.z, 0.0f);
+          a.prod.instance_id[out_pixel] = orec.instance_id;
+          a.prod.material_id[out_pixel] = s.material_aux[orec.material].material_id;
+          a.prod.primitive_id[out_pixel] = ir.prim_offset + s.tri_index[slot];
         }
-        if (MODE == 1) {
+        if (cpu_mode) {
           // CPU reference transport (path_tracer.py:74-87)
           float3 nrm = dot(ng, d) > 0.0f ? -ng : ng;
           rad += tp * m.emission;
           tp *= m.base;
-          if (bounce + 1u < fp.max_bounces) {
+          if (bounce + 1u < job.max_bounces) {
             float u1 = olc_rand(rng), u2 = olc_rand(rng);
             next_o = p + nrm * 1e-4f;
             next_d = reference_bounce_direction(nrm, u1, u2);
@@ -284,23 +300,23 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
             float mis = 1.0f;
             if (flags & OLC_PATH_FLAG_PREV_RESTIR) {
               mis = 0.0f;  // the primary vertex's area lighting came from ReSTIR
-            } else if ((flags & OLC_PATH_FLAG_PREV_NEE) && s.num_emitters > 0u) {
+            } else if ((flags & OLC_PATH_FLAG_PREV_NEE) && sc.num_emitters > 0u) {
               float area = 0.5f * length(gcross);
               float lc_raw = dot(ng, -d);
               float lc = m.two_sided ? fabsf(lc_raw) : fmaxf(lc_raw, 0.0f);
-              float sel = area * luminance(m.emission) / fmaxf(s.emissive_weight, 1e-6f);
-              float p_area = s.num_lights > 0u ? 0.5f : 1.0f;
+              float sel = area * luminance(m.emission) / fmaxf(sc.emissive_weight, 1e-6f);
+              float p_area = sc.num_lights > 0u ? 0.5f : 1.0f;
               float light_pdf = sel * t * t / fmaxf(lc * area, 1e-6f) * p_area;
               mis = power_heuristic(tp4.w, light_pdf);
             }
             rad += tp * m.emission * mis;
           }
           const uint32_t next_bounce = bounce + 1u;
-          if (next_bounce < fp.max_bounces) {
+          if (next_bounce < job.max_bounces) {
             const float3 view = -d;
-            bool did_area_nee = false, did_restir = false;
+            bool did_restir = false;
             // ---- next-event estimation: one shadow ray per path per bounce
-            if (bounce == 0u && a.restir != nullptr && s.num_emitters > 0u) {
+            if (bounce == 0u && job.restir && a.restir != nullptr && sc.num_emitters > 0u) {
               uint4 rs = a.restir[path];
               did_restir = true;
               float Wr = __uint_as_float(rs.z);
@@ -312,12 +328,12 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                 float dist2 = dot(off, off);
                 float dist = sqrtf(dist2);
                 float3 ldir = off / fmaxf(dist, 1e-6f);
-                float sc = fmaxf(dot(nrm, ldir), 0.0f);
+                float scos = fmaxf(dot(nrm, ldir), 0.0f);
                 float lc = emitter_cosine(e, ldir);
-                if (sc > 0.0f && lc > 1e-6f) {
+                if (scos > 0.0f && lc > 1e-6f) {
                   float3 f = pbr_eval(m, nrm, view, ldir);
                   float G = lc / fmaxf(dist2, 1e-12f);
-                  float3 c = tp * f * f3(e.emission) * (sc * G * Wr);
+                  float3 c = tp * f * f3(e.emission) * (scos * G * Wr);
                   if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
                     sh_o = p + nrm * 0.002f;
                     sh_d = ldir;
@@ -327,14 +343,13 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                   }
                 }
               }
-            } else if (fp.nee && (s.num_emitters > 0u || s.num_lights > 0u)) {
-              float p_area = s.num_emitters > 0u ? (s.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
+            } else if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
+              float p_area = sc.num_emitters > 0u ? (sc.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
               float choose = olc_rand(rng);
               if (choose < p_area) {
-                did_area_nee = true;
                 // area light (sampleAreaLightTechnique, lighting.glsl:341-403)
                 float sel = olc_rand(rng);
-                uint32_t li = select_emitter(s, sel);
+                uint32_t li = select_emitter(s, sc, sel);
                 const EmitterRec e = load_emitter(s, li);
                 float ru = sqrtf(olc_rand(rng));
                 float rv = olc_rand(rng);
@@ -343,14 +358,14 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                 float dist2 = dot(off, off);
                 float dist = sqrtf(dist2);
                 float3 ldir = off / fmaxf(dist, 1e-6f);
-                float sc = fmaxf(dot(nrm, ldir), 0.0f);
+                float scos = fmaxf(dot(nrm, ldir), 0.0f);
                 float lc = emitter_cosine(e, ldir);
-                if (sc > 0.0f && lc > 1e-6f) {
+                if (scos > 0.0f && lc > 1e-6f) {
                   float eff_pdf = e.a_pdf.w * dist2 / fmaxf(lc * e.e1_area.w, 1e-6f) * p_area;
                   float bsdf_pdf = pbr_pdf(m, nrm, view, ldir);
                   float mis = power_heuristic(eff_pdf, bsdf_pdf);
                   float3 f = pbr_eval(m, nrm, view, ldir);
-                  float3 c = tp * f * f3(e.emission) * (sc * mis / fmaxf(eff_pdf, 1e-6f));
+                  float3 c = tp * f * f3(e.emission) * (scos * mis / fmaxf(eff_pdf, 1e-6f));
                   if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
                     sh_o = p + nrm * 0.002f;
                     sh_d = ldir;
@@ -359,12 +374,12 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                     want_shadow = true;
                   }
                 }
-              } else if (s.num_lights > 0u) {
+              } else if (sc.num_lights > 0u) {
                 // analytic light (samplePointLights, lighting.glsl:260-312)
                 float pick = olc_rand(rng);
-                uint32_t li = min((uint32_t)(pick * (float)s.num_lights), s.num_lights - 1u);
-                float p_sel = (1.0f - p_area) / (float)s.num_lights;
-                const LightRec L = s.lights[li];
+                uint32_t li = min((uint32_t)(pick * (float)sc.num_lights), sc.num_lights - 1u);
+                float p_sel = (1.0f - p_area) / (float)sc.num_lights;
+                const LightRec L = s.lights[sc.light_base + li];
                 int type = (int)(L.position_type.w + 0.5f);
                 float3 ldir;
                 float dist2 = 1.0f, dist = 1e4f;
@@ -383,10 +398,10 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
                   float x = clampf((cone - L.spot.y) / (L.spot.x - L.spot.y), 0.0f, 1.0f);
                   atten *= x * x * (3.0f - 2.0f * x);
                 }
-                float sc = fmaxf(dot(nrm, ldir), 0.0f);
-                if (in_range && atten > 0.0f && sc > 0.0f) {
+                float scos = fmaxf(dot(nrm, ldir), 0.0f);
+                if (in_range && atten > 0.0f && scos > 0.0f) {
                   float3 f = pbr_eval(m, nrm, view, ldir);
-                  float3 c = tp * f * f3(L.color_intensity) * (L.color_intensity.w * atten * sc / p_sel);
+                  float3 c = tp * f * f3(L.color_intensity) * (L.color_intensity.w * atten * scos / p_sel);
                   if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
                     sh_o = p + nrm * 0.002f;
                     sh_d = ldir;
@@ -404,16 +419,15 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
             tp *= weight;
             new_pdf = pdf;
             if (did_restir) new_flags |= OLC_PATH_FLAG_PREV_RESTIR;
-            else if (fp.nee && s.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
-            (void)did_area_nee;
+            else if (job.nee && sc.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
             // (the reference also ends paths whose throughput falls below 1e-4,
             // wavefront_shade.comp:322-327; that cut-off is biased, so only
             // exactly-zero throughput ends a path here and Russian roulette
             // handles the rest)
             bool alive = sampled && max3(tp) > 0.0f;
             // Russian roulette (wavefront_shade.comp:569-580)
-            if (alive && fp.rr_start > 0u && next_bounce >= fp.rr_start) {
-              float survival = clampf(max3(tp), fp.rr_min_survival, 0.95f);
+            if (alive && job.rr_start > 0u && next_bounce >= job.rr_start) {
+              float survival = clampf(max3(tp), job.rr_min_survival, 0.95f);
               if (olc_rand(rng) >= survival) alive = false;
               else tp = tp * (1.0f / survival);
             }
@@ -438,8 +452,8 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
     uint32_t slot = warp_reserve(&a.cnt->queue_count[bounce + 1u], want_next);
     if (want_next) {
       if (slot < a.capacity) {
-        a.qout.origin_tmin[slot] = make_float4(next_o.x, next_o.y, next_o.z, cpu_mode ? 1e-4f : 0.001f);
-        a.qout.dir_tmax[slot] = make_float4(next_d.x, next_d.y, next_d.z, CUDART_INF_F);
+        a.qout.origin_tmin[slot] = make_float4(next_o.x, next_o.y, next_o.z, next_tmin);
+        a.qout.dir_root[slot] = make_float4(next_d.x, next_d.y, next_d.z, __uint_as_float(root));
         a.qout.path[slot] = path;
       } else {
         atomicAdd(&a.cnt->overflow, 1u);
@@ -450,7 +464,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs a) {
       if (sslot < a.capacity) {
         a.sq.origin_tmax[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
         a.sq.dir_path[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(path));
-        a.sq.contrib[sslot] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+        a.sq.contrib_root[sslot] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(root));
       } else {
         atomicAdd(&a.cnt->overflow, 1u);
       }
@@ -467,32 +481,42 @@ OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
   return __float2ull_rn(v * OLC_ACCUM_SCALE);
 }
 
-__global__ void k_accumulate(PathState ps, uint32_t chunk_count, unsigned long long* accum, Counters* cnt) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < chunk_count; i += gridDim.x * blockDim.x) {
-    float4 r = ps.radiance[i];
-    uint32_t pixel = ps.meta[i].x;
-    unsigned long long* dst = accum + 3ull * pixel;
+__global__ void k_accumulate(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, PathState ps,
+                             unsigned long long* accum, Counters* cnt) {
+  const uint32_t count = hdr->count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const float4 r = ps.radiance[i];
+    const uint4 meta = ps.meta[i];
+    unsigned long long* dst = accum + 3ull * (jobs[meta.w].pixel_base + meta.x);
     atomicAdd(dst + 0, to_fixed(r.x, &cnt->nan_samples));
     atomicAdd(dst + 1, to_fixed(r.y, &cnt->nan_samples));
     atomicAdd(dst + 2, to_fixed(r.z, &cnt->nan_samples));
   }
 }
 
-__global__ void k_resolve(const unsigned long long* __restrict__ accum, uint32_t npix, uint32_t spp, float4* out) {
-  const double scale = 1.0 / ((double)OLC_ACCUM_SCALE * (double)spp);
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-    const unsigned long long* a = accum + 3ull * p;
-    out[p] = make_float4((float)((double)a[0] * scale), (float)((double)a[1] * scale), (float)((double)a[2] * scale),
-                         0.0f);
+// Mean of the accumulated samples of each finished job (the host
+// accumulate-and-divide of render_wavefront_outputs,
+// ordinarylight/targets/vulkan/api.py:1404-1422, done on the device).
+__global__ void k_resolve(const ResolveEntry* __restrict__ entries, const uint32_t* __restrict__ num_entries,
+                          const unsigned long long* __restrict__ accum, float4* out) {
+  const uint32_t n = *num_entries;
+  for (uint32_t e = 0; e < n; ++e) {
+    const ResolveEntry en = entries[e];
+    const double scale = 1.0 / ((double)OLC_ACCUM_SCALE * (double)en.spp);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < en.npix; p += gridDim.x * blockDim.x) {
+      const unsigned long long* a = accum + 3ull * (en.pixel_base + p);
+      out[en.pixel_base + p] = make_float4((float)((double)a[0] * scale), (float)((double)a[1] * scale),
+                                           (float)((double)a[2] * scale), 0.0f);
+    }
   }
 }
 
-__global__ void k_camera_rays(const FrameParams* __restrict__ fp_ptr, uint32_t sample, float2 jitter_override,
+__global__ void k_camera_rays(const JobRec* __restrict__ job_ptr, uint32_t sample, float2 jitter_override,
                               int use_override, float* origins, float* dirs) {
-  const FrameParams fp = *fp_ptr;
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < fp.npix; p += gridDim.x * blockDim.x) {
+  const JobRec job = *job_ptr;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < job.npix; p += gridDim.x * blockDim.x) {
     float3 o, d;
-    camera_ray(fp, p, sample, use_override ? &jitter_override : nullptr, o, d);
+    camera_ray(job, p, sample, use_override ? &jitter_override : nullptr, o, d);
     origins[3ull * p + 0] = o.x;
     origins[3ull * p + 1] = o.y;
     origins[3ull * p + 2] = o.z;
@@ -503,16 +527,17 @@ __global__ void k_camera_rays(const FrameParams* __restrict__ fp_ptr, uint32_t s
 }
 
 template <int STACK>
-__global__ void __launch_bounds__(128) k_trace_rays(SceneView s, uint32_t n, const float* __restrict__ origins,
-                                                    const float* __restrict__ dirs, float t_min, uint32_t* inst_id,
-                                                    int32_t* prim, float* tout, float* bary, Counters* cnt) {
+__global__ void __launch_bounds__(256) k_trace_rays(SceneView s, uint32_t root, uint32_t n,
+                                                    const float* __restrict__ origins, const float* __restrict__ dirs,
+                                                    float t_min, uint32_t* inst_id, int32_t* prim, float* tout,
+                                                    float* bary, Counters* cnt) {
   extern __shared__ int smem_stack[];
   uint32_t err = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float3 o = f3(origins[3ull * i], origins[3ull * i + 1], origins[3ull * i + 2]);
     float3 d = f3(dirs[3ull * i], dirs[3ull * i + 1], dirs[3ull * i + 2]);
     HitResult hr;
-    bool hit = olc_traverse<STACK, false>(s, o, d, t_min, CUDART_INF_F, hr, smem_stack, err);
+    bool hit = olc_traverse<STACK, false>(s, root, o, d, t_min, CUDART_INF_F, hr, smem_stack, err);
     if (inst_id)
       inst_id[i] = hit ? s.instances[owner_instance(s.instances, s.tri_owner, hr.instance, hr.slot)].instance_id
                        : 0xffffffffu;
@@ -527,7 +552,8 @@ __global__ void __launch_bounds__(128) k_trace_rays(SceneView s, uint32_t n, con
 }
 
 template <int STACK>
-__global__ void __launch_bounds__(128) k_occluded_rays(SceneView s, uint32_t n, const float* __restrict__ origins,
+__global__ void __launch_bounds__(256) k_occluded_rays(SceneView s, uint32_t root, uint32_t n,
+                                                       const float* __restrict__ origins,
                                                        const float* __restrict__ dirs, float t_min,
                                                        const float* __restrict__ t_max, uint8_t* occ, Counters* cnt) {
   extern __shared__ int smem_stack[];
@@ -536,7 +562,7 @@ __global__ void __launch_bounds__(128) k_occluded_rays(SceneView s, uint32_t n, 
     float3 o = f3(origins[3ull * i], origins[3ull * i + 1], origins[3ull * i + 2]);
     float3 d = f3(dirs[3ull * i], dirs[3ull * i + 1], dirs[3ull * i + 2]);
     HitResult hr;
-    occ[i] = olc_traverse<STACK, true>(s, o, d, t_min, t_max[i], hr, smem_stack, err) ? 1 : 0;
+    occ[i] = olc_traverse<STACK, true>(s, root, o, d, t_min, t_max[i], hr, smem_stack, err) ? 1 : 0;
   }
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
@@ -550,16 +576,16 @@ void dispatch_stack(uint32_t depth, F&& f) {
   else f(std::integral_constant<int, 32>{});
 }
 
-inline size_t stack_bytes(uint32_t depth) {
+inline size_t stack_bytes(uint32_t depth, uint32_t threads) {
   uint32_t d = depth <= 16 ? 16 : (depth <= 24 ? 24 : 32);
-  return (size_t)d * kTraceThreads * sizeof(int);
+  return (size_t)d * threads * sizeof(int);
 }
 
 }  // namespace
 
-void launch_raygen(const LaunchShape& ls, const FrameParams* fp, uint64_t chunk_begin, uint32_t chunk_count,
-                   const RayQueue& q, const PathState& ps, Counters* cnt, float t_min, cudaStream_t stream) {
-  k_raygen<<<ls.grid_simple, ls.block, 0, stream>>>(fp, chunk_begin, chunk_count, q, ps, cnt, t_min);
+void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const SceneRec* scenes,
+                   const RayQueue& q, const PathState& ps, Counters* cnt, cudaStream_t stream) {
+  k_raygen<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, scenes, q, ps, cnt);
   OLC_LAUNCH_CHECK("k_raygen");
 }
 
@@ -568,9 +594,11 @@ void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQu
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
     if (ls.scheduler == 1)
-      k_trace_closest<D, 1><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
+      k_trace_closest<D, 1><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, q, h, cnt,
+                                                                                                        bounce);
     else
-      k_trace_closest<D, 0><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, q, h, cnt, bounce);
+      k_trace_closest<D, 0><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, q, h, cnt,
+                                                                                                        bounce);
   });
   OLC_LAUNCH_CHECK("k_trace_closest");
 }
@@ -580,19 +608,21 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
     if (ls.scheduler == 1)
-      k_trace_shadow<D, 1><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
+      k_trace_shadow<D, 1><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, sq, ps, cnt,
+                                                                                                       bounce);
     else
-      k_trace_shadow<D, 0><<<ls.grid_trace, kTraceThreads, stack_bytes(D), stream>>>(s, sq, ps, cnt, bounce);
+      k_trace_shadow<D, 0><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, sq, ps, cnt,
+                                                                                                       bounce);
   });
   OLC_LAUNCH_CHECK("k_trace_shadow");
 }
 
-void launch_shade(const LaunchShape& ls, uint32_t mode, const FrameParams* fp, const SceneView& s,
-                  const RayQueue& qin, const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq,
-                  const PathState& ps, Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod,
-                  const uint4* restir, cudaStream_t stream) {
+void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
+                  const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
+                  Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
+                  cudaStream_t stream) {
   ShadeArgs a;
-  a.fp = fp;
+  a.jobs = jobs;
   a.s = s;
   a.qin = qin;
   a.hits = hits;
@@ -602,64 +632,59 @@ void launch_shade(const LaunchShape& ls, uint32_t mode, const FrameParams* fp, c
   a.cnt = cnt;
   a.bounce = bounce;
   a.capacity = capacity;
-  a.prod.depth = prod.depth;
-  a.prod.normal = prod.normal;
-  a.prod.instance_id = prod.instance_id;
-  a.prod.material_id = prod.material_id;
-  a.prod.primitive_id = prod.primitive_id;
+  a.prod = prod;
   a.restir = restir;
-  if (mode == 1) k_shade<1><<<ls.grid_shade, 128, 0, stream>>>(a);
-  else k_shade<0><<<ls.grid_shade, 128, 0, stream>>>(a);
+  k_shade<<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_shade");
 }
 
-void launch_accumulate(const LaunchShape& ls, const PathState& ps, uint32_t chunk_count, unsigned long long* accum,
-                       Counters* cnt, cudaStream_t stream) {
-  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(ps, chunk_count, accum, cnt);
+void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
+                       unsigned long long* accum, Counters* cnt, cudaStream_t stream) {
+  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, ps, accum, cnt);
   OLC_LAUNCH_CHECK("k_accumulate");
 }
 
-void launch_resolve(const LaunchShape& ls, const unsigned long long* accum, uint32_t npix, uint32_t spp,
-                    float4* out, cudaStream_t stream) {
-  k_resolve<<<ls.grid_simple, ls.block, 0, stream>>>(accum, npix, spp, out);
+void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,
+                    const unsigned long long* accum, float4* out, cudaStream_t stream) {
+  k_resolve<<<ls.grid_simple, ls.block, 0, stream>>>(entries, num_entries, accum, out);
   OLC_LAUNCH_CHECK("k_resolve");
 }
 
-void launch_camera_rays(const LaunchShape& ls, const FrameParams* fp, uint32_t sample, const float* jitter,
+void launch_camera_rays(const LaunchShape& ls, const JobRec* job, uint32_t sample, const float* jitter,
                         float* origins, float* dirs, cudaStream_t stream) {
   float2 j = make_float2(0.5f, 0.5f);
   if (jitter) j = make_float2(jitter[0], jitter[1]);
-  k_camera_rays<<<ls.grid_simple, ls.block, 0, stream>>>(fp, sample, j, jitter ? 1 : 0, origins, dirs);
+  k_camera_rays<<<ls.grid_simple, ls.block, 0, stream>>>(job, sample, j, jitter ? 1 : 0, origins, dirs);
   OLC_LAUNCH_CHECK("k_camera_rays");
 }
 
-void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins, const float* dirs,
-                       float t_min, uint32_t* inst_id, int32_t* prim, float* t, float* bary, Counters* cnt,
-                       cudaStream_t stream) {
+void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t root, uint32_t n, const float* origins,
+                       const float* dirs, float t_min, uint32_t* inst_id, int32_t* prim, float* t, float* bary,
+                       Counters* cnt, cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
     uint32_t grid = std::max<uint32_t>(1u, std::min<uint32_t>((n + kTraceThreads - 1) / kTraceThreads, ls.grid_trace));
-    k_trace_rays<D><<<grid, kTraceThreads, stack_bytes(D), stream>>>(s, n, origins, dirs, t_min, inst_id, prim, t,
-                                                                      bary, cnt);
+    k_trace_rays<D><<<grid, kTraceThreads, stack_bytes(D, kTraceThreads), stream>>>(s, root, n, origins, dirs, t_min,
+                                                                                     inst_id, prim, t, bary, cnt);
   });
   OLC_LAUNCH_CHECK("k_trace_rays");
 }
 
-void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins,
+void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t root, uint32_t n, const float* origins,
                           const float* dirs, float t_min, const float* t_max, uint8_t* occ, Counters* cnt,
                           cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
     uint32_t grid = std::max<uint32_t>(1u, std::min<uint32_t>((n + kTraceThreads - 1) / kTraceThreads, ls.grid_trace));
-    k_occluded_rays<D><<<grid, kTraceThreads, stack_bytes(D), stream>>>(s, n, origins, dirs, t_min, t_max, occ, cnt);
+    k_occluded_rays<D><<<grid, kTraceThreads, stack_bytes(D, kTraceThreads), stream>>>(s, root, n, origins, dirs,
+                                                                                        t_min, t_max, occ, cnt);
   });
   OLC_LAUNCH_CHECK("k_occluded_rays");
 }
 
 void configure_trace_kernels() {
-  // Opt every traversal instantiation into the shared-memory carve-out it
-  // needs (default limit is 48 KB per block; ours stay below it, but the
-  // preferred carve-out lets more blocks share one SM).
+  // Prefer the largest shared-memory carve-out for the traversal kernels so
+  // more blocks (each holding its short stacks) share one SM.
   auto prefer = [](const void* fn) { cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100); };
   prefer((const void*)k_trace_closest<16, 0>);
   prefer((const void*)k_trace_closest<24, 0>);

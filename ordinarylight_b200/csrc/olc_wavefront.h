@@ -18,21 +18,20 @@ namespace olc {
 //   panoramic: yaw/pitch = ndc * half angles.
 // The jitter is the counter-based draw of (pixel, sample, frame) unless an
 // override is given.
-OLC_D void camera_ray(const FrameParams& fp, uint32_t pixel, uint32_t sample, const float2* jit, float3& o,
-                      float3& d) {
-  uint32_t y = pixel / fp.width;
-  uint32_t x = pixel - y * fp.width;
-  float2 j = jit ? *jit : olc_camera_jitter(pixel, sample, fp.frame);
-  float ndc_x = ((float)x + j.x) / (float)fp.width * 2.0f - 1.0f;
-  float ndc_y = 1.0f - ((float)y + j.y) / (float)fp.height * 2.0f;
-  float3 pos = f3(fp.cam_pos), fwd = f3(fp.cam_forward), right = f3(fp.cam_right), up = f3(fp.cam_up);
-  float sx = fp.cam_pos.w, sy = fp.cam_forward.w;
-  if (fp.projection == 2u) {
+OLC_D void camera_ray(const JobRec& job, uint32_t pixel, uint32_t sample, const float2* jit, float3& o, float3& d) {
+  uint32_t y = pixel / job.width;
+  uint32_t x = pixel - y * job.width;
+  float2 j = jit ? *jit : olc_camera_jitter(pixel, sample, job.frame);
+  float ndc_x = ((float)x + j.x) / (float)job.width * 2.0f - 1.0f;
+  float ndc_y = 1.0f - ((float)y + j.y) / (float)job.height * 2.0f;
+  float3 pos = f3(job.cam_pos), fwd = f3(job.cam_forward), right = f3(job.cam_right), up = f3(job.cam_up);
+  float sx = job.cam_pos.w, sy = job.cam_forward.w;
+  if (job.projection == 2u) {
     float yaw = ndc_x * sx, pitch = ndc_y * sy;
     float cp = cosf(pitch), sp = sinf(pitch), cy = cosf(yaw), sy2 = sinf(yaw);
     d = fwd * (cp * cy) + right * (cp * sy2) + up * sp;
     o = pos;
-  } else if (fp.projection == 1u) {
+  } else if (job.projection == 1u) {
     o = pos + right * (ndc_x * sx) + up * (ndc_y * sy);
     d = fwd;
   } else {
@@ -44,6 +43,7 @@ OLC_D void camera_ray(const FrameParams& fp, uint32_t pixel, uint32_t sample, co
 
 struct LaunchShape {
   uint32_t block = 256;        // simple grid-stride kernels
+  uint32_t trace_block = 128;  // traversal and shading kernels (64, 128 or 256)
   uint32_t grid_simple = 148 * 8;
   uint32_t grid_trace = 148 * 8;
   uint32_t grid_shade = 148 * 8;
@@ -51,6 +51,8 @@ struct LaunchShape {
   uint32_t scheduler = 0;      // traversal scheduling (olc_config.trace_scheduler)
 };
 
+// First-sample primary-hit products of the job flagged `products` (a plain
+// frame), indexed by pixel.
 struct ProductPtrs {
   float* depth = nullptr;
   float4* normal = nullptr;
@@ -60,26 +62,26 @@ struct ProductPtrs {
 };
 
 void configure_trace_kernels();
-void launch_raygen(const LaunchShape& ls, const FrameParams* fp, uint64_t chunk_begin, uint32_t chunk_count,
-                   const RayQueue& q, const PathState& ps, Counters* cnt, float t_min, cudaStream_t stream);
+void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const SceneRec* scenes,
+                   const RayQueue& q, const PathState& ps, Counters* cnt, cudaStream_t stream);
 void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
                           Counters* cnt, uint32_t bounce, cudaStream_t stream);
 void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const ShadowQueue& sq, const PathState& ps,
                          Counters* cnt, uint32_t bounce, cudaStream_t stream);
-void launch_shade(const LaunchShape& ls, uint32_t mode, const FrameParams* fp, const SceneView& s,
-                  const RayQueue& qin, const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq,
-                  const PathState& ps, Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod,
-                  const uint4* restir, cudaStream_t stream);
-void launch_accumulate(const LaunchShape& ls, const PathState& ps, uint32_t chunk_count, unsigned long long* accum,
-                       Counters* cnt, cudaStream_t stream);
-void launch_resolve(const LaunchShape& ls, const unsigned long long* accum, uint32_t npix, uint32_t spp,
-                    float4* out, cudaStream_t stream);
-void launch_camera_rays(const LaunchShape& ls, const FrameParams* fp, uint32_t sample, const float* jitter,
+void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
+                  const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
+                  Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
+                  cudaStream_t stream);
+void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
+                       unsigned long long* accum, Counters* cnt, cudaStream_t stream);
+void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,
+                    const unsigned long long* accum, float4* out, cudaStream_t stream);
+void launch_camera_rays(const LaunchShape& ls, const JobRec* job, uint32_t sample, const float* jitter,
                         float* origins, float* dirs, cudaStream_t stream);
-void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins, const float* dirs,
-                       float t_min, uint32_t* inst_id, int32_t* prim, float* t, float* bary, Counters* cnt,
-                       cudaStream_t stream);
-void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t n, const float* origins,
+void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t root, uint32_t n, const float* origins,
+                       const float* dirs, float t_min, uint32_t* inst_id, int32_t* prim, float* t, float* bary,
+                       Counters* cnt, cudaStream_t stream);
+void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t root, uint32_t n, const float* origins,
                           const float* dirs, float t_min, const float* t_max, uint8_t* occ, Counters* cnt,
                           cudaStream_t stream);
 

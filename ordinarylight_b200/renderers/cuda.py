@@ -26,6 +26,7 @@ next-event estimation, MIS, Russian roulette and optional ReSTIR DI.
 
 from __future__ import annotations
 
+from collections import OrderedDict
 from dataclasses import asdict, dataclass, fields, replace
 import ctypes
 import time
@@ -60,6 +61,7 @@ class CudaRendererConfig:
     restir_radius: float = 30.0
     restir_max_history: int = 20
     block_size: int = 256
+    trace_block: int = 128
     stack_depth: int = 24
     chunk_paths: int = 0
     use_graphs: bool = True
@@ -94,6 +96,8 @@ class CudaRendererConfig:
             raise ValueError("stack_depth must be 16, 24 or 32")
         if int(self.block_size) % 32 or not 64 <= int(self.block_size) <= 1024:
             raise ValueError("block_size must be a multiple of 32 in [64, 1024]")
+        if int(self.trace_block) not in (64, 128, 256):
+            raise ValueError("trace_block must be 64, 128 or 256")
         if int(self.chunk_paths) < 0:
             raise ValueError("chunk_paths cannot be negative")
         if self.trace_scheduler not in ("refill", "batch"):
@@ -115,6 +119,7 @@ class CudaRendererConfig:
         c.restir_radius = float(self.restir_radius)
         c.restir_max_history = int(self.restir_max_history)
         c.block_size = int(self.block_size)
+        c.trace_block = int(self.trace_block)
         c.stack_depth = int(self.stack_depth)
         c.chunk_paths = int(self.chunk_paths)
         c.use_graphs = int(bool(self.use_graphs))
@@ -122,6 +127,22 @@ class CudaRendererConfig:
         c.trace_scheduler = 0 if self.trace_scheduler == "refill" else 1
         c.disable_nee = 0 if self.nee else 1
         return c
+
+
+@dataclass(frozen=True)
+class RenderRequest:
+    """One render job of a batch or of a served stream: what
+    ``Renderer.render_async`` (ordinarylight/renderer/_core.py:614-651)
+    submits, plus a per-job bounce limit.  ``samples=None`` and
+    ``max_bounces=None`` take the renderer configuration's values."""
+
+    scene: object
+    camera: object
+    width: int
+    height: int
+    samples: int | None = None
+    frame_index: int = 0
+    max_bounces: int | None = None
 
 
 class CudaWavefrontRenderer(RendererImplementation):
@@ -145,6 +166,8 @@ class CudaWavefrontRenderer(RendererImplementation):
         self._closed = False
         self._scene_key = None
         self._packed = None
+        self._resident = OrderedDict()   # (id(scene), revision) -> (handle, scene)
+        self._served_outputs = {}        # ticket -> output array
         self.last_timings = {}
         self.device = f"cuda:{self.config.device}"
 
@@ -287,6 +310,174 @@ class CudaWavefrontRenderer(RendererImplementation):
             self._ctx, int(width), int(height), None, None, None, None, _native.ptr(prim)))
         return prim
 
+    # -- resident scene pool ---------------------------------------------------
+    def resident_scene(self, scene) -> int:
+        """Handle of ``scene`` in the device scene pool, uploading it on first
+        use.  Keyed by (scene object, ``Scene.revision``) like the reference's
+        resident scene (ordinarylight/targets/vulkan/core.py:4591-4611)."""
+        self._require_open()
+        key = (id(scene), getattr(scene, "revision", None))
+        entry = self._resident.get(key)
+        if entry is not None:
+            self._resident.move_to_end(key)
+            return entry[0]
+        packed = pack_scene(scene)
+        desc = packed.descriptor()
+        handle = ctypes.c_uint32()
+        _native.check(self._lib, self._ctx, self._lib.olc_add_scene(self._ctx, ctypes.byref(desc),
+                                                                    ctypes.byref(handle)))
+        # the entry keeps the scene alive so that its id() is not reused
+        self._resident[key] = (int(handle.value), scene)
+        return int(handle.value)
+
+    def release_scene(self, scene) -> None:
+        """Drop ``scene`` from the pool (its ranges are reused)."""
+        self._require_open()
+        key = (id(scene), getattr(scene, "revision", None))
+        entry = self._resident.pop(key, None)
+        if entry is None:
+            raise ValueError("scene is not resident")
+        _native.check(self._lib, self._ctx, self._lib.olc_remove_scene(self._ctx, entry[0]))
+
+    def resident_scenes(self):
+        """Resident pool scenes in least-recently-used order: (scene, handle, bytes)."""
+        out = []
+        for handle, scene in self._resident.values():
+            stats = _native.OlcSceneStats()
+            _native.check(self._lib, self._ctx, self._lib.olc_scene_stats_get(self._ctx, handle,
+                                                                              ctypes.byref(stats)))
+            out.append((scene, handle, int(stats.bytes)))
+        return out
+
+    def pool_info(self) -> dict:
+        info = _native.OlcPoolInfo()
+        _native.check(self._lib, self._ctx, self._lib.olc_pool_info_get(self._ctx, ctypes.byref(info)))
+        return {name: int(getattr(info, name)) for name, _ in info._fields_ if name != "reserved"}
+
+    # -- batched and served rendering ---------------------------------------------
+    def _job(self, request: RenderRequest, out, on_device: bool) -> _native.OlcJob:
+        width, height = int(request.width), int(request.height)
+        if width <= 0 or height <= 0:
+            raise ValueError("width and height must be positive")
+        spp = self.config.samples_per_pixel if request.samples is None else int(request.samples)
+        if not 1 <= spp <= 65536:
+            raise ValueError("samples must be between 1 and 65536")
+        bounces = 0 if request.max_bounces is None else int(request.max_bounces)
+        if request.max_bounces is not None and not 1 <= bounces <= 64:
+            raise ValueError("max_bounces must be between 1 and 64")
+        frame_index = int(request.frame_index)
+        if frame_index < 0:
+            raise ValueError("frame_index cannot be negative")
+        job = _native.OlcJob()
+        job.scene = self.resident_scene(request.scene)
+        job.width, job.height = width, height
+        job.samples_per_pixel = spp
+        job.frame_index = frame_index & 0xFFFFFFFF
+        job.max_bounces = bounces
+        job.camera = pack_camera(request.camera)
+        job.out_rgba = _native.ptr(out).value
+        job.out_is_device = 1 if on_device else 0
+        return job
+
+    def _record_timings(self, stats, total_ms, **extra):
+        rays = stats.camera_rays + stats.extension_rays + stats.shadow_rays
+        gpu_ms = float(stats.gpu_ms)
+        self.last_timings = {
+            "total_ms": total_ms,
+            "gpu_ms": gpu_ms,
+            "camera_rays": int(stats.camera_rays),
+            "extension_rays": int(stats.extension_rays),
+            "shadow_rays": int(stats.shadow_rays),
+            "rays": int(rays),
+            "closest_hit_rays": int(stats.camera_rays + stats.extension_rays),
+            "mrays_per_s": rays / (gpu_ms * 1e3) if gpu_ms > 0 else 0.0,
+            "queue_overflow": int(stats.overflow),
+            "traversal_errors": int(stats.traversal_errors),
+            "chunks": int(stats.chunks),
+            **extra,
+        }
+        if stats.traversal_errors:
+            raise RuntimeError(f"{stats.traversal_errors} traversal stack overflows")
+
+    def render_batch(self, requests, outs=None):
+        """Render many requests as one wavefront (chunks of paths from several
+        jobs and scenes share the ray queues; the chunk sequence replays from a
+        CUDA graph when the same mix recurs).  Each image equals, bit for bit,
+        ``render_frame`` of the same request on a fresh sequence.  Returns the
+        list of (height, width, 4) float32 images (or fills ``outs``)."""
+        self._require_open()
+        requests = list(requests)
+        if outs is None:
+            outs = [np.empty((int(r.height), int(r.width), 4), np.float32) for r in requests]
+        if len(outs) != len(requests):
+            raise ValueError("outs must match requests")
+        t0 = time.perf_counter()
+        jobs = (_native.OlcJob * max(len(requests), 1))()
+        for k, (request, out) in enumerate(zip(requests, outs)):
+            on_device = hasattr(out, "data_ptr") and getattr(out, "is_cuda", False)
+            jobs[k] = self._job(request, out, on_device)
+        stats = _native.OlcRenderStats()
+        _native.check(self._lib, self._ctx, self._lib.olc_render_batch(self._ctx, jobs, len(requests),
+                                                                       ctypes.byref(stats)))
+        self._record_timings(stats, (time.perf_counter() - t0) * 1e3, jobs=len(requests))
+        return outs
+
+    def submit(self, request: RenderRequest, out=None) -> int:
+        """Queue a request for continuous batching; returns its ticket.  The
+        request's paths join the shared wavefront at the next ``serve_step``."""
+        self._require_open()
+        if out is None:
+            out = np.empty((int(request.height), int(request.width), 4), np.float32)
+        on_device = hasattr(out, "data_ptr") and getattr(out, "is_cuda", False)
+        job = self._job(request, out, on_device)
+        ticket = ctypes.c_uint64()
+        _native.check(self._lib, self._ctx, self._lib.olc_submit(self._ctx, ctypes.byref(job), ctypes.byref(ticket)))
+        self._served_outputs[int(ticket.value)] = out
+        return int(ticket.value)
+
+    def serve_step(self):
+        """Run one chunk of the queued requests; returns [(ticket, image)] of
+        the requests it completed.  Statistics of the chunk land in
+        ``last_timings``."""
+        self._require_open()
+        capacity = max(len(self._served_outputs), 1)
+        done = (ctypes.c_uint64 * capacity)()
+        count = ctypes.c_uint32()
+        stats = _native.OlcRenderStats()
+        t0 = time.perf_counter()
+        status = self._lib.olc_serve_step(self._ctx, done, capacity, ctypes.byref(count), ctypes.byref(stats))
+        if status != _native.OLC_OK:
+            self._forget_dropped()
+            _native.check(self._lib, self._ctx, status)
+        self._record_timings(stats, (time.perf_counter() - t0) * 1e3, completed=int(count.value))
+        return [(int(done[k]), self._served_outputs.pop(int(done[k]))) for k in range(count.value)]
+
+    def queued_tickets(self):
+        count = ctypes.c_uint32()
+        _native.check(self._lib, self._ctx, self._lib.olc_queued_jobs(self._ctx, None, 0, ctypes.byref(count)))
+        tickets = (ctypes.c_uint64 * max(count.value, 1))()
+        _native.check(self._lib, self._ctx, self._lib.olc_queued_jobs(self._ctx, tickets, count.value,
+                                                                      ctypes.byref(count)))
+        return [int(tickets[k]) for k in range(count.value)]
+
+    def _forget_dropped(self):
+        queued = set(self.queued_tickets())
+        for ticket in [t for t in self._served_outputs if t not in queued]:
+            self._served_outputs.pop(ticket)
+
+    def cancel(self, ticket: int) -> None:
+        self._require_open()
+        _native.check(self._lib, self._ctx, self._lib.olc_cancel(self._ctx, int(ticket)))
+        self._served_outputs.pop(int(ticket), None)
+
+    def job_bytes(self, request: RenderRequest) -> int:
+        """Device bytes a queued request holds (its accumulator and output)."""
+        job = _native.OlcJob()
+        job.width, job.height = int(request.width), int(request.height)
+        value = ctypes.c_uint64()
+        _native.check(self._lib, self._ctx, self._lib.olc_job_bytes(self._ctx, ctypes.byref(job), ctypes.byref(value)))
+        return int(value.value)
+
     # -- tracing primitives ---------------------------------------------------
     def trace_closest(self, scene, origins, directions, t_min=1e-4):
         """Closest hits of host rays: (instance_id uint32, primitive int32,
@@ -400,4 +591,4 @@ def config_dict(config: CudaRendererConfig) -> dict:
     return asdict(config)
 
 
-__all__ = ["CudaRendererConfig", "CudaWavefrontRenderer"]
+__all__ = ["CudaRendererConfig", "CudaWavefrontRenderer", "RenderRequest"]

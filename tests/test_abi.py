@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol(native_library):
 
 
 def test_abi_version_and_error_path_without_gpu(native_library):
-    assert native_library.olc_abi_version() == 1
+    assert native_library.olc_abi_version() == 2
     # a null context is rejected before any device work
     assert native_library.olc_destroy(None) == 0
     from ordinarylight_b200 import _native
@@ -53,13 +53,16 @@ def test_struct_layouts_match_the_c_header(tmp_path):
 
     structs = {"olc_config": _native.OlcConfig, "olc_scene_desc": _native.OlcSceneDesc,
                "olc_camera": _native.OlcCamera, "olc_render_stats": _native.OlcRenderStats,
-               "olc_bvh_info": _native.OlcBvhInfo, "olc_launch_record": _native.OlcLaunchRecord}
+               "olc_bvh_info": _native.OlcBvhInfo, "olc_launch_record": _native.OlcLaunchRecord,
+               "olc_scene_stats": _native.OlcSceneStats, "olc_pool_info": _native.OlcPoolInfo,
+               "olc_job": _native.OlcJob}
     src = tmp_path / "layout.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname in structs:
         lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
     lines.append('  printf("scene.volume_density %zu\\n", offsetof(olc_scene_desc, volume_density));')
     lines.append('  printf("stats.gpu_ms %zu\\n", offsetof(olc_render_stats, gpu_ms));')
+    lines.append('  printf("job.out_rgba %zu\\n", offsetof(olc_job, out_rgba));')
     lines.append("  return 0; }")
     src.write_text("\n".join(lines))
     exe = tmp_path / "layout"
@@ -70,6 +73,7 @@ def test_struct_layouts_match_the_c_header(tmp_path):
         assert int(sizes[cname]) == ctypes.sizeof(ctype), cname
     assert int(sizes["scene.volume_density"]) == _native.OlcSceneDesc.volume_density.offset
     assert int(sizes["stats.gpu_ms"]) == _native.OlcRenderStats.gpu_ms.offset
+    assert int(sizes["job.out_rgba"]) == _native.OlcJob.out_rgba.offset
 
 
 def test_missing_library_fails_loudly(tmp_path):

@@ -1,0 +1,228 @@
+"""Host logic of the served and batched forms, on CPU: admission by an HBM
+budget, LRU eviction of idle scenes, rejection, failure handling, latency
+statistics and the autotuner's coordinate descent.  The device is replaced
+by a fake renderer with the same methods, so nothing here needs a GPU."""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+from ordinarylight_b200.renderers.cuda import RenderRequest
+from ordinarylight_b200.serving import AdmissionRejected, RenderServer, poisson_arrivals, run_stream
+
+
+class FakeScene:
+    def __init__(self, name, nbytes):
+        self.name = name
+        self.nbytes = nbytes
+        self.revision = 0
+
+
+class FakeRenderer:
+    """Mimics CudaWavefrontRenderer's pool / serving surface.  Each step
+    advances every queued job by `paths_per_step` paths of a shared chunk."""
+
+    def __init__(self, paths_per_step=10_000, fail_on_step=None):
+        self.resident = {}          # id -> (scene, handle)
+        self.order = []             # LRU order of ids
+        self.jobs = {}              # ticket -> [request, remaining paths]
+        self.next_ticket = 1
+        self.paths_per_step = paths_per_step
+        self.fail_on_step = fail_on_step
+        self.steps = 0
+        self.uploads = 0
+        self.evictions = []
+        self.last_timings = {}
+
+    # pool
+    def resident_scene(self, scene):
+        if id(scene) not in self.resident:
+            self.resident[id(scene)] = (scene, len(self.resident) + 1)
+            self.uploads += 1
+        else:
+            self.order.remove(id(scene))
+        self.order.append(id(scene))
+        return self.resident[id(scene)][1]
+
+    def release_scene(self, scene):
+        del self.resident[id(scene)]
+        self.order.remove(id(scene))
+        self.evictions.append(scene.name)
+
+    def resident_scenes(self):
+        return [(self.resident[i][0], self.resident[i][1], self.resident[i][0].nbytes) for i in self.order]
+
+    def job_bytes(self, request):
+        return request.width * request.height * 40
+
+    def pool_info(self):
+        used = sum(self.job_bytes(j[0]) for j in self.jobs.values())
+        return {"scene_bytes": sum(s.nbytes for s, _ in self.resident.values()), "wavefront_bytes": 1000,
+                "pixel_bytes_used": used, "pool_bytes": 0}
+
+    # serving
+    def submit(self, request):
+        t = self.next_ticket
+        self.next_ticket += 1
+        self.jobs[t] = [request, request.width * request.height * (request.samples or 1)]
+        return t
+
+    def serve_step(self):
+        self.steps += 1
+        if self.fail_on_step == self.steps:
+            victims = list(self.jobs)[:1]
+            for t in victims:
+                del self.jobs[t]
+            raise RuntimeError("simulated device failure")
+        budget = self.paths_per_step
+        done = []
+        # shortest remaining work first, as the native planner orders a step
+        for t in sorted(self.jobs, key=lambda k: self.jobs[k][1]):
+            take = min(budget, self.jobs[t][1])
+            self.jobs[t][1] -= take
+            budget -= take
+            if self.jobs[t][1] == 0:
+                req = self.jobs.pop(t)[0]
+                done.append((t, np.full((req.height, req.width, 4), float(t), np.float32)))
+            if budget == 0:
+                break
+        self.last_timings = {"rays": self.paths_per_step - budget, "gpu_ms": 1.0}
+        time.sleep(0.001)
+        return done
+
+    def queued_tickets(self):
+        return list(self.jobs)
+
+
+def _req(scene, w=16, h=16, spp=1):
+    return RenderRequest(scene, None, w, h, samples=spp)
+
+
+def test_requests_complete_and_report_latency():
+    r = FakeRenderer()
+    a, b = FakeScene("a", 100), FakeScene("b", 200)
+    reqs = [_req(a, 32, 32, 4), _req(b, 8, 8), _req(a, 16, 16, 2)] * 3
+    server = RenderServer(r, budget_bytes=10**9).start()
+    futures = run_stream(server, reqs, poisson_arrivals(500.0, len(reqs), seed=1))
+    server.stop()
+    s = server.stats.summary()
+    assert s["completed"] == len(reqs) and s["rejected"] == 0 and s["failed"] == 0
+    assert 0 < s["p50_ms"] <= s["p99_ms"]
+    assert all(f.result().shape == (q.height, q.width, 4) for f, q in zip(futures, reqs))
+    assert r.uploads == 2            # each scene uploaded once, then resident
+
+
+def test_small_requests_finish_inside_big_ones():
+    """Continuous batching: a small request submitted after a big one does
+    not wait for the big one to finish."""
+    r = FakeRenderer(paths_per_step=5_000)
+    s = FakeScene("s", 10)
+    server = RenderServer(r, budget_bytes=10**9).start()
+    big = server.submit(_req(s, 256, 256, 4))      # ~52 steps
+    time.sleep(0.01)
+    small = server.submit(_req(s, 8, 8, 1))
+    small.result(timeout=10)
+    assert not big.done()
+    big.result(timeout=30)
+    server.stop()
+
+
+def test_budget_evicts_idle_scenes_lru_first():
+    r = FakeRenderer()
+    scenes = [FakeScene(f"s{k}", 1000) for k in range(4)]
+    # room for the wavefront (1000), two scenes and one small request
+    server = RenderServer(r, budget_bytes=1000 + 2 * 1000 + 16 * 16 * 40).start()
+    for sc in scenes:
+        server.submit(_req(sc)).result(timeout=10)
+    server.stop()
+    assert r.evictions[:2] == ["s0", "s1"]
+    assert len(r.resident) == 2
+
+
+def test_request_that_cannot_fit_is_rejected_and_others_continue():
+    r = FakeRenderer()
+    sc = FakeScene("s", 10)
+    server = RenderServer(r, budget_bytes=1000 + 10 + 64 * 64 * 40).start()
+    too_big = server.submit(_req(sc, 512, 512))
+    with pytest.raises(AdmissionRejected):
+        too_big.result(timeout=10)
+    ok = server.submit(_req(sc, 64, 64))
+    assert ok.result(timeout=10).shape == (64, 64, 4)
+    server.stop()
+    assert server.stats.rejected == 1 and server.stats.completed == 1
+
+
+def test_requests_wait_for_budget_instead_of_failing():
+    r = FakeRenderer(paths_per_step=1_000)
+    sc = FakeScene("s", 10)
+    # two 64x64 requests do not fit together: the second waits for the first
+    server = RenderServer(r, budget_bytes=1000 + 10 + 64 * 64 * 40 + 100).start()
+    f1 = server.submit(_req(sc, 64, 64))
+    f2 = server.submit(_req(sc, 64, 64))
+    assert f1.result(timeout=10) is not None and f2.result(timeout=10) is not None
+    server.stop()
+    assert server.stats.queue_ms[1] > server.stats.queue_ms[0]
+
+
+def test_step_failure_fails_only_the_dropped_jobs():
+    r = FakeRenderer(paths_per_step=100, fail_on_step=2)
+    sc = FakeScene("s", 10)
+    server = RenderServer(r, budget_bytes=10**9).start()
+    f1 = server.submit(_req(sc, 16, 16))
+    f2 = server.submit(_req(sc, 16, 16))
+    with pytest.raises(RuntimeError):
+        f1.result(timeout=10)
+    assert f2.result(timeout=10).shape == (16, 16, 4)
+    server.stop()
+    assert server.stats.failed == 1
+
+
+def test_submit_after_stop_raises():
+    server = RenderServer(FakeRenderer(), budget_bytes=10**9).start()
+    server.stop()
+    with pytest.raises(RuntimeError):
+        server.submit(_req(FakeScene("s", 1)))
+
+
+def test_poisson_arrivals_rate():
+    t = poisson_arrivals(100.0, 20000, seed=0)
+    assert np.all(np.diff(t) > 0)
+    assert abs(len(t) / t[-1] - 100.0) < 3.0
+
+
+class FakeTunable:
+    """Batch time is a known function of the knobs; the autotuner must find
+    the minimum along each coordinate."""
+
+    def __init__(self):
+        from ordinarylight_b200.renderers.cuda import CudaRendererConfig
+        self.config = CudaRendererConfig()
+        self.calls = 0
+
+    def reconfigure(self, **changes):
+        from dataclasses import replace
+        self.config = replace(self.config, **changes)
+
+    def render_batch(self, requests, outs=None):
+        c = self.config
+        cost = abs(np.log2(max(c.chunk_paths, 1)) - 18) + abs(c.block_size - 128) / 64 + abs(c.stack_depth - 24) / 8
+        time.sleep(0.002 + 0.002 * cost)
+        self.calls += 1
+        return outs
+
+
+def test_autotuner_coordinate_descent():
+    from ordinarylight_b200.autotune import autotune
+
+    r = FakeTunable()
+    reqs = [_req(FakeScene("s", 1))]
+    result = autotune(r, reqs, repeats=1, use_cache=False)
+    assert (result.chunk_paths, result.block_size, result.stack_depth) == (1 << 18, 128, 24)
+    assert r.config.chunk_paths == 1 << 18
+    assert len(result.trials) <= 1 + 4 + 4 + 3
+    again = autotune(r, reqs, repeats=1)          # cached: no new trials
+    calls = r.calls
+    assert autotune(r, reqs, repeats=1) is again and r.calls == calls
