@@ -17,6 +17,7 @@
 #include "olc_internal.h"
 #include "olc_shading.cuh"
 #include "olc_trace.cuh"
+#include "olc_volume.cuh"
 #include "olc_wavefront.h"
 
 namespace olc {
@@ -204,6 +205,80 @@ struct ShadeArgs {
   const uint4* restir;   // per-path selected light sample (bounce 0), or null
 };
 
+// One next-event sample from p: an area emitter (alias-table choice, uniform
+// point; sampleAreaLightTechnique, lighting.glsl:341-403) or an analytic light
+// (samplePointLights, lighting.glsl:260-312), chosen with probability
+// p_area = 0.5 when the scene has both.  At a surface vertex the BSDF and the
+// cosine weight the light (MIS against the BSDF pdf); at a medium vertex
+// (`medium`) the isotropic phase function does (MIS against 1 / (4 pi)).
+// Returns false when the sample contributes nothing.
+OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& m, float3 p, float3 nrm, float3 view,
+                      float3 tp, bool medium, uint32_t& rng, float3& sh_o, float3& sh_d, float& sh_tmax,
+                      float3& sh_c) {
+  constexpr float kPhase = 0.25f / OLC_PI;
+  const float p_area = sc.num_emitters > 0u ? (sc.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
+  const float choose = olc_rand(rng);
+  float3 c = f3(0.0f, 0.0f, 0.0f);
+  float3 ldir;
+  float dist = 1e4f;
+  bool directional = false;
+  if (choose < p_area) {
+    const float sel = olc_rand(rng);
+    const uint32_t li = select_emitter(s, sc, sel);
+    const EmitterRec e = load_emitter(s, li);
+    const float ru = sqrtf(olc_rand(rng));
+    const float rv = olc_rand(rng);
+    const float3 lp = emitter_point(e, ru * (1.0f - rv), ru * rv);
+    const float3 off = lp - p;
+    const float dist2 = dot(off, off);
+    dist = sqrtf(dist2);
+    ldir = off / fmaxf(dist, 1e-6f);
+    const float scos = medium ? 1.0f : fmaxf(dot(nrm, ldir), 0.0f);
+    const float lc = emitter_cosine(e, ldir);
+    if (!(scos > 0.0f && lc > 1e-6f)) return false;
+    const float eff_pdf = e.a_pdf.w * dist2 / fmaxf(lc * e.e1_area.w, 1e-6f) * p_area;
+    const float scatter_pdf = medium ? kPhase : pbr_pdf(m, nrm, view, ldir);
+    const float mis = power_heuristic(eff_pdf, scatter_pdf);
+    const float3 f = medium ? f3(kPhase, kPhase, kPhase) : pbr_eval(m, nrm, view, ldir);
+    c = tp * f * f3(e.emission) * (scos * mis / fmaxf(eff_pdf, 1e-6f));
+  } else if (sc.num_lights > 0u) {
+    const float pick = olc_rand(rng);
+    const uint32_t li = min((uint32_t)(pick * (float)sc.num_lights), sc.num_lights - 1u);
+    const float p_sel = (1.0f - p_area) / (float)sc.num_lights;
+    const LightRec L = s.lights[sc.light_base + li];
+    const int type = (int)(L.position_type.w + 0.5f);
+    float dist2 = 1.0f;
+    if (type == 1) {
+      ldir = -normalize(f3(L.direction_range));
+      directional = true;
+    } else {
+      const float3 off = f3(L.position_type) - p;
+      dist2 = fmaxf(dot(off, off), 1e-6f);
+      dist = sqrtf(dist2);
+      ldir = off / dist;
+    }
+    const bool in_range = !(type != 1 && L.direction_range.w > 0.0f && dist > L.direction_range.w);
+    float atten = type == 1 ? 1.0f : 1.0f / dist2;
+    if (type == 2) {
+      const float cone = dot(normalize(f3(L.direction_range)), -ldir);
+      const float x = clampf((cone - L.spot.y) / (L.spot.x - L.spot.y), 0.0f, 1.0f);
+      atten *= x * x * (3.0f - 2.0f * x);
+    }
+    const float scos = medium ? 1.0f : fmaxf(dot(nrm, ldir), 0.0f);
+    if (!(in_range && atten > 0.0f && scos > 0.0f)) return false;
+    const float3 f = medium ? f3(kPhase, kPhase, kPhase) : pbr_eval(m, nrm, view, ldir);
+    c = tp * f * f3(L.color_intensity) * (L.color_intensity.w * atten * scos / p_sel);
+  } else {
+    return false;
+  }
+  if (!(c.x > 0.0f || c.y > 0.0f || c.z > 0.0f)) return false;
+  sh_o = medium ? p : p + nrm * 0.002f;
+  sh_d = ldir;
+  sh_tmax = directional ? 1e4f : fmaxf(dist - 0.004f, 0.001f);
+  sh_c = c;
+  return true;
+}
+
 __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
@@ -238,7 +313,46 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
       uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), bounce);
       uint32_t new_flags = 0;
       float new_pdf = 0.0f;
-      if (hit.x < 0.0f) {
+      const uint32_t next_bounce = bounce + 1u;
+      // ---- participating medium (production transport): a real collision
+      // before the surface (or before leaving the scene) makes this vertex a
+      // scattering event in the medium
+      Medium med;
+      const bool has_medium = !cpu_mode && load_medium(sc, med);
+      float t_med = 0.0f;
+      const bool scattered =
+          has_medium && medium_collision(med, o, d, ot.w, hit.x < 0.0f ? CUDART_INF_F : hit.x, rng, t_med);
+      if (scattered) {
+        const float3 p = o + d * t_med;
+        tp *= med.albedo;
+        if (write_products) {
+          a.prod.depth[out_pixel] = t_med;
+          a.prod.normal[out_pixel] = make_float4(0, 0, 0, 0);
+          a.prod.instance_id[out_pixel] = 0xffffffffu;
+          a.prod.material_id[out_pixel] = 0xffffffffu;
+          a.prod.primitive_id[out_pixel] = 0xffffffffu;
+        }
+        if (next_bounce < job.max_bounces) {
+          if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
+            SurfaceMat none{};
+            want_shadow = next_event(s, sc, none, p, f3(0, 0, 1), -d, tp, true, rng, sh_o, sh_d, sh_tmax, sh_c);
+            if (sc.num_emitters > 0u) new_flags |= OLC_PATH_FLAG_PREV_NEE;
+          }
+          const float u1 = olc_rand(rng), u2 = olc_rand(rng);
+          next_d = uniform_sphere(u1, u2);
+          new_pdf = 0.25f / OLC_PI;
+          bool alive = max3(tp) > 0.0f;
+          if (alive && job.rr_start > 0u && next_bounce >= job.rr_start) {
+            const float survival = clampf(max3(tp), job.rr_min_survival, 0.95f);
+            if (olc_rand(rng) >= survival) alive = false;
+            else tp = tp * (1.0f / survival);
+          }
+          if (alive) {
+            next_o = p;
+            want_next = true;
+          }
+        }
+      } else if (hit.x < 0.0f) {
         is_miss = true;
         // miss: environment (no environment NEE, so BSDF sampling carries it
         // with MIS weight 1)
@@ -278,7 +392,7 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
           float3 nrm = dot(ng, d) > 0.0f ? -ng : ng;
           rad += tp * m.emission;
           tp *= m.base;
-          if (bounce + 1u < job.max_bounces) {
+          if (next_bounce < job.max_bounces) {
             float u1 = olc_rand(rng), u2 = olc_rand(rng);
             next_o = p + nrm * 1e-4f;
             next_d = reference_bounce_direction(nrm, u1, u2);
@@ -311,7 +425,6 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
             }
             rad += tp * m.emission * mis;
           }
-          const uint32_t next_bounce = bounce + 1u;
           if (next_bounce < job.max_bounces) {
             const float3 view = -d;
             bool did_restir = false;
@@ -344,73 +457,7 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
                 }
               }
             } else if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
-              float p_area = sc.num_emitters > 0u ? (sc.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
-              float choose = olc_rand(rng);
-              if (choose < p_area) {
-                // area light (sampleAreaLightTechnique, lighting.glsl:341-403)
-                float sel = olc_rand(rng);
-                uint32_t li = select_emitter(s, sc, sel);
-                const EmitterRec e = load_emitter(s, li);
-                float ru = sqrtf(olc_rand(rng));
-                float rv = olc_rand(rng);
-                float3 lp = emitter_point(e, ru * (1.0f - rv), ru * rv);
-                float3 off = lp - p;
-                float dist2 = dot(off, off);
-                float dist = sqrtf(dist2);
-                float3 ldir = off / fmaxf(dist, 1e-6f);
-                float scos = fmaxf(dot(nrm, ldir), 0.0f);
-                float lc = emitter_cosine(e, ldir);
-                if (scos > 0.0f && lc > 1e-6f) {
-                  float eff_pdf = e.a_pdf.w * dist2 / fmaxf(lc * e.e1_area.w, 1e-6f) * p_area;
-                  float bsdf_pdf = pbr_pdf(m, nrm, view, ldir);
-                  float mis = power_heuristic(eff_pdf, bsdf_pdf);
-                  float3 f = pbr_eval(m, nrm, view, ldir);
-                  float3 c = tp * f * f3(e.emission) * (scos * mis / fmaxf(eff_pdf, 1e-6f));
-                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
-                    sh_o = p + nrm * 0.002f;
-                    sh_d = ldir;
-                    sh_tmax = fmaxf(dist - 0.004f, 0.001f);
-                    sh_c = c;
-                    want_shadow = true;
-                  }
-                }
-              } else if (sc.num_lights > 0u) {
-                // analytic light (samplePointLights, lighting.glsl:260-312)
-                float pick = olc_rand(rng);
-                uint32_t li = min((uint32_t)(pick * (float)sc.num_lights), sc.num_lights - 1u);
-                float p_sel = (1.0f - p_area) / (float)sc.num_lights;
-                const LightRec L = s.lights[sc.light_base + li];
-                int type = (int)(L.position_type.w + 0.5f);
-                float3 ldir;
-                float dist2 = 1.0f, dist = 1e4f;
-                if (type == 1) {
-                  ldir = -normalize(f3(L.direction_range));
-                } else {
-                  float3 off = f3(L.position_type) - p;
-                  dist2 = fmaxf(dot(off, off), 1e-6f);
-                  dist = sqrtf(dist2);
-                  ldir = off / dist;
-                }
-                bool in_range = !(type != 1 && L.direction_range.w > 0.0f && dist > L.direction_range.w);
-                float atten = type == 1 ? 1.0f : 1.0f / dist2;
-                if (type == 2) {
-                  float cone = dot(normalize(f3(L.direction_range)), -ldir);
-                  float x = clampf((cone - L.spot.y) / (L.spot.x - L.spot.y), 0.0f, 1.0f);
-                  atten *= x * x * (3.0f - 2.0f * x);
-                }
-                float scos = fmaxf(dot(nrm, ldir), 0.0f);
-                if (in_range && atten > 0.0f && scos > 0.0f) {
-                  float3 f = pbr_eval(m, nrm, view, ldir);
-                  float3 c = tp * f * f3(L.color_intensity) * (L.color_intensity.w * atten * scos / p_sel);
-                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
-                    sh_o = p + nrm * 0.002f;
-                    sh_d = ldir;
-                    sh_tmax = type == 1 ? 1e4f : fmaxf(dist - 0.004f, 0.001f);
-                    sh_c = c;
-                    want_shadow = true;
-                  }
-                }
-              }
+              want_shadow = next_event(s, sc, m, p, nrm, view, tp, false, rng, sh_o, sh_d, sh_tmax, sh_c);
             }
             // ---- BSDF sample
             float3 wdir, weight;
@@ -438,6 +485,11 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
             }
           }
         }
+      }
+      // shadow rays crossing the medium carry its ratio-tracked transmittance
+      if (want_shadow && has_medium) {
+        sh_c *= medium_transmittance(med, sh_o, sh_d, sh_tmax, rng);
+        want_shadow = sh_c.x > 0.0f || sh_c.y > 0.0f || sh_c.z > 0.0f;
       }
       a.ps.throughput[path] = make_float4(tp.x, tp.y, tp.z, new_pdf);
       a.ps.radiance[path] = make_float4(rad.x, rad.y, rad.z, 0.0f);

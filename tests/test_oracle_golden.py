@@ -103,3 +103,32 @@ def test_morton_degenerate_extent_gives_zero_axis():
     tris[:, :, 0] = np.arange(4)[:, None]
     codes = lbvh.morton_codes(tris)
     assert len(set(codes.tolist())) == 4
+
+
+# ---- participating medium oracle -------------------------------------------------
+
+def test_volume_oracle_trilinear_and_analytic_transmittance():
+    from oracle import volume as V
+
+    grid = np.arange(8, dtype=np.float32).reshape(2, 2, 2)   # value = 4z + 2y + x
+    corners = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1], [0.5, 0.5, 0.5]])
+    assert np.allclose(V.sample_trilinear(grid, corners), [0, 1, 2, 4, 7, 3.5])
+    assert np.allclose(V.sample_trilinear(grid, [[-3.0, 2.0, 0.25]]), [0 + 2 + 1.0])   # clipped to the box
+    # homogeneous slab of thickness 2 under scale(2): T = exp(-sigma * 2)
+    w2b = np.hstack([np.eye(3) * 0.5, np.zeros((3, 1))])
+    t = V.transmittance(np.ones((4, 4, 4), np.float32), w2b, 0.8, [[1.0, 1.0, -5.0], [0.5, 1.5, 9.0]],
+                        [[0, 0, 1.0], [0, 0, -1.0]])
+    assert np.allclose(t, np.exp(-1.6))
+
+
+def test_volume_oracle_monte_carlo_absorber_matches_analytic():
+    from oracle import volume as V
+
+    n = 40000
+    w2b = np.hstack([np.eye(3) * 0.5, np.zeros((3, 1))])
+    o = np.column_stack([np.full(n, 1.0), np.full(n, 1.0), np.full(n, -5.0)])
+    d = np.tile([0.0, 0.0, 1.0], (n, 1))
+    rad = V.render_medium(np.ones((4, 4, 4), np.float32), w2b, 0.8, 0.0, o, d, env=[1.0, 1.0, 1.0],
+                          max_bounces=2, seed=3)
+    expected = np.exp(-1.6)
+    assert abs(rad[:, 0].mean() - expected) < 4.0 * np.sqrt(expected * (1 - expected) / n)
