@@ -1,10 +1,11 @@
 """Benchmark of the wavefront path-tracing loop (one JSON line on rank 0).
 
-Workload (N=1): the instanced PBR scene — 64 instances of a 16,384-triangle
-sphere, a 2-triangle ground and 1,024 emissive triangles (1,049,602
-triangles) — at 1920x1080, 4 spp, 8 bounces, ReSTIR DI with 32 candidates,
-1 temporal and 1 spatial pass (5 neighbours, radius 30 px).  A step renders
-one frame.  Metric: Mrays/s (camera + extension + shadow rays per second).
+Headline workload (N=1): the instanced PBR scene — 64 instances of a
+16,384-triangle sphere, a 2-triangle ground and 1,024 emissive triangles
+(1,049,602 triangles) — at 1920x1080, 4 spp, 8 bounces, ReSTIR DI with 32
+candidates, 1 temporal and 1 spatial pass (5 neighbours, radius 30 px).  A
+step renders one frame.  Metric: Mrays/s (camera + extension + shadow rays
+per second).
 
 * ``value``: device time of the frame (CUDA events on the renderer's stream),
   scene resident, output into a device buffer; L2 flushed between steps.
@@ -14,10 +15,20 @@ one frame.  Metric: Mrays/s (camera + extension + shadow rays per second).
   average event-timed launch duration, against MEASURED_PEAKS.json.
 * ``cpu_baseline``: the oracle restatement of CpuReferenceRenderer on a
   bounded sample of the same scene, all host cores.
+* ``served``: the served form on a Poisson request stream over 8 resident
+  scenes of 10k-8M triangles (p50/p99 latency, throughput, rejections),
+  beside the plain path serving the same stream one request at a time.
+* ``batched``: 64 jobs over nine rescaled configuration scenes in one
+  wavefront after the launch-shape autotuner, beside the same jobs one at a
+  time.
+* ``config1`` / ``config3``: the closed-box room against the CPU reference
+  (reference-compatible mode, closest-hit rays) and the terrain with its
+  delta-tracked volume.
 
 ``--impl reference`` times that CPU reference alone (rank 0).
 For N > 1 (torchrun), every rank renders its own frames (weak scaling, no
-data-path collective); the step time is the max over ranks.
+data-path collective); the step time is the max over ranks, and only the
+headline section runs.
 """
 
 from __future__ import annotations
@@ -291,7 +302,7 @@ def run_ours(args, rank, world, device_index):
             stage_ms[stage] = stage_ms.get(stage, 0.0) + ms
             stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, items, misses)
             stage_launches[stage] = stage_launches.get(stage, 0) + 1
-            launches += 2 if stage == "restir" else 1
+            launches += 3 if stage == "restir" else 1   # compaction, initial, one spatial pass
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -313,10 +324,12 @@ def run_ours(args, rank, world, device_index):
     e2e_steps = max(1, min(args.steps, 5))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e2e_rays = 0
+    e2e_rays, h2d, d2h = 0, 0, 0
     for k in range(e2e_steps):
         img = renderer.render_frame(scene, camera, WIDTH, HEIGHT, frame_index=frame0 + 500 + k)
         e2e_rays += renderer.last_timings["rays"]
+        h2d += renderer.last_timings["h2d_bytes"]
+        d2h += renderer.last_timings["d2h_bytes"]
     e2e_s = time.perf_counter() - t0
     if world > 1:
         import torch.distributed as dist
@@ -362,8 +375,8 @@ def run_ours(args, rank, world, device_index):
                    "l2": "256 MiB buffer written between timed steps (L2 flush); per-frame queues 1.7 GB"},
         "rays_per_step": rays_all / args.steps,
         "mrays_closest_hit": None,
-        "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 64 + 112,
-                "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 1600, "steps": e2e_steps, "finite": finite},
+        "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": h2d // e2e_steps,
+                "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "finite": finite},
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": _traffic_from_profiles(dominant),
@@ -377,6 +390,190 @@ def run_ours(args, rank, world, device_index):
     cr = timings["camera_rays"] + timings["extension_rays"]
     line["mrays_closest_hit"] = cr * args.steps / (total_ms * 1e3) if world == 1 else None
     return line
+
+
+# ---------------------------------------------------------------------------
+# secondary sections (N = 1)
+# ---------------------------------------------------------------------------
+def _cpu_room_worker(args):
+    seed, width, height, bounces = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from oracle import reference_path_tracer as ref
+    from ordinarylight_b200 import scenes
+
+    scene, camera = scenes.box_room()
+    counter = ref.RayCounter()
+    t0 = time.perf_counter()
+    ref.render_frame(scene, camera, width, height, samples=1, max_bounces=bounces, seed=seed, counter=counter)
+    return counter.rays, time.perf_counter() - t0
+
+
+def run_config1(device_index, processes=None):
+    """Closed-box room, 256x256, 16 spp, 4 bounces, reference-compatible
+    transport: closest-hit rays per second on the GPU against the CPU
+    reference (oracle) on all host cores."""
+    import multiprocessing as mp
+
+    import torch
+
+    from ordinarylight_b200 import CudaWavefrontRenderer, scenes
+
+    scene, camera = scenes.box_room()
+    with CudaWavefrontRenderer(device=device_index, mode="reference_compatible", samples_per_pixel=16,
+                               max_bounces=4, seed=1) as r:
+        for k in range(3):
+            r.render_frame(scene, camera, 256, 256, frame_index=k)
+        rays, gpu_ms, wall = 0, 0.0, 0.0
+        for k in range(10):
+            t0 = time.perf_counter()
+            r.render_frame(scene, camera, 256, 256, frame_index=10 + k)
+            wall += time.perf_counter() - t0
+            rays += r.last_timings["closest_hit_rays"]
+            gpu_ms += r.last_timings["gpu_ms"]
+    torch.cuda.synchronize()
+    processes = processes or os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(processes) as pool:
+        res = pool.map(_cpu_room_worker, [(100 + k, 256, 256, 4) for k in range(processes)])
+    cpu_rays = sum(r for r, _ in res)
+    cpu_s = max(t for _, t in res)
+    gpu = rays / (gpu_ms * 1e3)
+    cpu = cpu_rays / cpu_s / 1e6
+    return {"workload": "closed-box room (36 tris), 256x256, 16 spp, 4 bounces, reference-compatible transport",
+            "gpu_mrays_closest_hit": gpu, "gpu_e2e_mrays_closest_hit": rays / wall / 1e6,
+            "cpu_mrays_closest_hit": cpu, "cpu_cores": processes,
+            "cpu_sample": f"{processes} processes x 256x256 at 1 spp, 4 bounces, slowest process timed",
+            "gpu_over_cpu": gpu / cpu, "e2e_over_cpu": rays / wall / 1e6 / cpu}
+
+
+def run_config3(device_index, steps=5):
+    """Terrain (2048^2 fBm heightfield, 8,380,418 triangles) under a 128^3
+    fBm volume (sigma_t scale 0.5, albedo 0.9), sky 1.0 + sun; 1280x720,
+    8 spp, 6 bounces."""
+    import torch
+
+    from ordinarylight_b200 import CudaWavefrontRenderer, scenes
+
+    scene, camera = scenes.terrain()
+    with CudaWavefrontRenderer(device=device_index, samples_per_pixel=8, max_bounces=6, seed=1) as r:
+        for k in range(3):
+            r.render_frame(scene, camera, 1280, 720, frame_index=k)
+        rays, gpu_ms = 0, 0.0
+        stage = {}
+        for k in range(steps):
+            r.render_frame(scene, camera, 1280, 720, frame_index=10 + k)
+            rays += r.last_timings["rays"]
+            gpu_ms += r.last_timings["gpu_ms"]
+            for name, _b, _i, _m, ms in _profile(r):
+                stage[name] = stage.get(name, 0.0) + ms / steps
+        build_ms = r.bvh_info()["build_ms"]
+    torch.cuda.synchronize()
+    return {"workload": "terrain 2048^2 fBm heightfield (8,380,418 tris) + 128^3 fBm volume "
+                        "(sigma_t 0.5, albedo 0.9, delta tracking), sky + sun, 1280x720, 8 spp, 6 bounces",
+            "mrays_per_s": rays / (gpu_ms * 1e3), "ms_per_frame": gpu_ms / steps, "bvh_build_ms": build_ms,
+            "stage_ms_per_frame": stage}
+
+
+def run_batched(device_index, tune=True):
+    """64 jobs over nine rescaled configuration scenes: one wavefront after
+    the autotuner, against the same jobs rendered one at a time (each job
+    alone in the executor; scenes resident in both arms)."""
+    import torch
+
+    from ordinarylight_b200 import CudaWavefrontRenderer, workloads
+    from ordinarylight_b200.autotune import autotune
+
+    variants = workloads.batch_scene_variants()
+    requests = workloads.batch_requests(variants, 64, seed=4)
+    outs = [np.empty((r.height, r.width, 4), np.float32) for r in requests]
+    with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
+                               restir_neighbours=5, restir_radius=30.0, seed=1) as r:
+        for v in variants:
+            r.resident_scene(v[0])
+        # plain arm: one job per run
+        for q, o in zip(requests[:4], outs[:4]):
+            r.render_batch([q], [o])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain_rays, plain_gpu = 0, 0.0
+        for q, o in zip(requests, outs):
+            r.render_batch([q], [o])
+            plain_rays += r.last_timings["rays"]
+            plain_gpu += r.last_timings["gpu_ms"]
+        plain_wall = time.perf_counter() - t0
+        tuned = None
+        if tune:
+            res = autotune(r, requests, repeats=1)
+            tuned = {"chunk_paths": res.chunk_paths, "block_size": res.block_size, "trace_block": res.trace_block,
+                     "stack_depth": res.stack_depth, "trials": len(res.trials), "best_s": res.seconds}
+        r.render_batch(requests, outs)
+        torch.cuda.synchronize()
+        walls, rays, gpu = [], 0, 0.0
+        for _ in range(3):
+            t0 = time.perf_counter()
+            r.render_batch(requests, outs)
+            walls.append(time.perf_counter() - t0)
+            rays = r.last_timings["rays"]
+            gpu = r.last_timings["gpu_ms"]
+        wall = min(walls)
+    return {"workload": "64 jobs: configs 1-3 rescaled to 10k-4M tris (9 scenes), resolutions {128^2, 256^2, "
+                        "512^2, 720p, 1080p}, spp {1, 4, 16}, seeded cameras",
+            "paths": workloads.request_paths(requests),
+            "mrays_per_s": rays / wall / 1e6, "gpu_mrays_per_s": rays / (gpu * 1e3),
+            "plain_mrays_per_s": plain_rays / plain_wall / 1e6,
+            "plain_gpu_mrays_per_s": plain_rays / (plain_gpu * 1e3),
+            "speedup": (rays / wall) / (plain_rays / plain_wall), "batch_s": wall, "plain_s": plain_wall,
+            "tuned": tuned}
+
+
+def run_served(device_index, rate, count, budget_bytes):
+    """Poisson request stream over 8 resident scenes: the continuous-batching
+    server against the plain path serving the stream one request at a time
+    in arrival order (the reference's serialised render_async worker)."""
+    import torch
+
+    from ordinarylight_b200 import CudaWavefrontRenderer, workloads
+    from ordinarylight_b200.serving import RenderServer, poisson_arrivals, run_stream
+
+    variants = workloads.served_scene_variants()
+    requests = workloads.served_requests(variants, count, seed=5)
+    arrivals = poisson_arrivals(rate, count, seed=6)
+    with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
+                               restir_neighbours=5, restir_radius=30.0, seed=1) as r:
+        for v in variants:
+            r.resident_scene(v[0])
+        warm = workloads.served_requests(variants, 8, seed=99)
+        r.render_batch(warm)
+        # plain arm: FIFO, one request at a time; latency = completion - arrival
+        service, plain_rays = [], 0
+        for q in requests:
+            t0 = time.perf_counter()
+            r.render_batch([q])
+            service.append(time.perf_counter() - t0)
+            plain_rays += r.last_timings["rays"]
+        finish, lat = 0.0, []
+        for at, sv in zip(arrivals, service):
+            finish = max(finish, at) + sv
+            lat.append((finish - at) * 1e3)
+        plain_wall = finish - arrivals[0]
+        # served arm, real-time arrivals
+        torch.cuda.synchronize()
+        server = RenderServer(r, budget_bytes=budget_bytes).start()
+        futures = run_stream(server, requests, arrivals)
+        server.stop()
+        summary = server.stats.summary()
+        ok = sum(1 for f in futures if f.exception() is None)
+    return {"workload": f"{count} requests, Poisson {rate:g} req/s, 8 resident scenes (10k-8.4M tris), "
+                        "resolutions {256^2, 512^2, 720p, 1080p}, spp {1, 4, 16}, bounces {4, 8}, "
+                        f"HBM budget {budget_bytes / 1e9:g} GB",
+            "requests": count, "completed": ok, "rejected": summary["rejected"], "failed": summary["failed"],
+            "p50_ms": summary["p50_ms"], "p99_ms": summary["p99_ms"], "mean_ms": summary["mean_ms"],
+            "throughput_req_s": summary["throughput_req_s"], "mrays_per_s": summary["mrays_per_s"],
+            "steps": summary["steps"],
+            "plain": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "mean_ms": float(np.mean(lat)), "throughput_req_s": count / plain_wall,
+                      "mrays_per_s": plain_rays / plain_wall / 1e6,
+                      "mean_service_ms": float(np.mean(service) * 1e3)},
+            "speedup_mrays": summary["mrays_per_s"] / (plain_rays / plain_wall / 1e6)}
 
 
 def run_reference_arm(args):
@@ -425,6 +622,11 @@ def main():
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--cpu-processes", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sections", default="config1,config3,batched,served",
+                   help="secondary sections run at N=1 (comma list; empty for the headline alone)")
+    p.add_argument("--served-rate", type=float, default=50.0)
+    p.add_argument("--served-requests", type=int, default=150)
+    p.add_argument("--served-budget-gb", type=float, default=150.0)
     args = p.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -447,10 +649,21 @@ def main():
                                 device_id=torch.device(f"cuda:{local}"))
     try:
         line = run_ours(args, rank, world, local)
-        if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            value, cores, sample = cpu_reference_measure(args.cpu_steps, args.cpu_processes)
-            line["cpu_baseline"] = {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
-                                    "sample": sample}
+        if rank == 0 and world == 1:
+            sections = [x for x in args.sections.split(",") if x]
+            if "config1" in sections:
+                line["config1"] = run_config1(local, args.cpu_processes)
+            if "config3" in sections:
+                line["config3"] = run_config3(local)
+            if "batched" in sections:
+                line["batched"] = run_batched(local)
+            if "served" in sections:
+                line["served"] = run_served(local, args.served_rate, args.served_requests,
+                                            args.served_budget_gb * 1e9)
+            if not args.no_cpu_baseline:
+                value, cores, sample = cpu_reference_measure(args.cpu_steps, args.cpu_processes)
+                line["cpu_baseline"] = {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                                        "sample": sample}
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -193,7 +193,10 @@ typedef struct olc_render_stats {
   float raygen_ms, trace_ms, shade_ms, shadow_ms, restir_ms, accumulate_ms;
   uint32_t chunks;
   uint32_t restir_history_used;
-  uint32_t reserved[6];
+  uint32_t jobs_completed;   /* jobs resolved by the call */
+  uint32_t reserved;
+  uint64_t h2d_bytes;        /* host->device bytes of the call (chunk tables) */
+  uint64_t d2h_bytes;        /* device->host bytes (counters, host outputs) */
 } olc_render_stats;
 
 /* ---- context --------------------------------------------------------- */

@@ -80,7 +80,8 @@ class OlcRenderStats(ctypes.Structure):
         ("overflow", c_uint64), ("traversal_errors", c_uint64), ("gpu_ms", c_float),
         ("raygen_ms", c_float), ("trace_ms", c_float), ("shade_ms", c_float), ("shadow_ms", c_float),
         ("restir_ms", c_float), ("accumulate_ms", c_float), ("chunks", c_uint32),
-        ("restir_history_used", c_uint32), ("reserved", c_uint32 * 6),
+        ("restir_history_used", c_uint32), ("jobs_completed", c_uint32), ("reserved", c_uint32),
+        ("h2d_bytes", c_uint64), ("d2h_bytes", c_uint64),
     ]
 
 

@@ -1207,6 +1207,11 @@ void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
     }
     OLC_CUDA(cudaEventElapsedTime(&stats->gpu_ms, ctx->ev_begin, ctx->ev_end));
     stats->chunks = nchunks;
+    stats->jobs_completed = (uint32_t)plan.finished.size();
+    stats->h2d_bytes = bytes;
+    stats->d2h_bytes = (uint64_t)nchunks * sizeof(Counters);
+    for (const QueuedJob* j : plan.finished)
+      if (j->out && !j->out_device) stats->d2h_bytes += (uint64_t)j->rec.npix * sizeof(float4);
   }
 }
 

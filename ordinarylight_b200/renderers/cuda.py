@@ -249,6 +249,8 @@ class CudaWavefrontRenderer(RendererImplementation):
             "chunks": int(stats.chunks),
             "restir_history_used": bool(stats.restir_history_used),
             "samples_per_pixel": spp,
+            "h2d_bytes": int(stats.h2d_bytes),
+            "d2h_bytes": int(stats.d2h_bytes),
         }
         if stats.traversal_errors:
             raise RuntimeError(f"{stats.traversal_errors} traversal stack overflows")
@@ -394,6 +396,8 @@ class CudaWavefrontRenderer(RendererImplementation):
             "queue_overflow": int(stats.overflow),
             "traversal_errors": int(stats.traversal_errors),
             "chunks": int(stats.chunks),
+            "h2d_bytes": int(stats.h2d_bytes),
+            "d2h_bytes": int(stats.d2h_bytes),
             **extra,
         }
         if stats.traversal_errors:

@@ -50,13 +50,29 @@ def _box(size):
     return v, np.array(idx, np.uint32)
 
 
-def box_room(module=None, *, light=ROOM_LIGHT):
+def _tessellate(quad, n):
+    """Split the quad (4 vertices, 2 triangles) into an n x n grid of quads."""
+    v, _ = quad
+    a, b, c, d = (np.asarray(x, np.float64) for x in v)
+    s = np.linspace(0.0, 1.0, n + 1)
+    u, w = np.meshgrid(s, s, indexing="ij")
+    pts = ((1 - u)[..., None] * (1 - w)[..., None] * a + u[..., None] * (1 - w)[..., None] * b
+           + u[..., None] * w[..., None] * c + (1 - u)[..., None] * w[..., None] * d)
+    grid = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    p0, p1, p2, p3 = grid[:-1, :-1], grid[1:, :-1], grid[1:, 1:], grid[:-1, 1:]
+    idx = np.concatenate([np.stack([p0, p1, p2], -1).reshape(-1, 3), np.stack([p0, p2, p3], -1).reshape(-1, 3)])
+    return pts.reshape(-1, 3).astype(np.float32), idx.astype(np.uint32)
+
+
+def box_room(module=None, *, light=ROOM_LIGHT, tessellation=1):
     """The closed-box room (36 triangles: 10 walls, 24 inner boxes, 2 emitter).
 
     Returns (scene, camera).  Geometry: walls x in [-1, 1], y in [0, 2],
     z in [-1, 1], front (z = -1) open; the emitter quad hangs 1e-3 below the
     ceiling and faces down; the inner boxes stand on the floor, rotated
-    about y by -18 and +15 degrees.
+    about y by -18 and +15 degrees.  ``tessellation`` n > 1 splits each wall
+    into n x n quads (10 n^2 wall triangles), the same room with more
+    geometry for the rescaled variants of the batched and served workloads.
     """
     m = module or _scene_module
     scene = m.Scene()
@@ -70,6 +86,8 @@ def box_room(module=None, *, light=ROOM_LIGHT):
         (_quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1)), red, "left"),
         (_quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)), green, "right"),
     ]
+    if tessellation > 1:
+        walls = [(_tessellate(q, int(tessellation)), mat, name) for q, mat, name in walls]
     for (v, i), mat, name in walls:
         scene.add_mesh(v, i, mat, name=name)
     short_v, short_i = _box((0.6, 0.6, 0.6))
