@@ -69,6 +69,7 @@ BYTES_PER_UNIT = {
     "restir": 408.0,         # ray+hit 52, reservoir write 32, history read 32; spatial: ray+hit 52,
                              # 6 reservoir reads 192, write 32, selected sample 16
     "resolve": 40.0,         # read 24 B fixed-point sums, write 16 B pixel
+    "sort": 104.0,           # key pass: read ray 32, write key 4; scatter: read key 4 + ray 32, write ray 32
 }
 
 
@@ -302,7 +303,8 @@ def run_ours(args, rank, world, device_index):
             stage_ms[stage] = stage_ms.get(stage, 0.0) + ms
             stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, items, misses)
             stage_launches[stage] = stage_launches.get(stage, 0) + 1
-            launches += 3 if stage == "restir" else 1   # compaction, initial, one spatial pass
+            launches += 3 if stage in ("restir", "sort") else 1   # restir: compaction, initial, one spatial
+                                                                     # pass; sort: keys, scan, scatter
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -322,6 +324,8 @@ def run_ours(args, rank, world, device_index):
 
     # end to end through the public API: host output, per-step host clock
     e2e_steps = max(1, min(args.steps, 5))
+    for k in range(2):   # page-locked output buffers come from a cache that warms up here
+        renderer.render_frame(scene, camera, WIDTH, HEIGHT, frame_index=frame0 + 490 + k)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_rays, h2d, d2h = 0, 0, 0
@@ -473,23 +477,55 @@ def run_config3(device_index, steps=5):
             "stage_ms_per_frame": stage}
 
 
+def _plain_frames(device_index, requests, limit=None):
+    """The plain per-request path as a user drives it: one renderer,
+    ``render_frame`` per request (the scene is uploaded and its BVH built
+    whenever it differs from the previous request's, as the reference's
+    resident-scene cache does), bounce limit set by ``reconfigure``.
+    Returns (service seconds per request, rays per request)."""
+    from ordinarylight_b200 import CudaWavefrontRenderer
+
+    service, rays = [], []
+    with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
+                               restir_neighbours=5, restir_radius=30.0, seed=1) as r:
+        for q in requests[:limit]:
+            t0 = time.perf_counter()
+            if q.max_bounces is not None and q.max_bounces != r.config.max_bounces:
+                r.reconfigure(max_bounces=q.max_bounces)
+            r.render_frame(q.scene, q.camera, q.width, q.height, samples=q.samples, frame_index=q.frame_index)
+            service.append(time.perf_counter() - t0)
+            rays.append(r.last_timings["rays"])
+    return service, rays
+
+
+def _fifo_latency_ms(arrivals, service):
+    """Completion minus arrival of a single FIFO worker."""
+    finish, lat = 0.0, []
+    for at, sv in zip(arrivals, service):
+        finish = max(finish, at) + sv
+        lat.append((finish - at) * 1e3)
+    return lat, finish - arrivals[0]
+
+
 def run_batched(device_index, tune=True):
     """64 jobs over nine rescaled configuration scenes: one wavefront after
-    the autotuner, against the same jobs rendered one at a time (each job
-    alone in the executor; scenes resident in both arms)."""
+    the autotuner, against the same jobs one at a time, both through
+    render_frame (scene uploads on change) and with every scene resident."""
     import torch
 
     from ordinarylight_b200 import CudaWavefrontRenderer, workloads
     from ordinarylight_b200.autotune import autotune
+    from ordinarylight_b200.renderers.cuda import host_image
 
     variants = workloads.batch_scene_variants()
     requests = workloads.batch_requests(variants, 64, seed=4)
-    outs = [np.empty((r.height, r.width, 4), np.float32) for r in requests]
+    outs = [host_image(r.height, r.width) for r in requests]
+    frame_service, frame_rays = _plain_frames(device_index, requests)
     with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
                                restir_neighbours=5, restir_radius=30.0, seed=1) as r:
         for v in variants:
             r.resident_scene(v[0])
-        # plain arm: one job per run
+        # one job per run, scenes resident
         for q, o in zip(requests[:4], outs[:4]):
             r.render_batch([q], [o])
         torch.cuda.synchronize()
@@ -504,7 +540,10 @@ def run_batched(device_index, tune=True):
         if tune:
             res = autotune(r, requests, repeats=1)
             tuned = {"chunk_paths": res.chunk_paths, "block_size": res.block_size, "trace_block": res.trace_block,
-                     "stack_depth": res.stack_depth, "trials": len(res.trials), "best_s": res.seconds}
+                     "stack_depth": res.stack_depth, "sort_rays": res.sort_rays, "trials": len(res.trials),
+                     "best_s": res.seconds,
+                     "trial_s": [(t[0]["chunk_paths"], t[0]["block_size"], t[0]["trace_block"], t[0]["stack_depth"],
+                                  t[0]["sort_rays"], round(t[1], 4)) for t in res.trials]}
         r.render_batch(requests, outs)
         torch.cuda.synchronize()
         walls, rays, gpu = [], 0, 0.0
@@ -515,20 +554,25 @@ def run_batched(device_index, tune=True):
             rays = r.last_timings["rays"]
             gpu = r.last_timings["gpu_ms"]
         wall = min(walls)
+    frame_mrays = sum(frame_rays) / sum(frame_service) / 1e6
     return {"workload": "64 jobs: configs 1-3 rescaled to 10k-4M tris (9 scenes), resolutions {128^2, 256^2, "
                         "512^2, 720p, 1080p}, spp {1, 4, 16}, seeded cameras",
             "paths": workloads.request_paths(requests),
-            "mrays_per_s": rays / wall / 1e6, "gpu_mrays_per_s": rays / (gpu * 1e3),
-            "plain_mrays_per_s": plain_rays / plain_wall / 1e6,
-            "plain_gpu_mrays_per_s": plain_rays / (plain_gpu * 1e3),
-            "speedup": (rays / wall) / (plain_rays / plain_wall), "batch_s": wall, "plain_s": plain_wall,
+            "mrays_per_s": rays / wall / 1e6, "gpu_mrays_per_s": rays / (gpu * 1e3), "batch_s": wall,
+            "plain_frame_mrays_per_s": frame_mrays, "plain_frame_s": sum(frame_service),
+            "speedup_vs_plain_frame": (rays / wall / 1e6) / frame_mrays,
+            "plain_resident_mrays_per_s": plain_rays / plain_wall / 1e6,
+            "plain_resident_gpu_mrays_per_s": plain_rays / (plain_gpu * 1e3), "plain_resident_s": plain_wall,
+            "speedup_vs_plain_resident": (rays / wall) / (plain_rays / plain_wall),
             "tuned": tuned}
 
 
-def run_served(device_index, rate, count, budget_bytes):
+def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit=40):
     """Poisson request stream over 8 resident scenes: the continuous-batching
     server against the plain path serving the stream one request at a time
-    in arrival order (the reference's serialised render_async worker)."""
+    in arrival order (the reference's serialised render_async worker), both
+    through render_frame (scene uploads on change; the first `frame_limit`
+    requests) and with every scene resident (all requests)."""
     import torch
 
     from ordinarylight_b200 import CudaWavefrontRenderer, workloads
@@ -537,24 +581,22 @@ def run_served(device_index, rate, count, budget_bytes):
     variants = workloads.served_scene_variants()
     requests = workloads.served_requests(variants, count, seed=5)
     arrivals = poisson_arrivals(rate, count, seed=6)
+    frame_service, frame_rays = _plain_frames(device_index, requests, frame_limit)
+    frame_lat, frame_wall = _fifo_latency_ms(arrivals[:frame_limit], frame_service)
     with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
-                               restir_neighbours=5, restir_radius=30.0, seed=1) as r:
+                               restir_neighbours=5, restir_radius=30.0, seed=1, chunk_paths=chunk_paths) as r:
         for v in variants:
             r.resident_scene(v[0])
         warm = workloads.served_requests(variants, 8, seed=99)
         r.render_batch(warm)
-        # plain arm: FIFO, one request at a time; latency = completion - arrival
+        # plain with resident scenes: FIFO, one request at a time
         service, plain_rays = [], 0
         for q in requests:
             t0 = time.perf_counter()
             r.render_batch([q])
             service.append(time.perf_counter() - t0)
             plain_rays += r.last_timings["rays"]
-        finish, lat = 0.0, []
-        for at, sv in zip(arrivals, service):
-            finish = max(finish, at) + sv
-            lat.append((finish - at) * 1e3)
-        plain_wall = finish - arrivals[0]
+        lat, plain_wall = _fifo_latency_ms(arrivals, service)
         # served arm, real-time arrivals
         torch.cuda.synchronize()
         server = RenderServer(r, budget_bytes=budget_bytes).start()
@@ -562,18 +604,24 @@ def run_served(device_index, rate, count, budget_bytes):
         server.stop()
         summary = server.stats.summary()
         ok = sum(1 for f in futures if f.exception() is None)
+    frame_mrays = sum(frame_rays) / frame_wall / 1e6
     return {"workload": f"{count} requests, Poisson {rate:g} req/s, 8 resident scenes (10k-8.4M tris), "
                         "resolutions {256^2, 512^2, 720p, 1080p}, spp {1, 4, 16}, bounces {4, 8}, "
-                        f"HBM budget {budget_bytes / 1e9:g} GB",
+                        f"HBM budget {budget_bytes / 1e9:g} GB, chunk {chunk_paths} paths",
             "requests": count, "completed": ok, "rejected": summary["rejected"], "failed": summary["failed"],
             "p50_ms": summary["p50_ms"], "p99_ms": summary["p99_ms"], "mean_ms": summary["mean_ms"],
             "throughput_req_s": summary["throughput_req_s"], "mrays_per_s": summary["mrays_per_s"],
             "steps": summary["steps"],
-            "plain": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                      "mean_ms": float(np.mean(lat)), "throughput_req_s": count / plain_wall,
-                      "mrays_per_s": plain_rays / plain_wall / 1e6,
-                      "mean_service_ms": float(np.mean(service) * 1e3)},
-            "speedup_mrays": summary["mrays_per_s"] / (plain_rays / plain_wall / 1e6)}
+            "plain_frame": {"requests": frame_limit, "p50_ms": float(np.percentile(frame_lat, 50)),
+                            "p99_ms": float(np.percentile(frame_lat, 99)),
+                            "throughput_req_s": frame_limit / frame_wall, "mrays_per_s": frame_mrays,
+                            "mean_service_ms": float(np.mean(frame_service) * 1e3)},
+            "plain_resident": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                               "mean_ms": float(np.mean(lat)), "throughput_req_s": count / plain_wall,
+                               "mrays_per_s": plain_rays / plain_wall / 1e6,
+                               "mean_service_ms": float(np.mean(service) * 1e3)},
+            "speedup_mrays_vs_plain_frame": summary["mrays_per_s"] / frame_mrays,
+            "speedup_mrays_vs_plain_resident": summary["mrays_per_s"] / (plain_rays / plain_wall / 1e6)}
 
 
 def run_reference_arm(args):
@@ -624,9 +672,11 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--sections", default="config1,config3,batched,served",
                    help="secondary sections run at N=1 (comma list; empty for the headline alone)")
-    p.add_argument("--served-rate", type=float, default=50.0)
+    p.add_argument("--served-rates", default="50,100",
+                   help="Poisson arrival rates (req/s); the first is reported as `served`, all in `served_sweep`")
     p.add_argument("--served-requests", type=int, default=150)
     p.add_argument("--served-budget-gb", type=float, default=150.0)
+    p.add_argument("--served-chunk", type=int, default=1 << 23)
     args = p.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -658,8 +708,12 @@ def main():
             if "batched" in sections:
                 line["batched"] = run_batched(local)
             if "served" in sections:
-                line["served"] = run_served(local, args.served_rate, args.served_requests,
-                                            args.served_budget_gb * 1e9)
+                sweep = [run_served(local, float(rate), args.served_requests, args.served_budget_gb * 1e9,
+                                    args.served_chunk) for rate in args.served_rates.split(",") if rate]
+                line["served"] = sweep[0]
+                line["served_sweep"] = [{k: v[k] for k in ("workload", "p50_ms", "p99_ms", "throughput_req_s",
+                                                          "mrays_per_s", "rejected", "plain_resident",
+                                                          "plain_frame")} for v in sweep]
             if not args.no_cpu_baseline:
                 value, cores, sample = cpu_reference_measure(args.cpu_steps, args.cpu_processes)
                 line["cpu_baseline"] = {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",

@@ -115,7 +115,10 @@ typedef struct olc_config {
                                    estimation (pure BSDF sampling) */
   uint32_t trace_block;         /* threads per block of the traversal and
                                    shading kernels: 64, 128 or 256; 0 = 128 */
-  uint32_t reserved[4];
+  uint32_t ray_sort;            /* reorder extension rays by origin cell and
+                                   direction before tracing them (helps
+                                   shading coherence on large scenes) */
+  uint32_t reserved[3];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the
@@ -309,11 +312,15 @@ OLC_API int olc_render_batch(olc_context* ctx, const olc_job* jobs, uint32_t num
  * valid until the ticket is reported complete. */
 OLC_API int olc_submit(olc_context* ctx, const olc_job* job, uint64_t* ticket);
 
-/* Run one chunk (at most chunk_paths paths) drawn from the queued jobs,
- * shortest remaining work first (a job passed over for 8 steps goes first),
- * then resolve and copy out the jobs whose last paths were in it.  done (host, capacity done_capacity) receives their tickets
- * and num_done their count; stats (may be NULL) the chunk's statistics.
- * Jobs submitted between steps join the next chunk. */
+/* One serving step: launch the next chunk (at most chunk_paths paths) drawn
+ * from the queued jobs, shortest remaining work first (a job passed over for
+ * 8 steps goes first), then wait for the chunk the previous step launched
+ * and report the jobs whose last paths were in it (resolved and copied out).
+ * Keeping one chunk in flight hides the host work of a step behind the
+ * device work of the previous one.  done (host, capacity done_capacity)
+ * receives the tickets and num_done their count; stats (may be NULL) the
+ * collected chunk's statistics.  Jobs submitted between steps join the next
+ * chunk; a job is queued until a step reports it. */
 OLC_API int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity,
                            uint32_t* num_done, olc_render_stats* stats);
 
@@ -367,7 +374,8 @@ enum olc_stage {
   OLC_STAGE_SHADE = 3,
   OLC_STAGE_SHADOW = 4,
   OLC_STAGE_ACCUMULATE = 5,
-  OLC_STAGE_RESOLVE = 6
+  OLC_STAGE_RESOLVE = 6,
+  OLC_STAGE_SORT = 7
 };
 typedef struct olc_launch_record {
   uint32_t stage;

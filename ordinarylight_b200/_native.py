@@ -45,7 +45,7 @@ class OlcConfig(ctypes.Structure):
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
         ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
         ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("trace_block", c_uint32),
-        ("reserved", c_uint32 * 4),
+        ("ray_sort", c_uint32), ("reserved", c_uint32 * 3),
     ]
 
 
@@ -122,7 +122,7 @@ class OlcJob(ctypes.Structure):
     ]
 
 
-STAGE_NAMES = ("raygen", "trace_closest", "restir", "shade", "trace_shadow", "accumulate", "resolve")
+STAGE_NAMES = ("raygen", "trace_closest", "restir", "shade", "trace_shadow", "accumulate", "resolve", "sort")
 
 
 # Exported symbols and their signatures (argument types, all return int

@@ -1,15 +1,18 @@
 """Launch-shape autotuner for batched rendering.
 
-The wavefront's throughput depends on three knobs that have no single best
-value across workloads: the chunk size (paths resident per wavefront: small
+The wavefront's throughput depends on knobs that have no single best value
+across workloads: the chunk size (paths resident per wavefront: small
 chunks keep the working set in L2, large ones amortise launches and keep
 every SM busy on the short queues of late bounces), the block shape of the
-queue and traversal kernels, and the traversal short-stack depth (shared
-memory per thread against spills to local memory).  :func:`autotune` times a
-given batch under candidate settings and leaves the renderer configured
-with the fastest.  The search is coordinate descent (chunk size, then block
-shape, then stack depth), 4 + 4 + 3 timed batches instead of the 48 of the
-full grid; results are cached per workload signature.
+queue and traversal kernels, the traversal short-stack depth (shared memory
+per thread against spills to local memory) and whether extension rays are
+reordered by origin and direction before tracing (better shading coherence
+on large scenes, at the cost of the reordering passes).  :func:`autotune`
+times a given batch under candidate settings and leaves the renderer
+configured with the fastest.  The search is coordinate descent (chunk size,
+block shape, stack depth, ray reordering), 4 + 4 + 3 + 2 timed batches
+instead of the 96 of the full grid; results are cached per workload
+signature.
 
 Changing these knobs never changes an image: the random numbers are keyed
 per path and accumulation is order independent.
@@ -23,6 +26,7 @@ import time
 CHUNKS = (1 << 16, 1 << 18, 1 << 20, 1 << 22)
 BLOCKS = ((64, 64), (128, 128), (256, 128), (512, 256))   # (queue kernels, traversal/shading)
 STACKS = (16, 24, 32)
+SORTS = (False, True)
 
 _cache: dict = {}
 
@@ -33,6 +37,7 @@ class TuneResult:
     block_size: int
     trace_block: int
     stack_depth: int
+    sort_rays: bool
     seconds: float
     trials: list = field(default_factory=list)
 
@@ -52,23 +57,25 @@ def _time_batch(renderer, requests, outs, repeats: int) -> float:
     return best
 
 
-def autotune(renderer, requests, *, chunks=CHUNKS, blocks=BLOCKS, stacks=STACKS, repeats: int = 2,
+def autotune(renderer, requests, *, chunks=CHUNKS, blocks=BLOCKS, stacks=STACKS, sorts=SORTS, repeats: int = 2,
              use_cache: bool = True) -> TuneResult:
-    """Find the fastest (chunk_paths, block shape, stack_depth) for
-    ``renderer.render_batch(requests)`` and apply it to the renderer."""
+    """Find the fastest (chunk_paths, block shape, stack_depth, ray
+    reordering) for ``renderer.render_batch(requests)`` and apply it to the
+    renderer."""
     requests = list(requests)
     key = (workload_signature(requests), renderer.config.mode, renderer.config.restir)
     if use_cache and key in _cache:
         result = _cache[key]
         renderer.reconfigure(chunk_paths=result.chunk_paths, block_size=result.block_size,
-                             trace_block=result.trace_block, stack_depth=result.stack_depth)
+                             trace_block=result.trace_block, stack_depth=result.stack_depth,
+                             sort_rays=result.sort_rays)
         return result
     import numpy as np
 
     outs = [np.empty((int(r.height), int(r.width), 4), np.float32) for r in requests]
     cfg = renderer.config
     current = {"chunk_paths": cfg.chunk_paths or chunks[-1], "block_size": cfg.block_size,
-               "trace_block": cfg.trace_block, "stack_depth": cfg.stack_depth}
+               "trace_block": cfg.trace_block, "stack_depth": cfg.stack_depth, "sort_rays": cfg.sort_rays}
     trials = []
 
     def trial(**changes):
@@ -81,7 +88,8 @@ def autotune(renderer, requests, *, chunks=CHUNKS, blocks=BLOCKS, stacks=STACKS,
     best = trial()
     for name, values in (("chunk_paths", [{"chunk_paths": c} for c in chunks]),
                          ("block", [{"block_size": b, "trace_block": t} for b, t in blocks]),
-                         ("stack_depth", [{"stack_depth": s} for s in stacks])):
+                         ("stack_depth", [{"stack_depth": s} for s in stacks]),
+                         ("sort_rays", [{"sort_rays": bool(v)} for v in sorts])):
         choice = None
         for changes in values:
             if all(current.get(k) == v for k, v in changes.items()):
@@ -93,9 +101,9 @@ def autotune(renderer, requests, *, chunks=CHUNKS, blocks=BLOCKS, stacks=STACKS,
             current.update(choice)
     renderer.reconfigure(**current)
     result = TuneResult(current["chunk_paths"], current["block_size"], current["trace_block"],
-                        current["stack_depth"], best, trials)
+                        current["stack_depth"], current["sort_rays"], best, trials)
     _cache[key] = result
     return result
 
 
-__all__ = ["autotune", "TuneResult", "workload_signature", "CHUNKS", "BLOCKS", "STACKS"]
+__all__ = ["autotune", "TuneResult", "workload_signature", "CHUNKS", "BLOCKS", "STACKS", "SORTS"]

@@ -180,6 +180,7 @@ struct QueuedJob {
   Range pixels;              // accumulator / output arena range
   float* out = nullptr;
   bool out_device = false;
+  bool out_staged = false;   // pageable host output: copied through the run's pinned staging
   // ReSTIR reservoirs at job-local indices (reservoir_base 0), where the next
   // plain frame's temporal pass finds them; otherwise chunk-local ones
   bool job_local_reservoirs = false;
@@ -212,6 +213,30 @@ struct GraphEntry {
   uint64_t last_used = 0;
 };
 
+// Host-visible state of one run: its tables (pinned staging and device
+// copy), the counters it copies back, its launch timeline and bracketing
+// events, and its plan.  Two slots let a serving step launch the next chunk
+// before it waits for the previous one.
+struct RunSlot {
+  DeviceBuffer table_dev;
+  char* table_host = nullptr;        // pinned
+  size_t table_capacity = 0;
+  size_t table_bytes = 0;            // bytes staged for the current run
+  Counters* counters_host = nullptr; // pinned, one per chunk
+  uint32_t counters_chunks = 0;
+  std::vector<cudaEvent_t> events;   // events[k] .. events[k+1] brackets launch k
+  std::vector<TimelineEntry> entries;
+  cudaEvent_t begin = nullptr, end = nullptr, done = nullptr;
+  // Pageable host outputs are copied into this pinned staging buffer by the
+  // device and from it by the host when the run is collected, so the
+  // device-to-host copy is asynchronous and overlaps the next run.
+  float4* staging = nullptr;
+  size_t staging_pixels = 0;
+  std::vector<std::pair<QueuedJob*, size_t>> staged;   // job, first staging pixel
+  RunPlan plan;
+  bool busy = false;
+};
+
 }  // namespace
 
 struct olc_context {
@@ -219,7 +244,6 @@ struct olc_context {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
   std::string error;
   BuildScratch scratch;
   LaunchShape ls;
@@ -236,24 +260,20 @@ struct olc_context {
   uint32_t default_scene = kNoScene;
   // wavefront buffers
   uint32_t capacity = 0;
-  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp, ps_rad, ps_meta;
+  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
+      ps_rad, ps_meta, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim;
   uint32_t prod_pixels = 0;
   PoolGroup pixels{{3 * sizeof(unsigned long long), sizeof(float4)}, 1 << 16};
-  // run tables: chunk headers + segments, then the resolve list
-  DeviceBuffer table_dev;
-  char* table_host = nullptr;  // pinned
-  size_t table_bytes = 0;
+  // run tables (chunk headers + segments, then the resolve list) per slot
+  RunSlot runs[2];
+  RunSlot* cur = nullptr;            // slot being recorded
+  int inflight = -1;                 // serving run launched but not yet finished
   uint32_t seg_capacity = 64;
-  Counters* counters_host = nullptr;  // pinned, one per chunk
-  uint32_t counters_host_chunks = 0;
   RestirState restir;
   std::map<std::vector<uint64_t>, GraphEntry> graphs;
   uint64_t graph_clock = 0;
-  // device timeline: events[k] .. events[k+1] brackets launch k
-  std::vector<cudaEvent_t> tl_events;
-  std::vector<TimelineEntry> tl_entries;
   bool capturing = false;
   std::vector<olc_launch_record> last_profile;
   std::vector<uint32_t> last_chunk_counts;
@@ -315,36 +335,39 @@ void apply_launch_shape(olc_context* ctx) {
   ctx->ls.trace_block = tb;
   ctx->ls.stack_depth = ctx->cfg.stack_depth ? ctx->cfg.stack_depth : 24;
   ctx->ls.scheduler = ctx->cfg.trace_scheduler;
+  ctx->ls.sort_rays = ctx->cfg.ray_sort ? 1u : 0u;
   ctx->ls.grid_simple = ctx->sm_count * 8;
   ctx->ls.grid_shade = ctx->sm_count * (1536 / tb);
   ctx->ls.grid_trace = ctx->sm_count * (1536 / tb);
 }
 
 void drop_graphs(olc_context* ctx) {
+  if (!ctx->graphs.empty()) cudaStreamSynchronize(ctx->stream);   // none may still run
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   ctx->graphs.clear();
 }
 
 void tl_record(olc_context* ctx, size_t index) {
-  while (ctx->tl_events.size() <= index) {
+  RunSlot& sl = *ctx->cur;
+  while (sl.events.size() <= index) {
     cudaEvent_t e;
     OLC_CUDA(cudaEventCreate(&e));
-    ctx->tl_events.push_back(e);
+    sl.events.push_back(e);
   }
   if (ctx->capturing)
-    OLC_CUDA(cudaEventRecordWithFlags(ctx->tl_events[index], ctx->stream, cudaEventRecordExternal));
+    OLC_CUDA(cudaEventRecordWithFlags(sl.events[index], ctx->stream, cudaEventRecordExternal));
   else
-    OLC_CUDA(cudaEventRecord(ctx->tl_events[index], ctx->stream));
+    OLC_CUDA(cudaEventRecord(sl.events[index], ctx->stream));
 }
 
 void tl_begin(olc_context* ctx) {
-  ctx->tl_entries.clear();
+  ctx->cur->entries.clear();
   tl_record(ctx, 0);
 }
 
 void tl_mark(olc_context* ctx, uint32_t stage, uint32_t bounce, uint32_t chunk) {
-  ctx->tl_entries.push_back(TimelineEntry{stage, bounce, chunk});
-  tl_record(ctx, ctx->tl_entries.size());
+  ctx->cur->entries.push_back(TimelineEntry{stage, bounce, chunk});
+  tl_record(ctx, ctx->cur->entries.size());
 }
 
 // Inverse of a row-major 3x4 affine (double precision on the host).
@@ -904,6 +927,11 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   ctx->q1_o.allocate(c * 16);
   ctx->q1_d.allocate(c * 16);
   ctx->q1_p.allocate(c * 4);
+  ctx->q2_o.allocate(c * 16);
+  ctx->q2_d.allocate(c * 16);
+  ctx->q2_p.allocate(c * 4);
+  ctx->sort_keys.allocate(c * 4);
+  if (!ctx->sort_bins.get()) ctx->sort_bins.allocate(sort_bins_bytes());
   ctx->hit_tuv.allocate(c * 16);
   ctx->hit_inst.allocate(c * 4);
   ctx->sh_o.allocate(c * 16);
@@ -930,30 +958,45 @@ void ensure_products(olc_context* ctx, uint32_t npix) {
 
 size_t chunk_stride(uint32_t seg_capacity) { return sizeof(ChunkHeader) + (size_t)seg_capacity * sizeof(JobRec); }
 
-void ensure_host_counters(olc_context* ctx, uint32_t chunks) {
-  if (chunks <= ctx->counters_host_chunks) return;
-  if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
-  ctx->counters_host = nullptr;
-  ctx->counters_host_chunks = 0;
-  OLC_CUDA(cudaMallocHost(&ctx->counters_host, sizeof(Counters) * chunks));
-  ctx->counters_host_chunks = chunks;
+void ensure_host_counters(olc_context* ctx, RunSlot& sl, uint32_t chunks) {
+  if (chunks <= sl.counters_chunks) return;
+  if (sl.counters_host) cudaFreeHost(sl.counters_host);
+  sl.counters_host = nullptr;
+  sl.counters_chunks = 0;
+  OLC_CUDA(cudaMallocHost(&sl.counters_host, sizeof(Counters) * chunks));
+  sl.counters_chunks = chunks;
   drop_graphs(ctx);
 }
 
-void ensure_table(olc_context* ctx, size_t bytes) {
-  if (bytes <= ctx->table_bytes) return;
+void ensure_table(olc_context* ctx, RunSlot& sl, size_t bytes) {
+  if (bytes <= sl.table_capacity) return;
   size_t b = std::max<size_t>(bytes, 64 * 1024);
-  ctx->table_dev.allocate(b);
-  if (ctx->table_host) cudaFreeHost(ctx->table_host);
-  ctx->table_host = nullptr;
-  ctx->table_bytes = 0;
-  OLC_CUDA(cudaMallocHost(&ctx->table_host, b));
-  ctx->table_bytes = b;
+  sl.table_dev.allocate(b);
+  if (sl.table_host) cudaFreeHost(sl.table_host);
+  sl.table_host = nullptr;
+  sl.table_capacity = 0;
+  OLC_CUDA(cudaMallocHost(&sl.table_host, b));
+  sl.table_capacity = b;
   drop_graphs(ctx);
+}
+
+void release_slot(RunSlot& sl) {
+  if (sl.table_host) cudaFreeHost(sl.table_host);
+  if (sl.counters_host) cudaFreeHost(sl.counters_host);
+  if (sl.staging) cudaFreeHost(sl.staging);
+  sl.table_host = nullptr;
+  sl.counters_host = nullptr;
+  sl.staging = nullptr;
+  sl.staging_pixels = 0;
+  for (cudaEvent_t e : sl.events) cudaEventDestroy(e);
+  sl.events.clear();
+  for (cudaEvent_t* e : {&sl.begin, &sl.end, &sl.done})
+    if (*e) cudaEventDestroy(*e);
+  sl.table_dev.release();
 }
 
 struct RunBuffers {
-  RayQueue qa, qb;
+  RayQueue qa, qb, qc;
   HitBuf hb;
   ShadowQueue sq;
   PathState ps;
@@ -966,10 +1009,11 @@ struct RunBuffers {
   size_t resolve_offset;
 };
 
-RunBuffers run_buffers(olc_context* ctx, size_t stride, size_t resolve_offset) {
+RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_t resolve_offset) {
   RunBuffers b;
   b.qa = RayQueue{ctx->q0_o.as<float4>(), ctx->q0_d.as<float4>(), ctx->q0_p.as<uint32_t>()};
   b.qb = RayQueue{ctx->q1_o.as<float4>(), ctx->q1_d.as<float4>(), ctx->q1_p.as<uint32_t>()};
+  b.qc = RayQueue{ctx->q2_o.as<float4>(), ctx->q2_d.as<float4>(), ctx->q2_p.as<uint32_t>()};
   b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
   b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
   b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>()};
@@ -981,7 +1025,7 @@ RunBuffers run_buffers(olc_context* ctx, size_t stride, size_t resolve_offset) {
   b.cnt = ctx->counters.as<Counters>();
   b.accum = ctx->pixels.at<unsigned long long>(0);
   b.out = ctx->pixels.at<float4>(1);
-  b.table = ctx->table_dev.as<char>();
+  b.table = sl.table_dev.as<char>();
   b.stride = stride;
   b.resolve_offset = resolve_offset;
   return b;
@@ -1002,7 +1046,14 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
     tl_mark(ctx, OLC_STAGE_RAYGEN, 0, c);
     const RayQueue* qin = &rb.qa;
     const RayQueue* qout = &rb.qb;
+    const RayQueue* spare = &rb.qc;
     for (uint32_t b = 0; b < ch.bounces; ++b) {
+      if (b > 0 && ctx->ls.sort_rays) {
+        launch_sort_rays(ctx->ls, s, *qin, *spare, rb.cnt, b, ctx->sort_keys.as<uint32_t>(),
+                         ctx->sort_bins.as<uint32_t>(), st);
+        tl_mark(ctx, OLC_STAGE_SORT, b, c);
+        std::swap(qin, spare);
+      }
       launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, st);
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
@@ -1018,7 +1069,7 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
     }
     launch_accumulate(ctx->ls, hdr, jobs, rb.ps, rb.accum, rb.cnt, st);
     tl_mark(ctx, OLC_STAGE_ACCUMULATE, 0, c);
-    OLC_CUDA(cudaMemcpyAsync(ctx->counters_host + c, rb.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaMemcpyAsync(ctx->cur->counters_host + c, rb.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
   }
   const uint32_t* num_entries = reinterpret_cast<const uint32_t*>(rb.table + rb.resolve_offset);
   const ResolveEntry* entries = reinterpret_cast<const ResolveEntry*>(rb.table + rb.resolve_offset + 16);
@@ -1037,12 +1088,15 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
   for (size_t i = 0; i < sizeof(SceneView) / sizeof(void*); ++i) ptr(sv[i]);
   for (const void* p : std::initializer_list<const void*>{(const void*)rb.qa.origin_tmin, (const void*)rb.qa.dir_root, (const void*)rb.qa.path,
                         (const void*)rb.qb.origin_tmin, (const void*)rb.qb.dir_root, (const void*)rb.qb.path,
+                        (const void*)rb.qc.origin_tmin, (const void*)rb.qc.dir_root, (const void*)rb.qc.path,
+                        ctx->sort_keys.get(), ctx->sort_bins.get(),
                         (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
                         (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
                         (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.cnt, (const void*)rb.accum,
-                        (const void*)rb.out, (const void*)rb.table, (const void*)ctx->counters_host,
+                        (const void*)rb.out, (const void*)rb.table, (const void*)ctx->cur->counters_host,
+                        (const void*)ctx->cur,
                         ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_b0.get(),
                         ctx->restir.res_b1.get(), ctx->restir.hist0.get(), ctx->restir.hist1.get(),
                         ctx->restir.selected.get(), ctx->restir.hit_list.get(), ctx->restir.hit_count.get()})
@@ -1099,18 +1153,17 @@ void launch_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
     OLC_CUDA(e);
     GraphEntry ge;
     ge.exec = exec;
-    ge.timeline = ctx->tl_entries;
+    ge.timeline = ctx->cur->entries;
     it = ctx->graphs.emplace(std::move(key), std::move(ge)).first;
   }
   it->second.last_used = ++ctx->graph_clock;
-  ctx->tl_entries = it->second.timeline;
+  ctx->cur->entries = it->second.timeline;
   OLC_CUDA(cudaGraphLaunch(it->second.exec, st));
 }
 
-// Execute a planned run: stage the tables, launch, copy finished outputs,
-// wait, and gather statistics.  The jobs in plan.finished are complete when
-// this returns.
-void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
+// Stage a planned run into slot `sl` and launch it with the output copies of
+// the jobs it completes; returns without waiting.
+void launch_planned(olc_context* ctx, RunSlot& sl, RunPlan&& plan) {
   cudaStream_t st = ctx->stream;
   const uint32_t nchunks = (uint32_t)plan.chunks.size();
   if (nchunks == 0) throw Error(OLC_ERR_RUNTIME, "a run without paths");
@@ -1121,62 +1174,97 @@ void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
     drop_graphs(ctx);
   }
   ensure_wavefront(ctx, std::max<uint32_t>(plan.max_count, 1));
-  ensure_host_counters(ctx, std::max<uint32_t>(nchunks, 1));
+  ensure_host_counters(ctx, sl, std::max<uint32_t>(nchunks, 1));
   if (!ctx->counters.get()) ctx->counters.allocate(sizeof(Counters));
+  for (cudaEvent_t* e : {&sl.begin, &sl.end, &sl.done})
+    if (!*e) OLC_CUDA(cudaEventCreate(e));
   const size_t stride = chunk_stride(ctx->seg_capacity);
   const size_t resolve_offset = stride * nchunks;
   const size_t bytes = resolve_offset + 16 + sizeof(ResolveEntry) * plan.finished.size();
-  ensure_table(ctx, bytes);
+  ensure_table(ctx, sl, bytes);
+  sl.table_bytes = bytes;
   // host staging of all chunk tables and the resolve list
   for (uint32_t c = 0; c < nchunks; ++c) {
     const ChunkPlan& ch = plan.chunks[c];
-    ChunkHeader* h = reinterpret_cast<ChunkHeader*>(ctx->table_host + c * stride);
+    ChunkHeader* h = reinterpret_cast<ChunkHeader*>(sl.table_host + c * stride);
     h->count = ch.count;
     h->num_segments = (uint32_t)ch.segs.size();
     h->stamp = plan.restir ? ctx->restir.run_first + c : 0u;
     h->history_first = ctx->restir.hist_first;
     h->history_last = ctx->restir.hist_last;
     h->pad[0] = h->pad[1] = h->pad[2] = 0;
-    std::memcpy(ctx->table_host + c * stride + sizeof(ChunkHeader), ch.segs.data(), ch.segs.size() * sizeof(JobRec));
+    std::memcpy(sl.table_host + c * stride + sizeof(ChunkHeader), ch.segs.data(), ch.segs.size() * sizeof(JobRec));
   }
   {
-    uint32_t* n = reinterpret_cast<uint32_t*>(ctx->table_host + resolve_offset);
+    uint32_t* n = reinterpret_cast<uint32_t*>(sl.table_host + resolve_offset);
     n[0] = (uint32_t)plan.finished.size();
     n[1] = n[2] = n[3] = 0;
-    ResolveEntry* e = reinterpret_cast<ResolveEntry*>(ctx->table_host + resolve_offset + 16);
+    ResolveEntry* e = reinterpret_cast<ResolveEntry*>(sl.table_host + resolve_offset + 16);
     for (size_t k = 0; k < plan.finished.size(); ++k) {
       e[k].pixel_base = plan.finished[k]->rec.pixel_base;
       e[k].npix = plan.finished[k]->rec.npix;
       e[k].spp = plan.finished[k]->rec.spp;
     }
   }
-  OLC_CUDA(cudaMemcpyAsync(ctx->table_dev.get(), ctx->table_host, bytes, cudaMemcpyHostToDevice, st));
-  const RunBuffers rb = run_buffers(ctx, stride, resolve_offset);
-  OLC_CUDA(cudaEventRecord(ctx->ev_begin, st));
+  OLC_CUDA(cudaMemcpyAsync(sl.table_dev.get(), sl.table_host, bytes, cudaMemcpyHostToDevice, st));
+  const RunBuffers rb = run_buffers(ctx, sl, stride, resolve_offset);
+  ctx->cur = &sl;
+  OLC_CUDA(cudaEventRecord(sl.begin, st));
   launch_run(ctx, plan, rb);
-  OLC_CUDA(cudaEventRecord(ctx->ev_end, st));
+  OLC_CUDA(cudaEventRecord(sl.end, st));
+  size_t staged_pixels = 0;
+  for (QueuedJob* j : plan.finished)
+    if (j->out && j->out_staged) staged_pixels += j->rec.npix;
+  if (staged_pixels > sl.staging_pixels) {
+    if (sl.staging) cudaFreeHost(sl.staging);
+    sl.staging = nullptr;
+    sl.staging_pixels = 0;
+    OLC_CUDA(cudaMallocHost(&sl.staging, staged_pixels * sizeof(float4)));
+    sl.staging_pixels = staged_pixels;
+  }
+  sl.staged.clear();
+  size_t at = 0;
   for (QueuedJob* j : plan.finished) {
     if (!j->out) continue;
-    OLC_CUDA(cudaMemcpyAsync(j->out, rb.out + j->rec.pixel_base, (size_t)j->rec.npix * sizeof(float4),
-                             j->out_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    const size_t bytes = (size_t)j->rec.npix * sizeof(float4);
+    if (j->out_staged) {
+      OLC_CUDA(cudaMemcpyAsync(sl.staging + at, rb.out + j->rec.pixel_base, bytes, cudaMemcpyDeviceToHost, st));
+      sl.staged.emplace_back(j, at);
+      at += j->rec.npix;
+    } else {
+      OLC_CUDA(cudaMemcpyAsync(j->out, rb.out + j->rec.pixel_base, bytes,
+                               j->out_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    }
   }
-  OLC_CUDA(cudaStreamSynchronize(st));
+  OLC_CUDA(cudaEventRecord(sl.done, st));
+  sl.plan = std::move(plan);
+  sl.busy = true;
+}
 
-  // per-launch device timeline
+// Wait for the run in slot `sl` (outputs included) and gather its timeline
+// and statistics.
+void finish_run(olc_context* ctx, RunSlot& sl, olc_render_stats* stats) {
+  OLC_CUDA(cudaEventSynchronize(sl.done));
+  sl.busy = false;
+  for (const auto& js : sl.staged)
+    std::memcpy(js.first->out, sl.staging + js.second, (size_t)js.first->rec.npix * sizeof(float4));
+  sl.staged.clear();
+  const RunPlan& plan = sl.plan;
+  const uint32_t nchunks = (uint32_t)plan.chunks.size();
   ctx->last_profile.clear();
   ctx->last_chunk_counts.clear();
   for (const ChunkPlan& ch : plan.chunks) ctx->last_chunk_counts.push_back(ch.count);
-  float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint64_t resolved_pixels = 0;
   for (const QueuedJob* j : plan.finished) resolved_pixels += j->rec.npix;
-  for (size_t k = 0; k < ctx->tl_entries.size(); ++k) {
-    const TimelineEntry& e = ctx->tl_entries[k];
+  for (size_t k = 0; k < sl.entries.size(); ++k) {
+    const TimelineEntry& e = sl.entries[k];
     olc_launch_record r{};
     r.stage = e.stage;
     r.bounce = e.bounce;
     r.chunk = e.chunk;
-    OLC_CUDA(cudaEventElapsedTime(&r.ms, ctx->tl_events[k], ctx->tl_events[k + 1]));
-    const Counters& kc = ctx->counters_host[std::min<uint32_t>(e.chunk, nchunks - 1)];
+    OLC_CUDA(cudaEventElapsedTime(&r.ms, sl.events[k], sl.events[k + 1]));
+    const Counters& kc = sl.counters_host[std::min<uint32_t>(e.chunk, nchunks - 1)];
     switch (e.stage) {
       case OLC_STAGE_RAYGEN: case OLC_STAGE_ACCUMULATE: r.items = plan.chunks[e.chunk].count; break;
       case OLC_STAGE_TRACE: case OLC_STAGE_SHADE: case OLC_STAGE_RESTIR:
@@ -1184,6 +1272,7 @@ void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
         r.misses = kc.miss_count[e.bounce];
         break;
       case OLC_STAGE_SHADOW: r.items = kc.shadow_count[e.bounce]; break;
+      case OLC_STAGE_SORT: r.items = kc.queue_count[e.bounce]; break;
       default: r.items = resolved_pixels; break;
     }
     stage_ms[e.stage] += r.ms;
@@ -1192,27 +1281,38 @@ void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->raygen_ms = stage_ms[OLC_STAGE_RAYGEN];
-    stats->trace_ms = stage_ms[OLC_STAGE_TRACE];
+    stats->trace_ms = stage_ms[OLC_STAGE_TRACE] + stage_ms[OLC_STAGE_SORT];
     stats->restir_ms = stage_ms[OLC_STAGE_RESTIR];
     stats->shade_ms = stage_ms[OLC_STAGE_SHADE];
     stats->shadow_ms = stage_ms[OLC_STAGE_SHADOW];
     stats->accumulate_ms = stage_ms[OLC_STAGE_ACCUMULATE] + stage_ms[OLC_STAGE_RESOLVE];
     for (uint32_t c = 0; c < nchunks; ++c) {
-      const Counters& k = ctx->counters_host[c];
+      const Counters& k = sl.counters_host[c];
       stats->camera_rays += k.queue_count[0];
       for (uint32_t b = 1; b < plan.chunks[c].bounces; ++b) stats->extension_rays += k.queue_count[b];
       for (uint32_t b = 0; b < plan.chunks[c].bounces; ++b) stats->shadow_rays += k.shadow_count[b];
       stats->overflow += k.overflow;
       stats->traversal_errors += k.traversal_errors;
     }
-    OLC_CUDA(cudaEventElapsedTime(&stats->gpu_ms, ctx->ev_begin, ctx->ev_end));
+    OLC_CUDA(cudaEventElapsedTime(&stats->gpu_ms, sl.begin, sl.end));
     stats->chunks = nchunks;
     stats->jobs_completed = (uint32_t)plan.finished.size();
-    stats->h2d_bytes = bytes;
+    stats->h2d_bytes = sl.table_bytes;
     stats->d2h_bytes = (uint64_t)nchunks * sizeof(Counters);
     for (const QueuedJob* j : plan.finished)
       if (j->out && !j->out_device) stats->d2h_bytes += (uint64_t)j->rec.npix * sizeof(float4);
   }
+}
+
+// A slot no run occupies (plain frames and batches run beside an in-flight
+// serving step).
+RunSlot& free_slot(olc_context* ctx) { return ctx->runs[0].busy ? ctx->runs[1] : ctx->runs[0]; }
+
+// Launch and wait: plain frames and batches.
+void execute_run(olc_context* ctx, RunPlan& plan, olc_render_stats* stats) {
+  RunSlot& sl = free_slot(ctx);
+  launch_planned(ctx, sl, std::move(plan));
+  finish_run(ctx, sl, stats);
 }
 
 // Render the given jobs to completion as one run (plain frames and batches).
@@ -1230,6 +1330,16 @@ void run_to_completion(olc_context* ctx, std::vector<QueuedJob*>& jobs, olc_rend
 
 void release_job(olc_context* ctx, QueuedJob& j) { ctx->pixels.release(j.pixels); }
 
+// Page-locked (or registered) host memory takes asynchronous copies directly.
+bool is_pinned(const void* p) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeHost;
+}
+
 // Fill an olc_job into a queued job (validated; not yet admitted).
 void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
   if (!d) throw Error(OLC_ERR_VALUE, "job is required");
@@ -1243,6 +1353,7 @@ void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
   q.total = (uint64_t)q.rec.npix * q.rec.spp;
   q.out = d->out_rgba;
   q.out_device = d->out_is_device != 0;
+  q.out_staged = !q.out_device && !is_pinned(q.out);
 }
 
 bool same_camera(const JobRec& a, const JobRec& b) {
@@ -1282,8 +1393,6 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     OLC_CUDA(cudaGetDeviceProperties(&prop, ctx->device));
     ctx->sm_count = prop.multiProcessorCount;
     OLC_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    OLC_CUDA(cudaEventCreate(&ctx->ev_begin));
-    OLC_CUDA(cudaEventCreate(&ctx->ev_end));
     configure_trace_kernels();
     apply_launch_shape(ctx.get());
     // pool record 0: the identity instance that baked triangles report
@@ -1315,11 +1424,7 @@ int olc_destroy(olc_context* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graphs(ctx);
   restir_release(ctx->restir);
-  if (ctx->table_host) cudaFreeHost(ctx->table_host);
-  if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
-  for (cudaEvent_t e : ctx->tl_events) cudaEventDestroy(e);
-  if (ctx->ev_begin) cudaEventDestroy(ctx->ev_begin);
-  if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
+  for (RunSlot& sl : ctx->runs) release_slot(sl);
   cudaStream_t st = ctx->stream;
   delete ctx;  // device buffers are freed here
   if (st) cudaStreamDestroy(st);
@@ -1398,9 +1503,11 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
   info->pool_bytes = ctx->nodes.bytes() + ctx->slots.bytes() + ctx->instances.bytes() + ctx->materials.bytes() +
                      ctx->emitters.bytes() + ctx->lights.bytes() + ctx->scene_table.bytes();
   uint64_t wf = 0;
-  for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p,
+  for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p, &ctx->q2_o,
+                                &ctx->q2_d, &ctx->q2_p, &ctx->sort_keys, &ctx->sort_bins,
                                 &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
-                                &ctx->ps_rad, &ctx->ps_meta, &ctx->table_dev, &ctx->prod_depth, &ctx->prod_normal,
+                                &ctx->ps_rad, &ctx->ps_meta, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
+                                &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->restir.res_a0,
                                 &ctx->restir.res_a1, &ctx->restir.res_b0, &ctx->restir.res_b1, &ctx->restir.hist0,
                                 &ctx->restir.hist1, &ctx->restir.selected, &ctx->restir.hit_list})
@@ -1426,6 +1533,7 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     job.total = (uint64_t)job.rec.npix * spp;
     job.out = out_rgba;
     job.out_device = out_is_device != 0;
+    job.out_staged = !job.out_device && !is_pinned(out_rgba);
     const bool restir = job.rec.restir != 0;
     // the frame's reservoirs live at job-local indices, where the next frame's
     // temporal pass finds them; the history survives only if the reservoir
@@ -1514,7 +1622,16 @@ int olc_cancel(olc_context* ctx, uint64_t ticket) {
   return guarded(ctx, [&] {
     for (auto it = ctx->served.begin(); it != ctx->served.end(); ++it) {
       if ((*it)->ticket != ticket) continue;
-      release_job(ctx, **it);
+      QueuedJob* job = it->get();
+      if (ctx->inflight >= 0) {
+        // the in-flight chunk may hold its paths: let it finish, and keep it
+        // from reporting the job
+        RunSlot& sl = ctx->runs[ctx->inflight];
+        OLC_CUDA(cudaEventSynchronize(sl.done));
+        auto& fin = sl.plan.finished;
+        fin.erase(std::remove(fin.begin(), fin.end(), job), fin.end());
+      }
+      release_job(ctx, *job);
       ctx->served.erase(it);
       return;
     }
@@ -1528,7 +1645,11 @@ int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uin
   return guarded(ctx, [&] {
     *num_done = 0;
     if (stats) std::memset(stats, 0, sizeof(*stats));
-    if (ctx->served.empty()) return;
+    RunSlot* prev = ctx->inflight >= 0 ? &ctx->runs[ctx->inflight] : nullptr;
+    if (prev && prev->plan.finished.size() > done_capacity)
+      throw Error(OLC_ERR_VALUE, "done_capacity is smaller than the number of jobs the step completes");
+    // 1. plan and launch the next chunk so the device stays busy while the
+    //    previous one is collected
     std::vector<QueuedJob*> jobs;
     std::vector<uint64_t> issued_before;
     for (auto& j : ctx->served) {
@@ -1545,43 +1666,47 @@ int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uin
     });
     RunPlan plan;
     plan_run(jobs, plan_capacity(ctx, jobs), 1, 0, plan);
-    if (plan.finished.size() > done_capacity) {
-      for (size_t k = 0; k < jobs.size(); ++k) jobs[k]->issued = issued_before[k];
-      throw Error(OLC_ERR_VALUE, "done_capacity is smaller than the number of jobs this step completes");
-    }
-    if (plan.restir)
-      restir_prepare(ctx->restir, plan.max_count, std::max<uint32_t>(plan.max_count, 1),
-                     (uint32_t)plan.chunks.size());
-    try {
-      execute_run(ctx, plan, stats);
-    } catch (...) {
-      // the chunk's jobs hold partial samples of a failed chunk: drop them
-      size_t k = 0;
-      for (auto it = ctx->served.begin(); it != ctx->served.end(); ++k) {
-        if ((*it)->issued != issued_before[k]) {
-          release_job(ctx, **it);
-          it = ctx->served.erase(it);
-        } else {
-          ++it;
+    int launched = -1;
+    if (!plan.chunks.empty()) {
+      RunSlot& sl = prev == &ctx->runs[0] ? ctx->runs[1] : ctx->runs[0];
+      try {
+        if (plan.restir)
+          restir_prepare(ctx->restir, plan.max_count, std::max<uint32_t>(plan.max_count, 1),
+                         (uint32_t)plan.chunks.size());
+        launch_planned(ctx, sl, std::move(plan));
+      } catch (...) {
+        // the chunk's jobs hold partial samples of a failed chunk: drop them
+        cudaStreamSynchronize(ctx->stream);
+        size_t k = 0;
+        for (auto it = ctx->served.begin(); it != ctx->served.end(); ++k) {
+          if ((*it)->issued != issued_before[k]) {
+            release_job(ctx, **it);
+            it = ctx->served.erase(it);
+          } else {
+            ++it;
+          }
         }
+        throw;
       }
-      throw;
-    }
-    for (QueuedJob* j : plan.finished) done[(*num_done)++] = j->ticket;
-    {
+      launched = (int)(&sl - ctx->runs);
       size_t k = 0;
       for (auto& j : ctx->served) {
         j->waited = j->issued == issued_before[k] ? j->waited + 1 : 0;
         ++k;
       }
     }
-    for (auto it = ctx->served.begin(); it != ctx->served.end();) {
-      if ((*it)->issued == (*it)->total) {
-        release_job(ctx, **it);
-        it = ctx->served.erase(it);
-      } else {
-        ++it;
+    ctx->inflight = launched;
+    // 2. collect the previous chunk: its finished jobs are complete
+    if (prev) {
+      finish_run(ctx, *prev, stats);
+      for (QueuedJob* j : prev->plan.finished) done[(*num_done)++] = j->ticket;
+      for (QueuedJob* j : prev->plan.finished) {
+        auto it = std::find_if(ctx->served.begin(), ctx->served.end(),
+                               [&](const std::unique_ptr<QueuedJob>& q) { return q.get() == j; });
+        release_job(ctx, *j);
+        ctx->served.erase(it);
       }
+      prev->plan = RunPlan{};
     }
   });
 }

@@ -524,6 +524,133 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
   }
 }
 
+// ---- ray reordering -------------------------------------------------------
+// Secondary rays leave the shading stage in path order, so a warp holds rays
+// that start anywhere in the scene and point anywhere, and its lanes
+// traverse unrelated parts of the hierarchy.  Before an extension bounce is
+// traced, the queue is reordered by a 15-bit key: an 8x8 octahedral
+// direction bin above the 9-bit Morton code of the origin within its scene's
+// root box (after the ray-sorting idea of Garanzha and Loop, "Fast Ray
+// Sorting and Breadth-First Packet Traversal for GPU Ray Tracing", EG 2010).
+// A counting sort over the 32,768 keys with warp-aggregated atomics; the
+// order inside a key is arbitrary, which changes no result because every ray
+// is traced independently and accumulation is order independent.
+constexpr uint32_t kSortBits = 15;
+constexpr uint32_t kSortBins = 1u << kSortBits;
+
+OLC_D uint32_t ray_sort_key(const SceneView& s, float3 o, float3 d, uint32_t root) {
+  const float4* p = reinterpret_cast<const float4*>(s.nodes + root);
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  const float3 lo = f3(fminf(a.x, b.x), fminf(a.z, b.z), fminf(c.x, c.z));
+  const float3 hi = f3(fmaxf(a.y, b.y), fmaxf(a.w, b.w), fmaxf(c.y, c.w));
+  const float3 ext = hi - lo;
+  auto cell = [](float v, float l, float e) -> uint32_t {
+    const float u = e > 0.0f ? (v - l) / e : 0.0f;
+    return (uint32_t)clampf(u * 8.0f, 0.0f, 7.0f);
+  };
+  const uint32_t cx = cell(o.x, lo.x, ext.x), cy = cell(o.y, lo.y, ext.y), cz = cell(o.z, lo.z, ext.z);
+  uint32_t morton = 0u;
+#pragma unroll
+  for (int bit = 0; bit < 3; ++bit)
+    morton |= (((cx >> bit) & 1u) << (3 * bit)) | (((cy >> bit) & 1u) << (3 * bit + 1)) |
+              (((cz >> bit) & 1u) << (3 * bit + 2));
+  const float l1 = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+  float ox = l1 > 0.0f ? d.x / l1 : 0.0f, oy = l1 > 0.0f ? d.y / l1 : 0.0f;
+  if (d.z < 0.0f) {
+    const float tx = (1.0f - fabsf(oy)) * (ox >= 0.0f ? 1.0f : -1.0f);
+    const float ty = (1.0f - fabsf(ox)) * (oy >= 0.0f ? 1.0f : -1.0f);
+    ox = tx;
+    oy = ty;
+  }
+  const uint32_t ux = (uint32_t)clampf((ox * 0.5f + 0.5f) * 8.0f, 0.0f, 7.0f);
+  const uint32_t uy = (uint32_t)clampf((oy * 0.5f + 0.5f) * 8.0f, 0.0f, 7.0f);
+  return ((ux | (uy << 3)) << 9) | morton;
+}
+
+// Adds `amount` per lane to counter[key], one atomic per distinct key of the
+// warp; returns each lane's previous count plus its rank among equal keys.
+OLC_D uint32_t warp_bin_add(uint32_t* counter, uint32_t key, bool active) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, active);
+  if (!active) return 0u;
+  const uint32_t peers = __match_any_sync(mask, key);
+  const uint32_t leader = __ffs(peers) - 1u;
+  uint32_t base = 0u;
+  if (lane_id() == leader) base = atomicAdd(counter + key, (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane_id()) - 1u));
+}
+
+__global__ void k_sort_keys(SceneView s, RayQueue q, const uint32_t* __restrict__ count, uint32_t* keys,
+                            uint32_t* hist) {
+  const uint32_t n = *count;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool active = i < n;
+    uint32_t key = 0u;
+    if (active) {
+      const float4 ot = q.origin_tmin[i];
+      const float4 dr = q.dir_root[i];
+      key = ray_sort_key(s, f3(ot), f3(dr), __float_as_uint(dr.w));
+      keys[i] = key;
+    }
+    warp_bin_add(hist, key, active);
+  }
+}
+
+// Exclusive prefix sum of the kSortBins counts, in place (one block of 1024).
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist) {
+  constexpr uint32_t kPer = kSortBins / 1024u;
+  __shared__ uint32_t warp_sums[32];
+  const uint32_t t = threadIdx.x;
+  uint32_t local[kPer];
+  uint32_t sum = 0u;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    local[k] = hist[t * kPer + k];
+    sum += local[k];
+  }
+  uint32_t incl = sum;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane_id() >= (uint32_t)off) incl += v;
+  }
+  if (lane_id() == 31u) warp_sums[t >> 5] = incl;
+  __syncthreads();
+  if (t < 32u) {
+    uint32_t w = warp_sums[t];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, w, off);
+      if (t >= (uint32_t)off) w += v;
+    }
+    warp_sums[t] = w;
+  }
+  __syncthreads();
+  uint32_t run = incl - sum + ((t >> 5) ? warp_sums[(t >> 5) - 1u] : 0u);
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    hist[t * kPer + k] = run;
+    run += local[k];
+  }
+}
+
+__global__ void k_sort_scatter(RayQueue in, const uint32_t* __restrict__ count, const uint32_t* __restrict__ keys,
+                               uint32_t* cursor, RayQueue out) {
+  const uint32_t n = *count;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool active = i < n;
+    const uint32_t key = active ? keys[i] : 0u;
+    const uint32_t pos = warp_bin_add(cursor, key, active);
+    if (active) {
+      out.origin_tmin[pos] = in.origin_tmin[i];
+      out.dir_root[pos] = in.dir_root[i];
+      out.path[pos] = in.path[i];
+    }
+  }
+}
+
 OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
   if (!(v == v)) {  // NaN
     atomicAdd(nan_counter, 1u);
@@ -689,6 +816,20 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   k_shade<<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_shade");
 }
+
+void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue& in, const RayQueue& out,
+                      Counters* cnt, uint32_t bounce, uint32_t* keys, uint32_t* bins, cudaStream_t stream) {
+  OLC_CUDA(cudaMemsetAsync(bins, 0, kSortBins * sizeof(uint32_t), stream));
+  const uint32_t* count = &cnt->queue_count[bounce];
+  k_sort_keys<<<ls.grid_simple, 256, 0, stream>>>(s, in, count, keys, bins);
+  OLC_LAUNCH_CHECK("k_sort_keys");
+  k_sort_scan<<<1, 1024, 0, stream>>>(bins);
+  OLC_LAUNCH_CHECK("k_sort_scan");
+  k_sort_scatter<<<ls.grid_simple, 256, 0, stream>>>(in, count, keys, bins, out);
+  OLC_LAUNCH_CHECK("k_sort_scatter");
+}
+
+size_t sort_bins_bytes() { return kSortBins * sizeof(uint32_t); }
 
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
                        unsigned long long* accum, Counters* cnt, cudaStream_t stream) {

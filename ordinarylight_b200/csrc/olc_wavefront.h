@@ -49,6 +49,7 @@ struct LaunchShape {
   uint32_t grid_shade = 148 * 8;
   uint32_t stack_depth = 24;
   uint32_t scheduler = 0;      // traversal scheduling (olc_config.trace_scheduler)
+  uint32_t sort_rays = 0;      // reorder extension rays before tracing them
 };
 
 // First-sample primary-hit products of the job flagged `products` (a plain
@@ -72,6 +73,11 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
                   cudaStream_t stream);
+// Reorder the bounce's ray queue `in` into `out` by origin cell and direction
+// bin (keys: one word per queue slot; bins: sort_bins_bytes() of scratch).
+void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue& in, const RayQueue& out,
+                      Counters* cnt, uint32_t bounce, uint32_t* keys, uint32_t* bins, cudaStream_t stream);
+size_t sort_bins_bytes();
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
                        unsigned long long* accum, Counters* cnt, cudaStream_t stream);
 void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,

@@ -68,6 +68,7 @@ class CudaRendererConfig:
     flatten_instances: bool = True
     trace_scheduler: str = "refill"
     nee: bool = True
+    sort_rays: bool = False
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -126,6 +127,7 @@ class CudaRendererConfig:
         c.flatten_instances = int(bool(self.flatten_instances))
         c.trace_scheduler = 0 if self.trace_scheduler == "refill" else 1
         c.disable_nee = 0 if self.nee else 1
+        c.ray_sort = 1 if self.sort_rays else 0
         return c
 
 
@@ -143,6 +145,16 @@ class RenderRequest:
     samples: int | None = None
     frame_index: int = 0
     max_bounces: int | None = None
+
+
+def host_image(height: int, width: int) -> np.ndarray:
+    """(height, width, 4) float32 host array in page-locked memory (torch's
+    caching host allocator), so the device-to-host copy of a frame runs at
+    full link bandwidth instead of through a pageable bounce buffer.  The
+    array returns to the allocator's cache when it is dropped."""
+    import torch
+
+    return torch.empty((int(height), int(width), 4), dtype=torch.float32, pin_memory=True).numpy()
 
 
 class CudaWavefrontRenderer(RendererImplementation):
@@ -261,7 +273,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         width, height = int(width), int(height)
         if width <= 0 or height <= 0:
             raise ValueError("width and height must be positive")
-        out = np.empty((height, width, 4), np.float32)
+        out = host_image(height, width)
         self._render(scene, camera, width, height, samples, frame_index, _native.ptr(out), False)
         return out
 

@@ -69,7 +69,7 @@ def test_batch_chunking_does_not_change_images(native_library, cuda_device, scen
     requests = _requests(scene_set)
     with CudaWavefrontRenderer(seed=1, restir=True) as r:
         base = r.render_batch(requests)
-        r.reconfigure(chunk_paths=chunk_paths, block_size=128, trace_block=64, stack_depth=16)
+        r.reconfigure(chunk_paths=chunk_paths, block_size=128, trace_block=64, stack_depth=16, sort_rays=True)
         chunked = r.render_batch(requests)
         assert r.last_timings["chunks"] > 1
     for a, b in zip(base, chunked):
@@ -115,8 +115,11 @@ def test_served_small_request_finishes_before_a_large_one(native_library, cuda_d
     with CudaWavefrontRenderer(seed=1, chunk_paths=65536) as r:
         t_big = r.submit(big)
         t_small = r.submit(small)
-        first = r.serve_step()
+        first = []
+        while not first:
+            first = r.serve_step()
         assert [t for t, _ in first] == [t_small]
+        assert t_big in r.queued_tickets()
         rest = []
         while r.queued_tickets():
             rest += r.serve_step()
@@ -184,7 +187,7 @@ def test_autotuner_keeps_images(native_library, cuda_device, scene_set):
     with CudaWavefrontRenderer(seed=1) as r:
         base = r.render_batch(requests)
         result = autotune(r, requests, chunks=(8192, 1 << 20), blocks=((128, 128), (256, 64)), stacks=(16, 24),
-                          repeats=1, use_cache=False)
+                          sorts=(False, True), repeats=1, use_cache=False)
         assert len(result.trials) >= 4
         assert r.config.chunk_paths == result.chunk_paths and r.config.stack_depth == result.stack_depth
         tuned = r.render_batch(requests)

@@ -222,7 +222,7 @@ def test_autotuner_coordinate_descent():
     result = autotune(r, reqs, repeats=1, use_cache=False)
     assert (result.chunk_paths, result.block_size, result.stack_depth) == (1 << 18, 128, 24)
     assert r.config.chunk_paths == 1 << 18
-    assert len(result.trials) <= 1 + 4 + 4 + 3
+    assert len(result.trials) <= 1 + 4 + 4 + 3 + 2
     again = autotune(r, reqs, repeats=1)          # cached: no new trials
     calls = r.calls
     assert autotune(r, reqs, repeats=1) is again and r.calls == calls
