@@ -118,7 +118,10 @@ typedef struct olc_config {
   uint32_t ray_sort;            /* reorder extension rays by origin cell and
                                    direction before tracing them (helps
                                    shading coherence on large scenes) */
-  uint32_t reserved[3];
+  uint32_t serve_aging_steps;   /* serving: jobs queued this many steps go
+                                   first, oldest first (0: shortest remaining
+                                   work first only) */
+  uint32_t reserved[2];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the
@@ -313,8 +316,9 @@ OLC_API int olc_render_batch(olc_context* ctx, const olc_job* jobs, uint32_t num
 OLC_API int olc_submit(olc_context* ctx, const olc_job* job, uint64_t* ticket);
 
 /* One serving step: launch the next chunk (at most chunk_paths paths) drawn
- * from the queued jobs, shortest remaining work first (a job passed over for
- * 8 steps goes first), then wait for the chunk the previous step launched
+ * from the queued jobs, shortest remaining work first (jobs queued for
+ * serve_aging_steps steps or more go first, oldest first), then wait for the
+ * chunk the previous step launched
  * and report the jobs whose last paths were in it (resolved and copied out).
  * Keeping one chunk in flight hides the host work of a step behind the
  * device work of the previous one.  done (host, capacity done_capacity)

@@ -45,7 +45,8 @@ class OlcConfig(ctypes.Structure):
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
         ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
         ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("trace_block", c_uint32),
-        ("ray_sort", c_uint32), ("reserved", c_uint32 * 3),
+        ("ray_sort", c_uint32), ("serve_aging_steps", c_uint32),
+        ("reserved", c_uint32 * 2),
     ]
 
 

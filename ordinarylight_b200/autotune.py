@@ -23,7 +23,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 import time
 
-CHUNKS = (1 << 16, 1 << 18, 1 << 20, 1 << 22)
+CHUNKS = (1 << 18, 1 << 20, 1 << 22, 1 << 24)
 BLOCKS = ((64, 64), (128, 128), (256, 128), (512, 256))   # (queue kernels, traversal/shading)
 STACKS = (16, 24, 32)
 SORTS = (False, True)

@@ -49,7 +49,6 @@ constexpr uint64_t kFlattenMaxTotal = 1ull << 24;
 constexpr size_t kMaxGraphs = 16;
 constexpr uint64_t kDefaultChunkPaths = 1ull << 24;
 constexpr uint32_t kNoScene = 0xffffffffu;
-constexpr uint32_t kMaxWaitSteps = 8;
 
 // First-fit allocator of element ranges in [0, capacity).
 class RangeAllocator {
@@ -184,7 +183,7 @@ struct QueuedJob {
   // ReSTIR reservoirs at job-local indices (reservoir_base 0), where the next
   // plain frame's temporal pass finds them; otherwise chunk-local ones
   bool job_local_reservoirs = false;
-  uint32_t waited = 0;       // serving steps that issued none of its paths
+  uint32_t age = 0;          // serving steps since it was queued
 };
 
 struct ChunkPlan {
@@ -879,8 +878,13 @@ uint64_t plan_capacity(const olc_context* ctx, const std::vector<QueuedJob*>& jo
 // reservoirs of a plain frame).
 void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, uint64_t reservoir_region,
               RunPlan& plan) {
+  struct Take {
+    QueuedJob* job;
+    uint64_t first, count;
+  };
   for (uint32_t c = 0; c < max_chunks; ++c) {
-    ChunkPlan ch;
+    // choose the chunk's segments in job order
+    std::vector<Take> takes;
     uint64_t fill = 0;
     for (QueuedJob* j : jobs) {
       if (j->issued >= j->total) continue;
@@ -894,22 +898,33 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
       } else {
         take = std::min<uint64_t>(left, j->total - j->issued);
       }
-      JobRec seg = j->rec;
-      seg.seg_begin = fill;
-      seg.seg_first = j->issued;
-      if (seg.restir && !j->job_local_reservoirs) {
-        // chunk-local reservoirs: index = reservoir_region + chunk path index
-        seg.reservoir_base = reservoir_region + fill - j->issued;  // modulo 2^64
-        plan.chunk_reservoirs = true;
-      }
-      ch.segs.push_back(seg);
-      ch.bounces = std::max(ch.bounces, seg.max_bounces);
-      ch.restir = ch.restir || seg.restir;
+      takes.push_back(Take{j, j->issued, take});
       fill += take;
       j->issued += take;
       if (j->issued == j->total) plan.finished.push_back(j);
     }
     if (fill == 0) break;
+    // lay the segments out grouped by scene: the persistent kernels walk the
+    // queue in order, so the SMs then work on few hierarchies at a time and
+    // more of each stays in L2 (the layout changes no image)
+    std::stable_sort(takes.begin(), takes.end(),
+                     [](const Take& a, const Take& b) { return a.job->rec.scene < b.job->rec.scene; });
+    ChunkPlan ch;
+    uint64_t at = 0;
+    for (const Take& t : takes) {
+      JobRec seg = t.job->rec;
+      seg.seg_begin = at;
+      seg.seg_first = t.first;
+      if (seg.restir && !t.job->job_local_reservoirs) {
+        // chunk-local reservoirs: index = reservoir_region + chunk path index
+        seg.reservoir_base = reservoir_region + at - t.first;  // modulo 2^64
+        plan.chunk_reservoirs = true;
+      }
+      ch.segs.push_back(seg);
+      ch.bounces = std::max(ch.bounces, seg.max_bounces);
+      ch.restir = ch.restir || seg.restir;
+      at += t.count;
+    }
     ch.count = (uint32_t)fill;
     plan.restir = plan.restir || ch.restir;
     plan.max_segments = std::max<uint32_t>(plan.max_segments, (uint32_t)ch.segs.size());
@@ -1216,11 +1231,13 @@ void launch_planned(olc_context* ctx, RunSlot& sl, RunPlan&& plan) {
   for (QueuedJob* j : plan.finished)
     if (j->out && j->out_staged) staged_pixels += j->rec.npix;
   if (staged_pixels > sl.staging_pixels) {
+    // page locking is slow: grow geometrically from 4 Mpixel (64 MB)
+    const size_t want = std::max<size_t>({staged_pixels, 2 * sl.staging_pixels, (size_t)1 << 22});
     if (sl.staging) cudaFreeHost(sl.staging);
     sl.staging = nullptr;
     sl.staging_pixels = 0;
-    OLC_CUDA(cudaMallocHost(&sl.staging, staged_pixels * sizeof(float4)));
-    sl.staging_pixels = staged_pixels;
+    OLC_CUDA(cudaMallocHost(&sl.staging, want * sizeof(float4)));
+    sl.staging_pixels = want;
   }
   sl.staged.clear();
   size_t at = 0;
@@ -1590,6 +1607,10 @@ int olc_render_batch(olc_context* ctx, const olc_job* jobs, uint32_t num_jobs, o
         admit_job(ctx, j);
         ptrs.push_back(&j);
       }
+      // jobs of one scene next to each other: a chunk then touches fewer
+      // hierarchies, which keeps more of each in L2 (the order changes no image)
+      std::stable_sort(ptrs.begin(), ptrs.end(),
+                       [](const QueuedJob* a, const QueuedJob* b) { return a->rec.scene < b->rec.scene; });
       run_to_completion(ctx, ptrs, stats);
     } catch (...) {
       for (QueuedJob* j : ptrs) release_job(ctx, *j);
@@ -1657,11 +1678,14 @@ int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uin
       issued_before.push_back(j->issued);
     }
     // Shortest remaining work first, so small requests finish inside the
-    // chunks of large ones instead of queueing behind them; a job passed
-    // over for kMaxWaitSteps steps goes first.  The order changes no image.
-    std::stable_sort(jobs.begin(), jobs.end(), [](const QueuedJob* a, const QueuedJob* b) {
-      const bool sa = a->waited >= kMaxWaitSteps, sb = b->waited >= kMaxWaitSteps;
+    // chunks of large ones instead of queueing behind them; jobs queued for
+    // serve_aging_steps steps or more go first, oldest first, which bounds
+    // how long large ones wait.  The order changes no image.
+    const uint32_t aging = ctx->cfg.serve_aging_steps ? ctx->cfg.serve_aging_steps : 0xffffffffu;
+    std::stable_sort(jobs.begin(), jobs.end(), [aging](const QueuedJob* a, const QueuedJob* b) {
+      const bool sa = a->age >= aging, sb = b->age >= aging;
       if (sa != sb) return sa;
+      if (sa) return a->ticket < b->ticket;
       return a->total - a->issued < b->total - b->issued;
     });
     RunPlan plan;
@@ -1689,12 +1713,8 @@ int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uin
         throw;
       }
       launched = (int)(&sl - ctx->runs);
-      size_t k = 0;
-      for (auto& j : ctx->served) {
-        j->waited = j->issued == issued_before[k] ? j->waited + 1 : 0;
-        ++k;
-      }
     }
+    for (auto& j : ctx->served) ++j->age;
     ctx->inflight = launched;
     // 2. collect the previous chunk: its finished jobs are complete
     if (prev) {

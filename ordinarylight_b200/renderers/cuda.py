@@ -69,6 +69,7 @@ class CudaRendererConfig:
     trace_scheduler: str = "refill"
     nee: bool = True
     sort_rays: bool = False
+    serve_aging_steps: int = 8
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -128,6 +129,7 @@ class CudaRendererConfig:
         c.trace_scheduler = 0 if self.trace_scheduler == "refill" else 1
         c.disable_nee = 0 if self.nee else 1
         c.ray_sort = 1 if self.sort_rays else 0
+        c.serve_aging_steps = int(self.serve_aging_steps)
         return c
 
 

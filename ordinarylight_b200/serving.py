@@ -246,6 +246,50 @@ class RenderServer:
                 self._running = False
 
 
+class SerialServer(RenderServer):
+    """The plain path under the same request stream: one request at a time in
+    arrival order, the way the reference serialises ``render_async``
+    submissions on one worker (ordinarylight/renderer/_core.py:614-651,
+    :709-717), with every scene resident.  Same ``submit``/``start``/``stop``
+    and statistics as :class:`RenderServer`, for latency comparisons."""
+
+    def _loop(self):
+        try:
+            while True:
+                with self._lock:
+                    while self._running and not self._waiting:
+                        self._lock.wait()
+                    if not self._waiting and (not self._running or not self._draining):
+                        break
+                    if not self._running and not self._draining:
+                        break
+                    pending = self._waiting.popleft()
+                pending.admitted = time.perf_counter()
+                try:
+                    image = self.renderer.render_batch([pending.request])[0]
+                except Exception as exc:
+                    self.stats.failed += 1
+                    pending.future.set_exception(exc)
+                    continue
+                t = self.renderer.last_timings
+                self.stats.rays += t.get("rays", 0)
+                self.stats.gpu_ms += t.get("gpu_ms", 0.0)
+                self.stats.steps += 1
+                now = time.perf_counter()
+                self.stats.completed += 1
+                self.stats.latencies_ms.append((now - pending.submitted) * 1e3)
+                self.stats.queue_ms.append((pending.admitted - pending.submitted) * 1e3)
+                pending.future.set_result(image)
+        except BaseException as exc:
+            self._error = exc
+            with self._lock:
+                for pending in list(self._waiting):
+                    if not pending.future.done():
+                        pending.future.set_exception(RuntimeError(f"render server failed: {exc}"))
+                self._waiting.clear()
+                self._running = False
+
+
 def poisson_arrivals(rate_per_s: float, count: int, seed: int = 0) -> np.ndarray:
     """Arrival times (seconds from 0) of a Poisson stream."""
     rng = np.random.default_rng(seed)
@@ -270,5 +314,5 @@ def run_stream(server: RenderServer, requests, arrivals) -> list:
     return futures
 
 
-__all__ = ["AdmissionRejected", "RenderServer", "ServerStatistics", "poisson_arrivals", "run_stream",
-           "DEFAULT_BUDGET_BYTES"]
+__all__ = ["AdmissionRejected", "RenderServer", "SerialServer", "ServerStatistics", "poisson_arrivals",
+           "run_stream", "DEFAULT_BUDGET_BYTES"]

@@ -180,6 +180,33 @@ def test_step_failure_fails_only_the_dropped_jobs():
     assert server.stats.failed == 1
 
 
+def test_serial_server_is_fifo_one_at_a_time():
+    from ordinarylight_b200.serving import SerialServer
+
+    class Serial(FakeRenderer):
+        def __init__(self):
+            super().__init__()
+            self.order = []
+
+        def render_batch(self, requests, outs=None):
+            assert len(requests) == 1
+            q = requests[0]
+            self.order.append(q.width)
+            self.last_timings = {"rays": q.width * q.height, "gpu_ms": 0.5}
+            time.sleep(0.002)
+            return [np.zeros((q.height, q.width, 4), np.float32)]
+
+    r = Serial()
+    sc = FakeScene("s", 1)
+    server = SerialServer(r).start()
+    futures = [server.submit(_req(sc, w, 4)) for w in (64, 8, 32)]
+    for f in futures:
+        f.result(timeout=10)
+    server.stop()
+    assert r.order == [64, 8, 32]
+    assert server.stats.completed == 3 and server.stats.latencies_ms[2] > server.stats.latencies_ms[0]
+
+
 def test_submit_after_stop_raises():
     server = RenderServer(FakeRenderer(), budget_bytes=10**9).start()
     server.stop()
