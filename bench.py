@@ -267,7 +267,8 @@ def run_ours(args, rank, world, device_index):
     torch.cuda.set_device(device_index)
     scene, camera = scenes.instanced_spheres()
     renderer = _make_renderer(device_index)
-    out = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, device=f"cuda:{device_index}")
+    width, height = args.width, args.height
+    out = torch.empty((height, width, 4), dtype=torch.float32, device=f"cuda:{device_index}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device_index}")
     import ctypes
 
@@ -277,7 +278,7 @@ def run_ours(args, rank, world, device_index):
     frame0 = 1000 * rank
     # warm-up (also builds the BVH and captures nothing: ReSTIR frames run uncaptured)
     for k in range(args.warmup):
-        renderer.render_frame_into(scene, camera, WIDTH, HEIGHT, out, frame_index=frame0 + k)
+        renderer.render_frame_into(scene, camera, width, height, out, frame_index=frame0 + k)
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -295,7 +296,7 @@ def run_ours(args, rank, world, device_index):
         with torch.cuda.stream(stream):
             flush.fill_(float(k))  # evict L2 between timed steps
             starts[k].record(stream)
-        renderer.render_frame_into(scene, camera, WIDTH, HEIGHT, out, frame_index=frame0 + args.warmup + k)
+        renderer.render_frame_into(scene, camera, width, height, out, frame_index=frame0 + args.warmup + k)
         with torch.cuda.stream(stream):
             ends[k].record(stream)
         rays += renderer.last_timings["rays"]
@@ -325,12 +326,12 @@ def run_ours(args, rank, world, device_index):
     # end to end through the public API: host output, per-step host clock
     e2e_steps = max(1, min(args.steps, 5))
     for k in range(2):   # page-locked output buffers come from a cache that warms up here
-        renderer.render_frame(scene, camera, WIDTH, HEIGHT, frame_index=frame0 + 490 + k)
+        renderer.render_frame(scene, camera, width, height, frame_index=frame0 + 490 + k)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_rays, h2d, d2h = 0, 0, 0
     for k in range(e2e_steps):
-        img = renderer.render_frame(scene, camera, WIDTH, HEIGHT, frame_index=frame0 + 500 + k)
+        img = renderer.render_frame(scene, camera, width, height, frame_index=frame0 + 500 + k)
         e2e_rays += renderer.last_timings["rays"]
         h2d += renderer.last_timings["h2d_bytes"]
         d2h += renderer.last_timings["d2h_bytes"]
@@ -374,7 +375,9 @@ def run_ours(args, rank, world, device_index):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded scene generators, ordinarylight_b200/scenes.py)",
-        "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_bounces": BOUNCES,
+        "config": {"workload": WORKLOAD if (width, height) == (WIDTH, HEIGHT) else
+                   WORKLOAD.replace("1920x1080", f"{width}x{height} (reduced for profiling)"),
+                   "width": width, "height": height, "spp": SPP, "max_bounces": BOUNCES,
                    "triangles": 1049602, "parallelism": f"replicas x{world} (independent frames per GPU)",
                    "l2": "256 MiB buffer written between timed steps (L2 flush); per-frame queues 1.7 GB"},
         "rays_per_step": rays_all / args.steps,
@@ -674,6 +677,8 @@ def main():
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--cpu-processes", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--width", type=int, default=WIDTH, help="image width (a smaller case for profiling)")
+    p.add_argument("--height", type=int, default=HEIGHT, help="image height (a smaller case for profiling)")
     p.add_argument("--sections", default="config1,config3,batched,served",
                    help="secondary sections run at N=1 (comma list; empty for the headline alone)")
     p.add_argument("--served-rates", default="50,100",

@@ -279,7 +279,9 @@ OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& 
   return true;
 }
 
-__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
+// Three blocks of 256 threads per SM (at most 85 registers): the shading
+// kernel is latency bound, and the occupancy gained outweighs its spills.
+__global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
   const uint32_t n = a.cnt->queue_count[bounce];
