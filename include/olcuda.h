@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OLC_ABI_VERSION 2
+#define OLC_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define OLC_API __attribute__((visibility("default")))
@@ -293,9 +293,22 @@ typedef struct olc_job {
   uint32_t samples_per_pixel;   /* 1..65536 */
   uint32_t frame_index;
   uint32_t max_bounces;         /* 0: the context's max_bounces; else 1..64 */
-  uint32_t reserved[2];
+  uint32_t first_sample;        /* RNG index of the job's first sample: a job
+                                   with first_sample s renders samples
+                                   s .. s + samples_per_pixel - 1 of the frame,
+                                   so disjoint shards of one frame's samples
+                                   can be rendered apart (other GPUs) */
+  uint32_t reserved;
   olc_camera camera;
-  float* out_rgba;              /* (height, width, 4) float32, host or device */
+  float* out_rgba;              /* (height, width, 4) float32 mean of the job's
+                                   samples, host or device; may be NULL when
+                                   out_sums is set */
+  uint64_t* out_sums;           /* optional (height, width, 3) fixed-point sums
+                                   of the job's samples (scale 2^28), host or
+                                   device like out_rgba: shards of a frame add
+                                   exactly, and sum * 2^-28 / spp resolved in
+                                   double and rounded to float equals the
+                                   single-device image bit for bit */
   int32_t out_is_device;
   uint32_t reserved2;
 } olc_job;

@@ -118,8 +118,9 @@ class OlcPoolInfo(ctypes.Structure):
 class OlcJob(ctypes.Structure):
     _fields_ = [
         ("scene", c_uint32), ("width", c_uint32), ("height", c_uint32), ("samples_per_pixel", c_uint32),
-        ("frame_index", c_uint32), ("max_bounces", c_uint32), ("reserved", c_uint32 * 2),
-        ("camera", OlcCamera), ("out_rgba", c_void_p), ("out_is_device", c_int32), ("reserved2", c_uint32),
+        ("frame_index", c_uint32), ("max_bounces", c_uint32), ("first_sample", c_uint32), ("reserved", c_uint32),
+        ("camera", OlcCamera), ("out_rgba", c_void_p), ("out_sums", c_void_p), ("out_is_device", c_int32),
+        ("reserved2", c_uint32),
     ]
 
 

@@ -180,6 +180,7 @@ struct QueuedJob {
   float* out = nullptr;
   bool out_device = false;
   bool out_staged = false;   // pageable host output: copied through the run's pinned staging
+  uint64_t* sums = nullptr;  // optional fixed-point sums output (same memory kind as out)
   // ReSTIR reservoirs at job-local indices (reservoir_base 0), where the next
   // plain frame's temporal pass finds them; otherwise chunk-local ones
   bool job_local_reservoirs = false;
@@ -1253,6 +1254,11 @@ void launch_planned(olc_context* ctx, RunSlot& sl, RunPlan&& plan) {
                                j->out_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
     }
   }
+  for (QueuedJob* j : plan.finished) {
+    if (!j->sums) continue;
+    OLC_CUDA(cudaMemcpyAsync(j->sums, rb.accum + 3ull * j->rec.pixel_base, (size_t)j->rec.npix * 3 * sizeof(uint64_t),
+                             j->out_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  }
   OLC_CUDA(cudaEventRecord(sl.done, st));
   sl.plan = std::move(plan);
   sl.busy = true;
@@ -1364,13 +1370,17 @@ void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
   check_size(d->width, d->height, d->samples_per_pixel);
   if (d->max_bounces > OLC_MAX_BOUNCES) throw Error(OLC_ERR_VALUE, "max_bounces must be between 1 and 64");
   scene_of(ctx, d->scene);
-  if (!d->out_rgba) throw Error(OLC_ERR_VALUE, "output pointer is required");
+  if (!d->out_rgba && !d->out_sums) throw Error(OLC_ERR_VALUE, "an output pointer is required");
+  if ((uint64_t)d->first_sample + d->samples_per_pixel > 0xffffffffull)
+    throw Error(OLC_ERR_VALUE, "first_sample + samples_per_pixel exceeds 2^32");
   q.rec = make_job(ctx, &d->camera, d->width, d->height, d->samples_per_pixel, d->frame_index, d->max_bounces,
                    d->scene);
+  q.rec.sample_base = d->first_sample;
   q.total = (uint64_t)q.rec.npix * q.rec.spp;
   q.out = d->out_rgba;
+  q.sums = d->out_sums;
   q.out_device = d->out_is_device != 0;
-  q.out_staged = !q.out_device && !is_pinned(q.out);
+  q.out_staged = q.out && !q.out_device && !is_pinned(q.out);
 }
 
 bool same_camera(const JobRec& a, const JobRec& b) {

@@ -322,7 +322,7 @@ struct __align__(16) JobRec {
   uint32_t scene;          // SceneRec index
   uint32_t history;        // ReSTIR temporal history valid for this job
   uint32_t products;       // write first-sample primary-hit products
-  uint32_t pad;
+  uint32_t sample_base;    // global index of the job's first sample (a shard of a frame's samples)
   unsigned long long seg_begin;       // chunk-local index of the segment's first path
   unsigned long long seg_first;       // job-local index (sample * npix + pixel) of that path
   unsigned long long pixel_base;      // first pixel of the job in the accumulator and outputs

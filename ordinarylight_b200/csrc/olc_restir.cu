@@ -198,7 +198,7 @@ OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, u
 
 // Reservoir index of (job, sample stream, pixel).
 OLC_D uint64_t reservoir_index(const JobRec& job, uint32_t sample, uint32_t pixel) {
-  return job.reservoir_base + (uint64_t)sample * job.npix + pixel;
+  return job.reservoir_base + (uint64_t)(sample - job.sample_base) * job.npix + pixel;
 }
 
 struct RestirArgs {
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
     if (job.history) {
       float pd;
       uint32_t pn, pstamp;
-      const uint64_t gh = job.history_base + (uint64_t)meta.y * job.npix + meta.x;
+      const uint64_t gh = job.history_base + (uint64_t)(meta.y - job.sample_base) * job.npix + meta.x;
       Res prev = load_res(a.hist0, a.hist1, gh, pd, pn, pstamp);
       if (pstamp != 0u && pstamp >= a.hdr->history_first && pstamp <= a.hdr->history_last && prev.light != 0xffffffffu && prev.M > 0u && prev.target > 0.0f &&
           similar(su, pn, pd)) {

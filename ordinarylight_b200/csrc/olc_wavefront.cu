@@ -59,8 +59,9 @@ __global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __re
     const uint32_t j = segment_of_path(jobs, num_segments, i);
     const JobRec& job = jobs[j];
     const uint64_t local = job.seg_first + (i - job.seg_begin);
-    const uint32_t sample = (uint32_t)(local / job.npix);
-    const uint32_t pixel = (uint32_t)(local - (uint64_t)sample * job.npix);
+    const uint32_t local_sample = (uint32_t)(local / job.npix);
+    const uint32_t pixel = (uint32_t)(local - (uint64_t)local_sample * job.npix);
+    const uint32_t sample = job.sample_base + local_sample;   // the RNG key's sample index
     float3 o, d;
     camera_ray(job, pixel, sample, nullptr, o, d);
     q.origin_tmin[i] = make_float4(o.x, o.y, o.z, job_t_min(job));
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
       const float3 o = f3(ot), d = f3(dr);
       const uint32_t flags = meta.z >> 8;
       const uint32_t out_pixel = meta.x;  // products belong to one plain frame's job
-      const bool write_products = job.products && bounce == 0u && meta.y == 0u && a.prod.depth;
+      const bool write_products = job.products && bounce == 0u && meta.y == job.sample_base && a.prod.depth;
       uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), bounce);
       uint32_t new_flags = 0;
       float new_pdf = 0.0f;

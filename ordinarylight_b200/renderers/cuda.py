@@ -147,6 +147,7 @@ class RenderRequest:
     samples: int | None = None
     frame_index: int = 0
     max_bounces: int | None = None
+    first_sample: int = 0       # RNG index of the first sample (a shard of a frame's samples)
 
 
 def host_image(height: int, width: int) -> np.ndarray:
@@ -371,7 +372,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         return {name: int(getattr(info, name)) for name, _ in info._fields_ if name != "reserved"}
 
     # -- batched and served rendering ---------------------------------------------
-    def _job(self, request: RenderRequest, out, on_device: bool) -> _native.OlcJob:
+    def _job(self, request: RenderRequest, out, on_device: bool, sums=None) -> _native.OlcJob:
         width, height = int(request.width), int(request.height)
         if width <= 0 or height <= 0:
             raise ValueError("width and height must be positive")
@@ -384,7 +385,11 @@ class CudaWavefrontRenderer(RendererImplementation):
         frame_index = int(request.frame_index)
         if frame_index < 0:
             raise ValueError("frame_index cannot be negative")
+        first_sample = int(request.first_sample)
+        if first_sample < 0 or first_sample + spp > 0xFFFFFFFF:
+            raise ValueError("first_sample must be non-negative and first_sample + samples below 2^32")
         job = _native.OlcJob()
+        job.first_sample = first_sample
         job.scene = self.resident_scene(request.scene)
         job.width, job.height = width, height
         job.samples_per_pixel = spp
@@ -392,6 +397,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         job.max_bounces = bounces
         job.camera = pack_camera(request.camera)
         job.out_rgba = _native.ptr(out).value
+        job.out_sums = _native.ptr(sums).value
         job.out_is_device = 1 if on_device else 0
         return job
 
@@ -417,12 +423,16 @@ class CudaWavefrontRenderer(RendererImplementation):
         if stats.traversal_errors:
             raise RuntimeError(f"{stats.traversal_errors} traversal stack overflows")
 
-    def render_batch(self, requests, outs=None):
+    def render_batch(self, requests, outs=None, sums=None):
         """Render many requests as one wavefront (chunks of paths from several
         jobs and scenes share the ray queues; the chunk sequence replays from a
         CUDA graph when the same mix recurs).  Each image equals, bit for bit,
         ``render_frame`` of the same request on a fresh sequence.  Returns the
-        list of (height, width, 4) float32 images (or fills ``outs``)."""
+        list of (height, width, 4) float32 images (or fills ``outs``).
+        ``sums`` (optional, one per request, same memory kind as the image):
+        (height, width, 3) uint64/int64 buffers that receive the requests'
+        fixed-point sample sums, which add exactly across shards of a frame
+        (``ordinarylight_b200.distributed``)."""
         self._require_open()
         requests = list(requests)
         if outs is None:
@@ -430,10 +440,19 @@ class CudaWavefrontRenderer(RendererImplementation):
         if len(outs) != len(requests):
             raise ValueError("outs must match requests")
         t0 = time.perf_counter()
+        if sums is not None and len(sums) != len(requests):
+            raise ValueError("sums must match requests")
         jobs = (_native.OlcJob * max(len(requests), 1))()
         for k, (request, out) in enumerate(zip(requests, outs)):
             on_device = hasattr(out, "data_ptr") and getattr(out, "is_cuda", False)
-            jobs[k] = self._job(request, out, on_device)
+            sm = None if sums is None else sums[k]
+            if sm is not None:
+                count = sm.numel() if hasattr(sm, "numel") else sm.size
+                if count != int(request.width) * int(request.height) * 3:
+                    raise ValueError("a sums buffer must hold height*width*3 64-bit values")
+                if (hasattr(sm, "is_cuda") and sm.is_cuda) != on_device:
+                    raise ValueError("sums and image buffers must both be on the device or both on the host")
+            jobs[k] = self._job(request, out, on_device, sm)
         stats = _native.OlcRenderStats()
         _native.check(self._lib, self._ctx, self._lib.olc_render_batch(self._ctx, jobs, len(requests),
                                                                        ctypes.byref(stats)))

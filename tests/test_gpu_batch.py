@@ -193,3 +193,32 @@ def test_autotuner_keeps_images(native_library, cuda_device, scene_set):
         tuned = r.render_batch(requests)
     for a, b in zip(base, tuned):
         assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("restir", [False, True])
+def test_sample_shards_add_up_to_the_frame_bit_for_bit(native_library, cuda_device, scene_set, restir):
+    import torch
+
+    from ordinarylight_b200.distributed import render_frame_sharded, resolve_sums, sample_shard
+
+    (room, rc), (sph, sc), _ = scene_set
+    for scene, camera in ((room, rc), (sph, sc)):
+        w, h, spp = 48, 40, 7
+        full = _plain(RenderRequest(scene, camera, w, h, samples=spp, frame_index=2, max_bounces=5), restir=restir)
+        with CudaWavefrontRenderer(seed=1, max_bounces=5, restir=restir) as r:
+            # three shards as three ranks would render them, summed on the device
+            total = torch.zeros((h, w, 3), dtype=torch.int64, device="cuda")
+            for rank in range(3):
+                first, count = sample_shard(spp, 3, rank)
+                sums = torch.empty((h, w, 3), dtype=torch.int64, device="cuda")
+                img = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+                r.render_batch([RenderRequest(scene, camera, w, h, samples=count, frame_index=2,
+                                              first_sample=first)], outs=[img], sums=[sums])
+                total += sums
+            assert resolve_sums(total, spp).cpu().numpy().tobytes() == full.tobytes()
+            # host sums, and the one-rank path of render_frame_sharded
+            host = np.empty((h, w, 3), np.uint64)
+            r.render_batch([RenderRequest(scene, camera, w, h, samples=spp, frame_index=2)], sums=[host])
+            assert resolve_sums(host, spp).tobytes() == full.tobytes()
+            single = render_frame_sharded(r, scene, camera, w, h, samples=spp, frame_index=2)
+            assert single.cpu().numpy().tobytes() == full.tobytes()
