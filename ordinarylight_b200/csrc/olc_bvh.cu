@@ -12,6 +12,7 @@
 // radix sort is stable, so the permutation equals
 // numpy.argsort(codes, kind="stable").
 #include <algorithm>
+#include <cmath>
 
 #include "olc_internal.h"
 
@@ -281,11 +282,13 @@ __global__ void k_bottom_up(int n, const int* __restrict__ left, const int* __re
 // (global slot flat_base + p - n_inst).
 struct TlasRefs {
   uint32_t n_inst = 0, inst_base = 0, flat_base = 0;
+  const uint32_t* remap = nullptr;   // build index -> primitive (a subset build), or identity
 };
-OLC_D int tlas_leaf(const TlasRefs& r, uint32_t p) {
+OLC_HD int tlas_prim_leaf(const TlasRefs& r, uint32_t p) {
   return p < r.n_inst ? olc_make_leaf(r.inst_base + p, OLC_TLAS_LEAF_INSTANCE)
                       : olc_make_leaf(r.flat_base + (p - r.n_inst), OLC_TLAS_LEAF_TRIANGLE);
 }
+OLC_D int tlas_leaf(const TlasRefs& r, uint32_t i) { return tlas_prim_leaf(r, r.remap ? r.remap[i] : i); }
 
 // Emit final nodes.  blas: leaves reference slot ranges (collapse subtrees of
 // at most leaf_max leaves); tlas: one instance or baked triangle per leaf.
@@ -569,6 +572,15 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
   return root;
 }
 
+// Large primitives (an instance or baked triangle whose box spans more than
+// a quarter of the scene along some axis, such as a ground plane) make every
+// ancestor in a Morton-ordered hierarchy as large as themselves, so most rays
+// would descend those ancestors.  They are split off: the TLAS root joins an
+// LBVH over the large primitives and an LBVH over the rest, and a ray pays
+// for the large ones once near the root.
+constexpr float kLargeFraction = 0.25f;
+constexpr uint32_t kHoistMaxPrims = 1u << 20;   // above this, one LBVH (no host pass)
+
 uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint32_t instance_base,
                     const float4* tri_verts, const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base,
                     BuildScratch& sc, BvhNode* nodes, uint32_t node_base, cudaStream_t stream) {
@@ -588,7 +600,82 @@ uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint
   tr.n_inst = n;
   tr.inst_base = instance_base;
   tr.flat_base = flat_slot_base;
-  return build_hierarchy(total, sc, 1, tr, 1, nodes, node_base, 0, stream);
+  if (total < 3 || total > kHoistMaxPrims) return build_hierarchy(total, sc, 1, tr, 1, nodes, node_base, 0, stream);
+
+  // classify on the host
+  std::vector<float4> lo(total), hi(total), ce(total);
+  OLC_CUDA(cudaMemcpyAsync(lo.data(), sc.boxes_lo.get(), total * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+  OLC_CUDA(cudaMemcpyAsync(hi.data(), sc.boxes_hi.get(), total * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+  OLC_CUDA(cudaMemcpyAsync(ce.data(), sc.centers.get(), total * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+  OLC_CUDA(cudaStreamSynchronize(stream));
+  float slo[3] = {INFINITY, INFINITY, INFINITY}, shi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t p = 0; p < total; ++p) {
+    const float l[3] = {lo[p].x, lo[p].y, lo[p].z}, h[3] = {hi[p].x, hi[p].y, hi[p].z};
+    for (int a = 0; a < 3; ++a) {
+      slo[a] = std::min(slo[a], l[a]);
+      shi[a] = std::max(shi[a], h[a]);
+    }
+  }
+  std::vector<uint32_t> large, small;
+  for (uint32_t p = 0; p < total; ++p) {
+    const float e[3] = {hi[p].x - lo[p].x, hi[p].y - lo[p].y, hi[p].z - lo[p].z};
+    bool big = false;
+    for (int a = 0; a < 3; ++a)
+      if (shi[a] > slo[a] && e[a] > kLargeFraction * (shi[a] - slo[a])) big = true;
+    (big ? large : small).push_back(p);
+  }
+  if (large.empty() || small.empty()) return build_hierarchy(total, sc, 1, tr, 1, nodes, node_base, 0, stream);
+
+  // two subset builds below a root node at node_base
+  DeviceBuffer remap(total * sizeof(uint32_t));
+  std::vector<float4> sub_lo, sub_hi, sub_ce;
+  int child_ref[2];
+  float4 child_lo[2], child_hi[2];
+  uint32_t next = node_base + 1;
+  const std::vector<uint32_t>* subsets[2] = {&large, &small};
+  uint32_t remap_off = 0;
+  for (int k = 0; k < 2; ++k) {
+    const std::vector<uint32_t>& ids = *subsets[k];
+    const uint32_t m = (uint32_t)ids.size();
+    float4 ul = make_float4(INFINITY, INFINITY, INFINITY, 0.0f), uh = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    for (uint32_t p : ids) {
+      ul = make_float4(std::min(ul.x, lo[p].x), std::min(ul.y, lo[p].y), std::min(ul.z, lo[p].z), 0.0f);
+      uh = make_float4(std::max(uh.x, hi[p].x), std::max(uh.y, hi[p].y), std::max(uh.z, hi[p].z), 0.0f);
+    }
+    child_lo[k] = ul;
+    child_hi[k] = uh;
+    if (m == 1) {
+      child_ref[k] = tlas_prim_leaf(tr, ids[0]);
+      continue;
+    }
+    sub_lo.resize(m);
+    sub_hi.resize(m);
+    sub_ce.resize(m);
+    for (uint32_t i = 0; i < m; ++i) {
+      sub_lo[i] = lo[ids[i]];
+      sub_hi[i] = hi[ids[i]];
+      sub_ce[i] = ce[ids[i]];
+    }
+    OLC_CUDA(cudaMemcpyAsync(sc.boxes_lo.get(), sub_lo.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    OLC_CUDA(cudaMemcpyAsync(sc.boxes_hi.get(), sub_hi.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    OLC_CUDA(cudaMemcpyAsync(sc.centers.get(), sub_ce.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    uint32_t* rm = remap.as<uint32_t>() + remap_off;
+    OLC_CUDA(cudaMemcpyAsync(rm, ids.data(), m * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    TlasRefs sub = tr;
+    sub.remap = rm;
+    child_ref[k] = (int)build_hierarchy(m, sc, 1, sub, 1, nodes, next, 0, stream);
+    next += m - 1;
+    remap_off += m;
+    OLC_CUDA(cudaStreamSynchronize(stream));   // the host staging vectors are reused
+  }
+  BvhNode root;
+  root.a = make_float4(child_lo[0].x, child_hi[0].x, child_lo[0].y, child_hi[0].y);
+  root.b = make_float4(child_lo[1].x, child_hi[1].x, child_lo[1].y, child_hi[1].y);
+  root.c = make_float4(child_lo[0].z, child_hi[0].z, child_lo[1].z, child_hi[1].z);
+  root.d = make_int4(child_ref[0], child_ref[1], 0, 0);
+  OLC_CUDA(cudaMemcpyAsync(nodes + node_base, &root, sizeof(root), cudaMemcpyHostToDevice, stream));
+  OLC_CUDA(cudaStreamSynchronize(stream));
+  return node_base;
 }
 
 // ---- validation ----------------------------------------------------------
