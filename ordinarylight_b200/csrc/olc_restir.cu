@@ -82,16 +82,24 @@ OLC_D PreparedBsdf prepare_bsdf(const SurfaceMat& m, float3 n, float3 view) {
   return b;
 }
 
+// The BSDF times the cosine-free factors for candidate direction l, with
+// hardware reciprocal square roots and approximate divisions: the resampling
+// target only has to be one fixed function of the sample (the estimator stays
+// unbiased for any such target), and this one costs about half of the
+// correctly rounded form per candidate.
 OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
-  float3 h = normalize(b.view + l);
-  float nh = fmaxf(dot(b.n, h), 0.0f);
-  float vh = fmaxf(dot(b.view, h), 0.0f);
-  float w = 1.0f - clampf(vh, 0.0f, 1.0f);
-  float w5 = w * w * w * w * w;
-  float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
-  float D = ggx_d(nh, b.a2);
-  float G = b.g1v * ggx_g1(nl, b.a2);
-  float3 spec = F * (D * G / fmaxf(4.0f * b.nv * nl, 1e-6f));
+  const float3 hv = b.view + l;
+  const float3 h = hv * rsqrtf(fmaxf(dot(hv, hv), 1e-30f));
+  const float nh = fmaxf(dot(b.n, h), 0.0f);
+  const float vh = fmaxf(dot(b.view, h), 0.0f);
+  const float w = 1.0f - clampf(vh, 0.0f, 1.0f);
+  const float w5 = w * w * w * w * w;
+  const float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
+  const float den = nh * nh * (b.a2 - 1.0f) + 1.0f;
+  const float D = __fdividef(b.a2, fmaxf(OLC_PI * den * den, 1e-6f));
+  const float x = b.a2 + (1.0f - b.a2) * nl * nl;
+  const float g1l = __fdividef(2.0f * nl, fmaxf(nl + x * rsqrtf(x), 1e-6f));
+  const float3 spec = F * __fdividef(D * b.g1v * g1l, fmaxf(4.0f * b.nv * nl, 1e-6f));
   return (f3(1.0f, 1.0f, 1.0f) - F) * b.diffuse + spec;
 }
 
@@ -129,7 +137,7 @@ OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uin
   float cl = emitter_cosine(e, l);
   if (cl <= 1e-6f) return 0.0f;
   float3 f = prepared_eval(s.bsdf, l, cs);
-  float t = luminance(f * f3(e.emission)) * cs * cl / d2;
+  float t = luminance(f * f3(e.emission)) * cs * cl * (inv * inv);
   return (t == t && t < 3.0e38f) ? fmaxf(t, 0.0f) : 0.0f;
 }
 
