@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OLC_ABI_VERSION 3
+#define OLC_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define OLC_API __attribute__((visibility("default")))
@@ -121,7 +121,10 @@ typedef struct olc_config {
   uint32_t serve_aging_steps;   /* serving: jobs queued this many steps go
                                    first, oldest first (0: shortest remaining
                                    work first only) */
-  uint32_t reserved[2];
+  uint32_t sample_variance;     /* olc_render keeps each sample's luminance so
+                                   olc_read_variance can return the per-pixel
+                                   sample variance (4 bytes per path sample) */
+  uint32_t reserved[1];
 } olc_config;
 
 /* Scene description: host arrays, copied at upload.  Geometry follows the
@@ -372,6 +375,16 @@ OLC_API int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t widt
 OLC_API int olc_read_products(olc_context* ctx, uint32_t width, uint32_t height,
                       float* depth, float* normal, uint32_t* instance_id,
                       uint32_t* material_id, uint32_t* primitive_id);
+
+/* Unbiased per-pixel sample variance of the luminance
+ * (0.2126 R + 0.7152 G + 0.0722 B) of the last olc_render's samples: the
+ * "variance" product of render_wavefront_outputs
+ * (ordinarylight/targets/vulkan/api.py:1400-1433), (sum(l^2) - sum(l)^2 / spp)
+ * / (spp - 1) in double precision over the samples in order, clamped at 0,
+ * and 0 for one sample.  Needs olc_config.sample_variance for that render.
+ * variance: height*width floats, host or device (out_is_device). */
+OLC_API int olc_read_variance(olc_context* ctx, uint32_t width, uint32_t height,
+                              float* variance, int out_is_device);
 
 /* Forget temporal history (Renderer.reset_sequence ->
  * reset_output_history, ordinarylight/renderer/_core.py:339-351, :447-451). */

@@ -45,8 +45,8 @@ class OlcConfig(ctypes.Structure):
         ("restir_max_history", c_uint32), ("block_size", c_uint32), ("stack_depth", c_uint32),
         ("chunk_paths", c_uint32), ("use_graphs", c_uint32), ("flatten_instances", c_uint32),
         ("trace_scheduler", c_uint32), ("disable_nee", c_uint32), ("trace_block", c_uint32),
-        ("ray_sort", c_uint32), ("serve_aging_steps", c_uint32),
-        ("reserved", c_uint32 * 2),
+        ("ray_sort", c_uint32), ("serve_aging_steps", c_uint32), ("sample_variance", c_uint32),
+        ("reserved", c_uint32 * 1),
     ]
 
 
@@ -150,6 +150,7 @@ _SIGNATURES = {
     "olc_render": ([c_void_p, POINTER(OlcCamera), c_uint32, c_uint32, c_uint32, c_uint32, c_void_p, c_int,
                     POINTER(OlcRenderStats)], c_int),
     "olc_read_products": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "olc_read_variance": ([c_void_p, c_uint32, c_uint32, c_void_p, c_int], c_int),
     "olc_reset_history": ([c_void_p], c_int),
     "olc_trace_closest": ([c_void_p, c_uint32, c_void_p, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
                            c_void_p], c_int),

@@ -265,6 +265,8 @@ struct olc_context {
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim;
   uint32_t prod_pixels = 0;
+  DeviceBuffer sample_lum;         // per-sample luminance of the last plain render (sample_variance)
+  uint32_t lum_spp = 0;            // its samples; 0: none kept
   PoolGroup pixels{{3 * sizeof(unsigned long long), sizeof(float4)}, 1 << 16};
   // run tables (chunk headers + segments, then the resolve list) per slot
   RunSlot runs[2];
@@ -850,6 +852,7 @@ JobRec make_job(const olc_context* ctx, const olc_camera* cam, uint32_t w, uint3
   f.rr_min_survival = ctx->cfg.russian_roulette_min_survival;
   f.nee = ctx->cfg.disable_nee ? 0u : 1u;
   f.scene = scene;
+  f.lum_base = ~0ull;
   const bool restir = ctx->cfg.restir && ctx->cfg.mode == OLC_MODE_PRODUCTION &&
                       scene < ctx->scenes.size() && ctx->scenes[scene] && ctx->scenes[scene]->rec.num_emitters > 0;
   f.restir = restir ? 1u : 0u;
@@ -1020,6 +1023,7 @@ struct RunBuffers {
   Counters* cnt;
   unsigned long long* accum;
   float4* out;
+  float* sample_lum;
   const char* table;
   size_t stride;
   size_t resolve_offset;
@@ -1041,6 +1045,7 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.cnt = ctx->counters.as<Counters>();
   b.accum = ctx->pixels.at<unsigned long long>(0);
   b.out = ctx->pixels.at<float4>(1);
+  b.sample_lum = ctx->sample_lum.as<float>();
   b.table = sl.table_dev.as<char>();
   b.stride = stride;
   b.resolve_offset = resolve_offset;
@@ -1083,7 +1088,7 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
       tl_mark(ctx, OLC_STAGE_SHADOW, b, c);
       std::swap(qin, qout);
     }
-    launch_accumulate(ctx->ls, hdr, jobs, rb.ps, rb.accum, rb.cnt, st);
+    launch_accumulate(ctx->ls, hdr, jobs, rb.ps, rb.accum, rb.sample_lum, rb.cnt, st);
     tl_mark(ctx, OLC_STAGE_ACCUMULATE, 0, c);
     OLC_CUDA(cudaMemcpyAsync(ctx->cur->counters_host + c, rb.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
   }
@@ -1111,7 +1116,7 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.cnt, (const void*)rb.accum,
-                        (const void*)rb.out, (const void*)rb.table, (const void*)ctx->cur->counters_host,
+                        (const void*)rb.out, (const void*)rb.sample_lum, (const void*)rb.table, (const void*)ctx->cur->counters_host,
                         (const void*)ctx->cur,
                         ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_b0.get(),
                         ctx->restir.res_b1.get(), ctx->restir.hist0.get(), ctx->restir.hist1.get(),
@@ -1535,7 +1540,7 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
                                 &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
                                 &ctx->ps_rad, &ctx->ps_meta, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
-                                &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->restir.res_a0,
+                                &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->sample_lum, &ctx->restir.res_a0,
                                 &ctx->restir.res_a1, &ctx->restir.res_b0, &ctx->restir.res_b1, &ctx->restir.hist0,
                                 &ctx->restir.hist1, &ctx->restir.selected, &ctx->restir.hit_list})
     wf += b->bytes();
@@ -1575,6 +1580,15 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     job.rec.reservoir_base = 0;
     job.rec.history_base = 0;
     ensure_products(ctx, job.rec.npix);
+    ctx->lum_spp = 0;
+    if (ctx->cfg.sample_variance) {
+      const size_t bytes = (size_t)job.total * sizeof(float);
+      if (bytes > ctx->sample_lum.bytes()) {
+        ctx->sample_lum.allocate(bytes);
+        drop_graphs(ctx);
+      }
+      job.rec.lum_base = 0;
+    }
     admit_job(ctx, job);
     std::vector<QueuedJob*> jobs{&job};
     try {
@@ -1586,6 +1600,7 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     release_job(ctx, job);
     ctx->last_w = width;
     ctx->last_h = height;
+    ctx->lum_spp = ctx->cfg.sample_variance ? spp : 0u;
     if (restir) {
       restir_finish(rst);
       rst.history_valid = true;
@@ -1794,6 +1809,29 @@ int olc_read_products(olc_context* ctx, uint32_t width, uint32_t height, float* 
         normal[3 * i + 1] = nrm[i].y;
         normal[3 * i + 2] = nrm[i].z;
       }
+  });
+}
+
+int olc_read_variance(olc_context* ctx, uint32_t width, uint32_t height, float* variance, int out_is_device) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (width != ctx->last_w || height != ctx->last_h || ctx->last_w == 0)
+      throw Error(OLC_ERR_VALUE, "products are available only for the size of the last render");
+    if (ctx->lum_spp == 0)
+      throw Error(OLC_ERR_RUNTIME, "the last render kept no sample luminance (enable sample_variance)");
+    if (!variance) throw Error(OLC_ERR_VALUE, "output pointer is required");
+    const uint32_t npix = width * height;
+    cudaStream_t st = ctx->stream;
+    DeviceBuffer staging;
+    float* dst = variance;
+    if (!out_is_device) {
+      staging.allocate((size_t)npix * sizeof(float));
+      dst = staging.as<float>();
+    }
+    launch_sample_variance(ctx->ls, ctx->sample_lum.as<float>(), npix, ctx->lum_spp, dst, st);
+    if (!out_is_device)
+      OLC_CUDA(cudaMemcpyAsync(variance, dst, (size_t)npix * sizeof(float), cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaStreamSynchronize(st));
   });
 }
 

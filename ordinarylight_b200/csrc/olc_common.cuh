@@ -328,6 +328,8 @@ struct __align__(16) JobRec {
   unsigned long long pixel_base;      // first pixel of the job in the accumulator and outputs
   unsigned long long reservoir_base;  // reservoir of (sample, pixel) = base + sample * npix + pixel (mod 2^64)
   unsigned long long history_base;    // first reservoir of its temporal history
+  unsigned long long lum_base;        // per-sample luminance of (sample, pixel) at base + sample * npix + pixel;
+                                      // ~0: not kept
 };
 
 // Header of one chunk's table in device memory, followed by num_segments

@@ -663,16 +663,50 @@ OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
   return __float2ull_rn(v * OLC_ACCUM_SCALE);
 }
 
+// A sample's colour channel as a one-sample image shows it: the fixed-point
+// value divided back (the division k_resolve does for spp = 1).
+OLC_D float from_fixed(unsigned long long v) { return (float)((double)v * (1.0 / (double)OLC_ACCUM_SCALE)); }
+
 __global__ void k_accumulate(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, PathState ps,
-                             unsigned long long* accum, Counters* cnt) {
+                             unsigned long long* accum, float* sample_lum, Counters* cnt) {
   const uint32_t count = hdr->count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const float4 r = ps.radiance[i];
     const uint4 meta = ps.meta[i];
-    unsigned long long* dst = accum + 3ull * (jobs[meta.w].pixel_base + meta.x);
-    atomicAdd(dst + 0, to_fixed(r.x, &cnt->nan_samples));
-    atomicAdd(dst + 1, to_fixed(r.y, &cnt->nan_samples));
-    atomicAdd(dst + 2, to_fixed(r.z, &cnt->nan_samples));
+    const JobRec& job = jobs[meta.w];
+    unsigned long long* dst = accum + 3ull * (job.pixel_base + meta.x);
+    const unsigned long long fr = to_fixed(r.x, &cnt->nan_samples);
+    const unsigned long long fg = to_fixed(r.y, &cnt->nan_samples);
+    const unsigned long long fb = to_fixed(r.z, &cnt->nan_samples);
+    atomicAdd(dst + 0, fr);
+    atomicAdd(dst + 1, fg);
+    atomicAdd(dst + 2, fb);
+    if (job.lum_base != ~0ull) {
+      // luminance in float32 in the reference's operation order
+      // (api.py:1404-1410: r * 0.2126 + g * 0.7152 + b * 0.0722), unfused
+      const float l = __fadd_rn(__fadd_rn(__fmul_rn(from_fixed(fr), 0.2126f), __fmul_rn(from_fixed(fg), 0.7152f)),
+                                __fmul_rn(from_fixed(fb), 0.0722f));
+      sample_lum[job.lum_base + (uint64_t)(meta.y - job.sample_base) * job.npix + meta.x] = l;
+    }
+  }
+}
+
+// Unbiased luminance variance over the samples of each pixel, summed in
+// double precision in sample order (api.py:1411-1431).
+__global__ void k_sample_variance(const float* __restrict__ sample_lum, uint32_t npix, uint32_t spp, float* out) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    if (spp <= 1u) {
+      out[p] = 0.0f;
+      continue;
+    }
+    double sum = 0.0, sq = 0.0;
+    for (uint32_t s = 0; s < spp; ++s) {
+      const double l = (double)sample_lum[(uint64_t)s * npix + p];
+      sum = __dadd_rn(sum, l);
+      sq = __dadd_rn(sq, __dmul_rn(l, l));
+    }
+    const double v = __ddiv_rn(__dsub_rn(sq, __ddiv_rn(__dmul_rn(sum, sum), (double)spp)), (double)(spp - 1u));
+    out[p] = (float)fmax(v, 0.0);
   }
 }
 
@@ -835,9 +869,15 @@ void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue&
 size_t sort_bins_bytes() { return kSortBins * sizeof(uint32_t); }
 
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
-                       unsigned long long* accum, Counters* cnt, cudaStream_t stream) {
-  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, ps, accum, cnt);
+                       unsigned long long* accum, float* sample_lum, Counters* cnt, cudaStream_t stream) {
+  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, ps, accum, sample_lum, cnt);
   OLC_LAUNCH_CHECK("k_accumulate");
+}
+
+void launch_sample_variance(const LaunchShape& ls, const float* sample_lum, uint32_t npix, uint32_t spp, float* out,
+                            cudaStream_t stream) {
+  k_sample_variance<<<ls.grid_simple, ls.block, 0, stream>>>(sample_lum, npix, spp, out);
+  OLC_LAUNCH_CHECK("k_sample_variance");
 }
 
 void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,

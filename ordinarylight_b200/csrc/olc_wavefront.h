@@ -79,7 +79,10 @@ void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue&
                       Counters* cnt, uint32_t bounce, uint32_t* keys, uint32_t* bins, cudaStream_t stream);
 size_t sort_bins_bytes();
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
-                       unsigned long long* accum, Counters* cnt, cudaStream_t stream);
+                       unsigned long long* accum, float* sample_lum, Counters* cnt, cudaStream_t stream);
+// Per-pixel luminance variance of npix pixels from spp sample planes.
+void launch_sample_variance(const LaunchShape& ls, const float* sample_lum, uint32_t npix, uint32_t spp, float* out,
+                            cudaStream_t stream);
 void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,
                     const unsigned long long* accum, float4* out, cudaStream_t stream);
 void launch_camera_rays(const LaunchShape& ls, const JobRec* job, uint32_t sample, const float* jitter,

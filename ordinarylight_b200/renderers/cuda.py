@@ -38,7 +38,7 @@ from ..packing import pack_camera, pack_scene
 from .base import RendererImplementation, RendererImplementationInfo
 
 _MODES = {"production": _native.MODE_PRODUCTION, "reference_compatible": _native.MODE_REFERENCE_COMPATIBLE}
-_PRODUCTS = ("color", "depth", "normal", "instance_id", "object_id", "material_id")
+_PRODUCTS = ("color", "variance", "depth", "normal", "instance_id", "object_id", "material_id")
 
 
 @dataclass(frozen=True)
@@ -70,6 +70,7 @@ class CudaRendererConfig:
     nee: bool = True
     sort_rays: bool = False
     serve_aging_steps: int = 8
+    sample_variance: bool = False
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -130,6 +131,7 @@ class CudaRendererConfig:
         c.disable_nee = 0 if self.nee else 1
         c.ray_sort = 1 if self.sort_rays else 0
         c.serve_aging_steps = int(self.serve_aging_steps)
+        c.sample_variance = 1 if self.sample_variance else 0
         return c
 
 
@@ -299,25 +301,33 @@ class CudaWavefrontRenderer(RendererImplementation):
         return out
 
     def render_products(self, scene, camera, width, height, *, outputs, samples=None, frame_index=0):
-        """Named products (ProductRendererProtocol, base.py:74-90): ``color``
-        plus the first sample's primary-hit ``depth``, ``normal``,
-        ``instance_id``/``object_id`` and ``material_id`` (shapes of
-        ordinarylight/renderer/_core.py:768-777)."""
+        """Named products (ProductRendererProtocol, base.py:74-90): ``color``,
+        the per-pixel luminance ``variance`` over the frame's samples
+        (api.py:1400-1433), and the first sample's primary-hit ``depth``,
+        ``normal``, ``instance_id``/``object_id`` and ``material_id`` (shapes
+        of ordinarylight/renderer/_core.py:768-777).  Asking for ``variance``
+        switches ``sample_variance`` on for this and later frames."""
         self._require_open()
         requested = (outputs,) if isinstance(outputs, str) else tuple(outputs)
         unknown = [name for name in requested if name not in self.available_outputs]
         if unknown:
             raise ValueError(f"unsupported render outputs {tuple(unknown)}")
+        if "variance" in requested and not self.config.sample_variance:
+            self.reconfigure(sample_variance=True)
         color = self.render_frame(scene, camera, width, height, samples=samples, frame_index=frame_index)
         h, w = int(height), int(width)
+        variance = None
+        if "variance" in requested:
+            variance = np.empty((h, w), np.float32)
+            _native.check(self._lib, self._ctx, self._lib.olc_read_variance(self._ctx, w, h, _native.ptr(variance), 0))
         depth = np.empty((h, w), np.float32)
         normal = np.empty((h, w, 3), np.float32)
         inst = np.empty((h, w), np.uint32)
         mat = np.empty((h, w), np.uint32)
         _native.check(self._lib, self._ctx, self._lib.olc_read_products(
             self._ctx, w, h, _native.ptr(depth), _native.ptr(normal), _native.ptr(inst), _native.ptr(mat), None))
-        table = {"color": color, "depth": depth, "normal": normal, "instance_id": inst, "object_id": inst.copy(),
-                 "material_id": mat}
+        table = {"color": color, "variance": variance, "depth": depth, "normal": normal, "instance_id": inst,
+                 "object_id": inst.copy(), "material_id": mat}
         return {name: table[name] for name in requested}
 
     def primitive_ids(self, width, height):

@@ -168,3 +168,38 @@ def test_render_products_follow_the_primary_hits(native_library, cuda_device):
     assert np.all(np.isinf(prods["depth"].reshape(-1)[~hit]))
     mats = {scene.material_id(m.material) for m in scene.meshes}
     assert set(np.unique(prods["material_id"].reshape(-1)[hit]).tolist()) <= mats
+
+
+def _reference_variance(per_sample):
+    """The variance product of render_wavefront_outputs
+    (ordinarylight/targets/vulkan/api.py:1404-1431) from per-sample images."""
+    lum_sum = lum_sq = None
+    for radiance in per_sample:
+        lum = (radiance[..., 0] * 0.2126 + radiance[..., 1] * 0.7152 + radiance[..., 2] * 0.0722).astype(np.float64)
+        if lum_sum is None:
+            lum_sum, lum_sq = lum, lum * lum
+        else:
+            lum_sum = lum_sum + lum
+            lum_sq = lum_sq + lum * lum
+    n = len(per_sample)
+    if n == 1:
+        return np.zeros(per_sample[0].shape[:2], np.float32)
+    return np.maximum((lum_sq - lum_sum * lum_sum / n) / (n - 1), 0.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("restir", [False, True])
+def test_variance_product_is_the_sample_variance_of_the_samples(native_library, cuda_device, restir):
+    from ordinarylight_b200.renderers.cuda import RenderRequest
+
+    scene, camera = scenes.instanced_spheres(seed=7, instances=6, segments=24, bands=13, emitters=32)
+    w, h, spp = 40, 32, 6
+    with CudaWavefrontRenderer(max_bounces=4, restir=restir) as r:
+        prods = r.render_products(scene, camera, w, h, outputs=("color", "variance"), samples=spp, frame_index=3)
+        per_sample = r.render_batch([RenderRequest(scene, camera, w, h, samples=1, frame_index=3, first_sample=s)
+                                     for s in range(spp)])
+        one = r.render_products(scene, camera, w, h, outputs="variance", samples=1, frame_index=4)["variance"]
+    var = prods["variance"]
+    assert var.shape == (h, w) and var.dtype == np.float32
+    assert var.tobytes() == _reference_variance([img[..., :3] for img in per_sample]).tobytes()
+    assert np.count_nonzero(var) > var.size // 10
+    assert not one.any()
