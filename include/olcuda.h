@@ -257,6 +257,26 @@ OLC_API int olc_add_scene(olc_context* ctx, const olc_scene_desc* scene, uint32_
  * later scenes.  Queued jobs that render it must have completed. */
 OLC_API int olc_remove_scene(olc_context* ctx, uint32_t handle);
 
+/* Handle that names the olc_upload_scene scene in olc_update_scene. */
+#define OLC_DEFAULT_SCENE 0xffffffffu
+
+/* Update a resident scene in place (animation, material or light edits)
+ * from a description with the same layout: per-mesh vertex and triangle
+ * counts, instance-to-mesh mapping, material/emitter/light counts and
+ * environment image size.  Meshes flagged in mesh_changed ([num_meshes];
+ * NULL = all) get their triangles rewritten and their BLAS refit with the
+ * hierarchy unchanged; instance transforms, baked triangles, the TLAS,
+ * materials, emitters, lights, environment and volume are rewritten.
+ * *applied = 1 on success; 0 (nothing changed) when the layout differs, in
+ * which case the caller uploads the scene again.  refitted (optional)
+ * receives the number of refit BLAS.  Temporal ReSTIR history of the scene
+ * is dropped.  Queued jobs that render the scene must have completed.
+ * Replaces _try_update_window_scene (ordinarylight/targets/vulkan/core.py:4696-4868),
+ * _refit_scene_blases and _rebuild_scene_tlas
+ * (ordinarylight/targets/vulkan/scene.py:1217-1330). */
+OLC_API int olc_update_scene(olc_context* ctx, uint32_t handle, const olc_scene_desc* scene,
+                             const uint8_t* mesh_changed, int32_t* applied, uint32_t* refitted);
+
 /* Statistics of one resident scene (handle from olc_add_scene). */
 typedef struct olc_scene_stats {
   uint64_t bytes;            /* device bytes of the scene's data and hierarchy */

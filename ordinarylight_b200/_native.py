@@ -31,6 +31,7 @@ PROJECTION_PANORAMIC = 2
 ENV_NONE = 0
 ENV_CONSTANT = 1
 ENV_EQUIRECT = 2
+DEFAULT_SCENE = 0xFFFFFFFF
 
 _f32p = POINTER(c_float)
 _u32p = POINTER(c_uint32)
@@ -139,6 +140,8 @@ _SIGNATURES = {
     "olc_scene_bytes": ([c_void_p, POINTER(c_uint64)], c_int),
     "olc_add_scene": ([c_void_p, POINTER(OlcSceneDesc), POINTER(c_uint32)], c_int),
     "olc_remove_scene": ([c_void_p, c_uint32], c_int),
+    "olc_update_scene": ([c_void_p, c_uint32, POINTER(OlcSceneDesc), c_void_p, POINTER(c_int32), POINTER(c_uint32)],
+                         c_int),
     "olc_scene_stats_get": ([c_void_p, c_uint32, POINTER(OlcSceneStats)], c_int),
     "olc_pool_info_get": ([c_void_p, POINTER(OlcPoolInfo)], c_int),
     "olc_render_batch": ([c_void_p, POINTER(OlcJob), c_uint32, POINTER(OlcRenderStats)], c_int),

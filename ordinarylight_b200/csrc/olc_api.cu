@@ -160,11 +160,33 @@ struct PoolGroup {
 };
 
 // One resident scene: its ranges of the pool and its own image and volume.
+// Placement of a scene description in the pool: which instances are baked
+// into world-space triangles, the scene-local instance order (TLAS members
+// first, then the baked originals, whose records hold material and Mesh.id),
+// and where each mesh's BLAS nodes and the TLAS go in the scene's node range.
+struct SceneLayout {
+  uint32_t nm = 0, ni = 0, total_v = 0, total_t = 0;
+  std::vector<uint8_t> flat;
+  uint64_t flat_tris = 0;
+  uint32_t flat_count = 0;
+  std::vector<uint32_t> order;       // member instances (not baked)
+  std::vector<uint32_t> local_of;    // scene-local record of each instance
+  uint32_t members = 0;
+  std::vector<uint8_t> mesh_used;    // a BLAS is built for the mesh
+  std::vector<uint32_t> node_local;  // first node of each built BLAS
+  uint32_t tlas_local = 0, tlas_nodes = 0, node_count = 0;
+  uint64_t slot_count = 0;
+  // what an in-place update must find unchanged
+  std::vector<uint32_t> mesh_vertex_offset, mesh_triangle_offset, instance_mesh;
+};
+
 struct ResidentScene {
   Range nodes, slots, instances, materials, emitters, lights;
   DeviceBuffer env_image, volume;
   SceneRec rec{};
+  SceneLayout layout;
   std::vector<BlasRange> blas_ranges;
+  std::vector<uint32_t> blas_root;   // per mesh (0 where no BLAS is built)
   uint32_t triangles = 0, blas_count = 0, blas_nodes = 0, tlas_nodes = 0, flattened = 0;
   uint64_t bytes = 0;
   double build_ms = 0.0;
@@ -511,9 +533,12 @@ void check_scene_desc(const olc_scene_desc* d) {
     if (d->mesh_vertex_offset[m + 1] < d->mesh_vertex_offset[m] ||
         d->mesh_triangle_offset[m + 1] < d->mesh_triangle_offset[m])
       throw Error(OLC_ERR_VALUE, "mesh offsets must be non-decreasing");
-    uint32_t nv = d->mesh_vertex_offset[m + 1] - d->mesh_vertex_offset[m];
-    for (uint64_t k = 3ull * d->mesh_triangle_offset[m]; k < 3ull * d->mesh_triangle_offset[m + 1]; ++k)
-      if (d->indices[k] >= nv) throw Error(OLC_ERR_VALUE, "an index refers to a vertex that does not exist");
+    const uint32_t nv = d->mesh_vertex_offset[m + 1] - d->mesh_vertex_offset[m];
+    const uint64_t k0 = 3ull * d->mesh_triangle_offset[m], k1 = 3ull * d->mesh_triangle_offset[m + 1];
+    if (k1 == k0) continue;
+    uint32_t largest = 0;  // a max reduction vectorises; an early exit would not
+    for (uint64_t k = k0; k < k1; ++k) largest = std::max(largest, d->indices[k]);
+    if (largest >= nv) throw Error(OLC_ERR_VALUE, "an index refers to a vertex that does not exist");
   }
   for (uint32_t i = 0; i < ni; ++i) {
     if (d->instance_mesh[i] >= nm) throw Error(OLC_ERR_VALUE, "instance refers to a missing mesh");
@@ -528,6 +553,222 @@ void check_scene_desc(const olc_scene_desc* d) {
     throw Error(OLC_ERR_VALUE, "equirect environment needs an image");
 }
 
+uint32_t mesh_triangles(const olc_scene_desc* d, uint32_t m) {
+  return d->mesh_triangle_offset[m + 1] - d->mesh_triangle_offset[m];
+}
+
+SceneLayout plan_scene(const olc_context* ctx, const olc_scene_desc* d) {
+  SceneLayout L;
+  const uint32_t nm = d->num_meshes, ni = d->num_instances;
+  L.nm = nm;
+  L.ni = ni;
+  L.total_v = nm ? d->mesh_vertex_offset[nm] : 0;
+  L.total_t = nm ? d->mesh_triangle_offset[nm] : 0;
+  L.flat.assign(ni, 0);
+  for (uint32_t i = 0; i < ni; ++i) {
+    uint32_t nt = mesh_triangles(d, d->instance_mesh[i]);
+    if (nt > 0 && nt <= kFlattenMaxTriangles) {
+      L.flat[i] = 1;
+      L.flat_tris += nt;
+      ++L.flat_count;
+    }
+  }
+  if (!ctx->cfg.flatten_instances || L.flat_count < 2 || L.flat_tris > kFlattenMaxTotal) {
+    std::fill(L.flat.begin(), L.flat.end(), 0);
+    L.flat_tris = 0;
+    L.flat_count = 0;
+  }
+  for (uint32_t i = 0; i < ni; ++i)
+    if (!L.flat[i]) L.order.push_back(i);
+  L.members = (uint32_t)L.order.size();
+  L.local_of.assign(ni, 0);
+  for (uint32_t k = 0; k < L.members; ++k) L.local_of[L.order[k]] = k;
+  {
+    uint32_t k = L.members;
+    for (uint32_t i = 0; i < ni; ++i)
+      if (L.flat[i]) L.local_of[i] = k++;
+  }
+  L.mesh_used.assign(nm, 0);
+  for (uint32_t k = 0; k < L.members; ++k) L.mesh_used[d->instance_mesh[L.order[k]]] = 1;
+  L.node_local.assign(nm, 0);
+  uint32_t node_count = 0;
+  for (uint32_t m = 0; m < nm; ++m) {
+    L.node_local[m] = node_count;
+    if (L.mesh_used[m]) node_count += blas_node_count(mesh_triangles(d, m));
+  }
+  L.tlas_local = node_count;
+  const uint64_t tlas_prims = (uint64_t)L.members + L.flat_tris;
+  L.tlas_nodes = tlas_prims > 1 ? (uint32_t)(tlas_prims - 1) : 1;
+  L.node_count = node_count + L.tlas_nodes;
+  L.slot_count = (uint64_t)L.total_t + L.flat_tris;
+  if (nm) {
+    L.mesh_vertex_offset.assign(d->mesh_vertex_offset, d->mesh_vertex_offset + nm + 1);
+    L.mesh_triangle_offset.assign(d->mesh_triangle_offset, d->mesh_triangle_offset + nm + 1);
+  }
+  L.instance_mesh.assign(d->instance_mesh, d->instance_mesh + ni);
+  return L;
+}
+
+bool same_layout(const SceneLayout& a, const SceneLayout& b) {
+  return a.flat == b.flat && a.mesh_vertex_offset == b.mesh_vertex_offset &&
+         a.mesh_triangle_offset == b.mesh_triangle_offset && a.instance_mesh == b.instance_mesh;
+}
+
+// Everything of a resident scene besides its BLAS: instance records, the
+// baked world-space triangles, the TLAS, materials, emitters, lights,
+// environment, volume and the SceneRec.  Runs at upload and at every
+// in-place update (a transform, material or light change rewrites all of
+// it; only the TLAS build costs more than a copy).
+void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs, uint64_t& own) {
+  cudaStream_t st = ctx->stream;
+  const SceneLayout& L = rs.layout;
+  const uint32_t ni = L.ni;
+  const uint32_t slot0 = (uint32_t)rs.slots.off, inst0 = (uint32_t)rs.instances.off;
+  const uint32_t node0 = (uint32_t)rs.nodes.off, mat0 = (uint32_t)rs.materials.off;
+  const uint32_t flat_slot0 = slot0 + L.total_t;
+  BvhNode* nodes = ctx->nodes.at<BvhNode>(0);
+  float4* tri_verts = ctx->slots.at<float4>(0);
+  float4* tri_normals = ctx->slots.at<float4>(1);
+  uint32_t* tri_index = ctx->slots.at<uint32_t>(2);
+  uint32_t* tri_owner = ctx->slots.at<uint32_t>(3);
+  uint64_t staging = 0;
+
+  // ---- instance records (global indices)
+  std::vector<InstanceRec> inst(ni);
+  std::vector<float> o2w(12ull * std::max<uint32_t>(L.members, 1), 0.0f);
+  for (uint32_t i = 0; i < ni; ++i) {
+    const float* m = d->instance_object_to_world + 12ull * i;
+    const uint32_t k = L.local_of[i];
+    InstanceRec& r = inst[k];
+    fill_instance(r, m);
+    r.blas_root = rs.blas_root[d->instance_mesh[i]];
+    r.material = mat0 + d->instance_material[i];
+    r.prim_offset = d->instance_primitive_offset[i];
+    r.instance_id = d->instance_id[i];
+    if (k < L.members)
+      for (int c = 0; c < 12; ++c) o2w[12ull * k + c] = m[c];
+  }
+  // world-space triangles of the baked instances, in packed order; the
+  // TLAS references their slots directly and hits report the identity
+  // record, whose tri_owner entries name the original instances
+  std::vector<float4> fv(3ull * L.flat_tris), fn(3ull * L.flat_tris);
+  std::vector<uint32_t> fpacked(L.flat_tris), fowner(L.flat_tris);
+  {
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < ni; ++i) {
+      if (!L.flat[i]) continue;
+      const InstanceRec& r = inst[L.local_of[i]];
+      Affine mo{r.o2w0, r.o2w1, r.o2w2}, mw{r.w2o0, r.w2o1, r.w2o2};
+      const uint32_t m = d->instance_mesh[i];
+      const uint32_t v0 = d->mesh_vertex_offset[m];
+      for (uint32_t lt = 0; lt < mesh_triangles(d, m); ++lt, ++t) {
+        for (int c = 0; c < 3; ++c) {
+          uint32_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
+          float3 p = xform_point(mo, make_float3(d->vertices[3ull * vi], d->vertices[3ull * vi + 1],
+                                                 d->vertices[3ull * vi + 2]));
+          float3 nn = normalize(xform_normal_by_inverse(
+              mw, make_float3(d->normals[3ull * vi], d->normals[3ull * vi + 1], d->normals[3ull * vi + 2])));
+          fv[3 * t + c] = make_float4(p.x, p.y, p.z, 0.0f);
+          fn[3 * t + c] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+        }
+        fpacked[t] = r.prim_offset + lt;
+        fowner[t] = inst0 + L.local_of[i];
+      }
+    }
+  }
+  upload_to(tri_verts + 3ull * flat_slot0, fv.data(), fv.size(), st);
+  upload_to(tri_normals + 3ull * flat_slot0, fn.data(), fn.size(), st);
+  upload_to(tri_index + flat_slot0, fpacked.data(), fpacked.size(), st);
+  upload_to(tri_owner + flat_slot0, fowner.data(), fowner.size(), st);
+  upload_to(ctx->instances.at<InstanceRec>(0, inst0), inst.data(), inst.size(), st);
+
+  // ---- TLAS over the member instances and the baked triangles
+  std::vector<uint2> ranges(std::max<uint32_t>(L.members, 1));
+  uint32_t max_tris = 0;
+  for (uint32_t k = 0; k < L.members; ++k) {
+    const uint32_t m = d->instance_mesh[L.order[k]];
+    ranges[k] = make_uint2(slot0 + d->mesh_triangle_offset[m], slot0 + d->mesh_triangle_offset[m + 1]);
+    max_tris = std::max(max_tris, mesh_triangles(d, m));
+  }
+  DeviceBuffer d_o2w, d_ranges;
+  upload(d_o2w, o2w.data(), o2w.size(), st, staging);
+  upload(d_ranges, ranges.data(), L.members, st, staging);
+  const uint32_t tlas_root =
+      build_tlas(d_o2w.as<float>(), d_ranges.as<uint2>(), L.members, max_tris, inst0, tri_verts, tri_verts + 3ull * flat_slot0,
+                 (uint32_t)L.flat_tris, flat_slot0, ctx->scratch, nodes, node0 + L.tlas_local, st);
+
+  // ---- materials, emitters, lights
+  std::vector<MaterialRec> mats(d->num_materials);
+  std::vector<MaterialAux> aux(d->num_materials);
+  for (uint32_t k = 0; k < d->num_materials; ++k) {
+    const float* p = d->materials + 16ull * k;
+    mats[k].base_rough = make_float4(p[0], p[1], p[2], p[3]);
+    mats[k].emit_metal = make_float4(p[4], p[5], p[6], p[7]);
+    aux[k].two_sided = p[8] > 0.5f ? 1u : 0u;
+    uint32_t mid;
+    std::memcpy(&mid, &p[9], 4);
+    aux[k].material_id = mid;
+    aux[k].pad0 = aux[k].pad1 = 0;
+  }
+  upload_to(ctx->materials.at<MaterialRec>(0, mat0), mats.data(), mats.size(), st);
+  upload_to(ctx->materials.at<MaterialAux>(1, mat0), aux.data(), aux.size(), st);
+  std::vector<EmitterRec> em;
+  std::vector<AliasEntry> alias;
+  build_emitters(d, em, alias);
+  upload_to(ctx->emitters.at<EmitterRec>(0, rs.emitters.off), em.data(), em.size(), st);
+  upload_to(ctx->emitters.at<AliasEntry>(1, rs.emitters.off), alias.data(), alias.size(), st);
+  if (d->num_lights && !d->lights) throw Error(OLC_ERR_VALUE, "light records are required");
+  upload_to(ctx->lights.at<LightRec>(0, rs.lights.off), reinterpret_cast<const LightRec*>(d->lights),
+            d->num_lights, st);
+  size_t env_count =
+      d->environment_kind == OLC_ENV_EQUIRECT ? 3ull * d->environment_width * d->environment_height : 0;
+  upload(rs.env_image, d->environment_image, env_count, st, own);
+  size_t vol_count = d->volume_present ? (size_t)d->volume_dims[0] * d->volume_dims[1] * d->volume_dims[2] : 0;
+  if (d->volume_present && (!d->volume_density || vol_count == 0))
+    throw Error(OLC_ERR_VALUE, "a volume needs a density grid");
+  upload(rs.volume, d->volume_density, vol_count, st, own);
+  OLC_CUDA(cudaStreamSynchronize(st));  // host staging vectors go out of scope
+
+  SceneRec& v = rs.rec;
+  std::memset(&v, 0, sizeof(v));
+  v.tlas_root = tlas_root;
+  v.emitter_base = (uint32_t)rs.emitters.off;
+  v.num_emitters = d->num_emitters;
+  v.emissive_weight = d->emissive_weight;
+  v.light_base = (uint32_t)rs.lights.off;
+  v.num_lights = d->num_lights;
+  v.env_kind = d->environment_kind;
+  v.env_rotation = d->environment_rotation;
+  v.env_color = make_float4(d->environment_color[0], d->environment_color[1], d->environment_color[2], 0.0f);
+  v.env_image = rs.env_image.as<float>();
+  v.env_w = d->environment_width;
+  v.env_h = d->environment_height;
+  v.volume = rs.volume.as<float>();
+  v.volume_present = d->volume_present;
+  v.vol_nx = d->volume_dims[0];
+  v.vol_ny = d->volume_dims[1];
+  v.vol_nz = d->volume_dims[2];
+  const float* vb = d->volume_world_to_box;
+  v.vol_w2b0 = make_float4(vb[0], vb[1], vb[2], vb[3]);
+  v.vol_w2b1 = make_float4(vb[4], vb[5], vb[6], vb[7]);
+  v.vol_w2b2 = make_float4(vb[8], vb[9], vb[10], vb[11]);
+  v.vol_sigma_t_scale = d->volume_sigma_t_scale;
+  v.vol_albedo = d->volume_albedo;
+  v.vol_max_density = d->volume_max_density;
+}
+
+BlasDesc mesh_blas_desc(const olc_scene_desc* d, uint32_t m, const DeviceBuffer& dv, const DeviceBuffer& dn,
+                        const DeviceBuffer& di) {
+  BlasDesc bd;
+  const uint32_t v0 = d->mesh_vertex_offset[m], t0 = d->mesh_triangle_offset[m];
+  bd.vertices = dv.as<float>() + 3ull * v0;
+  bd.normals = dn.as<float>() + 3ull * v0;
+  bd.indices = di.as<uint32_t>() + 3ull * t0;
+  bd.num_vertices = d->mesh_vertex_offset[m + 1] - v0;
+  bd.num_triangles = mesh_triangles(d, m);
+  return bd;
+}
+
 // Build one scene into the pool.  Every range is acquired before any data is
 // written (a growth moves the arrays), and all of them are released again if
 // the build fails.
@@ -535,67 +776,21 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs) {
   auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = ctx->stream;
   check_scene_desc(d);
-  const uint32_t nm = d->num_meshes, ni = d->num_instances;
-  const uint32_t total_v = nm ? d->mesh_vertex_offset[nm] : 0, total_t = nm ? d->mesh_triangle_offset[nm] : 0;
-  auto mesh_tris = [&](uint32_t m) { return d->mesh_triangle_offset[m + 1] - d->mesh_triangle_offset[m]; };
-  // ---- instance flattening
-  std::vector<uint8_t> flat(ni, 0);
-  uint64_t flat_tris = 0;
-  uint32_t flat_count = 0;
-  for (uint32_t i = 0; i < ni; ++i) {
-    uint32_t nt = mesh_tris(d->instance_mesh[i]);
-    if (nt > 0 && nt <= kFlattenMaxTriangles) {
-      flat[i] = 1;
-      flat_tris += nt;
-      ++flat_count;
-    }
-  }
-  if (!ctx->cfg.flatten_instances || flat_count < 2 || flat_tris > kFlattenMaxTotal) {
-    std::fill(flat.begin(), flat.end(), 0);
-    flat_tris = 0;
-    flat_count = 0;
-  }
-  // scene-local instance order: TLAS members (instances kept as instances),
-  // then the baked originals (their records hold material and Mesh.id)
-  std::vector<uint32_t> order;
-  for (uint32_t i = 0; i < ni; ++i)
-    if (!flat[i]) order.push_back(i);
-  const uint32_t members = (uint32_t)order.size();
-  std::vector<uint32_t> local_of(ni);
-  for (uint32_t k = 0; k < members; ++k) local_of[order[k]] = k;
-  {
-    uint32_t k = members;
-    for (uint32_t i = 0; i < ni; ++i)
-      if (flat[i]) local_of[i] = k++;
-  }
-  std::vector<uint8_t> mesh_used(nm, 0);
-  for (uint32_t k = 0; k < members; ++k) mesh_used[d->instance_mesh[order[k]]] = 1;
-  std::vector<uint32_t> node_local(nm, 0), blas_root(nm, 0);
-  uint32_t node_count = 0;
-  for (uint32_t m = 0; m < nm; ++m) {
-    node_local[m] = node_count;
-    if (mesh_used[m]) node_count += blas_node_count(mesh_tris(m));
-  }
-  const uint32_t tlas_local = node_count;
-  const uint64_t tlas_prims = (uint64_t)members + flat_tris;
-  const uint32_t tlas_nodes = tlas_prims > 1 ? (uint32_t)(tlas_prims - 1) : 1;
-  node_count += tlas_nodes;
-  const uint64_t slot_count = (uint64_t)total_t + flat_tris;
-
+  rs.layout = plan_scene(ctx, d);
+  const SceneLayout& L = rs.layout;
+  const uint32_t nm = L.nm;
   try {
     // ---- pool ranges (acquire everything first)
-    rs.nodes = ctx->nodes.acquire(node_count, st);
-    rs.slots = ctx->slots.acquire(std::max<uint64_t>(slot_count, 1), st);
-    rs.instances = ctx->instances.acquire(ni, st);
+    rs.nodes = ctx->nodes.acquire(L.node_count, st);
+    rs.slots = ctx->slots.acquire(std::max<uint64_t>(L.slot_count, 1), st);
+    rs.instances = ctx->instances.acquire(L.ni, st);
     rs.materials = ctx->materials.acquire(d->num_materials, st);
     rs.emitters = ctx->emitters.acquire(d->num_emitters, st);
     rs.lights = ctx->lights.acquire(d->num_lights, st);
     if (rs.slots.off + rs.slots.n >= (1ull << 28)) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^28 triangle slots");
     if (rs.instances.off + rs.instances.n >= (1ull << 28)) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^28 instances");
     if (rs.nodes.off + rs.nodes.n >= 0x7fffffffull) throw Error(OLC_ERR_MEMORY, "scene pool exceeds 2^31 nodes");
-    const uint32_t slot0 = (uint32_t)rs.slots.off, inst0 = (uint32_t)rs.instances.off;
-    const uint32_t node0 = (uint32_t)rs.nodes.off, mat0 = (uint32_t)rs.materials.off;
-    const uint32_t flat_slot0 = slot0 + total_t;
+    const uint32_t slot0 = (uint32_t)rs.slots.off, node0 = (uint32_t)rs.nodes.off;
     BvhNode* nodes = ctx->nodes.at<BvhNode>(0);
     float4* tri_verts = ctx->slots.at<float4>(0);
     float4* tri_normals = ctx->slots.at<float4>(1);
@@ -606,151 +801,27 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs) {
     // ---- geometry staging and BLAS builds
     uint64_t staging = 0;
     DeviceBuffer dv, dn, di;
-    upload(dv, d->vertices, 3ull * total_v, st, staging);
-    upload(dn, d->normals, 3ull * total_v, st, staging);
-    upload(di, d->indices, 3ull * total_t, st, staging);
+    upload(dv, d->vertices, 3ull * L.total_v, st, staging);
+    upload(dn, d->normals, 3ull * L.total_v, st, staging);
+    upload(di, d->indices, 3ull * L.total_t, st, staging);
     rs.blas_ranges.clear();
+    rs.blas_root.assign(nm, 0);
     for (uint32_t m = 0; m < nm; ++m) {
-      if (!mesh_used[m]) continue;
-      BlasDesc bd;
-      uint32_t v0 = d->mesh_vertex_offset[m], t0i = d->mesh_triangle_offset[m];
-      bd.vertices = dv.as<float>() + 3ull * v0;
-      bd.normals = dn.as<float>() + 3ull * v0;
-      bd.indices = di.as<uint32_t>() + 3ull * t0i;
-      bd.num_vertices = d->mesh_vertex_offset[m + 1] - v0;
-      bd.num_triangles = mesh_tris(m);
-      blas_root[m] = build_blas(bd, ctx->scratch, nodes, node0 + node_local[m], tri_verts, tri_normals, tri_index,
-                                slot0 + t0i, 4, st);
-      rs.blas_ranges.push_back({blas_root[m], slot0 + t0i, slot0 + t0i + bd.num_triangles});
+      if (!L.mesh_used[m]) continue;
+      const BlasDesc bd = mesh_blas_desc(d, m, dv, dn, di);
+      const uint32_t first_slot = slot0 + d->mesh_triangle_offset[m];
+      rs.blas_root[m] = build_blas(bd, ctx->scratch, nodes, node0 + L.node_local[m], tri_verts, tri_normals,
+                                   tri_index, first_slot, 4, st);
+      rs.blas_ranges.push_back({rs.blas_root[m], first_slot, first_slot + bd.num_triangles});
     }
-
-    // ---- instance records (global indices)
-    std::vector<InstanceRec> inst(ni);
-    std::vector<float> o2w(12ull * std::max<uint32_t>(members, 1), 0.0f);
-    for (uint32_t i = 0; i < ni; ++i) {
-      const float* m = d->instance_object_to_world + 12ull * i;
-      const uint32_t k = local_of[i];
-      InstanceRec& r = inst[k];
-      fill_instance(r, m);
-      r.blas_root = blas_root[d->instance_mesh[i]];
-      r.material = mat0 + d->instance_material[i];
-      r.prim_offset = d->instance_primitive_offset[i];
-      r.instance_id = d->instance_id[i];
-      if (k < members)
-        for (int c = 0; c < 12; ++c) o2w[12ull * k + c] = m[c];
-    }
-    // world-space triangles of the baked instances, in packed order; the
-    // TLAS references their slots directly and hits report the identity
-    // record, whose tri_owner entries name the original instances
-    std::vector<float4> fv(3ull * flat_tris), fn(3ull * flat_tris);
-    std::vector<uint32_t> fpacked(flat_tris), fowner(flat_tris);
-    {
-      uint64_t t = 0;
-      for (uint32_t i = 0; i < ni; ++i) {
-        if (!flat[i]) continue;
-        const InstanceRec& r = inst[local_of[i]];
-        Affine mo{r.o2w0, r.o2w1, r.o2w2}, mw{r.w2o0, r.w2o1, r.w2o2};
-        const uint32_t m = d->instance_mesh[i];
-        const uint32_t v0 = d->mesh_vertex_offset[m];
-        for (uint32_t lt = 0; lt < mesh_tris(m); ++lt, ++t) {
-          for (int c = 0; c < 3; ++c) {
-            uint32_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
-            float3 p = xform_point(mo, make_float3(d->vertices[3ull * vi], d->vertices[3ull * vi + 1],
-                                                   d->vertices[3ull * vi + 2]));
-            float3 nn = normalize(xform_normal_by_inverse(
-                mw, make_float3(d->normals[3ull * vi], d->normals[3ull * vi + 1], d->normals[3ull * vi + 2])));
-            fv[3 * t + c] = make_float4(p.x, p.y, p.z, 0.0f);
-            fn[3 * t + c] = make_float4(nn.x, nn.y, nn.z, 0.0f);
-          }
-          fpacked[t] = r.prim_offset + lt;
-          fowner[t] = inst0 + local_of[i];
-        }
-      }
-    }
-    upload_to(tri_verts + 3ull * flat_slot0, fv.data(), fv.size(), st);
-    upload_to(tri_normals + 3ull * flat_slot0, fn.data(), fn.size(), st);
-    upload_to(tri_index + flat_slot0, fpacked.data(), fpacked.size(), st);
-    upload_to(tri_owner + flat_slot0, fowner.data(), fowner.size(), st);
-    upload_to(ctx->instances.at<InstanceRec>(0, inst0), inst.data(), inst.size(), st);
-
-    // ---- TLAS over the member instances and the baked triangles
-    std::vector<uint2> ranges(std::max<uint32_t>(members, 1));
-    for (uint32_t k = 0; k < members; ++k) {
-      const uint32_t m = d->instance_mesh[order[k]];
-      ranges[k] = make_uint2(slot0 + d->mesh_triangle_offset[m], slot0 + d->mesh_triangle_offset[m + 1]);
-    }
-    DeviceBuffer d_o2w, d_ranges;
-    upload(d_o2w, o2w.data(), o2w.size(), st, staging);
-    upload(d_ranges, ranges.data(), members, st, staging);
-    const uint32_t tlas_root =
-        build_tlas(d_o2w.as<float>(), d_ranges.as<uint2>(), members, inst0, tri_verts, tri_verts + 3ull * flat_slot0,
-                   (uint32_t)flat_tris, flat_slot0, ctx->scratch, nodes, node0 + tlas_local, st);
-
-    // ---- materials, emitters, lights
-    std::vector<MaterialRec> mats(d->num_materials);
-    std::vector<MaterialAux> aux(d->num_materials);
-    for (uint32_t k = 0; k < d->num_materials; ++k) {
-      const float* p = d->materials + 16ull * k;
-      mats[k].base_rough = make_float4(p[0], p[1], p[2], p[3]);
-      mats[k].emit_metal = make_float4(p[4], p[5], p[6], p[7]);
-      aux[k].two_sided = p[8] > 0.5f ? 1u : 0u;
-      uint32_t mid;
-      std::memcpy(&mid, &p[9], 4);
-      aux[k].material_id = mid;
-      aux[k].pad0 = aux[k].pad1 = 0;
-    }
-    upload_to(ctx->materials.at<MaterialRec>(0, mat0), mats.data(), mats.size(), st);
-    upload_to(ctx->materials.at<MaterialAux>(1, mat0), aux.data(), aux.size(), st);
-    std::vector<EmitterRec> em;
-    std::vector<AliasEntry> alias;
-    build_emitters(d, em, alias);
-    upload_to(ctx->emitters.at<EmitterRec>(0, rs.emitters.off), em.data(), em.size(), st);
-    upload_to(ctx->emitters.at<AliasEntry>(1, rs.emitters.off), alias.data(), alias.size(), st);
-    if (d->num_lights && !d->lights) throw Error(OLC_ERR_VALUE, "light records are required");
-    upload_to(ctx->lights.at<LightRec>(0, rs.lights.off), reinterpret_cast<const LightRec*>(d->lights),
-              d->num_lights, st);
     uint64_t own = 0;
-    size_t env_count =
-        d->environment_kind == OLC_ENV_EQUIRECT ? 3ull * d->environment_width * d->environment_height : 0;
-    upload(rs.env_image, d->environment_image, env_count, st, own);
-    size_t vol_count = d->volume_present ? (size_t)d->volume_dims[0] * d->volume_dims[1] * d->volume_dims[2] : 0;
-    if (d->volume_present && (!d->volume_density || vol_count == 0))
-      throw Error(OLC_ERR_VALUE, "a volume needs a density grid");
-    upload(rs.volume, d->volume_density, vol_count, st, own);
-    OLC_CUDA(cudaStreamSynchronize(st));  // host staging vectors go out of scope
+    write_scene_records(ctx, d, rs, own);
 
-    SceneRec& v = rs.rec;
-    std::memset(&v, 0, sizeof(v));
-    v.tlas_root = tlas_root;
-    v.emitter_base = (uint32_t)rs.emitters.off;
-    v.num_emitters = d->num_emitters;
-    v.emissive_weight = d->emissive_weight;
-    v.light_base = (uint32_t)rs.lights.off;
-    v.num_lights = d->num_lights;
-    v.env_kind = d->environment_kind;
-    v.env_rotation = d->environment_rotation;
-    v.env_color = make_float4(d->environment_color[0], d->environment_color[1], d->environment_color[2], 0.0f);
-    v.env_image = rs.env_image.as<float>();
-    v.env_w = d->environment_width;
-    v.env_h = d->environment_height;
-    v.volume = rs.volume.as<float>();
-    v.volume_present = d->volume_present;
-    v.vol_nx = d->volume_dims[0];
-    v.vol_ny = d->volume_dims[1];
-    v.vol_nz = d->volume_dims[2];
-    const float* vb = d->volume_world_to_box;
-    v.vol_w2b0 = make_float4(vb[0], vb[1], vb[2], vb[3]);
-    v.vol_w2b1 = make_float4(vb[4], vb[5], vb[6], vb[7]);
-    v.vol_w2b2 = make_float4(vb[8], vb[9], vb[10], vb[11]);
-    v.vol_sigma_t_scale = d->volume_sigma_t_scale;
-    v.vol_albedo = d->volume_albedo;
-    v.vol_max_density = d->volume_max_density;
-
-    rs.triangles = total_t;
+    rs.triangles = L.total_t;
     rs.blas_count = (uint32_t)rs.blas_ranges.size();
-    rs.blas_nodes = tlas_local;
-    rs.tlas_nodes = tlas_nodes;
-    rs.flattened = flat_count;
+    rs.blas_nodes = L.tlas_local;
+    rs.tlas_nodes = L.tlas_nodes;
+    rs.flattened = L.flat_count;
     rs.bytes = ctx->nodes.range_bytes(rs.nodes) + ctx->slots.range_bytes(rs.slots) +
                ctx->instances.range_bytes(rs.instances) + ctx->materials.range_bytes(rs.materials) +
                ctx->emitters.range_bytes(rs.emitters) + ctx->lights.range_bytes(rs.lights) + own;
@@ -760,6 +831,85 @@ void build_scene(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs) {
     release_scene_ranges(ctx, rs);
     throw;
   }
+}
+
+// Update a resident scene in place from a description with the same layout
+// (_try_update_window_scene, ordinarylight/targets/vulkan/core.py:4696-4868):
+// the flagged meshes get their triangle slots rewritten and their BLAS
+// refit (_refit_scene_blases, targets/vulkan/scene.py:1217-1281); records,
+// baked triangles, the TLAS (_rebuild_scene_tlas, scene.py:1299-1330),
+// materials, emitters, lights, environment and volume are rewritten.  A
+// material, emitter or light table of another length moves to a new pool
+// range (a pool growth then invalidates the captured graphs).  Returns
+// false, with nothing changed, when the layout differs.
+bool update_scene(olc_context* ctx, ResidentScene& rs, const olc_scene_desc* d, const uint8_t* mesh_changed,
+                  uint32_t* refitted) {
+  auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t st = ctx->stream;
+  check_scene_desc(d);
+  const SceneLayout L = plan_scene(ctx, d);
+  if (!same_layout(L, rs.layout)) return false;
+  const uint32_t env_old = rs.rec.env_kind == OLC_ENV_EQUIRECT ? 3u * rs.rec.env_w * rs.rec.env_h : 0u;
+  const uint32_t env_new =
+      d->environment_kind == OLC_ENV_EQUIRECT ? 3u * d->environment_width * d->environment_height : 0u;
+  if (env_old != env_new) return false;
+  OLC_CUDA(cudaStreamSynchronize(st));  // no run reads the scene while it changes
+  {
+    // new ranges first (an allocation failure leaves the scene as it was)
+    Range mats = rs.materials, ems = rs.emitters, lts = rs.lights;
+    const void* bases[3] = {ctx->materials.bufs[0].get(), ctx->emitters.bufs[0].get(), ctx->lights.bufs[0].get()};
+    try {
+      if (d->num_materials != mats.n) mats = ctx->materials.acquire(d->num_materials, st);
+      if (d->num_emitters != ems.n) ems = ctx->emitters.acquire(d->num_emitters, st);
+      if (d->num_lights != lts.n) lts = ctx->lights.acquire(d->num_lights, st);
+    } catch (...) {
+      if (mats.off != rs.materials.off || mats.n != rs.materials.n) ctx->materials.release(mats);
+      if (ems.off != rs.emitters.off || ems.n != rs.emitters.n) ctx->emitters.release(ems);
+      throw;
+    }
+    auto swap_in = [](PoolGroup& pool, Range& held, const Range& next) {
+      if (next.off == held.off && next.n == held.n) return;
+      pool.release(held);
+      held = next;
+    };
+    swap_in(ctx->materials, rs.materials, mats);
+    swap_in(ctx->emitters, rs.emitters, ems);
+    swap_in(ctx->lights, rs.lights, lts);
+    if (bases[0] != ctx->materials.bufs[0].get() || bases[1] != ctx->emitters.bufs[0].get() ||
+        bases[2] != ctx->lights.bufs[0].get())
+      drop_graphs(ctx);
+  }
+  const uint32_t slot0 = (uint32_t)rs.slots.off, node0 = (uint32_t)rs.nodes.off;
+  BvhNode* nodes = ctx->nodes.at<BvhNode>(0);
+  float4* tri_verts = ctx->slots.at<float4>(0);
+  float4* tri_normals = ctx->slots.at<float4>(1);
+  const uint32_t* tri_index = ctx->slots.at<uint32_t>(2);
+  uint32_t count = 0;
+  bool any = false;
+  for (uint32_t m = 0; m < L.nm; ++m) any = any || (L.mesh_used[m] && (!mesh_changed || mesh_changed[m]));
+  if (any) {
+    uint64_t staging = 0;
+    DeviceBuffer dv, dn, di;
+    upload(dv, d->vertices, 3ull * L.total_v, st, staging);
+    upload(dn, d->normals, 3ull * L.total_v, st, staging);
+    upload(di, d->indices, 3ull * L.total_t, st, staging);
+    for (uint32_t m = 0; m < L.nm; ++m) {
+      if (!L.mesh_used[m] || (mesh_changed && !mesh_changed[m])) continue;
+      const BlasDesc bd = mesh_blas_desc(d, m, dv, dn, di);
+      refit_blas(bd, ctx->scratch, nodes, node0 + L.node_local[m], blas_node_count(bd.num_triangles), tri_verts,
+                 tri_normals, tri_index, slot0 + d->mesh_triangle_offset[m], st);
+      ++count;
+    }
+    OLC_CUDA(cudaStreamSynchronize(st));
+  }
+  uint64_t own = 0;
+  write_scene_records(ctx, d, rs, own);
+  rs.bytes = ctx->nodes.range_bytes(rs.nodes) + ctx->slots.range_bytes(rs.slots) +
+             ctx->instances.range_bytes(rs.instances) + ctx->materials.range_bytes(rs.materials) +
+             ctx->emitters.range_bytes(rs.emitters) + ctx->lights.range_bytes(rs.lights) + own;
+  if (refitted) *refitted = count;
+  rs.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return true;
 }
 
 // Upload the scene table (one SceneRec per handle).
@@ -1506,6 +1656,27 @@ int olc_add_scene(olc_context* ctx, const olc_scene_desc* scene, uint32_t* handl
 int olc_remove_scene(olc_context* ctx, uint32_t handle) {
   if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
   return guarded(ctx, [&] { remove_scene(ctx, handle); });
+}
+
+int olc_update_scene(olc_context* ctx, uint32_t handle, const olc_scene_desc* scene, const uint8_t* mesh_changed,
+                     int32_t* applied, uint32_t* refitted) {
+  if (!ctx || !applied) return fail(ctx, OLC_ERR_VALUE, "context and applied output are required");
+  return guarded(ctx, [&] {
+    *applied = 0;
+    if (refitted) *refitted = 0;
+    if (handle == OLC_DEFAULT_SCENE) {
+      if (ctx->default_scene == kNoScene) throw Error(OLC_ERR_RUNTIME, "no scene is resident; upload a scene first");
+      handle = ctx->default_scene;
+    }
+    if (handle >= ctx->scenes.size() || !ctx->scenes[handle]) throw Error(OLC_ERR_VALUE, "unknown scene handle");
+    for (const auto& j : ctx->served)
+      if (j->rec.scene == handle) throw Error(OLC_ERR_RUNTIME, "a queued job still renders this scene");
+    ResidentScene& rs = *ctx->scenes[handle];
+    if (!update_scene(ctx, rs, scene, mesh_changed, refitted)) return;
+    sync_scene_table(ctx);
+    if (ctx->restir.hist_scene == handle) restir_reset(ctx->restir);
+    *applied = 1;
+  });
 }
 
 int olc_scene_stats_get(const olc_context* ctx, uint32_t handle, olc_scene_stats* stats) {

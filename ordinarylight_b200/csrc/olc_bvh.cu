@@ -379,43 +379,68 @@ __global__ void k_flat_triangle_boxes(const float4* __restrict__ verts, uint32_t
 
 // Tight world box of each instance: the bounds of its BLAS's vertices after
 // the object-to-world transform (a rotated object-space box can be up to
-// sqrt(3) wider per axis than the object it holds).  One block per instance.
-__global__ void __launch_bounds__(256) k_instance_boxes(const float* __restrict__ o2w, uint32_t n,
-                                                        const uint2* __restrict__ slot_ranges,
-                                                        const float4* __restrict__ tri_verts, float4* lo, float4* hi,
-                                                        float4* centers) {
-  __shared__ float red[6][256];
-  const uint32_t i = blockIdx.x;
+// sqrt(3) wider per axis than the object it holds).  Blocks (instance, part)
+// each bound a stride of the instance's vertices and merge into per-instance
+// order-preserving integer bounds with atomics, so a single instance of
+// millions of triangles is spread over the whole GPU; min/max make the
+// result independent of the merge order.
+__global__ void __launch_bounds__(256) k_instance_box_parts(const float* __restrict__ o2w, uint32_t n,
+                                                            const uint2* __restrict__ slot_ranges,
+                                                            const float4* __restrict__ tri_verts, uint32_t* acc_mn,
+                                                            uint32_t* acc_mx) {
+  __shared__ uint32_t s[6];
+  const uint32_t i = blockIdx.x;   // instance; blockIdx.y is the part
   if (i >= n) return;
+  if (threadIdx.x < 3) s[threadIdx.x] = 0xffffffffu;
+  else if (threadIdx.x < 6) s[threadIdx.x] = 0u;
+  __syncthreads();
   Affine m;
   const float* p = o2w + 12ull * i;
   m.r0 = make_float4(p[0], p[1], p[2], p[3]);
   m.r1 = make_float4(p[4], p[5], p[6], p[7]);
   m.r2 = make_float4(p[8], p[9], p[10], p[11]);
   const uint2 range = slot_ranges[i];
-  float3 wl = f3(CUDART_INF_F, CUDART_INF_F, CUDART_INF_F), wh = -wl;
-  for (uint64_t v = 3ull * range.x + threadIdx.x; v < 3ull * range.y; v += blockDim.x) {
-    float3 w = xform_point(m, f3(tri_verts[v]));
-    wl = fminf3(wl, w);
-    wh = fmaxf3(wh, w);
+  uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+  const uint64_t stride = (uint64_t)gridDim.y * blockDim.x;
+  for (uint64_t v = 3ull * range.x + (uint64_t)blockIdx.y * blockDim.x + threadIdx.x; v < 3ull * range.y; v += stride) {
+    const float3 w = xform_point(m, f3(tri_verts[v]));
+    const uint32_t o[3] = {f2ord(w.x), f2ord(w.y), f2ord(w.z)};
+    for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], o[k]); mx[k] = max(mx[k], o[k]); }
   }
-  red[0][threadIdx.x] = wl.x;
-  red[1][threadIdx.x] = wl.y;
-  red[2][threadIdx.x] = wl.z;
-  red[3][threadIdx.x] = wh.x;
-  red[4][threadIdx.x] = wh.y;
-  red[5][threadIdx.x] = wh.z;
-  __syncthreads();
-  for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = fminf(red[k][threadIdx.x], red[k][threadIdx.x + s]);
-      for (int k = 3; k < 6; ++k) red[k][threadIdx.x] = fmaxf(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+  for (int k = 0; k < 3; ++k) {
+    for (int off = 16; off > 0; off >>= 1) {
+      mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], off));
+      mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], off));
     }
-    __syncthreads();
   }
-  if (threadIdx.x != 0) return;
-  wl = f3(red[0][0], red[1][0], red[2][0]);
-  wh = f3(red[3][0], red[4][0], red[5][0]);
+  if ((threadIdx.x & 31u) == 0u)
+    for (int k = 0; k < 3; ++k) { atomicMin(&s[k], mn[k]); atomicMax(&s[3 + k], mx[k]); }
+  __syncthreads();
+  if (threadIdx.x < 3) atomicMin(&acc_mn[3ull * i + threadIdx.x], s[threadIdx.x]);
+  else if (threadIdx.x < 6) atomicMax(&acc_mx[3ull * i + threadIdx.x - 3], s[threadIdx.x]);
+}
+
+__global__ void k_instance_box_init(uint32_t n, uint32_t* acc_mn, uint32_t* acc_mx) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3u * n) return;
+  acc_mn[i] = 0xffffffffu;
+  acc_mx[i] = 0u;
+}
+
+__global__ void k_instance_box_finish(uint32_t n, const uint32_t* __restrict__ acc_mn,
+                                      const uint32_t* __restrict__ acc_mx, float4* lo, float4* hi, float4* centers) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t* a = acc_mn + 3ull * i;
+  const uint32_t* b = acc_mx + 3ull * i;
+  float3 wl, wh;
+  if (a[0] > b[0]) {  // no vertices
+    wl = f3(CUDART_INF_F, CUDART_INF_F, CUDART_INF_F);
+    wh = -wl;
+  } else {
+    wl = f3(ord2f(a[0]), ord2f(a[1]), ord2f(a[2]));
+    wh = f3(ord2f(b[0]), ord2f(b[1]), ord2f(b[2]));
+  }
   // Pad by a relative epsilon: the traversal transforms the ray, not the
   // vertices, so its hit points are not bit-identical to these.
   float mag = fmaxf(fmaxf(max3(fmaxf3(wh, -wl)), max3(wh - wl)), 1e-3f);
@@ -572,6 +597,128 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
   return root;
 }
 
+// ---- refit: new triangle positions under an unchanged hierarchy ----------
+
+// Rewrite the triangle slots of one BLAS from new mesh arrays.  Slot order
+// (and so every leaf) stays; tri_index maps a slot to its mesh triangle.
+__global__ void k_refresh_slots(const float* __restrict__ vertices, const float* __restrict__ normals,
+                                const uint32_t* __restrict__ indices, uint32_t nt, float4* tri_verts,
+                                float4* tri_normals, const uint32_t* __restrict__ tri_index, uint32_t slot_base) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nt) return;
+  const uint32_t dst = slot_base + s;
+  const uint32_t t = tri_index[dst];
+  for (int k = 0; k < 3; ++k) {
+    uint32_t vi = indices[3 * t + k];
+    tri_verts[3ull * dst + k] = make_float4(vertices[3 * vi + 0], vertices[3 * vi + 1], vertices[3 * vi + 2], 0.0f);
+    tri_normals[3ull * dst + k] = make_float4(normals[3 * vi + 0], normals[3 * vi + 1], normals[3 * vi + 2], 0.0f);
+  }
+}
+
+__global__ void k_refit_init(uint32_t count, int* parent, uint32_t* done) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  parent[i] = -1;
+  done[i] = 0u;
+}
+
+// Parent of every internal node and how many internal children each node
+// waits for.  Nodes inside subtrees that the build collapsed into leaves are
+// unreachable; they get refit too, harmlessly.
+__global__ void k_refit_links(const BvhNode* __restrict__ nodes, uint32_t node_base, uint32_t count, int* parent,
+                              uint32_t* pending) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int4 d = nodes[node_base + i].d;
+  uint32_t internal = 0;
+  for (int c : {d.x, d.y})
+    if (c >= 0 && (uint32_t)c - node_base < count) {
+      parent[(uint32_t)c - node_base] = (int)i;
+      ++internal;
+    }
+  pending[i] = internal;
+}
+
+OLC_D void slot_range_box(const float4* tri_verts, int ref, float3& lo, float3& hi) {
+  lo = make_float3(CUDART_INF_F, CUDART_INF_F, CUDART_INF_F);
+  hi = make_float3(-CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F);
+  if (ref == OLC_EMPTY_CHILD) return;
+  const uint32_t first = olc_leaf_first(ref), n = olc_leaf_count(ref);
+  for (uint32_t k = 0; k < n; ++k)
+    for (int v = 0; v < 3; ++v) {
+      const float3 p = f3(tri_verts[3ull * (first + k) + v]);
+      lo = fminf3(lo, p);
+      hi = fmaxf3(hi, p);
+    }
+}
+
+// Union of a node's two child boxes (its own box).
+OLC_D void node_box(const BvhNode& n, float3& lo, float3& hi) {
+  lo = make_float3(fminf(n.a.x, n.b.x), fminf(n.a.z, n.b.z), fminf(n.c.x, n.c.z));
+  hi = make_float3(fmaxf(n.a.y, n.b.y), fmaxf(n.a.w, n.b.w), fmaxf(n.c.y, n.c.w));
+}
+
+// Bottom-up box pass: a thread starts at each node without internal
+// children and climbs while it is the last child to finish (Karras 2012's
+// atomic-counter traversal).  Boxes are min/max over the same vertices as at
+// build time, so refitting unchanged geometry reproduces the built nodes.
+__global__ void k_refit_up(BvhNode* nodes, uint32_t node_base, uint32_t count, const float4* __restrict__ tri_verts,
+                           const int* __restrict__ parent, const uint32_t* __restrict__ pending, uint32_t* done) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count || pending[i] != 0u) return;
+  uint32_t n = i;
+  for (uint32_t guard = 0; guard < count; ++guard) {
+    BvhNode* nd = nodes + node_base + n;
+    const int4 d = nd->d;
+    float3 lo[2], hi[2];
+    const int ref[2] = {d.x, d.y};
+    for (int c = 0; c < 2; ++c) {
+      if (ref[c] >= 0 && (uint32_t)ref[c] - node_base < count) {
+        const float4* cp = reinterpret_cast<const float4*>(nodes + ref[c]);
+        BvhNode child;
+        child.a = __ldcg(cp + 0);
+        child.b = __ldcg(cp + 1);
+        child.c = __ldcg(cp + 2);
+        node_box(child, lo[c], hi[c]);
+      } else {
+        slot_range_box(tri_verts, ref[c], lo[c], hi[c]);
+      }
+    }
+    nd->a = make_float4(lo[0].x, hi[0].x, lo[0].y, hi[0].y);
+    nd->b = make_float4(lo[1].x, hi[1].x, lo[1].y, hi[1].y);
+    nd->c = make_float4(lo[0].z, hi[0].z, lo[1].z, hi[1].z);
+    const int p = parent[n];
+    if (p < 0) return;
+    __threadfence();
+    const uint32_t before = atomicAdd(&done[p], 1u);
+    if (before + 1u < pending[p]) return;
+    __threadfence();
+    n = (uint32_t)p;
+  }
+}
+
+void refit_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_t node_base, uint32_t node_count,
+                float4* tri_verts, float4* tri_normals, const uint32_t* tri_index, uint32_t slot_base,
+                cudaStream_t stream) {
+  const uint32_t n = d.num_triangles;
+  if (n > 0) {
+    k_refresh_slots<<<blocks_for(n), kThreads, 0, stream>>>(d.vertices, d.normals, d.indices, n, tri_verts,
+                                                              tri_normals, tri_index, slot_base);
+    OLC_LAUNCH_CHECK("k_refresh_slots");
+  }
+  sc.ensure(std::max<uint32_t>(node_count, 1u));
+  int* parent = sc.parent.as<int>();
+  uint32_t* pending = sc.first.as<uint32_t>();
+  uint32_t* done = sc.flags.as<uint32_t>();
+  k_refit_init<<<blocks_for(node_count), kThreads, 0, stream>>>(node_count, parent, done);
+  OLC_LAUNCH_CHECK("k_refit_init");
+  k_refit_links<<<blocks_for(node_count), kThreads, 0, stream>>>(nodes, node_base, node_count, parent, pending);
+  OLC_LAUNCH_CHECK("k_refit_links");
+  k_refit_up<<<blocks_for(node_count), kThreads, 0, stream>>>(nodes, node_base, node_count, tri_verts, parent,
+                                                                pending, done);
+  OLC_LAUNCH_CHECK("k_refit_up");
+}
+
 // Large primitives (an instance or baked triangle whose box spans more than
 // a quarter of the scene along some axis, such as a ground plane) make every
 // ancestor in a Morton-ordered hierarchy as large as themselves, so most rays
@@ -581,15 +728,27 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
 constexpr float kLargeFraction = 0.25f;
 constexpr uint32_t kHoistMaxPrims = 1u << 20;   // above this, one LBVH (no host pass)
 
-uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint32_t instance_base,
-                    const float4* tri_verts, const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base,
-                    BuildScratch& sc, BvhNode* nodes, uint32_t node_base, cudaStream_t stream) {
+uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint32_t max_instance_triangles,
+                    uint32_t instance_base, const float4* tri_verts, const float4* flat_verts, uint32_t n_flat,
+                    uint32_t flat_slot_base, BuildScratch& sc, BvhNode* nodes, uint32_t node_base,
+                    cudaStream_t stream) {
   const uint32_t total = n + n_flat;
   sc.ensure(std::max<uint32_t>(total, 1u));
   if (n > 0) {
-    k_instance_boxes<<<n, 256, 0, stream>>>(o2w, n, slot_ranges, tri_verts, sc.boxes_lo.as<float4>(),
-                                            sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
-    OLC_LAUNCH_CHECK("k_instance_boxes");
+    // enough parts per instance for about 16 vertices per thread in the
+    // largest instance
+    const uint32_t parts =
+        std::max<uint32_t>(1u, std::min<uint32_t>(2048u, (uint32_t)((3ull * max_instance_triangles + 4095) / 4096)));
+    // 3 words per instance in each of two 16-byte-per-primitive scratch arrays
+    uint32_t* acc_mn = reinterpret_cast<uint32_t*>(sc.node_lo.get());
+    uint32_t* acc_mx = reinterpret_cast<uint32_t*>(sc.node_hi.get());
+    k_instance_box_init<<<blocks_for(3ull * n), kThreads, 0, stream>>>(n, acc_mn, acc_mx);
+    OLC_LAUNCH_CHECK("k_instance_box_init");
+    k_instance_box_parts<<<dim3(n, parts), 256, 0, stream>>>(o2w, n, slot_ranges, tri_verts, acc_mn, acc_mx);
+    OLC_LAUNCH_CHECK("k_instance_box_parts");
+    k_instance_box_finish<<<blocks_for(n), kThreads, 0, stream>>>(n, acc_mn, acc_mx, sc.boxes_lo.as<float4>(),
+                                                                    sc.boxes_hi.as<float4>(), sc.centers.as<float4>());
+    OLC_LAUNCH_CHECK("k_instance_box_finish");
   }
   if (n_flat > 0) {
     k_flat_triangle_boxes<<<blocks_for(n_flat), kThreads, 0, stream>>>(

@@ -108,16 +108,25 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& scratch, BvhNode* nodes, ui
                     uint32_t leaf_max, cudaStream_t stream);
 inline uint32_t blas_node_count(uint32_t nt) { return nt > 1 ? nt - 1 : 1; }
 
+// Refit one BLAS in place for new positions of the same triangles: rewrite
+// its slots [slot_base, +nt) from d and recompute the boxes of its
+// node_count nodes at node_base bottom-up.  The hierarchy is unchanged.
+void refit_blas(const BlasDesc& d, BuildScratch& scratch, BvhNode* nodes, uint32_t node_base, uint32_t node_count,
+                float4* tri_verts, float4* tri_normals, const uint32_t* tri_index, uint32_t slot_base,
+                cudaStream_t stream);
+
 // Build the TLAS over n instances (world boxes computed from BLAS roots) and
 // n_flat world-space triangles referenced directly (flat_verts: 3 float4 per
 // triangle, the same data as pool slots [flat_slot_base, +n_flat)).  Build
 // primitive p < n becomes an instance leaf of global instance
 // instance_base + p; p >= n a triangle leaf of global slot
 // flat_slot_base + p - n.  slot_ranges[i] = triangle slot range of instance
-// i's BLAS (its world box is the transformed bounds of those vertices).
-uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint32_t n, uint32_t instance_base,
-                    const float4* tri_verts, const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base,
-                    BuildScratch& scratch, BvhNode* nodes, uint32_t node_base, cudaStream_t stream);
+// i's BLAS (its world box is the transformed bounds of those vertices);
+// max_instance_triangles is the largest of those ranges.
+uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint32_t n,
+                    uint32_t max_instance_triangles, uint32_t instance_base, const float4* tri_verts,
+                    const float4* flat_verts, uint32_t n_flat, uint32_t flat_slot_base, BuildScratch& scratch,
+                    BvhNode* nodes, uint32_t node_base, cudaStream_t stream);
 
 // One built bottom-level structure: its root node and triangle slot range.
 struct BlasRange {

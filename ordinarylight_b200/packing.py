@@ -47,6 +47,7 @@ class PackedScene:
     environment_image: np.ndarray | None
     volume: dict | None
     total_triangles: int
+    mesh_sources: tuple = ()      # the MeshResource (or Mesh) behind each packed mesh
 
     def descriptor(self) -> _native.OlcSceneDesc:
         d = _native.OlcSceneDesc()
@@ -195,6 +196,7 @@ def _volume_record(scene):
 def pack_scene(scene) -> PackedScene:
     """Flatten a scene into the arrays of olc_scene_desc."""
     mesh_index = {}
+    sources = []
     vertices, normals, indices = [], [], []
     v_off, t_off = [0], [0]
     inst_xf, inst_mesh, inst_mat, inst_id, inst_prim = [], [], [], [], []
@@ -208,6 +210,7 @@ def pack_scene(scene) -> PackedScene:
         key = id(mesh.resource) if getattr(mesh, "resource", None) is not None else id(mesh)
         if key not in mesh_index:
             mesh_index[key] = len(v_off) - 1
+            sources.append(mesh.resource if getattr(mesh, "resource", None) is not None else mesh)
             verts = np.ascontiguousarray(mesh.vertices, np.float32).reshape(-1, 3)
             vertices.append(verts)
             n = getattr(mesh, "normals", None)
@@ -267,7 +270,40 @@ def pack_scene(scene) -> PackedScene:
         environment_image=env_img,
         volume=_volume_record(scene),
         total_triangles=prim,
+        mesh_sources=tuple(sources),
     )
+
+
+def refit_mask(old: PackedScene, new: PackedScene):
+    """Meshes to refit when ``new`` replaces ``old`` in place, or None when
+    the scene must be uploaded again.  The rules of the reference's in-place
+    update (_try_update_window_scene, ordinarylight/targets/vulkan/core.py:4696-4760):
+    the same meshes with the same topology, and new vertex positions only
+    for meshes marked ``deformable``."""
+    if (len(old.mesh_sources) != len(new.mesh_sources)
+            or any(a is not b for a, b in zip(old.mesh_sources, new.mesh_sources))
+            or not np.array_equal(old.mesh_vertex_offset, new.mesh_vertex_offset)
+            or not np.array_equal(old.mesh_triangle_offset, new.mesh_triangle_offset)
+            or not np.array_equal(old.instance_mesh, new.instance_mesh)
+            or old.environment_kind != new.environment_kind
+            or (old.environment_image is None) != (new.environment_image is None)
+            or (old.environment_image is not None and old.environment_image.shape != new.environment_image.shape)
+            or (old.volume is None) != (new.volume is None)):
+        return None
+    if old.volume is not None and np.shape(old.volume["density"]) != np.shape(new.volume["density"]):
+        return None
+    mask = np.zeros(len(new.mesh_sources), np.uint8)
+    for m, source in enumerate(new.mesh_sources):
+        v0, v1 = int(new.mesh_vertex_offset[m]), int(new.mesh_vertex_offset[m + 1])
+        t0, t1 = int(new.mesh_triangle_offset[m]), int(new.mesh_triangle_offset[m + 1])
+        if not np.array_equal(old.indices[t0:t1], new.indices[t0:t1]):
+            return None
+        moved = not np.array_equal(old.vertices[v0:v1], new.vertices[v0:v1])
+        if moved and not getattr(source, "deformable", False):
+            return None
+        if moved or not np.array_equal(old.normals[v0:v1], new.normals[v0:v1]):
+            mask[m] = 1
+    return mask
 
 
 def camera_kind(camera) -> int:

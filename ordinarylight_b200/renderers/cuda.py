@@ -34,7 +34,7 @@ import time
 import numpy as np
 
 from .. import _native
-from ..packing import pack_camera, pack_scene
+from ..packing import refit_mask, pack_camera, pack_scene
 from .base import RendererImplementation, RendererImplementationInfo
 
 _MODES = {"production": _native.MODE_PRODUCTION, "reference_compatible": _native.MODE_REFERENCE_COMPATIBLE}
@@ -183,6 +183,9 @@ class CudaWavefrontRenderer(RendererImplementation):
         self._closed = False
         self._scene_key = None
         self._packed = None
+        self._scene_obj = None
+        self.last_update = None          # what the last in-place scene update did
+        self._resident_packed = {}       # pool handle -> PackedScene it holds
         self._resident = OrderedDict()   # (id(scene), revision) -> (handle, scene)
         self._served_outputs = {}        # ticket -> output array
         self.last_timings = {}
@@ -211,11 +214,33 @@ class CudaWavefrontRenderer(RendererImplementation):
             return 0.0
         t0 = time.perf_counter()
         packed = pack_scene(scene)
-        desc = packed.descriptor()
-        _native.check(self._lib, self._ctx, self._lib.olc_upload_scene(self._ctx, ctypes.byref(desc)))
+        self.last_update = None
+        if (not force and self._packed is not None and self._scene_obj is scene
+                and self._update_in_place(_native.DEFAULT_SCENE, self._packed, packed)):
+            pass
+        else:
+            desc = packed.descriptor()
+            _native.check(self._lib, self._ctx, self._lib.olc_upload_scene(self._ctx, ctypes.byref(desc)))
         self._packed = packed
+        self._scene_obj = scene
         self._scene_key = key
         return (time.perf_counter() - t0) * 1e3
+
+    def _update_in_place(self, handle, old, new) -> bool:
+        """Refit/rewrite a resident scene for ``new`` when the reference's
+        in-place update rules allow it (see :func:`packing.refit_mask`)."""
+        mask = refit_mask(old, new)
+        if mask is None:
+            return False
+        desc = new.descriptor()
+        applied, refitted = ctypes.c_int32(), ctypes.c_uint32()
+        _native.check(self._lib, self._ctx, self._lib.olc_update_scene(
+            self._ctx, handle, ctypes.byref(desc), _native.ptr(mask) if len(mask) else None,
+            ctypes.byref(applied), ctypes.byref(refitted)))
+        if not applied.value:
+            return False
+        self.last_update = {"refitted_blas": int(refitted.value), "meshes": int(len(mask))}
+        return True
 
     def replace_scene(self, scene) -> None:
         """Make ``scene`` resident (ResidentSceneRendererProtocol,
@@ -349,12 +374,28 @@ class CudaWavefrontRenderer(RendererImplementation):
             self._resident.move_to_end(key)
             return entry[0]
         packed = pack_scene(scene)
+        self.last_update = None
+        # an older revision of the same scene is updated in place when the
+        # in-place rules allow it and no queued job still renders it
+        stale = [k for k, (_h, sc) in self._resident.items() if sc is scene]
+        for old_key in stale:
+            handle = self._resident[old_key][0]
+            try:
+                updated = self._update_in_place(handle, self._resident_packed[handle], packed)
+            except RuntimeError:
+                updated = False
+            if updated:
+                del self._resident[old_key]
+                self._resident[key] = (handle, scene)
+                self._resident_packed[handle] = packed
+                return handle
         desc = packed.descriptor()
         handle = ctypes.c_uint32()
         _native.check(self._lib, self._ctx, self._lib.olc_add_scene(self._ctx, ctypes.byref(desc),
                                                                     ctypes.byref(handle)))
         # the entry keeps the scene alive so that its id() is not reused
         self._resident[key] = (int(handle.value), scene)
+        self._resident_packed[int(handle.value)] = packed
         return int(handle.value)
 
     def release_scene(self, scene) -> None:
@@ -364,6 +405,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         entry = self._resident.pop(key, None)
         if entry is None:
             raise ValueError("scene is not resident")
+        self._resident_packed.pop(entry[0], None)
         _native.check(self._lib, self._ctx, self._lib.olc_remove_scene(self._ctx, entry[0]))
 
     def resident_scenes(self):

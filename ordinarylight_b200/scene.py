@@ -322,11 +322,14 @@ class Mesh:
     visible: bool = True
     name: str | None = None
     metadata: dict = field(default_factory=dict, repr=False)
+    deformable: bool = False
     id: int | None = field(default=None, init=False)
 
     def __post_init__(self):
         if not isinstance(self.visible, bool):
             raise TypeError("visible must be a bool")
+        if not isinstance(self.deformable, bool):
+            raise TypeError("deformable must be a bool")
         if not isinstance(self.transform, Transform):
             self.transform = Transform(self.transform)
         self.metadata = MappingProxyType(dict(self.metadata))
@@ -334,6 +337,7 @@ class Mesh:
             self.vertices = self.resource.vertices
             self.indices = self.resource.indices
             self.normals = self.resource.normals
+            self.deformable = self.resource.deformable
             return
         self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float32)
         self.indices = np.ascontiguousarray(self.indices, dtype=np.uint32)
@@ -378,9 +382,12 @@ class MeshResource:
     normals: np.ndarray | None = None
     name: str | None = None
     metadata: dict = field(default_factory=dict, repr=False)
+    deformable: bool = False      # positions may change in place (refit instead of rebuild)
     id: int | None = field(default=None, init=False)
 
     def __post_init__(self):
+        if not isinstance(self.deformable, bool):
+            raise TypeError("deformable must be a bool")
         checked = Mesh(self.vertices, self.indices, self.material, normals=self.normals)
         self.vertices = checked.vertices
         self.indices = checked.indices
@@ -531,9 +538,10 @@ class Scene:
     def visible_volumes(self):
         return tuple(volume for volume in self.volumes if volume.visible)
 
-    def create_mesh(self, vertices, indices, material=None, *, normals=None, name=None, metadata=None):
+    def create_mesh(self, vertices, indices, material=None, *, normals=None, name=None, metadata=None,
+                    deformable=False):
         resource = MeshResource(vertices, indices, material or Material(), normals=normals, name=name,
-                                metadata={} if metadata is None else metadata)
+                                metadata={} if metadata is None else metadata, deformable=deformable)
         self._attach_mesh_resource(resource)
         self.mesh_resources.append(resource)
         return resource
@@ -541,8 +549,9 @@ class Scene:
     create_mesh_resource = create_mesh
 
     def add_mesh(self, vertices, indices, material=None, *, normals=None, transform=None, name=None,
-                 metadata=None):
-        resource = self.create_mesh(vertices, indices, material, normals=normals, name=name, metadata=metadata)
+                 metadata=None, deformable=False):
+        resource = self.create_mesh(vertices, indices, material, normals=normals, name=name, metadata=metadata,
+                                    deformable=deformable)
         return self.add_instance(resource, transform=transform, name=name, metadata=metadata)
 
     def _resolve_resource(self, resource):
@@ -588,6 +597,44 @@ class Scene:
         if created:
             self._changed(geometry=True, shading=True)
         return tuple(created)
+
+    def update_mesh_resource(self, resource, *, vertices=None, indices=None, normals=None, material=None):
+        """Replace shared geometry or its default material and synchronise
+        every instance of it (scene/_core.py:1579-1636).  New positions or
+        topology without new normals regenerate the normals."""
+        resource = self._resolve_resource(resource)
+        geometry = vertices is not None or indices is not None
+        if normals is None and not geometry:
+            normals = resource.normals
+        old_material = resource.material
+        candidate = MeshResource(resource.vertices if vertices is None else vertices,
+                                 resource.indices if indices is None else indices,
+                                 resource.material if material is None else material,
+                                 normals=normals, deformable=resource.deformable)
+        resource.vertices, resource.indices, resource.normals = candidate.vertices, candidate.indices, candidate.normals
+        resource.material = candidate.material
+        for instance in self.meshes:
+            if instance.resource is not resource:
+                continue
+            instance.vertices, instance.indices, instance.normals = (candidate.vertices, candidate.indices,
+                                                                     candidate.normals)
+            if material is not None and instance.material is old_material:
+                instance.material = candidate.material
+        self._register_material(candidate.material)
+        self._changed(geometry=geometry, shading=geometry or material is not None or normals is not None)
+        return resource
+
+    def update_instance_transforms(self, instances, transforms):
+        """New transforms for several instances, one revision step
+        (scene/_core.py:1809-1811)."""
+        instances, transforms = list(instances), list(transforms)
+        if len(instances) != len(transforms):
+            raise ValueError("instances and transforms must have the same length")
+        for instance, transform in zip(instances, transforms):
+            instance.transform = transform if isinstance(transform, Transform) else Transform(transform)
+        if instances:
+            self._changed(transform=True)
+        return tuple(instances)
 
     def update_instance(self, instance, *, transform=None, material=None, visible=None):
         if transform is not None:
