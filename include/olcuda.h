@@ -406,6 +406,45 @@ OLC_API int olc_read_products(olc_context* ctx, uint32_t width, uint32_t height,
 OLC_API int olc_read_variance(olc_context* ctx, uint32_t width, uint32_t height,
                               float* variance, int out_is_device);
 
+/* World hit point (height*width*3 floats) and barycentrics (height*width*2,
+ * (u, v) in the triangle's index order) of the last olc_render's first
+ * sample's primary hits; host arrays, either may be NULL (the
+ * primary_position / primary_barycentric readback of
+ * render_wavefront_outputs, ordinarylight/targets/vulkan/api.py:1302-1397). */
+OLC_API int olc_read_hit_geometry(olc_context* ctx, uint32_t width, uint32_t height,
+                                  float* position, float* barycentric);
+
+/* Camera frame of the motion projection (_project_positions,
+ * ordinarylight/targets/vulkan/api.py:1118-1136): origin, unit forward,
+ * right and up, and tan(vertical fov / 2). */
+typedef struct olc_motion_camera {
+  double origin[3], forward[3], right[3], up[3];
+  double scale;
+} olc_motion_camera;
+
+/* One visible mesh of the current frame: its packed triangles
+ * [first, first + count) and the first packed triangle of the same mesh in
+ * the captured frame (0xffffffff: the mesh has no motion history). */
+typedef struct olc_motion_mesh {
+  uint32_t first, count, previous_first, reserved;
+} olc_motion_mesh;
+
+/* Keep the default scene's world-space triangles (packed order) as the
+ * previous frame of later olc_read_motion calls (_capture_motion_state,
+ * ordinarylight/targets/vulkan/api.py:1139-1149). */
+OLC_API int olc_capture_motion_state(olc_context* ctx);
+
+/* Motion product (height*width*2 floats, host): for each pixel whose first
+ * sample hit a triangle of a mesh with history, its projection now minus the
+ * projection under `before` of the same barycentric point of that triangle
+ * in the captured frame; 0 elsewhere (_motion_product,
+ * ordinarylight/targets/vulkan/api.py:1151-1200).  meshes are sorted by
+ * first. */
+OLC_API int olc_read_motion(olc_context* ctx, uint32_t width, uint32_t height,
+                            const olc_motion_mesh* meshes, uint32_t num_meshes,
+                            const olc_motion_camera* now, const olc_motion_camera* before,
+                            float* motion);
+
 /* Forget temporal history (Renderer.reset_sequence ->
  * reset_output_history, ordinarylight/renderer/_core.py:339-351, :447-451). */
 OLC_API int olc_reset_history(olc_context* ctx);

@@ -116,6 +116,15 @@ class OlcPoolInfo(ctypes.Structure):
     ]
 
 
+class OlcMotionCamera(ctypes.Structure):
+    _fields_ = [("origin", c_double * 3), ("forward", c_double * 3), ("right", c_double * 3), ("up", c_double * 3),
+                ("scale", c_double)]
+
+
+class OlcMotionMesh(ctypes.Structure):
+    _fields_ = [("first", c_uint32), ("count", c_uint32), ("previous_first", c_uint32), ("reserved", c_uint32)]
+
+
 class OlcJob(ctypes.Structure):
     _fields_ = [
         ("scene", c_uint32), ("width", c_uint32), ("height", c_uint32), ("samples_per_pixel", c_uint32),
@@ -154,6 +163,10 @@ _SIGNATURES = {
                     POINTER(OlcRenderStats)], c_int),
     "olc_read_products": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "olc_read_variance": ([c_void_p, c_uint32, c_uint32, c_void_p, c_int], c_int),
+    "olc_read_hit_geometry": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
+    "olc_capture_motion_state": ([c_void_p], c_int),
+    "olc_read_motion": ([c_void_p, c_uint32, c_uint32, POINTER(OlcMotionMesh), c_uint32, POINTER(OlcMotionCamera),
+                         POINTER(OlcMotionCamera), c_void_p], c_int),
     "olc_reset_history": ([c_void_p], c_int),
     "olc_trace_closest": ([c_void_p, c_uint32, c_void_p, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
                            c_void_p], c_int),

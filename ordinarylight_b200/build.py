@@ -13,7 +13,7 @@ CSRC = PACKAGE / "csrc"
 INCLUDE = PACKAGE.parent / "include"
 LIB_DIR = PACKAGE / "_lib"
 LIBRARY = LIB_DIR / "libolcuda.so"
-SOURCES = ("olc_bvh.cu", "olc_wavefront.cu", "olc_restir.cu", "olc_api.cu", "olc_noalloc.cu")
+SOURCES = ("olc_bvh.cu", "olc_wavefront.cu", "olc_restir.cu", "olc_motion.cu", "olc_api.cu", "olc_noalloc.cu")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 FLAGS = (
     "-O3", "-std=c++17", "-lineinfo",

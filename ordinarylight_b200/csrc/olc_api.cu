@@ -32,6 +32,7 @@
 
 #include "olcuda.h"
 #include "olc_internal.h"
+#include "olc_motion.h"
 #include "olc_restir.h"
 #include "olc_wavefront.h"
 
@@ -178,6 +179,8 @@ struct SceneLayout {
   uint64_t slot_count = 0;
   // what an in-place update must find unchanged
   std::vector<uint32_t> mesh_vertex_offset, mesh_triangle_offset, instance_mesh;
+  std::vector<uint32_t> instance_prim_offset;   // packed triangle base of each instance
+  uint64_t packed_triangles = 0;                // Scene.triangles() length
 };
 
 struct ResidentScene {
@@ -285,8 +288,10 @@ struct olc_context {
   DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
       ps_rad, ps_meta, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
-  DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim;
+  DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary;
   uint32_t prod_pixels = 0;
+  DeviceBuffer motion_prev;        // world-space triangles of the motion history frame (3 float4 each)
+  uint32_t motion_prev_count = 0;  // packed triangles in it; 0: none captured
   DeviceBuffer sample_lum;         // per-sample luminance of the last plain render (sample_variance)
   uint32_t lum_spp = 0;            // its samples; 0: none kept
   PoolGroup pixels{{3 * sizeof(unsigned long long), sizeof(float4)}, 1 << 16};
@@ -606,6 +611,10 @@ SceneLayout plan_scene(const olc_context* ctx, const olc_scene_desc* d) {
     L.mesh_triangle_offset.assign(d->mesh_triangle_offset, d->mesh_triangle_offset + nm + 1);
   }
   L.instance_mesh.assign(d->instance_mesh, d->instance_mesh + ni);
+  L.instance_prim_offset.assign(d->instance_primitive_offset, d->instance_primitive_offset + ni);
+  for (uint32_t i = 0; i < ni; ++i)
+    L.packed_triangles =
+        std::max<uint64_t>(L.packed_triangles, (uint64_t)d->instance_primitive_offset[i] + mesh_triangles(d, d->instance_mesh[i]));
   return L;
 }
 
@@ -1121,6 +1130,8 @@ void ensure_products(olc_context* ctx, uint32_t npix) {
   ctx->prod_inst.allocate(n * 4);
   ctx->prod_mat.allocate(n * 4);
   ctx->prod_prim.allocate(n * 4);
+  ctx->prod_pos.allocate(n * 16);
+  ctx->prod_bary.allocate(n * 8);
   ctx->prod_pixels = npix;
   drop_graphs(ctx);
 }
@@ -1192,6 +1203,8 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.prod.instance_id = ctx->prod_inst.as<uint32_t>();
   b.prod.material_id = ctx->prod_mat.as<uint32_t>();
   b.prod.primitive_id = ctx->prod_prim.as<uint32_t>();
+  b.prod.position = ctx->prod_pos.as<float4>();
+  b.prod.barycentric = ctx->prod_bary.as<float2>();
   b.cnt = ctx->counters.as<Counters>();
   b.accum = ctx->pixels.at<unsigned long long>(0);
   b.out = ctx->pixels.at<float4>(1);
@@ -1265,7 +1278,8 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
                         (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
-                        (const void*)rb.prod.primitive_id, (const void*)rb.cnt, (const void*)rb.accum,
+                        (const void*)rb.prod.primitive_id, (const void*)rb.prod.position,
+                        (const void*)rb.prod.barycentric, (const void*)rb.cnt, (const void*)rb.accum,
                         (const void*)rb.out, (const void*)rb.sample_lum, (const void*)rb.table, (const void*)ctx->cur->counters_host,
                         (const void*)ctx->cur,
                         ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_b0.get(),
@@ -1711,7 +1725,8 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
                                 &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
                                 &ctx->ps_rad, &ctx->ps_meta, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
-                                &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->sample_lum, &ctx->restir.res_a0,
+                                &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,
+                                &ctx->sample_lum, &ctx->motion_prev, &ctx->restir.res_a0,
                                 &ctx->restir.res_a1, &ctx->restir.res_b0, &ctx->restir.res_b1, &ctx->restir.hist0,
                                 &ctx->restir.hist1, &ctx->restir.selected, &ctx->restir.hit_list})
     wf += b->bytes();
@@ -2002,6 +2017,107 @@ int olc_read_variance(olc_context* ctx, uint32_t width, uint32_t height, float* 
     launch_sample_variance(ctx->ls, ctx->sample_lum.as<float>(), npix, ctx->lum_spp, dst, st);
     if (!out_is_device)
       OLC_CUDA(cudaMemcpyAsync(variance, dst, (size_t)npix * sizeof(float), cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int olc_read_hit_geometry(olc_context* ctx, uint32_t width, uint32_t height, float* position, float* barycentric) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (width != ctx->last_w || height != ctx->last_h || ctx->last_w == 0)
+      throw Error(OLC_ERR_VALUE, "products are available only for the size of the last render");
+    const size_t n = (size_t)width * height;
+    cudaStream_t st = ctx->stream;
+    std::vector<float4> pos;
+    if (position) {
+      pos.resize(n);
+      OLC_CUDA(cudaMemcpyAsync(pos.data(), ctx->prod_pos.get(), n * 16, cudaMemcpyDeviceToHost, st));
+    }
+    if (barycentric) OLC_CUDA(cudaMemcpyAsync(barycentric, ctx->prod_bary.get(), n * 8, cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < pos.size(); ++i) {
+      position[3 * i + 0] = pos[i].x;
+      position[3 * i + 1] = pos[i].y;
+      position[3 * i + 2] = pos[i].z;
+    }
+  });
+}
+
+int olc_capture_motion_state(olc_context* ctx) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    const ResidentScene& rs = default_scene(ctx);
+    const SceneLayout& L = rs.layout;
+    cudaStream_t st = ctx->stream;
+    std::vector<MotionSegment> segs;
+    std::vector<uint32_t> prefix;
+    uint32_t total = 0;
+    for (uint32_t k = 0; k < L.members; ++k) {
+      const uint32_t i = L.order[k], m = L.instance_mesh[i];
+      const uint32_t nt = L.mesh_triangle_offset[m + 1] - L.mesh_triangle_offset[m];
+      if (nt == 0) continue;
+      segs.push_back({total, (uint32_t)rs.slots.off + L.mesh_triangle_offset[m], (uint32_t)rs.instances.off + k,
+                      L.instance_prim_offset[i]});
+      prefix.push_back(total);
+      total += nt;
+    }
+    if (L.flat_tris) {
+      segs.push_back({total, (uint32_t)rs.slots.off + L.total_t, 0u, 0xffffffffu});
+      prefix.push_back(total);
+      total += (uint32_t)L.flat_tris;
+    }
+    const uint32_t packed = (uint32_t)L.packed_triangles;
+    ctx->motion_prev.ensure(std::max<size_t>((size_t)packed * 48, 48));
+    OLC_CUDA(cudaMemsetAsync(ctx->motion_prev.get(), 0, std::max<size_t>((size_t)packed * 48, 48), st));
+    DeviceBuffer d_segs, d_prefix;
+    uint64_t staging = 0;
+    upload(d_segs, segs.data(), segs.size(), st, staging);
+    upload(d_prefix, prefix.data(), prefix.size(), st, staging);
+    world_triangles(pool_view(ctx), d_segs.as<MotionSegment>(), d_prefix.as<uint32_t>(), (uint32_t)segs.size(), total,
+                    packed, ctx->motion_prev.as<float4>(), st);
+    OLC_CUDA(cudaStreamSynchronize(st));
+    ctx->motion_prev_count = packed;
+  });
+}
+
+int olc_read_motion(olc_context* ctx, uint32_t width, uint32_t height, const olc_motion_mesh* meshes,
+                    uint32_t num_meshes, const olc_motion_camera* now, const olc_motion_camera* before,
+                    float* motion) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (width != ctx->last_w || height != ctx->last_h || ctx->last_w == 0)
+      throw Error(OLC_ERR_VALUE, "products are available only for the size of the last render");
+    if (!motion || !now || !before) throw Error(OLC_ERR_VALUE, "cameras and output are required");
+    if (num_meshes && !meshes) throw Error(OLC_ERR_VALUE, "mesh table is required");
+    std::vector<MotionMesh> table(num_meshes);
+    for (uint32_t k = 0; k < num_meshes; ++k) {
+      const olc_motion_mesh& m = meshes[k];
+      if (k && m.first < meshes[k - 1].first) throw Error(OLC_ERR_VALUE, "motion meshes must be sorted by first");
+      uint32_t prev = m.previous_first;
+      if (prev != 0xffffffffu && (uint64_t)prev + m.count > ctx->motion_prev_count)
+        throw Error(OLC_ERR_VALUE, "a motion mesh lies outside the captured frame");
+      table[k] = MotionMesh{m.first, m.count, prev, 0u};
+    }
+    auto cam = [](const olc_motion_camera* c) {
+      MotionCamera r;
+      for (int k = 0; k < 3; ++k) {
+        r.origin[k] = c->origin[k];
+        r.forward[k] = c->forward[k];
+        r.right[k] = c->right[k];
+        r.up[k] = c->up[k];
+      }
+      r.scale = c->scale;
+      return r;
+    };
+    const size_t n = (size_t)width * height;
+    cudaStream_t st = ctx->stream;
+    DeviceBuffer d_table, d_out(n * sizeof(float2));
+    uint64_t staging = 0;
+    upload(d_table, table.data(), table.size(), st, staging);
+    motion_vectors(ctx->prod_prim.as<uint32_t>(), ctx->prod_pos.as<float4>(), ctx->prod_bary.as<float2>(), width,
+                   height, d_table.as<MotionMesh>(), ctx->motion_prev_count ? num_meshes : 0u,
+                   ctx->motion_prev.as<float4>(), cam(now), cam(before), d_out.as<float2>(), st);
+    OLC_CUDA(cudaMemcpyAsync(motion, d_out.get(), n * sizeof(float2), cudaMemcpyDeviceToHost, st));
     OLC_CUDA(cudaStreamSynchronize(st));
   });
 }

@@ -334,6 +334,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.instance_id[out_pixel] = 0xffffffffu;
           a.prod.material_id[out_pixel] = 0xffffffffu;
           a.prod.primitive_id[out_pixel] = 0xffffffffu;
+          a.prod.position[out_pixel] = make_float4(p.x, p.y, p.z, 0.0f);
+          a.prod.barycentric[out_pixel] = make_float2(0.0f, 0.0f);
         }
         if (next_bounce < job.max_bounces) {
           if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
@@ -366,6 +368,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.instance_id[out_pixel] = 0xffffffffu;
           a.prod.material_id[out_pixel] = 0xffffffffu;
           a.prod.primitive_id[out_pixel] = 0xffffffffu;
+          a.prod.position[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          a.prod.barycentric[out_pixel] = make_float2(0.0f, 0.0f);
         }
       } else {
         const float t = hit.x, bu = hit.y, bv = hit.z;
@@ -389,6 +393,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.instance_id[out_pixel] = orec.instance_id;
           a.prod.material_id[out_pixel] = s.material_aux[orec.material].material_id;
           a.prod.primitive_id[out_pixel] = ir.prim_offset + s.tri_index[slot];
+          a.prod.position[out_pixel] = make_float4(p.x, p.y, p.z, 0.0f);
+          a.prod.barycentric[out_pixel] = make_float2(bu, bv);
         }
         if (cpu_mode) {
           // CPU reference transport (path_tracer.py:74-87)

@@ -60,6 +60,8 @@ struct ProductPtrs {
   uint32_t* instance_id = nullptr;
   uint32_t* material_id = nullptr;
   uint32_t* primitive_id = nullptr;
+  float4* position = nullptr;      // world hit point (xyz)
+  float2* barycentric = nullptr;   // (u, v) of the hit in the triangle's index order
 };
 
 void configure_trace_kernels();

@@ -38,7 +38,7 @@ from ..packing import refit_mask, pack_camera, pack_scene
 from .base import RendererImplementation, RendererImplementationInfo
 
 _MODES = {"production": _native.MODE_PRODUCTION, "reference_compatible": _native.MODE_REFERENCE_COMPATIBLE}
-_PRODUCTS = ("color", "variance", "depth", "normal", "instance_id", "object_id", "material_id")
+_PRODUCTS = ("color", "variance", "depth", "normal", "instance_id", "object_id", "material_id", "motion")
 
 
 @dataclass(frozen=True)
@@ -186,6 +186,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         self._scene_obj = None
         self.last_update = None          # what the last in-place scene update did
         self._resident_packed = {}       # pool handle -> PackedScene it holds
+        self._output_history = None      # previous products frame of the motion output
         self._resident = OrderedDict()   # (id(scene), revision) -> (handle, scene)
         self._served_outputs = {}        # ticket -> output array
         self.last_timings = {}
@@ -353,7 +354,75 @@ class CudaWavefrontRenderer(RendererImplementation):
             self._ctx, w, h, _native.ptr(depth), _native.ptr(normal), _native.ptr(inst), _native.ptr(mat), None))
         table = {"color": color, "variance": variance, "depth": depth, "normal": normal, "instance_id": inst,
                  "object_id": inst.copy(), "material_id": mat}
+        if "motion" in requested:
+            table["motion"] = self._motion_product(scene, camera, w, h)
+            self._capture_motion_state(scene, camera, (w, h))
         return {name: table[name] for name in requested}
+
+    def hit_geometry(self, width, height):
+        """World hit points (h, w, 3) and barycentrics (h, w, 2) of the last
+        render's first-sample primary hits."""
+        pos = np.empty((int(height), int(width), 3), np.float32)
+        bary = np.empty((int(height), int(width), 2), np.float32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_hit_geometry(
+            self._ctx, int(width), int(height), _native.ptr(pos), _native.ptr(bary)))
+        return pos, bary
+
+    @staticmethod
+    def _motion_camera(camera):
+        """_project_positions' frame (api.py:1118-1136) in double precision."""
+        origin = np.asarray(camera.position, np.float64)
+        forward = np.asarray(camera.target, np.float64) - origin
+        forward /= np.linalg.norm(forward)
+        right = np.cross(forward, np.asarray(camera.up, np.float64))
+        right /= np.linalg.norm(right)
+        up = np.cross(right, forward)
+        c = _native.OlcMotionCamera()
+        for name, v in (("origin", origin), ("forward", forward), ("right", right), ("up", up)):
+            getattr(c, name)[:] = [float(x) for x in v]
+        c.scale = float(np.tan(np.radians(camera.vertical_fov_degrees) * 0.5))
+        return c
+
+    def _motion_product(self, scene, camera, width, height):
+        """Screen-space motion of the first sample's primary hits since the
+        previous motion frame (_motion_product, api.py:1151-1200): meshes
+        match by Mesh.id and need the same topology and vertex count."""
+        motion = np.zeros((height, width, 2), np.float32)
+        previous = self._output_history
+        if previous is None or previous["scene"] is not scene or previous["size"] != (width, height):
+            return motion
+        table, offset = [], 0
+        for mesh in scene.visible_meshes:
+            count = len(mesh.indices)
+            old = previous["meshes"].get(mesh.id)
+            first = 0xFFFFFFFF
+            if count and old is not None:
+                old_indices, old_vertex_count, old_first = old
+                if (old_indices.shape == mesh.indices.shape and np.array_equal(old_indices, mesh.indices)
+                        and old_vertex_count == len(mesh.vertices)):
+                    first = old_first
+            if count:
+                table.append((offset, count, first))
+            offset += count
+        meshes = (_native.OlcMotionMesh * max(len(table), 1))()
+        for k, (first, count, prev) in enumerate(table):
+            meshes[k].first, meshes[k].count, meshes[k].previous_first = first, count, prev
+        now, before = self._motion_camera(camera), self._motion_camera(previous["camera"])
+        _native.check(self._lib, self._ctx, self._lib.olc_read_motion(
+            self._ctx, width, height, meshes, len(table), ctypes.byref(now), ctypes.byref(before),
+            _native.ptr(motion)))
+        return motion
+
+    def _capture_motion_state(self, scene, camera, size):
+        """Keep this frame as the motion history (_capture_motion_state,
+        api.py:1139-1149): topology per Mesh.id on the host, world-space
+        triangles on the device."""
+        meshes, offset = {}, 0
+        for mesh in scene.visible_meshes:
+            meshes[mesh.id] = (np.array(mesh.indices, copy=True), len(mesh.vertices), offset)
+            offset += len(mesh.indices)
+        _native.check(self._lib, self._ctx, self._lib.olc_capture_motion_state(self._ctx))
+        self._output_history = {"scene": scene, "camera": camera, "size": size, "meshes": meshes}
 
     def primitive_ids(self, width, height):
         """Packed primitive index of the last render's first-sample primary hits."""
@@ -635,6 +704,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         """Forget temporal (ReSTIR) history; called by Renderer.reset_sequence
         (ordinarylight/renderer/_core.py:339-351)."""
         self._require_open()
+        self._output_history = None
         _native.check(self._lib, self._ctx, self._lib.olc_reset_history(self._ctx))
 
     reset_accumulation = reset_output_history

@@ -9,7 +9,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from oracle import pbr
+from oracle import pbr, products
 from oracle import reference_path_tracer as ref
 from ordinarylight_b200 import CudaWavefrontRenderer, scenes
 import ordinarylight_b200 as ol
@@ -170,23 +170,6 @@ def test_render_products_follow_the_primary_hits(native_library, cuda_device):
     assert set(np.unique(prods["material_id"].reshape(-1)[hit]).tolist()) <= mats
 
 
-def _reference_variance(per_sample):
-    """The variance product of render_wavefront_outputs
-    (ordinarylight/targets/vulkan/api.py:1404-1431) from per-sample images."""
-    lum_sum = lum_sq = None
-    for radiance in per_sample:
-        lum = (radiance[..., 0] * 0.2126 + radiance[..., 1] * 0.7152 + radiance[..., 2] * 0.0722).astype(np.float64)
-        if lum_sum is None:
-            lum_sum, lum_sq = lum, lum * lum
-        else:
-            lum_sum = lum_sum + lum
-            lum_sq = lum_sq + lum * lum
-    n = len(per_sample)
-    if n == 1:
-        return np.zeros(per_sample[0].shape[:2], np.float32)
-    return np.maximum((lum_sq - lum_sum * lum_sum / n) / (n - 1), 0.0).astype(np.float32)
-
-
 @pytest.mark.parametrize("restir", [False, True])
 def test_variance_product_is_the_sample_variance_of_the_samples(native_library, cuda_device, restir):
     from ordinarylight_b200.renderers.cuda import RenderRequest
@@ -200,6 +183,6 @@ def test_variance_product_is_the_sample_variance_of_the_samples(native_library, 
         one = r.render_products(scene, camera, w, h, outputs="variance", samples=1, frame_index=4)["variance"]
     var = prods["variance"]
     assert var.shape == (h, w) and var.dtype == np.float32
-    assert var.tobytes() == _reference_variance([img[..., :3] for img in per_sample]).tobytes()
+    assert var.tobytes() == products.sample_variance([img[..., :3] for img in per_sample]).tobytes()
     assert np.count_nonzero(var) > var.size // 10
     assert not one.any()

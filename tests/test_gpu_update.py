@@ -149,3 +149,35 @@ def test_pool_scene_updates_in_place(native_library, cuda_device):
         assert len(r.resident_scenes()) == 1
     with CudaWavefrontRenderer(max_bounces=4) as f:
         assert moved.tobytes() == f.render_batch([req])[0].tobytes()
+
+
+def test_motion_product_matches_the_reference_arithmetic(native_library, cuda_device):
+    from oracle import products
+
+    scene, camera, blob, inst, lights = _animated_scene(seed=8)
+    rng = np.random.default_rng(4)
+    w, h = 64, 48
+    with CudaWavefrontRenderer(max_bounces=2) as r:
+        first = r.render_products(scene, camera, w, h, outputs=("color", "motion"), samples=1, frame_index=0)
+        assert not first["motion"].any()          # no history yet
+        before = products.capture_state(scene, camera, (w, h))
+        scene.update_instance_transforms(inst[:4], _moved(inst[:4], rng))
+        scene.update_mesh_resource(blob, vertices=_deformed(np.array(blob.vertices), 0.4))
+        moved_camera = ol.PerspectiveCamera(position=(0.4, 3.2, -11.5), target=(0.1, 0.0, 0.2),
+                                            vertical_fov_degrees=45.0)
+        out = r.render_products(scene, moved_camera, w, h, outputs=("motion", "depth"), samples=1, frame_index=1)
+        prim = r.primitive_ids(w, h)
+        pos, bary = r.hit_geometry(w, h)
+        expected = products.motion_product(before, scene, moved_camera, w, h, prim, pos, bary)
+        assert out["motion"].shape == (h, w, 2) and out["motion"].dtype == np.float32
+        np.testing.assert_allclose(out["motion"], expected, atol=2e-3, rtol=0)
+        assert np.count_nonzero(np.abs(expected).max(axis=-1) > 0.05) > w * h // 10
+        hit = prim != 0xFFFFFFFF
+        np.testing.assert_allclose(np.linalg.norm(pos[hit] - np.array(moved_camera.position, np.float32), axis=-1),
+                                   out["depth"][hit] * np.linalg.norm(
+                                       np.asarray(r.camera_rays(moved_camera, w, h, sample=0, frame_index=1)[1])
+                                       .reshape(h, w, 3)[hit], axis=-1), rtol=1e-4)
+        # a reset forgets the history
+        r.reset_output_history()
+        again = r.render_products(scene, moved_camera, w, h, outputs="motion", samples=1, frame_index=2)
+        assert not again["motion"].any()
