@@ -148,7 +148,7 @@ typedef struct olc_scene_desc {
   const uint32_t* instance_primitive_offset; /* [num_instances] packed base */
   /* materials: 16 floats each:
    * base_color.rgb, roughness, emission.rgb, metallic, emission_two_sided,
-   * material_id (as float bits), 6 reserved */
+   * material_id (as float bits), transmission, ior, 4 reserved */
   uint32_t num_materials;
   const float* materials;
   /* emissive triangles, 20 floats each, the layout of

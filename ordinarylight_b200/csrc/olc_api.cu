@@ -286,7 +286,7 @@ struct olc_context {
   // wavefront buffers
   uint32_t capacity = 0;
   DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
-      ps_rad, ps_meta, sort_keys, sort_bins;
+      ps_rad, ps_meta, ps_ior, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary;
   uint32_t prod_pixels = 0;
@@ -717,7 +717,11 @@ void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScen
     uint32_t mid;
     std::memcpy(&mid, &p[9], 4);
     aux[k].material_id = mid;
-    aux[k].pad0 = aux[k].pad1 = 0;
+    if (!(p[10] >= 0.0f && p[10] <= 1.0f)) throw Error(OLC_ERR_VALUE, "material transmission must be in [0, 1]");
+    if (p[10] > 0.001f && !(p[11] > 0.0f && std::isfinite(p[11])))
+      throw Error(OLC_ERR_VALUE, "a transmissive material needs a positive index of refraction");
+    aux[k].transmission = p[10];
+    aux[k].ior = p[11];
   }
   upload_to(ctx->materials.at<MaterialRec>(0, mat0), mats.data(), mats.size(), st);
   upload_to(ctx->materials.at<MaterialAux>(1, mat0), aux.data(), aux.size(), st);
@@ -1117,6 +1121,7 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   ctx->sh_c.allocate(c * 16);
   ctx->ps_tp.allocate(c * 16);
   ctx->ps_rad.allocate(c * 16);
+  ctx->ps_ior.allocate(c * 32);
   ctx->ps_meta.allocate(c * 16);
   ctx->capacity = capacity;
   drop_graphs(ctx);
@@ -1197,7 +1202,8 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.qc = RayQueue{ctx->q2_o.as<float4>(), ctx->q2_d.as<float4>(), ctx->q2_p.as<uint32_t>()};
   b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
   b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
-  b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>()};
+  b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>(),
+                   ctx->ps_ior.as<float4>()};
   b.prod.depth = ctx->prod_depth.as<float>();
   b.prod.normal = ctx->prod_normal.as<float4>();
   b.prod.instance_id = ctx->prod_inst.as<uint32_t>();
@@ -1276,7 +1282,7 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         ctx->sort_keys.get(), ctx->sort_bins.get(),
                         (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
                         (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
-                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.prod.depth,
+                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.prod.position,
                         (const void*)rb.prod.barycentric, (const void*)rb.cnt, (const void*)rb.accum,
@@ -1723,7 +1729,7 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
   for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p, &ctx->q2_o,
                                 &ctx->q2_d, &ctx->q2_p, &ctx->sort_keys, &ctx->sort_bins,
                                 &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
-                                &ctx->ps_rad, &ctx->ps_meta, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
+                                &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,
                                 &ctx->sample_lum, &ctx->motion_prev, &ctx->restir.res_a0,

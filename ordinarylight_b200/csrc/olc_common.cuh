@@ -171,7 +171,8 @@ struct __align__(16) MaterialRec {
 struct __align__(16) MaterialAux {
   uint32_t two_sided;
   uint32_t material_id;
-  uint32_t pad0, pad1;
+  float transmission;      // > 0.001: a dielectric interface (wavefront_shade.comp:480-505)
+  float ior;
 };
 
 // Emitter record (area light), 80 bytes: the reference's emissive-triangle
@@ -284,10 +285,16 @@ struct PathState {
   float4* throughput;      // rgb, previous BSDF pdf
   float4* radiance;        // rgb, unused
   uint4* meta;             // pixel, sample, bounce | flags << 8, job
+  float4* ior_stack;       // 2 per path: indices of refraction of the media entered, entries 1..8
 };
 
 #define OLC_PATH_FLAG_PREV_NEE 1u     // the previous vertex sampled area lights
 #define OLC_PATH_FLAG_PREV_RESTIR 2u  // area lights of the previous vertex came from ReSTIR
+// Depth of the path's medium stack minus one (the reference's medium depth,
+// metadata.w >> 8, wavefront_shade.comp:447); entry 0 is the outside, IOR 1.
+#define OLC_PATH_DEPTH_SHIFT 4u
+#define OLC_PATH_DEPTH_MASK (15u << OLC_PATH_DEPTH_SHIFT)
+#define OLC_MAX_MEDIUM_DEPTH 9u       // entry 0 plus the 8 stored ones
 
 // Fixed-point scale of the per-pixel radiance accumulator.  Sums of
 // non-negative samples in unsigned 64-bit fixed point are independent of the

@@ -97,6 +97,8 @@ struct SurfaceMat {
   float3 emission;
   float metallic;
   uint32_t two_sided;
+  float transmission;
+  float ior;
 };
 
 OLC_D float spec_probability(const SurfaceMat& m) {
@@ -195,7 +197,10 @@ OLC_D SurfaceMat load_material(const SceneView& s, uint32_t mi) {
   m.roughness = r.base_rough.w;
   m.emission = f3(r.emit_metal);
   m.metallic = r.emit_metal.w;
-  m.two_sided = s.material_aux[mi].two_sided;
+  const MaterialAux aux = s.material_aux[mi];
+  m.two_sided = aux.two_sided;
+  m.transmission = aux.transmission;
+  m.ior = aux.ior;
   return m;
 }
 

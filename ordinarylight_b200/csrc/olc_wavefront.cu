@@ -26,6 +26,27 @@ namespace {
 
 OLC_D uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Entry k of a path's medium stack (entry 0 is the outside, IOR 1).
+OLC_D float medium_ior(const float4* stack, uint32_t path, uint32_t k) {
+  if (k == 0u) return 1.0f;
+  const float4 v = stack[2ull * path + ((k - 1u) >> 2)];
+  const uint32_t c = (k - 1u) & 3u;
+  return c == 0u ? v.x : c == 1u ? v.y : c == 2u ? v.z : v.w;
+}
+OLC_D void set_medium_ior(float4* stack, uint32_t path, uint32_t k, float ior) {
+  float* v = reinterpret_cast<float*>(stack + 2ull * path + ((k - 1u) >> 2));
+  v[(k - 1u) & 3u] = ior;
+}
+
+// GLSL refract(i, n, eta): the transmitted direction for unit i and n, or
+// zero on total internal reflection.
+OLC_D float3 refract_dir(float3 i, float3 n, float eta) {
+  const float ni = dot(n, i);
+  const float k = 1.0f - eta * eta * (1.0f - ni * ni);
+  if (k < 0.0f) return f3(0.0f, 0.0f, 0.0f);
+  return i * eta - n * (eta * ni + sqrtf(k));
+}
+
 // Warp-aggregated slot reservation: one atomic per warp for all lanes that
 // want a slot (reserveOutputIndex, wavefront_shade.comp:199-213).  Must be
 // called by all 32 lanes.
@@ -314,7 +335,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
       const uint32_t out_pixel = meta.x;  // products belong to one plain frame's job
       const bool write_products = job.products && bounce == 0u && meta.y == job.sample_base && a.prod.depth;
       uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), bounce);
-      uint32_t new_flags = 0;
+      uint32_t new_flags = flags & OLC_PATH_DEPTH_MASK;   // the medium stack depth carries over
       float new_pdf = 0.0f;
       const uint32_t next_bounce = bounce + 1u;
       // ---- participating medium (production transport): a real collision
@@ -434,7 +455,32 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             }
             rad += tp * m.emission * mis;
           }
-          if (next_bounce < job.max_bounces) {
+          if (next_bounce < job.max_bounces && m.transmission > 0.001f) {
+            // ---- dielectric interface (wavefront_shade.comp:480-505): refract
+            // into or out of the medium stack, reflect on total internal
+            // reflection; no light sampling, no roulette, previous pdf kept
+            uint32_t depth = ((flags & OLC_PATH_DEPTH_MASK) >> OLC_PATH_DEPTH_SHIFT) + 1u;
+            const float current = medium_ior(a.ps.ior_stack, path, depth - 1u);
+            const float target = entering ? fmaxf(m.ior, 1.0001f) : (depth > 1u ? medium_ior(a.ps.ior_stack, path, depth - 2u) : 1.0f);
+            float3 wdir = refract_dir(d, nrm, current / target);
+            if (dot(wdir, wdir) < 0.01f) {
+              wdir = d - nrm * (2.0f * dot(nrm, d));
+            } else if (entering && depth < OLC_MAX_MEDIUM_DEPTH) {
+              set_medium_ior(a.ps.ior_stack, path, depth, target);
+              ++depth;
+            } else if (!entering && depth > 1u) {
+              --depth;
+            }
+            tp *= (f3(0.8f, 0.8f, 0.8f) + m.base * 0.2f) * m.transmission;
+            new_flags = (depth - 1u) << OLC_PATH_DEPTH_SHIFT;
+            new_pdf = tp4.w;
+            wdir = normalize(wdir);
+            if (max3(tp) > 0.0f) {
+              next_o = p + wdir * 0.002f;
+              next_d = wdir;
+              want_next = true;
+            }
+          } else if (next_bounce < job.max_bounces) {
             const float3 view = -d;
             bool did_restir = false;
             // ---- next-event estimation: one shadow ray per path per bounce

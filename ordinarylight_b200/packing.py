@@ -100,6 +100,8 @@ def _material_record(material, material_id: int) -> np.ndarray:
     rec[7] = float(getattr(material, "metallic", 0.0))
     rec[8] = 1.0 if getattr(material, "emission_two_sided", False) else 0.0
     rec[9] = np.array([material_id], np.uint32).view(np.float32)[0]
+    rec[10] = float(getattr(material, "transmission", 0.0))
+    rec[11] = float(getattr(material, "ior", 1.5))
     return rec
 
 

@@ -186,3 +186,67 @@ def test_variance_product_is_the_sample_variance_of_the_samples(native_library, 
     assert var.tobytes() == products.sample_variance([img[..., :3] for img in per_sample]).tobytes()
     assert np.count_nonzero(var) > var.size // 10
     assert not one.any()
+
+
+def _glass_cube(size, angles, center):
+    """Cube with one vertex set per face and face normals, so that shading
+    normals equal geometric ones."""
+    ax, ay = angles
+    rx = np.array([[1, 0, 0], [0, np.cos(ax), -np.sin(ax)], [0, np.sin(ax), np.cos(ax)]])
+    ry = np.array([[np.cos(ay), 0, np.sin(ay)], [0, 1, 0], [-np.sin(ay), 0, np.cos(ay)]])
+    rot = ry @ rx
+    h = size / 2.0
+    faces = []
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            n = np.zeros(3)
+            n[axis] = sign
+            u = np.zeros(3)
+            u[(axis + 1) % 3] = h
+            w = np.cross(n, u)
+            c = n * h
+            quad = [c - u - w, c + u - w, c + u + w, c - u + w]
+            faces.append((quad, n))
+    verts, norms, idx = [], [], []
+    for quad, n in faces:
+        b = len(verts)
+        verts += [rot @ q + center for q in quad]
+        norms += [rot @ n] * 4
+        idx += [(b, b + 1, b + 2), (b, b + 2, b + 3)]
+    return np.array(verts, np.float32), np.array(idx, np.uint32), np.array(norms, np.float32)
+
+
+def test_dielectric_interfaces_match_the_restated_refraction(native_library, cuda_device):
+    """Nested glass cubes (IOR 1.5 around IOR 1.25) under an equirect
+    environment: each pixel's path is deterministic (refraction, total
+    internal reflection, the medium stack), so every robust pixel must equal
+    the oracle's deterministic trace of the same camera ray."""
+    from oracle import dielectric
+
+    rng = np.random.default_rng(12)
+    scene = ol.Scene()
+    outer = dict(base_color=(0.6, 0.8, 1.0), transmission=0.9, ior=1.5, roughness=0.0)
+    inner = dict(base_color=(1.0, 0.7, 0.5), transmission=1.0, ior=1.25, roughness=0.0)
+    tri_props = []
+    for size, angles, props in ((3.0, (0.5, 0.7), outer), (1.3, (-0.3, 0.9), inner)):
+        v, i, n = _glass_cube(size, angles, np.zeros(3))
+        scene.add_mesh(v, i, ol.Material(**props), normals=n)
+        tri_props.append((v[i], props))
+    env = rng.uniform(0.05, 2.0, (16, 32, 3)).astype(np.float32)
+    scene.set_environment(ol.EnvironmentLight(image=env))
+    camera = ol.PerspectiveCamera(position=(0.3, 0.8, -7.0), target=(0.0, 0.0, 0.0), vertical_fov_degrees=35.0)
+    w, h, bounces = 96, 80, 16
+    with CudaWavefrontRenderer(max_bounces=bounces, samples_per_pixel=1, russian_roulette_start=0) as r:
+        img = r.render_frame(scene, camera, w, h, frame_index=5)
+        o, d = r.camera_rays(camera, w, h, sample=0, frame_index=5)
+    tris = np.concatenate([t for t, _ in tri_props])
+    transmission = np.concatenate([np.full(len(t), p["transmission"]) for t, p in tri_props])
+    ior = np.concatenate([np.full(len(t), p["ior"]) for t, p in tri_props])
+    base = np.concatenate([np.tile(np.asarray(p["base_color"]), (len(t), 1)) for t, p in tri_props])
+    expected, robust = dielectric.trace(np.asarray(o), np.asarray(d), tris, transmission, ior, base, env,
+                                        max_bounces=bounces)
+    got = img[..., :3].reshape(-1, 3)
+    hit_glass = np.any(np.abs(expected - dielectric.trace(np.asarray(o), np.asarray(d), tris[:0], transmission[:0],
+                                                          ior[:0], base[:0], env, max_bounces=1)[0]) > 0, axis=1)
+    assert robust.mean() > 0.9 and (robust & hit_glass).sum() > w * h // 5
+    np.testing.assert_allclose(got[robust], expected[robust], rtol=1e-4, atol=1e-6)
