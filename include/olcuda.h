@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OLC_ABI_VERSION 4
+#define OLC_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define OLC_API __attribute__((visibility("default")))
@@ -176,6 +176,22 @@ typedef struct olc_scene_desc {
   float volume_albedo;
   float volume_max_density;
   uint32_t reserved[7];
+  /* textures (num_texture_bindings = 0: an untextured scene; the rest may
+   * then be NULL) */
+  const float* texcoords;                /* [total_vertices * 4]: uv0.xy, uv1.xy */
+  const float* tangents;                 /* [total_vertices * 4]: object-space xyz, handedness */
+  uint32_t num_texture_words;
+  const uint32_t* texture_words;         /* Scene.texture_data layout: count, 8 words per
+                                            texture (sRGB offset, linear offset, width, height,
+                                            wrap/filter flags, levels, 0, 0), then RGBA8 mip
+                                            pyramids (scene/_core.py:3005-3077) */
+  uint32_t num_texture_bindings;
+  const float* texture_bindings;         /* [n * 8]: texture, cos, sin, texcoord set, offset.xy,
+                                            scale.xy (Scene.texture_binding_data) */
+  const float* material_textures;        /* [num_materials * 12]: binding of the base colour,
+                                            metallic-roughness, emissive, normal, occlusion and
+                                            transmission maps (-1: none), normal scale, occlusion
+                                            strength, uses texcoord set 1, 3 reserved */
 } olc_scene_desc;
 
 /* Camera basis computed by the caller in float32 exactly as the reference's
@@ -444,6 +460,16 @@ OLC_API int olc_read_motion(olc_context* ctx, uint32_t width, uint32_t height,
                             const olc_motion_mesh* meshes, uint32_t num_meshes,
                             const olc_motion_camera* now, const olc_motion_camera* before,
                             float* motion);
+
+/* Material texture lookups of a resident scene (handle, or
+ * OLC_DEFAULT_SCENE): for each of n points, the texture of `binding` at
+ * uv0/uv1 (host, n*2 floats each) with ray-cone footprints fp0/fp1 (n
+ * floats each), sRGB-decoded when srgb != 0, as the shading stage samples
+ * it (sampleMaterialTexture, ordinarylight/shaders/wavefront_textures.glsl:134-204);
+ * out: n*4 floats (host). */
+OLC_API int olc_sample_texture(olc_context* ctx, uint32_t handle, int32_t binding, uint32_t n,
+                               const float* uv0, const float* uv1, const float* fp0, const float* fp1,
+                               int srgb, float* out);
 
 /* Forget temporal history (Renderer.reset_sequence ->
  * reset_output_history, ordinarylight/renderer/_core.py:339-351, :447-451). */

@@ -29,7 +29,12 @@ def _normalize(v):
 
 
 def pbr_evaluate(base, roughness, metallic, n, view, out):
+    """roughness and metallic: scalars or one value per point."""
     base = np.asarray(base, np.float64)
+    roughness = np.asarray(roughness, np.float64)
+    metallic = np.asarray(metallic, np.float64)
+    if metallic.ndim:
+        metallic = metallic[..., None]
     n, view, out = _normalize(n), _normalize(view), _normalize(out)
     nv = np.maximum(np.sum(n * view, -1), 0.0)
     nl = np.maximum(np.sum(n * out, -1), 0.0)
@@ -39,7 +44,7 @@ def pbr_evaluate(base, roughness, metallic, n, view, out):
     f0 = 0.04 + (base - 0.04) * metallic
     w = (1.0 - np.clip(vh, 0.0, 1.0)) ** 5
     F = f0 + (1.0 - f0) * w[..., None]
-    a = max(roughness * roughness, 0.0009)
+    a = np.maximum(roughness * roughness, 0.0009)
     a2 = a * a
     den = nh * nh * (a2 - 1.0) + 1.0
     D = a2 / np.maximum(PI * den * den, 1e-6)

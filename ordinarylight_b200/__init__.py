@@ -6,16 +6,18 @@ Public surface:
   ``renderers.cuda`` RendererImplementation (sm_100a kernels via the C ABI of
   ``libolcuda.so``, declared in ``include/olcuda.h``);
 * :class:`Renderer` — the renderer-neutral facade (``renderer_preference="cuda"``);
-* the scene model mirror (``Scene``, ``Material``, ``Transform``, cameras,
-  lights) for use without the reference package;
-* :mod:`ordinarylight_b200.batch` and :mod:`ordinarylight_b200.serve` — the
-  batched and served forms of the same path.
+* the scene model mirror (``Scene``, ``Material``, ``Texture``,
+  ``Transform``, cameras, lights) for use without the reference package;
+* ``CudaWavefrontRenderer.render_batch`` / ``submit`` / ``serve_step`` and
+  :mod:`ordinarylight_b200.serving` — the batched and served forms of the
+  same path; :mod:`ordinarylight_b200.autotune` and
+  :mod:`ordinarylight_b200.distributed` around them.
 """
 
 from .scene import (  # noqa: F401
     CAMERA_TYPES, LIGHT_TYPES, DirectionalLight, EnvironmentLight, Instance, Material, Mesh, MeshResource,
-    OrthographicCamera, PanoramicCamera, PerspectiveCamera, PointLight, Scene, SpotLight, Transform, Volume,
-    VolumeMaterial,
+    OrthographicCamera, PanoramicCamera, PerspectiveCamera, PointLight, Scene, SpotLight, Texture, TextureTransform,
+    Transform, Volume, VolumeMaterial,
 )
 from .renderer import Renderer, RenderJob, RenderStatistics, install_cuda_preference  # noqa: F401
 from .renderers.cuda import CudaRendererConfig, CudaWavefrontRenderer  # noqa: F401

@@ -65,6 +65,8 @@ class OlcSceneDesc(ctypes.Structure):
         ("volume_present", c_uint32), ("volume_dims", c_uint32 * 3), ("volume_density", _f32p),
         ("volume_world_to_box", c_float * 12), ("volume_sigma_t_scale", c_float), ("volume_albedo", c_float),
         ("volume_max_density", c_float), ("reserved", c_uint32 * 7),
+        ("texcoords", _f32p), ("tangents", _f32p), ("num_texture_words", c_uint32), ("texture_words", _u32p),
+        ("num_texture_bindings", c_uint32), ("texture_bindings", _f32p), ("material_textures", _f32p),
     ]
 
 
@@ -165,6 +167,8 @@ _SIGNATURES = {
     "olc_read_variance": ([c_void_p, c_uint32, c_uint32, c_void_p, c_int], c_int),
     "olc_read_hit_geometry": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
     "olc_capture_motion_state": ([c_void_p], c_int),
+    "olc_sample_texture": ([c_void_p, c_uint32, c_int32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                            c_void_p], c_int),
     "olc_read_motion": ([c_void_p, c_uint32, c_uint32, POINTER(OlcMotionMesh), c_uint32, POINTER(OlcMotionCamera),
                          POINTER(OlcMotionCamera), c_void_p], c_int),
     "olc_reset_history": ([c_void_p], c_int),

@@ -186,6 +186,7 @@ struct SceneLayout {
 struct ResidentScene {
   Range nodes, slots, instances, materials, emitters, lights;
   DeviceBuffer env_image, volume;
+  DeviceBuffer tex_words, tex_bindings, tex_attr, mat_tex;   // textured scenes only
   SceneRec rec{};
   SceneLayout layout;
   std::vector<BlasRange> blas_ranges;
@@ -209,6 +210,7 @@ struct QueuedJob {
   // ReSTIR reservoirs at job-local indices (reservoir_base 0), where the next
   // plain frame's temporal pass finds them; otherwise chunk-local ones
   bool job_local_reservoirs = false;
+  bool textured = false;     // its scene has textures (the run uses the textured kernels)
   uint32_t age = 0;          // serving steps since it was queued
 };
 
@@ -225,6 +227,7 @@ struct RunPlan {
   uint32_t max_segments = 0;
   uint32_t max_count = 0;
   bool restir = false;               // some chunk runs ReSTIR
+  bool textures = false;             // some job's scene has textures
   bool chunk_reservoirs = false;     // some ReSTIR segment uses chunk-local reservoirs
 };
 
@@ -286,10 +289,11 @@ struct olc_context {
   // wavefront buffers
   uint32_t capacity = 0;
   DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
-      ps_rad, ps_meta, ps_ior, sort_keys, sort_bins;
+      ps_rad, ps_meta, ps_ior, ps_cone, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary;
   uint32_t prod_pixels = 0;
+  DeviceBuffer srgb_lut;           // 256 sRGB-to-linear values for texture decoding
   DeviceBuffer motion_prev;        // world-space triangles of the motion history frame (3 float4 each)
   uint32_t motion_prev_count = 0;  // packed triangles in it; 0: none captured
   DeviceBuffer sample_lum;         // per-sample luminance of the last plain render (sample_variance)
@@ -623,6 +627,116 @@ bool same_layout(const SceneLayout& a, const SceneLayout& b) {
          a.mesh_triangle_offset == b.mesh_triangle_offset && a.instance_mesh == b.instance_mesh;
 }
 
+// Texture data of a scene: the texture words, bindings, per-material binding
+// records and per-slot vertex attributes (texcoords, tangents), validated
+// so that no device lookup can leave its array.  Member instances' slots
+// take their corners from the mesh arrays in BLAS slot order; baked
+// triangles get texcoords and world-space tangents (Mesh.world_tangents,
+// scene/_core.py:702-714) in packed order.
+void write_textures(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs, uint64_t& own) {
+  for (DeviceBuffer* b : {&rs.tex_words, &rs.tex_bindings, &rs.tex_attr, &rs.mat_tex}) b->release();
+  if (d->num_texture_bindings == 0) return;
+  cudaStream_t st = ctx->stream;
+  const SceneLayout& L = rs.layout;
+  if (!d->texture_words || !d->texture_bindings || !d->material_textures || !d->texcoords || !d->tangents)
+    throw Error(OLC_ERR_VALUE, "a textured scene needs texture words, bindings, material textures, texcoords and tangents");
+  const uint32_t nw = d->num_texture_words;
+  if (nw < 1 || (uint64_t)1 + 8ull * d->texture_words[0] > nw) throw Error(OLC_ERR_VALUE, "texture header is truncated");
+  const uint32_t ntex = d->texture_words[0];
+  for (uint32_t t = 0; t < ntex; ++t) {
+    const uint32_t* m = d->texture_words + 1 + 8ull * t;
+    const uint64_t w = m[2], h = m[3], levels = m[5];
+    if (w == 0 || h == 0 || levels == 0 || levels > 32) throw Error(OLC_ERR_VALUE, "texture size or level count is invalid");
+    uint64_t words = 0, lw = w, lh = h;
+    for (uint64_t l = 0; l < levels; ++l) {
+      words += lw * lh;
+      lw = std::max<uint64_t>((lw + 1) / 2, 1);
+      lh = std::max<uint64_t>((lh + 1) / 2, 1);
+    }
+    if ((uint64_t)m[0] + words > nw || (uint64_t)m[1] + words > nw) throw Error(OLC_ERR_VALUE, "texture data is truncated");
+  }
+  const uint32_t nb = d->num_texture_bindings;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const float t = d->texture_bindings[8ull * b];
+    if (!(t == -1.0f || (t >= 0.0f && t < (float)ntex && t == std::floor(t))))
+      throw Error(OLC_ERR_VALUE, "a texture binding refers to a missing texture");
+    for (int k = 0; k < 8; ++k)
+      if (!std::isfinite(d->texture_bindings[8ull * b + k])) throw Error(OLC_ERR_VALUE, "texture bindings must be finite");
+  }
+  for (uint32_t mi = 0; mi < d->num_materials; ++mi)
+    for (int k = 0; k < 6; ++k) {
+      const float v = d->material_textures[12ull * mi + k];
+      if (!(v < 0.0f || (v < (float)nb && v == std::floor(v))))
+        throw Error(OLC_ERR_VALUE, "a material refers to a missing texture binding");
+    }
+  uint64_t staging = 0;
+  upload(rs.tex_words, d->texture_words, nw, st, own);
+  upload(rs.tex_bindings, d->texture_bindings, 8ull * nb, st, own);
+  upload(rs.mat_tex, d->material_textures, 12ull * std::max<uint32_t>(d->num_materials, 1), st, own);
+  const uint64_t slots = std::max<uint64_t>(L.slot_count, 1);
+  rs.tex_attr.allocate(slots * 6 * sizeof(float4));
+  own += rs.tex_attr.bytes();
+  const uint32_t slot0 = (uint32_t)rs.slots.off;
+  DeviceBuffer duv, dtan, di;
+  upload(duv, d->texcoords, 4ull * L.total_v, st, staging);
+  upload(dtan, d->tangents, 4ull * L.total_v, st, staging);
+  upload(di, d->indices, 3ull * L.total_t, st, staging);
+  const uint32_t* tri_index = ctx->slots.at<uint32_t>(2);
+  for (uint32_t m = 0; m < L.nm; ++m) {
+    if (!L.mesh_used[m]) continue;
+    slot_attributes(duv.as<float4>(), dtan.as<float4>(), di.as<uint32_t>() + 3ull * d->mesh_triangle_offset[m],
+                    mesh_triangles(d, m), d->mesh_vertex_offset[m], tri_index, slot0 + d->mesh_triangle_offset[m],
+                    slot0, rs.tex_attr.as<float4>(), st);
+  }
+  if (L.flat_tris) {
+    std::vector<float4> fa(6ull * L.flat_tris);
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < L.ni; ++i) {
+      if (!L.flat[i]) continue;
+      const float* x = d->instance_object_to_world + 12ull * i;
+      const double lin[3][3] = {{x[0], x[1], x[2]}, {x[4], x[5], x[6]}, {x[8], x[9], x[10]}};
+      const double det = lin[0][0] * (lin[1][1] * lin[2][2] - lin[1][2] * lin[2][1]) -
+                         lin[0][1] * (lin[1][0] * lin[2][2] - lin[1][2] * lin[2][0]) +
+                         lin[0][2] * (lin[1][0] * lin[2][1] - lin[1][1] * lin[2][0]);
+      double inv[3][3];   // inverse transpose: normals to world space
+      inv[0][0] = (lin[1][1] * lin[2][2] - lin[1][2] * lin[2][1]) / det;
+      inv[0][1] = (lin[1][2] * lin[2][0] - lin[1][0] * lin[2][2]) / det;
+      inv[0][2] = (lin[1][0] * lin[2][1] - lin[1][1] * lin[2][0]) / det;
+      inv[1][0] = (lin[0][2] * lin[2][1] - lin[0][1] * lin[2][2]) / det;
+      inv[1][1] = (lin[0][0] * lin[2][2] - lin[0][2] * lin[2][0]) / det;
+      inv[1][2] = (lin[0][1] * lin[2][0] - lin[0][0] * lin[2][1]) / det;
+      inv[2][0] = (lin[0][1] * lin[1][2] - lin[0][2] * lin[1][1]) / det;
+      inv[2][1] = (lin[0][2] * lin[1][0] - lin[0][0] * lin[1][2]) / det;
+      inv[2][2] = (lin[0][0] * lin[1][1] - lin[0][1] * lin[1][0]) / det;
+      const uint32_t m = d->instance_mesh[i];
+      const uint32_t v0 = d->mesh_vertex_offset[m];
+      for (uint32_t lt = 0; lt < mesh_triangles(d, m); ++lt, ++t) {
+        for (int c = 0; c < 3; ++c) {
+          const uint64_t vi = v0 + d->indices[3ull * (d->mesh_triangle_offset[m] + lt) + c];
+          const float* uv = d->texcoords + 4 * vi;
+          const float* tg = d->tangents + 4 * vi;
+          const float* nm = d->normals + 3 * vi;
+          double tw[3], nw3[3];
+          for (int r = 0; r < 3; ++r) {
+            tw[r] = lin[r][0] * tg[0] + lin[r][1] * tg[1] + lin[r][2] * tg[2];
+            nw3[r] = inv[r][0] * nm[0] + inv[r][1] * nm[1] + inv[r][2] * nm[2];
+          }
+          const double nl = std::sqrt(nw3[0] * nw3[0] + nw3[1] * nw3[1] + nw3[2] * nw3[2]);
+          for (double& v : nw3) v /= (nl > 0 ? nl : 1.0);
+          const double dn = tw[0] * nw3[0] + tw[1] * nw3[1] + tw[2] * nw3[2];
+          for (int r = 0; r < 3; ++r) tw[r] -= nw3[r] * dn;
+          const double tl = std::sqrt(tw[0] * tw[0] + tw[1] * tw[1] + tw[2] * tw[2]);
+          for (double& v : tw) v /= (tl > 0 ? tl : 1.0);
+          fa[6 * t + 2 * c] = make_float4(uv[0], uv[1], uv[2], uv[3]);
+          fa[6 * t + 2 * c + 1] = make_float4((float)tw[0], (float)tw[1], (float)tw[2], det < 0.0 ? -tg[3] : tg[3]);
+        }
+      }
+    }
+    upload_to(rs.tex_attr.as<float4>() + 6ull * L.total_t, fa.data(), fa.size(), st);
+  }
+  OLC_CUDA(cudaStreamSynchronize(st));
+}
+
 // Everything of a resident scene besides its BLAS: instance records, the
 // baked world-space triangles, the TLAS, materials, emitters, lights,
 // environment, volume and the SceneRec.  Runs at upload and at every
@@ -768,6 +882,14 @@ void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScen
   v.vol_sigma_t_scale = d->volume_sigma_t_scale;
   v.vol_albedo = d->volume_albedo;
   v.vol_max_density = d->volume_max_density;
+  write_textures(ctx, d, rs, own);
+  v.tex_words = rs.tex_words.as<uint32_t>();
+  v.tex_bindings = rs.tex_bindings.as<float4>();
+  v.tex_attr = rs.tex_attr.as<float4>();
+  v.mat_tex = rs.mat_tex.as<float4>();
+  v.srgb_lut = ctx->srgb_lut.as<float>();
+  v.slot_base = (uint32_t)rs.slots.off;
+  v.material_base = (uint32_t)rs.materials.off;
 }
 
 BlasDesc mesh_blas_desc(const olc_scene_desc* d, uint32_t m, const DeviceBuffer& dv, const DeviceBuffer& dn,
@@ -1094,6 +1216,7 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
     }
     ch.count = (uint32_t)fill;
     plan.restir = plan.restir || ch.restir;
+    for (const Take& t : takes) plan.textures = plan.textures || t.job->textured;
     plan.max_segments = std::max<uint32_t>(plan.max_segments, (uint32_t)ch.segs.size());
     plan.max_count = std::max<uint32_t>(plan.max_count, ch.count);
     plan.chunks.push_back(std::move(ch));
@@ -1122,6 +1245,7 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   ctx->ps_tp.allocate(c * 16);
   ctx->ps_rad.allocate(c * 16);
   ctx->ps_ior.allocate(c * 32);
+  ctx->ps_cone.allocate(c * 8);
   ctx->ps_meta.allocate(c * 16);
   ctx->capacity = capacity;
   drop_graphs(ctx);
@@ -1203,7 +1327,7 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
   b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
   b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>(),
-                   ctx->ps_ior.as<float4>()};
+                   ctx->ps_ior.as<float4>(), ctx->ps_cone.as<float2>()};
   b.prod.depth = ctx->prod_depth.as<float>();
   b.prod.normal = ctx->prod_normal.as<float4>();
   b.prod.instance_id = ctx->prod_inst.as<uint32_t>();
@@ -1248,10 +1372,11 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
       if (b == 0 && ch.restir) {
-        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, st);
+        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, plan.textures, st);
         tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
-      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir, st);
+      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
+                   plan.textures, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, st);
       tl_mark(ctx, OLC_STAGE_SHADOW, b, c);
@@ -1272,6 +1397,7 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
   std::vector<uint64_t> k;
   k.push_back(plan.chunks.size());
   for (const ChunkPlan& c : plan.chunks) k.push_back(((uint64_t)c.bounces << 1) | (c.restir ? 1u : 0u));
+  k.push_back(plan.textures ? 1u : 0u);
   auto ptr = [&](const void* p) { k.push_back((uint64_t)(uintptr_t)p); };
   const SceneView s = pool_view(ctx);
   const void* const* sv = reinterpret_cast<const void* const*>(&s);
@@ -1282,7 +1408,7 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         ctx->sort_keys.get(), ctx->sort_bins.get(),
                         (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
                         (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
-                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.prod.depth,
+                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.ps.cone, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.prod.position,
                         (const void*)rb.prod.barycentric, (const void*)rb.cnt, (const void*)rb.accum,
@@ -1551,6 +1677,7 @@ void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
   q.rec = make_job(ctx, &d->camera, d->width, d->height, d->samples_per_pixel, d->frame_index, d->max_bounces,
                    d->scene);
   q.rec.sample_base = d->first_sample;
+  q.textured = scene_of(ctx, d->scene).rec.tex_words != nullptr;
   q.total = (uint64_t)q.rec.npix * q.rec.spp;
   q.out = d->out_rgba;
   q.sums = d->out_sums;
@@ -1609,6 +1736,8 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     id.instance_id = 0xffffffffu;
     id.flags = OLC_INSTANCE_FLATTENED;
     upload_to(ctx->instances.at<InstanceRec>(0, OLC_IDENTITY_INSTANCE), &id, 1, ctx->stream);
+    ctx->srgb_lut.allocate(256 * sizeof(float));
+    srgb_table(ctx->srgb_lut.as<float>(), ctx->stream);
     sync_scene_table(ctx.get());
   });
   if (rc != OLC_OK) {
@@ -1729,7 +1858,7 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
   for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p, &ctx->q2_o,
                                 &ctx->q2_d, &ctx->q2_p, &ctx->sort_keys, &ctx->sort_bins,
                                 &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
-                                &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
+                                &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->ps_cone, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,
                                 &ctx->sample_lum, &ctx->motion_prev, &ctx->restir.res_a0,
@@ -1749,11 +1878,11 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     check_camera(camera);
     check_size(width, height, spp);
     const ResidentScene& rs = default_scene(ctx);
-    (void)rs;
     if (!out_rgba) throw Error(OLC_ERR_VALUE, "output pointer is required");
     QueuedJob job;
     job.rec = make_job(ctx, camera, width, height, spp, frame_index, 0, ctx->default_scene);
     job.rec.products = 1;
+    job.textured = rs.rec.tex_words != nullptr;
     job.total = (uint64_t)job.rec.npix * spp;
     job.out = out_rgba;
     job.out_device = out_is_device != 0;
@@ -2124,6 +2253,30 @@ int olc_read_motion(olc_context* ctx, uint32_t width, uint32_t height, const olc
                    height, d_table.as<MotionMesh>(), ctx->motion_prev_count ? num_meshes : 0u,
                    ctx->motion_prev.as<float4>(), cam(now), cam(before), d_out.as<float2>(), st);
     OLC_CUDA(cudaMemcpyAsync(motion, d_out.get(), n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int olc_sample_texture(olc_context* ctx, uint32_t handle, int32_t binding, uint32_t n, const float* uv0,
+                       const float* uv1, const float* fp0, const float* fp1, int srgb, float* out) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (handle == OLC_DEFAULT_SCENE) handle = ctx->default_scene;
+    const ResidentScene& rs = scene_of(ctx, handle);
+    if (!rs.rec.tex_words) throw Error(OLC_ERR_VALUE, "the scene has no textures");
+    if (binding < -1 || binding >= (int32_t)(rs.tex_bindings.bytes() / 32)) throw Error(OLC_ERR_VALUE, "unknown texture binding");
+    if (n == 0) return;
+    if (!uv0 || !uv1 || !fp0 || !fp1 || !out) throw Error(OLC_ERR_VALUE, "inputs and output are required");
+    cudaStream_t st = ctx->stream;
+    uint64_t staging = 0;
+    DeviceBuffer d0, d1, f0, f1, dout(n * sizeof(float4));
+    upload(d0, uv0, 2ull * n, st, staging);
+    upload(d1, uv1, 2ull * n, st, staging);
+    upload(f0, fp0, n, st, staging);
+    upload(f1, fp1, n, st, staging);
+    launch_sample_textures(ctx->ls, ctx->scene_table.as<SceneRec>(), handle, (float)binding, n, d0.as<float2>(),
+                           d1.as<float2>(), f0.as<float>(), f1.as<float>(), srgb, dout.as<float4>(), st);
+    OLC_CUDA(cudaMemcpyAsync(out, dout.get(), n * sizeof(float4), cudaMemcpyDeviceToHost, st));
     OLC_CUDA(cudaStreamSynchronize(st));
   });
 }

@@ -597,6 +597,49 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& sc, BvhNode* nodes, uint32_
   return root;
 }
 
+// ---- texture attributes of triangle slots --------------------------------
+
+// Per-slot vertex attributes of one mesh's BLAS slots, in slot order:
+// (uv0, uv1) and (object tangent, handedness) of each corner.
+__global__ void k_slot_attributes(const float4* __restrict__ texcoords, const float4* __restrict__ tangents,
+                                  const uint32_t* __restrict__ indices, uint32_t nt, uint32_t vertex_base,
+                                  const uint32_t* __restrict__ tri_index, uint32_t first_slot, uint32_t scene_slot0,
+                                  float4* attr) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nt) return;
+  const uint32_t slot = first_slot + s;
+  const uint32_t t = tri_index[slot];
+  float4* out = attr + 6ull * (slot - scene_slot0);
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t vi = vertex_base + indices[3ull * t + k];
+    out[2 * k] = texcoords[vi];
+    out[2 * k + 1] = tangents[vi];
+  }
+}
+
+void slot_attributes(const float4* texcoords, const float4* tangents, const uint32_t* mesh_indices, uint32_t nt,
+                     uint32_t vertex_base, const uint32_t* tri_index, uint32_t first_slot, uint32_t scene_slot0,
+                     float4* attr, cudaStream_t stream) {
+  if (nt == 0) return;
+  k_slot_attributes<<<blocks_for(nt), kThreads, 0, stream>>>(texcoords, tangents, mesh_indices, nt, vertex_base,
+                                                               tri_index, first_slot, scene_slot0, attr);
+  OLC_LAUNCH_CHECK("k_slot_attributes");
+}
+
+// sRGB-to-linear decode of the 256 byte values, c / 12.92 below 0.04045 and
+// ((c + 0.055) / 1.055)^2.4 above (IEC 61966-2-1), in double precision.
+__global__ void k_srgb_table(float* out) {
+  const uint32_t i = threadIdx.x;
+  if (i >= 256u) return;
+  const double c = (double)i / 255.0;
+  out[i] = (float)(c <= 0.04045 ? c / 12.92 : pow((c + 0.055) / 1.055, 2.4));
+}
+
+void srgb_table(float* out, cudaStream_t stream) {
+  k_srgb_table<<<1, 256, 0, stream>>>(out);
+  OLC_LAUNCH_CHECK("k_srgb_table");
+}
+
 // ---- refit: new triangle positions under an unchanged hierarchy ----------
 
 // Rewrite the triangle slots of one BLAS from new mesh arrays.  Slot order

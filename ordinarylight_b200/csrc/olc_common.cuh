@@ -240,6 +240,14 @@ struct __align__(16) SceneRec {
   float vol_albedo;
   float vol_max_density;
   uint32_t pad;
+  // textures (tex_words == nullptr: an untextured scene)
+  const uint32_t* tex_words;     // Scene.texture_data layout
+  const float4* tex_bindings;    // 2 per binding: (texture, cos, sin, texcoord set), (offset, scale)
+  const float4* tex_attr;        // 6 per triangle slot of the scene: per vertex (uv0, uv1), (tangent, handedness)
+  const float4* mat_tex;         // 3 per material of the scene: binding indices and map parameters
+  const float* srgb_lut;         // 256 sRGB-to-linear values
+  uint32_t slot_base;            // first triangle slot of the scene
+  uint32_t material_base;        // first material record of the scene
 };
 
 // Device view of the scene pool shared by every resident scene: all BLAS and
@@ -286,6 +294,7 @@ struct PathState {
   float4* radiance;        // rgb, unused
   uint4* meta;             // pixel, sample, bounce | flags << 8, job
   float4* ior_stack;       // 2 per path: indices of refraction of the media entered, entries 1..8
+  float2* cone;            // ray cone (width, spread) of the path's next ray; textured scenes only
 };
 
 #define OLC_PATH_FLAG_PREV_NEE 1u     // the previous vertex sampled area lights

@@ -108,6 +108,15 @@ uint32_t build_blas(const BlasDesc& d, BuildScratch& scratch, BvhNode* nodes, ui
                     uint32_t leaf_max, cudaStream_t stream);
 inline uint32_t blas_node_count(uint32_t nt) { return nt > 1 ? nt - 1 : 1; }
 
+// Texture attributes of one mesh's BLAS slots [first_slot, +nt) into
+// attr[6 * (slot - scene_slot0) ...] (texcoords / tangents: float4 per vertex
+// of the concatenated mesh arrays, mesh_indices: the mesh's index triples).
+void slot_attributes(const float4* texcoords, const float4* tangents, const uint32_t* mesh_indices, uint32_t nt,
+                     uint32_t vertex_base, const uint32_t* tri_index, uint32_t first_slot, uint32_t scene_slot0,
+                     float4* attr, cudaStream_t stream);
+// The 256-entry sRGB decode table.
+void srgb_table(float* out, cudaStream_t stream);
+
 // Refit one BLAS in place for new positions of the same triangles: rewrite
 // its slots [slot_base, +nt) from d and recompute the boxes of its
 // node_count nodes at node_base bottom-up.  The hierarchy is unchanged.

@@ -27,6 +27,7 @@
 
 #include "olc_restir.h"
 #include "olc_shading.cuh"
+#include "olc_textures.cuh"
 
 namespace olc {
 
@@ -152,7 +153,8 @@ OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float
 }
 
 // Primary surface of path slot i (its ray hit: only listed hits get here).
-OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i) {
+template <bool kTextures>
+OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i, uint32_t scene) {
   Surface su;
   const float4 hit = h.tuv_slot[i];
   const float4 dr = q.dir_root[i];
@@ -175,7 +177,18 @@ OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBu
   const bool entering = dot(d, ng) < 0.0f;
   su.p = f3(ot) + d * hit.x;
   const uint32_t owner = owner_instance(s.instances, s.tri_owner, inst, slot);
-  su.bsdf = prepare_bsdf(load_material(s, s.instances[owner].material), entering ? ns : -ns, -d);
+  const uint32_t mi = s.instances[owner].material;
+  SurfaceMat mat = load_material(s, mi);
+  // the textured material and mapped normal the shading stage will see (the
+  // camera ray's cone has width 0)
+  const SceneRec& sc = s.scenes[scene];
+  if (kTextures && sc.tex_words != nullptr) {
+    const TexturedHit th = apply_textures(sc, mi - sc.material_base, slot, v0, v1, v2, o2w, w2o, tn, hit.y, hit.z,
+                                          0.0f, ng, ns, mat);
+    mat = th.m;
+    ns = th.ns;
+  }
+  su.bsdf = prepare_bsdf(mat, entering ? ns : -ns, -d);
   su.depth = hit.x;
   return su;
 }
@@ -252,6 +265,7 @@ __global__ void k_restir_compact(const ChunkHeader* __restrict__ hdr, const JobR
   }
 }
 
+template <bool kTextures>
 __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
@@ -261,7 +275,7 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
     const JobRec& job = a.jobs[meta.w];
     const SceneRec& sc = s.scenes[job.scene];
     const uint64_t g = reservoir_index(job, meta.y, meta.x);
-    const Surface su = primary_surface(s, a.q, a.h, i);
+    const Surface su = primary_surface<kTextures>(s, a.q, a.h, i, job.scene);
     const uint32_t stamp = a.hdr->stamp;
     Res r{0xffffffffu, 0u, 0.0f, 0u, 0.0f};
     uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream);
@@ -295,6 +309,7 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
   }
 }
 
+template <bool kTextures>
 __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
@@ -304,7 +319,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
     const JobRec& job = a.jobs[meta.w];
     const uint64_t g = reservoir_index(job, meta.y, meta.x);
     const uint64_t stream_base = g - meta.x;
-    const Surface su = primary_surface(s, a.q, a.h, i);
+    const Surface su = primary_surface<kTextures>(s, a.q, a.h, i, job.scene);
     const uint32_t stamp = a.hdr->stamp;
     float d0;
     uint32_t n0, st0;
@@ -376,7 +391,7 @@ void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32
 
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
                         const ChunkHeader* hdr, const JobRec* jobs, const RayQueue& q, const HitBuf& hits,
-                        const PathState& ps, cudaStream_t stream) {
+                        const PathState& ps, bool textures, cudaStream_t stream) {
   RestirArgs a{};
   a.hdr = hdr;
   a.jobs = jobs;
@@ -400,7 +415,8 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
                                                         st.hit_count.as<uint32_t>());
   OLC_LAUNCH_CHECK("k_restir_compact");
   const uint32_t grid = ls.grid_shade;
-  k_restir_initial<<<grid, 128, 0, stream>>>(a);
+  if (textures) k_restir_initial<true><<<grid, 128, 0, stream>>>(a);
+  else k_restir_initial<false><<<grid, 128, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_restir_initial");
   // spatial passes ping-pong A -> B -> A ...; the last pass finalises.
   uint32_t passes = std::max<uint32_t>(cfg.restir_spatial, 1u);
@@ -414,7 +430,8 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
     b.out0 = in_a ? st.res_b0.as<uint4>() : st.res_a0.as<uint4>();
     b.out1 = in_a ? st.res_b1.as<uint4>() : st.res_a1.as<uint4>();
     b.finalize = (p + 1 == passes) ? 1u : 0u;
-    k_restir_spatial<<<grid, 128, 0, stream>>>(b);
+    if (textures) k_restir_spatial<true><<<grid, 128, 0, stream>>>(b);
+    else k_restir_spatial<false><<<grid, 128, 0, stream>>>(b);
     OLC_LAUNCH_CHECK("k_restir_spatial");
     in_a = !in_a;
   }

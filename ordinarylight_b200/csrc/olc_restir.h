@@ -39,7 +39,7 @@ void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32
 // so the launches can be captured in a graph and replayed.
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
                         const ChunkHeader* hdr, const JobRec* jobs, const RayQueue& q, const HitBuf& hits,
-                        const PathState& ps, cudaStream_t stream);
+                        const PathState& ps, bool textures, cudaStream_t stream);
 // Promote this wavefront's final reservoirs to history (plain frames only).
 void restir_finish(RestirState& st);
 void restir_reset(RestirState& st);

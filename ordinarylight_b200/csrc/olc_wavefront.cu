@@ -16,6 +16,7 @@
 // can be captured once as a CUDA graph.
 #include "olc_internal.h"
 #include "olc_shading.cuh"
+#include "olc_textures.cuh"
 #include "olc_trace.cuh"
 #include "olc_volume.cuh"
 #include "olc_wavefront.h"
@@ -303,6 +304,9 @@ OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& 
 
 // Three blocks of 256 threads per SM (at most 85 registers): the shading
 // kernel is latency bound, and the occupancy gained outweighs its spills.
+// kTextures: a variant for runs with a textured scene; the untextured one
+// carries none of the texture code's registers.
+template <bool kTextures>
 __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
@@ -349,6 +353,10 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
       if (scattered) {
         const float3 p = o + d * t_med;
         tp *= med.albedo;
+        if (kTextures && sc.tex_words != nullptr) {
+          const float2 c = bounce > 0u ? a.ps.cone[path] : make_float2(0.0f, 0.0f);
+          a.ps.cone[path] = make_float2(c.x + t_med * c.y, c.y);
+        }
         if (write_products) {
           a.prod.depth[out_pixel] = t_med;
           a.prod.normal[out_pixel] = make_float4(0, 0, 0, 0);
@@ -437,6 +445,22 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           if (!(dot(ns, ns) > 0.5f)) ns = ng;
           if (dot(ns, ng) < 0.0f) ns = -ns;
           const bool entering = dot(d, ng) < 0.0f;
+          // textures (wavefront_shade.comp:368-391), looked up with the ray
+          // cone's footprint; camera rays start with width and spread 0
+          const bool textured = kTextures && sc.tex_words != nullptr;
+          float cone_w = 0.0f, cone_s = 0.0f, occlusion = 1.0f;
+          if (textured) {
+            if (bounce > 0u) {
+              const float2 c = a.ps.cone[path];
+              cone_s = c.y;
+              cone_w = c.x + t * c.y;
+            }
+            const TexturedHit th = apply_textures(sc, orec.material - sc.material_base, slot, v0, v1, v2, o2w, w2o,
+                                                  tn, bu, bv, cone_w, ng, ns, m);
+            m = th.m;
+            ns = th.ns;
+            occlusion = th.occlusion;
+          }
           const float3 nrm = entering ? ns : -ns;
           // emission with power-heuristic MIS against the previous BSDF pdf
           // (wavefront_shade.comp:412-433)
@@ -474,6 +498,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             tp *= (f3(0.8f, 0.8f, 0.8f) + m.base * 0.2f) * m.transmission;
             new_flags = (depth - 1u) << OLC_PATH_DEPTH_SHIFT;
             new_pdf = tp4.w;
+            if (textured) a.ps.cone[path] = make_float2(cone_w, cone_s);
             wdir = normalize(wdir);
             if (max3(tp) > 0.0f) {
               next_o = p + wdir * 0.002f;
@@ -518,6 +543,13 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             float3 wdir, weight;
             float pdf;
             const bool sampled = pbr_sample(m, nrm, d, rng, wdir, weight, pdf);
+            if (textured) {
+              // occlusion map on the sampled weight (ordinarylight_pbr_weight,
+              // ordinaryshade_primary.glsl:605-609); the cone spreads with
+              // roughness (wavefront_shade.comp:546)
+              weight = weight * (occlusion * (1.0f - m.metallic) + m.metallic);
+              a.ps.cone[path] = make_float2(cone_w, cone_s + m.roughness * 0.25f);
+            }
             tp *= weight;
             new_pdf = pdf;
             if (did_restir) new_flags |= OLC_PATH_FLAG_PREV_RESTIR;
@@ -779,6 +811,16 @@ __global__ void k_resolve(const ResolveEntry* __restrict__ entries, const uint32
   }
 }
 
+// Material texture lookups of a scene for given coordinates and footprints
+// (the sampler alone, for its parity tests).
+__global__ void k_sample_textures(const SceneRec* __restrict__ scenes, uint32_t scene, float binding, uint32_t n,
+                                  const float2* __restrict__ uv0, const float2* __restrict__ uv1,
+                                  const float* __restrict__ fp0, const float* __restrict__ fp1, int srgb, float4* out) {
+  const SceneRec& sc = scenes[scene];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = sample_material_texture(sc, binding, uv0[i], uv1[i], srgb != 0, fp0[i], fp1[i]);
+}
+
 __global__ void k_camera_rays(const JobRec* __restrict__ job_ptr, uint32_t sample, float2 jitter_override,
                               int use_override, float* origins, float* dirs) {
   const JobRec job = *job_ptr;
@@ -888,7 +930,7 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
-                  cudaStream_t stream) {
+                  bool textures, cudaStream_t stream) {
   ShadeArgs a;
   a.jobs = jobs;
   a.s = s;
@@ -902,7 +944,8 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   a.capacity = capacity;
   a.prod = prod;
   a.restir = restir;
-  k_shade<<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  if (textures) k_shade<true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  else k_shade<false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_shade");
 }
 
@@ -936,6 +979,14 @@ void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const ui
                     const unsigned long long* accum, float4* out, cudaStream_t stream) {
   k_resolve<<<ls.grid_simple, ls.block, 0, stream>>>(entries, num_entries, accum, out);
   OLC_LAUNCH_CHECK("k_resolve");
+}
+
+void launch_sample_textures(const LaunchShape& ls, const SceneRec* scenes, uint32_t scene, float binding, uint32_t n,
+                            const float2* uv0, const float2* uv1, const float* fp0, const float* fp1, int srgb,
+                            float4* out, cudaStream_t stream) {
+  if (n == 0) return;
+  k_sample_textures<<<ls.grid_simple, ls.block, 0, stream>>>(scenes, scene, binding, n, uv0, uv1, fp0, fp1, srgb, out);
+  OLC_LAUNCH_CHECK("k_sample_textures");
 }
 
 void launch_camera_rays(const LaunchShape& ls, const JobRec* job, uint32_t sample, const float* jitter,

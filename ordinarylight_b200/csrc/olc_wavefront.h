@@ -74,7 +74,7 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
-                  cudaStream_t stream);
+                  bool textures, cudaStream_t stream);
 // Reorder the bounce's ray queue `in` into `out` by origin cell and direction
 // bin (keys: one word per queue slot; bins: sort_bins_bytes() of scratch).
 void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue& in, const RayQueue& out,
@@ -87,6 +87,9 @@ void launch_sample_variance(const LaunchShape& ls, const float* sample_lum, uint
                             cudaStream_t stream);
 void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,
                     const unsigned long long* accum, float4* out, cudaStream_t stream);
+void launch_sample_textures(const LaunchShape& ls, const SceneRec* scenes, uint32_t scene, float binding, uint32_t n,
+                            const float2* uv0, const float2* uv1, const float* fp0, const float* fp1, int srgb,
+                            float4* out, cudaStream_t stream);
 void launch_camera_rays(const LaunchShape& ls, const JobRec* job, uint32_t sample, const float* jitter,
                         float* origins, float* dirs, cudaStream_t stream);
 void launch_trace_rays(const LaunchShape& ls, const SceneView& s, uint32_t root, uint32_t n, const float* origins,

@@ -48,6 +48,12 @@ class PackedScene:
     volume: dict | None
     total_triangles: int
     mesh_sources: tuple = ()      # the MeshResource (or Mesh) behind each packed mesh
+    # textures (texture_bindings empty: an untextured scene)
+    texcoords: np.ndarray | None = None          # [total_vertices, 4] uv0, uv1
+    tangents: np.ndarray | None = None           # [total_vertices, 4] object-space xyz, handedness
+    texture_words: np.ndarray | None = None      # Scene.texture_data layout
+    texture_bindings: np.ndarray | None = None   # [n, 8]
+    material_textures: np.ndarray | None = None  # [num_materials, 12]
 
     def descriptor(self) -> _native.OlcSceneDesc:
         d = _native.OlcSceneDesc()
@@ -89,6 +95,14 @@ class PackedScene:
             d.volume_sigma_t_scale = float(v["sigma_t_scale"])
             d.volume_albedo = float(v["albedo"])
             d.volume_max_density = float(v["max_density"])
+        if self.texture_bindings is not None and len(self.texture_bindings):
+            d.texcoords = _native.typed_ptr(self.texcoords, f32)
+            d.tangents = _native.typed_ptr(self.tangents, f32)
+            d.num_texture_words = len(self.texture_words)
+            d.texture_words = _native.typed_ptr(self.texture_words, u32)
+            d.num_texture_bindings = len(self.texture_bindings)
+            d.texture_bindings = _native.typed_ptr(self.texture_bindings, f32)
+            d.material_textures = _native.typed_ptr(self.material_textures, f32)
         return d
 
 
@@ -103,6 +117,93 @@ def _material_record(material, material_id: int) -> np.ndarray:
     rec[10] = float(getattr(material, "transmission", 0.0))
     rec[11] = float(getattr(material, "ior", 1.5))
     return rec
+
+
+# -- textures ---------------------------------------------------------------
+TEXTURE_SLOTS = ("base_color", "metallic_roughness", "emissive", "normal", "occlusion", "transmission")
+_WRAP_CODES = {"repeat": 0, "clamp": 1, "mirror": 2}
+
+
+def texture_mips(pixels, *, srgb):
+    """RGBA8 mip pyramid down to 1x1: 2x2 box filter of edge-padded levels,
+    averaged in linear space for sRGB data and re-encoded per level
+    (Scene._texture_mips, scene/_core.py:3045-3077)."""
+    current = np.asarray(pixels, dtype=np.float32) / 255.0
+    if srgb:
+        rgb = current[..., :3]
+        current[..., :3] = np.where(rgb <= 0.04045, rgb / 12.92, ((rgb + 0.055) / 1.055) ** 2.4)
+    levels = []
+    while True:
+        encoded = current.copy()
+        if srgb:
+            rgb = np.maximum(encoded[..., :3], 0.0)
+            encoded[..., :3] = np.where(rgb <= 0.0031308, rgb * 12.92, 1.055 * rgb ** (1.0 / 2.4) - 0.055)
+        levels.append(np.clip(encoded * 255.0 + 0.5, 0, 255).astype(np.uint8))
+        height, width, _ = current.shape
+        if width == 1 and height == 1:
+            return levels
+        nw, nh = max(1, (width + 1) // 2), max(1, (height + 1) // 2)
+        padded = np.pad(current, ((0, height & 1), (0, width & 1), (0, 0)), mode="edge")
+        current = padded.reshape(nh, 2, nw, 2, 4).mean(axis=(1, 3))
+
+
+def texture_words(textures):
+    """Header (count, then 8 words per texture: sRGB offset, linear offset,
+    width, height, wrap/filter flags, levels, 0, 0) followed by each
+    texture's sRGB and linear RGBA8 pyramids (Scene.texture_data,
+    scene/_core.py:3005-3043)."""
+    header = np.zeros(1 + 8 * len(textures), np.uint32)
+    header[0] = len(textures)
+    chunks, offset = [header], len(header)
+    for index, texture in enumerate(textures):
+        height, width, _ = texture.pixels.shape
+        flags = _WRAP_CODES[texture.wrap_s] | (_WRAP_CODES[texture.wrap_t] << 2) | (int(texture.linear_filter) << 4)
+        words = []
+        for srgb in (True, False):
+            levels = texture_mips(texture.pixels, srgb=srgb)
+            words.append(np.concatenate([lv.reshape(-1, 4).copy().view(np.uint32).reshape(-1) for lv in levels]))
+        header[1 + 8 * index:9 + 8 * index] = (offset, offset + len(words[0]), width, height, flags, len(levels), 0, 0)
+        chunks += words
+        offset += len(words[0]) + len(words[1])
+    return np.ascontiguousarray(np.concatenate(chunks), dtype=np.uint32)
+
+
+def _texture_tables(meshes, materials_in_order):
+    """Textures in first-use order, (texture, transform) bindings and the
+    per-material binding records (Scene.textures / texture_bindings /
+    texture_binding_data, scene/_core.py:2928-3003)."""
+    textures, bindings = [], []
+    for mesh in meshes:
+        material = mesh.material
+        for slot in TEXTURE_SLOTS:
+            texture = getattr(material, f"{slot}_texture", None)
+            if texture is None:
+                continue
+            transform = getattr(material, f"{slot}_transform")
+            if all(texture is not t for t in textures):
+                textures.append(texture)
+            if all(texture is not t or transform != tf for t, tf in bindings):
+                bindings.append((texture, transform))
+    if not bindings:
+        return None
+    records = np.zeros((len(bindings), 8), np.float32)
+    for k, (texture, transform) in enumerate(bindings):
+        index = next(i for i, t in enumerate(textures) if t is texture)
+        records[k] = (index, np.cos(transform.rotation), np.sin(transform.rotation), transform.texcoord_set,
+                      *transform.offset, *transform.scale)
+    mat = np.zeros((len(materials_in_order), 12), np.float32)
+    for m, material in enumerate(materials_in_order):
+        uses_uv1 = 0.0
+        for k, slot in enumerate(TEXTURE_SLOTS):
+            texture = getattr(material, f"{slot}_texture", None)
+            transform = getattr(material, f"{slot}_transform", None)
+            mat[m, k] = next((i for i, (t, tf) in enumerate(bindings) if t is texture and tf == transform), -1)
+            if texture is not None and transform.texcoord_set == 1:
+                uses_uv1 = 1.0
+        mat[m, 6] = float(getattr(material, "normal_scale", 1.0))
+        mat[m, 7] = float(getattr(material, "occlusion_strength", 1.0))
+        mat[m, 8] = uses_uv1
+    return texture_words(textures), records, mat
 
 
 def emitter_records(scene):
@@ -199,7 +300,8 @@ def pack_scene(scene) -> PackedScene:
     """Flatten a scene into the arrays of olc_scene_desc."""
     mesh_index = {}
     sources = []
-    vertices, normals, indices = [], [], []
+    vertices, normals, indices, texcoords, tangents = [], [], [], [], []
+    material_objects = []
     v_off, t_off = [0], [0]
     inst_xf, inst_mesh, inst_mat, inst_id, inst_prim = [], [], [], [], []
     materials, material_index = [], {}
@@ -218,6 +320,14 @@ def pack_scene(scene) -> PackedScene:
             n = getattr(mesh, "normals", None)
             normals.append(np.ascontiguousarray(n if n is not None else np.zeros_like(verts), np.float32))
             indices.append(np.ascontiguousarray(mesh.indices, np.uint32).reshape(-1, 3))
+            uv0 = getattr(mesh, "texcoords", None)
+            uv1 = getattr(mesh, "texcoords1", None)
+            tan = getattr(mesh, "tangents", None)
+            zeros2 = np.zeros((len(verts), 2), np.float32)
+            texcoords.append(np.column_stack((zeros2 if uv0 is None else np.asarray(uv0, np.float32),
+                                              zeros2 if uv1 is None else np.asarray(uv1, np.float32))))
+            tangents.append(np.tile(np.array([1.0, 0.0, 0.0, 1.0], np.float32), (len(verts), 1)) if tan is None
+                            else np.asarray(tan, np.float32).reshape(-1, 4))
             v_off.append(v_off[-1] + len(verts))
             t_off.append(t_off[-1] + len(mesh.indices))
         mat = mesh.material
@@ -230,6 +340,7 @@ def pack_scene(scene) -> PackedScene:
                     mid = 0
             material_index[id(mat)] = len(materials)
             materials.append(_material_record(mat, mid))
+            material_objects.append(mat)
         inst_xf.append(np.asarray(mesh.transform.matrix, np.float32)[:3, :4].reshape(-1))
         inst_mesh.append(mesh_index[id(mesh.resource) if getattr(mesh, "resource", None) is not None else id(mesh)])
         inst_mat.append(material_index[id(mat)])
@@ -250,6 +361,12 @@ def pack_scene(scene) -> PackedScene:
 
     def stack(parts, dtype, shape):
         return np.ascontiguousarray(np.concatenate(parts), dtype) if parts else np.zeros(shape, dtype)
+
+    tables = _texture_tables([m for m in scene.visible_meshes if len(m.indices)], material_objects)
+    tex = {}
+    if tables is not None:
+        tex = dict(texcoords=stack(texcoords, np.float32, (0, 4)), tangents=stack(tangents, np.float32, (0, 4)),
+                   texture_words=tables[0], texture_bindings=tables[1], material_textures=tables[2])
 
     return PackedScene(
         mesh_vertex_offset=np.asarray(v_off, np.uint32),
@@ -273,6 +390,7 @@ def pack_scene(scene) -> PackedScene:
         volume=_volume_record(scene),
         total_triangles=prim,
         mesh_sources=tuple(sources),
+        **tex,
     )
 
 

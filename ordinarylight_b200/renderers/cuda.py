@@ -359,6 +359,21 @@ class CudaWavefrontRenderer(RendererImplementation):
             self._capture_motion_state(scene, camera, (w, h))
         return {name: table[name] for name in requested}
 
+    def sample_texture(self, scene, binding, uv0, uv1, footprint0, footprint1, *, srgb):
+        """The shading stage's lookup of texture binding ``binding`` of
+        ``scene`` at n points (its parity tests): (n, 4) float32."""
+        self._require_open()
+        self._ensure_scene(scene)
+        uv0 = np.ascontiguousarray(uv0, np.float32)
+        uv1 = np.ascontiguousarray(uv1, np.float32)
+        fp0 = np.ascontiguousarray(footprint0, np.float32)
+        fp1 = np.ascontiguousarray(footprint1, np.float32)
+        out = np.empty((len(uv0), 4), np.float32)
+        _native.check(self._lib, self._ctx, self._lib.olc_sample_texture(
+            self._ctx, _native.DEFAULT_SCENE, int(binding), len(uv0), _native.ptr(uv0), _native.ptr(uv1),
+            _native.ptr(fp0), _native.ptr(fp1), 1 if srgb else 0, _native.ptr(out)))
+        return out
+
     def hit_geometry(self, width, height):
         """World hit points (h, w, 3) and barycentrics (h, w, 2) of the last
         render's first-sample primary hits."""

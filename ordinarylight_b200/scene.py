@@ -27,7 +27,7 @@ from types import MappingProxyType
 import numpy as np
 
 __all__ = [
-    "Transform", "Material", "Mesh", "MeshResource", "Instance", "Scene",
+    "Transform", "Material", "Texture", "TextureTransform", "Mesh", "MeshResource", "Instance", "Scene",
     "Volume", "VolumeMaterial",
     "PerspectiveCamera", "OrthographicCamera", "PanoramicCamera",
     "PointLight", "DirectionalLight", "SpotLight", "EnvironmentLight",
@@ -260,8 +260,59 @@ class Transform:
 
 
 @dataclass(frozen=True)
+class Texture:
+    """Decoded RGBA8 texture with glTF sampler state (scene/_core.py:115-135)."""
+
+    pixels: np.ndarray = field(compare=False, repr=False)
+    wrap_s: str = "repeat"
+    wrap_t: str = "repeat"
+    linear_filter: bool = True
+
+    def __post_init__(self):
+        pixels = np.ascontiguousarray(self.pixels, dtype=np.uint8)
+        if pixels.ndim != 3 or pixels.shape[2] != 4 or min(pixels.shape[:2]) < 1:
+            raise ValueError("texture pixels must have shape (height, width, 4)")
+        for name in ("wrap_s", "wrap_t"):
+            if getattr(self, name) not in {"repeat", "clamp", "mirror"}:
+                raise ValueError(f"{name} must be repeat, clamp, or mirror")
+        pixels.flags.writeable = False
+        object.__setattr__(self, "pixels", pixels)
+
+
+@dataclass(frozen=True)
+class TextureTransform:
+    """KHR_texture_transform UV mapping (scene/_core.py:402-428)."""
+
+    offset: tuple = (0.0, 0.0)
+    scale: tuple = (1.0, 1.0)
+    rotation: float = 0.0
+    texcoord_set: int = 0
+
+    def __post_init__(self):
+        offset = tuple(float(v) for v in self.offset)
+        scale = tuple(float(v) for v in self.scale)
+        if len(offset) != 2 or len(scale) != 2:
+            raise ValueError("texture transform offset and scale must be vec2 values")
+        if not np.all(np.isfinite((*offset, *scale, float(self.rotation)))):
+            raise ValueError("texture transform values must be finite")
+        if abs(scale[0]) < 1e-8 or abs(scale[1]) < 1e-8:
+            raise ValueError("texture transform scale components cannot be zero")
+        if int(self.texcoord_set) not in (0, 1):
+            raise ValueError("texcoord_set must be zero or one")
+        object.__setattr__(self, "offset", offset)
+        object.__setattr__(self, "scale", scale)
+        object.__setattr__(self, "rotation", float(self.rotation))
+        object.__setattr__(self, "texcoord_set", int(self.texcoord_set))
+
+
+_TEXTURE_SLOTS = ("base_color", "metallic_roughness", "emissive", "normal", "occlusion", "transmission")
+
+
+@dataclass(frozen=True)
 class Material:
-    """PBR material (scene/_core.py:431-553)."""
+    """PBR material (scene/_core.py:431-553): the parameters and textures the
+    wavefront shades (base colour, metallic-roughness, emissive, normal,
+    occlusion and transmission maps, each with a KHR texture transform)."""
 
     base_color: tuple = (0.8, 0.8, 0.8)
     emission: tuple = (0.0, 0.0, 0.0)
@@ -271,8 +322,32 @@ class Material:
     ior: float = 1.5
     opacity: float = 1.0
     emission_two_sided: bool = False
+    base_color_texture: Texture | None = field(default=None, compare=False)
+    metallic_roughness_texture: Texture | None = field(default=None, compare=False)
+    emissive_texture: Texture | None = field(default=None, compare=False)
+    normal_texture: Texture | None = field(default=None, compare=False)
+    normal_scale: float = 1.0
+    occlusion_texture: Texture | None = field(default=None, compare=False)
+    occlusion_strength: float = 1.0
+    transmission_texture: Texture | None = field(default=None, compare=False)
+    base_color_transform: TextureTransform = field(default_factory=TextureTransform)
+    metallic_roughness_transform: TextureTransform = field(default_factory=TextureTransform)
+    emissive_transform: TextureTransform = field(default_factory=TextureTransform)
+    normal_transform: TextureTransform = field(default_factory=TextureTransform)
+    occlusion_transform: TextureTransform = field(default_factory=TextureTransform)
+    transmission_transform: TextureTransform = field(default_factory=TextureTransform)
 
     def __post_init__(self):
+        for slot in _TEXTURE_SLOTS:
+            texture = getattr(self, f"{slot}_texture")
+            if texture is not None and not isinstance(texture, Texture):
+                raise TypeError(f"{slot}_texture must be a Texture")
+            if not isinstance(getattr(self, f"{slot}_transform"), TextureTransform):
+                raise TypeError(f"{slot}_transform must be a TextureTransform")
+        if self.normal_scale < 0.0:
+            raise ValueError("normal_scale cannot be negative")
+        if not 0.0 <= self.occlusion_strength <= 1.0:
+            raise ValueError("occlusion_strength must be between zero and one")
         color = _vec3(self.base_color, "base_color")
         emission = _vec3(self.emission, "emission")
         if np.any(color < 0.0) or np.any(color > 1.0):
@@ -286,6 +361,45 @@ class Material:
             raise ValueError("ior must be positive")
         if not isinstance(self.emission_two_sided, bool):
             raise TypeError("emission_two_sided must be a bool")
+
+
+def _generate_tangents(vertices, indices, normals, texcoords):
+    """Per-vertex tangents from UV gradients, orthogonalised against the
+    normal, with handedness from the accumulated bitangent; an axis-derived
+    tangent where the UVs are degenerate (Mesh._generate_tangents,
+    scene/_core.py:740-772)."""
+    vertices = np.asarray(vertices, np.float32)
+    tri = vertices[indices]
+    uv = np.asarray(texcoords, np.float32)[indices]
+    edge_a, edge_b = tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
+    uv_a, uv_b = uv[:, 1] - uv[:, 0], uv[:, 2] - uv[:, 0]
+    det = uv_a[:, 0] * uv_b[:, 1] - uv_a[:, 1] * uv_b[:, 0]
+    ok = np.abs(det) >= 1e-10
+    inv = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0).astype(np.float32)[:, None]
+    tangent = (edge_a * uv_b[:, 1:2] - edge_b * uv_a[:, 1:2]) * inv
+    bitangent = (edge_b * uv_a[:, 0:1] - edge_a * uv_b[:, 0:1]) * inv
+    nv = len(vertices)
+    t_sum = np.zeros((nv, 3), np.float64)
+    b_sum = np.zeros((nv, 3), np.float64)
+    for corner in range(3):
+        ids = indices[ok, corner]
+        for c in range(3):
+            t_sum[:, c] += np.bincount(ids, weights=tangent[ok, c], minlength=nv)
+            b_sum[:, c] += np.bincount(ids, weights=bitangent[ok, c], minlength=nv)
+    t_sum = t_sum.astype(np.float32)
+    b_sum = b_sum.astype(np.float32)
+    n = np.asarray(normals, np.float32)
+    t = t_sum - n * np.sum(n * t_sum, axis=1, keepdims=True)
+    length = np.linalg.norm(t, axis=1)
+    weak = length < 1e-8
+    if np.any(weak):
+        axis = np.where((np.abs(n[weak, 2]) < 0.999)[:, None], np.array([0.0, 0.0, 1.0], np.float32),
+                        np.array([0.0, 1.0, 0.0], np.float32))
+        t[weak] = np.cross(n[weak], axis)
+        length[weak] = np.linalg.norm(t[weak], axis=1)
+    t /= np.maximum(length, 1e-8)[:, None]
+    hand = np.where(np.sum(np.cross(n, t) * b_sum, axis=1) < 0.0, -1.0, 1.0).astype(np.float32)
+    return np.ascontiguousarray(np.column_stack((t, hand)), dtype=np.float32)
 
 
 def _generate_normals(vertices, indices):
@@ -323,6 +437,9 @@ class Mesh:
     name: str | None = None
     metadata: dict = field(default_factory=dict, repr=False)
     deformable: bool = False
+    texcoords: np.ndarray | None = field(default=None, repr=False)
+    texcoords1: np.ndarray | None = field(default=None, repr=False)
+    tangents: np.ndarray | None = field(default=None, repr=False)
     id: int | None = field(default=None, init=False)
 
     def __post_init__(self):
@@ -334,10 +451,8 @@ class Mesh:
             self.transform = Transform(self.transform)
         self.metadata = MappingProxyType(dict(self.metadata))
         if self.resource is not None:
-            self.vertices = self.resource.vertices
-            self.indices = self.resource.indices
-            self.normals = self.resource.normals
-            self.deformable = self.resource.deformable
+            for name in ("vertices", "indices", "normals", "deformable", "texcoords", "texcoords1", "tangents"):
+                setattr(self, name, getattr(self.resource, name))
             return
         self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float32)
         self.indices = np.ascontiguousarray(self.indices, dtype=np.uint32)
@@ -357,12 +472,46 @@ class Mesh:
             if np.any(lengths < 1e-8):
                 raise ValueError("normals cannot contain zero vectors")
             self.normals = n / lengths[:, None]
+        for name in ("texcoords", "texcoords1"):
+            value = getattr(self, name)
+            if value is None:
+                value = np.zeros((len(self.vertices), 2), np.float32)
+            value = np.ascontiguousarray(value, dtype=np.float32)
+            if value.shape != (len(self.vertices), 2):
+                raise ValueError(f"{name} must have shape (vertex_count, 2)")
+            setattr(self, name, value)
+        if self.tangents is None:
+            self.tangents = _generate_tangents(self.vertices, self.indices, self.normals, self.texcoords)
+        else:
+            t = np.array(self.tangents, dtype=np.float32)
+            if t.shape != (len(self.vertices), 4):
+                raise ValueError("tangents must have shape (vertex_count, 4)")
+            lengths = np.linalg.norm(t[:, :3], axis=1)
+            if np.any(lengths < 1e-8):
+                raise ValueError("tangent directions cannot contain zero vectors")
+            t[:, :3] /= lengths[:, None]
+            t[:, 3] = np.where(t[:, 3] < 0.0, -1.0, 1.0)
+            self.tangents = t
 
     @property
     def world_vertices(self):
         linear = self.transform.matrix[:3, :3]
         translation = self.transform.matrix[:3, 3]
         return np.ascontiguousarray(self.vertices @ linear.T + translation, dtype=np.float32)
+
+    @property
+    def world_tangents(self):
+        """Tangents in world space, orthogonal to the world normals, with the
+        handedness flipped by a mirroring transform (scene/_core.py:702-714)."""
+        linear = self.transform.matrix[:3, :3]
+        directions = self.tangents[:, :3] @ linear.T
+        normals = self.world_normals
+        directions -= normals * np.sum(directions * normals, axis=1)[:, None]
+        directions /= np.linalg.norm(directions, axis=1, keepdims=True)
+        handedness = self.tangents[:, 3].copy()
+        if np.linalg.det(linear) < 0.0:
+            handedness *= -1.0
+        return np.ascontiguousarray(np.column_stack((directions, handedness)), dtype=np.float32)
 
     @property
     def world_normals(self):
@@ -383,18 +532,20 @@ class MeshResource:
     name: str | None = None
     metadata: dict = field(default_factory=dict, repr=False)
     deformable: bool = False      # positions may change in place (refit instead of rebuild)
+    texcoords: np.ndarray | None = field(default=None, repr=False)
+    texcoords1: np.ndarray | None = field(default=None, repr=False)
+    tangents: np.ndarray | None = field(default=None, repr=False)
     id: int | None = field(default=None, init=False)
 
     def __post_init__(self):
         if not isinstance(self.deformable, bool):
             raise TypeError("deformable must be a bool")
-        checked = Mesh(self.vertices, self.indices, self.material, normals=self.normals)
-        self.vertices = checked.vertices
-        self.indices = checked.indices
-        self.normals = checked.normals
-        self.vertices.flags.writeable = False
-        self.indices.flags.writeable = False
-        self.normals.flags.writeable = False
+        checked = Mesh(self.vertices, self.indices, self.material, normals=self.normals, texcoords=self.texcoords,
+                       texcoords1=self.texcoords1, tangents=self.tangents)
+        for name in ("vertices", "indices", "normals", "texcoords", "texcoords1", "tangents"):
+            value = getattr(checked, name)
+            value.flags.writeable = False
+            setattr(self, name, value)
 
 
 class Instance(Mesh):
@@ -539,9 +690,10 @@ class Scene:
         return tuple(volume for volume in self.volumes if volume.visible)
 
     def create_mesh(self, vertices, indices, material=None, *, normals=None, name=None, metadata=None,
-                    deformable=False):
+                    deformable=False, texcoords=None, texcoords1=None, tangents=None):
         resource = MeshResource(vertices, indices, material or Material(), normals=normals, name=name,
-                                metadata={} if metadata is None else metadata, deformable=deformable)
+                                metadata={} if metadata is None else metadata, deformable=deformable,
+                                texcoords=texcoords, texcoords1=texcoords1, tangents=tangents)
         self._attach_mesh_resource(resource)
         self.mesh_resources.append(resource)
         return resource
@@ -549,9 +701,10 @@ class Scene:
     create_mesh_resource = create_mesh
 
     def add_mesh(self, vertices, indices, material=None, *, normals=None, transform=None, name=None,
-                 metadata=None, deformable=False):
+                 metadata=None, deformable=False, texcoords=None, texcoords1=None, tangents=None):
         resource = self.create_mesh(vertices, indices, material, normals=normals, name=name, metadata=metadata,
-                                    deformable=deformable)
+                                    deformable=deformable, texcoords=texcoords, texcoords1=texcoords1,
+                                    tangents=tangents)
         return self.add_instance(resource, transform=transform, name=name, metadata=metadata)
 
     def _resolve_resource(self, resource):
