@@ -430,6 +430,17 @@ OLC_API int olc_read_variance(olc_context* ctx, uint32_t width, uint32_t height,
 OLC_API int olc_read_hit_geometry(olc_context* ctx, uint32_t width, uint32_t height,
                                   float* position, float* barycentric);
 
+/* Denoiser path signals of the last olc_render's first sample (the
+ * secondary path state, ordinarylight/wavefront/_core.py:75-87, written by
+ * wavefront_shade.comp:406-410 and :561-568): signals, height*width*4
+ * floats: the specular-lobe probability of the primary hit's material, 1
+ * when that hit is opaque (0 for transmissive hits, misses and medium
+ * events), 0, 0; secondary, height*width*4 floats: the world position of
+ * the path's next surface vertex and 1, or zeros when it has none.  Host
+ * arrays; either may be NULL. */
+OLC_API int olc_read_path_signals(olc_context* ctx, uint32_t width, uint32_t height,
+                                  float* signals, float* secondary);
+
 /* Camera frame of the motion projection (_project_positions,
  * ordinarylight/targets/vulkan/api.py:1118-1136): origin, unit forward,
  * right and up, and tan(vertical fov / 2). */

@@ -167,6 +167,7 @@ _SIGNATURES = {
     "olc_read_variance": ([c_void_p, c_uint32, c_uint32, c_void_p, c_int], c_int),
     "olc_read_hit_geometry": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
     "olc_capture_motion_state": ([c_void_p], c_int),
+    "olc_read_path_signals": ([c_void_p, c_uint32, c_uint32, c_void_p, c_void_p], c_int),
     "olc_sample_texture": ([c_void_p, c_uint32, c_int32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                             c_void_p], c_int),
     "olc_read_motion": ([c_void_p, c_uint32, c_uint32, POINTER(OlcMotionMesh), c_uint32, POINTER(OlcMotionCamera),

@@ -291,7 +291,8 @@ struct olc_context {
   DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
       ps_rad, ps_meta, ps_ior, ps_cone, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
-  DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary;
+  DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary, prod_signals,
+      prod_secondary;
   uint32_t prod_pixels = 0;
   DeviceBuffer srgb_lut;           // 256 sRGB-to-linear values for texture decoding
   DeviceBuffer motion_prev;        // world-space triangles of the motion history frame (3 float4 each)
@@ -1261,6 +1262,8 @@ void ensure_products(olc_context* ctx, uint32_t npix) {
   ctx->prod_prim.allocate(n * 4);
   ctx->prod_pos.allocate(n * 16);
   ctx->prod_bary.allocate(n * 8);
+  ctx->prod_signals.allocate(n * 16);
+  ctx->prod_secondary.allocate(n * 16);
   ctx->prod_pixels = npix;
   drop_graphs(ctx);
 }
@@ -1335,6 +1338,8 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.prod.primitive_id = ctx->prod_prim.as<uint32_t>();
   b.prod.position = ctx->prod_pos.as<float4>();
   b.prod.barycentric = ctx->prod_bary.as<float2>();
+  b.prod.signals = ctx->prod_signals.as<float4>();
+  b.prod.secondary = ctx->prod_secondary.as<float4>();
   b.cnt = ctx->counters.as<Counters>();
   b.accum = ctx->pixels.at<unsigned long long>(0);
   b.out = ctx->pixels.at<float4>(1);
@@ -1411,7 +1416,8 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.ps.cone, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.prod.position,
-                        (const void*)rb.prod.barycentric, (const void*)rb.cnt, (const void*)rb.accum,
+                        (const void*)rb.prod.barycentric, (const void*)rb.prod.signals,
+                        (const void*)rb.prod.secondary, (const void*)rb.cnt, (const void*)rb.accum,
                         (const void*)rb.out, (const void*)rb.sample_lum, (const void*)rb.table, (const void*)ctx->cur->counters_host,
                         (const void*)ctx->cur,
                         ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_b0.get(),
@@ -1861,6 +1867,7 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
                                 &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->ps_cone, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,
+                                &ctx->prod_signals, &ctx->prod_secondary,
                                 &ctx->sample_lum, &ctx->motion_prev, &ctx->restir.res_a0,
                                 &ctx->restir.res_a1, &ctx->restir.res_b0, &ctx->restir.res_b1, &ctx->restir.hist0,
                                 &ctx->restir.hist1, &ctx->restir.selected, &ctx->restir.hit_list})
@@ -2175,6 +2182,19 @@ int olc_read_hit_geometry(olc_context* ctx, uint32_t width, uint32_t height, flo
       position[3 * i + 1] = pos[i].y;
       position[3 * i + 2] = pos[i].z;
     }
+  });
+}
+
+int olc_read_path_signals(olc_context* ctx, uint32_t width, uint32_t height, float* signals, float* secondary) {
+  if (!ctx) return fail(nullptr, OLC_ERR_VALUE, "context is required");
+  return guarded(ctx, [&] {
+    if (width != ctx->last_w || height != ctx->last_h || ctx->last_w == 0)
+      throw Error(OLC_ERR_VALUE, "products are available only for the size of the last render");
+    const size_t n = (size_t)width * height;
+    cudaStream_t st = ctx->stream;
+    if (signals) OLC_CUDA(cudaMemcpyAsync(signals, ctx->prod_signals.get(), n * 16, cudaMemcpyDeviceToHost, st));
+    if (secondary) OLC_CUDA(cudaMemcpyAsync(secondary, ctx->prod_secondary.get(), n * 16, cudaMemcpyDeviceToHost, st));
+    OLC_CUDA(cudaStreamSynchronize(st));
   });
 }
 

@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
       const uint32_t flags = meta.z >> 8;
       const uint32_t out_pixel = meta.x;  // products belong to one plain frame's job
       const bool write_products = job.products && bounce == 0u && meta.y == job.sample_base && a.prod.depth;
+      const bool write_secondary = job.products && bounce == 1u && meta.y == job.sample_base && a.prod.depth;
       uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), bounce);
       uint32_t new_flags = flags & OLC_PATH_DEPTH_MASK;   // the medium stack depth carries over
       float new_pdf = 0.0f;
@@ -365,6 +366,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.primitive_id[out_pixel] = 0xffffffffu;
           a.prod.position[out_pixel] = make_float4(p.x, p.y, p.z, 0.0f);
           a.prod.barycentric[out_pixel] = make_float2(0.0f, 0.0f);
+          a.prod.signals[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          a.prod.secondary[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (next_bounce < job.max_bounces) {
           if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
@@ -399,6 +402,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.primitive_id[out_pixel] = 0xffffffffu;
           a.prod.position[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           a.prod.barycentric[out_pixel] = make_float2(0.0f, 0.0f);
+          a.prod.signals[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          a.prod.secondary[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
       } else {
         const float t = hit.x, bu = hit.y, bv = hit.z;
@@ -424,6 +429,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
           a.prod.primitive_id[out_pixel] = ir.prim_offset + s.tri_index[slot];
           a.prod.position[out_pixel] = make_float4(p.x, p.y, p.z, 0.0f);
           a.prod.barycentric[out_pixel] = make_float2(bu, bv);
+          a.prod.signals[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          a.prod.secondary[out_pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (cpu_mode) {
           // CPU reference transport (path_tracer.py:74-87)
@@ -462,6 +469,13 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             occlusion = th.occlusion;
           }
           const float3 nrm = entering ? ns : -ns;
+          // denoiser path signals (the secondary path state of
+          // wavefront_shade.comp:406-410, :561-568): the specular-lobe
+          // probability of the (textured) primary material and whether it is
+          // opaque, then the position of the path's next surface vertex
+          if (write_products)
+            a.prod.signals[out_pixel] = make_float4(spec_probability(m), m.transmission <= 0.001f ? 1.0f : 0.0f, 0.0f, 0.0f);
+          if (write_secondary) a.prod.secondary[out_pixel] = make_float4(p.x, p.y, p.z, 1.0f);
           // emission with power-heuristic MIS against the previous BSDF pdf
           // (wavefront_shade.comp:412-433)
           if ((entering || m.two_sided) && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f)) {

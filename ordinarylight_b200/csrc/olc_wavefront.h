@@ -62,6 +62,8 @@ struct ProductPtrs {
   uint32_t* primitive_id = nullptr;
   float4* position = nullptr;      // world hit point (xyz)
   float2* barycentric = nullptr;   // (u, v) of the hit in the triangle's index order
+  float4* signals = nullptr;       // specular-lobe probability, opaque (1) or transmissive (0) hit
+  float4* secondary = nullptr;     // hit point of the path's next vertex (xyz), recorded (w = 1)
 };
 
 void configure_trace_kernels();

@@ -71,6 +71,7 @@ class CudaRendererConfig:
     sort_rays: bool = False
     serve_aging_steps: int = 8
     sample_variance: bool = False
+    denoiser_signal_capture: bool = False
 
     def __post_init__(self):
         if not 1 <= int(self.samples_per_pixel) <= 65536:
@@ -373,6 +374,114 @@ class CudaWavefrontRenderer(RendererImplementation):
             self._ctx, _native.DEFAULT_SCENE, int(binding), len(uv0), _native.ptr(uv0), _native.ptr(uv1),
             _native.ptr(fp0), _native.ptr(fp1), 1 if srgb else 0, _native.ptr(out)))
         return out
+
+    # -- denoiser inputs ----------------------------------------------------------
+    def capture_denoiser_raw(self, scene, camera, width, height, *, frame_index=0):
+        """One-sample frame and its denoiser path signals
+        (capture_denoiser_raw, ordinarylight/targets/vulkan/api.py:1453-1582):
+        the radiance is split between a diffuse and a specular channel by the
+        primary material's specular-lobe probability, as the reference's
+        path-to-HDR partition does (not physically separated lobes), and both
+        carry the distance from the primary hit to the path's next surface
+        vertex (0 when it has none).  Needs ``denoiser_signal_capture=True``."""
+        self._require_open()
+        if not self.config.denoiser_signal_capture:
+            raise RuntimeError("capture_denoiser_raw requires denoiser_signal_capture=True")
+        width, height = int(width), int(height)
+        if width < 1 or height < 1:
+            raise ValueError("width and height must be positive")
+        radiance = self.render_frame(scene, camera, width, height, samples=1, frame_index=frame_index)
+        depth = np.empty((height, width), np.float32)
+        normal = np.empty((height, width, 3), np.float32)
+        prim = np.empty((height, width), np.uint32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_products(
+            self._ctx, width, height, _native.ptr(depth), _native.ptr(normal), None, None, _native.ptr(prim)))
+        position, bary = self.hit_geometry(width, height)
+        signals = np.empty((height, width, 4), np.float32)
+        secondary = np.empty((height, width, 4), np.float32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_path_signals(
+            self._ctx, width, height, _native.ptr(signals), _native.ptr(secondary)))
+        resolved = np.maximum(radiance[..., :3], 0.0)
+        captured = signals[..., 1] > 0.5
+        probability = np.where(captured, np.clip(signals[..., 0], 0.0, 1.0), 0.0)[..., None].astype(np.float32)
+        distance = np.zeros((height, width), np.float32)
+        valid = captured & (secondary[..., 3] > 0.5)
+        distance[valid] = np.linalg.norm(secondary[valid, :3] - position[valid], axis=-1)
+        diffuse = np.empty((height, width, 4), np.float32)
+        specular = np.empty((height, width, 4), np.float32)
+        diffuse[..., :3] = resolved * (1.0 - probability)
+        specular[..., :3] = resolved * probability
+        diffuse[..., 3] = distance
+        specular[..., 3] = distance
+        path_state = {"diffuse_radiance_hit_distance": diffuse, "specular_radiance_hit_distance": specular,
+                      "specular_probability": probability[..., 0], "secondary_position": secondary}
+        return {"radiance": radiance, "path_state": path_state, "depth": depth, "normal": normal,
+                "primitive_id": prim, "primary_position": position, "primary_barycentric": bary}
+
+    def capture_denoiser_signals(self, scene, camera, width, height, *, frame_index=0):
+        """Canonical diffuse/specular denoiser inputs of one frame
+        (capture_denoiser_signals, ordinarylight/targets/vulkan/api.py:1584-1660):
+        radiance and hit distance per channel, unit normal and material
+        roughness, linear view depth, motion from the pixel centre to its
+        previous-frame location, material ids, and the frame's matrices."""
+        try:
+            from ordinarylight.denoising import DenoiserFrameInfo, DenoiserSignals
+        except ImportError:
+            from ..denoising import DenoiserFrameInfo, DenoiserSignals
+        from ..denoising import camera_matrix
+
+        raw = self.capture_denoiser_raw(scene, camera, width, height, frame_index=frame_index)
+        width, height = int(width), int(height)
+        prim = raw["primitive_id"]
+        foreground = prim != np.uint32(0xFFFFFFFF)
+        material_id = np.full((height, width), np.uint32(0xFFFFFFFF), np.uint32)
+        ids = np.empty((height, width), np.uint32)
+        _native.check(self._lib, self._ctx, self._lib.olc_read_products(
+            self._ctx, width, height, None, None, None, _native.ptr(ids), None))
+        material_id[foreground] = ids[foreground]
+        normal_roughness = np.zeros((height, width, 4), np.float32)
+        normal_roughness[..., :3] = raw["normal"]
+        lengths = np.linalg.norm(normal_roughness[..., :3], axis=-1)
+        ok = foreground & (lengths > 1e-12)
+        normal_roughness[ok, :3] /= lengths[ok, None]
+        material_id_of = getattr(scene, "material_id", None)
+        meshes = getattr(scene, "render_meshes", None) or scene.visible_meshes
+        for mesh in meshes:
+            if callable(material_id_of):
+                normal_roughness[material_id == material_id_of(mesh.material), 3] = float(mesh.material.roughness)
+        origin = np.asarray(camera.position, np.float64)
+        forward = np.asarray(camera.target, np.float64) - origin
+        forward /= np.linalg.norm(forward)
+        view_z = np.zeros((height, width), np.float32)
+        view_z[foreground] = ((raw["primary_position"][foreground] - origin) @ forward).astype(np.float32)
+        previous = self._output_history
+        compatible = previous is not None and previous["scene"] is scene and previous["size"] == (width, height)
+        motion = self._motion_product(scene, camera, width, height)
+        if compatible:
+            # previous-minus-current from the pixel centre, including the
+            # current ray jitter (api.py:1630-1641)
+            now = self._motion_camera(camera)
+            o = np.asarray(now.origin[:], np.float64)
+            f, r_, u = (np.asarray(getattr(now, k)[:], np.float64) for k in ("forward", "right", "up"))
+            rel = raw["primary_position"].reshape(-1, 3).astype(np.float64) - o
+            dist = rel @ f
+            safe = np.maximum(dist, 1e-12)
+            px = ((rel @ r_) / (safe * now.scale * (width / height)) + 1.0) * 0.5 * width
+            py = (-(rel @ u) / (safe * now.scale) + 1.0) * 0.5 * height
+            yy, xx = np.indices((height, width))
+            projected = np.stack((px.reshape(height, width), py.reshape(height, width)), axis=-1)
+            centres = np.stack((xx, yy), axis=-1) + 0.5
+            motion = (projected - centres - motion).astype(np.float32)
+            motion[~(foreground & (dist.reshape(height, width) > 1e-8))] = 0.0
+        current = camera_matrix(camera, width, height)
+        before = camera_matrix(previous["camera"], width, height) if compatible else current
+        self._capture_motion_state(scene, camera, (width, height))
+        ps = raw["path_state"]
+        return DenoiserSignals(
+            np.ascontiguousarray(ps["diffuse_radiance_hit_distance"], np.float32),
+            np.ascontiguousarray(ps["specular_radiance_hit_distance"], np.float32),
+            normal_roughness, view_z, motion, material_id,
+            DenoiserFrameInfo(current, before, int(frame_index), camera_cut=not compatible))
 
     def hit_geometry(self, width, height):
         """World hit points (h, w, 3) and barycentrics (h, w, 2) of the last
