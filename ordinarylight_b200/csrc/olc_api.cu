@@ -236,8 +236,11 @@ struct RunPlan {
   bool chunk_reservoirs = false;     // some ReSTIR segment uses chunk-local reservoirs
 };
 
+// One timed stage of a run: its events (indices into the run slot's event
+// list) bracket it on the stream it ran on.
 struct TimelineEntry {
   uint32_t stage, bounce, chunk;
+  uint32_t start, end;
 };
 
 struct GraphEntry {
@@ -277,6 +280,13 @@ struct olc_context {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
+  // any-hit traversal of a bounce's shadow rays runs on a second stream,
+  // beside the next bounce's closest-hit traversal, and joins the main
+  // stream before the next shading pass
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_event = nullptr, join_event = nullptr;
+  bool side_pending = false;
+  uint32_t tl_next = 0, tl_last = 0;   // next event index; last event on the main stream
   std::string error;
   BuildScratch scratch;
   LaunchShape ls;
@@ -386,27 +396,42 @@ void drop_graphs(olc_context* ctx) {
   ctx->graphs.clear();
 }
 
-void tl_record(olc_context* ctx, size_t index) {
+// Record the next timeline event on `stream`; returns its index.
+uint32_t tl_record(olc_context* ctx, cudaStream_t stream) {
   RunSlot& sl = *ctx->cur;
+  const uint32_t index = ctx->tl_next++;
   while (sl.events.size() <= index) {
     cudaEvent_t e;
     OLC_CUDA(cudaEventCreate(&e));
     sl.events.push_back(e);
   }
   if (ctx->capturing)
-    OLC_CUDA(cudaEventRecordWithFlags(sl.events[index], ctx->stream, cudaEventRecordExternal));
+    OLC_CUDA(cudaEventRecordWithFlags(sl.events[index], stream, cudaEventRecordExternal));
   else
-    OLC_CUDA(cudaEventRecord(sl.events[index], ctx->stream));
+    OLC_CUDA(cudaEventRecord(sl.events[index], stream));
+  return index;
 }
 
 void tl_begin(olc_context* ctx) {
   ctx->cur->entries.clear();
-  tl_record(ctx, 0);
+  ctx->side_pending = false;
+  ctx->tl_next = 0;
+  ctx->tl_last = tl_record(ctx, ctx->stream);
 }
 
+// A stage that just ran on the main stream.
 void tl_mark(olc_context* ctx, uint32_t stage, uint32_t bounce, uint32_t chunk) {
-  ctx->cur->entries.push_back(TimelineEntry{stage, bounce, chunk});
-  tl_record(ctx, ctx->cur->entries.size());
+  const uint32_t end = tl_record(ctx, ctx->stream);
+  ctx->cur->entries.push_back(TimelineEntry{stage, bounce, chunk, ctx->tl_last, end});
+  ctx->tl_last = end;
+}
+
+// Wait on the main stream for the side stream's pending work.
+void side_join(olc_context* ctx) {
+  if (!ctx->side_pending) return;
+  OLC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0));
+  ctx->side_pending = false;
+  ctx->tl_last = tl_record(ctx, ctx->stream);   // later stages start after the wait
 }
 
 // Inverse of a row-major 3x4 affine (double precision on the host).
@@ -1385,13 +1410,26 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, plan.textures, st);
         tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
+      // shading adds to path radiance and refills the shadow queue: the
+      // previous bounce's shadow rays must be done
+      side_join(ctx);
       launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
                    plan.textures, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
-      launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, st);
-      tl_mark(ctx, OLC_STAGE_SHADOW, b, c);
+      // this bounce's shadow rays on the side stream: they touch only the
+      // shadow queue and path radiance, so the next bounce's closest-hit
+      // traversal runs beside them and fills their tail
+      OLC_CUDA(cudaEventRecord(ctx->fork_event, st));
+      OLC_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_event, 0));
+      const uint32_t side_start = tl_record(ctx, ctx->side);
+      launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, ctx->side);
+      const uint32_t side_end = tl_record(ctx, ctx->side);
+      ctx->cur->entries.push_back(TimelineEntry{OLC_STAGE_SHADOW, b, c, side_start, side_end});
+      OLC_CUDA(cudaEventRecord(ctx->join_event, ctx->side));
+      ctx->side_pending = true;
       std::swap(qin, qout);
     }
+    side_join(ctx);
     launch_accumulate(ctx->ls, hdr, jobs, rb.ps, rb.accum, rb.sample_lum, rb.cnt, st);
     tl_mark(ctx, OLC_STAGE_ACCUMULATE, 0, c);
     OLC_CUDA(cudaMemcpyAsync(ctx->cur->counters_host + c, rb.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -1598,7 +1636,7 @@ void finish_run(olc_context* ctx, RunSlot& sl, olc_render_stats* stats) {
     r.stage = e.stage;
     r.bounce = e.bounce;
     r.chunk = e.chunk;
-    OLC_CUDA(cudaEventElapsedTime(&r.ms, sl.events[k], sl.events[k + 1]));
+    OLC_CUDA(cudaEventElapsedTime(&r.ms, sl.events[e.start], sl.events[e.end]));
     const Counters& kc = sl.counters_host[std::min<uint32_t>(e.chunk, nchunks - 1)];
     switch (e.stage) {
       case OLC_STAGE_RAYGEN: case OLC_STAGE_ACCUMULATE: r.items = plan.chunks[e.chunk].count; break;
@@ -1733,6 +1771,9 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     OLC_CUDA(cudaGetDeviceProperties(&prop, ctx->device));
     ctx->sm_count = prop.multiProcessorCount;
     OLC_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    OLC_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    OLC_CUDA(cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming));
+    OLC_CUDA(cudaEventCreateWithFlags(&ctx->join_event, cudaEventDisableTiming));
     configure_trace_kernels();
     apply_launch_shape(ctx.get());
     // pool record 0: the identity instance that baked triangles report
@@ -1753,6 +1794,9 @@ int olc_create(const olc_config* cfg, olc_context** out) {
   });
   if (rc != OLC_OK) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
+    if (ctx->join_event) cudaEventDestroy(ctx->join_event);
     ctx->stream = nullptr;
     return rc;
   }
@@ -1767,9 +1811,14 @@ int olc_destroy(olc_context* ctx) {
   drop_graphs(ctx);
   restir_release(ctx->restir);
   for (RunSlot& sl : ctx->runs) release_slot(sl);
-  cudaStream_t st = ctx->stream;
+  if (ctx->side) cudaStreamSynchronize(ctx->side);
+  cudaStream_t st = ctx->stream, side = ctx->side;
+  cudaEvent_t fork = ctx->fork_event, join = ctx->join_event;
   delete ctx;  // device buffers are freed here
   if (st) cudaStreamDestroy(st);
+  if (side) cudaStreamDestroy(side);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
   return OLC_OK;
 }
 
