@@ -124,9 +124,11 @@ OLC_D uint32_t pack_bary(float b1, float b2) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// Unshadowed target of light sample (light, bary) at surface s.
-OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary) {
+// Unshadowed target of light sample (light, bary) at surface s; with
+// p_src, also the sample's source pdf per unit area (from the same record).
+OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary, float* p_src = nullptr) {
   const EmitterRec e = load_emitter(sc, light);
+  if (p_src) *p_src = e.normal.w;
   float2 b = unpack_bary(bary);
   float3 off = emitter_point(e, b.x, b.y) - s.p;
   float d2 = dot(off, off);
@@ -284,10 +286,8 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
       float ru = sqrtf(olc_rand(rng));
       float rv = olc_rand(rng);
       uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
-      float t = target_of(s, su, li, bary);
-      const float4 ap = __ldg(&s.emitters[li].a_pdf);
-      const float area = __ldg(&s.emitters[li].e1_area.w);
-      float p_src = ap.w / fmaxf(area, 1e-12f);
+      float p_src;
+      float t = target_of(s, su, li, bary, &p_src);
       float w = p_src > 0.0f ? t / p_src : 0.0f;
       res_update(r, li, bary, t, w, 1u, olc_rand(rng));
     }
