@@ -73,6 +73,26 @@ OLC_D uint32_t segment_of_path(const JobRec* jobs, uint32_t num_segments, uint64
 
 OLC_D float job_t_min(const JobRec& j) { return j.mode == 1u ? 1e-4f : 0.001f; }
 
+// Pixel of index k (0 <= k < w * h) of a sample stream: 8x4-pixel tiles in
+// bands of 4 rows (the band's last w % 8 columns and a last short band in
+// row order), so the 32 consecutive camera rays of a warp cover one tile.
+// A bijection per stream: each pixel still gets exactly one path per sample.
+OLC_D uint32_t stream_pixel(uint32_t k, uint32_t w, uint32_t h) {
+  const uint32_t band_pixels = 4u * w;
+  const uint32_t band = k / band_pixels;
+  const uint32_t y0 = band * 4u;
+  uint32_t r = k - band * band_pixels;
+  if (h - y0 < 4u) return y0 * w + r;
+  const uint32_t full = (w >> 3) * 32u;
+  if (r < full) {
+    const uint32_t tile = r >> 5, within = r & 31u;
+    return (y0 + (within >> 3)) * w + tile * 8u + (within & 7u);
+  }
+  r -= full;
+  const uint32_t rem = w & 7u;
+  return (y0 + r / rem) * w + (w - rem) + r % rem;
+}
+
 __global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs,
                          const SceneRec* __restrict__ scenes, RayQueue q, PathState ps, Counters* cnt) {
   const uint32_t count = hdr->count;
@@ -82,7 +102,8 @@ __global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __re
     const JobRec& job = jobs[j];
     const uint64_t local = job.seg_first + (i - job.seg_begin);
     const uint32_t local_sample = (uint32_t)(local / job.npix);
-    const uint32_t pixel = (uint32_t)(local - (uint64_t)local_sample * job.npix);
+    const uint32_t pixel =
+        stream_pixel((uint32_t)(local - (uint64_t)local_sample * job.npix), job.width, job.height);
     const uint32_t sample = job.sample_base + local_sample;   // the RNG key's sample index
     float3 o, d;
     camera_ray(job, pixel, sample, nullptr, o, d);
@@ -917,7 +938,9 @@ void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQu
                           Counters* cnt, uint32_t bounce, cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
-    if (ls.scheduler == 1)
+    // camera rays come in 8x4-pixel tiles: a warp keeps its 32 coherent rays
+    // to the end instead of refilling lanes with rays of other tiles
+    if (ls.scheduler == 1 || bounce == 0)
       k_trace_closest<D, 1><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, q, h, cnt,
                                                                                                         bounce);
     else
