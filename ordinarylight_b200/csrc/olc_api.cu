@@ -223,6 +223,7 @@ struct ChunkPlan {
   uint32_t count = 0;
   uint32_t bounces = 0;
   bool restir = false;
+  bool textures = false;     // its jobs' scenes have textures (all or none of them)
   std::vector<JobRec> segs;
 };
 
@@ -232,7 +233,6 @@ struct RunPlan {
   uint32_t max_segments = 0;
   uint32_t max_count = 0;
   bool restir = false;               // some chunk runs ReSTIR
-  bool textures = false;             // some job's scene has textures
   bool chunk_reservoirs = false;     // some ReSTIR segment uses chunk-local reservoirs
 };
 
@@ -1208,6 +1208,9 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
     uint64_t fill = 0;
     for (QueuedJob* j : jobs) {
       if (j->issued >= j->total) continue;
+      // textured and untextured jobs never share a chunk: each chunk runs
+      // one kernel variant, so a job's bits do not depend on its company
+      if (!takes.empty() && j->textured != takes.front().job->textured) continue;
       const uint64_t left = cap - fill;
       if (left == 0) break;
       uint64_t take;
@@ -1246,8 +1249,8 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
       at += t.count;
     }
     ch.count = (uint32_t)fill;
+    ch.textures = takes.front().job->textured;
     plan.restir = plan.restir || ch.restir;
-    for (const Take& t : takes) plan.textures = plan.textures || t.job->textured;
     plan.max_segments = std::max<uint32_t>(plan.max_segments, (uint32_t)ch.segs.size());
     plan.max_count = std::max<uint32_t>(plan.max_count, ch.count);
     plan.chunks.push_back(std::move(ch));
@@ -1407,14 +1410,14 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
       if (b == 0 && ch.restir) {
-        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, plan.textures, st);
+        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, ch.textures, st);
         tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
       // shading adds to path radiance and refills the shadow queue: the
       // previous bounce's shadow rays must be done
       side_join(ctx);
       launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
-                   plan.textures, st);
+                   ch.textures, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       // this bounce's shadow rays on the side stream: they touch only the
       // shadow queue and path radiance, so the next bounce's closest-hit
@@ -1444,8 +1447,8 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
 std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
   std::vector<uint64_t> k;
   k.push_back(plan.chunks.size());
-  for (const ChunkPlan& c : plan.chunks) k.push_back(((uint64_t)c.bounces << 1) | (c.restir ? 1u : 0u));
-  k.push_back(plan.textures ? 1u : 0u);
+  for (const ChunkPlan& c : plan.chunks)
+    k.push_back(((uint64_t)c.bounces << 2) | (c.textures ? 2u : 0u) | (c.restir ? 1u : 0u));
   auto ptr = [&](const void* p) { k.push_back((uint64_t)(uintptr_t)p); };
   const SceneView s = pool_view(ctx);
   const void* const* sv = reinterpret_cast<const void* const*>(&s);

@@ -132,3 +132,28 @@ def test_base_metallic_roughness_and_normal_maps_under_a_directional_light(nativ
                                         light.intensity)
     assert ok.mean() > 0.5
     np.testing.assert_allclose(img[..., :3].reshape(-1, 3)[ok], expected[ok], rtol=3e-3, atol=2e-5)
+
+
+def test_textured_and_untextured_scenes_mix_in_one_batch(native_library, cuda_device):
+    """A run with a textured scene uses the textured kernel variants for all
+    of its jobs; an untextured job's image must still equal its plain frame
+    (rendered with the untextured variants) bit for bit."""
+    from ordinarylight_b200 import scenes
+    from ordinarylight_b200.renderers.cuda import RenderRequest
+
+    rng = np.random.default_rng(3)
+    tex = ol.Texture(_texture(rng, 16, 16))
+    textured, tcam = _textured_floor(dict(base_color=(0.9, 0.9, 0.9), roughness=0.6, base_color_texture=tex))
+    textured.set_environment(ol.EnvironmentLight(color=(0.6, 0.7, 0.9), intensity=1.0))
+    plain_scene, pcam = scenes.instanced_spheres(seed=7, instances=6, segments=24, bands=13, emitters=32,
+                                                 extent=5.0)
+    reqs = [RenderRequest(textured, tcam, 48, 40, samples=2, frame_index=1, max_bounces=4),
+            RenderRequest(plain_scene, pcam, 64, 48, samples=2, frame_index=2, max_bounces=4)]
+    for restir in (False, True):
+        with CudaWavefrontRenderer(max_bounces=4, restir=restir) as r:
+            batch = r.render_batch(reqs)
+        for req, img in zip(reqs, batch):
+            with CudaWavefrontRenderer(max_bounces=4, restir=restir) as p:
+                ref = p.render_frame(req.scene, req.camera, req.width, req.height, samples=req.samples,
+                                     frame_index=req.frame_index)
+            assert img.tobytes() == ref.tobytes()
