@@ -18,8 +18,9 @@ triangles under an equirect environment, where a path is deterministic:
   bounce limit ends dark.
 
 ``trace`` also reports, per ray, whether every step stayed clear of
-triangle edges and environment texel borders (where float rounding may pick
-the other side), so a test compares only robust pixels.
+triangle edges, environment texel borders and the critical angle of total
+internal reflection (where float rounding may pick the other side), so a
+test compares only robust pixels.
 """
 
 from __future__ import annotations
@@ -27,10 +28,12 @@ from __future__ import annotations
 import numpy as np
 
 
-def _hits(origins, dirs, tris):
-    """Closest hit (t > 1e-4) of each ray by brute force: t, index, u, v."""
+def _hits(origins, dirs, tris, second=False):
+    """Closest hit (t > 1e-4) of each ray by brute force: t, index, u, v
+    (and, with second=True, the distance of the next-closest hit)."""
     n = len(origins)
     best_t = np.full(n, np.inf)
+    next_t = np.full(n, np.inf)
     best = np.full(n, -1, np.int64)
     bu = np.zeros(n)
     bv = np.zeros(n)
@@ -45,17 +48,21 @@ def _hits(origins, dirs, tris):
         q = np.cross(s, e1)
         v = np.sum(dirs * q, axis=1) * inv
         t = (q @ e2) * inv
-        hit = ok & (u >= 0) & (v >= 0) & (u + v <= 1) & (t > 1e-4) & (t < best_t)
+        valid = ok & (u >= 0) & (v >= 0) & (u + v <= 1) & (t > 1e-4)
+        hit = valid & (t < best_t)
+        next_t = np.where(hit, best_t, np.where(valid, np.minimum(next_t, t), next_t))
         best_t[hit], best[hit], bu[hit], bv[hit] = t[hit], k, u[hit], v[hit]
+    if second:
+        return best_t, best, bu, bv, next_t
     return best_t, best, bu, bv
 
 
-def _refract(d, n, eta):
+def _refract(d, n, eta, with_k=False):
     ni = np.sum(n * d, axis=1)
     k = 1.0 - eta * eta * (1.0 - ni * ni)
     out = eta[:, None] * d - (eta * ni + np.sqrt(np.maximum(k, 0.0)))[:, None] * n
     out[k < 0.0] = 0.0
-    return out
+    return (out, k) if with_k else out
 
 
 def _environment(dirs, image, color, rotation, margin):
@@ -71,7 +78,7 @@ def _environment(dirs, image, color, rotation, margin):
 
 
 def trace(origins, dirs, tris, transmission, ior, base, env_image, env_color=(1.0, 1.0, 1.0), env_rotation=0.0,
-          max_bounces=16, max_depth=9, edge_margin=1e-3, texel_margin=2e-3):
+          max_bounces=16, max_depth=16, edge_margin=1e-3, texel_margin=2e-3, critical_margin=1e-3):
     """Radiance of each ray and whether its path is robust.  tris (N, 3, 3)
     world space; transmission, ior (N,) and base (N, 3) per triangle."""
     o = np.asarray(origins, np.float64).copy()
@@ -91,7 +98,9 @@ def trace(origins, dirs, tris, transmission, ior, base, env_image, env_color=(1.
         idx = np.flatnonzero(alive)
         if not len(idx):
             break
-        t, k, u, v = _hits(o[idx], d[idx], tris)
+        t, k, u, v, t2 = _hits(o[idx], d[idx], tris, second=True)
+        gap = np.where(np.isfinite(t2), t2 - np.where(np.isfinite(t), t, 0.0), np.inf)
+        robust[idx] &= (gap > 1e-4 * np.maximum(np.where(np.isfinite(t), t, 1.0), 1.0)) | (k < 0)   # no near-tie
         miss = k < 0
         if np.any(miss):
             mi = idx[miss]
@@ -115,7 +124,8 @@ def trace(origins, dirs, tris, transmission, ior, base, env_image, env_color=(1.
         current = stack[hi, dep - 1]
         below = np.where(dep > 1, stack[hi, np.maximum(dep - 2, 0)], 1.0)
         target = np.where(entering, np.maximum(ior[k], 1.0001), below)
-        w = _refract(di, nrm, current / target)
+        w, k_disc = _refract(di, nrm, current / target, with_k=True)
+        robust[hi] &= np.abs(k_disc) > critical_margin      # not at the critical angle
         tir = np.sum(w * w, axis=1) < 0.01
         w[tir] = di[tir] - 2.0 * np.sum(nrm[tir] * di[tir], axis=1)[:, None] * nrm[tir]
         push = ~tir & entering & (dep < max_depth)

@@ -1278,7 +1278,7 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   ctx->sh_c.allocate(c * 16);
   ctx->ps_tp.allocate(c * 16);
   ctx->ps_rad.allocate(c * 16);
-  ctx->ps_ior.allocate(c * 32);
+  ctx->ps_ior.allocate(c * 64);
   ctx->ps_cone.allocate(c * 8);
   ctx->ps_meta.allocate(c * 16);
   ctx->capacity = capacity;

@@ -293,7 +293,7 @@ struct PathState {
   float4* throughput;      // rgb, previous BSDF pdf
   float4* radiance;        // rgb, unused
   uint4* meta;             // pixel, sample, bounce | flags << 8, job
-  float4* ior_stack;       // 2 per path: indices of refraction of the media entered, entries 1..8
+  float4* ior_stack;       // 4 per path: indices of refraction of the media entered, entries 1..15
   float2* cone;            // ray cone (width, spread) of the path's next ray; textured scenes only
 };
 
@@ -303,7 +303,7 @@ struct PathState {
 // metadata.w >> 8, wavefront_shade.comp:447); entry 0 is the outside, IOR 1.
 #define OLC_PATH_DEPTH_SHIFT 4u
 #define OLC_PATH_DEPTH_MASK (15u << OLC_PATH_DEPTH_SHIFT)
-#define OLC_MAX_MEDIUM_DEPTH 9u       // entry 0 plus the 8 stored ones
+#define OLC_MAX_MEDIUM_DEPTH 16u      // entry 0 plus the 15 stored ones (the reference's depth)
 
 // Fixed-point scale of the per-pixel radiance accumulator.  Sums of
 // non-negative samples in unsigned 64-bit fixed point are independent of the

@@ -30,12 +30,12 @@ OLC_D uint32_t lane_id() { return threadIdx.x & 31u; }
 // Entry k of a path's medium stack (entry 0 is the outside, IOR 1).
 OLC_D float medium_ior(const float4* stack, uint32_t path, uint32_t k) {
   if (k == 0u) return 1.0f;
-  const float4 v = stack[2ull * path + ((k - 1u) >> 2)];
+  const float4 v = stack[4ull * path + ((k - 1u) >> 2)];
   const uint32_t c = (k - 1u) & 3u;
   return c == 0u ? v.x : c == 1u ? v.y : c == 2u ? v.z : v.w;
 }
 OLC_D void set_medium_ior(float4* stack, uint32_t path, uint32_t k, float ior) {
-  float* v = reinterpret_cast<float*>(stack + 2ull * path + ((k - 1u) >> 2));
+  float* v = reinterpret_cast<float*>(stack + 4ull * path + ((k - 1u) >> 2));
   v[(k - 1u) & 3u] = ior;
 }
 
