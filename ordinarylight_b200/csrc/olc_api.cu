@@ -291,7 +291,7 @@ struct olc_context {
   BuildScratch scratch;
   LaunchShape ls;
   // scene pool
-  PoolGroup nodes{{sizeof(BvhNode)}, 4096};
+  PoolGroup nodes{{sizeof(BvhNode), sizeof(BvhNode4)}, 4096};
   PoolGroup slots{{3 * sizeof(float4), 3 * sizeof(float4), sizeof(uint32_t), sizeof(uint32_t)}, 4096};
   PoolGroup instances{{sizeof(InstanceRec)}, 256};
   PoolGroup materials{{sizeof(MaterialRec), sizeof(MaterialAux)}, 64};
@@ -476,6 +476,7 @@ void upload_to(T* dst, const T* host, size_t count, cudaStream_t stream) {
 SceneView pool_view(const olc_context* ctx) {
   SceneView v{};
   v.nodes = ctx->nodes.at<BvhNode>(0);
+  v.wide = ctx->nodes.at<BvhNode4>(1);
   v.tri_verts = ctx->slots.at<float4>(0);
   v.tri_normals = ctx->slots.at<float4>(1);
   v.tri_index = ctx->slots.at<uint32_t>(2);
@@ -850,6 +851,8 @@ void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScen
   const uint32_t tlas_root =
       build_tlas(d_o2w.as<float>(), d_ranges.as<uint2>(), L.members, max_tris, inst0, tri_verts, tri_verts + 3ull * flat_slot0,
                  (uint32_t)L.flat_tris, flat_slot0, ctx->scratch, nodes, node0 + L.tlas_local, st);
+  // traversal reads the BVH4 form of every BLAS and of the TLAS
+  build_bvh4(nodes, ctx->nodes.at<BvhNode4>(1), node0, (uint32_t)rs.nodes.n, st);
 
   // ---- materials, emitters, lights
   std::vector<MaterialRec> mats(d->num_materials);

@@ -880,11 +880,73 @@ uint32_t build_tlas(const float* o2w, const uint2* slot_ranges, uint32_t n, uint
   return node_base;
 }
 
+// ---- BVH4 form --------------------------------------------------------------
+namespace {
+OLC_D void set_lane(float4& v, int k, float x) {
+  if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
+}
+OLC_D void set_lane(int4& v, int k, int x) {
+  if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
+}
+// Append child `which` of BVH2 node `parent` (box from the parent) as slot k.
+OLC_D void put_child(BvhNode4& w, int& k, const BvhNode& parent, int which, int ref) {
+  const float lx = which ? parent.b.x : parent.a.x, hx = which ? parent.b.y : parent.a.y;
+  const float ly = which ? parent.b.z : parent.a.z, hy = which ? parent.b.w : parent.a.w;
+  const float lz = which ? parent.c.z : parent.c.x, hz = which ? parent.c.w : parent.c.y;
+  set_lane(w.lox, k, lx); set_lane(w.hix, k, hx);
+  set_lane(w.loy, k, ly); set_lane(w.hiy, k, hy);
+  set_lane(w.loz, k, lz); set_lane(w.hiz, k, hz);
+  set_lane(w.child, k, ref);
+  ++k;
+}
+
+// BVH4 node of BVH2 node i: its children in order, each internal child
+// replaced by that child's own two children.  Internal children outside
+// [begin, end) (the nodes of an unbuilt mesh in a scene's node range) are
+// left out, so no fetch leaves the range.
+OLC_D BvhNode4 bvh4_of(const BvhNode* __restrict__ nodes, uint32_t i, uint32_t begin, uint32_t end) {
+  BvhNode4 w;
+  w.lox = w.hix = w.loy = w.hiy = w.loz = w.hiz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  w.child = make_int4(OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD);
+  w.reserved = make_int4(0, 0, 0, 0);
+  const BvhNode nd = nodes[i];
+  int k = 0;
+  for (int c = 0; c < 2; ++c) {
+    const int ref = c ? nd.d.y : nd.d.x;
+    if (ref == OLC_EMPTY_CHILD) continue;
+    if (ref < 0) {
+      put_child(w, k, nd, c, ref);
+    } else if ((uint32_t)ref >= begin && (uint32_t)ref < end) {
+      const BvhNode cn = nodes[ref];
+      for (int g = 0; g < 2; ++g) {
+        const int gref = g ? cn.d.y : cn.d.x;
+        if (gref != OLC_EMPTY_CHILD) put_child(w, k, cn, g, gref);
+      }
+    }
+  }
+  return w;
+}
+
+__global__ void k_bvh4(const BvhNode* __restrict__ nodes, BvhNode4* __restrict__ wide, uint32_t begin,
+                       uint32_t count) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  wide[begin + t] = bvh4_of(nodes, begin + t, begin, begin + count);
+}
+}  // namespace
+
+void build_bvh4(const BvhNode* nodes, BvhNode4* wide, uint32_t begin, uint32_t count, cudaStream_t stream) {
+  if (count == 0) return;
+  k_bvh4<<<blocks_for(count), kThreads, 0, stream>>>(nodes, wide, begin, count);
+  OLC_LAUNCH_CHECK("k_bvh4");
+}
+
 // ---- validation ----------------------------------------------------------
 namespace {
 // Walk each built BLAS from its root; count how often each slot is reached,
-// leaves outside the BLAS's own slot range, and child boxes that do not lie
-// inside the box stored for them in the parent.
+// leaves outside the BLAS's own slot range, child boxes that do not lie
+// inside the box stored for them in the parent, and BVH4 nodes that differ
+// from the collapse of their BVH2 node.
 __global__ void k_validate(SceneView s, const BlasRange* ranges, uint32_t count, uint32_t* slot_hits,
                            unsigned long long* bad) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -900,6 +962,16 @@ __global__ void k_validate(SceneView s, const BlasRange* ranges, uint32_t count,
     }
     int node = stack[--sp];
     if (node < 0) continue;
+    {
+      // the BVH4 form must be current: equal to the collapse of this node
+      const BvhNode4 want = bvh4_of(s.nodes, (uint32_t)node, 0u, 0x7fffffffu);
+      const BvhNode4 have = s.wide[node];
+      const int* a = reinterpret_cast<const int*>(&want);
+      const int* h = reinterpret_cast<const int*>(&have);
+      bool same = true;
+      for (int k = 0; k < 28; ++k) same = same && a[k] == h[k];   // six box float4 and the child refs
+      if (!same) atomicAdd(bad, 1ull);
+    }
     BvhNode nd = s.nodes[node];
     int ch[2] = {nd.d.x, nd.d.y};
     for (int c = 0; c < 2; ++c) {

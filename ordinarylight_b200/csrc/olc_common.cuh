@@ -141,6 +141,19 @@ OLC_HD uint32_t olc_leaf_first(int ref) { return ((uint32_t)(~ref)) >> 3; }
 OLC_HD uint32_t olc_leaf_count(int ref) { return (((uint32_t)(~ref)) & 7u) + 1u; }
 #define OLC_EMPTY_CHILD ((int)0x80000000)
 
+// BVH4 node, 128 bytes (one L2 line, seven 16-byte loads): the four
+// grandchildren of BVH2 node i (a leaf child stands for itself), stored at
+// index i of a second array parallel to the BVH2 nodes.  Traversal descends
+// two BVH2 levels per dependent fetch.  Child references keep the BVH2
+// encoding, and an internal child's index is its BVH2 index, so roots,
+// instance records and leaves are shared by both forms.  Box slot k of the
+// six float4 is child k; unused slots hold OLC_EMPTY_CHILD.
+struct __align__(16) BvhNode4 {
+  float4 lox, hix, loy, hiy, loz, hiz;
+  int4 child;
+  int4 reserved;
+};
+
 // Instance record, 128 bytes: world->object 3x4 and identity/offsets (the
 // 64 bytes traversal reads), then object->world 3x4 for shading, then flags.
 //
@@ -256,6 +269,7 @@ struct __align__(16) SceneRec {
 // different scenes and each ray needs only its scene's TLAS root.
 struct SceneView {
   const BvhNode* nodes;          // BLAS and TLAS nodes
+  const BvhNode4* wide;          // their BVH4 form, same indices (traversal reads only these)
   const float4* tri_verts;       // 3 float4 per triangle slot (object space)
   const float4* tri_normals;     // 3 float4 per triangle slot (object space)
   const uint32_t* tri_index;     // slot -> mesh-local triangle index (packed index for baked triangles)

@@ -4,6 +4,9 @@
 // (nativeTraceSurface, ordinarylight/shaders/wavefront_intersect.comp:96-235;
 // nativeOccluded in ordinarylight/shaders/transport_v1/lighting.glsl).
 // * TLAS and BLAS nodes share one node pool; a TLAS leaf is one instance.
+//   Traversal reads the BVH4 form of the pool (BvhNode4: the four
+//   grandchildren of a BVH2 node in one 128-byte line), so each dependent
+//   fetch descends two levels of the binary hierarchy.
 //   Entering an instance transforms the ray to object space (t is preserved
 //   because the direction is not renormalised) and pushes a marker that
 //   restores the world ray when the instance's subtree is exhausted.
@@ -135,34 +138,29 @@ OLC_D void load_instance_w2o(const InstanceRec* inst, uint32_t i, Affine& w2o, u
   prim_offset = m.z;
 }
 
-// Intersect both child boxes of a node with the current ray.
-OLC_D void node_boxes(const BvhNode* nodes, int node, const TraceRay& r, float t_min, float t_max,
-                      bool& hit0, bool& hit1, float& near0, float& near1, int& c0, int& c1) {
-  const float4* p = reinterpret_cast<const float4*>(nodes + node);
-  float4 a = __ldg(p + 0);
-  float4 b = __ldg(p + 1);
-  float4 c = __ldg(p + 2);
-  int4 d = __ldg(reinterpret_cast<const int4*>(p + 3));
-  const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
-  const float ox = r.oinv.x, oy = r.oinv.y, oz = r.oinv.z;
-  float l0x = __fmaf_rn(a.x, ix, -ox), h0x = __fmaf_rn(a.y, ix, -ox);
-  float l0y = __fmaf_rn(a.z, iy, -oy), h0y = __fmaf_rn(a.w, iy, -oy);
-  float l0z = __fmaf_rn(c.x, iz, -oz), h0z = __fmaf_rn(c.y, iz, -oz);
-  float l1x = __fmaf_rn(b.x, ix, -ox), h1x = __fmaf_rn(b.y, ix, -ox);
-  float l1y = __fmaf_rn(b.z, iy, -oy), h1y = __fmaf_rn(b.w, iy, -oy);
-  float l1z = __fmaf_rn(c.z, iz, -oz), h1z = __fmaf_rn(c.w, iz, -oz);
-  float n0 = fmaxf(fmaxf(fminf(l0x, h0x), fminf(l0y, h0y)), fmaxf(fminf(l0z, h0z), t_min));
-  float f0 = fminf(fminf(fmaxf(l0x, h0x), fmaxf(l0y, h0y)), fminf(fmaxf(l0z, h0z), t_max));
-  float n1 = fmaxf(fmaxf(fminf(l1x, h1x), fminf(l1y, h1y)), fmaxf(fminf(l1z, h1z), t_min));
-  float f1 = fminf(fminf(fmaxf(l1x, h1x), fmaxf(l1y, h1y)), fminf(fmaxf(l1z, h1z), t_max));
-  // Conservative far bound (robust traversal, Ize 2013): a few ulps of slack
-  // so rounding in the slab test never culls a box the ray touches.
-  c0 = d.x;
-  c1 = d.y;
-  hit0 = (n0 <= f0 * 1.0000004f) && (c0 != OLC_EMPTY_CHILD);
-  hit1 = (n1 <= f1 * 1.0000004f) && (c1 != OLC_EMPTY_CHILD);
-  near0 = n0;
-  near1 = n1;
+// Slab test of one child box (Kay and Kajiya) with the conservative far
+// bound of robust traversal (Ize 2013): a few ulps of slack so rounding in
+// the slab test never culls a box the ray touches.
+OLC_D bool child_box(float lx, float hx, float ly, float hy, float lz, float hz, int child, const TraceRay& r,
+                     float t_min, float t_max, float& near_t) {
+  const float l_x = __fmaf_rn(lx, r.inv.x, -r.oinv.x), h_x = __fmaf_rn(hx, r.inv.x, -r.oinv.x);
+  const float l_y = __fmaf_rn(ly, r.inv.y, -r.oinv.y), h_y = __fmaf_rn(hy, r.inv.y, -r.oinv.y);
+  const float l_z = __fmaf_rn(lz, r.inv.z, -r.oinv.z), h_z = __fmaf_rn(hz, r.inv.z, -r.oinv.z);
+  const float n = fmaxf(fmaxf(fminf(l_x, h_x), fminf(l_y, h_y)), fmaxf(fminf(l_z, h_z), t_min));
+  const float f = fminf(fminf(fmaxf(l_x, h_x), fmaxf(l_y, h_y)), fminf(fmaxf(l_z, h_z), t_max));
+  near_t = n;
+  return (n <= f * 1.0000004f) && (child != OLC_EMPTY_CHILD);
+}
+
+// One compare-exchange of a sorting network over (key, child) pairs.
+OLC_D void order_pair(float& ka, int& ca, float& kb, int& cb) {
+  const bool swap = kb < ka;
+  const float k = swap ? kb : ka;
+  const int c = swap ? cb : ca;
+  kb = swap ? ka : kb;
+  cb = swap ? ca : cb;
+  ka = k;
+  ca = c;
 }
 
 // Resumable traversal of the two-level structure.  ANY_HIT stops at the
@@ -212,19 +210,45 @@ struct Traversal {
         return true;
       }
       if (node >= 0 && node != OLC_MARKER) {
-        bool h0, h1;
-        float n0, n1;
-        int c0, c1;
-        node_boxes(s.nodes, node, ray, t_min, hit.t, h0, h1, n0, n1, c0, c1);
-        if (h0 && h1) {
-          int near_c = (n0 <= n1) ? c0 : c1;
-          int far_c = (n0 <= n1) ? c1 : c0;
-          st.push(far_c, err);
-          node = near_c;
+        // BVH4 node: test the four child boxes, descend into the nearest
+        // hit child and push the others, farthest first (closest hit) or in
+        // slot order (any hit, where the order changes nothing but time).
+        const float4* p = reinterpret_cast<const float4*>(s.wide + node);
+        const float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3);
+        const float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
+        const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
+        float n0, n1, n2, n3;
+        const bool h0 = child_box(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, ch.x, ray, t_min, hit.t, n0);
+        const bool h1 = child_box(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, ch.y, ray, t_min, hit.t, n1);
+        const bool h2 = child_box(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, ch.z, ray, t_min, hit.t, n2);
+        const bool h3 = child_box(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, ch.w, ray, t_min, hit.t, n3);
+        const int hits = (int)h0 + (int)h1 + (int)h2 + (int)h3;
+        if (hits == 0) {
+          // nothing to enter: fall through to the pop
+        } else if (ANY_HIT) {
+          int next = OLC_EMPTY_CHILD;
+          if (h3) next = ch.w;
+          if (h2) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.z; }
+          if (h1) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.y; }
+          if (h0) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.x; }
+          node = next;
+          continue;
+        } else {
+          // misses sort last (+inf); a hit's key is finite
+          float k0 = h0 ? fminf(n0, 3.0e38f) : CUDART_INF_F, k1 = h1 ? fminf(n1, 3.0e38f) : CUDART_INF_F;
+          float k2 = h2 ? fminf(n2, 3.0e38f) : CUDART_INF_F, k3 = h3 ? fminf(n3, 3.0e38f) : CUDART_INF_F;
+          int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+          order_pair(k0, c0, k1, c1);
+          order_pair(k2, c2, k3, c3);
+          order_pair(k0, c0, k2, c2);
+          order_pair(k1, c1, k3, c3);
+          order_pair(k1, c1, k2, c2);
+          if (hits > 3) st.push(c3, err);
+          if (hits > 2) st.push(c2, err);
+          if (hits > 1) st.push(c1, err);
+          node = c0;
           continue;
         }
-        if (h0) { node = c0; continue; }
-        if (h1) { node = c1; continue; }
       } else if (node != OLC_MARKER) {
         uint32_t first = olc_leaf_first(node);
         uint32_t count = olc_leaf_count(node);
