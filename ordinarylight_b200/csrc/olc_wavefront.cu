@@ -205,9 +205,12 @@ __global__ void __launch_bounds__(256) k_trace_closest(SceneView s, RayQueue q, 
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
 
+// 72 registers: any-hit traversal fits them without spilling (79 uncapped),
+// which gives 7 instead of 6 blocks of 128 threads per SM (measured 2 %
+// faster shadow rays; the closest-hit kernel spills under the same cap).
 template <int STACK, int SCHED>
-__global__ void __launch_bounds__(256) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
-                                                      uint32_t bounce) {
+__global__ void __maxnreg__(72) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
+                                               uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->shadow_count[bounce];
   uint32_t err = 0;
