@@ -171,16 +171,24 @@ class ClockSampler:
         self.index = str(index)
         self.proc = None
         self.lines = []
+        self.skip = 0    # samples taken before the timed region started
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-i", self.index, "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", self.index, "-lms", "100"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait for its first sample so
+        # that the samples cover the whole timed region after this returns
+        deadline = time.perf_counter() + 5.0
+        while not self.lines and self.proc.poll() is None and time.perf_counter() < deadline:
+            time.sleep(0.01)
+        self.skip = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -197,7 +205,7 @@ class ClockSampler:
         self.thread.join(timeout=2)
         sm, mx, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in self.lines:
+        for line in self.lines[self.skip:]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -391,7 +399,11 @@ def run_ours(args, rank, world, device_index):
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": _traffic_from_profiles(dominant),
-                     "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
+                     "limiter": ("dependent-load latency and SIMD divergence, not HBM: BVH traversal with the "
+                                 "instanced scene in L2 (ncu: 68-87 % L2 hits, 8-17 of 32 lanes active, "
+                                 "~3 long-scoreboard stalls per issue; profiles/hot_kernels_instanced_640x360.md)")
+                     if dominant == "trace_closest" else None},
         "stages": stages,
         "gpu_launches": launches,
         "clocks": clock_info,
@@ -677,7 +689,7 @@ def run_reference_arm(args):
 def main():
     p = argparse.ArgumentParser(description=__doc__)
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--cpu-steps", type=int, default=1)

@@ -28,6 +28,9 @@
 #include "olc_common.cuh"
 
 #define OLC_SPILL 96
+// Shared words per thread beyond the stack: the world ray's derived terms,
+// saved on entering an instance and restored on leaving it.
+#define OLC_RAY_SAVE 10
 #define OLC_MARKER 0x7fffffff
 #define OLC_TRAVERSAL_BUDGET (1u << 22)
 
@@ -93,6 +96,25 @@ OLC_D bool intersect_triangle(const TraceRay& r, float3 v0, float3 v1, float3 v2
   b1 = V * rcp;
   b2 = W * rcp;
   return true;
+}
+
+// Save / restore the terms setup_ray derives from (o, d): the slab
+// reciprocals, the shear permutation and constants.  `w` is this thread's
+// column (stride threads).
+OLC_D void save_ray(float* w, int stride, const TraceRay& r) {
+  w[0 * stride] = r.inv.x; w[1 * stride] = r.inv.y; w[2 * stride] = r.inv.z;
+  w[3 * stride] = r.oinv.x; w[4 * stride] = r.oinv.y; w[5 * stride] = r.oinv.z;
+  w[6 * stride] = r.sx; w[7 * stride] = r.sy; w[8 * stride] = r.sz;
+  w[9 * stride] = __int_as_float(r.kx | (r.ky << 2) | (r.kz << 4));
+}
+OLC_D void restore_ray(const float* w, int stride, TraceRay& r, float3 o, float3 d) {
+  r.o = o;
+  r.d = d;
+  r.inv = f3(w[0 * stride], w[1 * stride], w[2 * stride]);
+  r.oinv = f3(w[3 * stride], w[4 * stride], w[5 * stride]);
+  r.sx = w[6 * stride]; r.sy = w[7 * stride]; r.sz = w[8 * stride];
+  const int k = __float_as_int(w[9 * stride]);
+  r.kx = k & 3; r.ky = (k >> 2) & 3; r.kz = (k >> 4) & 3;
 }
 
 struct HitResult {
@@ -179,11 +201,13 @@ struct Traversal {
   uint32_t cur_inst, cur_prim_offset;
   uint32_t budget;
   bool found;
+  float* save;         // this thread's column of OLC_RAY_SAVE shared words
   TraversalStack<STACK> st;
 
   OLC_D void begin(const SceneView& s, float3 o, float3 d, float tmin, float tmax, uint32_t tlas_root,
                    int* smem_base, int* spill_area) {
     st.init(smem_base, threadIdx.x, blockDim.x, spill_area);
+    save = reinterpret_cast<float*>(smem_base + STACK * blockDim.x) + threadIdx.x;
     wo = o;
     wd = d;
     t_min = tmin;
@@ -283,14 +307,13 @@ struct Traversal {
           uint32_t root;
           load_instance_w2o(s.instances, first, w2o, root, cur_prim_offset);
           cur_inst = first;
-          setup_ray(ray, xform_point(w2o, wo), xform_vector(w2o, wd));
-          level = 1;
           if (st.push(OLC_MARKER, err)) {
+            save_ray(save, st.stride, ray);
+            setup_ray(ray, xform_point(w2o, wo), xform_vector(w2o, wd));
+            level = 1;
             node = (int)root;
             continue;
           }
-          level = 0;
-          setup_ray(ray, wo, wd);
         } else {
           for (uint32_t k = 0; k < count; ++k) {
             uint32_t slot = first + k;
@@ -324,7 +347,7 @@ struct Traversal {
       node = st.pop();
       if (node == OLC_MARKER) {
         level = 0;
-        setup_ray(ray, wo, wd);
+        restore_ray(save, st.stride, ray, wo, wd);
         if (st.sp == 0) return true;
         node = st.pop();
       }

@@ -926,7 +926,7 @@ void dispatch_stack(uint32_t depth, F&& f) {
 
 inline size_t stack_bytes(uint32_t depth, uint32_t threads) {
   uint32_t d = depth <= 16 ? 16 : (depth <= 24 ? 24 : 32);
-  return (size_t)d * threads * sizeof(int);
+  return (size_t)(d + OLC_RAY_SAVE) * threads * sizeof(int);
 }
 
 }  // namespace
