@@ -515,7 +515,8 @@ void build_emitters(const olc_scene_desc* d, std::vector<EmitterRec>& em, std::v
     em[i].e1_area = make_float4(e1.x, e1.y, e1.z, r[15]);
     em[i].e2_sided = make_float4(e2.x, e2.y, e2.z, r[18] > 0.5f ? 1.0f : 0.0f);
     em[i].normal = make_float4(nrm.x, nrm.y, nrm.z, pdf / fmaxf(r[15], 1e-12f));
-    em[i].emission = make_float4(r[12], r[13], r[14], 0.0f);
+    const float area = fmaxf(r[15], 1e-12f);
+    em[i].emission = make_float4(r[12], r[13], r[14], pdf > 0.0f ? area / pdf : 0.0f);
     p[i] = pdf;
     total += pdf;
   }

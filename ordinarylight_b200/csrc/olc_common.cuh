@@ -198,7 +198,7 @@ struct __align__(16) EmitterRec {
   float4 e1_area;          // b - a, area
   float4 e2_sided;         // c - a, two-sided flag (0/1)
   float4 normal;           // unit normal of cross(e1, e2), area-measure source pdf (probability / area)
-  float4 emission;         // rgb, 0
+  float4 emission;         // rgb, reciprocal of the source pdf (area / probability; 0 if never selected)
 };
 
 // Walker/Vose alias table entry over the emitter power distribution: O(1)

@@ -125,10 +125,12 @@ OLC_D uint32_t pack_bary(float b1, float b2) {
 }
 
 // Unshadowed target of light sample (light, bary) at surface s; with
-// p_src, also the sample's source pdf per unit area (from the same record).
-OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary, float* p_src = nullptr) {
+// inv_src, also the reciprocal of the sample's source pdf per unit area
+// (from the same record).
+OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary,
+                      float* inv_src = nullptr) {
   const EmitterRec e = load_emitter(sc, light);
-  if (p_src) *p_src = e.normal.w;
+  if (inv_src) *inv_src = e.emission.w;
   float2 b = unpack_bary(bary);
   float3 off = emitter_point(e, b.x, b.y) - s.p;
   float d2 = dot(off, off);
@@ -283,12 +285,15 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
     uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream);
     for (uint32_t c = 0; c < a.candidates; ++c) {
       uint32_t li = select_emitter(s, sc, olc_rand(rng));
-      float ru = sqrtf(olc_rand(rng));
+      // the square root's last bits do not survive the half-precision
+      // barycentrics, so the hardware reciprocal square root serves
+      const float u0 = olc_rand(rng);
+      float ru = u0 > 0.0f ? u0 * rsqrtf(u0) : 0.0f;
       float rv = olc_rand(rng);
       uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
-      float p_src;
-      float t = target_of(s, su, li, bary, &p_src);
-      float w = p_src > 0.0f ? t / p_src : 0.0f;
+      float inv_src;
+      float t = target_of(s, su, li, bary, &inv_src);
+      float w = t * inv_src;
       res_update(r, li, bary, t, w, 1u, olc_rand(rng));
     }
     // temporal reuse
