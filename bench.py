@@ -93,43 +93,60 @@ def _cpu_worker_init():
     os.environ["MKL_NUM_THREADS"] = "1"
     from ordinarylight_b200 import scenes
 
+    from oracle import reference_path_tracer as ref
+
     scene, camera = scenes.instanced_spheres()
     _CPU_STATE["triangles"] = scene.triangles()
-    _CPU_STATE["camera"] = camera
+    # the frame's camera rays (one jittered sample per pixel), made once
+    _CPU_STATE["rays"] = ref.camera_rays(camera, WIDTH, HEIGHT, np.random.default_rng(1000))
 
 
 def _cpu_tile(args):
     """Closest-hit rays of one tile of the workload's first bounce, traced by
-    the oracle's brute-force intersector (path_tracer.py:154-176)."""
-    tile, size = args
+    the oracle's brute-force intersector (path_tracer.py:154-176) against a
+    contiguous block of `count` of the scene's triangles.  That intersector
+    loops over triangles with every ray of the call in one numpy vector, so
+    its time is the same for every triangle: the block's time, scaled by
+    (all triangles / count), is the time of the whole scene.  Returns
+    (rays, scaled seconds)."""
+    tile, size, count = args
     from oracle import reference_path_tracer as ref
 
     tris = _CPU_STATE["triangles"][0]
-    camera = _CPU_STATE["camera"]
-    rng = np.random.default_rng(1000 + tile)
-    o, d = ref.camera_rays(camera, WIDTH, HEIGHT, rng)
+    o, d = _CPU_STATE["rays"]
     tiles_x = WIDTH // size
     tx, ty = tile % tiles_x, (tile // tiles_x) % (HEIGHT // size)
     sel = ((np.arange(HEIGHT)[:, None] // size == ty) & (np.arange(WIDTH)[None, :] // size == tx)).reshape(-1)
+    count = max(1, min(int(count), len(tris)))
+    first = (tile * 7919 * count) % (len(tris) - count + 1)
     counter = ref.RayCounter()
     t0 = time.perf_counter()
-    ref.intersect(o[sel], d[sel], tris, counter)
-    return counter.rays, time.perf_counter() - t0
+    ref.intersect(o[sel], d[sel], tris[first:first + count], counter)
+    return counter.rays, (time.perf_counter() - t0) * (len(tris) / count)
 
 
 class CpuReference:
-    """Pool of spawn workers, each holding the workload's triangle soup."""
+    """Pool of spawn workers, each holding the workload's triangle soup.
 
-    def __init__(self, processes=None, tile=8):
+    A step traces one tile x tile block of camera rays per process (64 x 64 =
+    4,096 rays: the batch at which the reference's per-ray cost is lowest;
+    fewer rays pay the per-triangle loop overhead for few rays, more rays
+    leave the caches) against `triangles` of the scene's triangles, timed
+    and scaled to all of them."""
+
+    def __init__(self, processes=None, tile=64, triangles=32768):
         import multiprocessing as mp
 
         self.processes = processes or os.cpu_count() or 1
         self.tile = tile
+        self.triangles = triangles
         self.pool = mp.get_context("spawn").Pool(self.processes, initializer=_cpu_worker_init)
         self.step = 0
 
-    def run_step(self):
-        jobs = [(self.step * self.processes + k, self.tile) for k in range(self.processes)]
+    def run_step(self, triangles=None):
+        if triangles is not None:
+            self.triangles = triangles
+        jobs = [(self.step * self.processes + k, self.tile, self.triangles) for k in range(self.processes)]
         self.step += 1
         results = self.pool.map(_cpu_tile, jobs)
         rays = sum(r for r, _ in results)
@@ -141,9 +158,10 @@ class CpuReference:
         self.pool.join()
 
     def describe(self, steps):
-        return (f"first bounce (camera rays) of {self.processes} {self.tile}x{self.tile}-pixel tiles per step at "
-                f"1 spp, {steps} step(s), brute-force intersection over all 1,049,602 triangles as the CPU "
-                "reference does; one process per core, slowest process timed")
+        return (f"first bounce (camera rays) at 1 spp: per step, one {self.tile}x{self.tile}-pixel tile per process "
+                f"traced by brute force as the CPU reference does, timed against a block of {self.triangles:,} "
+                f"of the 1,049,602 triangles and scaled to all of them (the reference's loop costs the same per "
+                f"triangle); {steps} step(s), one process per core, slowest process timed")
 
 
 def cpu_reference_measure(steps, processes=None):
@@ -649,12 +667,23 @@ def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit
             "speedup_mrays_vs_plain_resident": summary["mrays_per_s"] / plain["mrays_per_s"]}
 
 
+# Seconds of CPU work the reference arm's timed steps take together.
+REFERENCE_BUDGET_S = 120.0
+
+
 def run_reference_arm(args):
     steps = args.steps
     ref = CpuReference(args.cpu_processes)
     try:
-        for _ in range(args.warmup):
-            ref.run_step()
+        # short warm-up steps start the pool and measure the time per
+        # triangle; the timed steps' triangle blocks are sized from it so
+        # that all of them together take about REFERENCE_BUDGET_S
+        warm = 1024
+        per_triangle = 1e-3
+        for _ in range(max(args.warmup, 1)):
+            _rays, secs = ref.run_step(triangles=warm)
+            per_triangle = max(secs / 1049602, 1e-7)   # seconds per triangle (secs is scaled to all of them)
+        ref.triangles = int(max(warm, min(1049602, REFERENCE_BUDGET_S / (steps * per_triangle))))
         total_rays, total_s = 0, 0.0
         for _ in range(steps):
             rays, secs = ref.run_step()
