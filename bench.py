@@ -667,7 +667,7 @@ def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit
             "speedup_mrays_vs_plain_resident": summary["mrays_per_s"] / plain["mrays_per_s"]}
 
 
-# Seconds of CPU work the reference arm's timed steps take together.
+# Seconds of CPU work the reference arm's timed steps take together (default).
 REFERENCE_BUDGET_S = 120.0
 
 
@@ -677,13 +677,14 @@ def run_reference_arm(args):
     try:
         # short warm-up steps start the pool and measure the time per
         # triangle; the timed steps' triangle blocks are sized from it so
-        # that all of them together take about REFERENCE_BUDGET_S
+        # that all of them together take about the budget
+        budget = args.reference_seconds
         warm = 1024
         per_triangle = 1e-3
         for _ in range(max(args.warmup, 1)):
             _rays, secs = ref.run_step(triangles=warm)
             per_triangle = max(secs / 1049602, 1e-7)   # seconds per triangle (secs is scaled to all of them)
-        ref.triangles = int(max(warm, min(1049602, REFERENCE_BUDGET_S / (steps * per_triangle))))
+        ref.triangles = int(max(warm, min(1049602, budget / (steps * per_triangle))))
         total_rays, total_s = 0, 0.0
         for _ in range(steps):
             rays, secs = ref.run_step()
@@ -723,6 +724,8 @@ def main():
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--cpu-processes", type=int, default=None)
+    p.add_argument("--reference-seconds", type=float, default=REFERENCE_BUDGET_S,
+                   help="CPU seconds the reference arm's timed steps take together")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--width", type=int, default=WIDTH, help="image width (a smaller case for profiling)")
     p.add_argument("--height", type=int, default=HEIGHT, help="image height (a smaller case for profiling)")
