@@ -9,12 +9,15 @@
 //   fetch descends two levels of the binary hierarchy.
 //   Entering an instance transforms the ray to object space (t is preserved
 //   because the direction is not renormalised) and pushes a marker that
-//   restores the world ray when the instance's subtree is exhausted.
+//   restores the world ray when the instance's subtree is exhausted; the
+//   world ray's derived terms are kept meanwhile in OLC_RAY_SAVE shared
+//   words per thread instead of being recomputed.
 // * The traversal stack lives in shared memory (STACK entries per thread,
 //   entry k of thread t at k * blockDim.x + t, so a warp's pushes hit 32
-//   distinct banks); deeper entries spill to a bounded local array.  A push
-//   beyond both is counted as a traversal error instead of writing out of
-//   bounds.
+//   distinct banks), followed by the saved world-ray words in the same
+//   column layout; a launch gives (STACK + OLC_RAY_SAVE) * blockDim.x words.
+//   Deeper entries spill to a bounded local array.  A push beyond both is
+//   counted as a traversal error instead of writing out of bounds.
 // * Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013):
 //   the edge functions are evaluated without FMA contraction so that an edge
 //   shared by two triangles gets exactly negated values, with a double
