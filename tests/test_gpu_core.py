@@ -149,6 +149,48 @@ def test_camera_rays_follow_the_reference_camera_model(renderer):
     np.testing.assert_array_equal(o, np.repeat(pos[None].astype(np.float32), w * h, axis=0))
 
 
+def _expected_rays(camera, w, h, jx, jy):
+    """The reference camera model (path_tracer.py:110-151) in float64 with
+    the device's jitter: orthographic origins on the image plane along the
+    forward direction; panoramic yaw and pitch proportional to NDC."""
+    import ordinarylight_b200 as ol
+
+    pos, fwd, right, up = (np.asarray(v, np.float64) for v in _basis(camera))
+    ys, xs = np.divmod(np.arange(w * h), w)
+    ndc_x = (xs + jx.astype(np.float64)) / w * 2.0 - 1.0
+    ndc_y = 1.0 - (ys + jy.astype(np.float64)) / h * 2.0
+    if isinstance(camera, ol.OrthographicCamera):
+        half = camera.vertical_size * 0.5
+        origins = pos + ndc_x[:, None] * (w / h * half) * right + ndc_y[:, None] * half * up
+        dirs = np.repeat((fwd / np.linalg.norm(fwd))[None], w * h, axis=0)
+    else:
+        yaw = ndc_x * math.radians(camera.horizontal_fov_degrees) * 0.5
+        pitch = ndc_y * math.radians(camera.vertical_fov_degrees) * 0.5
+        dirs = (np.cos(pitch)[:, None] * np.cos(yaw)[:, None] * fwd + np.cos(pitch)[:, None] * np.sin(yaw)[:, None]
+                * right + np.sin(pitch)[:, None] * up)
+        dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+        origins = np.repeat(pos[None], w * h, axis=0)
+    return origins, dirs
+
+
+@pytest.mark.parametrize("kind", ["orthographic", "panoramic"])
+def test_orthographic_and_panoramic_rays_follow_the_reference_camera_model(renderer, kind):
+    import ordinarylight_b200 as ol
+
+    if kind == "orthographic":
+        camera = ol.OrthographicCamera(position=(0.3, 1.2, -4.0), target=(0.0, 0.5, 0.0), vertical_size=3.0)
+    else:
+        camera = ol.PanoramicCamera(position=(0.3, 1.2, -4.0), target=(0.0, 0.5, 0.0),
+                                    horizontal_fov_degrees=300.0, vertical_fov_degrees=150.0)
+    w, h = 64, 48
+    o, d = renderer.camera_rays(camera, w, h, sample=3, frame_index=5)
+    jx, jy = sampling.camera_jitter(np.arange(w * h, dtype=np.uint32), 3, 1 + 5)
+    origins, dirs = _expected_rays(camera, w, h, jx, jy)
+    # float32 device arithmetic (sinf/cosf, products of unit vectors)
+    np.testing.assert_allclose(d, dirs, atol=1e-5)
+    np.testing.assert_allclose(o, origins, atol=2e-5)
+
+
 def _basis(camera):
     from ordinarylight_b200.packing import camera_basis
 
