@@ -1,5 +1,5 @@
 """The oracle against the reference's own outputs (tests/golden/, written by
-make_golden.py from the reference at /root/reference).  CPU only."""
+the make_*golden.py scripts from the reference checkout).  CPU only."""
 
 from __future__ import annotations
 
@@ -132,3 +132,38 @@ def test_volume_oracle_monte_carlo_absorber_matches_analytic():
                           max_bounces=2, seed=3)
     expected = np.exp(-1.6)
     assert abs(rad[:, 0].mean() - expected) < 4.0 * np.sqrt(expected * (1 - expected) / n)
+
+
+def _lights_from_table(ol, table):
+    """The lights of analytic_lights.npz's table: rows of (kind, position,
+    direction, color, intensity, range (0: none), inner, outer angle), kind 0
+    point, 1 directional, 2 spot."""
+    lights = []
+    for row in table:
+        kind = int(row[0])
+        pos, direction, color = tuple(row[1:4]), tuple(row[4:7]), tuple(row[7:10])
+        intensity, rng_range, inner, outer = float(row[10]), float(row[11]), float(row[12]), float(row[13])
+        rng_range = rng_range if rng_range > 0.0 else None
+        if kind == 0:
+            lights.append(ol.PointLight(position=pos, color=color, intensity=intensity, range=rng_range))
+        elif kind == 1:
+            lights.append(ol.DirectionalLight(direction=direction, color=color, intensity=intensity))
+        else:
+            lights.append(ol.SpotLight(position=pos, direction=direction, color=color, intensity=intensity,
+                                       inner_cone_angle=inner, outer_cone_angle=outer, range=rng_range))
+    return lights
+
+
+def test_analytic_light_records_match_reference_analytic_light_data(golden):
+    """Point, directional and spot lights (ranges, unnormalised directions,
+    cone angles) pack to the reference's Scene.analytic_light_data records
+    (tests/golden/make_light_golden.py ran the reference on the same lights)."""
+    import ordinarylight_b200 as ol
+
+    data = golden("analytic_lights.npz")
+    scene = ol.Scene()
+    for light in _lights_from_table(ol, data["table"]):
+        scene.add_light(light)
+    records = packing.light_records(scene)
+    assert records.shape == (len(data["table"]), 16)
+    np.testing.assert_array_equal(records.reshape(-1, 4, 4), data["records"])
