@@ -14,7 +14,10 @@ per second).
 * ``roofline``: the dominant kernel's algorithmic bytes per launch over its
   average event-timed launch duration, against MEASURED_PEAKS.json.
 * ``cpu_baseline``: the oracle restatement of CpuReferenceRenderer on a
-  bounded sample of the same scene, all host cores.
+  bounded sample of the same scene, all host cores: per process one
+  64x64-pixel tile of camera rays (4,096 rays, the reference's cheapest
+  batch) against a block of the triangles, its time scaled to all of them
+  (the reference's loop over triangles costs the same per triangle).
 * ``served``: the served form on a Poisson request stream over 8 resident
   scenes of 10k-8M triangles (p50/p99 latency, throughput, rejections),
   beside the plain path serving the same stream one request at a time.
@@ -25,7 +28,9 @@ per second).
   (reference-compatible mode, closest-hit rays) and the terrain with its
   delta-tracked volume.
 
-``--impl reference`` times that CPU reference alone (rank 0).
+``--impl reference`` times that CPU reference alone (rank 0), its timed
+steps sized from short warm-up steps to take about ``--reference-seconds``
+together.
 For N > 1 (torchrun), every rank renders its own frames (weak scaling, no
 data-path collective); the step time is the max over ranks, and only the
 headline section runs.
