@@ -307,7 +307,8 @@ def run_ours(args, rank, world, device_index):
     _native.check(renderer._lib, renderer._ctx, renderer._lib.olc_stream(renderer._ctx, ctypes.byref(handle)))
     stream = torch.cuda.ExternalStream(handle.value, device=f"cuda:{device_index}")
     frame0 = 1000 * rank
-    # warm-up (also builds the BVH and captures nothing: ReSTIR frames run uncaptured)
+    # warm-up: uploads the scene, builds its hierarchy and captures the frame's run into a CUDA graph,
+    # which the timed frames replay
     for k in range(args.warmup):
         renderer.render_frame_into(scene, camera, width, height, out, frame_index=frame0 + k)
     torch.cuda.synchronize()

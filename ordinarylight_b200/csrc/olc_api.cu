@@ -1142,7 +1142,8 @@ void check_camera(const olc_camera* cam) {
 void check_size(uint32_t w, uint32_t h, uint32_t spp) {
   if (w == 0 || h == 0) throw Error(OLC_ERR_VALUE, "width and height must be positive");
   if ((uint64_t)w * h > (1ull << 28)) throw Error(OLC_ERR_VALUE, "image is too large");
-  if (spp < 1 || spp > 65536) throw Error(OLC_ERR_VALUE, "samples must be between 1 and 65536");
+  // the accumulator's clamp keeps a pixel's sum below 2^63 up to this many samples
+  if (spp < 1 || spp > OLC_MAX_FRAME_SAMPLES) throw Error(OLC_ERR_VALUE, "samples must be between 1 and 65536");
 }
 
 JobRec make_job(const olc_context* ctx, const olc_camera* cam, uint32_t w, uint32_t h, uint32_t spp,

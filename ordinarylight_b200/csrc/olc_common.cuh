@@ -323,9 +323,16 @@ struct PathState {
 // non-negative samples in unsigned 64-bit fixed point are independent of the
 // order of the atomic additions, so every launch shape, chunking and batch
 // mix produces the same bits.
+//
+// Each sample's channel is clamped to [0, 2^19 - 1] before scaling, so one
+// sample adds below 2^47 and a pixel's sum over the largest frame accepted
+// (65,536 = 2^16 samples, also when its sample range is split into shards)
+// stays below 2^63: it fits an unsigned 64-bit word and also the signed
+// 64-bit tensors the multi-GPU all-reduce adds, without wrapping.
 #define OLC_ACCUM_SHIFT 28
 #define OLC_ACCUM_SCALE 268435456.0f
-#define OLC_SAMPLE_CLAMP 1.0e7f
+#define OLC_SAMPLE_CLAMP 524287.0f
+#define OLC_MAX_FRAME_SAMPLES 65536u
 
 // One segment of a render job inside a chunk: the job's camera, image,
 // samples, transport knobs and scene, plus where this segment's paths sit in

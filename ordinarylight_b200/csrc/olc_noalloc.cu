@@ -17,7 +17,10 @@
 //   held until the process exits.
 // * The first call on a device looks up the array's device address
 //   (cudaGetSymbolAddress) with that device current; make that first call
-//   before any stream capture on the device.
+//   before any stream capture on the device.  The address is cached per
+//   CUDA context, so after the context is torn down (cudaDeviceReset) the
+//   next call on that device looks it up again instead of reusing a
+//   dangling address; make that call, too, outside any capture.
 // * Every call on a device shares the one array and it keeps the last call's
 //   contents.  Nothing in it needs to start at zero: the histogram and both
 //   ping-pong arrays are fully rewritten by each pass before they are read.
@@ -39,21 +42,50 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_lock;
-uint32_t* g_scratch_address[kMaxDevices] = {};
+struct ScratchAddress {
+  void* context = nullptr;      // the CUDA context the address belongs to
+  uint32_t* address = nullptr;
+};
+ScratchAddress g_scratch[kMaxDevices];
 
-// Device address of the scratch array on the current device, looked up once
-// per device.
+// cuCtxGetCurrent, reached through the runtime so that the library does not
+// link the driver library itself (it must load on machines without a GPU).
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* entry = nullptr;
+    cudaDriverEntryPointQueryResult found;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &entry, cudaEnableDefault, &found) != cudaSuccess ||
+        found != cudaDriverEntryPointSuccess)
+      entry = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(entry);
+  }();
+  return fn;
+}
+
+// Device address of the scratch array in the current device's context,
+// looked up once per device and context.  A thread on which the runtime has
+// not yet made a context current gets one from the symbol lookup itself
+// (cudaGetSymbolAddress initialises the device's primary context).
 uint32_t* scratch_on_current_device() {
   int device = 0;
   OLC_CUDA(cudaGetDevice(&device));
   if (device < 0 || device >= kMaxDevices) throw olc::Error(OLC_ERR_VALUE, "device ordinal out of range");
+  CtxGetCurrentFn get = ctx_get_current();
+  if (!get) throw olc::Error(OLC_ERR_CUDA, "cuCtxGetCurrent is not available from the CUDA driver");
   std::lock_guard<std::mutex> lock(g_setup_lock);
-  if (!g_scratch_address[device]) {
+  void* context = nullptr;
+  if (get(&context) != 0) throw olc::Error(OLC_ERR_CUDA, "the current CUDA context could not be determined");
+  ScratchAddress& entry = g_scratch[device];
+  if (!context || entry.context != context || !entry.address) {
     void* ptr = nullptr;
     OLC_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    g_scratch_address[device] = static_cast<uint32_t*>(ptr);
+    if (get(&context) != 0 || !context)
+      throw olc::Error(OLC_ERR_CUDA, "the current CUDA context could not be determined");
+    entry.context = context;
+    entry.address = static_cast<uint32_t*>(ptr);
   }
-  return g_scratch_address[device];
+  return entry.address;
 }
 
 }  // namespace

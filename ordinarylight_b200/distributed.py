@@ -20,6 +20,8 @@ from __future__ import annotations
 import numpy as np
 
 ACCUM_SCALE = 268435456.0   # 2^28, the device accumulator's fixed-point scale
+SAMPLE_CLAMP = 524287.0     # 2^19 - 1, the device's per-sample clamp of each channel
+MAX_FRAME_SAMPLES = 65536   # samples of one frame, over all shards: sums stay below 2^63
 
 
 def sample_shard(samples: int, world: int, rank: int) -> tuple[int, int]:
@@ -63,6 +65,9 @@ def render_frame_sharded(renderer, scene, camera, width: int, height: int, *, sa
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     spp = renderer.config.samples_per_pixel if samples is None else int(samples)
+    if not 1 <= spp <= MAX_FRAME_SAMPLES:
+        # the signed 64-bit all-reduce stays exact only up to this many samples per pixel
+        raise ValueError(f"samples must be between 1 and {MAX_FRAME_SAMPLES}")
     first, count = sample_shard(spp, world, rank)
     device = torch.device(renderer.device)
     sums = torch.zeros((int(height), int(width), 3), dtype=torch.int64, device=device)
@@ -76,4 +81,4 @@ def render_frame_sharded(renderer, scene, camera, width: int, height: int, *, sa
     return resolve_sums(sums, spp)
 
 
-__all__ = ["ACCUM_SCALE", "sample_shard", "resolve_sums", "render_frame_sharded"]
+__all__ = ["ACCUM_SCALE", "SAMPLE_CLAMP", "MAX_FRAME_SAMPLES", "sample_shard", "resolve_sums", "render_frame_sharded"]

@@ -1,6 +1,8 @@
 """Generate the golden fixtures of tests/golden/ by running the REFERENCE.
 
-Imports OrdinaryLight from /root/reference (read-only) with three stub
+Imports OrdinaryLight from a reference checkout (read-only; ``--reference
+PATH``, else the ``OL_REFERENCE_ROOT`` environment variable, else a
+``reference`` directory beside this repository) with three stub
 modules for its un-vendored dependencies (``ordinaryshade``, ``pygltflib`` and
 the material compiler ``ordinarylight.materials.shade``, none of which the
 CPU reference renderer uses), builds the benchmark scenes through the
@@ -21,7 +23,7 @@ computes:
                            standard error of the mean
 The reference is not available where the GPU tests run; these files are.
 
-Run:  python tests/golden/make_golden.py [--skip-converged]
+Run:  python tests/golden/make_golden.py [--reference PATH] [--skip-converged]
 """
 
 from __future__ import annotations
@@ -35,9 +37,22 @@ import types
 
 import numpy as np
 
-REFERENCE = Path("/root/reference")
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
+
+
+def reference_root() -> Path:
+    """The reference checkout: ``--reference PATH`` on the command line, else
+    ``OL_REFERENCE_ROOT``, else ``reference`` beside this repository."""
+    if "--reference" in sys.argv:
+        return Path(sys.argv[sys.argv.index("--reference") + 1]).resolve()
+    if os.environ.get("OL_REFERENCE_ROOT"):
+        return Path(os.environ["OL_REFERENCE_ROOT"]).resolve()
+    return REPO.parent / "reference"
+
+
+def reference_available() -> bool:
+    return (reference_root() / "ordinarylight" / "__init__.py").exists()
 
 
 def import_reference():
@@ -63,8 +78,11 @@ def import_reference():
     shade.compile_material = lambda *a, **k: None
     shade.compile_dispatch = lambda *a, **k: None
     sys.modules["ordinarylight.materials.shade"] = shade
-    if str(REFERENCE) not in sys.path:
-        sys.path.insert(0, str(REFERENCE))
+    root = reference_root()
+    if not reference_available():
+        raise RuntimeError(f"no OrdinaryLight checkout at {root}; pass --reference PATH or set OL_REFERENCE_ROOT")
+    if str(root) not in sys.path:
+        sys.path.insert(0, str(root))
     import ordinarylight as ol
     import ordinarylight.renderers.reference.cpu  # noqa: F401
 

@@ -75,6 +75,33 @@ def test_noalloc_sort_matches_the_allocating_sort_on_two_calls(native_library, c
         np.testing.assert_array_equal(got[1], np.argsort(keys, kind="stable").astype(np.uint32))
 
 
+@pytest.mark.parametrize("n,bits", [(1, 8), (2, 24), (2047, 8), (2047, 24), (2048, 24), (5000, 16)])
+def test_noalloc_sort_on_a_side_stream_with_odd_pass_counts(native_library, cuda_device, n, bits):
+    """Key widths of 8 and 24 bits take one and three digit passes, so the
+    sorted pairs end in the scratch array and are copied back; sizes at and
+    below one 2,048-key tile; the call is ordered on a side stream that is
+    not the default one.  Against a stable host sort."""
+    import torch
+
+    from ordinarylight_b200 import _native
+
+    rng = np.random.default_rng(n * 31 + bits)
+    pool = rng.integers(0, 1 << bits, size=max(2, n // 4), dtype=np.uint64)     # repeated keys test stability
+    keys = rng.choice(pool, size=n).astype(np.uint32)
+    values = rng.permutation(n).astype(np.uint32)
+    side = torch.cuda.Stream()
+    k = torch.as_tensor(keys.view(np.int32).copy(), device="cuda")
+    v = torch.as_tensor(values.view(np.int32).copy(), device="cuda")
+    torch.cuda.synchronize()
+    status = native_library.olc_radix_sort_pairs_noalloc(n, bits, _native.ptr(k), _native.ptr(v),
+                                                         ctypes.c_void_p(side.cuda_stream))
+    _native.check(native_library, None, status)
+    side.synchronize()
+    order = np.argsort(keys, kind="stable")
+    np.testing.assert_array_equal(k.cpu().numpy().view(np.uint32), keys[order])
+    np.testing.assert_array_equal(v.cpu().numpy().view(np.uint32), values[order])
+
+
 def test_noalloc_sort_rejects_requests_beyond_its_limit(native_library, cuda_device):
     from ordinarylight_b200 import _native
 
