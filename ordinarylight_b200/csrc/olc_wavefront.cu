@@ -258,12 +258,15 @@ struct ShadeArgs {
 // p_area = 0.5 when the scene has both.  At a surface vertex the BSDF and the
 // cosine weight the light (MIS against the BSDF pdf); at a medium vertex
 // (`medium`) the isotropic phase function does (MIS against 1 / (4 pi)).
-// Returns false when the sample contributes nothing.
+// With `lights_only` only the analytic lights are sampled (a ReSTIR vertex,
+// whose emitter light comes from its reservoir).  Returns false when the
+// sample contributes nothing.
 OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& m, float3 p, float3 nrm, float3 view,
                       float3 tp, bool medium, uint32_t& rng, float3& sh_o, float3& sh_d, float& sh_tmax,
-                      float3& sh_c) {
+                      float3& sh_c, bool lights_only = false) {
   constexpr float kPhase = 0.25f / OLC_PI;
-  const float p_area = sc.num_emitters > 0u ? (sc.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
+  const float p_area =
+      (sc.num_emitters > 0u && !lights_only) ? (sc.num_lights > 0u ? 0.5f : 1.0f) : 0.0f;
   const float choose = olc_rand(rng);
   float3 c = f3(0.0f, 0.0f, 0.0f);
   float3 ldir;
@@ -550,8 +553,18 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             if (bounce == 0u && job.restir && a.restir != nullptr && sc.num_emitters > 0u) {
               uint4 rs = a.restir[path];
               did_restir = true;
-              float Wr = __uint_as_float(rs.z);
-              if (rs.x != 0xffffffffu && Wr > 0.0f) {
+              // A scene that also has analytic lights: one of the two
+              // estimators runs, the reservoir's emitter sample or one
+              // analytic light, each with probability 1/2 and its
+              // contribution divided by that probability.
+              const bool with_lights = job.nee && sc.num_lights > 0u;
+              const bool use_reservoir = !with_lights || olc_rand(rng) < 0.5f;
+              const float pick = with_lights ? 2.0f : 1.0f;
+              float Wr = __uint_as_float(rs.z) * pick;
+              if (!use_reservoir) {
+                want_shadow = next_event(s, sc, m, p, nrm, view, tp, false, rng, sh_o, sh_d, sh_tmax, sh_c, true);
+                sh_c *= pick;
+              } else if (rs.x != 0xffffffffu && Wr > 0.0f) {
                 const EmitterRec e = load_emitter(s, rs.x);
                 float2 bary = __half22float2(*reinterpret_cast<const __half2*>(&rs.y));
                 float3 lp = emitter_point(e, bary.x, bary.y);

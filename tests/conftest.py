@@ -9,8 +9,9 @@ import pytest
 
 REPO = Path(__file__).resolve().parents[1]
 GOLDEN = REPO / "tests" / "golden"
-if str(REPO) not in sys.path:
-    sys.path.insert(0, str(REPO))
+for path in (REPO, REPO / "tests"):
+    if str(path) not in sys.path:
+        sys.path.insert(0, str(path))
 
 
 def pytest_configure(config):
@@ -22,7 +23,10 @@ def native_library():
     """Build (if stale) and load libolcuda.so."""
     from ordinarylight_b200 import _native, build
 
+    from oracle import production
+
     build.build()
+    production.build()
     return _native.load()
 
 
