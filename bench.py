@@ -13,14 +13,17 @@ per second).
   per-step device->host image copy), timed by the host clock.
 * ``roofline``: the dominant kernel's algorithmic bytes per launch over its
   average event-timed launch duration, against MEASURED_PEAKS.json.
-* ``cpu_baseline``: the oracle restatement of CpuReferenceRenderer on a
-  bounded sample of the same scene, all host cores: per process one
-  64x64-pixel tile of camera rays (4,096 rays, the reference's cheapest
-  batch) against a block of the triangles, its time scaled to all of them
-  (the reference's loop over triangles costs the same per triangle).
-* ``served``: the served form on a Poisson request stream over 8 resident
-  scenes of 10k-8M triangles (p50/p99 latency, throughput, rejections),
-  beside the plain path serving the same stream one request at a time.
+* ``cpu_baseline``: the oracle restatement of CpuReferenceRenderer on all
+  host cores, rendering config 2 scaled for its brute-force intersector
+  (4 x 1,280-tri spheres, 5,138 tris) in full: camera rays and every
+  extension segment of 8 bounces, nothing extrapolated; ``scaled_c2`` is the
+  CUDA renderer on that scene with the same transport.
+* ``served``: the served form on Poisson request streams of 5-200 req/s over
+  8 resident scenes of 10k-8M triangles (p50/p99 latency, throughput,
+  rejections), beside the plain path serving the same streams one request at
+  a time; ``served`` is the 200 req/s point, ``served_sweep`` all of them.
+* ``targets``: the north star's ratios (config 1 over the CPU reference,
+  batched and served over the plain per-request path).
 * ``batched``: 64 jobs over nine rescaled configuration scenes in one
   wavefront after the launch-shape autotuner, beside the same jobs one at a
   time.
@@ -28,9 +31,8 @@ per second).
   (reference-compatible mode, closest-hit rays) and the terrain with its
   delta-tracked volume.
 
-``--impl reference`` times that CPU reference alone (rank 0), its timed
-steps sized from short warm-up steps to take about ``--reference-seconds``
-together.
+``--impl reference`` times that CPU reference alone (rank 0): each step one
+full render of the scaled config-2 scene per host core.
 For N > 1 (torchrun), every rank renders its own frames (weak scaling, no
 data-path collective); the step time is the max over ranks, and only the
 headline section runs.
@@ -87,86 +89,70 @@ def _peaks():
 
 
 # ---------------------------------------------------------------------------
-# CPU reference sample (oracle restatement of CpuReferenceRenderer)
+# CPU reference (oracle restatement of CpuReferenceRenderer), full renders of
+# config 2 scaled for its brute-force intersector
 # ---------------------------------------------------------------------------
-_CPU_STATE = {}
+# The CPU reference intersects every ray with every triangle in a Python loop
+# over the triangles (renderers/reference/path_tracer.py:154-176): about 8
+# rays/s at the headline scene's 1,049,602 triangles.  Its timed workload is
+# therefore config 2 rescaled, rendered in full (camera and every extension
+# segment of 8 bounces, its Lambert transport and CPU sky), never
+# extrapolated; the CUDA renderer renders the same scene with the same
+# transport in the `scaled_c2` section for the like-for-like ratio.
+SCALED_C2 = dict(seed=5, instances=4, segments=32, bands=21, emitters=16, extent=4.0)
+SCALED_C2_TRIANGLES = 4 * 1280 + 2 + 16
+SCALED_C2_BOUNCES = 8
+SCALED_C2_TILE = (48, 32)   # pixels one CPU process renders per step, 1 spp
+SCALED_C2_WORKLOAD = ("config 2 scaled for the CPU reference's brute-force intersector: 4 instances of a "
+                      "1,280-tri sphere + 2-tri ground + 16 emissive tris (5,138 tris), reference-compatible "
+                      "transport (Lambert, CPU sky), 8 bounces, all closest-hit segments rendered")
 
 
-def _cpu_worker_init():
+def _cpu_scaled_worker(seed):
+    """One full reference render (48x32, 1 spp, every bounce) of the scaled
+    scene by the oracle restatement of CpuReferenceRenderer; returns
+    (closest-hit rays, seconds)."""
     os.environ["OMP_NUM_THREADS"] = "1"
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ["MKL_NUM_THREADS"] = "1"
+    from oracle import reference_path_tracer as ref
     from ordinarylight_b200 import scenes
 
-    from oracle import reference_path_tracer as ref
-
-    scene, camera = scenes.instanced_spheres()
-    _CPU_STATE["triangles"] = scene.triangles()
-    # the frame's camera rays (one jittered sample per pixel), made once
-    _CPU_STATE["rays"] = ref.camera_rays(camera, WIDTH, HEIGHT, np.random.default_rng(1000))
-
-
-def _cpu_tile(args):
-    """Closest-hit rays of one tile of the workload's first bounce, traced by
-    the oracle's brute-force intersector (path_tracer.py:154-176) against a
-    contiguous block of `count` of the scene's triangles.  That intersector
-    loops over triangles with every ray of the call in one numpy vector, so
-    its time is the same for every triangle: the block's time, scaled by
-    (all triangles / count), is the time of the whole scene.  Returns
-    (rays, scaled seconds)."""
-    tile, size, count = args
-    from oracle import reference_path_tracer as ref
-
-    tris = _CPU_STATE["triangles"][0]
-    o, d = _CPU_STATE["rays"]
-    tiles_x = WIDTH // size
-    tx, ty = tile % tiles_x, (tile // tiles_x) % (HEIGHT // size)
-    sel = ((np.arange(HEIGHT)[:, None] // size == ty) & (np.arange(WIDTH)[None, :] // size == tx)).reshape(-1)
-    count = max(1, min(int(count), len(tris)))
-    first = (tile * 7919 * count) % (len(tris) - count + 1)
+    scene, camera = scenes.instanced_spheres(**SCALED_C2)
     counter = ref.RayCounter()
     t0 = time.perf_counter()
-    ref.intersect(o[sel], d[sel], tris[first:first + count], counter)
-    return counter.rays, (time.perf_counter() - t0) * (len(tris) / count)
+    ref.render_frame(scene, camera, SCALED_C2_TILE[0], SCALED_C2_TILE[1], samples=1, max_bounces=SCALED_C2_BOUNCES,
+                     seed=int(seed), counter=counter)
+    return counter.rays, time.perf_counter() - t0
 
 
 class CpuReference:
-    """Pool of spawn workers, each holding the workload's triangle soup.
+    """Pool of spawn workers, one per host core: a step is one full render of
+    the scaled scene per process (distinct seeds), rays summed, the slowest
+    process's time taken."""
 
-    A step traces one tile x tile block of camera rays per process (64 x 64 =
-    4,096 rays: the batch at which the reference's per-ray cost is lowest;
-    fewer rays pay the per-triangle loop overhead for few rays, more rays
-    leave the caches) against `triangles` of the scene's triangles, timed
-    and scaled to all of them."""
-
-    def __init__(self, processes=None, tile=64, triangles=32768):
+    def __init__(self, processes=None):
         import multiprocessing as mp
 
         self.processes = processes or os.cpu_count() or 1
-        self.tile = tile
-        self.triangles = triangles
-        self.pool = mp.get_context("spawn").Pool(self.processes, initializer=_cpu_worker_init)
+        self.pool = mp.get_context("spawn").Pool(self.processes)
         self.step = 0
 
-    def run_step(self, triangles=None):
-        if triangles is not None:
-            self.triangles = triangles
-        jobs = [(self.step * self.processes + k, self.tile, self.triangles) for k in range(self.processes)]
+    def run_step(self):
+        seeds = [1000 + self.step * self.processes + k for k in range(self.processes)]
         self.step += 1
-        results = self.pool.map(_cpu_tile, jobs)
-        rays = sum(r for r, _ in results)
-        seconds = max(s for _, s in results)
-        return rays, seconds
+        results = self.pool.map(_cpu_scaled_worker, seeds)
+        return sum(r for r, _ in results), max(t for _, t in results)
 
     def close(self):
         self.pool.close()
         self.pool.join()
 
     def describe(self, steps):
-        return (f"first bounce (camera rays) at 1 spp: per step, one {self.tile}x{self.tile}-pixel tile per process "
-                f"traced by brute force as the CPU reference does, timed against a block of {self.triangles:,} "
-                f"of the 1,049,602 triangles and scaled to all of them (the reference's loop costs the same per "
-                f"triangle); {steps} step(s), one process per core, slowest process timed")
+        w, h = SCALED_C2_TILE
+        return (f"{SCALED_C2_WORKLOAD}: per step, one {w}x{h} render at 1 spp per process (camera rays and all "
+                f"extension segments, counted as the reference's intersector sees them), {steps} step(s), one "
+                f"process per core, slowest process timed; nothing extrapolated")
 
 
 def cpu_reference_measure(steps, processes=None):
@@ -492,6 +478,32 @@ def run_config1(device_index, processes=None):
             "gpu_over_cpu": gpu / cpu, "e2e_over_cpu": rays / wall / 1e6 / cpu}
 
 
+def run_scaled_c2(device_index, steps=5):
+    """The CPU reference's workload on the GPU: the scaled config-2 scene with
+    the reference-compatible transport and 8 bounces, at 1920x1080 and 1 spp
+    so that the device is filled; closest-hit rays per second (camera and
+    extension segments, what the CPU reference's counter counts)."""
+    import torch
+
+    from ordinarylight_b200 import CudaWavefrontRenderer, scenes
+
+    scene, camera = scenes.instanced_spheres(**SCALED_C2)
+    with CudaWavefrontRenderer(device=device_index, mode="reference_compatible", samples_per_pixel=1,
+                               max_bounces=SCALED_C2_BOUNCES, seed=1) as r:
+        for k in range(3):
+            r.render_frame(scene, camera, 1920, 1080, frame_index=k)
+        rays, gpu_ms, wall = 0, 0.0, 0.0
+        for k in range(steps):
+            t0 = time.perf_counter()
+            r.render_frame(scene, camera, 1920, 1080, frame_index=10 + k)
+            wall += time.perf_counter() - t0
+            rays += r.last_timings["closest_hit_rays"]
+            gpu_ms += r.last_timings["gpu_ms"]
+    torch.cuda.synchronize()
+    return {"workload": SCALED_C2_WORKLOAD + "; GPU image 1920x1080 at 1 spp",
+            "gpu_mrays_closest_hit": rays / (gpu_ms * 1e3), "gpu_e2e_mrays_closest_hit": rays / wall / 1e6}
+
+
 def run_config3(device_index, steps=5):
     """Terrain (2048^2 fBm heightfield, 8,380,418 triangles) under a 128^3
     fBm volume (sigma_t scale 0.5, albedo 0.9), sky 1.0 + sun; 1280x720,
@@ -612,13 +624,14 @@ def run_batched(device_index, tune=True):
             "tuned": tuned}
 
 
-def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit=40):
-    """Poisson request stream over 8 resident scenes: the continuous-batching
-    server against the plain path serving the stream one request at a time
-    in arrival order (the reference's serialised render_async worker), both
-    through render_frame (scene uploads on change; the first `frame_limit`
-    requests, latency from measured service times) and with every scene
-    resident (all requests, in real time on the same arrivals)."""
+def run_served(device_index, rates, count, budget_bytes, chunk_paths, frame_limit=40):
+    """Poisson request streams over 8 resident scenes, one per arrival rate:
+    the continuous-batching server against the plain path serving the stream
+    one request at a time in arrival order (the reference's serialised
+    render_async worker), both through render_frame (scene uploads on
+    change; the first `frame_limit` requests, whose measured service times
+    give the FIFO latency at every rate) and with every scene resident (all
+    requests, in real time on the same arrivals)."""
     import torch
 
     from ordinarylight_b200 import CudaWavefrontRenderer, workloads
@@ -626,9 +639,8 @@ def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit
 
     variants = workloads.served_scene_variants()
     requests = workloads.served_requests(variants, count, seed=5)
-    arrivals = poisson_arrivals(rate, count, seed=6)
     frame_service, frame_rays = _plain_frames(device_index, requests, frame_limit)
-    frame_lat, frame_wall = _fifo_latency_ms(arrivals[:frame_limit], frame_service)
+    results = []
     with CudaWavefrontRenderer(device=device_index, restir=True, restir_candidates=32, restir_spatial=1,
                                restir_neighbours=5, restir_radius=30.0, seed=1, chunk_paths=chunk_paths) as r:
         for v in variants:
@@ -638,59 +650,86 @@ def run_served(device_index, rate, count, budget_bytes, chunk_paths, frame_limit
         # one-time costs of the serving path (graph captures, arena and
         # staging growth) are paid by a short warm-up stream
         warm_server = RenderServer(r, budget_bytes=budget_bytes).start()
-        run_stream(warm_server, warm, poisson_arrivals(rate, len(warm), seed=98))
+        run_stream(warm_server, warm, poisson_arrivals(float(rates[0]), len(warm), seed=98))
         warm_server.stop()
         torch.cuda.synchronize()
-        # plain with resident scenes, real time: one request at a time in
-        # arrival order on a worker thread (SerialServer)
-        serial = SerialServer(r).start()
-        run_stream(serial, requests, arrivals)
-        serial.stop()
-        plain = serial.stats.summary()
-        # served arm, same arrivals
-        torch.cuda.synchronize()
-        server = RenderServer(r, budget_bytes=budget_bytes).start()
-        futures = run_stream(server, requests, arrivals)
-        server.stop()
-        summary = server.stats.summary()
-        ok = sum(1 for f in futures if f.exception() is None)
-    frame_mrays = sum(frame_rays) / frame_wall / 1e6
-    return {"workload": f"{count} requests, Poisson {rate:g} req/s, 8 resident scenes (10k-8.4M tris), "
-                        "resolutions {256^2, 512^2, 720p, 1080p}, spp {1, 4, 16}, bounces {4, 8}, "
-                        f"HBM budget {budget_bytes / 1e9:g} GB, chunk {chunk_paths} paths",
-            "requests": count, "completed": ok, "rejected": summary["rejected"], "failed": summary["failed"],
-            "p50_ms": summary["p50_ms"], "p99_ms": summary["p99_ms"], "mean_ms": summary["mean_ms"],
-            "throughput_req_s": summary["throughput_req_s"], "mrays_per_s": summary["mrays_per_s"],
-            "steps": summary["steps"],
-            "plain_frame": {"requests": frame_limit, "p50_ms": float(np.percentile(frame_lat, 50)),
-                            "p99_ms": float(np.percentile(frame_lat, 99)),
-                            "throughput_req_s": frame_limit / frame_wall, "mrays_per_s": frame_mrays,
-                            "mean_service_ms": float(np.mean(frame_service) * 1e3)},
-            "plain_resident": {"p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"], "mean_ms": plain["mean_ms"],
-                               "throughput_req_s": plain["throughput_req_s"], "mrays_per_s": plain["mrays_per_s"],
-                               "gpu_mrays_per_s": plain["gpu_mrays_per_s"]},
-            "speedup_mrays_vs_plain_frame": summary["mrays_per_s"] / frame_mrays,
-            "speedup_mrays_vs_plain_resident": summary["mrays_per_s"] / plain["mrays_per_s"]}
+        for rate in rates:
+            rate = float(rate)
+            arrivals = poisson_arrivals(rate, count, seed=6)
+            frame_lat, frame_wall = _fifo_latency_ms(arrivals[:frame_limit], frame_service)
+            frame_mrays = sum(frame_rays) / frame_wall / 1e6
+            # plain with resident scenes, real time: one request at a time in
+            # arrival order on a worker thread (SerialServer)
+            serial = SerialServer(r).start()
+            run_stream(serial, requests, arrivals)
+            serial.stop()
+            plain = serial.stats.summary()
+            # served arm, same arrivals
+            torch.cuda.synchronize()
+            server = RenderServer(r, budget_bytes=budget_bytes).start()
+            futures = run_stream(server, requests, arrivals)
+            server.stop()
+            summary = server.stats.summary()
+            ok = sum(1 for f in futures if f.exception() is None)
+            results.append({
+                "workload": f"{count} requests, Poisson {rate:g} req/s, 8 resident scenes (10k-8.4M tris), "
+                            "resolutions {256^2, 512^2, 720p, 1080p}, spp {1, 4, 16}, bounces {4, 8}, "
+                            f"HBM budget {budget_bytes / 1e9:g} GB, chunk {chunk_paths} paths",
+                "rate_req_s": rate, "requests": count, "completed": ok, "rejected": summary["rejected"],
+                "failed": summary["failed"], "p50_ms": summary["p50_ms"], "p99_ms": summary["p99_ms"],
+                "mean_ms": summary["mean_ms"], "throughput_req_s": summary["throughput_req_s"],
+                "mrays_per_s": summary["mrays_per_s"], "steps": summary["steps"],
+                "plain_frame": {"requests": frame_limit, "p50_ms": float(np.percentile(frame_lat, 50)),
+                                "p99_ms": float(np.percentile(frame_lat, 99)),
+                                "throughput_req_s": frame_limit / frame_wall, "mrays_per_s": frame_mrays,
+                                "mean_service_ms": float(np.mean(frame_service) * 1e3)},
+                "plain_resident": {"p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"],
+                                   "mean_ms": plain["mean_ms"], "throughput_req_s": plain["throughput_req_s"],
+                                   "mrays_per_s": plain["mrays_per_s"], "gpu_mrays_per_s": plain["gpu_mrays_per_s"]},
+                "speedup_mrays_vs_plain_frame": summary["mrays_per_s"] / frame_mrays,
+                "speedup_mrays_vs_plain_resident": summary["mrays_per_s"] / plain["mrays_per_s"]})
+    return results
 
 
-# Seconds of CPU work the reference arm's timed steps take together (default).
-REFERENCE_BUDGET_S = 120.0
+def targets_summary(line):
+    """The north star's ratios in one place (the batched/served >= 3x over the
+    plain per-request path, config 1 >= 100x the CPU reference)."""
+    t = {}
+    c1 = line.get("config1")
+    if c1:
+        t["config1_gpu_over_cpu"] = c1["gpu_over_cpu"]
+        t["config1_e2e_over_cpu"] = c1["e2e_over_cpu"]
+        t["config1_required"] = 100.0
+    c2 = line.get("scaled_c2")
+    cpu = line.get("cpu_baseline")
+    if c2 and cpu:
+        t["scaled_c2_gpu_over_cpu"] = c2["gpu_mrays_closest_hit"] / cpu["value"]
+    b = line.get("batched")
+    if b:
+        t["batched_speedup_vs_plain_frame"] = b["speedup_vs_plain_frame"]
+        t["batched_speedup_vs_plain_resident"] = b["speedup_vs_plain_resident"]
+    sv = line.get("served")
+    if sv:
+        t["served_rate_req_s"] = sv["rate_req_s"]
+        t["served_speedup_vs_plain_frame"] = sv["speedup_mrays_vs_plain_frame"]
+        t["served_speedup_vs_plain_resident"] = sv["speedup_mrays_vs_plain_resident"]
+        t["served_p50_ms"] = sv["p50_ms"]
+        t["served_p99_ms"] = sv["p99_ms"]
+        t["served_rejected"] = sv["rejected"]
+    if b or sv:
+        t["systems_required"] = 3.0
+    return t
 
 
 def run_reference_arm(args):
+    """The CPU reference's own implementation of the path (the oracle
+    restatement of CpuReferenceRenderer) on all host cores, on the scaled
+    config-2 workload, each step a full render per process."""
     steps = args.steps
     ref = CpuReference(args.cpu_processes)
     try:
-        # short warm-up steps start the pool and measure the time per
-        # triangle; the timed steps' triangle blocks are sized from it so
-        # that all of them together take about the budget
-        budget = args.reference_seconds
-        warm = 1024
-        per_triangle = 1e-3
         for _ in range(max(args.warmup, 1)):
-            _rays, secs = ref.run_step(triangles=warm)
-            per_triangle = max(secs / 1049602, 1e-7)   # seconds per triangle (secs is scaled to all of them)
-        ref.triangles = int(max(warm, min(1049602, budget / (steps * per_triangle))))
+            ref.run_step()
         total_rays, total_s = 0, 0.0
         for _ in range(steps):
             rays, secs = ref.run_step()
@@ -713,8 +752,12 @@ def run_reference_arm(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded scene generators, ordinarylight_b200/scenes.py)",
-        "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_bounces": BOUNCES,
-                   "triangles": 1049602, "parallelism": "host cores"},
+        "config": {"workload": SCALED_C2_WORKLOAD, "width": SCALED_C2_TILE[0], "height": SCALED_C2_TILE[1],
+                   "spp": 1, "max_bounces": SCALED_C2_BOUNCES, "triangles": SCALED_C2_TRIANGLES,
+                   "parallelism": f"host cores x{ref.processes} (one render per process per step)",
+                   "full_config_2": "the 1,049,602-triangle scene is beyond the brute-force intersector "
+                                    "(about 8 rays/s); the CUDA line's scaled_c2 section renders this scaled "
+                                    "scene with the same transport"},
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": ref.processes, "kind": "port",
                          "sample": ref.describe(steps)},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -730,15 +773,14 @@ def main():
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--cpu-processes", type=int, default=None)
-    p.add_argument("--reference-seconds", type=float, default=REFERENCE_BUDGET_S,
-                   help="CPU seconds the reference arm's timed steps take together")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--width", type=int, default=WIDTH, help="image width (a smaller case for profiling)")
     p.add_argument("--height", type=int, default=HEIGHT, help="image height (a smaller case for profiling)")
-    p.add_argument("--sections", default="config1,config3,batched,served",
+    p.add_argument("--sections", default="config1,scaled_c2,config3,batched,served",
                    help="secondary sections run at N=1 (comma list; empty for the headline alone)")
-    p.add_argument("--served-rates", default="50,100",
-                   help="Poisson arrival rates (req/s); the first is reported as `served`, all in `served_sweep`")
+    p.add_argument("--served-rates", default="5,25,50,100,200",
+                   help="Poisson arrival rates (req/s), ascending; the last is reported as `served`, all in "
+                        "`served_sweep`")
     p.add_argument("--served-requests", type=int, default=150)
     p.add_argument("--served-budget-gb", type=float, default=150.0)
     p.add_argument("--served-chunk", type=int, default=1 << 23)
@@ -768,21 +810,35 @@ def main():
             sections = [x for x in args.sections.split(",") if x]
             if "config1" in sections:
                 line["config1"] = run_config1(local, args.cpu_processes)
+            if "scaled_c2" in sections:
+                line["scaled_c2"] = run_scaled_c2(local)
             if "config3" in sections:
                 line["config3"] = run_config3(local)
             if "batched" in sections:
                 line["batched"] = run_batched(local)
             if "served" in sections:
-                sweep = [run_served(local, float(rate), args.served_requests, args.served_budget_gb * 1e9,
-                                    args.served_chunk) for rate in args.served_rates.split(",") if rate]
-                line["served"] = sweep[0]
-                line["served_sweep"] = [{k: v[k] for k in ("workload", "p50_ms", "p99_ms", "throughput_req_s",
-                                                          "mrays_per_s", "rejected", "plain_resident",
+                rates = [float(x) for x in args.served_rates.split(",") if x]
+                sweep = run_served(local, rates, args.served_requests, args.served_budget_gb * 1e9,
+                                   args.served_chunk)
+                # the headline serving point: the highest swept rate, where the
+                # plain path is far past its capacity and the server runs saturated
+                line["served"] = sweep[-1]
+                line["served_sweep"] = [{k: v[k] for k in ("rate_req_s", "p50_ms", "p99_ms", "throughput_req_s",
+                                                          "mrays_per_s", "rejected", "completed",
+                                                          "speedup_mrays_vs_plain_frame",
+                                                          "speedup_mrays_vs_plain_resident", "plain_resident",
                                                           "plain_frame")} for v in sweep]
             if not args.no_cpu_baseline:
                 value, cores, sample = cpu_reference_measure(args.cpu_steps, args.cpu_processes)
                 line["cpu_baseline"] = {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
-                                        "sample": sample}
+                                        "sample": sample,
+                                        "workload": SCALED_C2_WORKLOAD + "; see scaled_c2 for the GPU's rate"}
+            targets = targets_summary(line)
+            if targets:
+                # placed right after `config` so that a truncated log keeps it
+                keys = list(line)
+                at = keys.index("config") + 1
+                line = {**{k: line[k] for k in keys[:at]}, "targets": targets, **{k: line[k] for k in keys[at:]}}
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

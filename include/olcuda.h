@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define OLC_ABI_VERSION 5
+#define OLC_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define OLC_API __attribute__((visibility("default")))
@@ -192,6 +192,22 @@ typedef struct olc_scene_desc {
                                             metallic-roughness, emissive, normal, occlusion and
                                             transmission maps (-1: none), normal scale, occlusion
                                             strength, uses texcoord set 1, 3 reserved */
+  /* volumes in the reference's own model, which the reference-compatible mode
+   * integrates along every ray segment (ReferencePathTracer.render_hdr,
+   * renderers/reference/path_tracer.py:55-65; volume/_core.py:252-504); at
+   * most 8, 72 floats each (integers as bit patterns):
+   *   world->local unit cube rows (12), nx ny nz lut_len, grid offset,
+   *   lut offset, address (0 clamp, 1 repeat, 2 mirror), linear filter,
+   *   missing data, clip-plane count, Henyey-Greenstein phase, scattering
+   *   orders, density scale, emission scale, step size, scattering scale,
+   *   scattering colour rgb + anisotropy, scattering albedo rgb + 0,
+   *   8 clip planes (a, b, c, d), 4 reserved */
+  uint32_t num_ref_volumes;
+  const float* ref_volume_records;       /* [n * 72] */
+  uint64_t ref_grid_values;
+  const float* ref_volume_grids;         /* Volume.normalized_data of each volume (z, y, x), concatenated */
+  uint64_t ref_lut_entries;
+  const float* ref_volume_luts;          /* transfer-function RGBA entries, concatenated */
 } olc_scene_desc;
 
 /* Camera basis computed by the caller in float32 exactly as the reference's

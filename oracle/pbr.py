@@ -7,7 +7,8 @@ pinned by the GLSL sources as specification):
 * ``pbr_evaluate``  ordinarylight_pbr_evaluate
   (ordinarylight/shaders/ordinaryshade_primary.glsl:541-564):
   f0 = mix(0.04, base, metallic); F = f0 + (1 - f0)(1 - v.h)^5;
-  alpha = max(roughness^2, 0.0009); D = a2 / max(pi ((n.h)^2 (a2 - 1) + 1)^2, 1e-6);
+  alpha = max(roughness^2, 0.0009); D = a2 / (pi ((n.h)^2 (a2 - 1) + 1)^2)
+  (uncapped: see _ggx_d);
   G1(x) = 2x / max(x + sqrt(a2 + (1 - a2) x^2), 1e-6);
   f = (1 - F)(1 - metallic) base / pi + F D G1(n.v) G1(n.l) / max(4 n.v n.l, 1e-6)
 * ``pbr_pdf``       ordinarylight_pbr_pdf (:565-581)
@@ -28,6 +29,17 @@ def _normalize(v):
     return v / np.linalg.norm(v, axis=-1, keepdims=True)
 
 
+def _ggx_d(n, h, nh, a2):
+    """GGX D = a2 / (pi ((n.h)^2 (a2 - 1) + 1)^2), the bracket as
+    |n x h|^2 + (n.h)^2 a2, uncapped (the reference's 1e-6 floor of pi den^2
+    caps D near its peak below roughness 0.155, where its sampler still draws
+    the uncapped distribution; above it both are the same function)."""
+    c = np.cross(n, h)
+    s2 = np.where(nh > 0.0, np.sum(c * c, -1), 1.0)
+    den = s2 + nh * nh * a2
+    return a2 / np.maximum(PI * den * den, 1e-300)
+
+
 def pbr_evaluate(base, roughness, metallic, n, view, out):
     """roughness and metallic: scalars or one value per point."""
     base = np.asarray(base, np.float64)
@@ -46,8 +58,7 @@ def pbr_evaluate(base, roughness, metallic, n, view, out):
     F = f0 + (1.0 - f0) * w[..., None]
     a = np.maximum(roughness * roughness, 0.0009)
     a2 = a * a
-    den = nh * nh * (a2 - 1.0) + 1.0
-    D = a2 / np.maximum(PI * den * den, 1e-6)
+    D = _ggx_d(n, h, nh, a2)
 
     def g1(x):
         return 2.0 * x / np.maximum(x + np.sqrt(a2 + (1.0 - a2) * x * x), 1e-6)
@@ -69,9 +80,7 @@ def pbr_pdf(base, roughness, metallic, n, view, out):
     vh = np.maximum(np.sum(view * h, -1), 1e-6)
     a = max(roughness * roughness, 0.0009)
     a2 = a * a
-    den = nh * nh * (a2 - 1.0) + 1.0
-    D = a2 / np.maximum(PI * den * den, 1e-6)
-    spec_pdf = D * nh / (4.0 * vh)
+    spec_pdf = _ggx_d(n, h, nh, a2) * nh / (4.0 * vh)
     diff_pdf = nl / PI
     f0 = 0.04 + (base - 0.04) * metallic
     p = np.clip(np.max(f0), 0.1, 0.9)

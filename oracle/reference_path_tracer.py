@@ -27,6 +27,10 @@ matters for bit-exactness):
   1e-4 along the normal flipped against the ray, new direction
   normalize(n + s) with s a normalised ``rng.normal`` vector flipped into
   the hemisphere (path_tracer.py:74-87, :205-211);
+* volumes: after each intersection, every active segment up to its hit
+  (or unbounded for a miss) crosses the visible volumes' emission–absorption
+  ray march (oracle/reference_volume.py, path_tracer.py:55-65): radiance +=
+  throughput * volume radiance, throughput *= volume transmittance;
 * average over samples, alpha 0 (path_tracer.py:89-95).
 """
 
@@ -35,6 +39,8 @@ from __future__ import annotations
 import math
 
 import numpy as np
+
+from . import reference_volume
 
 __all__ = ["ReferencePathTracer", "render_hdr", "camera_rays", "intersect", "RayCounter"]
 
@@ -152,8 +158,8 @@ def render_hdr(scene, camera, width, height, samples=1, max_bounces=3, seed=1, c
         raise ValueError("width and height must be positive")
     if samples <= 0 or max_bounces <= 0:
         raise ValueError("samples and max_bounces must be positive")
-    if tuple(getattr(scene, "visible_volumes", ())):
-        raise NotImplementedError("the oracle restates surface transport only")
+    volumes = tuple(getattr(scene, "visible_volumes", ()))
+    lights = tuple(getattr(scene, "lights", ()))
     triangles, colors, emissions = scene.triangles()
     rng = np.random.default_rng(seed)
     accumulated = np.zeros((height * width, 3), dtype=np.float32)
@@ -168,6 +174,13 @@ def render_hdr(scene, camera, width, height, samples=1, max_bounces=3, seed=1, c
             if not len(ids):
                 break
             hit_t, hit_tri = intersect(origins[ids], directions[ids], triangles, counter)
+            if volumes:
+                # every segment crosses the media first (path_tracer.py:55-65)
+                entries, exits = reference_volume.intersect_unit_boxes(origins[ids], directions[ids], volumes)
+                vol_rad, vol_t = reference_volume.integrate_volumes(volumes, origins[ids], directions[ids], entries,
+                                                                    exits, max_distance=hit_t, lights=lights)
+                radiance[ids] += throughput[ids] * vol_rad
+                throughput[ids] *= vol_t[:, None]
             missed = hit_tri < 0
             if np.any(missed):
                 rid = ids[missed]

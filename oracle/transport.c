@@ -11,14 +11,14 @@
  *  that samplePbr calls, transport_v1/lighting.glsl:218-246):
  *    f0 = mix(0.04, base, metallic); F = f0 + (1 - f0)(1 - v.h)^5;
  *    alpha = max(roughness^2, 0.0009), a2 = alpha^2;
- *    D = a2 / max(pi ((n.h)^2 (a2 - 1) + 1)^2, 1e-6);
+ *    D = a2 / (pi ((n.h)^2 (a2 - 1) + 1)^2) (uncapped; see ggx_d);
  *    G1(x) = 2x / max(x + sqrt(a2 + (1 - a2) x^2), 1e-6);
  *    f = (1 - F)(1 - metallic) base / pi + F D G1(n.v) G1(n.l) / max(4 n.v n.l, 1e-6);
  *    p_spec = clamp(max(f0), 0.1, 0.9);
  *    pdf = mix(n.l / pi, D n.h / (4 max(v.h, 1e-6)), p_spec), floored at 1e-6.
  *  Sampling: lobe with p_spec; diffuse = cosine hemisphere in the frame
  *  tangent = normalize(cross(n, z or y)); specular = GGX half vector
- *  cos = sqrt((1 - u) / max(1 + (a2 - 1) u, 1e-6)), reflected.  A reflection
+ *  cos = sqrt((1 - u) / (1 + (a2 - 1) u)), reflected.  A reflection
  *  below the surface: the reference draws a fresh cosine direction but keeps
  *  the mixture pdf (lighting.glsl:238-241), which overstates the weight of
  *  such directions; OLO_INVALID_RESAMPLE reproduces that, the default ends
@@ -333,9 +333,20 @@ static inline double alpha2_of(double roughness) {
   double a = fmax(roughness * roughness, 0.0009);
   return a * a;
 }
-static inline double ggx_d(double nh, double a2) {
-  double den = nh * nh * (a2 - 1.0) + 1.0;
-  return a2 / fmax(OLO_PI * den * den, 1e-6);
+/* GGX D with the bracket (n.h)^2 (a2 - 1) + 1 written as |n x h|^2 + (n.h)^2 a2
+ * and not capped: the reference floors pi den^2 at 1e-6, which for roughness
+ * below about 0.155 caps D near its peak while the sampler draws the uncapped
+ * distribution, so f cos / pdf no longer integrates f and the estimators of
+ * one scene disagree (by a fifth at roughness 0.05).  Above roughness 0.155
+ * both are the same function. */
+static inline double ggx_d(double nh, double s2, double a2) {
+  double den = s2 + nh * nh * a2;
+  return a2 / fmax(OLO_PI * den * den, 1e-300);
+}
+static inline double sin2_between(v3 n, v3 h, double nh) {
+  if (!(nh > 0.0)) return 1.0;
+  v3 c = cross(n, h);
+  return dot(c, c);
 }
 static inline double ggx_g1(double x, double a2) { return 2.0 * x / fmax(x + sqrt(a2 + (1.0 - a2) * x * x), 1e-6); }
 static inline v3 f0_of(const mat_t* m) { return add(scl(mk(0.04, 0.04, 0.04), 1.0 - m->metallic), scl(m->base, m->metallic)); }
@@ -350,7 +361,7 @@ static v3 bsdf_eval(const mat_t* m, v3 n, v3 view, v3 out) {
   double w = pow(1.0 - clampd(vh, 0.0, 1.0), 5.0);
   v3 F = add(f0, scl(sub(mk(1, 1, 1), f0), w));
   double a2 = alpha2_of(m->roughness);
-  double spec = ggx_d(nh, a2) * ggx_g1(nv, a2) * ggx_g1(nl, a2) / fmax(4.0 * nv * nl, 1e-6);
+  double spec = ggx_d(nh, sin2_between(n, h, nh), a2) * ggx_g1(nv, a2) * ggx_g1(nl, a2) / fmax(4.0 * nv * nl, 1e-6);
   v3 diff = scl(mul(sub(mk(1, 1, 1), F), m->base), (1.0 - m->metallic) / OLO_PI);
   return add(diff, scl(F, spec));
 }
@@ -360,7 +371,7 @@ static double bsdf_pdf(const mat_t* m, v3 n, v3 view, v3 out) {
   if (nl <= 0.0) return 0.0;
   v3 h = nrm(add(view, out));
   double nh = fmax(dot(n, h), 0.0), vh = fmax(dot(view, h), 1e-6);
-  double sp = ggx_d(nh, alpha2_of(m->roughness)) * nh / (4.0 * vh);
+  double sp = ggx_d(nh, sin2_between(n, h, nh), alpha2_of(m->roughness)) * nh / (4.0 * vh);
   double dp = nl / OLO_PI;
   double p = spec_prob(m);
   return dp + (sp - dp) * p;
@@ -477,8 +488,9 @@ static int sample_bsdf(const mat_t* m, v3 n, v3 d, const double* u, uint32_t fla
   v3 out;
   if (u[0] < spec_prob(m)) {
     const double a2 = alpha2_of(m->roughness);
-    const double c = sqrt((1.0 - u[1]) / fmax(1.0 + (a2 - 1.0) * u[1], 1e-6));
-    const double sn = sqrt(fmax(0.0, 1.0 - c * c)), phi = 2.0 * OLO_PI * u[2];
+    const double den = fmax((1.0 - u[1]) + a2 * u[1], 1e-300);   /* 1 + (a2 - 1) u */
+    const double c = sqrt((1.0 - u[1]) / den);
+    const double sn = sqrt(a2 * u[1] / den), phi = 2.0 * OLO_PI * u[2];
     v3 ta, bi;
     frame_of(n, &ta, &bi);
     v3 h = nrm(add(add(scl(ta, sn * cos(phi)), scl(bi, sn * sin(phi))), scl(n, c)));

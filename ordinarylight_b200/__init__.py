@@ -17,7 +17,7 @@ Public surface:
 from .scene import (  # noqa: F401
     CAMERA_TYPES, LIGHT_TYPES, DirectionalLight, EnvironmentLight, Instance, Material, Mesh, MeshResource,
     OrthographicCamera, PanoramicCamera, PerspectiveCamera, PointLight, Scene, SpotLight, Texture, TextureTransform,
-    Transform, Volume, VolumeMaterial,
+    Texture1D, Transform, Volume, VolumeMaterial,
 )
 from .renderer import Renderer, RenderJob, RenderStatistics, install_cuda_preference  # noqa: F401
 from .renderers.cuda import CudaRendererConfig, CudaWavefrontRenderer  # noqa: F401

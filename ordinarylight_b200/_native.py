@@ -67,6 +67,8 @@ class OlcSceneDesc(ctypes.Structure):
         ("volume_max_density", c_float), ("reserved", c_uint32 * 7),
         ("texcoords", _f32p), ("tangents", _f32p), ("num_texture_words", c_uint32), ("texture_words", _u32p),
         ("num_texture_bindings", c_uint32), ("texture_bindings", _f32p), ("material_textures", _f32p),
+        ("num_ref_volumes", c_uint32), ("ref_volume_records", _f32p), ("ref_grid_values", c_uint64),
+        ("ref_volume_grids", _f32p), ("ref_lut_entries", c_uint64), ("ref_volume_luts", _f32p),
     ]
 
 

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "olcuda.h"
+#include "olc_refvolume.cuh"
 #include "olc_internal.h"
 #include "olc_motion.h"
 #include "olc_restir.h"
@@ -192,6 +193,7 @@ struct ResidentScene {
   Range nodes, slots, instances, materials, emitters, lights;
   DeviceBuffer env_image, volume;
   DeviceBuffer tex_words, tex_bindings, tex_attr, mat_tex;   // textured scenes only
+  DeviceBuffer ref_vol_recs, ref_vol_grid, ref_vol_lut;      // volumes in the reference's model
   SceneRec rec{};
   SceneLayout layout;
   std::vector<BlasRange> blas_ranges;
@@ -216,6 +218,7 @@ struct QueuedJob {
   // plain frame's temporal pass finds them; otherwise chunk-local ones
   bool job_local_reservoirs = false;
   bool textured = false;     // its scene has textures (the run uses the textured kernels)
+  bool ref_volumes = false;  // reference-compatible job whose scene has volumes (their ray march runs)
   uint32_t age = 0;          // serving steps since it was queued
 };
 
@@ -224,6 +227,7 @@ struct ChunkPlan {
   uint32_t bounces = 0;
   bool restir = false;
   bool textures = false;     // its jobs' scenes have textures (all or none of them)
+  bool ref_volumes = false;  // some job marches reference volumes
   std::vector<JobRec> segs;
 };
 
@@ -770,6 +774,30 @@ void write_textures(olc_context* ctx, const olc_scene_desc* d, ResidentScene& rs
   OLC_CUDA(cudaStreamSynchronize(st));
 }
 
+// The reference-model volume records index the concatenated grids and
+// transfer tables on the device: every offset, size and parameter is checked
+// here, before upload.
+void check_ref_volumes(const olc_scene_desc* d) {
+  if (d->num_ref_volumes == 0) return;
+  if (d->num_ref_volumes > kMaxRefVolumes) throw Error(OLC_ERR_VALUE, "at most 8 visible volumes per scene");
+  if (!d->ref_volume_records || !d->ref_volume_grids || !d->ref_volume_luts)
+    throw Error(OLC_ERR_VALUE, "volume records, grids and transfer tables are required");
+  for (uint32_t k = 0; k < d->num_ref_volumes; ++k) {
+    RefVolume v;
+    std::memcpy(&v, d->ref_volume_records + 72ull * k, sizeof(RefVolume));
+    if (v.nx < 2 || v.ny < 2 || v.nz < 2) throw Error(OLC_ERR_VALUE, "volume grids need at least 2 samples per axis");
+    if ((uint64_t)v.grid_off + (uint64_t)v.nx * v.ny * v.nz > d->ref_grid_values)
+      throw Error(OLC_ERR_VALUE, "a volume grid lies outside the grid values");
+    if (v.lut_len < 1 || (uint64_t)v.lut_off + v.lut_len > d->ref_lut_entries)
+      throw Error(OLC_ERR_VALUE, "a transfer function lies outside the transfer entries");
+    if (v.address > 2 || v.num_clip > 8 || v.orders < 1 || v.orders > 8)
+      throw Error(OLC_ERR_VALUE, "invalid volume addressing, clip-plane count or scattering orders");
+    if (!(v.step_size > 0.0f) || !std::isfinite(v.step_size) || !(v.density_scale >= 0.0f) ||
+        !(v.emission_scale >= 0.0f) || !(v.scattering_scale >= 0.0f))
+      throw Error(OLC_ERR_VALUE, "volume step size must be positive and scales non-negative");
+  }
+}
+
 // Everything of a resident scene besides its BLAS: instance records, the
 // baked world-space triangles, the TLAS, materials, emitters, lights,
 // environment, volume and the SceneRec.  Runs at upload and at every
@@ -889,6 +917,11 @@ void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScen
   if (d->volume_present && (!d->volume_density || vol_count == 0))
     throw Error(OLC_ERR_VALUE, "a volume needs a density grid");
   upload(rs.volume, d->volume_density, vol_count, st, own);
+  check_ref_volumes(d);
+  upload(rs.ref_vol_recs, reinterpret_cast<const RefVolume*>(d->ref_volume_records), d->num_ref_volumes, st, own);
+  upload(rs.ref_vol_grid, d->ref_volume_grids, d->num_ref_volumes ? d->ref_grid_values : 0, st, own);
+  upload(rs.ref_vol_lut, reinterpret_cast<const float4*>(d->ref_volume_luts),
+         d->num_ref_volumes ? d->ref_lut_entries : 0, st, own);
   OLC_CUDA(cudaStreamSynchronize(st));  // host staging vectors go out of scope
 
   SceneRec& v = rs.rec;
@@ -925,6 +958,10 @@ void write_scene_records(olc_context* ctx, const olc_scene_desc* d, ResidentScen
   v.srgb_lut = ctx->srgb_lut.as<float>();
   v.slot_base = (uint32_t)rs.slots.off;
   v.material_base = (uint32_t)rs.materials.off;
+  v.ref_vols = rs.ref_vol_recs.as<RefVolume>();
+  v.ref_grid = rs.ref_vol_grid.as<float>();
+  v.ref_lut = rs.ref_vol_lut.as<float4>();
+  v.num_ref_vols = d->num_ref_volumes;
 }
 
 BlasDesc mesh_blas_desc(const olc_scene_desc* d, uint32_t m, const DeviceBuffer& dv, const DeviceBuffer& dn,
@@ -1251,6 +1288,7 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
       ch.segs.push_back(seg);
       ch.bounces = std::max(ch.bounces, seg.max_bounces);
       ch.restir = ch.restir || seg.restir;
+      ch.ref_volumes = ch.ref_volumes || t.job->ref_volumes;
       at += t.count;
     }
     ch.count = (uint32_t)fill;
@@ -1421,6 +1459,11 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
       // shading adds to path radiance and refills the shadow queue: the
       // previous bounce's shadow rays must be done
       side_join(ctx);
+      if (ch.ref_volumes) {
+        // reference-compatible paths cross their scene's volumes before shading
+        launch_ref_volumes(ctx->ls, jobs, s, *qin, rb.hb, rb.ps, rb.cnt, b, st);
+        tl_mark(ctx, OLC_STAGE_SHADE, b, c);
+      }
       launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
                    ch.textures, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
@@ -1453,7 +1496,8 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
   std::vector<uint64_t> k;
   k.push_back(plan.chunks.size());
   for (const ChunkPlan& c : plan.chunks)
-    k.push_back(((uint64_t)c.bounces << 2) | (c.textures ? 2u : 0u) | (c.restir ? 1u : 0u));
+    k.push_back(((uint64_t)c.bounces << 3) | (c.ref_volumes ? 4u : 0u) | (c.textures ? 2u : 0u) |
+                (c.restir ? 1u : 0u));
   auto ptr = [&](const void* p) { k.push_back((uint64_t)(uintptr_t)p); };
   const SceneView s = pool_view(ctx);
   const void* const* sv = reinterpret_cast<const void* const*>(&s);
@@ -1735,6 +1779,7 @@ void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
                    d->scene);
   q.rec.sample_base = d->first_sample;
   q.textured = scene_of(ctx, d->scene).rec.tex_words != nullptr;
+  q.ref_volumes = q.rec.mode == OLC_MODE_REFERENCE_COMPATIBLE && scene_of(ctx, d->scene).rec.num_ref_vols > 0u;
   q.total = (uint64_t)q.rec.npix * q.rec.spp;
   q.out = d->out_rgba;
   q.sums = d->out_sums;
@@ -1952,6 +1997,7 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     job.rec = make_job(ctx, camera, width, height, spp, frame_index, 0, ctx->default_scene);
     job.rec.products = 1;
     job.textured = rs.rec.tex_words != nullptr;
+    job.ref_volumes = job.rec.mode == OLC_MODE_REFERENCE_COMPATIBLE && rs.rec.num_ref_vols > 0u;
     job.total = (uint64_t)job.rec.npix * spp;
     job.out = out_rgba;
     job.out_device = out_is_device != 0;

@@ -231,6 +231,23 @@ OLC_D uint32_t owner_instance(const InstanceRec* instances, const uint32_t* tri_
 #define OLC_TLAS_LEAF_INSTANCE 1u
 #define OLC_TLAS_LEAF_TRIANGLE 2u
 
+// One visible volume in the reference's volume model (the reference-
+// compatible mode's ray march; 288 bytes, the olc_scene_desc record of 72
+// floats with its integer fields as bit patterns).
+struct __align__(16) RefVolume {
+  float4 w2b0, w2b1, w2b2;          // world -> local unit cube (rows of the inverse transform)
+  uint32_t nx, ny, nz, lut_len;     // grid size (x fastest in memory: z, y, x), transfer entries
+  uint32_t grid_off, lut_off;       // offsets of the normalized grid and of the transfer table
+  uint32_t address, linear;         // transfer addressing: 0 clamp, 1 repeat, 2 mirror; linear filter
+  uint32_t missing, num_clip, phase_hg, orders;
+  float density_scale, emission_scale, step_size, scattering_scale;
+  float4 scat_color_aniso;          // scattering colour, Henyey-Greenstein anisotropy
+  float4 scat_albedo;               // scattering albedo (multiple orders)
+  float4 clip[8];                   // (a, b, c, d): keep (a, b, c) . p >= d
+  float4 reserved;
+};
+static_assert(sizeof(RefVolume) == 288, "RefVolume must match the 72-float scene-description record");
+
 // One resident scene of the pool: its TLAS root and its lighting.  Emitter
 // indices of the alias table are scene-local (add emitter_base).
 struct __align__(16) SceneRec {
@@ -261,6 +278,12 @@ struct __align__(16) SceneRec {
   const float* srgb_lut;         // 256 sRGB-to-linear values
   uint32_t slot_base;            // first triangle slot of the scene
   uint32_t material_base;        // first material record of the scene
+  // volumes in the reference's model (reference-compatible mode; none: 0)
+  const RefVolume* ref_vols;
+  const float* ref_grid;         // normalized values of every volume
+  const float4* ref_lut;         // transfer-function entries of every volume
+  uint32_t num_ref_vols;
+  uint32_t pad2[3];
 };
 
 // Device view of the scene pool shared by every resident scene: all BLAS and
@@ -329,6 +352,7 @@ struct PathState {
 // (65,536 = 2^16 samples, also when its sample range is split into shards)
 // stays below 2^63: it fits an unsigned 64-bit word and also the signed
 // 64-bit tensors the multi-GPU all-reduce adds, without wrapping.
+#define OLC_PI_F 3.14159265358979f
 #define OLC_ACCUM_SHIFT 28
 #define OLC_ACCUM_SCALE 268435456.0f
 #define OLC_SAMPLE_CLAMP 524287.0f

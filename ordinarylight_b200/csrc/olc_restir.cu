@@ -96,8 +96,8 @@ OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
   const float w = 1.0f - clampf(vh, 0.0f, 1.0f);
   const float w5 = w * w * w * w * w;
   const float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
-  const float den = nh * nh * (b.a2 - 1.0f) + 1.0f;
-  const float D = __fdividef(b.a2, fmaxf(OLC_PI * den * den, 1e-6f));
+  const float den = sin2_between(b.n, h, nh) + nh * nh * b.a2;   // the GGX bracket of ggx_d
+  const float D = __fdividef(b.a2, fmaxf(OLC_PI * den * den, 1e-30f));
   const float x = b.a2 + (1.0f - b.a2) * nl * nl;
   const float g1l = __fdividef(2.0f * nl, fmaxf(nl + x * rsqrtf(x), 1e-6f));
   const float3 spec = F * __fdividef(D * b.g1v * g1l, fmaxf(4.0f * b.nv * nl, 1e-6f));
@@ -154,6 +154,47 @@ OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float
     r.bary = bary;
     r.target = target;
   }
+}
+
+// Whether light sample (light, bary) lies in the support of the target at a
+// surface (position p, viewer-side shading normal n, view direction): the
+// conditions under which target_of is not zero (the BSDF of an opaque
+// surface is positive wherever both cosines are; emitters have positive
+// luminance).
+OLC_D bool in_support(const SceneView& sc, uint32_t light, uint32_t bary, float3 p, float3 n, float3 view) {
+  if (!(dot(n, view) > 0.0f)) return false;
+  const EmitterRec e = load_emitter(sc, light);
+  const float2 b = unpack_bary(bary);
+  const float3 off = emitter_point(e, b.x, b.y) - p;
+  const float d2 = dot(off, off);
+  if (!(d2 > 1e-12f)) return false;
+  const float3 l = off * rsqrtf(d2);
+  return dot(n, l) > 0.0f && emitter_cosine(e, l) > 1e-6f;
+}
+
+// The surface a stored reservoir belongs to, rebuilt from its primary depth
+// and normal along the camera ray of (pixel, sample stream, frame): the
+// reservoir's own pixel in the same frame, or in the previous frame for the
+// temporal history (the same camera, by the history's rule).
+OLC_D void stored_surface(const JobRec& job, uint32_t pixel, uint32_t sample, uint32_t frame, float depth,
+                          uint32_t normal, float3& p, float3& n, float3& view) {
+  const float2 jitter = olc_camera_jitter(pixel, sample, frame);
+  float3 o, d;
+  camera_ray(job, pixel, sample, &jitter, o, d);
+  p = o + d * depth;
+  n = oct_decode(normal);
+  view = -d;
+}
+
+// Unbiased normalisation of a combined reservoir (Bitterli et al. 2020,
+// "Spatiotemporal reservoir resampling", Algorithm 6): W = w_sum / (Z p_hat)
+// with Z the sample counts of only those combined reservoirs whose own target
+// is positive at the selected sample, instead of all of them (1 / M weights
+// darken wherever a reused reservoir could not have produced the sample).
+// Stored as w_sum M / Z, so W = w_sum / (M p_hat) and the reuse weight
+// p_hat w_sum / p_hat_src of later passes stay as they are.
+OLC_D void normalise_support(Res& r, uint32_t Z) {
+  if (Z > 0u && Z < r.M) r.w_sum *= (float)r.M / (float)Z;
 }
 
 // Primary surface of path slot i (its ray hit: only listed hits get here).
@@ -308,6 +349,13 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
         float wsum = prev.w_sum * ((float)m / (float)prev.M);
         float t = target_of(s, su, prev.light, prev.bary);
         res_update(r, prev.light, prev.bary, t, t * wsum / prev.target, m, olc_rand(rng));
+        // the candidates always count; the history only where the selected
+        // sample is in the support of the previous frame's target
+        if (r.light != 0xffffffffu) {
+          float3 hp, hn, hv;
+          stored_surface(job, meta.x, meta.y, job.frame - 1u, pd, pn, hp, hn, hv);
+          normalise_support(r, r.M - (in_support(s, r.light, r.bary, hp, hn, hv) ? 0u : m));
+        }
       }
     }
     store_res(a.out0, a.out1, g, r, su, stamp);
@@ -330,25 +378,52 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
     uint32_t n0, st0;
     Res r = load_res(a.in0, a.in1, g, d0, n0, st0);
     if (a.neighbours > 0u) {
-      uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 1u + a.pass);
+      const uint32_t rng0 = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 1u + a.pass);
       const int px = (int)(meta.x % job.width), py = (int)(meta.x / job.width);
-      for (uint32_t j = 0; j < a.neighbours; ++j) {
+      // The j-th neighbour of this pixel from the pass's stream (drawn the
+      // same way twice: to merge, then to normalise); false when it is off
+      // the image, this pixel, invalid or not similar.
+      auto neighbour = [&](uint32_t& rng, uint32_t& q, Res& nb, float& dq, uint32_t& nq, float& u) {
         float rr = a.radius * sqrtf(olc_rand(rng));
         float th = 2.0f * OLC_PI * olc_rand(rng);
-        float u = olc_rand(rng);
+        u = olc_rand(rng);
         float sn, cs;
         __sincosf(th, &sn, &cs);
         int qx = px + __float2int_rn(rr * cs);
         int qy = py + __float2int_rn(rr * sn);
-        if (qx < 0 || qy < 0 || qx >= (int)job.width || qy >= (int)job.height || (qx == px && qy == py)) continue;
-        uint64_t gq = stream_base + (uint64_t)qy * job.width + (uint64_t)qx;
-        float dq;
-        uint32_t nq, sq;
-        Res nb = load_res(a.in0, a.in1, gq, dq, nq, sq);
-        if (sq != stamp || nb.light == 0xffffffffu || nb.M == 0u || !(nb.target > 0.0f) || !similar(su, nq, dq))
-          continue;
+        if (qx < 0 || qy < 0 || qx >= (int)job.width || qy >= (int)job.height || (qx == px && qy == py)) return false;
+        q = (uint32_t)qy * job.width + (uint32_t)qx;
+        uint32_t sq;
+        nb = load_res(a.in0, a.in1, stream_base + q, dq, nq, sq);
+        return sq == stamp && nb.light != 0xffffffffu && nb.M != 0u && nb.target > 0.0f && similar(su, nq, dq);
+      };
+      uint32_t rng = rng0;
+      uint32_t reused = 0;
+      for (uint32_t j = 0; j < a.neighbours; ++j) {
+        uint32_t q, nq;
+        Res nb;
+        float dq, u;
+        if (!neighbour(rng, q, nb, dq, nq, u)) continue;
         float t = target_of(s, su, nb.light, nb.bary);
         res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u);
+        ++reused;
+      }
+      if (reused && r.light != 0xffffffffu) {
+        // this pixel's reservoir always counts (the selected sample has a
+        // positive target here); each neighbour where the sample is in the
+        // support of its own target
+        uint32_t Z = r.M;
+        rng = rng0;
+        for (uint32_t j = 0; j < a.neighbours; ++j) {
+          uint32_t q, nq;
+          Res nb;
+          float dq, u;
+          if (!neighbour(rng, q, nb, dq, nq, u)) continue;
+          float3 qp, qn, qv;
+          stored_surface(job, q, meta.y, job.frame, dq, nq, qp, qn, qv);
+          if (!in_support(s, r.light, r.bary, qp, qn, qv)) Z -= nb.M;
+        }
+        normalise_support(r, Z);
       }
     }
     store_res(a.out0, a.out1, g, r, su, stamp);

@@ -5,7 +5,8 @@
 // _sample_half_vector / _reflect / _weight / _specular_probability,
 // ordinarylight/shaders/ordinaryshade_primary.glsl:506-609):
 //   f0 = mix(0.04, base, metallic); F = Schlick(f0, v.h);
-//   D = GGX with alpha = max(roughness^2, 0.0009); G = Smith G1(n.v) G1(n.l);
+//   D = GGX with alpha = max(roughness^2, 0.0009) (not capped, see ggx_d);
+//   G = Smith G1(n.v) G1(n.l);
 //   f = (1 - F)(1 - metallic) base / pi + F D G / (4 n.v n.l);
 //   specular lobe probability = clamp(max(f0), 0.1, 0.9);
 //   pdf = mix(n.l / pi, D n.h / (4 v.h), p_spec).
@@ -83,9 +84,23 @@ OLC_D float ggx_alpha2(float roughness) {
   float a = fmaxf(roughness * roughness, 0.0009f);
   return a * a;
 }
-OLC_D float ggx_d(float nh, float a2) {
-  float den = nh * nh * (a2 - 1.0f) + 1.0f;
-  return a2 / fmaxf(OLC_PI * den * den, 1e-6f);
+// GGX distribution a2 / (pi ((n.h)^2 (a2 - 1) + 1)^2), with the bracket
+// written as |n x h|^2 + (n.h)^2 a2 (the same value for unit vectors) so that
+// float32 resolves it near the peak, where 1 + (n.h)^2 (a2 - 1) cancels.  The
+// reference floors pi den^2 at 1e-6, which caps D near the peak for
+// roughness below about 0.155 while its sampler still draws the uncapped
+// distribution: f cos / pdf then no longer integrates f, and estimators of
+// one scene disagree (by a fifth at roughness 0.05).  Here D is the GGX
+// distribution the sampler draws; above roughness 0.155 the two are equal.
+OLC_D float ggx_d(float nh, float s2, float a2) {
+  float den = s2 + nh * nh * a2;
+  return a2 / fmaxf(OLC_PI * den * den, 1e-30f);
+}
+// |n x h|^2 for the GGX bracket (1 where n.h <= 0, whose terms vanish).
+OLC_D float sin2_between(float3 n, float3 h, float nh) {
+  if (!(nh > 0.0f)) return 1.0f;
+  const float3 c = cross(n, h);
+  return dot(c, c);
 }
 OLC_D float ggx_g1(float nd, float a2) {
   return 2.0f * nd / fmaxf(nd + sqrtf(a2 + (1.0f - a2) * nd * nd), 1e-6f);
@@ -118,7 +133,7 @@ OLC_D float3 pbr_eval(const SurfaceMat& m, float3 n, float3 view, float3 out) {
   float w5 = w * w * w * w * w;
   float3 F = f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * w5;
   float a2 = ggx_alpha2(m.roughness);
-  float D = ggx_d(nh, a2);
+  float D = ggx_d(nh, sin2_between(n, h, nh), a2);
   float G = ggx_g1(nv, a2) * ggx_g1(nl, a2);
   float3 spec = F * (D * G / fmaxf(4.0f * nv * nl, 1e-6f));
   float3 diff = (f3(1.0f, 1.0f, 1.0f) - F) * m.base * ((1.0f - m.metallic) / OLC_PI);
@@ -132,7 +147,7 @@ OLC_D float pbr_pdf(const SurfaceMat& m, float3 n, float3 view, float3 out) {
   float nh = fmaxf(dot(n, h), 0.0f);
   float vh = fmaxf(dot(view, h), 1e-6f);
   float a2 = ggx_alpha2(m.roughness);
-  float spec_pdf = ggx_d(nh, a2) * nh / (4.0f * vh);
+  float spec_pdf = ggx_d(nh, sin2_between(n, h, nh), a2) * nh / (4.0f * vh);
   float diff_pdf = nl / OLC_PI;
   float p = spec_probability(m);
   return diff_pdf + (spec_pdf - diff_pdf) * p;
@@ -141,8 +156,12 @@ OLC_D float pbr_pdf(const SurfaceMat& m, float3 n, float3 view, float3 out) {
 OLC_D float3 sample_half_vector(float3 n, float roughness, float u, float v) {
   float a2 = ggx_alpha2(roughness);
   float phi = 2.0f * OLC_PI * v;
-  float c = sqrtf((1.0f - u) / fmaxf(1.0f + (a2 - 1.0f) * u, 1e-6f));
-  float sn = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+  // cos^2 = (1 - u) / (1 + (a2 - 1) u) and sin^2 = a2 u / (1 + (a2 - 1) u),
+  // the bracket as (1 - u) + a2 u and sin from its own ratio: both forms
+  // with 1 - ... cancel in float32 for narrow lobes
+  const float den = fmaxf(fmaf(a2, u, 1.0f - u), 1e-30f);
+  float c = sqrtf((1.0f - u) / den);
+  float sn = sqrtf(a2 * u / den);
   float3 t, b;
   tangent_frame(n, t, b);
   float sp, cp;

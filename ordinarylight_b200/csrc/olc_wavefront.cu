@@ -16,6 +16,7 @@
 // can be captured once as a CUDA graph.
 #include "olc_internal.h"
 #include "olc_shading.cuh"
+#include "olc_refvolume.cuh"
 #include "olc_textures.cuh"
 #include "olc_trace.cuh"
 #include "olc_volume.cuh"
@@ -789,6 +790,39 @@ __global__ void k_sort_scatter(RayQueue in, const uint32_t* __restrict__ count, 
   }
 }
 
+// ---- the reference volume model (reference-compatible mode) ---------------
+// Each queued ray of a reference-compatible path whose scene has visible
+// volumes crosses them over [0, hit distance] (unbounded for a miss) before
+// shading: path radiance += throughput * volume radiance, throughput *=
+// volume transmittance (ReferencePathTracer.render_hdr,
+// renderers/reference/path_tracer.py:55-65; the march is in
+// olc_refvolume.cuh).  A grid-stride pass over the bounce's queue; rays of
+// other paths are skipped.
+__global__ void __launch_bounds__(128) k_ref_volumes(const JobRec* __restrict__ jobs, SceneView s, RayQueue q,
+                                                     HitBuf h, PathState ps, const Counters* __restrict__ cnt,
+                                                     uint32_t bounce) {
+  const uint32_t n = cnt->queue_count[bounce];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t path = q.path[i];
+    const uint4 meta = ps.meta[path];
+    const JobRec& job = jobs[meta.w];
+    if (job.mode != 1u) continue;
+    const SceneRec& sc = s.scenes[job.scene];
+    if (sc.num_ref_vols == 0u) continue;
+    const float4 hit = h.tuv_slot[i];
+    const float t_max = hit.x < 0.0f ? CUDART_INF_F : hit.x;
+    float3 rad;
+    float T;
+    rv_integrate(ref_volumes_of(sc), s.lights + sc.light_base, sc.num_lights, f3(q.origin_tmin[i]),
+                 f3(q.dir_root[i]), t_max, rad, T);
+    if (T == 1.0f && rad.x == 0.0f && rad.y == 0.0f && rad.z == 0.0f) continue;
+    const float4 tp = ps.throughput[path];
+    const float4 r = ps.radiance[path];
+    ps.radiance[path] = make_float4(r.x + tp.x * rad.x, r.y + tp.y * rad.y, r.z + tp.z * rad.z, r.w);
+    ps.throughput[path] = make_float4(tp.x * T, tp.y * T, tp.z * T, tp.w);
+  }
+}
+
 OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
   if (!(v == v)) {  // NaN
     atomicAdd(nan_counter, 1u);
@@ -1015,6 +1049,13 @@ void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue&
 }
 
 size_t sort_bins_bytes() { return kSortBins * sizeof(uint32_t); }
+
+void launch_ref_volumes(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& q,
+                        const HitBuf& hits, const PathState& ps, const Counters* cnt, uint32_t bounce,
+                        cudaStream_t stream) {
+  k_ref_volumes<<<ls.grid_shade, 128, 0, stream>>>(jobs, s, q, hits, ps, cnt, bounce);
+  OLC_LAUNCH_CHECK("k_ref_volumes");
+}
 
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
                        unsigned long long* accum, float* sample_lum, Counters* cnt, cudaStream_t stream) {

@@ -82,6 +82,9 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
 void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue& in, const RayQueue& out,
                       Counters* cnt, uint32_t bounce, uint32_t* keys, uint32_t* bins, cudaStream_t stream);
 size_t sort_bins_bytes();
+void launch_ref_volumes(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& q,
+                        const HitBuf& hits, const PathState& ps, const Counters* cnt, uint32_t bounce,
+                        cudaStream_t stream);
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
                        unsigned long long* accum, float* sample_lum, Counters* cnt, cudaStream_t stream);
 // Per-pixel luminance variance of npix pixels from spp sample planes.

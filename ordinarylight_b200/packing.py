@@ -15,7 +15,7 @@ device-reported primitive index equals the index into ``Scene.triangles()``
 
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, fields
 import math
 
 import numpy as np
@@ -54,6 +54,9 @@ class PackedScene:
     texture_words: np.ndarray | None = None      # Scene.texture_data layout
     texture_bindings: np.ndarray | None = None   # [n, 8]
     material_textures: np.ndarray | None = None  # [num_materials, 12]
+    # volumes in the reference's model (records [n, 72], grids, luts [m, 4])
+    ref_volumes: dict | None = None
+    volume_count: int = 0          # visible volumes of the scene
 
     def descriptor(self) -> _native.OlcSceneDesc:
         d = _native.OlcSceneDesc()
@@ -95,6 +98,14 @@ class PackedScene:
             d.volume_sigma_t_scale = float(v["sigma_t_scale"])
             d.volume_albedo = float(v["albedo"])
             d.volume_max_density = float(v["max_density"])
+        if self.ref_volumes is not None:
+            rv = self.ref_volumes
+            d.num_ref_volumes = len(rv["records"])
+            d.ref_volume_records = _native.typed_ptr(rv["records"], f32)
+            d.ref_grid_values = len(rv["grids"])
+            d.ref_volume_grids = _native.typed_ptr(rv["grids"], f32)
+            d.ref_lut_entries = len(rv["luts"])
+            d.ref_volume_luts = _native.typed_ptr(rv["luts"], f32)
         if self.texture_bindings is not None and len(self.texture_bindings):
             d.texcoords = _native.typed_ptr(self.texcoords, f32)
             d.tangents = _native.typed_ptr(self.tangents, f32)
@@ -104,6 +115,54 @@ class PackedScene:
             d.texture_bindings = _native.typed_ptr(self.texture_bindings, f32)
             d.material_textures = _native.typed_ptr(self.material_textures, f32)
         return d
+
+    # -- files -------------------------------------------------------------
+    _DICT_FIELDS = ("volume", "ref_volumes")
+
+    def save(self, path) -> None:
+        """Write the packed arrays to an .npz file (the mesh source objects
+        are not kept): a scene packed where its objects exist, rendered
+        elsewhere."""
+        out = {}
+        for f in fields(self):
+            value = getattr(self, f.name)
+            if f.name == "mesh_sources":
+                continue
+            if f.name in self._DICT_FIELDS:
+                out[f"{f.name}__present"] = np.array(value is not None)
+                for k, v in (value or {}).items():
+                    out[f"{f.name}__{k}"] = np.asarray(v)
+            elif value is None:
+                out[f"{f.name}__none"] = np.array(True)
+            else:
+                out[f.name] = np.asarray(value)
+        np.savez_compressed(path, **out)
+
+    @classmethod
+    def load(cls, path) -> "PackedScene":
+        data = np.load(path, allow_pickle=False)
+        values = {}
+        for f in fields(cls):
+            if f.name == "mesh_sources":
+                continue
+            if f.name in cls._DICT_FIELDS:
+                if bool(data[f"{f.name}__present"]):
+                    prefix = f"{f.name}__"
+                    values[f.name] = {k[len(prefix):]: (data[k][()] if data[k].ndim == 0 else data[k])
+                                      for k in data.files if k.startswith(prefix) and k != f"{f.name}__present"}
+                else:
+                    values[f.name] = None
+            elif f"{f.name}__none" in data.files:
+                values[f.name] = None
+            else:
+                v = data[f.name]
+                values[f.name] = v[()] if v.ndim == 0 else v
+        values["environment_color"] = tuple(float(c) for c in values["environment_color"])
+        for name in ("emissive_weight", "environment_rotation"):
+            values[name] = float(values[name])
+        for name in ("environment_kind", "total_triangles", "volume_count"):
+            values[name] = int(values[name])
+        return cls(**values)
 
 
 def _material_record(material, material_id: int) -> np.ndarray:
@@ -283,17 +342,68 @@ def _volume_record(scene):
     if not volumes:
         return None
     if len(volumes) > 1:
-        raise RuntimeError("the CUDA renderer supports one visible volume per scene")
+        return None   # the production medium is one grid; the renderer refuses such scenes in production mode
     vol = volumes[0]
     density = np.ascontiguousarray(getattr(vol, "data", None), np.float32)
     if density.ndim != 3:
         raise RuntimeError("volume data must be a dense 3D grid")
     material = getattr(vol, "material", None)
-    sigma = float(getattr(material, "sigma_t_scale", getattr(material, "density_scale", 1.0)))
-    albedo = float(getattr(material, "albedo", 0.9)) if material is not None else 0.9
+    sigma = getattr(material, "sigma_t_scale", None)
+    if sigma is None:
+        sigma = getattr(material, "density_scale", 1.0)
+    albedo = getattr(material, "albedo", None)
+    sigma, albedo = float(sigma), 0.9 if albedo is None else float(albedo)
     w2b = np.linalg.inv(np.asarray(vol.transform.matrix, np.float64))[:3, :4].astype(np.float32)
     return {"density": density, "world_to_box": w2b, "sigma_t_scale": sigma, "albedo": albedo,
             "max_density": float(density.max()) if density.size else 0.0}
+
+
+_ADDRESS = {"clamp": 0, "repeat": 1, "mirror": 2}
+
+
+def _ref_volume_tables(scene):
+    """Visible volumes in the reference's model for the reference-compatible
+    ray march (olc_scene_desc's 72-float records): the inverse transform, the
+    normalized grid (Volume.normalized_data), the transfer function and the
+    optical parameters (ordinarylight/volume/_core.py:252-504)."""
+    volumes = tuple(getattr(scene, "visible_volumes", ()))
+    if not volumes:
+        return None
+    if any(getattr(v.material, "transfer_function", None) is None for v in volumes):
+        return None   # volumes without the reference's optical model
+    if len(volumes) > 8:
+        raise ValueError("the reference-compatible mode integrates at most 8 visible volumes per scene")
+    records, grids, luts = [], [], []
+    grid_off = lut_off = 0
+    for vol in volumes:
+        m = vol.material
+        tf = m.transfer_function
+        grid = np.ascontiguousarray(vol.normalized_data, np.float32)
+        nz, ny, nx = grid.shape
+        lut = np.ascontiguousarray(tf.values, np.float32).reshape(-1, 4)
+        planes = [tuple(map(float, p)) for p in getattr(vol, "clip_planes", ())]
+        if len(planes) > 8:
+            raise ValueError("a volume has at most 8 clip planes")
+        rec = np.zeros(72, np.float32)
+        ints = rec.view(np.uint32)
+        rec[0:12] = np.linalg.inv(np.asarray(vol.transform.matrix, np.float64)).astype(np.float32)[:3, :4].reshape(-1)
+        ints[12:16] = (nx, ny, nz, len(lut))
+        ints[16:24] = (grid_off, lut_off, _ADDRESS[tf.address_mode], int(bool(tf.linear_filter)),
+                       int(bool(getattr(vol, "missing_data", False))), len(planes),
+                       int(m.phase_function == "henyey_greenstein"), int(m.scattering_orders))
+        rec[24:28] = (m.density_scale, m.emission_scale, m.step_size, m.scattering_scale)
+        rec[28:31] = m.scattering_color
+        rec[31] = m.anisotropy
+        rec[32:35] = m.scattering_albedo
+        for k, plane in enumerate(planes):
+            rec[36 + 4 * k:40 + 4 * k] = plane
+        records.append(rec)
+        grids.append(grid.reshape(-1))
+        luts.append(lut)
+        grid_off += grid.size
+        lut_off += len(lut)
+    return {"records": np.ascontiguousarray(np.stack(records)), "grids": np.ascontiguousarray(np.concatenate(grids)),
+            "luts": np.ascontiguousarray(np.concatenate(luts))}
 
 
 def pack_scene(scene) -> PackedScene:
@@ -388,6 +498,8 @@ def pack_scene(scene) -> PackedScene:
         environment_rotation=env_rot,
         environment_image=env_img,
         volume=_volume_record(scene),
+        ref_volumes=_ref_volume_tables(scene),
+        volume_count=len(tuple(getattr(scene, "visible_volumes", ()))),
         total_triangles=prim,
         mesh_sources=tuple(sources),
         **tex,

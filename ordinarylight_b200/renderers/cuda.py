@@ -34,7 +34,7 @@ import time
 import numpy as np
 
 from .. import _native
-from ..packing import refit_mask, pack_camera, pack_scene
+from ..packing import PackedScene, refit_mask, pack_camera, pack_scene
 from .base import RendererImplementation, RendererImplementationInfo
 
 _MODES = {"production": _native.MODE_PRODUCTION, "reference_compatible": _native.MODE_REFERENCE_COMPATIBLE}
@@ -153,6 +153,19 @@ class RenderRequest:
     first_sample: int = 0       # RNG index of the first sample (a shard of a frame's samples)
 
 
+def _packed(scene, mode: str) -> PackedScene:
+    """The arrays of a scene: a reference or mirror ``Scene`` is flattened;
+    an already packed scene (``PackedScene``, for instance one loaded from a
+    file written where the scene objects exist) is used as it is.  The
+    production transport's medium is one density grid: a scene with several
+    visible volumes renders only in the reference-compatible mode, whose ray
+    march integrates up to eight."""
+    packed = scene if isinstance(scene, PackedScene) else pack_scene(scene)
+    if mode == "production" and packed.volume_count > 1:
+        raise RuntimeError("the production transport supports one visible volume per scene")
+    return packed
+
+
 def host_image(height: int, width: int) -> np.ndarray:
     """(height, width, 4) float32 host array in page-locked memory (torch's
     caching host allocator), so the device-to-host copy of a frame runs at
@@ -215,7 +228,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         if not force and key == self._scene_key:
             return 0.0
         t0 = time.perf_counter()
-        packed = pack_scene(scene)
+        packed = _packed(scene, self.config.mode)
         self.last_update = None
         if (not force and self._packed is not None and self._scene_obj is scene
                 and self._update_in_place(_native.DEFAULT_SCENE, self._packed, packed)):
@@ -566,7 +579,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         if entry is not None:
             self._resident.move_to_end(key)
             return entry[0]
-        packed = pack_scene(scene)
+        packed = _packed(scene, self.config.mode)
         self.last_update = None
         # an older revision of the same scene is updated in place when the
         # in-place rules allow it and no queued job still renders it

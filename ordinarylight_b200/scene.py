@@ -28,7 +28,7 @@ import numpy as np
 
 __all__ = [
     "Transform", "Material", "Texture", "TextureTransform", "Mesh", "MeshResource", "Instance", "Scene",
-    "Volume", "VolumeMaterial",
+    "Volume", "VolumeMaterial", "Texture1D",
     "PerspectiveCamera", "OrthographicCamera", "PanoramicCamera",
     "PointLight", "DirectionalLight", "SpotLight", "EnvironmentLight",
     "CAMERA_TYPES", "LIGHT_TYPES",
@@ -552,42 +552,151 @@ class Instance(Mesh):
     """A placed occurrence of a MeshResource."""
 
 
-@dataclass
-class VolumeMaterial:
-    """Participating-medium parameters of a dense density grid."""
+@dataclass(frozen=True)
+class Texture1D:
+    """RGBA lookup table with its sampler state (scene/_core.py:137-186): the
+    transfer function of a volume.  Three-channel values get an opaque
+    alpha."""
 
-    sigma_t_scale: float = 1.0
-    albedo: float = 0.9
+    values: np.ndarray = field(compare=False, repr=False)
+    address_mode: str = "clamp"
+    linear_filter: bool = True
 
     def __post_init__(self):
-        if not (self.sigma_t_scale >= 0.0 and math.isfinite(self.sigma_t_scale)):
+        values = np.array(self.values, dtype=np.float32, copy=True)
+        if values.ndim != 2 or values.shape[1] not in (3, 4) or len(values) < 1:
+            raise ValueError("1D texture values must have shape (length, 3 or 4)")
+        if not np.all(np.isfinite(values)):
+            raise ValueError("1D texture values must be finite")
+        if values.shape[1] == 3:
+            values = np.column_stack((values, np.ones(len(values), np.float32)))
+        if self.address_mode not in ("clamp", "repeat", "mirror"):
+            raise ValueError("address_mode must be clamp, repeat, or mirror")
+        values = np.ascontiguousarray(values, np.float32)
+        values.flags.writeable = False
+        object.__setattr__(self, "values", values)
+
+
+def _identity_transfer():
+    return Texture1D(np.array([[0.0, 0.0, 0.0, 0.0], [1.0, 1.0, 1.0, 1.0]], np.float32))
+
+
+@dataclass(frozen=True)
+class VolumeMaterial:
+    """A volume's optical parameters.  The reference's fields
+    (scene/_core.py:189-246) drive the reference-compatible emission-
+    absorption ray march: the transfer function maps the normalized value to
+    emitted RGB and an opacity per ``step_size`` world units, with point-light
+    single scattering when ``scattering_scale`` > 0.  ``sigma_t_scale`` and
+    ``albedo`` drive the production transport's delta-tracked medium
+    (extinction = sigma_t_scale x value; unset, they are density_scale and
+    0.9, as for the reference's own material)."""
+
+    sigma_t_scale: float | None = None
+    albedo: float | None = None
+    transfer_function: Texture1D = field(default_factory=_identity_transfer)
+    density_scale: float = 1.0
+    emission_scale: float = 1.0
+    step_size: float = 0.01
+    scattering_scale: float = 0.0
+    scattering_color: tuple = (1.0, 1.0, 1.0)
+    phase_function: str = "isotropic"
+    anisotropy: float = 0.0
+    scattering_albedo: tuple = (0.9, 0.9, 0.9)
+    scattering_orders: int = 1
+
+    def __post_init__(self):
+        if self.sigma_t_scale is not None and not (self.sigma_t_scale >= 0.0 and math.isfinite(self.sigma_t_scale)):
             raise ValueError("sigma_t_scale must be finite and non-negative")
-        if not 0.0 <= self.albedo <= 1.0:
+        if self.albedo is not None and not 0.0 <= self.albedo <= 1.0:
             raise ValueError("albedo must be between zero and one")
+        if not isinstance(self.transfer_function, Texture1D):
+            raise TypeError("transfer_function must be a Texture1D")
+        for name in ("density_scale", "emission_scale", "scattering_scale"):
+            if not (math.isfinite(getattr(self, name)) and getattr(self, name) >= 0.0):
+                raise ValueError(f"{name} must be finite and non-negative")
+        if not (math.isfinite(self.step_size) and self.step_size > 0.0):
+            raise ValueError("step_size must be positive")
+        if self.phase_function not in ("isotropic", "henyey_greenstein"):
+            raise ValueError("phase_function must be 'isotropic' or 'henyey_greenstein'")
+        if not -0.99 <= self.anisotropy <= 0.99:
+            raise ValueError("anisotropy must be between -0.99 and 0.99")
+        albedo = _vec3(self.scattering_albedo, "scattering_albedo")
+        if np.any(albedo < 0.0) or np.any(albedo > 1.0):
+            raise ValueError("scattering_albedo components must be in [0, 1]")
+        if np.any(_vec3(self.scattering_color, "scattering_color") < 0.0):
+            raise ValueError("scattering_color components cannot be negative")
+        if isinstance(self.scattering_orders, bool) or not 1 <= int(self.scattering_orders) <= 8:
+            raise ValueError("scattering_orders must be between 1 and 8")
 
 
 @dataclass
 class Volume:
-    """Dense density grid (z, y, x) filling the unit box [0,1]^3 under
-    ``transform`` (scene/_core.py:249-400)."""
+    """Dense scalar field (z, y, x) filling the unit box [0,1]^3 under
+    ``transform`` (scene/_core.py:249-400): values are normalized over
+    ``value_range`` (linear, log or symlog mapping); with ``missing_data``
+    non-finite values are kept as missing; ``clip_planes`` (a, b, c, d) keep
+    the points with (a, b, c) . p >= d."""
 
     data: np.ndarray
     material: VolumeMaterial = field(default_factory=VolumeMaterial)
     transform: Transform = field(default_factory=Transform)
+    value_range: tuple | None = None
+    value_mapping: str = "linear"
+    linear_threshold: float = 1.0
+    missing_data: bool = False
+    clip_planes: tuple = ()
     visible: bool = True
     name: str | None = None
     id: int | None = field(default=None, init=False)
 
     def __post_init__(self):
-        d = np.ascontiguousarray(self.data, dtype=np.float32)
-        if d.ndim != 3 or min(d.shape) < 1:
-            raise ValueError("volume data must be a non-empty 3D array")
-        if not np.all(np.isfinite(d)) or np.any(d < 0.0):
-            raise ValueError("volume densities must be finite and non-negative")
+        d = np.array(self.data, dtype=np.float32, copy=True, order="C")
+        if d.ndim != 3 or min(d.shape) < 2:
+            raise ValueError("volume data must have shape (depth, height, width) with dimensions >= 2")
+        if self.missing_data:
+            d[~np.isfinite(d)] = np.nan
+        elif not np.all(np.isfinite(d)):
+            raise ValueError("volume data must contain finite values")
         d.flags.writeable = False
         self.data = d
+        if self.value_mapping not in ("linear", "log", "symlog"):
+            raise ValueError("value_mapping must be 'linear', 'log' or 'symlog'")
+        if self.value_range is None:
+            finite = d[np.isfinite(d)]
+            if not finite.size:
+                raise ValueError("volume data must contain at least one finite value")
+            lo, hi = float(finite.min()), float(finite.max())
+            self.value_range = (min(0.0, lo), max(1.0, lo)) if lo == hi else (lo, hi)
+        else:
+            self.value_range = tuple(float(v) for v in self.value_range)
+            if len(self.value_range) != 2 or not self.value_range[0] < self.value_range[1]:
+                raise ValueError("value_range must be two increasing values")
+        self.clip_planes = tuple(tuple(float(c) for c in plane) for plane in self.clip_planes)
+        if any(len(plane) != 4 for plane in self.clip_planes) or len(self.clip_planes) > 8:
+            raise ValueError("clip_planes must hold at most eight (a, b, c, d) planes")
         if not isinstance(self.transform, Transform):
             self.transform = Transform(self.transform)
+
+    @property
+    def shape(self):
+        return self.data.shape
+
+    @property
+    def normalized_data(self):
+        """Values mapped to [0, 1] over value_range (missing values NaN when
+        missing_data, else 0), as the reference normalizes them."""
+        low, high = self.value_range
+        with np.errstate(divide="ignore", invalid="ignore"):
+            if self.value_mapping == "log":
+                normalized = (np.log(self.data) - np.log(low)) / (np.log(high) - np.log(low))
+            elif self.value_mapping == "symlog":
+                f = lambda v: np.sign(v) * np.log1p(np.abs(v) / self.linear_threshold)  # noqa: E731
+                normalized = (f(self.data) - f(low)) / (f(high) - f(low))
+            else:
+                normalized = (self.data - low) / (high - low)
+        return np.ascontiguousarray(np.where(np.isfinite(normalized), np.clip(normalized, 0.0, 1.0),
+                                             np.nan if self.missing_data else 0.0))
 
 
 class Scene:
@@ -827,9 +936,11 @@ class Scene:
         self._changed(shading=True)
         return environment
 
-    def add_volume(self, data, material=None, *, transform=None, name=None):
+    def add_volume(self, data, material=None, *, transform=None, value_range=None, value_mapping="linear",
+                   linear_threshold=1.0, missing_data=False, clip_planes=(), visible=True, name=None):
         volume = Volume(data, material or VolumeMaterial(), Transform() if transform is None else transform,
-                        name=name)
+                        value_range=value_range, value_mapping=value_mapping, linear_threshold=linear_threshold,
+                        missing_data=missing_data, clip_planes=clip_planes, visible=visible, name=name)
         self._attach(volume)
         self.volumes.append(volume)
         self._changed(geometry=True, shading=True)

@@ -39,10 +39,11 @@ def make(name: str) -> None:
     spp = SAMPLES.get(name, DEFAULT_SAMPLES)
     t0 = time.time()
     mean, sem = production.render(scene, camera, w, h, samples=spp, max_bounces=case["max_bounces"],
-                                  rr_start=case["rr_start"], rr_min_survival=case["rr_min"], seed=SEED)
+                                  rr_start=case["rr_start"], rr_min_survival=case["rr_min"],
+                                  env_nee=case["env_nee"], seed=SEED)
     np.savez_compressed(HERE / f"production_{name}.npz", mean=mean.astype(np.float32), sem=sem.astype(np.float16),
                         samples=spp, seed=SEED, width=w, height=h, max_bounces=case["max_bounces"],
-                        rr_start=case["rr_start"], rr_min=case["rr_min"])
+                        rr_start=case["rr_start"], rr_min=case["rr_min"], env_nee=case["env_nee"])
     print(f"{name}: {spp} spp in {time.time() - t0:.1f} s, mean {mean.mean(axis=(0, 1))}", flush=True)
 
 

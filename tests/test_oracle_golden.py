@@ -69,6 +69,21 @@ def test_oracle_render_is_bit_identical_to_reference(golden):
     assert np.all(data["frame0"][..., 3] == 0.0)
 
 
+def test_oracle_volume_render_is_bit_identical_to_reference(golden):
+    """The reference's CpuReferenceRenderer on a room with two overlapping
+    volumes (emission, clip plane, missing data, log mapping, a mirrored
+    nearest transfer function, Henyey-Greenstein single scattering of point,
+    spot and directional lights with a second order): the oracle's ray
+    march (oracle/reference_volume.py) reproduces its image bit for bit."""
+    import parity_scenes
+
+    data = golden("volume_small.npz")
+    scene, camera = parity_scenes.volume_room()
+    image = ref.render_frame(scene, camera, int(data["width"]), int(data["height"]), samples=int(data["samples"]),
+                             max_bounces=int(data["max_bounces"]), seed=int(data["seed"]))
+    assert image.tobytes() == data["image"].tobytes()
+
+
 def test_oracle_counts_closest_hit_rays():
     scene, camera = scenes.box_room()
     counter = ref.RayCounter()

@@ -136,9 +136,13 @@ def test_one_bounce_under_a_unit_sky_is_the_directional_albedo(base, roughness, 
         assert np.all((got >= 0.85) & (got <= 1.01))
 
 
-@pytest.mark.parametrize("name", ["box_room", "ggx_r0.5_m1"])
+@pytest.mark.parametrize("name", ["box_room", "ggx_r0.5_m1", "ggx_r0.05_m1"])
 def test_the_oracles_estimators_agree(name):
-    from image_parity import compare, oracle_image_se
+    """Each estimator as 8 independent batches (seeds), so that the standard
+    errors come from batch means: BSDF sampling of small emitters off a
+    near-mirror is heavy-tailed, and its per-sample variance understates
+    the noise."""
+    from image_parity import batch_estimate, compare
 
     case = parity_scenes.CASES[name]
     scene, camera = parity_scenes.build(name)
@@ -147,13 +151,14 @@ def test_the_oracles_estimators_agree(name):
             scene.lights.remove(light)
     w, h = 32, 32
     runs = {}
-    for label, kw in (("full", {}), ("no-env-nee", dict(env_nee=False)), ("bsdf", dict(nee=False))):
-        runs[label] = production.render(scene, camera, w, h, samples=4096, max_bounces=case["max_bounces"],
-                                        rr_start=case["rr_start"], seed=hash(label) & 0xFFFF, **kw)
-    m0, s0 = runs["full"]
+    full = dict(env_nee=case["env_nee"])
+    for label, kw in (("full", full), ("no-env-nee", dict(env_nee=False)), ("bsdf", dict(nee=False))):
+        batches = [production.render(scene, camera, w, h, samples=512, max_bounces=case["max_bounces"],
+                                     rr_start=case["rr_start"], seed=1000 * k + len(label), **kw)[0]
+                   for k in range(8)]
+        runs[label] = batch_estimate(np.stack(batches))
     for label in ("no-env-nee", "bsdf"):
-        m1, s1 = runs[label]
-        compare(m0, s0, oracle_image_se(s0), m1, s1, oracle_image_se(s1), tolerance=0.01, label=label)
+        compare(*runs["full"], *runs[label], tolerance=0.01, label=label)
 
 
 def test_oracle_geometry_reproduces_the_reference_hits(golden):
@@ -178,6 +183,6 @@ def test_production_fixtures_are_this_oracles_output(golden, name):
     x0, y0 = w // 2 - 1, h // 3
     mean, _ = production.render(scene, camera, w, h, samples=int(data["samples"]),
                                 max_bounces=int(data["max_bounces"]), rr_start=int(data["rr_start"]),
-                                rr_min_survival=float(data["rr_min"]), seed=int(data["seed"]),
-                                window=(x0, y0, 3, 2))
+                                rr_min_survival=float(data["rr_min"]), env_nee=bool(data["env_nee"]),
+                                seed=int(data["seed"]), window=(x0, y0, 3, 2))
     assert mean.astype(np.float32).tobytes() == data["mean"][y0:y0 + 2, x0:x0 + 3].tobytes()
