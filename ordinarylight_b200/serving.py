@@ -1,4 +1,5 @@
-"""Served rendering: a request loop with continuous batching on one device.
+"""Served rendering: a request loop with continuous batching on one device,
+and a router that places requests across one such loop per GPU.
 
 The reference renders submissions one at a time on a renderer-owned worker
 (``Renderer.render_async`` -> ``_render_serialized``,
@@ -290,6 +291,131 @@ class SerialServer(RenderServer):
                 self._running = False
 
 
+class ReplicaRouter:
+    """Serving across GPUs: one :class:`RenderServer` per device (each with
+    its own renderer, scene pool and budget) behind one ``submit``.  The
+    path shards by request, so the GPUs exchange nothing; the router only
+    places requests.
+
+    Placement is by scene affinity and outstanding work (the paths, width x
+    height x samples, of a replica's unfinished requests):
+
+    * a request whose scene is already placed goes to the replica that holds
+      it, unless that replica's outstanding work exceeds the least-loaded
+      replica's by more than ``spill_factor`` x the request's own work (plus
+      ``spill_paths``); the request then goes to the least-loaded replica and
+      the scene becomes resident there too (a hot scene is replicated);
+    * a request with a new scene goes to the least-loaded replica (ties: the
+      one holding the fewest scenes, then the lowest index).
+
+    Each result is the image that replica's renderer produces, which is the
+    image any device produces: random numbers are keyed by (pixel, sample,
+    bounce, seed + frame_index), not by device or batch.
+    """
+
+    def __init__(self, servers, *, spill_factor: float = 2.0, spill_paths: int = 1 << 22):
+        if not servers:
+            raise ValueError("a router needs at least one server")
+        self.servers = list(servers)
+        self.spill_factor = float(spill_factor)
+        self.spill_paths = int(spill_paths)
+        self._lock = threading.Lock()
+        self._outstanding = [0] * len(self.servers)
+        self._holders: dict[int, list[int]] = {}    # scene key -> replicas it was placed on
+        self._scenes_on = [0] * len(self.servers)
+        self.placements: list[int] = []             # replica of every submitted request, in order
+
+    @staticmethod
+    def _scene_key(scene) -> int:
+        return id(scene)
+
+    @staticmethod
+    def _work(request: RenderRequest) -> int:
+        spp = request.samples if request.samples is not None else 1
+        return int(request.width) * int(request.height) * int(spp)
+
+    def place(self, request: RenderRequest) -> int:
+        """The replica `request` goes to (and books its work there)."""
+        work = self._work(request)
+        key = self._scene_key(request.scene)
+        with self._lock:
+            least = min(range(len(self.servers)), key=lambda i: (self._outstanding[i], self._scenes_on[i], i))
+            holders = self._holders.get(key, [])
+            choice = least
+            if holders:
+                best = min(holders, key=lambda i: (self._outstanding[i], i))
+                if self._outstanding[best] <= self._outstanding[least] + self.spill_factor * work + self.spill_paths:
+                    choice = best
+            if choice not in holders:
+                self._holders.setdefault(key, []).append(choice)
+                self._scenes_on[choice] += 1
+            self._outstanding[choice] += work
+            self.placements.append(choice)
+            return choice
+
+    def _done(self, replica: int, work: int):
+        with self._lock:
+            self._outstanding[replica] -= work
+
+    def submit(self, request: RenderRequest) -> Future:
+        replica = self.place(request)
+        work = self._work(request)
+        try:
+            future = self.servers[replica].submit(request)
+        except BaseException:
+            self._done(replica, work)
+            raise
+        future.add_done_callback(lambda _f: self._done(replica, work))
+        return future
+
+    def outstanding(self) -> list:
+        with self._lock:
+            return list(self._outstanding)
+
+    def start(self):
+        for server in self.servers:
+            server.start()
+        return self
+
+    def stop(self, *, drain: bool = True, timeout: float | None = None):
+        errors = []
+        for server in self.servers:
+            try:
+                server.stop(drain=drain, timeout=timeout)
+            except BaseException as exc:   # stop every replica, then report
+                errors.append(exc)
+        if errors:
+            raise errors[0]
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *_exc):
+        self.stop()
+
+    def summary(self) -> dict:
+        """Statistics over all replicas: latency percentiles of every
+        completed request, throughput over the longest replica wall time."""
+        lat, rays, gpu_ms, completed, rejected, failed, steps = [], 0, 0.0, 0, 0, 0, 0
+        started = min(s.stats.started for s in self.servers)
+        finished = max(s.stats.finished for s in self.servers)
+        for s in self.servers:
+            st = s.stats
+            lat += st.latencies_ms
+            rays += st.rays
+            gpu_ms += st.gpu_ms
+            completed += st.completed
+            rejected += st.rejected
+            failed += st.failed
+            steps += st.steps
+        wall = max(finished - started, 1e-9)
+        return {"replicas": len(self.servers), "completed": completed, "rejected": rejected, "failed": failed,
+                "p50_ms": float(np.percentile(lat, 50)) if lat else float("nan"),
+                "p99_ms": float(np.percentile(lat, 99)) if lat else float("nan"),
+                "throughput_req_s": completed / wall, "mrays_per_s": rays / wall / 1e6, "steps": steps,
+                "per_replica_requests": [self.placements.count(i) for i in range(len(self.servers))]}
+
+
 def poisson_arrivals(rate_per_s: float, count: int, seed: int = 0) -> np.ndarray:
     """Arrival times (seconds from 0) of a Poisson stream."""
     rng = np.random.default_rng(seed)
@@ -314,5 +440,5 @@ def run_stream(server: RenderServer, requests, arrivals) -> list:
     return futures
 
 
-__all__ = ["AdmissionRejected", "RenderServer", "SerialServer", "ServerStatistics", "poisson_arrivals",
+__all__ = ["AdmissionRejected", "RenderServer", "ReplicaRouter", "SerialServer", "ServerStatistics", "poisson_arrivals",
            "run_stream", "DEFAULT_BUDGET_BYTES"]

@@ -253,3 +253,92 @@ def test_autotuner_coordinate_descent():
     again = autotune(r, reqs, repeats=1)          # cached: no new trials
     calls = r.calls
     assert autotune(r, reqs, repeats=1) is again and r.calls == calls
+
+
+# ---------------------------------------------------------------------------
+# multi-GPU placement (ReplicaRouter): one RenderServer per device
+# ---------------------------------------------------------------------------
+class _StubServer:
+    """Accepts submissions and leaves their futures pending until `finish`."""
+
+    def __init__(self):
+        self.requests = []
+        self.futures = []
+
+    def submit(self, request):
+        from concurrent.futures import Future
+
+        f = Future()
+        self.requests.append(request)
+        self.futures.append(f)
+        return f
+
+    def finish(self):
+        for f in self.futures:
+            if not f.done():
+                f.set_result(None)
+
+
+def test_router_keeps_a_scenes_requests_on_one_replica_and_spreads_new_scenes():
+    from ordinarylight_b200.serving import ReplicaRouter
+
+    a, b, c = FakeScene("a", 10), FakeScene("b", 10), FakeScene("c", 10)
+    servers = [_StubServer(), _StubServer()]
+    router = ReplicaRouter(servers, spill_factor=2.0, spill_paths=0)
+    for scene in (a, b, a, b, a):
+        router.submit(_req(scene, 8, 8))
+    assert router.placements == [0, 1, 0, 1, 0]
+    assert [r.scene for r in servers[0].requests] == [a, a, a]
+    router.submit(_req(c, 8, 8))          # new scene: the less loaded replica
+    assert router.placements[-1] == 1
+
+
+def test_router_replicates_a_hot_scene_when_its_holder_is_overloaded():
+    from ordinarylight_b200.serving import ReplicaRouter
+
+    hot = FakeScene("hot", 10)
+    servers = [_StubServer(), _StubServer()]
+    router = ReplicaRouter(servers, spill_factor=1.0, spill_paths=0)
+    placed = [router.place(_req(hot, 16, 16)) for _ in range(4)]
+    # holder 0 takes requests while it is within one request's work of the
+    # least-loaded replica, then the scene spills onto replica 1 as well,
+    # and the less loaded of its two holders takes the next one
+    assert placed == [0, 0, 1, 1]
+    assert router.outstanding() == [512, 512]
+
+
+def test_router_releases_work_on_completion_and_is_deterministic():
+    from ordinarylight_b200.serving import ReplicaRouter
+
+    scenes = [FakeScene(str(k), 10) for k in range(5)]
+    runs = []
+    for _ in range(2):
+        servers = [_StubServer() for _ in range(3)]
+        router = ReplicaRouter(servers, spill_factor=1.5, spill_paths=64)
+        rng = np.random.default_rng(3)
+        for k in range(40):
+            router.submit(_req(scenes[int(rng.integers(5))], 8, 8, int(rng.integers(1, 4))))
+        runs.append(list(router.placements))
+        for s in servers:
+            s.finish()
+        assert router.outstanding() == [0, 0, 0]
+        assert sum(len(s.requests) for s in servers) == 40
+    assert runs[0] == runs[1]
+    assert len(set(runs[0])) == 3          # every replica gets work
+
+
+def test_router_over_two_servers_returns_every_image():
+    """Two RenderServers stand in for two GPUs (each with its own fake
+    renderer): every request completes with its own replica's image and the
+    merged statistics count each once."""
+    from ordinarylight_b200.serving import ReplicaRouter
+
+    scenes = [FakeScene(str(k), 100) for k in range(4)]
+    servers = [RenderServer(FakeRenderer(paths_per_step=5000), budget_bytes=10**9) for _ in range(2)]
+    with ReplicaRouter(servers) as router:
+        futures = [router.submit(_req(scenes[k % 4], 16, 8, 2)) for k in range(12)]
+        images = [f.result(timeout=10) for f in futures]
+    assert all(img.shape == (8, 16, 4) for img in images)
+    s = router.summary()
+    assert s["completed"] == 12 and s["replicas"] == 2 and sum(s["per_replica_requests"]) == 12
+    assert min(s["per_replica_requests"]) > 0
