@@ -318,12 +318,18 @@ def run_ours(args, rank, world, device_index):
         with torch.cuda.stream(stream):
             ends[k].record(stream)
         rays += renderer.last_timings["rays"]
+        restir_records = 0
         for stage, _b, items, misses, ms in _profile(renderer):
             stage_ms[stage] = stage_ms.get(stage, 0.0) + ms
             stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, items, misses)
             stage_launches[stage] = stage_launches.get(stage, 0) + 1
-            launches += 3 if stage in ("restir", "sort") else 1   # restir: compaction, initial, one spatial
-                                                                     # pass; sort: keys, scan, scatter
+            if stage == "restir":
+                # per chunk two records: resampling (compaction, initial, one
+                # spatial pass), then the reservoir samples' shadow-ray emission
+                launches += 3 if restir_records % 2 == 0 else 1
+                restir_records += 1
+            else:
+                launches += 3 if stage == "sort" else 1   # sort: keys, scan, scatter
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]

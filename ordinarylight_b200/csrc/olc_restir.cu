@@ -12,9 +12,11 @@
 // merge, spatial merge, final visibility (here: the bounce-0 shadow ray).
 // Target p_hat = luminance(f * Le * G) without visibility.
 //
-// Storage: two uint4 words per reservoir,
+// Storage: three uint4 words per reservoir,
 //   w0 = (light index, barycentrics as half2, w_sum, M)
 //   w1 = (p_hat of the selected sample, primary depth, octahedral normal, stamp)
+//   w2 = (primary surface position, 0): where the support test of the
+//        unbiased combination evaluates a reused reservoir's target
 // indexed by the job's reservoir base + sample stream * npix + pixel, so a
 // stream's reservoirs survive chunking and batching.  A reservoir is valid
 // only when its stamp equals the stamp of the wavefront that should have
@@ -28,12 +30,14 @@
 #include "olc_restir.h"
 #include "olc_shading.cuh"
 #include "olc_textures.cuh"
+#include "olc_volume.cuh"
 
 namespace olc {
 
 namespace {
 
 constexpr uint32_t kRestirStream = 0x52455354u;  // stream key offset of the reuse passes
+constexpr uint32_t kMaxNeighbours = 16;          // restir_neighbours' upper bound
 
 OLC_D uint32_t lane() { return threadIdx.x & 31u; }
 
@@ -156,34 +160,18 @@ OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float
   }
 }
 
-// Whether light sample (light, bary) lies in the support of the target at a
-// surface (position p, viewer-side shading normal n, view direction): the
-// conditions under which target_of is not zero (the BSDF of an opaque
-// surface is positive wherever both cosines are; emitters have positive
-// luminance).
-OLC_D bool in_support(const SceneView& sc, uint32_t light, uint32_t bary, float3 p, float3 n, float3 view) {
-  if (!(dot(n, view) > 0.0f)) return false;
-  const EmitterRec e = load_emitter(sc, light);
-  const float2 b = unpack_bary(bary);
+// Whether light sample (emitter e, barycentrics b) lies in the support of
+// the target at a surface (position p, viewer-side shading normal n): both
+// cosines positive.  Only reservoirs with a positive target of their own
+// sample are ever reused, so their surfaces face the viewer (n.v > 0); the
+// BSDF of an opaque surface is positive wherever both cosines are, and
+// emitters have positive luminance, so this is where target_of is not zero.
+OLC_D bool in_support(const EmitterRec& e, float2 b, float3 p, float3 n) {
   const float3 off = emitter_point(e, b.x, b.y) - p;
   const float d2 = dot(off, off);
   if (!(d2 > 1e-12f)) return false;
   const float3 l = off * rsqrtf(d2);
   return dot(n, l) > 0.0f && emitter_cosine(e, l) > 1e-6f;
-}
-
-// The surface a stored reservoir belongs to, rebuilt from its primary depth
-// and normal along the camera ray of (pixel, sample stream, frame): the
-// reservoir's own pixel in the same frame, or in the previous frame for the
-// temporal history (the same camera, by the history's rule).
-OLC_D void stored_surface(const JobRec& job, uint32_t pixel, uint32_t sample, uint32_t frame, float depth,
-                          uint32_t normal, float3& p, float3& n, float3& view) {
-  const float2 jitter = olc_camera_jitter(pixel, sample, frame);
-  float3 o, d;
-  camera_ray(job, pixel, sample, &jitter, o, d);
-  p = o + d * depth;
-  n = oct_decode(normal);
-  view = -d;
 }
 
 // Unbiased normalisation of a combined reservoir (Bitterli et al. 2020,
@@ -197,10 +185,20 @@ OLC_D void normalise_support(Res& r, uint32_t Z) {
   if (Z > 0u && Z < r.M) r.w_sum *= (float)r.M / (float)Z;
 }
 
-// Primary surface of path slot i (its ray hit: only listed hits get here).
+// The primary vertex of path slot i (its ray hit: only listed hits get
+// here) as the shading stage sees it at bounce 0: position, viewer-side
+// shading normal (normal-mapped when textured), material (textured; the
+// camera ray's cone has width 0), view direction, depth.
+struct PrimaryVertex {
+  float3 p, n, view;
+  SurfaceMat m;
+  float depth;
+};
+
 template <bool kTextures>
-OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i, uint32_t scene) {
-  Surface su;
+OLC_D PrimaryVertex primary_vertex(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i,
+                                   uint32_t scene) {
+  PrimaryVertex pv;
   const float4 hit = h.tuv_slot[i];
   const float4 dr = q.dir_root[i];
   const float4 ot = q.origin_tmin[i];
@@ -220,21 +218,30 @@ OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBu
   if (!(dot(ns, ns) > 0.5f)) ns = ng;
   if (dot(ns, ng) < 0.0f) ns = -ns;
   const bool entering = dot(d, ng) < 0.0f;
-  su.p = f3(ot) + d * hit.x;
+  pv.p = f3(ot) + d * hit.x;
   const uint32_t owner = owner_instance(s.instances, s.tri_owner, inst, slot);
   const uint32_t mi = s.instances[owner].material;
-  SurfaceMat mat = load_material(s, mi);
-  // the textured material and mapped normal the shading stage will see (the
-  // camera ray's cone has width 0)
+  pv.m = load_material(s, mi);
   const SceneRec& sc = s.scenes[scene];
   if (kTextures && sc.tex_words != nullptr) {
     const TexturedHit th = apply_textures(sc, mi - sc.material_base, slot, v0, v1, v2, o2w, w2o, tn, hit.y, hit.z,
-                                          0.0f, ng, ns, mat);
-    mat = th.m;
+                                          0.0f, ng, ns, pv.m);
+    pv.m = th.m;
     ns = th.ns;
   }
-  su.bsdf = prepare_bsdf(mat, entering ? ns : -ns, -d);
-  su.depth = hit.x;
+  pv.n = entering ? ns : -ns;
+  pv.view = -d;
+  pv.depth = hit.x;
+  return pv;
+}
+
+template <bool kTextures>
+OLC_D Surface primary_surface(const SceneView& s, const RayQueue& q, const HitBuf& h, uint32_t i, uint32_t scene) {
+  const PrimaryVertex pv = primary_vertex<kTextures>(s, q, h, i, scene);
+  Surface su;
+  su.p = pv.p;
+  su.bsdf = prepare_bsdf(pv.m, pv.n, pv.view);
+  su.depth = pv.depth;
   return su;
 }
 
@@ -243,9 +250,15 @@ OLC_D bool similar(const Surface& s, uint32_t w1_normal, float depth) {
   return fabsf(depth - s.depth) <= 0.1f * s.depth;
 }
 
-OLC_D void store_res(uint4* w0, uint4* w1, uint64_t g, const Res& r, const Surface& s, uint32_t stamp) {
+OLC_D void store_res(uint4* w0, uint4* w1, uint4* w2, uint64_t g, const Res& r, const Surface& s, uint32_t stamp) {
   w0[g] = make_uint4(r.light, r.bary, __float_as_uint(r.w_sum), r.M);
   w1[g] = make_uint4(__float_as_uint(r.target), __float_as_uint(s.depth), oct_encode(s.bsdf.n), stamp);
+  w2[g] = make_uint4(__float_as_uint(s.p.x), __float_as_uint(s.p.y), __float_as_uint(s.p.z), 0u);
+}
+
+OLC_D float3 stored_position(const uint4* w2, uint64_t g) {
+  const uint4 v = w2[g];
+  return f3(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z));
 }
 
 OLC_D Res load_res(const uint4* w0, const uint4* w1, uint64_t g, float& depth, uint32_t& nrm, uint32_t& stamp) {
@@ -282,10 +295,13 @@ struct RestirArgs {
   float radius;
   const uint4* hist0;
   const uint4* hist1;
+  const uint4* hist2;
   const uint4* in0;
   const uint4* in1;
+  const uint4* in2;
   uint4* out0;
   uint4* out1;
+  uint4* out2;
   uint32_t pass;
   uint4* selected;
   uint32_t finalize;
@@ -352,13 +368,13 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
         // the candidates always count; the history only where the selected
         // sample is in the support of the previous frame's target
         if (r.light != 0xffffffffu) {
-          float3 hp, hn, hv;
-          stored_surface(job, meta.x, meta.y, job.frame - 1u, pd, pn, hp, hn, hv);
-          normalise_support(r, r.M - (in_support(s, r.light, r.bary, hp, hn, hv) ? 0u : m));
+          const bool supported = in_support(load_emitter(s, r.light), unpack_bary(r.bary),
+                                            stored_position(a.hist2, gh), oct_decode(pn));
+          normalise_support(r, r.M - (supported ? 0u : m));
         }
       }
     }
-    store_res(a.out0, a.out1, g, r, su, stamp);
+    store_res(a.out0, a.out1, a.out2, g, r, su, stamp);
   }
 }
 
@@ -380,9 +396,8 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
     if (a.neighbours > 0u) {
       const uint32_t rng0 = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 1u + a.pass);
       const int px = (int)(meta.x % job.width), py = (int)(meta.x / job.width);
-      // The j-th neighbour of this pixel from the pass's stream (drawn the
-      // same way twice: to merge, then to normalise); false when it is off
-      // the image, this pixel, invalid or not similar.
+      // The j-th neighbour of this pixel from the pass's stream; false when
+      // it is off the image, this pixel, invalid or not similar.
       auto neighbour = [&](uint32_t& rng, uint32_t& q, Res& nb, float& dq, uint32_t& nq, float& u) {
         float rr = a.radius * sqrtf(olc_rand(rng));
         float th = 2.0f * OLC_PI * olc_rand(rng);
@@ -398,6 +413,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
         return sq == stamp && nb.light != 0xffffffffu && nb.M != 0u && nb.target > 0.0f && similar(su, nq, dq);
       };
       uint32_t rng = rng0;
+      uint32_t reused_q[kMaxNeighbours];
       uint32_t reused = 0;
       for (uint32_t j = 0; j < a.neighbours; ++j) {
         uint32_t q, nq;
@@ -406,27 +422,25 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
         if (!neighbour(rng, q, nb, dq, nq, u)) continue;
         float t = target_of(s, su, nb.light, nb.bary);
         res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u);
-        ++reused;
+        reused_q[reused++] = q;
       }
       if (reused && r.light != 0xffffffffu) {
         // this pixel's reservoir always counts (the selected sample has a
-        // positive target here); each neighbour where the sample is in the
-        // support of its own target
+        // positive target here); each reused neighbour where the sample is
+        // in the support of its own target
+        const EmitterRec e = load_emitter(s, r.light);
+        const float2 b = unpack_bary(r.bary);
         uint32_t Z = r.M;
-        rng = rng0;
-        for (uint32_t j = 0; j < a.neighbours; ++j) {
-          uint32_t q, nq;
-          Res nb;
-          float dq, u;
-          if (!neighbour(rng, q, nb, dq, nq, u)) continue;
-          float3 qp, qn, qv;
-          stored_surface(job, q, meta.y, job.frame, dq, nq, qp, qn, qv);
-          if (!in_support(s, r.light, r.bary, qp, qn, qv)) Z -= nb.M;
+        for (uint32_t k = 0; k < reused; ++k) {
+          const uint64_t gq = stream_base + reused_q[k];
+          const uint4 w0 = a.in0[gq];
+          const uint4 w1 = a.in1[gq];
+          if (!in_support(e, b, stored_position(a.in2, gq), oct_decode(w1.z))) Z -= w0.w;
         }
         normalise_support(r, Z);
       }
     }
-    store_res(a.out0, a.out1, g, r, su, stamp);
+    store_res(a.out0, a.out1, a.out2, g, r, su, stamp);
     if (a.finalize) {
       float W = (r.light != 0xffffffffu && r.M > 0u && r.target > 0.0f) ? r.w_sum / ((float)r.M * r.target) : 0.0f;
       if (!(W == W) || W > 3.0e38f) W = 0.0f;
@@ -435,17 +449,109 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
   }
 }
 
+// The reservoir samples' shadow rays: for every listed primary hit whose
+// shading pass chose its reservoir (OLC_PATH_FLAG_RESERVOIR_SHADOW), the
+// contribution of the selected light sample, f Le cos G W (times 2 when the
+// scene's analytic lights shared the choice; a camera path's throughput is 1
+// at its first surface), appended to the bounce-0 shadow queue, which is
+// traced after it.  Runs on the side stream once both resampling and the
+// bounce-0 shading pass are done, beside the bounce-1 closest-hit rays.
+struct EmitArgs {
+  const JobRec* jobs;
+  SceneView s;
+  RayQueue q;
+  HitBuf h;
+  PathState ps;
+  ShadowQueue sq;
+  Counters* cnt;
+  const uint32_t* hit_list;
+  const uint32_t* hit_count;
+  const uint4* selected;
+  uint32_t capacity;
+};
+
+template <bool kTextures>
+__global__ void __launch_bounds__(128) k_restir_emit(EmitArgs a) {
+  const SceneView& s = a.s;
+  const uint32_t n = *a.hit_count;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t k = base + lane();
+    bool want = false;
+    float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), sh_c = f3(0, 0, 0);
+    float sh_tmax = 0.0f;
+    uint32_t path = 0, root = 0;
+    if (k < n) {
+      const uint32_t i = a.hit_list[k];
+      path = a.q.path[i];
+      const uint4 meta = a.ps.meta[path];
+      const uint4 sel = a.selected[i];
+      const float W = __uint_as_float(sel.z);
+      if (((meta.z >> 8) & OLC_PATH_FLAG_RESERVOIR_SHADOW) && sel.x != 0xffffffffu && W > 0.0f) {
+        const JobRec& job = a.jobs[meta.w];
+        const SceneRec& sc = s.scenes[job.scene];
+        const PrimaryVertex pv = primary_vertex<kTextures>(s, a.q, a.h, i, job.scene);
+        const EmitterRec e = load_emitter(s, sel.x);
+        const float2 b = unpack_bary(sel.y);
+        const float3 off = emitter_point(e, b.x, b.y) - pv.p;
+        const float dist2 = dot(off, off);
+        const float dist = sqrtf(dist2);
+        const float3 ldir = off / fmaxf(dist, 1e-6f);
+        const float scos = fmaxf(dot(pv.n, ldir), 0.0f);
+        const float lc = emitter_cosine(e, ldir);
+        if (scos > 0.0f && lc > 1e-6f) {
+          const float pick = (job.nee && sc.num_lights > 0u) ? 2.0f : 1.0f;
+          const float G = lc / fmaxf(dist2, 1e-12f);
+          sh_c = pbr_eval(pv.m, pv.n, pv.view, ldir) * f3(e.emission) * (scos * G * W * pick);
+          sh_o = pv.p + pv.n * 0.002f;
+          sh_d = ldir;
+          sh_tmax = fmaxf(dist - 0.004f, 0.001f);
+          Medium med;
+          if (load_medium(sc, med)) {
+            uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 64u);
+            sh_c *= medium_transmittance(med, sh_o, sh_d, sh_tmax, rng);
+          }
+          want = sh_c.x > 0.0f || sh_c.y > 0.0f || sh_c.z > 0.0f;
+          root = __float_as_uint(a.q.dir_root[i].w);
+        }
+      }
+    }
+    // warp-aggregated append to the bounce-0 shadow queue
+    const uint32_t ballot = __ballot_sync(0xffffffffu, want);
+    uint32_t first = 0;
+    if (ballot && lane() == (uint32_t)(__ffs(ballot) - 1)) first = atomicAdd(&a.cnt->shadow_count[0], __popc(ballot));
+    first = __shfl_sync(0xffffffffu, first, __ffs(ballot | 1u) - 1);
+    if (want) {
+      const uint32_t slot = first + __popc(ballot & ((1u << lane()) - 1u));
+      if (slot < a.capacity) {
+        a.sq.origin_tmax[slot] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
+        a.sq.dir_path[slot] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(path));
+        a.sq.contrib_root[slot] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(root));
+      } else {
+        atomicAdd(&a.cnt->overflow, 1u);
+      }
+    }
+  }
+}
+
 }  // namespace
+
+void restir_emit(RestirState& st, const LaunchShape& ls, const SceneView& s, const JobRec* jobs, const RayQueue& q,
+                 const HitBuf& hits, const PathState& ps, const ShadowQueue& sq, Counters* cnt, uint32_t capacity,
+                 bool textures, cudaStream_t stream) {
+  EmitArgs a{jobs, s, q, hits, ps, sq, cnt, st.hit_list.as<uint32_t>(), st.hit_count.as<uint32_t>(),
+             st.selected.as<uint4>(), capacity};
+  if (textures) k_restir_emit<true><<<ls.grid_shade, 128, 0, stream>>>(a);
+  else k_restir_emit<false><<<ls.grid_shade, 128, 0, stream>>>(a);
+  OLC_LAUNCH_CHECK("k_restir_emit");
+}
 
 void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks) {
   if (reservoirs > st.reservoirs) {
     // the history survives only if its buffers are kept
-    st.res_a0.allocate(reservoirs * 16);
-    st.res_a1.allocate(reservoirs * 16);
-    st.res_b0.allocate(reservoirs * 16);
-    st.res_b1.allocate(reservoirs * 16);
-    st.hist0.allocate(reservoirs * 16);
-    st.hist1.allocate(reservoirs * 16);
+    for (DeviceBuffer* b : {&st.res_a0, &st.res_a1, &st.res_a2, &st.res_b0, &st.res_b1, &st.res_b2, &st.hist0,
+                            &st.hist1, &st.hist2})
+      b->allocate(reservoirs * 16);
     // stamps start at 1: zero-filled reservoirs are never valid
     for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, reservoirs * 16));
     st.reservoirs = reservoirs;
@@ -487,9 +593,11 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.radius = cfg.restir_radius > 0.0f ? cfg.restir_radius : 30.0f;
   a.hist0 = st.hist0.as<uint4>();
   a.hist1 = st.hist1.as<uint4>();
+  a.hist2 = st.hist2.as<uint4>();
   a.selected = st.selected.as<uint4>();
   a.out0 = st.res_a0.as<uint4>();
   a.out1 = st.res_a1.as<uint4>();
+  a.out2 = st.res_a2.as<uint4>();
   OLC_CUDA(cudaMemsetAsync(st.hit_count.get(), 0, 4, stream));
   k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, hits, ps, st.hit_list.as<uint32_t>(),
                                                         st.hit_count.as<uint32_t>());
@@ -507,8 +615,10 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
     b.neighbours = cfg.restir_spatial ? cfg.restir_neighbours : 0u;
     b.in0 = in_a ? st.res_a0.as<uint4>() : st.res_b0.as<uint4>();
     b.in1 = in_a ? st.res_a1.as<uint4>() : st.res_b1.as<uint4>();
+    b.in2 = in_a ? st.res_a2.as<uint4>() : st.res_b2.as<uint4>();
     b.out0 = in_a ? st.res_b0.as<uint4>() : st.res_a0.as<uint4>();
     b.out1 = in_a ? st.res_b1.as<uint4>() : st.res_a1.as<uint4>();
+    b.out2 = in_a ? st.res_b2.as<uint4>() : st.res_a2.as<uint4>();
     b.finalize = (p + 1 == passes) ? 1u : 0u;
     if (textures) k_restir_spatial<true><<<grid, 128, 0, stream>>>(b);
     else k_restir_spatial<false><<<grid, 128, 0, stream>>>(b);
@@ -526,9 +636,11 @@ void restir_finish(RestirState& st) {
   if (st.final_in_b) {
     std::swap(st.hist0, st.res_b0);
     std::swap(st.hist1, st.res_b1);
+    std::swap(st.hist2, st.res_b2);
   } else {
     std::swap(st.hist0, st.res_a0);
     std::swap(st.hist1, st.res_a1);
+    std::swap(st.hist2, st.res_a2);
   }
 }
 
@@ -538,12 +650,9 @@ void restir_reset(RestirState& st) {
 }
 
 void restir_release(RestirState& st) {
-  st.res_a0.release();
-  st.res_a1.release();
-  st.res_b0.release();
-  st.res_b1.release();
-  st.hist0.release();
-  st.hist1.release();
+  for (DeviceBuffer* b : {&st.res_a0, &st.res_a1, &st.res_a2, &st.res_b0, &st.res_b1, &st.res_b2, &st.hist0,
+                          &st.hist1, &st.hist2})
+    b->release();
   st.selected.release();
   st.hit_list.release();
   st.hit_count.release();

