@@ -307,7 +307,7 @@ struct olc_context {
   uint32_t default_scene = kNoScene;
   // wavefront buffers
   uint32_t capacity = 0;
-  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, hit_tuv1, hit_inst1, sh_o, sh_d, sh_c, ps_tp,
+  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
       ps_rad, ps_meta, ps_ior, ps_cone, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary, prod_signals,
@@ -1316,10 +1316,6 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   if (!ctx->sort_bins.get()) ctx->sort_bins.allocate(sort_bins_bytes());
   ctx->hit_tuv.allocate(c * 16);
   ctx->hit_inst.allocate(c * 4);
-  // a second hit buffer for odd bounces: the bounce-0 hits stay readable on
-  // the side stream (ReSTIR) while bounce 1 is traced
-  ctx->hit_tuv1.allocate(c * 16);
-  ctx->hit_inst1.allocate(c * 4);
   ctx->sh_o.allocate(c * 16);
   ctx->sh_d.allocate(c * 16);
   ctx->sh_c.allocate(c * 16);
@@ -1389,7 +1385,7 @@ void release_slot(RunSlot& sl) {
 
 struct RunBuffers {
   RayQueue qa, qb, qc;
-  HitBuf hb[2];            // hits of even and odd bounces
+  HitBuf hb;
   ShadowQueue sq;
   PathState ps;
   ProductPtrs prod;
@@ -1407,8 +1403,7 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.qa = RayQueue{ctx->q0_o.as<float4>(), ctx->q0_d.as<float4>(), ctx->q0_p.as<uint32_t>()};
   b.qb = RayQueue{ctx->q1_o.as<float4>(), ctx->q1_d.as<float4>(), ctx->q1_p.as<uint32_t>()};
   b.qc = RayQueue{ctx->q2_o.as<float4>(), ctx->q2_d.as<float4>(), ctx->q2_p.as<uint32_t>()};
-  b.hb[0] = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
-  b.hb[1] = HitBuf{ctx->hit_tuv1.as<float4>(), ctx->hit_inst1.as<uint32_t>()};
+  b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
   b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
   b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>(),
                    ctx->ps_ior.as<float4>(), ctx->ps_cone.as<float2>()};
@@ -1454,31 +1449,22 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         tl_mark(ctx, OLC_STAGE_SORT, b, c);
         std::swap(qin, spare);
       }
-      const HitBuf& hb = rb.hb[b & 1u];
-      launch_trace_closest(ctx->ls, s, *qin, hb, rb.cnt, b, st);
+      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, st);
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
-      const bool restir = b == 0 && ch.restir;
-      if (restir) {
-        // ReSTIR resampling reads only the bounce-0 hits and writes only
-        // reservoirs: it runs on the side stream beside bounce-0 shading (no
-        // side work is pending at bounce 0), and its shadow rays are emitted
-        // once both are done
-        OLC_CUDA(cudaEventRecord(ctx->fork_event, st));
-        OLC_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_event, 0));
-        const uint32_t rs_start = tl_record(ctx, ctx->side);
-        restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, hb, rb.ps, ch.textures, ctx->side);
-        const uint32_t rs_end = tl_record(ctx, ctx->side);
-        ctx->cur->entries.push_back(TimelineEntry{OLC_STAGE_RESTIR, b, c, rs_start, rs_end});
+      const uint4* restir = nullptr;
+      if (b == 0 && ch.restir) {
+        restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, ch.textures, st);
+        tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
       // shading adds to path radiance and refills the shadow queue: the
       // previous bounce's shadow rays must be done
       side_join(ctx);
       if (ch.ref_volumes) {
         // reference-compatible paths cross their scene's volumes before shading
-        launch_ref_volumes(ctx->ls, jobs, s, *qin, hb, rb.ps, rb.cnt, b, st);
+        launch_ref_volumes(ctx->ls, jobs, s, *qin, rb.hb, rb.ps, rb.cnt, b, st);
         tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       }
-      launch_shade(ctx->ls, jobs, s, *qin, hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
+      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
                    ch.textures, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       // this bounce's shadow rays on the side stream: they touch only the
@@ -1486,14 +1472,6 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
       // traversal runs beside them and fills their tail
       OLC_CUDA(cudaEventRecord(ctx->fork_event, st));
       OLC_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_event, 0));
-      if (restir) {
-        // the reservoir samples' shadow rays join the bounce-0 shadow queue
-        const uint32_t em_start = tl_record(ctx, ctx->side);
-        restir_emit(ctx->restir, ctx->ls, s, jobs, *qin, hb, rb.ps, rb.sq, rb.cnt, ctx->capacity, ch.textures,
-                    ctx->side);
-        const uint32_t em_end = tl_record(ctx, ctx->side);
-        ctx->cur->entries.push_back(TimelineEntry{OLC_STAGE_RESTIR, b, c, em_start, em_end});
-      }
       const uint32_t side_start = tl_record(ctx, ctx->side);
       launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, ctx->side);
       const uint32_t side_end = tl_record(ctx, ctx->side);
@@ -1528,8 +1506,7 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         (const void*)rb.qb.origin_tmin, (const void*)rb.qb.dir_root, (const void*)rb.qb.path,
                         (const void*)rb.qc.origin_tmin, (const void*)rb.qc.dir_root, (const void*)rb.qc.path,
                         ctx->sort_keys.get(), ctx->sort_bins.get(),
-                        (const void*)rb.hb[0].tuv_slot, (const void*)rb.hb[0].instance,
-                        (const void*)rb.hb[1].tuv_slot, (const void*)rb.hb[1].instance, (const void*)rb.sq.origin_tmax,
+                        (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
                         (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
                         (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.ps.cone, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
@@ -1994,7 +1971,7 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
   uint64_t wf = 0;
   for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p, &ctx->q2_o,
                                 &ctx->q2_d, &ctx->q2_p, &ctx->sort_keys, &ctx->sort_bins,
-                                &ctx->hit_tuv, &ctx->hit_inst, &ctx->hit_tuv1, &ctx->hit_inst1, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
+                                &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
                                 &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->ps_cone, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,

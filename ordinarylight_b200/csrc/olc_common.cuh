@@ -336,7 +336,6 @@ struct PathState {
 
 #define OLC_PATH_FLAG_PREV_NEE 1u     // the previous vertex sampled area lights
 #define OLC_PATH_FLAG_PREV_RESTIR 2u  // area lights of the previous vertex came from ReSTIR
-#define OLC_PATH_FLAG_RESERVOIR_SHADOW 4u  // the primary vertex's reservoir sample is still to be traced
 // Depth of the path's medium stack minus one (the reference's medium depth,
 // metadata.w >> 8, wavefront_shade.comp:447); entry 0 is the outside, IOR 1.
 #define OLC_PATH_DEPTH_SHIFT 4u

@@ -449,102 +449,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
   }
 }
 
-// The reservoir samples' shadow rays: for every listed primary hit whose
-// shading pass chose its reservoir (OLC_PATH_FLAG_RESERVOIR_SHADOW), the
-// contribution of the selected light sample, f Le cos G W (times 2 when the
-// scene's analytic lights shared the choice; a camera path's throughput is 1
-// at its first surface), appended to the bounce-0 shadow queue, which is
-// traced after it.  Runs on the side stream once both resampling and the
-// bounce-0 shading pass are done, beside the bounce-1 closest-hit rays.
-struct EmitArgs {
-  const JobRec* jobs;
-  SceneView s;
-  RayQueue q;
-  HitBuf h;
-  PathState ps;
-  ShadowQueue sq;
-  Counters* cnt;
-  const uint32_t* hit_list;
-  const uint32_t* hit_count;
-  const uint4* selected;
-  uint32_t capacity;
-};
-
-template <bool kTextures>
-__global__ void __launch_bounds__(128) k_restir_emit(EmitArgs a) {
-  const SceneView& s = a.s;
-  const uint32_t n = *a.hit_count;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-    const uint32_t k = base + lane();
-    bool want = false;
-    float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), sh_c = f3(0, 0, 0);
-    float sh_tmax = 0.0f;
-    uint32_t path = 0, root = 0;
-    if (k < n) {
-      const uint32_t i = a.hit_list[k];
-      path = a.q.path[i];
-      const uint4 meta = a.ps.meta[path];
-      const uint4 sel = a.selected[i];
-      const float W = __uint_as_float(sel.z);
-      if (((meta.z >> 8) & OLC_PATH_FLAG_RESERVOIR_SHADOW) && sel.x != 0xffffffffu && W > 0.0f) {
-        const JobRec& job = a.jobs[meta.w];
-        const SceneRec& sc = s.scenes[job.scene];
-        const PrimaryVertex pv = primary_vertex<kTextures>(s, a.q, a.h, i, job.scene);
-        const EmitterRec e = load_emitter(s, sel.x);
-        const float2 b = unpack_bary(sel.y);
-        const float3 off = emitter_point(e, b.x, b.y) - pv.p;
-        const float dist2 = dot(off, off);
-        const float dist = sqrtf(dist2);
-        const float3 ldir = off / fmaxf(dist, 1e-6f);
-        const float scos = fmaxf(dot(pv.n, ldir), 0.0f);
-        const float lc = emitter_cosine(e, ldir);
-        if (scos > 0.0f && lc > 1e-6f) {
-          const float pick = (job.nee && sc.num_lights > 0u) ? 2.0f : 1.0f;
-          const float G = lc / fmaxf(dist2, 1e-12f);
-          sh_c = pbr_eval(pv.m, pv.n, pv.view, ldir) * f3(e.emission) * (scos * G * W * pick);
-          sh_o = pv.p + pv.n * 0.002f;
-          sh_d = ldir;
-          sh_tmax = fmaxf(dist - 0.004f, 0.001f);
-          Medium med;
-          if (load_medium(sc, med)) {
-            uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream + 64u);
-            sh_c *= medium_transmittance(med, sh_o, sh_d, sh_tmax, rng);
-          }
-          want = sh_c.x > 0.0f || sh_c.y > 0.0f || sh_c.z > 0.0f;
-          root = __float_as_uint(a.q.dir_root[i].w);
-        }
-      }
-    }
-    // warp-aggregated append to the bounce-0 shadow queue
-    const uint32_t ballot = __ballot_sync(0xffffffffu, want);
-    uint32_t first = 0;
-    if (ballot && lane() == (uint32_t)(__ffs(ballot) - 1)) first = atomicAdd(&a.cnt->shadow_count[0], __popc(ballot));
-    first = __shfl_sync(0xffffffffu, first, __ffs(ballot | 1u) - 1);
-    if (want) {
-      const uint32_t slot = first + __popc(ballot & ((1u << lane()) - 1u));
-      if (slot < a.capacity) {
-        a.sq.origin_tmax[slot] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
-        a.sq.dir_path[slot] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(path));
-        a.sq.contrib_root[slot] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(root));
-      } else {
-        atomicAdd(&a.cnt->overflow, 1u);
-      }
-    }
-  }
-}
-
 }  // namespace
-
-void restir_emit(RestirState& st, const LaunchShape& ls, const SceneView& s, const JobRec* jobs, const RayQueue& q,
-                 const HitBuf& hits, const PathState& ps, const ShadowQueue& sq, Counters* cnt, uint32_t capacity,
-                 bool textures, cudaStream_t stream) {
-  EmitArgs a{jobs, s, q, hits, ps, sq, cnt, st.hit_list.as<uint32_t>(), st.hit_count.as<uint32_t>(),
-             st.selected.as<uint4>(), capacity};
-  if (textures) k_restir_emit<true><<<ls.grid_shade, 128, 0, stream>>>(a);
-  else k_restir_emit<false><<<ls.grid_shade, 128, 0, stream>>>(a);
-  OLC_LAUNCH_CHECK("k_restir_emit");
-}
 
 void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks) {
   if (reservoirs > st.reservoirs) {

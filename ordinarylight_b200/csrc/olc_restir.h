@@ -34,18 +34,12 @@ struct RestirState {
 // each chunk header).
 void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks);
 // Run initial RIS (+ temporal for jobs with history) + spatial reuse for one
-// chunk; returns the per-path-slot selected sample buffer consumed by
-// restir_emit.  Every host-side input is a pointer or a configuration value,
+// chunk; returns the per-path-slot selected sample buffer consumed by the
+// bounce-0 shading pass.  Every host-side input is a pointer or a configuration value,
 // so the launches can be captured in a graph and replayed.
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,
                         const ChunkHeader* hdr, const JobRec* jobs, const RayQueue& q, const HitBuf& hits,
                         const PathState& ps, bool textures, cudaStream_t stream);
-// Trace-ready shadow rays of the reservoir samples the bounce-0 shading pass
-// left to ReSTIR (appended to the bounce-0 shadow queue); after restir_run
-// and the bounce-0 shading pass.
-void restir_emit(RestirState& st, const LaunchShape& ls, const SceneView& s, const JobRec* jobs, const RayQueue& q,
-                 const HitBuf& hits, const PathState& ps, const ShadowQueue& sq, Counters* cnt, uint32_t capacity,
-                 bool textures, cudaStream_t stream);
 // Promote this wavefront's final reservoirs to history (plain frames only).
 void restir_finish(RestirState& st);
 void restir_reset(RestirState& st);

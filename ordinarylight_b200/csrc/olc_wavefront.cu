@@ -250,7 +250,7 @@ struct ShadeArgs {
   uint32_t bounce;
   uint32_t capacity;
   ProductPtrs prod;
-  uint32_t restir;       // this bounce-0 pass serves ReSTIR jobs (their reservoirs are traced separately)
+  const uint4* restir;   // per-path selected light sample (bounce 0), or null
 };
 
 // One next-event sample from p: an area emitter (alias-table choice, uniform
@@ -551,20 +551,42 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
             const float3 view = -d;
             bool did_restir = false;
             // ---- next-event estimation: one shadow ray per path per bounce
-            if (bounce == 0u && job.restir && a.restir && sc.num_emitters > 0u) {
+            if (bounce == 0u && job.restir && a.restir != nullptr && sc.num_emitters > 0u) {
+              uint4 rs = a.restir[path];
               did_restir = true;
               // A scene that also has analytic lights: one of the two
               // estimators runs, the reservoir's emitter sample or one
               // analytic light, each with probability 1/2 and its
-              // contribution divided by that probability.  The reservoir's
-              // sample is traced by k_restir_emit, which runs beside the
-              // next bounce once resampling (beside this pass) is done.
+              // contribution divided by that probability.
               const bool with_lights = job.nee && sc.num_lights > 0u;
-              if (!with_lights || olc_rand(rng) < 0.5f) {
-                new_flags |= OLC_PATH_FLAG_RESERVOIR_SHADOW;
-              } else {
+              const bool use_reservoir = !with_lights || olc_rand(rng) < 0.5f;
+              const float pick = with_lights ? 2.0f : 1.0f;
+              float Wr = __uint_as_float(rs.z) * pick;
+              if (!use_reservoir) {
                 want_shadow = next_event(s, sc, m, p, nrm, view, tp, false, rng, sh_o, sh_d, sh_tmax, sh_c, true);
-                sh_c *= 2.0f;
+                sh_c *= pick;
+              } else if (rs.x != 0xffffffffu && Wr > 0.0f) {
+                const EmitterRec e = load_emitter(s, rs.x);
+                float2 bary = __half22float2(*reinterpret_cast<const __half2*>(&rs.y));
+                float3 lp = emitter_point(e, bary.x, bary.y);
+                float3 off = lp - p;
+                float dist2 = dot(off, off);
+                float dist = sqrtf(dist2);
+                float3 ldir = off / fmaxf(dist, 1e-6f);
+                float scos = fmaxf(dot(nrm, ldir), 0.0f);
+                float lc = emitter_cosine(e, ldir);
+                if (scos > 0.0f && lc > 1e-6f) {
+                  float3 f = pbr_eval(m, nrm, view, ldir);
+                  float G = lc / fmaxf(dist2, 1e-12f);
+                  float3 c = tp * f * f3(e.emission) * (scos * G * Wr);
+                  if (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f) {
+                    sh_o = p + nrm * 0.002f;
+                    sh_d = ldir;
+                    sh_tmax = fmaxf(dist - 0.004f, 0.001f);
+                    sh_c = c;
+                    want_shadow = true;
+                  }
+                }
               }
             } else if (job.nee && (sc.num_emitters > 0u || sc.num_lights > 0u)) {
               want_shadow = next_event(s, sc, m, p, nrm, view, tp, false, rng, sh_o, sh_d, sh_tmax, sh_c);
@@ -994,7 +1016,7 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
 
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
-                  Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, bool restir,
+                  Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
                   bool textures, cudaStream_t stream) {
   ShadeArgs a;
   a.jobs = jobs;
@@ -1008,7 +1030,7 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   a.bounce = bounce;
   a.capacity = capacity;
   a.prod = prod;
-  a.restir = restir ? 1u : 0u;
+  a.restir = restir;
   if (textures) k_shade<true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   else k_shade<false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_shade");

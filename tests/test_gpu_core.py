@@ -215,3 +215,32 @@ def test_flattened_small_instances_hit_the_same_primitives(native_library, cuda_
         ids = scene.triangle_instance_ids()
         ok = prim >= 0
         np.testing.assert_array_equal(inst[ok], ids[prim[ok]])
+
+
+@pytest.mark.parametrize("grid", [256, 300])
+def test_both_hierarchy_builders_give_valid_trees_and_the_oracles_hits(renderer, grid):
+    """A heightfield of 2 (grid - 1)^2 triangles: 130,050 (binned SAH on the
+    host, up to 131,072 primitives) and 178,802 (the device's Morton-order
+    build).  Either tree validates and gives the closest hits of the
+    oracle's own hierarchy (oracle/transport.c), up to exact ties."""
+    import ordinarylight_b200 as ol
+    from oracle import production
+
+    heights = scenes.fbm_heightfield(grid, seed=9, octaves=4, amplitude=6.0)
+    v, i = scenes.grid_mesh(heights, 0.25)
+    scene = ol.Scene()
+    scene.add_mesh(v, i, ol.Material(base_color=(0.5, 0.5, 0.5)))
+    assert renderer.validate_bvh(scene) == 0
+    rng = np.random.default_rng(grid)
+    n = 20000
+    o = np.column_stack([rng.uniform(-30, 30, n), np.full(n, 20.0), rng.uniform(-30, 30, n)]).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d[:, 1] = -np.abs(d[:, 1]) - 0.2
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    _inst, prim, t, _ = renderer.trace_closest(scene, o, d, t_min=1e-4)
+    cpu_prim, cpu_t = production.trace(scene, o, d, t_min=1e-4)
+    assert int((cpu_prim >= 0).sum()) > n // 2
+    mismatches, _ties, tie_ok = _classify(prim, t, cpu_prim, cpu_t.astype(np.float32))
+    assert mismatches == tie_ok
+    hit = cpu_prim >= 0
+    np.testing.assert_allclose(t[hit], cpu_t[hit], rtol=1e-4)
