@@ -102,13 +102,13 @@ OLC_HD uint32_t olc_bounce_state(uint32_t path_seed, uint32_t bounce) {
   return olc_hash(path_seed ^ olc_hash(bounce * 0x9e3779b9u + 0x632be5abu));
 }
 
-// One PCG-RXS-M-XS step; returns a float in [0, 1).
-OLC_HD float olc_rand(uint32_t& state) {
+// One PCG-RXS-M-XS step: a uniform 32-bit word, or a float in [0, 1).
+OLC_HD uint32_t olc_rand_word(uint32_t& state) {
   state = state * 747796405u + 2891336453u;
-  uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
-  word = (word >> 22u) ^ word;
-  return (float)word * (1.0f / 4294967296.0f);
+  const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+  return (word >> 22u) ^ word;
 }
+OLC_HD float olc_rand(uint32_t& state) { return (float)olc_rand_word(state) * (1.0f / 4294967296.0f); }
 
 // Camera jitter of (pixel, sample, frame): two hash steps of the path seed,
 // the reference raygen's jitter draws (wavefront_generate.comp:117-121).

@@ -88,10 +88,11 @@ OLC_D PreparedBsdf prepare_bsdf(const SurfaceMat& m, float3 n, float3 view) {
 }
 
 // The BSDF times the cosine-free factors for candidate direction l, with
-// hardware reciprocal square roots and approximate divisions: the resampling
-// target only has to be one fixed function of the sample (the estimator stays
-// unbiased for any such target), and this one costs about half of the
-// correctly rounded form per candidate.
+// hardware reciprocal square roots, approximate divisions and the GGX
+// bracket's sin^2(n, h) as 1 - (n.h)^2: the resampling target only has to be
+// one fixed function of the sample, positive where both cosines are (the
+// estimator stays unbiased for any such target), and this one costs about
+// half of the correctly rounded form per candidate.
 OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
   const float3 hv = b.view + l;
   const float3 h = hv * rsqrtf(fmaxf(dot(hv, hv), 1e-30f));
@@ -100,7 +101,7 @@ OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
   const float w = 1.0f - clampf(vh, 0.0f, 1.0f);
   const float w5 = w * w * w * w * w;
   const float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
-  const float den = sin2_between(b.n, h, nh) + nh * nh * b.a2;   // the GGX bracket of ggx_d
+  const float den = fmaf(nh * nh, b.a2, fmaxf(fmaf(-nh, nh, 1.0f), 0.0f));   // the GGX bracket of ggx_d
   const float D = __fdividef(b.a2, fmaxf(OLC_PI * den * den, 1e-30f));
   const float x = b.a2 + (1.0f - b.a2) * nl * nl;
   const float g1l = __fdividef(2.0f * nl, fmaxf(nl + x * rsqrtf(x), 1e-6f));
@@ -150,24 +151,27 @@ OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uin
   return (t == t && t < 3.0e38f) ? fmaxf(t, 0.0f) : 0.0f;
 }
 
-OLC_D void res_update(Res& r, uint32_t light, uint32_t bary, float target, float w, uint32_t m, float u) {
+// Returns whether the offered sample was selected.
+OLC_D bool res_update(Res& r, uint32_t light, uint32_t bary, float target, float w, uint32_t m, float u) {
   r.M += m;
   r.w_sum += w;
   if (w > 0.0f && (r.light == 0xffffffffu || u * r.w_sum < w)) {
     r.light = light;
     r.bary = bary;
     r.target = target;
+    return true;
   }
+  return false;
 }
 
-// Whether light sample (emitter e, barycentrics b) lies in the support of
+// Whether the light sample at point lp of emitter e lies in the support of
 // the target at a surface (position p, viewer-side shading normal n): both
 // cosines positive.  Only reservoirs with a positive target of their own
 // sample are ever reused, so their surfaces face the viewer (n.v > 0); the
 // BSDF of an opaque surface is positive wherever both cosines are, and
 // emitters have positive luminance, so this is where target_of is not zero.
-OLC_D bool in_support(const EmitterRec& e, float2 b, float3 p, float3 n) {
-  const float3 off = emitter_point(e, b.x, b.y) - p;
+OLC_D bool in_support(const EmitterRec& e, float3 lp, float3 p, float3 n) {
+  const float3 off = lp - p;
   const float d2 = dot(off, off);
   if (!(d2 > 1e-12f)) return false;
   const float3 l = off * rsqrtf(d2);
@@ -342,11 +346,14 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
     uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream);
     for (uint32_t c = 0; c < a.candidates; ++c) {
       uint32_t li = select_emitter(s, sc, olc_rand(rng));
-      // the square root's last bits do not survive the half-precision
-      // barycentrics, so the hardware reciprocal square root serves
-      const float u0 = olc_rand(rng);
-      float ru = u0 > 0.0f ? u0 * rsqrtf(u0) : 0.0f;
-      float rv = olc_rand(rng);
+      // The barycentrics are stored in half precision, so 16 bits of each of
+      // their two uniforms suffice: both come from one word (each half
+      // placed in a float's mantissa, [1, 2) minus 1), and the hardware
+      // reciprocal square root serves for the same reason.
+      const uint32_t bits = olc_rand_word(rng);
+      const float u0 = __uint_as_float(0x3f800000u | ((bits >> 16) << 7)) - 1.0f;
+      const float rv = __uint_as_float(0x3f800000u | ((bits & 0xffffu) << 7)) - 1.0f;
+      const float ru = u0 > 0.0f ? u0 * rsqrtf(u0) : 0.0f;
       uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
       float inv_src;
       float t = target_of(s, su, li, bary, &inv_src);
@@ -368,8 +375,10 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
         // the candidates always count; the history only where the selected
         // sample is in the support of the previous frame's target
         if (r.light != 0xffffffffu) {
-          const bool supported = in_support(load_emitter(s, r.light), unpack_bary(r.bary),
-                                            stored_position(a.hist2, gh), oct_decode(pn));
+          const EmitterRec e = load_emitter(s, r.light);
+          const float2 b = unpack_bary(r.bary);
+          const bool supported =
+              in_support(e, emitter_point(e, b.x, b.y), stored_position(a.hist2, gh), oct_decode(pn));
           normalise_support(r, r.M - (supported ? 0u : m));
         }
       }
@@ -415,27 +424,31 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
       uint32_t rng = rng0;
       uint32_t reused_q[kMaxNeighbours];
       uint32_t reused = 0;
+      uint32_t winner = kMaxNeighbours;   // the reused neighbour whose sample was selected last
       for (uint32_t j = 0; j < a.neighbours; ++j) {
         uint32_t q, nq;
         Res nb;
         float dq, u;
         if (!neighbour(rng, q, nb, dq, nq, u)) continue;
         float t = target_of(s, su, nb.light, nb.bary);
-        res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u);
+        if (res_update(r, nb.light, nb.bary, t, t * nb.w_sum / nb.target, nb.M, u)) winner = reused;
         reused_q[reused++] = q;
       }
       if (reused && r.light != 0xffffffffu) {
         // this pixel's reservoir always counts (the selected sample has a
-        // positive target here); each reused neighbour where the sample is
-        // in the support of its own target
+        // positive target here), and so does the neighbour whose own sample
+        // won (reused only with a positive target of it); each other reused
+        // neighbour where the sample is in the support of its own target
         const EmitterRec e = load_emitter(s, r.light);
         const float2 b = unpack_bary(r.bary);
+        const float3 lp = emitter_point(e, b.x, b.y);
         uint32_t Z = r.M;
         for (uint32_t k = 0; k < reused; ++k) {
+          if (k == winner) continue;
           const uint64_t gq = stream_base + reused_q[k];
           const uint4 w0 = a.in0[gq];
           const uint4 w1 = a.in1[gq];
-          if (!in_support(e, b, stored_position(a.in2, gq), oct_decode(w1.z))) Z -= w0.w;
+          if (!in_support(e, lp, stored_position(a.in2, gq), oct_decode(w1.z))) Z -= w0.w;
         }
         normalise_support(r, Z);
       }
