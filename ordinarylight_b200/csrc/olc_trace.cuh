@@ -10,12 +10,15 @@
 //   Entering an instance transforms the ray to object space (t is preserved
 //   because the direction is not renormalised) and pushes a marker that
 //   restores the world ray when the instance's subtree is exhausted; the
-//   world ray's derived terms are kept meanwhile in OLC_RAY_SAVE shared
+//   world ray and its derived terms are kept meanwhile in OLC_RAY_SAVE shared
 //   words per thread instead of being recomputed.
 // * The traversal stack lives in shared memory (STACK entries per thread,
 //   entry k of thread t at k * blockDim.x + t, so a warp's pushes hit 32
-//   distinct banks), followed by the saved world-ray words in the same
+//   distinct banks), followed by the per-thread shared words in the same
 //   column layout; a launch gives (STACK + OLC_RAY_SAVE) * blockDim.x words.
+//   What a ray needs only at instance transitions or at its end (the world
+//   ray, the closest hit's barycentrics) lives there rather than in
+//   registers, which keeps seven blocks of 128 threads resident per SM.
 //   Deeper entries spill to a bounded local array.  A push beyond both is
 //   counted as a traversal error instead of writing out of bounds.
 // * Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013):
@@ -31,14 +34,19 @@
 #include "olc_common.cuh"
 
 #define OLC_SPILL 96
-// Shared words per thread beyond the stack: the world ray's derived terms,
-// saved on entering an instance and restored on leaving it.
-#define OLC_RAY_SAVE 10
+// Shared words per thread beyond the stack: the world ray's derived terms
+// (0-9), restored on leaving an instance; the world ray's origin (10-12) and
+// direction (13-15); the closest hit's barycentrics (16-17).
+#define OLC_RAY_SAVE 18
+#define OLC_SAVE_ORIGIN 10
+#define OLC_SAVE_DIR 13
+#define OLC_SAVE_UV 16
+#define OLC_NO_INSTANCE 0xffffffffu
 #define OLC_MARKER 0x7fffffff
 #define OLC_TRAVERSAL_BUDGET (1u << 22)
 
 struct TraceRay {
-  float3 o, d;
+  float3 o;
   float3 inv, oinv;
   int kx, ky, kz;
   float sx, sy, sz;
@@ -46,7 +54,6 @@ struct TraceRay {
 
 OLC_D void setup_ray(TraceRay& r, float3 o, float3 d) {
   r.o = o;
-  r.d = d;
   float dx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
   float dy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
   float dz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
@@ -101,18 +108,17 @@ OLC_D bool intersect_triangle(const TraceRay& r, float3 v0, float3 v1, float3 v2
   return true;
 }
 
-// Save / restore the terms setup_ray derives from (o, d): the slab
-// reciprocals, the shear permutation and constants.  `w` is this thread's
-// column (stride threads).
+// Save / restore the terms setup_ray derives from the world ray (o, d): the
+// slab reciprocals, the shear permutation and constants; restoring also reads
+// back the world origin.  `w` is this thread's column (stride threads).
 OLC_D void save_ray(float* w, int stride, const TraceRay& r) {
   w[0 * stride] = r.inv.x; w[1 * stride] = r.inv.y; w[2 * stride] = r.inv.z;
   w[3 * stride] = r.oinv.x; w[4 * stride] = r.oinv.y; w[5 * stride] = r.oinv.z;
   w[6 * stride] = r.sx; w[7 * stride] = r.sy; w[8 * stride] = r.sz;
   w[9 * stride] = __int_as_float(r.kx | (r.ky << 2) | (r.kz << 4));
 }
-OLC_D void restore_ray(const float* w, int stride, TraceRay& r, float3 o, float3 d) {
-  r.o = o;
-  r.d = d;
+OLC_D void restore_ray(const float* w, int stride, TraceRay& r) {
+  r.o = f3(w[(OLC_SAVE_ORIGIN + 0) * stride], w[(OLC_SAVE_ORIGIN + 1) * stride], w[(OLC_SAVE_ORIGIN + 2) * stride]);
   r.inv = f3(w[0 * stride], w[1 * stride], w[2 * stride]);
   r.oinv = f3(w[3 * stride], w[4 * stride], w[5 * stride]);
   r.sx = w[6 * stride]; r.sy = w[7 * stride]; r.sz = w[8 * stride];
@@ -152,15 +158,31 @@ struct TraversalStack {
   }
 };
 
-OLC_D void load_instance_w2o(const InstanceRec* inst, uint32_t i, Affine& w2o, uint32_t& root,
-                             uint32_t& prim_offset) {
+OLC_D void load_instance_w2o(const InstanceRec* inst, uint32_t i, Affine& w2o, uint32_t& root) {
   const float4* p = reinterpret_cast<const float4*>(inst + i);
   w2o.r0 = __ldg(p + 0);
   w2o.r1 = __ldg(p + 1);
   w2o.r2 = __ldg(p + 2);
-  uint4 m = __ldg(reinterpret_cast<const uint4*>(p + 3));
-  root = m.x;
-  prim_offset = m.z;
+  root = __ldg(&inst[i].blas_root);
+}
+
+// Packed triangle index (Scene.triangles order) of triangle slot `slot` hit
+// through instance `inst`: the closest-hit tie-break key.  Record 0, the
+// identity instance of baked world-space triangles, has offset 0.
+OLC_D uint32_t packed_index(const SceneView& s, uint32_t inst, uint32_t slot) {
+  return __ldg(&s.instances[inst].prim_offset) + __ldg(s.tri_index + slot);
+}
+
+// Three-input float max / min (one instruction on sm_100).
+OLC_D float fmax3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+OLC_D float fmin3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
 }
 
 // Slab test of one child box (Kay and Kajiya) with the conservative far
@@ -171,8 +193,8 @@ OLC_D bool child_box(float lx, float hx, float ly, float hy, float lz, float hz,
   const float l_x = __fmaf_rn(lx, r.inv.x, -r.oinv.x), h_x = __fmaf_rn(hx, r.inv.x, -r.oinv.x);
   const float l_y = __fmaf_rn(ly, r.inv.y, -r.oinv.y), h_y = __fmaf_rn(hy, r.inv.y, -r.oinv.y);
   const float l_z = __fmaf_rn(lz, r.inv.z, -r.oinv.z), h_z = __fmaf_rn(hz, r.inv.z, -r.oinv.z);
-  const float n = fmaxf(fmaxf(fminf(l_x, h_x), fminf(l_y, h_y)), fmaxf(fminf(l_z, h_z), t_min));
-  const float f = fminf(fminf(fmaxf(l_x, h_x), fmaxf(l_y, h_y)), fminf(fmaxf(l_z, h_z), t_max));
+  const float n = fmax3(fminf(l_x, h_x), fminf(l_y, h_y), fmaxf(fminf(l_z, h_z), t_min));
+  const float f = fmin3(fmaxf(l_x, h_x), fmaxf(l_y, h_y), fminf(fmaxf(l_z, h_z), t_max));
   near_t = n;
   return (n <= f * 1.0000004f) && (child != OLC_EMPTY_CHILD);
 }
@@ -193,41 +215,82 @@ OLC_D void order_pair(float& ka, int& ca, float& kb, int& cb) {
 // iterations (node visits, leaf tests, instance transitions) and returns true
 // once the ray is finished, so a persistent kernel can refill lanes whose rays
 // finished while the other lanes of the warp are still traversing.
+//
+// Register state is kept to what every iteration reads: the current ray, the
+// closest t with its slot and instance, the node, the instance being walked
+// (OLC_NO_INSTANCE in the TLAS) and the stack pointer.  The world ray and the
+// closest hit's barycentrics live in the thread's shared words, and the
+// packed tie-break index is looked up only when two hits have equal t.
 template <int STACK, bool ANY_HIT>
 struct Traversal {
   TraceRay ray;
-  float3 wo, wd;
   float t_min;
-  HitResult hit;
+  float hit_t;
+  uint32_t hit_slot;   // triangle slot (BVH order) of the closest hit so far
+  uint32_t hit_inst;   // its instance; OLC_NO_INSTANCE while nothing was hit
   int node;
-  int level;
-  uint32_t cur_inst, cur_prim_offset;
+  uint32_t cur_inst;   // instance whose BLAS is being walked, or OLC_NO_INSTANCE
   uint32_t budget;
-  bool found;
   float* save;         // this thread's column of OLC_RAY_SAVE shared words
   TraversalStack<STACK> st;
+
+  OLC_D bool found() const { return hit_inst != OLC_NO_INSTANCE; }
+  OLC_D float hit_u() const { return save[OLC_SAVE_UV * st.stride]; }
+  OLC_D float hit_v() const { return save[(OLC_SAVE_UV + 1) * st.stride]; }
+  OLC_D HitResult result(const SceneView& s) const {
+    HitResult h;
+    h.t = hit_t;
+    h.slot = hit_slot;
+    h.instance = hit_inst;
+    h.u = found() ? hit_u() : 0.0f;
+    h.v = found() ? hit_v() : 0.0f;
+    h.packed = found() ? packed_index(s, hit_inst, hit_slot) : 0xffffffffu;
+    return h;
+  }
 
   OLC_D void begin(const SceneView& s, float3 o, float3 d, float tmin, float tmax, uint32_t tlas_root,
                    int* smem_base, int* spill_area) {
     st.init(smem_base, threadIdx.x, blockDim.x, spill_area);
     save = reinterpret_cast<float*>(smem_base + STACK * blockDim.x) + threadIdx.x;
-    wo = o;
-    wd = d;
+    const int w = st.stride;
+    save[(OLC_SAVE_ORIGIN + 0) * w] = o.x;
+    save[(OLC_SAVE_ORIGIN + 1) * w] = o.y;
+    save[(OLC_SAVE_ORIGIN + 2) * w] = o.z;
+    save[(OLC_SAVE_DIR + 0) * w] = d.x;
+    save[(OLC_SAVE_DIR + 1) * w] = d.y;
+    save[(OLC_SAVE_DIR + 2) * w] = d.z;
     t_min = tmin;
     setup_ray(ray, o, d);
-    hit.t = tmax;
-    hit.instance = 0xffffffffu;
-    hit.slot = 0;
-    hit.u = hit.v = 0.0f;
-    hit.packed = 0xffffffffu;
-    found = false;
-    level = 0;
-    cur_inst = 0;
-    cur_prim_offset = 0;
+    save_ray(save, w, ray);   // the world ray's terms, restored on leaving an instance
+    hit_t = tmax;
+    hit_inst = OLC_NO_INSTANCE;
+    hit_slot = 0;
+    cur_inst = OLC_NO_INSTANCE;
     node = (int)tlas_root;
     // A well-formed tree is acyclic and finite; the budget only guarantees
     // the loop ends (and reports an error) should the structure be corrupt.
     budget = OLC_TRAVERSAL_BUDGET;
+  }
+
+  // A triangle hit at t (<= hit_t) through instance `inst`: keep it if it is
+  // nearer, or equally near with a lower packed index.  Returns true when the
+  // ray is finished (any hit).
+  OLC_D bool offer(const SceneView& s, uint32_t inst, uint32_t slot, float t, float b1, float b2) {
+    if (ANY_HIT) {
+      hit_t = t;
+      hit_inst = inst;
+      hit_slot = slot;
+      return true;
+    }
+    if (hit_inst == OLC_NO_INSTANCE || t < hit_t ||
+        packed_index(s, inst, slot) < packed_index(s, hit_inst, hit_slot)) {
+      hit_t = t;
+      hit_inst = inst;
+      hit_slot = slot;
+      save[OLC_SAVE_UV * st.stride] = b1;
+      save[(OLC_SAVE_UV + 1) * st.stride] = b2;
+    }
+    return false;
   }
 
   OLC_D bool advance(const SceneView& s, int iterations, uint32_t& err) {
@@ -245,10 +308,10 @@ struct Traversal {
         const float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
         const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
         float n0, n1, n2, n3;
-        const bool h0 = child_box(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, ch.x, ray, t_min, hit.t, n0);
-        const bool h1 = child_box(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, ch.y, ray, t_min, hit.t, n1);
-        const bool h2 = child_box(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, ch.z, ray, t_min, hit.t, n2);
-        const bool h3 = child_box(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, ch.w, ray, t_min, hit.t, n3);
+        const bool h0 = child_box(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, ch.x, ray, t_min, hit_t, n0);
+        const bool h1 = child_box(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, ch.y, ray, t_min, hit_t, n1);
+        const bool h2 = child_box(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, ch.z, ray, t_min, hit_t, n2);
+        const bool h3 = child_box(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, ch.w, ray, t_min, hit_t, n3);
         const int hits = (int)h0 + (int)h1 + (int)h2 + (int)h3;
         if (hits == 0) {
           // nothing to enter: fall through to the pop
@@ -277,71 +340,40 @@ struct Traversal {
           continue;
         }
       } else if (node != OLC_MARKER) {
-        uint32_t first = olc_leaf_first(node);
-        uint32_t count = olc_leaf_count(node);
-        if (level == 0 && count == OLC_TLAS_LEAF_TRIANGLE) {
+        const uint32_t first = olc_leaf_first(node);
+        const uint32_t count = olc_leaf_count(node);
+        if (cur_inst == OLC_NO_INSTANCE && count == OLC_TLAS_LEAF_TRIANGLE) {
           // baked world-space triangle referenced directly by the TLAS
           const uint32_t slot = first;
           const float4* tv = s.tri_verts + 3u * slot;
           float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
           float t, b1, b2;
-          if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
-            if (ANY_HIT) {
-              hit.t = t;
-              hit.instance = OLC_IDENTITY_INSTANCE;
-              hit.slot = slot;
-              found = true;
-              return true;
-            }
-            uint32_t packed = __ldg(s.tri_index + slot);
-            if (t < hit.t || packed < hit.packed) {
-              hit.t = t;
-              hit.u = b1;
-              hit.v = b2;
-              hit.slot = slot;
-              hit.instance = OLC_IDENTITY_INSTANCE;
-              hit.packed = packed;
-              found = true;
-            }
-          }
-        } else if (level == 0) {
+          if (intersect_triangle(ray, v0, v1, v2, t_min, hit_t, t, b1, b2) &&
+              offer(s, OLC_IDENTITY_INSTANCE, slot, t, b1, b2))
+            return true;
+        } else if (cur_inst == OLC_NO_INSTANCE) {
           // instance leaf (TLAS leaves hold one instance)
           Affine w2o;
           uint32_t root;
-          load_instance_w2o(s.instances, first, w2o, root, cur_prim_offset);
-          cur_inst = first;
+          load_instance_w2o(s.instances, first, w2o, root);
           if (st.push(OLC_MARKER, err)) {
-            save_ray(save, st.stride, ray);
-            setup_ray(ray, xform_point(w2o, wo), xform_vector(w2o, wd));
-            level = 1;
+            const int w = st.stride;
+            const float3 wd = f3(save[(OLC_SAVE_DIR + 0) * w], save[(OLC_SAVE_DIR + 1) * w],
+                                 save[(OLC_SAVE_DIR + 2) * w]);
+            setup_ray(ray, xform_point(w2o, ray.o), xform_vector(w2o, wd));
+            cur_inst = first;
             node = (int)root;
             continue;
           }
         } else {
           for (uint32_t k = 0; k < count; ++k) {
-            uint32_t slot = first + k;
+            const uint32_t slot = first + k;
             const float4* tv = s.tri_verts + 3u * slot;
             float3 v0 = f3(__ldg(tv + 0)), v1 = f3(__ldg(tv + 1)), v2 = f3(__ldg(tv + 2));
             float t, b1, b2;
-            if (intersect_triangle(ray, v0, v1, v2, t_min, hit.t, t, b1, b2)) {
-              if (ANY_HIT) {
-                hit.t = t;
-                hit.instance = cur_inst;
-                hit.slot = slot;
-                found = true;
-                return true;
-              }
-              uint32_t packed = cur_prim_offset + __ldg(s.tri_index + slot);
-              if (t < hit.t || packed < hit.packed) {
-                hit.t = t;
-                hit.u = b1;
-                hit.v = b2;
-                hit.slot = slot;
-                hit.instance = cur_inst;
-                hit.packed = packed;
-                found = true;
-              }
-            }
+            if (intersect_triangle(ray, v0, v1, v2, t_min, hit_t, t, b1, b2) &&
+                offer(s, cur_inst, slot, t, b1, b2))
+              return true;
           }
         }
       }
@@ -349,8 +381,8 @@ struct Traversal {
       if (st.sp == 0) return true;
       node = st.pop();
       if (node == OLC_MARKER) {
-        level = 0;
-        restore_ray(save, st.stride, ray, wo, wd);
+        cur_inst = OLC_NO_INSTANCE;
+        restore_ray(save, st.stride, ray);
         if (st.sp == 0) return true;
         node = st.pop();
       }
@@ -368,6 +400,6 @@ OLC_D bool olc_traverse(const SceneView& s, uint32_t tlas_root, float3 wo, float
   tr.begin(s, wo, wd, t_min, t_max, tlas_root, smem_base, spill);
   while (!tr.advance(s, 1 << 30, err)) {
   }
-  hit = tr.hit;
-  return tr.found;
+  hit = tr.result(s);
+  return tr.found();
 }

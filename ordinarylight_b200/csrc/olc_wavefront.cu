@@ -180,9 +180,20 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
   }
 }
 
+// Register caps of the traversal kernels: 64 registers hold the traversal
+// state without spilling (the world ray and the hit's barycentrics live in
+// shared memory), so eight blocks of 128 threads stay resident per SM.
+// The camera-ray form keeps its 32 rays to the end and spills a few words
+// at 64, so it gets 72 (seven blocks).
+template <int SCHED>
+struct TraceRegisters {
+  static constexpr int kClosest = SCHED == 1 ? 72 : 64;
+  static constexpr int kShadow = 64;
+};
+
 template <int STACK, int SCHED>
-__global__ void __launch_bounds__(256) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
-                                                       uint32_t bounce) {
+__global__ void __maxnreg__(TraceRegisters<SCHED>::kClosest) k_trace_closest(SceneView s, RayQueue q, HitBuf h,
+                                                                             Counters* cnt, uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->queue_count[bounce];
   uint32_t err = 0;
@@ -198,20 +209,17 @@ __global__ void __launch_bounds__(256) k_trace_closest(SceneView s, RayQueue q, 
         root = __float_as_uint(dr.w);
       },
       [&](uint32_t i, const Traversal<STACK, false>& tr) {
-        h.tuv_slot[i] = tr.found ? make_float4(tr.hit.t, tr.hit.u, tr.hit.v, __uint_as_float(tr.hit.slot))
-                                 : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
-        h.instance[i] = tr.found ? tr.hit.instance : 0xffffffffu;
+        h.tuv_slot[i] = tr.found() ? make_float4(tr.hit_t, tr.hit_u(), tr.hit_v(), __uint_as_float(tr.hit_slot))
+                                   : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+        h.instance[i] = tr.found() ? tr.hit_inst : 0xffffffffu;
       },
       err);
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
 }
 
-// 72 registers: any-hit traversal fits them without spilling (79 uncapped),
-// which gives 7 instead of 6 blocks of 128 threads per SM (measured 2 %
-// faster shadow rays; the closest-hit kernel spills under the same cap).
 template <int STACK, int SCHED>
-__global__ void __maxnreg__(72) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps, Counters* cnt,
-                                               uint32_t bounce) {
+__global__ void __maxnreg__(TraceRegisters<SCHED>::kShadow) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps,
+                                                                           Counters* cnt, uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->shadow_count[bounce];
   uint32_t err = 0;
@@ -227,7 +235,7 @@ __global__ void __maxnreg__(72) k_trace_shadow(SceneView s, ShadowQueue sq, Path
         root = __float_as_uint(sq.contrib_root[i].w);
       },
       [&](uint32_t i, const Traversal<STACK, true>& tr) {
-        if (!tr.found) {
+        if (!tr.found()) {
           uint32_t path = __float_as_uint(sq.dir_path[i].w);
           float4 c = sq.contrib_root[i];
           float4 r = ps.radiance[path];
@@ -1135,8 +1143,14 @@ void launch_occluded_rays(const LaunchShape& ls, const SceneView& s, uint32_t ro
 
 void configure_trace_kernels() {
   // Prefer the largest shared-memory carve-out for the traversal kernels so
-  // more blocks (each holding its short stacks) share one SM.
-  auto prefer = [](const void* fn) { cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100); };
+  // more blocks (each holding its short stacks) share one SM, and allow the
+  // largest launch's stacks (32 entries, 256 threads: above the 48 KB that
+  // needs no opt-in).
+  const int most = (int)stack_bytes(32, 256);
+  auto prefer = [most](const void* fn) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+  };
   prefer((const void*)k_trace_closest<16, 0>);
   prefer((const void*)k_trace_closest<24, 0>);
   prefer((const void*)k_trace_closest<32, 0>);
@@ -1149,6 +1163,12 @@ void configure_trace_kernels() {
   prefer((const void*)k_trace_shadow<16, 1>);
   prefer((const void*)k_trace_shadow<24, 1>);
   prefer((const void*)k_trace_shadow<32, 1>);
+  prefer((const void*)k_trace_rays<16>);
+  prefer((const void*)k_trace_rays<24>);
+  prefer((const void*)k_trace_rays<32>);
+  prefer((const void*)k_occluded_rays<16>);
+  prefer((const void*)k_occluded_rays<24>);
+  prefer((const void*)k_occluded_rays<32>);
 }
 
 }  // namespace olc
