@@ -949,30 +949,75 @@ OLC_D void put_child(BvhNode4& w, int& k, const BvhNode& parent, int which, int 
   ++k;
 }
 
-// BVH4 node of BVH2 node i: its children in order, each internal child
-// replaced by that child's own two children.  Internal children outside
-// [begin, end) (the nodes of an unbuilt mesh in a scene's node range) are
-// left out, so no fetch leaves the range.
+// Half surface area of child `which` of BVH2 node `nd`.
+OLC_D float child_half_area(const BvhNode& nd, int which) {
+  const float dx = which ? nd.b.y - nd.b.x : nd.a.y - nd.a.x;
+  const float dy = which ? nd.b.w - nd.b.z : nd.a.w - nd.a.z;
+  const float dz = which ? nd.c.w - nd.c.z : nd.c.y - nd.c.x;
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// One slot candidate of a BVH4 node: child `which` of BVH2 node `parent`.
+struct WideEntry {
+  uint32_t parent;
+  int which;
+  int ref;
+  float area;
+};
+
+// BVH4 node of BVH2 node i, collapsed greedily by surface area: start from
+// i's two children and repeatedly open the internal entry with the largest
+// box (replacing it, in place, by its own children) while the result still
+// fits four slots.  Where one child is a leaf this fills the slots the
+// fixed two-level collapse would leave empty, so fewer nodes are fetched
+// per ray.  Internal nodes outside [begin, end) (the nodes of an unbuilt
+// mesh in a scene's node range) are left out, so no fetch leaves the range;
+// the number of openings is bounded, so a corrupt structure cannot keep the
+// loop running.
 OLC_D BvhNode4 bvh4_of(const BvhNode* __restrict__ nodes, uint32_t i, uint32_t begin, uint32_t end) {
   BvhNode4 w;
   w.lox = w.hix = w.loy = w.hiy = w.loz = w.hiz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   w.child = make_int4(OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD);
   w.reserved = make_int4(0, 0, 0, 0);
-  const BvhNode nd = nodes[i];
-  int k = 0;
-  for (int c = 0; c < 2; ++c) {
-    const int ref = c ? nd.d.y : nd.d.x;
-    if (ref == OLC_EMPTY_CHILD) continue;
-    if (ref < 0) {
-      put_child(w, k, nd, c, ref);
-    } else if ((uint32_t)ref >= begin && (uint32_t)ref < end) {
-      const BvhNode cn = nodes[ref];
-      for (int g = 0; g < 2; ++g) {
-        const int gref = g ? cn.d.y : cn.d.x;
-        if (gref != OLC_EMPTY_CHILD) put_child(w, k, cn, g, gref);
-      }
-    }
+  auto admit = [&](const BvhNode& nd, int which) {
+    const int ref = which ? nd.d.y : nd.d.x;
+    return ref != OLC_EMPTY_CHILD && (ref < 0 || ((uint32_t)ref >= begin && (uint32_t)ref < end));
+  };
+  WideEntry e[4];
+  int n = 0;
+  {
+    const BvhNode nd = nodes[i];
+    for (int c = 0; c < 2; ++c)
+      if (admit(nd, c)) e[n++] = WideEntry{i, c, c ? nd.d.y : nd.d.x, child_half_area(nd, c)};
   }
+  for (int opening = 0; opening < 16; ++opening) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (int k = 0; k < n; ++k)
+      if (e[k].ref >= 0 && e[k].area > best_area) {
+        best = k;
+        best_area = e[k].area;
+      }
+    if (best < 0) break;
+    const uint32_t at = (uint32_t)e[best].ref;
+    const BvhNode cn = nodes[at];
+    WideEntry kids[2];
+    int m = 0;
+    for (int g = 0; g < 2; ++g)
+      if (admit(cn, g)) kids[m++] = WideEntry{at, g, g ? cn.d.y : cn.d.x, child_half_area(cn, g)};
+    if (n - 1 + m > 4) break;
+    // replace entry `best` by its m children, keeping the slot order
+    if (m == 0) {
+      for (int k = best; k + 1 < n; ++k) e[k] = e[k + 1];
+    } else if (m == 2) {
+      for (int k = n - 1; k > best; --k) e[k + 1] = e[k];
+      e[best + 1] = kids[1];
+    }
+    if (m > 0) e[best] = kids[0];
+    n += m - 1;
+  }
+  int k = 0;
+  for (int j = 0; j < n; ++j) put_child(w, k, nodes[e[j].parent], e[j].which, e[j].ref);
   return w;
 }
 
