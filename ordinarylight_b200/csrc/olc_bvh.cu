@@ -976,7 +976,9 @@ struct WideEntry {
 // loop running.
 OLC_D BvhNode4 bvh4_of(const BvhNode* __restrict__ nodes, uint32_t i, uint32_t begin, uint32_t end) {
   BvhNode4 w;
-  w.lox = w.hix = w.loy = w.hiy = w.loz = w.hiz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float inf = __int_as_float(0x7f800000);
+  w.lox = w.loy = w.loz = make_float4(inf, inf, inf, inf);
+  w.hix = w.hiy = w.hiz = make_float4(-inf, -inf, -inf, -inf);
   w.child = make_int4(OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD, OLC_EMPTY_CHILD);
   w.reserved = make_int4(0, 0, 0, 0);
   auto admit = [&](const BvhNode& nd, int which) {

@@ -48,8 +48,9 @@
 struct TraceRay {
   float3 o;
   float3 inv, oinv;
-  int kx, ky, kz;
+  int kp;              // shear permutation kx | ky << 2 | kz << 4
   float sx, sy, sz;
+  int nx, ny, nz;      // float4 index of each axis's near plane in a BvhNode4 (its far plane is index ^ 1)
 };
 
 OLC_D void setup_ray(TraceRay& r, float3 o, float3 d) {
@@ -59,13 +60,16 @@ OLC_D void setup_ray(TraceRay& r, float3 o, float3 d) {
   float dz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
   r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dz);
   r.oinv = f3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+  r.nx = r.inv.x < 0.0f ? 1 : 0;
+  r.ny = r.inv.y < 0.0f ? 3 : 2;
+  r.nz = r.inv.z < 0.0f ? 5 : 4;
   float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
   int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
   int kx = kz + 1 == 3 ? 0 : kz + 1;
   int ky = kx + 1 == 3 ? 0 : kx + 1;
   float dkz = get(d, kz);
   if (dkz < 0.0f) { int t = kx; kx = ky; ky = t; }
-  r.kx = kx; r.ky = ky; r.kz = kz;
+  r.kp = kx | (ky << 2) | (kz << 4);
   r.sx = get(d, kx) / dkz;
   r.sy = get(d, ky) / dkz;
   r.sz = 1.0f / dkz;
@@ -75,14 +79,15 @@ OLC_D void setup_ray(TraceRay& r, float3 o, float3 d) {
 // b2 (weight of v2) when the ray hits with t_min < t <= t_max.
 OLC_D bool intersect_triangle(const TraceRay& r, float3 v0, float3 v1, float3 v2,
                               float t_min, float t_max, float& t_out, float& b1, float& b2) {
+  const int kx = r.kp & 3, ky = (r.kp >> 2) & 3, kz = r.kp >> 4;
   float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
-  float Akz = get(A, r.kz), Bkz = get(B, r.kz), Ckz = get(C, r.kz);
-  float Ax = __fmaf_rn(-r.sx, Akz, get(A, r.kx));
-  float Ay = __fmaf_rn(-r.sy, Akz, get(A, r.ky));
-  float Bx = __fmaf_rn(-r.sx, Bkz, get(B, r.kx));
-  float By = __fmaf_rn(-r.sy, Bkz, get(B, r.ky));
-  float Cx = __fmaf_rn(-r.sx, Ckz, get(C, r.kx));
-  float Cy = __fmaf_rn(-r.sy, Ckz, get(C, r.ky));
+  float Akz = get(A, kz), Bkz = get(B, kz), Ckz = get(C, kz);
+  float Ax = __fmaf_rn(-r.sx, Akz, get(A, kx));
+  float Ay = __fmaf_rn(-r.sy, Akz, get(A, ky));
+  float Bx = __fmaf_rn(-r.sx, Bkz, get(B, kx));
+  float By = __fmaf_rn(-r.sy, Bkz, get(B, ky));
+  float Cx = __fmaf_rn(-r.sx, Ckz, get(C, kx));
+  float Cy = __fmaf_rn(-r.sy, Ckz, get(C, ky));
   float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
   float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
   float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
@@ -115,7 +120,7 @@ OLC_D void save_ray(float* w, int stride, const TraceRay& r) {
   w[0 * stride] = r.inv.x; w[1 * stride] = r.inv.y; w[2 * stride] = r.inv.z;
   w[3 * stride] = r.oinv.x; w[4 * stride] = r.oinv.y; w[5 * stride] = r.oinv.z;
   w[6 * stride] = r.sx; w[7 * stride] = r.sy; w[8 * stride] = r.sz;
-  w[9 * stride] = __int_as_float(r.kx | (r.ky << 2) | (r.kz << 4));
+  w[9 * stride] = __int_as_float(r.kp | (r.nx << 6) | (r.ny << 9) | (r.nz << 12));
 }
 OLC_D void restore_ray(const float* w, int stride, TraceRay& r) {
   r.o = f3(w[(OLC_SAVE_ORIGIN + 0) * stride], w[(OLC_SAVE_ORIGIN + 1) * stride], w[(OLC_SAVE_ORIGIN + 2) * stride]);
@@ -123,7 +128,8 @@ OLC_D void restore_ray(const float* w, int stride, TraceRay& r) {
   r.oinv = f3(w[3 * stride], w[4 * stride], w[5 * stride]);
   r.sx = w[6 * stride]; r.sy = w[7 * stride]; r.sz = w[8 * stride];
   const int k = __float_as_int(w[9 * stride]);
-  r.kx = k & 3; r.ky = (k >> 2) & 3; r.kz = (k >> 4) & 3;
+  r.kp = k & 63;
+  r.nx = (k >> 6) & 7; r.ny = (k >> 9) & 7; r.nz = (k >> 12) & 7;
 }
 
 struct HitResult {
@@ -185,18 +191,20 @@ OLC_D float fmin3(float a, float b, float c) {
   return r;
 }
 
-// Slab test of one child box (Kay and Kajiya) with the conservative far
-// bound of robust traversal (Ize 2013): a few ulps of slack so rounding in
-// the slab test never culls a box the ray touches.
-OLC_D bool child_box(float lx, float hx, float ly, float hy, float lz, float hz, int child, const TraceRay& r,
+// Slab test of one child box (Kay and Kajiya) on its near and far planes
+// (chosen per ray by the direction's signs, so no min/max per axis), with the
+// conservative far bound of robust traversal (Ize 2013): a few ulps of slack
+// so rounding in the slab test never culls a box the ray touches.  Unused
+// slots hold an inverted box (lo +inf, hi -inf), whose near distance is +inf
+// and far distance -inf for every ray.
+OLC_D bool child_box(float nxp, float fxp, float nyp, float fyp, float nzp, float fzp, const TraceRay& r,
                      float t_min, float t_max, float& near_t) {
-  const float l_x = __fmaf_rn(lx, r.inv.x, -r.oinv.x), h_x = __fmaf_rn(hx, r.inv.x, -r.oinv.x);
-  const float l_y = __fmaf_rn(ly, r.inv.y, -r.oinv.y), h_y = __fmaf_rn(hy, r.inv.y, -r.oinv.y);
-  const float l_z = __fmaf_rn(lz, r.inv.z, -r.oinv.z), h_z = __fmaf_rn(hz, r.inv.z, -r.oinv.z);
-  const float n = fmax3(fminf(l_x, h_x), fminf(l_y, h_y), fmaxf(fminf(l_z, h_z), t_min));
-  const float f = fmin3(fmaxf(l_x, h_x), fmaxf(l_y, h_y), fminf(fmaxf(l_z, h_z), t_max));
+  const float n = fmax3(__fmaf_rn(nxp, r.inv.x, -r.oinv.x), __fmaf_rn(nyp, r.inv.y, -r.oinv.y),
+                        fmaxf(__fmaf_rn(nzp, r.inv.z, -r.oinv.z), t_min));
+  const float f = fmin3(__fmaf_rn(fxp, r.inv.x, -r.oinv.x), __fmaf_rn(fyp, r.inv.y, -r.oinv.y),
+                        fminf(__fmaf_rn(fzp, r.inv.z, -r.oinv.z), t_max));
   near_t = n;
-  return (n <= f * 1.0000004f) && (child != OLC_EMPTY_CHILD);
+  return n <= f * 1.0000004f;
 }
 
 // One compare-exchange of a sorting network over (key, child) pairs.
@@ -304,14 +312,15 @@ struct Traversal {
         // hit child and push the others, farthest first (closest hit) or in
         // slot order (any hit, where the order changes nothing but time).
         const float4* p = reinterpret_cast<const float4*>(s.wide + node);
-        const float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3);
-        const float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
+        const float4 nx = __ldg(p + ray.nx), fx = __ldg(p + (ray.nx ^ 1));
+        const float4 ny = __ldg(p + ray.ny), fy = __ldg(p + (ray.ny ^ 1));
+        const float4 nz = __ldg(p + ray.nz), fz = __ldg(p + (ray.nz ^ 1));
         const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
         float n0, n1, n2, n3;
-        const bool h0 = child_box(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, ch.x, ray, t_min, hit_t, n0);
-        const bool h1 = child_box(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, ch.y, ray, t_min, hit_t, n1);
-        const bool h2 = child_box(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, ch.z, ray, t_min, hit_t, n2);
-        const bool h3 = child_box(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, ch.w, ray, t_min, hit_t, n3);
+        const bool h0 = child_box(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, ray, t_min, hit_t, n0);
+        const bool h1 = child_box(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, ray, t_min, hit_t, n1);
+        const bool h2 = child_box(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, ray, t_min, hit_t, n2);
+        const bool h3 = child_box(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, ray, t_min, hit_t, n3);
         const int hits = (int)h0 + (int)h1 + (int)h2 + (int)h3;
         if (hits == 0) {
           // nothing to enter: fall through to the pop

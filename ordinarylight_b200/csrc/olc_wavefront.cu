@@ -183,11 +183,9 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
 // Register caps of the traversal kernels: 64 registers hold the traversal
 // state without spilling (the world ray and the hit's barycentrics live in
 // shared memory), so eight blocks of 128 threads stay resident per SM.
-// The camera-ray form keeps its 32 rays to the end and spills a few words
-// at 64, so it gets 72 (seven blocks).
 template <int SCHED>
 struct TraceRegisters {
-  static constexpr int kClosest = SCHED == 1 ? 72 : 64;
+  static constexpr int kClosest = 64;
   static constexpr int kShadow = 64;
 };
 
