@@ -1518,7 +1518,8 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         ctx->restir.res_a0.get(), ctx->restir.res_a1.get(), ctx->restir.res_a2.get(),
                         ctx->restir.res_b0.get(), ctx->restir.res_b1.get(), ctx->restir.res_b2.get(),
                         ctx->restir.hist0.get(), ctx->restir.hist1.get(), ctx->restir.hist2.get(),
-                        ctx->restir.selected.get(), ctx->restir.hit_list.get(), ctx->restir.hit_count.get()})
+                        ctx->restir.selected.get(), ctx->restir.hit_list.get(), ctx->restir.hit_count.get(),
+                        ctx->restir.pool0.get(), ctx->restir.pool1.get(), ctx->restir.pool2.get()})
     ptr(p);
   k.push_back(rb.stride);
   k.push_back(rb.resolve_offset);
@@ -1750,7 +1751,7 @@ void run_to_completion(olc_context* ctx, std::vector<QueuedJob*>& jobs, olc_rend
   plan_run(jobs, plan_capacity(ctx, jobs), 0xffffffffu, job_local, plan);
   if (plan.restir)
     restir_prepare(ctx->restir, job_local + (plan.chunk_reservoirs ? plan.max_count : 0),
-                   std::max<uint32_t>(plan.max_count, 1), (uint32_t)plan.chunks.size());
+                   std::max<uint32_t>(plan.max_count, 1), (uint32_t)plan.chunks.size(), plan.max_segments);
   execute_run(ctx, plan, stats);
 }
 
@@ -2159,7 +2160,7 @@ int olc_serve_step(olc_context* ctx, uint64_t* done, uint32_t done_capacity, uin
       try {
         if (plan.restir)
           restir_prepare(ctx->restir, plan.max_count, std::max<uint32_t>(plan.max_count, 1),
-                         (uint32_t)plan.chunks.size());
+                         (uint32_t)plan.chunks.size(), plan.max_segments);
         launch_planned(ctx, sl, std::move(plan));
       } catch (...) {
         // the chunk's jobs hold partial samples of a failed chunk: drop them

@@ -38,6 +38,8 @@ namespace {
 
 constexpr uint32_t kRestirStream = 0x52455354u;  // stream key offset of the reuse passes
 constexpr uint32_t kMaxNeighbours = 16;          // restir_neighbours' upper bound
+constexpr uint32_t kPoolStream = 0x504f4f4cu;    // stream key of the light pool and its block starts
+constexpr uint32_t kPoolSize = 1u << 15;         // light-pool entries per ReSTIR job and frame
 
 OLC_D uint32_t lane() { return threadIdx.x & 31u; }
 
@@ -129,26 +131,30 @@ OLC_D uint32_t pack_bary(float b1, float b2) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// Unshadowed target of light sample (light, bary) at surface s; with
-// inv_src, also the reciprocal of the sample's source pdf per unit area
-// (from the same record).
-OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary,
-                      float* inv_src = nullptr) {
-  const EmitterRec e = load_emitter(sc, light);
-  if (inv_src) *inv_src = e.emission.w;
-  float2 b = unpack_bary(bary);
-  float3 off = emitter_point(e, b.x, b.y) - s.p;
+// Unshadowed target of a light sample at surface s, given the sample's point,
+// the emitter's normal, sidedness and radiance: luminance(f Le) cos_s cos_l / d^2.
+OLC_D float target_at(const Surface& s, float3 lp, float3 lnormal, bool two_sided, float3 Le) {
+  float3 off = lp - s.p;
   float d2 = dot(off, off);
   if (!(d2 > 1e-12f)) return 0.0f;
   float inv = rsqrtf(d2);
   float3 l = off * inv;
   float cs = dot(s.bsdf.n, l);
   if (cs <= 0.0f || s.bsdf.nv <= 0.0f) return 0.0f;
-  float cl = emitter_cosine(e, l);
+  const float c = -dot(lnormal, l);
+  float cl = two_sided ? fabsf(c) : fmaxf(c, 0.0f);   // emitter_cosine
   if (cl <= 1e-6f) return 0.0f;
   float3 f = prepared_eval(s.bsdf, l, cs);
-  float t = luminance(f * f3(e.emission)) * cs * cl * (inv * inv);
+  float t = luminance(f * Le) * cs * cl * (inv * inv);
   return (t == t && t < 3.0e38f) ? fmaxf(t, 0.0f) : 0.0f;
+}
+
+// Unshadowed target of light sample (light, bary) at surface s, from the
+// emitter record (the reuse passes; the light pool stores the same terms).
+OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary) {
+  const EmitterRec e = load_emitter(sc, light);
+  const float2 b = unpack_bary(bary);
+  return target_at(s, emitter_point(e, b.x, b.y), f3(e.normal), e.e2_sided.w > 0.5f, f3(e.emission));
 }
 
 // Returns whether the offered sample was selected.
@@ -309,6 +315,9 @@ struct RestirArgs {
   uint32_t pass;
   uint4* selected;
   uint32_t finalize;
+  const float4* pool0;      // light pool: kPoolSize entries per chunk segment
+  const float4* pool1;
+  const float4* pool2;
 };
 
 // List the chunk's primary rays that hit something and belong to ReSTIR
@@ -330,6 +339,43 @@ __global__ void k_restir_compact(const ChunkHeader* __restrict__ hdr, const JobR
   }
 }
 
+// Light pool of every ReSTIR job of the chunk (after the presampled light
+// tiles of Wyman and Panteleev, HPG 2021): kPoolSize emitter samples drawn
+// from the scene's source distribution (alias-table emitter, uniform point
+// with the reference's square-root mapping, ordinaryshade_primary.glsl:668-671),
+// each stored with the terms the resampling target reads: the point and the
+// reciprocal source pdf per unit area (negative for a two-sided emitter), the
+// emitter's normal and the sample's half-precision barycentrics, its radiance
+// and index.  Entries are keyed by (entry, job.frame) only, so every chunking
+// and batch mix draws the same pool.
+__global__ void k_restir_pool(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, SceneView s,
+                              float4* __restrict__ p0, float4* __restrict__ p1, float4* __restrict__ p2) {
+  const uint64_t n = (uint64_t)hdr->num_segments * kPoolSize;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+    const JobRec& job = jobs[k / kPoolSize];
+    if (!job.restir) continue;
+    const SceneRec& sc = s.scenes[job.scene];
+    if (sc.num_emitters == 0u) continue;
+    const uint32_t entry = (uint32_t)(k % kPoolSize);
+    uint32_t rng = olc_bounce_state(olc_path_seed(entry, kPoolStream, job.frame), kPoolStream);
+    const uint32_t li = select_emitter(s, sc, olc_rand(rng));
+    // The barycentrics are stored in half precision, so 16 bits of each of
+    // their two uniforms suffice: both come from one word (each half placed
+    // in a float's mantissa, [1, 2) minus 1).
+    const uint32_t bits = olc_rand_word(rng);
+    const float u0 = __uint_as_float(0x3f800000u | ((bits >> 16) << 7)) - 1.0f;
+    const float rv = __uint_as_float(0x3f800000u | ((bits & 0xffffu) << 7)) - 1.0f;
+    const float ru = u0 > 0.0f ? u0 * rsqrtf(u0) : 0.0f;
+    const uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
+    const EmitterRec e = load_emitter(s, li);
+    const float2 b = unpack_bary(bary);
+    const float3 lp = emitter_point(e, b.x, b.y);
+    p0[k] = make_float4(lp.x, lp.y, lp.z, e.e2_sided.w > 0.5f ? -e.emission.w : e.emission.w);
+    p1[k] = make_float4(e.normal.x, e.normal.y, e.normal.z, __uint_as_float(bary));
+    p2[k] = make_float4(e.emission.x, e.emission.y, e.emission.z, __uint_as_float(li));
+  }
+}
+
 template <bool kTextures>
 __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
   const SceneView& s = a.s;
@@ -344,21 +390,24 @@ __global__ void __launch_bounds__(128) k_restir_initial(RestirArgs a) {
     const uint32_t stamp = a.hdr->stamp;
     Res r{0xffffffffu, 0u, 0.0f, 0u, 0.0f};
     uint32_t rng = olc_bounce_state(olc_path_seed(meta.x, meta.y, job.frame), kRestirStream);
-    for (uint32_t c = 0; c < a.candidates; ++c) {
-      uint32_t li = select_emitter(s, sc, olc_rand(rng));
-      // The barycentrics are stored in half precision, so 16 bits of each of
-      // their two uniforms suffice: both come from one word (each half
-      // placed in a float's mantissa, [1, 2) minus 1), and the hardware
-      // reciprocal square root serves for the same reason.
-      const uint32_t bits = olc_rand_word(rng);
-      const float u0 = __uint_as_float(0x3f800000u | ((bits >> 16) << 7)) - 1.0f;
-      const float rv = __uint_as_float(0x3f800000u | ((bits & 0xffffu) << 7)) - 1.0f;
-      const float ru = u0 > 0.0f ? u0 * rsqrtf(u0) : 0.0f;
-      uint32_t bary = pack_bary(ru * (1.0f - rv), ru * rv);
-      float inv_src;
-      float t = target_of(s, su, li, bary, &inv_src);
-      float w = t * inv_src;
-      res_update(r, li, bary, t, w, 1u, olc_rand(rng));
+    if (sc.num_emitters > 0u) {
+      // Candidates come from the job's light pool: the 32 pixels of an 8x4
+      // block of one sample stream read 32 consecutive entries per candidate
+      // from a block-specific start, so each pixel's candidates are distinct
+      // pool entries, i.e. independent draws of the source distribution.
+      const uint32_t px = meta.x % job.width, py = meta.x / job.width;
+      const uint32_t block = (py >> 2) * ((job.width + 7u) >> 3) + (px >> 3);
+      uint32_t e = olc_hash(olc_path_seed(block, meta.y, job.frame) ^ kPoolStream) + ((px & 7u) | ((py & 3u) << 3));
+      const size_t base = (size_t)meta.w * kPoolSize;
+      const float4* q0 = a.pool0 + base;
+      const float4* q1 = a.pool1 + base;
+      const float4* q2 = a.pool2 + base;
+      for (uint32_t c = 0; c < a.candidates; ++c, e += 32u) {
+        const uint32_t k = e & (kPoolSize - 1u);
+        const float4 w0 = __ldg(q0 + k), w1 = __ldg(q1 + k), w2 = __ldg(q2 + k);
+        const float t = target_at(su, f3(w0), f3(w1), w0.w < 0.0f, f3(w2));
+        res_update(r, __float_as_uint(w2.w), __float_as_uint(w1.w), t, t * fabsf(w0.w), 1u, olc_rand(rng));
+      }
     }
     // temporal reuse
     if (job.history) {
@@ -464,7 +513,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(RestirArgs a) {
 
 }  // namespace
 
-void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks) {
+void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks, uint32_t segments) {
   if (reservoirs > st.reservoirs) {
     // the history survives only if its buffers are kept
     for (DeviceBuffer* b : {&st.res_a0, &st.res_a1, &st.res_a2, &st.res_b0, &st.res_b1, &st.res_b2, &st.hist0,
@@ -474,6 +523,10 @@ void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32
     for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, reservoirs * 16));
     st.reservoirs = reservoirs;
     st.history_valid = false;
+  }
+  if (segments > st.pool_segments) {
+    for (DeviceBuffer* b : {&st.pool0, &st.pool1, &st.pool2}) b->allocate((size_t)segments * kPoolSize * 16);
+    st.pool_segments = segments;
   }
   if (slots > st.slots) {
     st.selected.allocate((size_t)slots * 16);
@@ -516,6 +569,12 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.out0 = st.res_a0.as<uint4>();
   a.out1 = st.res_a1.as<uint4>();
   a.out2 = st.res_a2.as<uint4>();
+  a.pool0 = st.pool0.as<float4>();
+  a.pool1 = st.pool1.as<float4>();
+  a.pool2 = st.pool2.as<float4>();
+  k_restir_pool<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, s, st.pool0.as<float4>(), st.pool1.as<float4>(),
+                                                    st.pool2.as<float4>());
+  OLC_LAUNCH_CHECK("k_restir_pool");
   OLC_CUDA(cudaMemsetAsync(st.hit_count.get(), 0, 4, stream));
   k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, hits, ps, st.hit_list.as<uint32_t>(),
                                                         st.hit_count.as<uint32_t>());
@@ -572,6 +631,8 @@ void restir_release(RestirState& st) {
                           &st.hist1, &st.hist2})
     b->release();
   st.selected.release();
+  for (DeviceBuffer* b : {&st.pool0, &st.pool1, &st.pool2}) b->release();
+  st.pool_segments = 0;
   st.hit_list.release();
   st.hit_count.release();
   st.reservoirs = 0;

@@ -13,10 +13,12 @@ struct RestirState {
   DeviceBuffer res_b0, res_b1, res_b2;   // spatial ping-pong
   DeviceBuffer hist0, hist1, hist2;      // previous frame's final reservoirs
   DeviceBuffer selected;           // per path slot: light, bary, W
+  DeviceBuffer pool0, pool1, pool2;  // light pool of each chunk segment (k_restir_pool)
   DeviceBuffer hit_list;           // path slots whose primary ray hit (ReSTIR jobs only)
   DeviceBuffer hit_count;
   uint64_t reservoirs = 0;         // reservoir capacity (pixel-samples of ReSTIR jobs)
   uint32_t slots = 0;              // path slot capacity
+  uint32_t pool_segments = 0;      // chunk segments the light pool has room for
   uint32_t next_stamp = 1;         // stamp of the next chunk (0 never marks a valid reservoir)
   uint32_t run_first = 0, run_last = 0;    // stamps of this run's chunks
   uint32_t hist_first = 0, hist_last = 0;  // stamps of the history's chunks (set by restir_finish)
@@ -28,11 +30,11 @@ struct RestirState {
   JobRec hist_camera{};
 };
 
-// Size buffers for `reservoirs` pixel-samples and `slots` path slots, and
-// reserve one stamp per chunk of the run (chunk c of the run gets
-// st.run_first + c; the caller stores it and the history's stamp range in
-// each chunk header).
-void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks);
+// Size buffers for `reservoirs` pixel-samples, `slots` path slots and light
+// pools for `segments` chunk segments, and reserve one stamp per chunk of the
+// run (chunk c of the run gets st.run_first + c; the caller stores it and the
+// history's stamp range in each chunk header).
+void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks, uint32_t segments);
 // Run initial RIS (+ temporal for jobs with history) + spatial reuse for one
 // chunk; returns the per-path-slot selected sample buffer consumed by the
 // bounce-0 shading pass.  Every host-side input is a pointer or a configuration value,

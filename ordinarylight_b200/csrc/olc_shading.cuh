@@ -249,8 +249,12 @@ OLC_D EmitterRec load_emitter(const SceneView& s, uint32_t i) {
 // Point of barycentrics (b1, b2) on the emitter: a + b1 (b - a) + b2 (c - a).
 // Uniform area sampling uses b1 = sqrt(u)(1 - v), b2 = sqrt(u) v, the
 // mapping of ordinarylight_area_light_position (ordinaryshade_primary.glsl:668-671).
+// The fused multiply-adds are written out so that every kernel (ReSTIR's
+// light pool, its reuse passes, shading) computes the same point bit for bit.
 OLC_D float3 emitter_point(const EmitterRec& e, float b1, float b2) {
-  return f3(e.a_pdf) + f3(e.e1_area) * b1 + f3(e.e2_sided) * b2;
+  return f3(__fmaf_rn(e.e2_sided.x, b2, __fmaf_rn(e.e1_area.x, b1, e.a_pdf.x)),
+            __fmaf_rn(e.e2_sided.y, b2, __fmaf_rn(e.e1_area.y, b1, e.a_pdf.y)),
+            __fmaf_rn(e.e2_sided.z, b2, __fmaf_rn(e.e1_area.z, b1, e.a_pdf.z)));
 }
 
 OLC_D float emitter_cosine(const EmitterRec& e, float3 dir) {
