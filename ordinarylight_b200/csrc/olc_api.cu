@@ -219,6 +219,7 @@ struct QueuedJob {
   bool job_local_reservoirs = false;
   bool textured = false;     // its scene has textures (the run uses the textured kernels)
   bool ref_volumes = false;  // reference-compatible job whose scene has volumes (their ray march runs)
+  bool media = false;        // production job whose scene has a participating medium
   uint32_t age = 0;          // serving steps since it was queued
 };
 
@@ -228,6 +229,7 @@ struct ChunkPlan {
   bool restir = false;
   bool textures = false;     // its jobs' scenes have textures (all or none of them)
   bool ref_volumes = false;  // some job marches reference volumes
+  bool media = false;        // some job tracks a participating medium (the shading kernel with media)
   std::vector<JobRec> segs;
 };
 
@@ -1289,6 +1291,7 @@ void plan_run(std::vector<QueuedJob*>& jobs, uint64_t cap, uint32_t max_chunks, 
       ch.bounces = std::max(ch.bounces, seg.max_bounces);
       ch.restir = ch.restir || seg.restir;
       ch.ref_volumes = ch.ref_volumes || t.job->ref_volumes;
+      ch.media = ch.media || t.job->media;
       at += t.count;
     }
     ch.count = (uint32_t)fill;
@@ -1465,7 +1468,7 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       }
       launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
-                   ch.textures, st);
+                   ch.textures, ch.media, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       // this bounce's shadow rays on the side stream: they touch only the
       // shadow queue and path radiance, so the next bounce's closest-hit
@@ -1496,8 +1499,8 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
   std::vector<uint64_t> k;
   k.push_back(plan.chunks.size());
   for (const ChunkPlan& c : plan.chunks)
-    k.push_back(((uint64_t)c.bounces << 3) | (c.ref_volumes ? 4u : 0u) | (c.textures ? 2u : 0u) |
-                (c.restir ? 1u : 0u));
+    k.push_back(((uint64_t)c.bounces << 4) | (c.media ? 8u : 0u) | (c.ref_volumes ? 4u : 0u) |
+                (c.textures ? 2u : 0u) | (c.restir ? 1u : 0u));
   auto ptr = [&](const void* p) { k.push_back((uint64_t)(uintptr_t)p); };
   const SceneView s = pool_view(ctx);
   const void* const* sv = reinterpret_cast<const void* const*>(&s);
@@ -1782,6 +1785,7 @@ void job_from_desc(olc_context* ctx, const olc_job* d, QueuedJob& q) {
   q.rec.sample_base = d->first_sample;
   q.textured = scene_of(ctx, d->scene).rec.tex_words != nullptr;
   q.ref_volumes = q.rec.mode == OLC_MODE_REFERENCE_COMPATIBLE && scene_of(ctx, d->scene).rec.num_ref_vols > 0u;
+  q.media = q.rec.mode != OLC_MODE_REFERENCE_COMPATIBLE && scene_of(ctx, d->scene).rec.volume_present != 0u;
   q.total = (uint64_t)q.rec.npix * q.rec.spp;
   q.out = d->out_rgba;
   q.sums = d->out_sums;
@@ -2001,6 +2005,7 @@ int olc_render(olc_context* ctx, const olc_camera* camera, uint32_t width, uint3
     job.rec.products = 1;
     job.textured = rs.rec.tex_words != nullptr;
     job.ref_volumes = job.rec.mode == OLC_MODE_REFERENCE_COMPATIBLE && rs.rec.num_ref_vols > 0u;
+    job.media = job.rec.mode != OLC_MODE_REFERENCE_COMPATIBLE && rs.rec.volume_present != 0u;
     job.total = (uint64_t)job.rec.npix * spp;
     job.out = out_rgba;
     job.out_device = out_is_device != 0;

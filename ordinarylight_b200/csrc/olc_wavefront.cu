@@ -336,12 +336,20 @@ OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& 
   return true;
 }
 
-// Three blocks of 256 threads per SM (at most 85 registers): the shading
-// kernel is latency bound, and the occupancy gained outweighs its spills.
-// kTextures: a variant for runs with a textured scene; the untextured one
-// carries none of the texture code's registers.
-template <bool kTextures>
-__global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
+// The shading kernel is latency bound, and the occupancy gained by a
+// register cap outweighs its spills: 80 registers (six blocks of 128
+// threads per SM) with media, 72 (seven) without.  kTextures: a variant for
+// runs with a textured scene; the untextured one carries none of the texture
+// code's registers.  kMedia: the same for participating media (delta
+// tracking at the vertex, ratio tracking of the shadow ray), whose code
+// raises the uncapped kernel from 90 to 110 registers; without it the
+// spills at 80 registers fall from 312 to 72 bytes.
+template <bool kMedia>
+struct ShadeRegisters {
+  static constexpr int kCap = kMedia ? 80 : 72;
+};
+template <bool kTextures, bool kMedia>
+__global__ void __maxnreg__(ShadeRegisters<kMedia>::kCap) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
   const uint32_t n = a.cnt->queue_count[bounce];
@@ -381,7 +389,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(ShadeArgs a) {
       // before the surface (or before leaving the scene) makes this vertex a
       // scattering event in the medium
       Medium med;
-      const bool has_medium = !cpu_mode && load_medium(sc, med);
+      const bool has_medium = kMedia && !cpu_mode && load_medium(sc, med);
       float t_med = 0.0f;
       const bool scattered =
           has_medium && medium_collision(med, o, d, ot.w, hit.x < 0.0f ? CUDART_INF_F : hit.x, rng, t_med);
@@ -1041,7 +1049,7 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
-                  bool textures, cudaStream_t stream) {
+                  bool textures, bool media, cudaStream_t stream) {
   ShadeArgs a;
   a.jobs = jobs;
   a.s = s;
@@ -1055,8 +1063,10 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   a.capacity = capacity;
   a.prod = prod;
   a.restir = restir;
-  if (textures) k_shade<true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
-  else k_shade<false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  if (textures && media) k_shade<true, true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  else if (textures) k_shade<true, false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  else if (media) k_shade<false, true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  else k_shade<false, false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_shade");
 }
 
