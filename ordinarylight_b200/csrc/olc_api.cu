@@ -1452,7 +1452,16 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         tl_mark(ctx, OLC_STAGE_SORT, b, c);
         std::swap(qin, spare);
       }
-      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, st);
+      HitListOut hl;
+      if (b == 0 && ch.restir) {
+        // the primary hits of the chunk's ReSTIR jobs, listed by the traversal
+        hl.jobs = jobs;
+        hl.meta = rb.ps.meta;
+        hl.list = ctx->restir.hit_list.as<uint32_t>();
+        hl.count = ctx->restir.hit_count.as<uint32_t>();
+        OLC_CUDA(cudaMemsetAsync(hl.count, 0, 4, st));
+      }
+      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, hl, st);
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
       if (b == 0 && ch.restir) {

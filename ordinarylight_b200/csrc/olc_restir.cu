@@ -22,9 +22,9 @@
 // only when its stamp equals the stamp of the wavefront that should have
 // written it, so pixels whose primary ray missed never need clearing.
 //
-// Only primary rays that hit take part: a compaction pass lists them first,
-// so the candidate loop runs with full warps even when much of the image is
-// sky.
+// Only primary rays that hit take part: the bounce-0 traversal lists them
+// (k_trace_closest's hit list), so the candidate loop runs with full warps
+// even when much of the image is sky.
 #include <cuda_fp16.h>
 
 #include "olc_restir.h"
@@ -40,8 +40,6 @@ constexpr uint32_t kRestirStream = 0x52455354u;  // stream key offset of the reu
 constexpr uint32_t kMaxNeighbours = 16;          // restir_neighbours' upper bound
 constexpr uint32_t kPoolStream = 0x504f4f4cu;    // stream key of the light pool and its block starts
 constexpr uint32_t kPoolSize = 1u << 15;         // light-pool entries per ReSTIR job and frame
-
-OLC_D uint32_t lane() { return threadIdx.x & 31u; }
 
 OLC_D uint32_t oct_encode(float3 n) {
   float s = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
@@ -320,25 +318,6 @@ struct RestirArgs {
   const float4* pool2;
 };
 
-// List the chunk's primary rays that hit something and belong to ReSTIR
-// jobs (warp-aggregated append; the list order does not affect any result).
-__global__ void k_restir_compact(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, HitBuf h,
-                                 PathState ps, uint32_t* list, uint32_t* count) {
-  const uint32_t n = hdr->count;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-    uint32_t i = base + lane();
-    bool take = i < n && h.tuv_slot[i].x >= 0.0f && jobs[ps.meta[i].w].restir;
-    uint32_t ballot = __ballot_sync(0xffffffffu, take);
-    if (ballot == 0u) continue;
-    uint32_t leader = __ffs(ballot) - 1u;
-    uint32_t off = 0;
-    if (lane() == leader) off = atomicAdd(count, __popc(ballot));
-    off = __shfl_sync(0xffffffffu, off, leader);
-    if (take) list[off + __popc(ballot & ((1u << lane()) - 1u))] = i;
-  }
-}
-
 // Light pool of every ReSTIR job of the chunk (after the presampled light
 // tiles of Wyman and Panteleev, HPG 2021): kPoolSize emitter samples drawn
 // from the scene's source distribution (alias-table emitter, uniform point
@@ -575,10 +554,6 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   k_restir_pool<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, s, st.pool0.as<float4>(), st.pool1.as<float4>(),
                                                     st.pool2.as<float4>());
   OLC_LAUNCH_CHECK("k_restir_pool");
-  OLC_CUDA(cudaMemsetAsync(st.hit_count.get(), 0, 4, stream));
-  k_restir_compact<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, hits, ps, st.hit_list.as<uint32_t>(),
-                                                        st.hit_count.as<uint32_t>());
-  OLC_LAUNCH_CHECK("k_restir_compact");
   const uint32_t grid = ls.grid_shade;
   if (textures) k_restir_initial<true><<<grid, 128, 0, stream>>>(a);
   else k_restir_initial<false><<<grid, 128, 0, stream>>>(a);

@@ -36,7 +36,8 @@ struct RestirState {
 // history's stamp range in each chunk header).
 void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32_t chunks, uint32_t segments);
 // Run initial RIS (+ temporal for jobs with history) + spatial reuse for one
-// chunk; returns the per-path-slot selected sample buffer consumed by the
+// chunk over the primary hits the bounce-0 traversal listed in hit_list /
+// hit_count; returns the per-path-slot selected sample buffer consumed by the
 // bounce-0 shading pass.  Every host-side input is a pointer or a configuration value,
 // so the launches can be captured in a graph and replayed.
 const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShape& ls, const SceneView& s,

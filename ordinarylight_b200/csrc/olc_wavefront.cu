@@ -191,7 +191,8 @@ struct TraceRegisters {
 
 template <int STACK, int SCHED>
 __global__ void __maxnreg__(TraceRegisters<SCHED>::kClosest) k_trace_closest(SceneView s, RayQueue q, HitBuf h,
-                                                                             Counters* cnt, uint32_t bounce) {
+                                                                             Counters* cnt, uint32_t bounce,
+                                                                             HitListOut hl) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->queue_count[bounce];
   uint32_t err = 0;
@@ -210,6 +211,21 @@ __global__ void __maxnreg__(TraceRegisters<SCHED>::kClosest) k_trace_closest(Sce
         h.tuv_slot[i] = tr.found() ? make_float4(tr.hit_t, tr.hit_u(), tr.hit_v(), __uint_as_float(tr.hit_slot))
                                    : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
         h.instance[i] = tr.found() ? tr.hit_inst : 0xffffffffu;
+        if (hl.list != nullptr) {
+          // bounce 0 (path slot i is queue slot i): list the primary hits of
+          // ReSTIR jobs for the resampling passes, one atomic per group of
+          // lanes finishing together; the list order affects no result
+          const bool take = tr.found() && hl.jobs[hl.meta[i].w].restir != 0u;
+          const uint32_t group = __activemask();
+          const uint32_t ballot = __ballot_sync(group, take);
+          if (ballot != 0u) {
+            const uint32_t leader = __ffs(ballot) - 1u;
+            uint32_t base = 0;
+            if (lane_id() == leader) base = atomicAdd(hl.count, __popc(ballot));
+            base = __shfl_sync(group, base, leader);
+            if (take) hl.list[base + __popc(ballot & ((1u << lane_id()) - 1u))] = i;
+          }
+        }
       },
       err);
   if (err) atomicAdd(&cnt->traversal_errors, 1u);
@@ -1017,17 +1033,17 @@ void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* 
 }
 
 void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
-                          Counters* cnt, uint32_t bounce, cudaStream_t stream) {
+                          Counters* cnt, uint32_t bounce, const HitListOut& hl, cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
+    const size_t smem = stack_bytes(D, ls.trace_block);
     // camera rays come in 8x4-pixel tiles: a warp keeps its 32 coherent rays
     // to the end instead of refilling lanes with rays of other tiles
     if (ls.scheduler == 1 || bounce == 0)
-      k_trace_closest<D, 1><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, q, h, cnt,
-                                                                                                        bounce);
+      k_trace_closest<D, 1><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce,
+                                                                             bounce == 0 ? hl : HitListOut{});
     else
-      k_trace_closest<D, 0><<<ls.grid_trace, ls.trace_block, stack_bytes(D, ls.trace_block), stream>>>(s, q, h, cnt,
-                                                                                                        bounce);
+      k_trace_closest<D, 0><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce, HitListOut{});
   });
   OLC_LAUNCH_CHECK("k_trace_closest");
 }

@@ -69,8 +69,17 @@ struct ProductPtrs {
 void configure_trace_kernels();
 void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const SceneRec* scenes,
                    const RayQueue& q, const PathState& ps, Counters* cnt, cudaStream_t stream);
+// Where camera-ray traversal lists the chunk's primary hits of ReSTIR jobs
+// (path slots, in completion order; `count` zeroed before the launch), or
+// list == nullptr for no list.
+struct HitListOut {
+  const JobRec* jobs = nullptr;
+  const uint4* meta = nullptr;   // path records (job index in .w)
+  uint32_t* list = nullptr;
+  uint32_t* count = nullptr;
+};
 void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
-                          Counters* cnt, uint32_t bounce, cudaStream_t stream);
+                          Counters* cnt, uint32_t bounce, const HitListOut& hl, cudaStream_t stream);
 void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const ShadowQueue& sq, const PathState& ps,
                          Counters* cnt, uint32_t bounce, cudaStream_t stream);
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
