@@ -72,7 +72,8 @@ OLC_D float3 oct_decode(uint32_t v) {
 // then costs only the half-vector terms.
 struct PreparedBsdf {
   float3 n, view, f0, diffuse;
-  float nv, a2, g1v;
+  float nv, a2;
+  float spec_scale;   // a2 G1(v) / (2 pi n.v): the GGX lobe's light-independent factor
 };
 
 OLC_D PreparedBsdf prepare_bsdf(const SurfaceMat& m, float3 n, float3 view) {
@@ -83,30 +84,34 @@ OLC_D PreparedBsdf prepare_bsdf(const SurfaceMat& m, float3 n, float3 view) {
   b.f0 = lerp3(f3(0.04f, 0.04f, 0.04f), m.base, m.metallic);
   b.diffuse = m.base * ((1.0f - m.metallic) / OLC_PI);
   b.a2 = ggx_alpha2(m.roughness);
-  b.g1v = ggx_g1(b.nv, b.a2);
+  b.spec_scale = b.nv > 0.0f ? b.a2 * ggx_g1(b.nv, b.a2) / (2.0f * OLC_PI * b.nv) : 0.0f;
   return b;
 }
 
 // The BSDF times the cosine-free factors for candidate direction l, with
-// hardware reciprocal square roots, approximate divisions and the GGX
-// bracket's sin^2(n, h) as 1 - (n.h)^2: the resampling target only has to be
-// one fixed function of the sample, positive where both cosines are (the
-// estimator stays unbiased for any such target), and this one costs about
-// half of the correctly rounded form per candidate.
+// hardware reciprocal square roots, one approximate division and the GGX
+// bracket's sin^2(n, h) as 1 - (n.h)^2.  The specular lobe
+// F D G1(v) G1(l) / (4 n.v n.l), with D = a2 / (pi den^2) and
+// G1(l) = 2 n.l / (n.l + sqrt(a2 + (1 - a2) (n.l)^2)), is evaluated as
+// F spec_scale / (den^2 (n.l + sqrt(...))) (n.l cancels), and
+// (1 - F) diffuse + F spec as diffuse + F (spec - diffuse).  The resampling
+// target only has to be one fixed function of the sample, positive where
+// both cosines are (the estimator stays unbiased for any such target).
 OLC_D float3 prepared_eval(const PreparedBsdf& b, float3 l, float nl) {
   const float3 hv = b.view + l;
   const float3 h = hv * rsqrtf(fmaxf(dot(hv, hv), 1e-30f));
   const float nh = fmaxf(dot(b.n, h), 0.0f);
   const float vh = fmaxf(dot(b.view, h), 0.0f);
-  const float w = 1.0f - clampf(vh, 0.0f, 1.0f);
-  const float w5 = w * w * w * w * w;
-  const float3 F = b.f0 + (f3(1.0f, 1.0f, 1.0f) - b.f0) * w5;
+  const float w = 1.0f - fminf(vh, 1.0f);
+  const float w2 = w * w;
+  const float w5 = w2 * w2 * w;
+  const float iw5 = 1.0f - w5;
   const float den = fmaf(nh * nh, b.a2, fmaxf(fmaf(-nh, nh, 1.0f), 0.0f));   // the GGX bracket of ggx_d
-  const float D = __fdividef(b.a2, fmaxf(OLC_PI * den * den, 1e-30f));
-  const float x = b.a2 + (1.0f - b.a2) * nl * nl;
-  const float g1l = __fdividef(2.0f * nl, fmaxf(nl + x * rsqrtf(x), 1e-6f));
-  const float3 spec = F * __fdividef(D * b.g1v * g1l, fmaxf(4.0f * b.nv * nl, 1e-6f));
-  return (f3(1.0f, 1.0f, 1.0f) - F) * b.diffuse + spec;
+  const float x = fmaf(1.0f - b.a2, nl * nl, b.a2);
+  const float spec = __fdividef(b.spec_scale, fmaxf(den * den * (nl + x * rsqrtf(x)), 1e-30f));
+  const float3 F = f3(fmaf(b.f0.x, iw5, w5), fmaf(b.f0.y, iw5, w5), fmaf(b.f0.z, iw5, w5));
+  return f3(fmaf(F.x, spec - b.diffuse.x, b.diffuse.x), fmaf(F.y, spec - b.diffuse.y, b.diffuse.y),
+            fmaf(F.z, spec - b.diffuse.z, b.diffuse.z));
 }
 
 struct Surface {
@@ -129,9 +134,14 @@ OLC_D uint32_t pack_bary(float b1, float b2) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
+// The emitter radiance weighted by the luminance coefficients, so that
+// luminance(f Le) = dot(f, luminance_weighted(Le)).
+OLC_D float3 luminance_weighted(float3 Le) { return f3(Le.x * 0.2126f, Le.y * 0.7152f, Le.z * 0.0722f); }
+
 // Unshadowed target of a light sample at surface s, given the sample's point,
-// the emitter's normal, sidedness and radiance: luminance(f Le) cos_s cos_l / d^2.
-OLC_D float target_at(const Surface& s, float3 lp, float3 lnormal, bool two_sided, float3 Le) {
+// the emitter's normal, sidedness and luminance-weighted radiance Lw:
+// dot(f, Lw) cos_s cos_l / d^2 = luminance(f Le) cos_s cos_l / d^2.
+OLC_D float target_at(const Surface& s, float3 lp, float3 lnormal, bool two_sided, float3 Lw) {
   float3 off = lp - s.p;
   float d2 = dot(off, off);
   if (!(d2 > 1e-12f)) return 0.0f;
@@ -143,7 +153,7 @@ OLC_D float target_at(const Surface& s, float3 lp, float3 lnormal, bool two_side
   float cl = two_sided ? fabsf(c) : fmaxf(c, 0.0f);   // emitter_cosine
   if (cl <= 1e-6f) return 0.0f;
   float3 f = prepared_eval(s.bsdf, l, cs);
-  float t = luminance(f * Le) * cs * cl * (inv * inv);
+  float t = dot(f, Lw) * cs * cl * (inv * inv);
   return (t == t && t < 3.0e38f) ? fmaxf(t, 0.0f) : 0.0f;
 }
 
@@ -152,7 +162,8 @@ OLC_D float target_at(const Surface& s, float3 lp, float3 lnormal, bool two_side
 OLC_D float target_of(const SceneView& sc, const Surface& s, uint32_t light, uint32_t bary) {
   const EmitterRec e = load_emitter(sc, light);
   const float2 b = unpack_bary(bary);
-  return target_at(s, emitter_point(e, b.x, b.y), f3(e.normal), e.e2_sided.w > 0.5f, f3(e.emission));
+  return target_at(s, emitter_point(e, b.x, b.y), f3(e.normal), e.e2_sided.w > 0.5f,
+                   luminance_weighted(f3(e.emission)));
 }
 
 // Returns whether the offered sample was selected.
@@ -324,8 +335,8 @@ struct RestirArgs {
 // with the reference's square-root mapping, ordinaryshade_primary.glsl:668-671),
 // each stored with the terms the resampling target reads: the point and the
 // reciprocal source pdf per unit area (negative for a two-sided emitter), the
-// emitter's normal and the sample's half-precision barycentrics, its radiance
-// and index.  Entries are keyed by (entry, job.frame) only, so every chunking
+// emitter's normal and the sample's half-precision barycentrics, its
+// luminance-weighted radiance and index.  Entries are keyed by (entry, job.frame) only, so every chunking
 // and batch mix draws the same pool.
 __global__ void k_restir_pool(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, SceneView s,
                               float4* __restrict__ p0, float4* __restrict__ p1, float4* __restrict__ p2) {
@@ -351,7 +362,8 @@ __global__ void k_restir_pool(const ChunkHeader* __restrict__ hdr, const JobRec*
     const float3 lp = emitter_point(e, b.x, b.y);
     p0[k] = make_float4(lp.x, lp.y, lp.z, e.e2_sided.w > 0.5f ? -e.emission.w : e.emission.w);
     p1[k] = make_float4(e.normal.x, e.normal.y, e.normal.z, __uint_as_float(bary));
-    p2[k] = make_float4(e.emission.x, e.emission.y, e.emission.z, __uint_as_float(li));
+    const float3 lw = luminance_weighted(f3(e.emission));
+    p2[k] = make_float4(lw.x, lw.y, lw.z, __uint_as_float(li));
   }
 }
 

@@ -64,6 +64,22 @@ def test_batch_equals_plain_bit_for_bit(native_library, cuda_device, scene_set, 
         assert image2.tobytes() == image.tobytes()
 
 
+def test_a_medium_scene_in_the_chunk_keeps_the_other_images(native_library, cuda_device, scene_set):
+    """Chunks whose scenes have no participating medium run the shading
+    kernel built without the medium code; a chunk that also holds a job over
+    a scene with a medium runs the full kernel for all of its jobs.  The
+    medium-free jobs must come out bit for bit as their plain renders do
+    (which ran the medium-free kernel), and the medium job as its own."""
+    terrain, terrain_cam = scenes.terrain(size=64, volume_size=16)
+    requests = _requests(scene_set)[:3] + [RenderRequest(terrain, terrain_cam, 48, 32, samples=2, frame_index=2,
+                                                         max_bounces=4)]
+    with CudaWavefrontRenderer(seed=1) as r:
+        images = r.render_batch(requests)
+        assert r.last_timings["chunks"] == 1   # one chunk: every job is shaded by the full kernel
+    for request, image in zip(requests, images):
+        assert image.tobytes() == _plain(request).tobytes()
+
+
 @pytest.mark.parametrize("chunk_paths", [4096, 20000])
 def test_batch_chunking_does_not_change_images(native_library, cuda_device, scene_set, chunk_paths):
     requests = _requests(scene_set)
