@@ -148,18 +148,26 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
   uint32_t my = 0xffffffffu;
   bool exhausted = false;
   const uint32_t lt = (1u << lane_id()) - 1u;
+  // A queue shorter than the grid's warp count is spread one ray per warp,
+  // so its rays run in separate warps instead of diverging in a few: the
+  // launch then takes about one ray's latency.
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  const uint32_t cap = n < warps ? 1u : 32u;
   while (true) {
     const bool idle = my == 0xffffffffu;
     if (!exhausted) {
       const uint32_t idle_mask = __ballot_sync(0xffffffffu, idle);
       const uint32_t want = __popc(idle_mask);
-      if (want >= kRefillLanes || idle_mask == 0xffffffffu) {
+      const uint32_t busy = 32u - want;
+      const uint32_t take = busy >= cap ? 0u : min(want, cap - busy);
+      if (take > 0u && (want >= kRefillLanes || idle_mask == 0xffffffffu || cap < 32u)) {
         const uint32_t leader = __ffs(idle_mask) - 1u;
         uint32_t base = 0;
-        if (lane_id() == leader) base = atomicAdd(cursor, want);
+        if (lane_id() == leader) base = atomicAdd(cursor, take);
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (idle) {
-          const uint32_t cand = base + __popc(idle_mask & lt);
+        const uint32_t rank = __popc(idle_mask & lt);
+        if (idle && rank < take) {
+          const uint32_t cand = base + rank;
           if (cand < n) {
             my = cand;
             float3 o, d;
@@ -169,7 +177,7 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
             tr.begin(s, o, d, tmin, tmax, root, smem, spill);
           }
         }
-        if (base + want >= n) exhausted = true;
+        if (base + take >= n) exhausted = true;
       }
     }
     if (__ballot_sync(0xffffffffu, my != 0xffffffffu) == 0u) break;
