@@ -874,45 +874,49 @@ OLC_D unsigned long long to_fixed(float v, uint32_t* nan_counter) {
 // value divided back (the division k_resolve does for spp = 1).
 OLC_D float from_fixed(unsigned long long v) { return (float)((double)v * (1.0 / (double)OLC_ACCUM_SCALE)); }
 
-// Each thread takes four paths a grid stride apart and loads all their
-// radiance and path records before the first job lookup and atomic: the
-// kernel waits on these loads, not on the atomics (fire-and-forget
-// reductions).  Integer sums make the result independent of the order.
+// Path samples into their pixels' fixed-point sums.  A segment made of whole
+// sample streams (its first path and its length multiples of the image's
+// pixel count, as ReSTIR jobs and single-chunk frames are) holds every one of
+// its samples of a pixel at the same position of each stream, so the thread
+// of the first stream's path adds them all with one atomic per channel
+// instead of one per sample; other segments add path by path.  Integer sums
+// make the result independent of the grouping and the order.
 __global__ void k_accumulate(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs, PathState ps,
                              unsigned long long* accum, float* sample_lum, Counters* cnt) {
-  constexpr uint32_t kPaths = 4;
   const uint32_t count = hdr->count;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < count; i0 += kPaths * stride) {
-    float4 r[kPaths];
-    uint4 meta[kPaths];
-#pragma unroll
-    for (uint32_t u = 0; u < kPaths; ++u) {
-      const uint32_t i = i0 + u * stride;
-      if (i < count) {
-        r[u] = ps.radiance[i];
-        meta[u] = ps.meta[i];
-      }
+  const uint32_t num_segments = hdr->num_segments;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint4 meta = ps.meta[i];
+    const JobRec& job = jobs[meta.w];
+    const uint32_t seg_begin = (uint32_t)job.seg_begin;
+    const uint32_t seg_end = meta.w + 1u < num_segments ? (uint32_t)jobs[meta.w + 1u].seg_begin : count;
+    const uint32_t seg_count = seg_end - seg_begin;
+    uint32_t samples = 1u;
+    if (job.seg_first % job.npix == 0ull && seg_count % job.npix == 0u) {
+      if (i - seg_begin >= job.npix) continue;   // added with its pixel's first-stream path
+      samples = seg_count / job.npix;
     }
-#pragma unroll
-    for (uint32_t u = 0; u < kPaths; ++u) {
-      if (i0 + u * stride >= count) break;
-      const JobRec& job = jobs[meta[u].w];
-      unsigned long long* dst = accum + 3ull * (job.pixel_base + meta[u].x);
-      const unsigned long long fr = to_fixed(r[u].x, &cnt->nan_samples);
-      const unsigned long long fg = to_fixed(r[u].y, &cnt->nan_samples);
-      const unsigned long long fb = to_fixed(r[u].z, &cnt->nan_samples);
-      atomicAdd(dst + 0, fr);
-      atomicAdd(dst + 1, fg);
-      atomicAdd(dst + 2, fb);
+    unsigned long long fr = 0ull, fg = 0ull, fb = 0ull;
+    for (uint32_t k = 0; k < samples; ++k) {
+      const float4 r = ps.radiance[i + k * job.npix];
+      const unsigned long long sr = to_fixed(r.x, &cnt->nan_samples);
+      const unsigned long long sg = to_fixed(r.y, &cnt->nan_samples);
+      const unsigned long long sb = to_fixed(r.z, &cnt->nan_samples);
+      fr += sr;
+      fg += sg;
+      fb += sb;
       if (job.lum_base != ~0ull) {
         // luminance in float32 in the reference's operation order
         // (api.py:1404-1410: r * 0.2126 + g * 0.7152 + b * 0.0722), unfused
-        const float l = __fadd_rn(__fadd_rn(__fmul_rn(from_fixed(fr), 0.2126f), __fmul_rn(from_fixed(fg), 0.7152f)),
-                                  __fmul_rn(from_fixed(fb), 0.0722f));
-        sample_lum[job.lum_base + (uint64_t)(meta[u].y - job.sample_base) * job.npix + meta[u].x] = l;
+        const float l = __fadd_rn(__fadd_rn(__fmul_rn(from_fixed(sr), 0.2126f), __fmul_rn(from_fixed(sg), 0.7152f)),
+                                  __fmul_rn(from_fixed(sb), 0.0722f));
+        sample_lum[job.lum_base + (uint64_t)(meta.y - job.sample_base + k) * job.npix + meta.x] = l;
       }
     }
+    unsigned long long* dst = accum + 3ull * (job.pixel_base + meta.x);
+    atomicAdd(dst + 0, fr);
+    atomicAdd(dst + 1, fg);
+    atomicAdd(dst + 2, fb);
   }
 }
 
