@@ -660,10 +660,13 @@ def run_served(device_index, rates, count, budget_bytes, chunk_paths, frame_limi
             r.resident_scene(v[0])
         warm = workloads.served_requests(variants, 16, seed=99)
         r.render_batch(warm)
-        # one-time costs of the serving path (graph captures, arena and
-        # staging growth) are paid by a short warm-up stream
+        # one-time costs of the serving path (graph captures, growth of the
+        # pixel arena, the chunk tables and the light pools) are paid by a
+        # warm-up stream at the highest rate, whose many requests in flight
+        # grow every buffer to what the measured streams need
         warm_server = RenderServer(r, budget_bytes=budget_bytes).start()
         run_stream(warm_server, warm, poisson_arrivals(float(rates[0]), len(warm), seed=98))
+        run_stream(warm_server, requests, poisson_arrivals(float(max(rates)), len(requests), seed=97))
         warm_server.stop()
         torch.cuda.synchronize()
         for rate in rates:
