@@ -188,19 +188,14 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
   }
 }
 
-// Register caps of the traversal kernels: 64 registers hold the traversal
+// Register cap of the traversal kernels: 64 registers hold the traversal
 // state without spilling (the world ray and the hit's barycentrics live in
 // shared memory), so eight blocks of 128 threads stay resident per SM.
-template <int SCHED>
-struct TraceRegisters {
-  static constexpr int kClosest = 64;
-  static constexpr int kShadow = 64;
-};
+constexpr int kTraceRegisters = 64;
 
 template <int STACK, int SCHED>
-__global__ void __maxnreg__(TraceRegisters<SCHED>::kClosest) k_trace_closest(SceneView s, RayQueue q, HitBuf h,
-                                                                             Counters* cnt, uint32_t bounce,
-                                                                             HitListOut hl) {
+__global__ void __maxnreg__(kTraceRegisters) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
+                                                              uint32_t bounce, HitListOut hl) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->queue_count[bounce];
   uint32_t err = 0;
@@ -240,8 +235,8 @@ __global__ void __maxnreg__(TraceRegisters<SCHED>::kClosest) k_trace_closest(Sce
 }
 
 template <int STACK, int SCHED>
-__global__ void __maxnreg__(TraceRegisters<SCHED>::kShadow) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps,
-                                                                           Counters* cnt, uint32_t bounce) {
+__global__ void __maxnreg__(kTraceRegisters) k_trace_shadow(SceneView s, ShadowQueue sq, PathState ps,
+                                                             Counters* cnt, uint32_t bounce) {
   extern __shared__ int smem_stack[];
   const uint32_t n = cnt->shadow_count[bounce];
   uint32_t err = 0;
@@ -366,8 +361,8 @@ OLC_D bool next_event(const SceneView& s, const SceneRec& sc, const SurfaceMat& 
 // runs with a textured scene; the untextured one carries none of the texture
 // code's registers.  kMedia: the same for participating media (delta
 // tracking at the vertex, ratio tracking of the shadow ray), whose code
-// raises the uncapped kernel from 90 to 110 registers; without it the
-// spills at 80 registers fall from 312 to 72 bytes.
+// raises the uncapped kernel from 90 to 110 registers (312 bytes of spills
+// at 80 registers with it, 96 at 72 without it).
 template <bool kMedia>
 struct ShadeRegisters {
   static constexpr int kCap = kMedia ? 80 : 72;
