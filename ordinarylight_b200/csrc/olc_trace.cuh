@@ -302,12 +302,14 @@ struct Traversal {
   }
 
   OLC_D bool advance(const SceneView& s, int iterations, uint32_t& err) {
-    for (int it = 0; it < iterations; ++it) {
-      if (--budget == 0u) {
-        err = 1u;
-        return true;
-      }
-      if (node >= 0 && node != OLC_MARKER) {
+    // The budget is charged per call, not per iteration (a call may charge
+    // more than it uses; the bound only has to end a corrupt walk).
+    const uint32_t steps = min((uint32_t)iterations, budget);
+    budget -= steps;
+    for (uint32_t it = 0; it < steps; ++it) {
+      // `node` is never the instance marker here: a marker is only popped,
+      // and the pop below steps past it.
+      if (node >= 0) {
         // BVH4 node: test the four child boxes, descend into the nearest
         // hit child and push the others, farthest first (closest hit) or in
         // slot order (any hit, where the order changes nothing but time).
@@ -348,7 +350,7 @@ struct Traversal {
           node = c0;
           continue;
         }
-      } else if (node != OLC_MARKER) {
+      } else {
         const uint32_t first = olc_leaf_first(node);
         const uint32_t count = olc_leaf_count(node);
         if (cur_inst == OLC_NO_INSTANCE && count == OLC_TLAS_LEAF_TRIANGLE) {
@@ -395,6 +397,10 @@ struct Traversal {
         if (st.sp == 0) return true;
         node = st.pop();
       }
+    }
+    if (budget == 0u) {
+      err = 1u;
+      return true;
     }
     return false;
   }
