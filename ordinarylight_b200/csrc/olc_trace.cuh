@@ -323,18 +323,18 @@ struct Traversal {
         const bool h1 = child_box(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, ray, t_min, hit_t, n1);
         const bool h2 = child_box(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, ray, t_min, hit_t, n2);
         const bool h3 = child_box(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, ray, t_min, hit_t, n3);
-        const int hits = (int)h0 + (int)h1 + (int)h2 + (int)h3;
-        if (hits == 0) {
+        if (ANY_HIT) {
+          if (h0 || h1 || h2 || h3) {
+            int next = OLC_EMPTY_CHILD;
+            if (h3) next = ch.w;
+            if (h2) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.z; }
+            if (h1) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.y; }
+            if (h0) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.x; }
+            node = next;
+            continue;
+          }
           // nothing to enter: fall through to the pop
-        } else if (ANY_HIT) {
-          int next = OLC_EMPTY_CHILD;
-          if (h3) next = ch.w;
-          if (h2) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.z; }
-          if (h1) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.y; }
-          if (h0) { if (next != OLC_EMPTY_CHILD) st.push(next, err); next = ch.x; }
-          node = next;
-          continue;
-        } else {
+        } else if (const int hits = (int)h0 + (int)h1 + (int)h2 + (int)h3) {
           // misses sort last (+inf); a hit's key is finite
           float k0 = h0 ? fminf(n0, 3.0e38f) : CUDART_INF_F, k1 = h1 ? fminf(n1, 3.0e38f) : CUDART_INF_F;
           float k2 = h2 ? fminf(n2, 3.0e38f) : CUDART_INF_F, k3 = h3 ? fminf(n3, 3.0e38f) : CUDART_INF_F;
