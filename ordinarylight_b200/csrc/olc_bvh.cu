@@ -1,7 +1,8 @@
 // Device LBVH construction: 30-bit Morton codes, a stable LSD radix sort,
 // Karras' parallel hierarchy emission, bottom-up boxes, leaf collapse and a
 // node layout of two child boxes per 64-byte node; refit; the BVH4 form
-// traversal reads (four grandchildren per 128-byte node); validation.
+// traversal reads (up to four descendants per 128-byte node, collapsed
+// greedily by surface area); validation.
 //
 // Replaces the driver-built hardware BLAS/TLAS of the reference
 // (VulkanSceneUploader._build_scene, ordinarylight/targets/vulkan/scene.py:1484-1560):

@@ -141,13 +141,15 @@ OLC_HD uint32_t olc_leaf_first(int ref) { return ((uint32_t)(~ref)) >> 3; }
 OLC_HD uint32_t olc_leaf_count(int ref) { return (((uint32_t)(~ref)) & 7u) + 1u; }
 #define OLC_EMPTY_CHILD ((int)0x80000000)
 
-// BVH4 node, 128 bytes (one L2 line, seven 16-byte loads): the four
-// grandchildren of BVH2 node i (a leaf child stands for itself), stored at
-// index i of a second array parallel to the BVH2 nodes.  Traversal descends
-// two BVH2 levels per dependent fetch.  Child references keep the BVH2
-// encoding, and an internal child's index is its BVH2 index, so roots,
-// instance records and leaves are shared by both forms.  Box slot k of the
-// six float4 is child k; unused slots hold OLC_EMPTY_CHILD.
+// BVH4 node, 128 bytes (one L2 line, seven 16-byte loads): up to four
+// descendants of BVH2 node i (its children, each internal one opened in turn
+// while the largest box still fits four slots; a leaf stands for itself),
+// stored at index i of a second array parallel to the BVH2 nodes.  Traversal
+// descends about two BVH2 levels per dependent fetch.  Child references keep
+// the BVH2 encoding, and an internal child's index is its BVH2 index, so
+// roots, instance records and leaves are shared by both forms.  Box slot k of
+// the six float4 is child k; unused slots hold OLC_EMPTY_CHILD and an
+// inverted box (lo +inf, hi -inf) that no ray enters.
 struct __align__(16) BvhNode4 {
   float4 lox, hix, loy, hiy, loz, hiz;
   int4 child;

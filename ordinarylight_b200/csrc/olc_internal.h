@@ -138,8 +138,8 @@ uint32_t build_tlas(const float* object_to_world, const uint2* slot_ranges, uint
                     BvhNode* nodes, uint32_t node_base, cudaStream_t stream);
 
 // The BVH4 form (BvhNode4) of BVH2 nodes [begin, begin + count): wide[i]
-// holds the grandchildren of nodes[i].  Run after every build or refit that
-// wrote those nodes.
+// holds up to four descendants of nodes[i] (greedy surface-area collapse).
+// Run after every build or refit that wrote those nodes.
 void build_bvh4(const BvhNode* nodes, BvhNode4* wide, uint32_t begin, uint32_t count, cudaStream_t stream);
 
 // One built bottom-level structure: its root node and triangle slot range.

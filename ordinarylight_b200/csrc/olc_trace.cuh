@@ -4,9 +4,11 @@
 // (nativeTraceSurface, ordinarylight/shaders/wavefront_intersect.comp:96-235;
 // nativeOccluded in ordinarylight/shaders/transport_v1/lighting.glsl).
 // * TLAS and BLAS nodes share one node pool; a TLAS leaf is one instance.
-//   Traversal reads the BVH4 form of the pool (BvhNode4: the four
-//   grandchildren of a BVH2 node in one 128-byte line), so each dependent
-//   fetch descends two levels of the binary hierarchy.
+//   Traversal reads the BVH4 form of the pool (BvhNode4: up to four
+//   descendants of a BVH2 node in one 128-byte line, collapsed greedily by
+//   surface area), so each dependent fetch descends about two levels of the
+//   binary hierarchy.  A ray picks each axis's near and far box planes once
+//   from its direction's signs, so the slab test needs no per-axis min/max.
 //   Entering an instance transforms the ray to object space (t is preserved
 //   because the direction is not renormalised) and pushes a marker that
 //   restores the world ray when the instance's subtree is exhausted; the
@@ -18,7 +20,7 @@
 //   column layout; a launch gives (STACK + OLC_RAY_SAVE) * blockDim.x words.
 //   What a ray needs only at instance transitions or at its end (the world
 //   ray, the closest hit's barycentrics) lives there rather than in
-//   registers, which keeps seven blocks of 128 threads resident per SM.
+//   registers, which keeps eight blocks of 128 threads resident per SM.
 //   Deeper entries spill to a bounded local array.  A push beyond both is
 //   counted as a traversal error instead of writing out of bounds.
 // * Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013):
