@@ -287,11 +287,14 @@ struct olc_context {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   // any-hit traversal of a bounce's shadow rays runs on a second stream,
-  // beside the next bounce's closest-hit traversal, and joins the main
-  // stream before the next shading pass
+  // beside the later bounces' traversal and shading.  Shadow queues
+  // alternate between two buffers by bounce parity, so shading waits only
+  // for the shadow rays of two bounces back (which read the queue it
+  // refills); accumulation waits for all of them
   cudaStream_t side = nullptr;
-  cudaEvent_t fork_event = nullptr, join_event = nullptr;
-  bool side_pending = false;
+  cudaEvent_t fork_event = nullptr, join_event[2] = {nullptr, nullptr};
+  bool side_pending[2] = {false, false};
+  uint32_t side_last = 0;   // parity of the latest shadow launch
   uint32_t tl_next = 0, tl_last = 0;   // next event index; last event on the main stream
   std::string error;
   BuildScratch scratch;
@@ -309,8 +312,8 @@ struct olc_context {
   uint32_t default_scene = kNoScene;
   // wavefront buffers
   uint32_t capacity = 0;
-  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, ps_tp,
-      ps_rad, ps_meta, ps_ior, ps_cone, sort_keys, sort_bins;
+  DeviceBuffer q0_o, q0_d, q0_p, q1_o, q1_d, q1_p, q2_o, q2_d, q2_p, hit_tuv, hit_inst, sh_o, sh_d, sh_c, sh1_o,
+      sh1_d, sh1_c, ps_tp, ps_rad, ps_shadow, ps_meta, ps_ior, ps_cone, sort_keys, sort_bins;
   DeviceBuffer counters, job_dev;
   DeviceBuffer prod_depth, prod_normal, prod_inst, prod_mat, prod_prim, prod_pos, prod_bary, prod_signals,
       prod_secondary;
@@ -420,7 +423,7 @@ uint32_t tl_record(olc_context* ctx, cudaStream_t stream) {
 
 void tl_begin(olc_context* ctx) {
   ctx->cur->entries.clear();
-  ctx->side_pending = false;
+  ctx->side_pending[0] = ctx->side_pending[1] = false;
   ctx->tl_next = 0;
   ctx->tl_last = tl_record(ctx, ctx->stream);
 }
@@ -432,12 +435,20 @@ void tl_mark(olc_context* ctx, uint32_t stage, uint32_t bounce, uint32_t chunk) 
   ctx->tl_last = end;
 }
 
-// Wait on the main stream for the side stream's pending work.
-void side_join(olc_context* ctx) {
-  if (!ctx->side_pending) return;
-  OLC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0));
-  ctx->side_pending = false;
+// Wait on the main stream for the side stream's shadow launches of one
+// bounce parity (and, the side stream being in order, for every one before).
+void side_wait(olc_context* ctx, uint32_t parity) {
+  if (!ctx->side_pending[parity]) return;
+  OLC_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_event[parity], 0));
+  ctx->side_pending[parity] = false;
+  if (parity == ctx->side_last) ctx->side_pending[parity ^ 1u] = false;
   ctx->tl_last = tl_record(ctx, ctx->stream);   // later stages start after the wait
+}
+
+// Wait on the main stream for all of the side stream's pending work.
+void side_join(olc_context* ctx) {
+  if (ctx->side_pending[ctx->side_last]) side_wait(ctx, ctx->side_last);
+  else if (ctx->side_pending[ctx->side_last ^ 1u]) side_wait(ctx, ctx->side_last ^ 1u);
 }
 
 // Inverse of a row-major 3x4 affine (double precision on the host).
@@ -1322,8 +1333,12 @@ void ensure_wavefront(olc_context* ctx, uint32_t capacity) {
   ctx->sh_o.allocate(c * 16);
   ctx->sh_d.allocate(c * 16);
   ctx->sh_c.allocate(c * 16);
+  ctx->sh1_o.allocate(c * 16);
+  ctx->sh1_d.allocate(c * 16);
+  ctx->sh1_c.allocate(c * 16);
   ctx->ps_tp.allocate(c * 16);
   ctx->ps_rad.allocate(c * 16);
+  ctx->ps_shadow.allocate(c * 16);
   ctx->ps_ior.allocate(c * 64);
   ctx->ps_cone.allocate(c * 8);
   ctx->ps_meta.allocate(c * 16);
@@ -1389,7 +1404,7 @@ void release_slot(RunSlot& sl) {
 struct RunBuffers {
   RayQueue qa, qb, qc;
   HitBuf hb;
-  ShadowQueue sq;
+  ShadowQueue sq[2];   // by bounce parity
   PathState ps;
   ProductPtrs prod;
   Counters* cnt;
@@ -1407,9 +1422,10 @@ RunBuffers run_buffers(olc_context* ctx, const RunSlot& sl, size_t stride, size_
   b.qb = RayQueue{ctx->q1_o.as<float4>(), ctx->q1_d.as<float4>(), ctx->q1_p.as<uint32_t>()};
   b.qc = RayQueue{ctx->q2_o.as<float4>(), ctx->q2_d.as<float4>(), ctx->q2_p.as<uint32_t>()};
   b.hb = HitBuf{ctx->hit_tuv.as<float4>(), ctx->hit_inst.as<uint32_t>()};
-  b.sq = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
+  b.sq[0] = ShadowQueue{ctx->sh_o.as<float4>(), ctx->sh_d.as<float4>(), ctx->sh_c.as<float4>()};
+  b.sq[1] = ShadowQueue{ctx->sh1_o.as<float4>(), ctx->sh1_d.as<float4>(), ctx->sh1_c.as<float4>()};
   b.ps = PathState{ctx->ps_tp.as<float4>(), ctx->ps_rad.as<float4>(), ctx->ps_meta.as<uint4>(),
-                   ctx->ps_ior.as<float4>(), ctx->ps_cone.as<float2>()};
+                   ctx->ps_ior.as<float4>(), ctx->ps_cone.as<float2>(), ctx->ps_shadow.as<float4>()};
   b.prod.depth = ctx->prod_depth.as<float>();
   b.prod.normal = ctx->prod_normal.as<float4>();
   b.prod.instance_id = ctx->prod_inst.as<uint32_t>();
@@ -1468,28 +1484,29 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         restir = restir_run(ctx->restir, ctx->cfg, ctx->ls, s, hdr, jobs, *qin, rb.hb, rb.ps, ch.textures, st);
         tl_mark(ctx, OLC_STAGE_RESTIR, b, c);
       }
-      // shading adds to path radiance and refills the shadow queue: the
-      // previous bounce's shadow rays must be done
-      side_join(ctx);
+      // shading refills the shadow queue of its bounce's parity: the shadow
+      // rays of two bounces back, which read it, must be done
+      side_wait(ctx, b & 1u);
       if (ch.ref_volumes) {
         // reference-compatible paths cross their scene's volumes before shading
         launch_ref_volumes(ctx->ls, jobs, s, *qin, rb.hb, rb.ps, rb.cnt, b, st);
         tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       }
-      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq, rb.ps, rb.cnt, b, ctx->capacity, rb.prod, restir,
-                   ch.textures, ch.media, st);
+      launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq[b & 1u], rb.ps, rb.cnt, b, ctx->capacity, rb.prod,
+                   restir, ch.textures, ch.media, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
-      // this bounce's shadow rays on the side stream: they touch only the
-      // shadow queue and path radiance, so the next bounce's closest-hit
-      // traversal runs beside them and fills their tail
+      // this bounce's shadow rays on the side stream: they read only their
+      // queue and add only to the paths' shadow sums, so the later bounces'
+      // traversal and shading run beside them and fill their tail
       OLC_CUDA(cudaEventRecord(ctx->fork_event, st));
       OLC_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_event, 0));
       const uint32_t side_start = tl_record(ctx, ctx->side);
-      launch_trace_shadow(ctx->ls, s, rb.sq, rb.ps, rb.cnt, b, ctx->side);
+      launch_trace_shadow(ctx->ls, s, rb.sq[b & 1u], rb.ps, rb.cnt, b, ctx->side);
       const uint32_t side_end = tl_record(ctx, ctx->side);
       ctx->cur->entries.push_back(TimelineEntry{OLC_STAGE_SHADOW, b, c, side_start, side_end});
-      OLC_CUDA(cudaEventRecord(ctx->join_event, ctx->side));
-      ctx->side_pending = true;
+      OLC_CUDA(cudaEventRecord(ctx->join_event[b & 1u], ctx->side));
+      ctx->side_pending[b & 1u] = true;
+      ctx->side_last = b & 1u;
       std::swap(qin, qout);
     }
     side_join(ctx);
@@ -1518,9 +1535,11 @@ std::vector<uint64_t> run_signature(const olc_context* ctx, const RunPlan& plan,
                         (const void*)rb.qb.origin_tmin, (const void*)rb.qb.dir_root, (const void*)rb.qb.path,
                         (const void*)rb.qc.origin_tmin, (const void*)rb.qc.dir_root, (const void*)rb.qc.path,
                         ctx->sort_keys.get(), ctx->sort_bins.get(),
-                        (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq.origin_tmax,
-                        (const void*)rb.sq.dir_path, (const void*)rb.sq.contrib_root, (const void*)rb.ps.throughput,
-                        (const void*)rb.ps.radiance, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.ps.cone, (const void*)rb.prod.depth,
+                        (const void*)rb.hb.tuv_slot, (const void*)rb.hb.instance, (const void*)rb.sq[0].origin_tmax,
+                        (const void*)rb.sq[0].dir_path, (const void*)rb.sq[0].contrib_root,
+                        (const void*)rb.sq[1].origin_tmax, (const void*)rb.sq[1].dir_path,
+                        (const void*)rb.sq[1].contrib_root, (const void*)rb.ps.throughput,
+                        (const void*)rb.ps.radiance, (const void*)rb.ps.shadow, (const void*)rb.ps.meta, (const void*)rb.ps.ior_stack, (const void*)rb.ps.cone, (const void*)rb.prod.depth,
                         (const void*)rb.prod.normal, (const void*)rb.prod.instance_id, (const void*)rb.prod.material_id,
                         (const void*)rb.prod.primitive_id, (const void*)rb.prod.position,
                         (const void*)rb.prod.barycentric, (const void*)rb.prod.signals,
@@ -1841,7 +1860,8 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     OLC_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     OLC_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
     OLC_CUDA(cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming));
-    OLC_CUDA(cudaEventCreateWithFlags(&ctx->join_event, cudaEventDisableTiming));
+    OLC_CUDA(cudaEventCreateWithFlags(&ctx->join_event[0], cudaEventDisableTiming));
+    OLC_CUDA(cudaEventCreateWithFlags(&ctx->join_event[1], cudaEventDisableTiming));
     configure_trace_kernels();
     apply_launch_shape(ctx.get());
     // pool record 0: the identity instance that baked triangles report
@@ -1864,7 +1884,8 @@ int olc_create(const olc_config* cfg, olc_context** out) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
-    if (ctx->join_event) cudaEventDestroy(ctx->join_event);
+    for (cudaEvent_t e : ctx->join_event)
+      if (e) cudaEventDestroy(e);
     ctx->stream = nullptr;
     return rc;
   }
@@ -1881,12 +1902,13 @@ int olc_destroy(olc_context* ctx) {
   for (RunSlot& sl : ctx->runs) release_slot(sl);
   if (ctx->side) cudaStreamSynchronize(ctx->side);
   cudaStream_t st = ctx->stream, side = ctx->side;
-  cudaEvent_t fork = ctx->fork_event, join = ctx->join_event;
+  cudaEvent_t fork = ctx->fork_event, join0 = ctx->join_event[0], join1 = ctx->join_event[1];
   delete ctx;  // device buffers are freed here
   if (st) cudaStreamDestroy(st);
   if (side) cudaStreamDestroy(side);
   if (fork) cudaEventDestroy(fork);
-  if (join) cudaEventDestroy(join);
+  if (join0) cudaEventDestroy(join0);
+  if (join1) cudaEventDestroy(join1);
   return OLC_OK;
 }
 
@@ -1985,8 +2007,8 @@ int olc_pool_info_get(const olc_context* ctx, olc_pool_info* info) {
   uint64_t wf = 0;
   for (const DeviceBuffer* b : {&ctx->q0_o, &ctx->q0_d, &ctx->q0_p, &ctx->q1_o, &ctx->q1_d, &ctx->q1_p, &ctx->q2_o,
                                 &ctx->q2_d, &ctx->q2_p, &ctx->sort_keys, &ctx->sort_bins,
-                                &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->ps_tp,
-                                &ctx->ps_rad, &ctx->ps_meta, &ctx->ps_ior, &ctx->ps_cone, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
+                                &ctx->hit_tuv, &ctx->hit_inst, &ctx->sh_o, &ctx->sh_d, &ctx->sh_c, &ctx->sh1_o,
+                                &ctx->sh1_d, &ctx->sh1_c, &ctx->ps_tp, &ctx->ps_rad, &ctx->ps_shadow, &ctx->ps_meta, &ctx->ps_ior, &ctx->ps_cone, &ctx->runs[0].table_dev, &ctx->runs[1].table_dev,
                                 &ctx->prod_depth, &ctx->prod_normal,
                                 &ctx->prod_inst, &ctx->prod_mat, &ctx->prod_prim, &ctx->prod_pos, &ctx->prod_bary,
                                 &ctx->prod_signals, &ctx->prod_secondary,

@@ -334,6 +334,8 @@ struct PathState {
   uint4* meta;             // pixel, sample, bounce | flags << 8, job
   float4* ior_stack;       // 4 per path: indices of refraction of the media entered, entries 1..15
   float2* cone;            // ray cone (width, spread) of the path's next ray; textured scenes only
+  float4* shadow;          // rgb the path's unoccluded shadow rays carried, unused; written only by the
+                           // any-hit kernel, so the shadow rays of a bounce run beside later bounces
 };
 
 #define OLC_PATH_FLAG_PREV_NEE 1u     // the previous vertex sampled area lights

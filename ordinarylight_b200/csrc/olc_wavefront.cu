@@ -113,6 +113,7 @@ __global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __re
     q.path[i] = i;
     ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ps.shadow[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     ps.meta[i] = make_uint4(pixel, sample, 0u, j);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = count;
@@ -255,8 +256,8 @@ __global__ void __maxnreg__(kTraceRegisters) k_trace_shadow(SceneView s, ShadowQ
         if (!tr.found()) {
           uint32_t path = __float_as_uint(sq.dir_path[i].w);
           float4 c = sq.contrib_root[i];
-          float4 r = ps.radiance[path];
-          ps.radiance[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
+          float4 r = ps.shadow[path];
+          ps.shadow[path] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, r.w);
         }
       },
       err);
@@ -893,10 +894,12 @@ __global__ void k_accumulate(const ChunkHeader* __restrict__ hdr, const JobRec* 
     }
     unsigned long long fr = 0ull, fg = 0ull, fb = 0ull;
     for (uint32_t k = 0; k < samples; ++k) {
+      // the path's own emission terms, then its shadow rays' sum
       const float4 r = ps.radiance[i + k * job.npix];
-      const unsigned long long sr = to_fixed(r.x, &cnt->nan_samples);
-      const unsigned long long sg = to_fixed(r.y, &cnt->nan_samples);
-      const unsigned long long sb = to_fixed(r.z, &cnt->nan_samples);
+      const float4 sh = ps.shadow[i + k * job.npix];
+      const unsigned long long sr = to_fixed(r.x + sh.x, &cnt->nan_samples);
+      const unsigned long long sg = to_fixed(r.y + sh.y, &cnt->nan_samples);
+      const unsigned long long sb = to_fixed(r.z + sh.z, &cnt->nan_samples);
       fr += sr;
       fg += sg;
       fb += sb;
