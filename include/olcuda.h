@@ -231,6 +231,8 @@ typedef struct olc_render_stats {
   uint64_t overflow;         /* queue overflows (paths terminated) */
   uint64_t traversal_errors; /* stack overflows (0 on a healthy run) */
   float gpu_ms;              /* CUDA-event time of the device work */
+  /* raygen_ms stays 0: bounce-0 closest-hit traversal generates the camera
+   * rays it traces, so their generation is part of trace_ms */
   float raygen_ms, trace_ms, shade_ms, shadow_ms, restir_ms, accumulate_ms;
   uint32_t chunks;
   uint32_t restir_history_used;
@@ -510,7 +512,7 @@ OLC_API int olc_reset_history(olc_context* ctx);
  * (camera rays, rays, hits+misses, shadow rays, path samples, pixels);
  * misses = rays of the launch's bounce that left the scene. */
 enum olc_stage {
-  OLC_STAGE_RAYGEN = 0,
+  OLC_STAGE_RAYGEN = 0,   /* no longer recorded: part of bounce 0's OLC_STAGE_TRACE */
   OLC_STAGE_TRACE = 1,
   OLC_STAGE_RESTIR = 2,
   OLC_STAGE_SHADE = 3,

@@ -1456,8 +1456,6 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
     const ChunkHeader* hdr = reinterpret_cast<const ChunkHeader*>(rb.table + c * rb.stride);
     const JobRec* jobs = reinterpret_cast<const JobRec*>(rb.table + c * rb.stride + sizeof(ChunkHeader));
     OLC_CUDA(cudaMemsetAsync(rb.cnt, 0, sizeof(Counters), st));
-    launch_raygen(ctx->ls, hdr, jobs, scenes, rb.qa, rb.ps, rb.cnt, st);
-    tl_mark(ctx, OLC_STAGE_RAYGEN, 0, c);
     const RayQueue* qin = &rb.qa;
     const RayQueue* qout = &rb.qb;
     const RayQueue* spare = &rb.qc;
@@ -1477,7 +1475,9 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         hl.count = ctx->restir.hit_count.as<uint32_t>();
         OLC_CUDA(cudaMemsetAsync(hl.count, 0, 4, st));
       }
-      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, hl, st);
+      // bounce 0 generates the chunk's camera rays as it traces them
+      const CameraPaths cam{hdr, jobs, scenes, rb.ps};
+      launch_trace_closest(ctx->ls, s, *qin, rb.hb, rb.cnt, b, hl, b == 0 ? &cam : nullptr, st);
       tl_mark(ctx, OLC_STAGE_TRACE, b, c);
       const uint4* restir = nullptr;
       if (b == 0 && ch.restir) {

@@ -3,7 +3,8 @@
 // fixed-point HDR accumulation.
 //
 // Stage map against the reference wavefront (ordinarylight/shaders/):
-//   k_raygen         wavefront_generate.comp:86-167 (+ path init)
+//   start_camera_path wavefront_generate.comp:86-167 (+ path init), run by
+//                    bounce-0 k_trace_closest for each ray it takes
 //   k_trace_closest  wavefront_intersect.comp:317-356 (software traversal)
 //   k_shade          wavefront_shade.comp:262-596
 //   k_trace_shadow   nativeOccluded in transport_v1/lighting.glsl
@@ -94,29 +95,30 @@ OLC_D uint32_t stream_pixel(uint32_t k, uint32_t w, uint32_t h) {
   return (y0 + r / rem) * w + (w - rem) + r % rem;
 }
 
-__global__ void k_raygen(const ChunkHeader* __restrict__ hdr, const JobRec* __restrict__ jobs,
-                         const SceneRec* __restrict__ scenes, RayQueue q, PathState ps, Counters* cnt) {
-  const uint32_t count = hdr->count;
-  const uint32_t num_segments = hdr->num_segments;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t j = segment_of_path(jobs, num_segments, i);
-    const JobRec& job = jobs[j];
-    const uint64_t local = job.seg_first + (i - job.seg_begin);
-    const uint32_t local_sample = (uint32_t)(local / job.npix);
-    const uint32_t pixel =
-        stream_pixel((uint32_t)(local - (uint64_t)local_sample * job.npix), job.width, job.height);
-    const uint32_t sample = job.sample_base + local_sample;   // the RNG key's sample index
-    float3 o, d;
-    camera_ray(job, pixel, sample, nullptr, o, d);
-    q.origin_tmin[i] = make_float4(o.x, o.y, o.z, job_t_min(job));
-    q.dir_root[i] = make_float4(d.x, d.y, d.z, __uint_as_float(scenes[job.scene].tlas_root));
-    q.path[i] = i;
-    ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ps.shadow[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ps.meta[i] = make_uint4(pixel, sample, 0u, j);
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = count;
+// Camera ray and initial state of chunk path i (the ray generation of
+// wavefront_generate.comp:86-167 and the path init): writes the bounce-0
+// queue entry and the path record, and returns the ray.  Bounce-0
+// closest-hit traversal calls it for each ray it takes, so no separate pass
+// writes the queue for the traversal to read back.
+OLC_D void start_camera_path(const JobRec* __restrict__ jobs, uint32_t num_segments,
+                             const SceneRec* __restrict__ scenes, const RayQueue& q, const PathState& ps, uint32_t i,
+                             float3& o, float3& d, float& tmin, uint32_t& root) {
+  const uint32_t j = segment_of_path(jobs, num_segments, i);
+  const JobRec& job = jobs[j];
+  const uint64_t local = job.seg_first + (i - job.seg_begin);
+  const uint32_t local_sample = (uint32_t)(local / job.npix);
+  const uint32_t pixel = stream_pixel((uint32_t)(local - (uint64_t)local_sample * job.npix), job.width, job.height);
+  const uint32_t sample = job.sample_base + local_sample;   // the RNG key's sample index
+  camera_ray(job, pixel, sample, nullptr, o, d);
+  tmin = job_t_min(job);
+  root = scenes[job.scene].tlas_root;
+  q.origin_tmin[i] = make_float4(o.x, o.y, o.z, tmin);
+  q.dir_root[i] = make_float4(d.x, d.y, d.z, __uint_as_float(root));
+  q.path[i] = i;
+  ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  ps.shadow[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  ps.meta[i] = make_uint4(pixel, sample, 0u, j);
 }
 
 // Persistent traversal (Aila and Laine, "Understanding the Efficiency of Ray
@@ -194,31 +196,45 @@ OLC_D void persistent_trace(const SceneView& s, uint32_t n, uint32_t* cursor, in
 // shared memory), so eight blocks of 128 threads stay resident per SM.
 constexpr int kTraceRegisters = 64;
 
-template <int STACK, int SCHED>
+// kCamera: bounce 0, whose rays the kernel generates itself (the chunk's
+// paths in order, `cam` their jobs and path records) and whose primary hits
+// of ReSTIR jobs it lists for the resampling passes.
+template <int STACK, int SCHED, bool kCamera>
 __global__ void __maxnreg__(kTraceRegisters) k_trace_closest(SceneView s, RayQueue q, HitBuf h, Counters* cnt,
-                                                              uint32_t bounce, HitListOut hl) {
+                                                              uint32_t bounce, HitListOut hl, CameraPaths cam) {
   extern __shared__ int smem_stack[];
-  const uint32_t n = cnt->queue_count[bounce];
+  uint32_t n, num_segments = 0;
+  if (kCamera) {
+    n = cam.hdr->count;
+    num_segments = cam.hdr->num_segments;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->queue_count[0] = n;
+  } else {
+    n = cnt->queue_count[bounce];
+  }
   uint32_t err = 0;
   persistent_trace<STACK, false, SCHED>(
       s, n, &cnt->closest_cursor[bounce], smem_stack,
       [&](uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& root) {
-        float4 ot = q.origin_tmin[i];
-        float4 dr = q.dir_root[i];
-        o = f3(ot);
-        d = f3(dr);
-        tmin = ot.w;
         tmax = CUDART_INF_F;
-        root = __float_as_uint(dr.w);
+        if (kCamera) {
+          start_camera_path(cam.jobs, num_segments, cam.scenes, q, cam.ps, i, o, d, tmin, root);
+        } else {
+          float4 ot = q.origin_tmin[i];
+          float4 dr = q.dir_root[i];
+          o = f3(ot);
+          d = f3(dr);
+          tmin = ot.w;
+          root = __float_as_uint(dr.w);
+        }
       },
       [&](uint32_t i, const Traversal<STACK, false>& tr) {
         h.tuv_slot[i] = tr.found() ? make_float4(tr.hit_t, tr.hit_u(), tr.hit_v(), __uint_as_float(tr.hit_slot))
                                    : make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
         h.instance[i] = tr.found() ? tr.hit_inst : 0xffffffffu;
-        if (hl.list != nullptr) {
-          // bounce 0 (path slot i is queue slot i): list the primary hits of
-          // ReSTIR jobs for the resampling passes, one atomic per group of
-          // lanes finishing together; the list order affects no result
+        if (kCamera && hl.list != nullptr) {
+          // (path slot i is queue slot i): list the primary hits of ReSTIR
+          // jobs, one atomic per group of lanes finishing together; the list
+          // order affects no result
           const bool take = tr.found() && hl.jobs[hl.meta[i].w].restir != 0u;
           const uint32_t group = __activemask();
           const uint32_t ballot = __ballot_sync(group, take);
@@ -1036,24 +1052,22 @@ inline size_t stack_bytes(uint32_t depth, uint32_t threads) {
 
 }  // namespace
 
-void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const SceneRec* scenes,
-                   const RayQueue& q, const PathState& ps, Counters* cnt, cudaStream_t stream) {
-  k_raygen<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, scenes, q, ps, cnt);
-  OLC_LAUNCH_CHECK("k_raygen");
-}
-
 void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
-                          Counters* cnt, uint32_t bounce, const HitListOut& hl, cudaStream_t stream) {
+                          Counters* cnt, uint32_t bounce, const HitListOut& hl, const CameraPaths* cam,
+                          cudaStream_t stream) {
   dispatch_stack(ls.stack_depth, [&](auto depth) {
     constexpr int D = decltype(depth)::value;
     const size_t smem = stack_bytes(D, ls.trace_block);
     // camera rays come in 8x4-pixel tiles: a warp keeps its 32 coherent rays
     // to the end instead of refilling lanes with rays of other tiles
-    if (ls.scheduler == 1 || bounce == 0)
-      k_trace_closest<D, 1><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce,
-                                                                             bounce == 0 ? hl : HitListOut{});
+    if (cam != nullptr)
+      k_trace_closest<D, 1, true><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, 0u, hl, *cam);
+    else if (ls.scheduler == 1)
+      k_trace_closest<D, 1, false><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce,
+                                                                                    HitListOut{}, CameraPaths{});
     else
-      k_trace_closest<D, 0><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce, HitListOut{});
+      k_trace_closest<D, 0, false><<<ls.grid_trace, ls.trace_block, smem, stream>>>(s, q, h, cnt, bounce,
+                                                                                    HitListOut{}, CameraPaths{});
   });
   OLC_LAUNCH_CHECK("k_trace_closest");
 }
@@ -1185,15 +1199,18 @@ void configure_trace_kernels() {
     cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
   };
-  prefer((const void*)k_trace_closest<16, 0>);
-  prefer((const void*)k_trace_closest<24, 0>);
-  prefer((const void*)k_trace_closest<32, 0>);
+  prefer((const void*)k_trace_closest<16, 0, false>);
+  prefer((const void*)k_trace_closest<24, 0, false>);
+  prefer((const void*)k_trace_closest<32, 0, false>);
+  prefer((const void*)k_trace_closest<16, 1, true>);
+  prefer((const void*)k_trace_closest<24, 1, true>);
+  prefer((const void*)k_trace_closest<32, 1, true>);
   prefer((const void*)k_trace_shadow<16, 0>);
   prefer((const void*)k_trace_shadow<24, 0>);
   prefer((const void*)k_trace_shadow<32, 0>);
-  prefer((const void*)k_trace_closest<16, 1>);
-  prefer((const void*)k_trace_closest<24, 1>);
-  prefer((const void*)k_trace_closest<32, 1>);
+  prefer((const void*)k_trace_closest<16, 1, false>);
+  prefer((const void*)k_trace_closest<24, 1, false>);
+  prefer((const void*)k_trace_closest<32, 1, false>);
   prefer((const void*)k_trace_shadow<16, 1>);
   prefer((const void*)k_trace_shadow<24, 1>);
   prefer((const void*)k_trace_shadow<32, 1>);

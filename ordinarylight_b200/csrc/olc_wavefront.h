@@ -67,8 +67,6 @@ struct ProductPtrs {
 };
 
 void configure_trace_kernels();
-void launch_raygen(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const SceneRec* scenes,
-                   const RayQueue& q, const PathState& ps, Counters* cnt, cudaStream_t stream);
 // Where camera-ray traversal lists the chunk's primary hits of ReSTIR jobs
 // (path slots, in completion order; `count` zeroed before the launch), or
 // list == nullptr for no list.
@@ -78,8 +76,20 @@ struct HitListOut {
   uint32_t* list = nullptr;
   uint32_t* count = nullptr;
 };
+// The chunk whose camera paths bounce-0 traversal starts: its header (path
+// count, segments), job segments, scene records and path records.
+struct CameraPaths {
+  const ChunkHeader* hdr = nullptr;
+  const JobRec* jobs = nullptr;
+  const SceneRec* scenes = nullptr;
+  PathState ps{};
+};
+// Closest-hit traversal of a bounce's queue; with `cam` (bounce 0) the
+// kernel generates the chunk's camera rays into the queue and initialises
+// the path records itself.
 void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQueue& q, const HitBuf& h,
-                          Counters* cnt, uint32_t bounce, const HitListOut& hl, cudaStream_t stream);
+                          Counters* cnt, uint32_t bounce, const HitListOut& hl, const CameraPaths* cam,
+                          cudaStream_t stream);
 void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const ShadowQueue& sq, const PathState& ps,
                          Counters* cnt, uint32_t bounce, cudaStream_t stream);
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,

@@ -809,7 +809,7 @@ class CudaWavefrontRenderer(RendererImplementation):
         return occ.cpu().numpy().astype(bool)
 
     def camera_rays(self, camera, width, height, *, sample=0, frame_index=0, jitter=None):
-        """Device camera rays of one sample (the raygen kernel's model)."""
+        """Device camera rays of one sample (the model of the camera rays that bounce-0 traversal generates)."""
         import torch
 
         self._require_open()
