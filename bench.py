@@ -67,7 +67,7 @@ WORKLOAD = ("instanced PBR scene: 64 x 16,384-tri spheres + 2-tri ground + 1,024
 # the layout): ray 32 B, hit 20 B, path 36 B, material 32 B, shading triangle
 # 72 B, shadow ray 44 B.
 BYTES_PER_UNIT = {
-    "raygen": 68.0,          # write ray 32 + path 36 per camera ray
+    "raygen": 68.0,          # write ray 32 + path 36 per camera ray (in bounce-0 traversal)
     "trace_closest": 52.0,   # read ray 32, write hit 20 per ray
     "shade_hit": 304.0,      # read 32+20+36+32+36+36, write 36+32+44 per surface hit
     "shade_miss": 124.0,     # read ray 32 + hit 20 + path 36, write path 36
@@ -256,7 +256,10 @@ def _profile(renderer):
     return [(_native.STAGE_NAMES[r.stage], r.bounce, int(r.items), int(r.misses), float(r.ms)) for r in records]
 
 
-def _launch_bytes(stage, items, misses):
+def _launch_bytes(stage, bounce, items, misses):
+    if stage == "trace_closest" and bounce == 0:
+        # bounce-0 traversal generates its camera rays and their path records
+        return (BYTES_PER_UNIT["raygen"] + BYTES_PER_UNIT["trace_closest"]) * items
     if stage == "shade":
         return BYTES_PER_UNIT["shade_hit"] * (items - misses) + BYTES_PER_UNIT["shade_miss"] * misses
     return BYTES_PER_UNIT[stage] * items
@@ -319,9 +322,9 @@ def run_ours(args, rank, world, device_index):
             ends[k].record(stream)
         rays += renderer.last_timings["rays"]
         restir_records = 0
-        for stage, _b, items, misses, ms in _profile(renderer):
+        for stage, bounce, items, misses, ms in _profile(renderer):
             stage_ms[stage] = stage_ms.get(stage, 0.0) + ms
-            stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, items, misses)
+            stage_bytes[stage] = stage_bytes.get(stage, 0.0) + _launch_bytes(stage, bounce, items, misses)
             stage_launches[stage] = stage_launches.get(stage, 0) + 1
             if stage == "restir":
                 # per chunk two records: resampling (compaction, initial, one
