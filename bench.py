@@ -420,8 +420,9 @@ def run_ours(args, rank, world, device_index):
                      "traffic": _traffic_from_profiles(dominant),
                      "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
                      "limiter": ("dependent-load latency and SIMD divergence, not HBM: BVH traversal with the "
-                                 "instanced scene in L2 (ncu: 62-85 % L2 hits, 8-18 of 32 lanes active, "
-                                 "~3 long-scoreboard stalls per issue, ALU pipe ~46 % of peak; "
+                                 "instanced scene's nodes in L2 (ncu: 2 MB of DRAM reads per 921,600 camera "
+                                 "rays, 8-19 of 32 lanes active, ~3 long-scoreboard stalls per issue, "
+                                 "ALU pipe 45-47 % of peak; "
                                  "profiles/hot_kernels_instanced_640x360.md)")
                      if dominant == "trace_closest" else None},
         "stages": stages,
