@@ -571,8 +571,10 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
                                                     st.pool2.as<float4>());
   OLC_LAUNCH_CHECK("k_restir_pool");
   const uint32_t grid = ls.grid_shade;
-  if (textures) k_restir_initial<true><<<grid, 128, 0, stream>>>(a);
-  else k_restir_initial<false><<<grid, 128, 0, stream>>>(a);
+  if (textures)
+    k_restir_initial<true><<<resident_grid((const void*)k_restir_initial<true>, 128, 0, grid), 128, 0, stream>>>(a);
+  else
+    k_restir_initial<false><<<resident_grid((const void*)k_restir_initial<false>, 128, 0, grid), 128, 0, stream>>>(a);
   OLC_LAUNCH_CHECK("k_restir_initial");
   // spatial passes ping-pong A -> B -> A ...; the last pass finalises.
   uint32_t passes = std::max<uint32_t>(cfg.restir_spatial, 1u);
@@ -588,8 +590,11 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
     b.out1 = in_a ? st.res_b1.as<uint4>() : st.res_a1.as<uint4>();
     b.out2 = in_a ? st.res_b2.as<uint4>() : st.res_a2.as<uint4>();
     b.finalize = (p + 1 == passes) ? 1u : 0u;
-    if (textures) k_restir_spatial<true><<<grid, 128, 0, stream>>>(b);
-    else k_restir_spatial<false><<<grid, 128, 0, stream>>>(b);
+    if (textures)
+      k_restir_spatial<true><<<resident_grid((const void*)k_restir_spatial<true>, 128, 0, grid), 128, 0, stream>>>(b);
+    else
+      k_restir_spatial<false><<<resident_grid((const void*)k_restir_spatial<false>, 128, 0, grid), 128, 0, stream>>>(
+          b);
     OLC_LAUNCH_CHECK("k_restir_spatial");
     in_a = !in_a;
   }

@@ -15,6 +15,10 @@
 // is in its state, a queued ray carries its scene's TLAS root.  Queue counts
 // never leave the device: persistent kernels read them, so the bounce loop
 // can be captured once as a CUDA graph.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
 #include "olc_internal.h"
 #include "olc_shading.cuh"
 #include "olc_refvolume.cuh"
@@ -1086,6 +1090,29 @@ void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const Shadow
   OLC_LAUNCH_CHECK("k_trace_shadow");
 }
 
+uint32_t resident_grid(const void* fn, uint32_t block, size_t smem, uint32_t max_grid) {
+  struct Entry {
+    const void* fn;
+    uint32_t block;
+    size_t smem;
+    int device;
+    uint32_t grid;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> cache;
+  int device = 0;
+  OLC_CUDA(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(mu);
+  for (const Entry& e : cache)
+    if (e.fn == fn && e.block == block && e.smem == smem && e.device == device) return std::min(e.grid, max_grid);
+  int per_sm = 0, sms = 0;
+  OLC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)block, smem));
+  OLC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const uint32_t grid = (uint32_t)std::max(1, per_sm) * (uint32_t)std::max(1, sms);
+  cache.push_back(Entry{fn, block, smem, device, grid});
+  return std::min(grid, max_grid);
+}
+
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
@@ -1103,10 +1130,13 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   a.capacity = capacity;
   a.prod = prod;
   a.restir = restir;
-  if (textures && media) k_shade<true, true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
-  else if (textures) k_shade<true, false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
-  else if (media) k_shade<false, true><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
-  else k_shade<false, false><<<ls.grid_shade, ls.trace_block, 0, stream>>>(a);
+  auto launch = [&](auto kernel) {
+    kernel<<<resident_grid((const void*)kernel, ls.trace_block, 0, ls.grid_shade), ls.trace_block, 0, stream>>>(a);
+  };
+  if (textures && media) launch(k_shade<true, true>);
+  else if (textures) launch(k_shade<true, false>);
+  else if (media) launch(k_shade<false, true>);
+  else launch(k_shade<false, false>);
   OLC_LAUNCH_CHECK("k_shade");
 }
 
@@ -1127,13 +1157,15 @@ size_t sort_bins_bytes() { return kSortBins * sizeof(uint32_t); }
 void launch_ref_volumes(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& q,
                         const HitBuf& hits, const PathState& ps, const Counters* cnt, uint32_t bounce,
                         cudaStream_t stream) {
-  k_ref_volumes<<<ls.grid_shade, 128, 0, stream>>>(jobs, s, q, hits, ps, cnt, bounce);
+  k_ref_volumes<<<resident_grid((const void*)k_ref_volumes, 128, 0, ls.grid_shade), 128, 0, stream>>>(
+      jobs, s, q, hits, ps, cnt, bounce);
   OLC_LAUNCH_CHECK("k_ref_volumes");
 }
 
 void launch_accumulate(const LaunchShape& ls, const ChunkHeader* hdr, const JobRec* jobs, const PathState& ps,
                        unsigned long long* accum, float* sample_lum, Counters* cnt, cudaStream_t stream) {
-  k_accumulate<<<ls.grid_simple, ls.block, 0, stream>>>(hdr, jobs, ps, accum, sample_lum, cnt);
+  k_accumulate<<<resident_grid((const void*)k_accumulate, ls.block, 0, ls.grid_simple), ls.block, 0, stream>>>(
+      hdr, jobs, ps, accum, sample_lum, cnt);
   OLC_LAUNCH_CHECK("k_accumulate");
 }
 

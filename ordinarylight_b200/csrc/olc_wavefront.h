@@ -67,6 +67,12 @@ struct ProductPtrs {
 };
 
 void configure_trace_kernels();
+// Grid of a grid-stride kernel: the blocks of `block` threads (and `smem`
+// bytes of dynamic shared memory) that all SMs of the current device hold at
+// once, at most `max_grid`.  A grid-stride loop over a fixed share of the
+// items per block then runs in one wave; a larger grid leaves a partial
+// second wave whose blocks start only as the first ones finish.
+uint32_t resident_grid(const void* fn, uint32_t block, size_t smem, uint32_t max_grid);
 // Where camera-ray traversal lists the chunk's primary hits of ReSTIR jobs
 // (path slots, in completion order; `count` zeroed before the launch), or
 // list == nullptr for no list.
