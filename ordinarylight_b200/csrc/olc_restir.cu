@@ -567,8 +567,8 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   a.pool0 = st.pool0.as<float4>();
   a.pool1 = st.pool1.as<float4>();
   a.pool2 = st.pool2.as<float4>();
-  k_restir_pool<<<ls.grid_simple, 256, 0, stream>>>(hdr, jobs, s, st.pool0.as<float4>(), st.pool1.as<float4>(),
-                                                    st.pool2.as<float4>());
+  k_restir_pool<<<resident_grid((const void*)k_restir_pool, 256, 0, ls.grid_simple), 256, 0, stream>>>(
+      hdr, jobs, s, st.pool0.as<float4>(), st.pool1.as<float4>(), st.pool2.as<float4>());
   OLC_LAUNCH_CHECK("k_restir_pool");
   const uint32_t grid = ls.grid_shade;
   if (textures)

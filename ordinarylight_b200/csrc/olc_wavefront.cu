@@ -1177,7 +1177,8 @@ void launch_sample_variance(const LaunchShape& ls, const float* sample_lum, uint
 
 void launch_resolve(const LaunchShape& ls, const ResolveEntry* entries, const uint32_t* num_entries,
                     const unsigned long long* accum, float4* out, cudaStream_t stream) {
-  k_resolve<<<ls.grid_simple, ls.block, 0, stream>>>(entries, num_entries, accum, out);
+  k_resolve<<<resident_grid((const void*)k_resolve, ls.block, 0, ls.grid_simple), ls.block, 0, stream>>>(
+      entries, num_entries, accum, out);
   OLC_LAUNCH_CHECK("k_resolve");
 }
 
