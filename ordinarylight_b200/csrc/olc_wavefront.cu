@@ -393,8 +393,20 @@ __global__ void __maxnreg__(ShadeRegisters<kMedia>::kCap) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
   const uint32_t n = a.cnt->queue_count[bounce];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+  // Warps take the queue in grabs of 64 paths (one atomic per grab), so a
+  // block whose paths cost more (media crossings, refractions) does not
+  // hold the launch open while others idle.
+  uint32_t grab = 0, grab_end = 0;
+  while (true) {
+    if (grab == grab_end) {
+      uint32_t g = 0;
+      if (lane_id() == 0u) g = atomicAdd(&a.cnt->shade_cursor[bounce], 64u);
+      grab = __shfl_sync(0xffffffffu, g, 0);
+      grab_end = grab + 64u;
+    }
+    const uint32_t base = grab;
+    grab += 32u;
+    if (base >= n) break;
     const uint32_t i = base + lane_id();
     const bool valid = i < n;
     bool want_next = false, want_shadow = false, is_miss = false;
