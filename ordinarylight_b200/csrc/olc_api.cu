@@ -1473,7 +1473,7 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         hl.meta = rb.ps.meta;
         hl.list = ctx->restir.hit_list.as<uint32_t>();
         hl.count = ctx->restir.hit_count.as<uint32_t>();
-        OLC_CUDA(cudaMemsetAsync(hl.count, 0, 4, st));
+        OLC_CUDA(cudaMemsetAsync(hl.count, 0, 32, st));   // count and the passes' cursors
       }
       // bounce 0 generates the chunk's camera rays as it traces them
       const CameraPaths cam{hdr, jobs, scenes, rb.ps};

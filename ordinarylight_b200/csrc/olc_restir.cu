@@ -308,6 +308,7 @@ struct RestirArgs {
   PathState ps;
   const uint32_t* hit_list;
   const uint32_t* hit_count;
+  uint32_t* cursor;           // work cursor of this launch (zeroed with hit_count)
   uint32_t candidates;
   uint32_t history_cap;     // M cap of the temporal history
   uint32_t neighbours;
@@ -375,7 +376,19 @@ template <bool kTextures>
 __global__ void __launch_bounds__(128, kTextures ? 4 : 8) k_restir_initial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+  // warps take the hit list in grabs of 64 entries (one atomic per grab),
+  // so blocks whose hits cost more do not hold the launch open
+  for (uint32_t grab = 0, grab_end = 0;;) {
+    if (grab == grab_end) {
+      uint32_t g = 0;
+      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 64u);
+      grab = __shfl_sync(0xffffffffu, g, 0);
+      grab_end = grab + 64u;
+    }
+    const uint32_t k = grab + (threadIdx.x & 31u);
+    grab += 32u;
+    if (grab - 32u >= n) break;
+    if (k >= n) continue;
     const uint32_t i = a.hit_list[k];
     const uint4 meta = a.ps.meta[i];
     const JobRec& job = a.jobs[meta.w];
@@ -439,7 +452,19 @@ template <bool kTextures>
 __global__ void __launch_bounds__(128, kTextures ? 4 : 8) k_restir_spatial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+  // warps take the hit list in grabs of 64 entries (one atomic per grab),
+  // so blocks whose hits cost more do not hold the launch open
+  for (uint32_t grab = 0, grab_end = 0;;) {
+    if (grab == grab_end) {
+      uint32_t g = 0;
+      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 64u);
+      grab = __shfl_sync(0xffffffffu, g, 0);
+      grab_end = grab + 64u;
+    }
+    const uint32_t k = grab + (threadIdx.x & 31u);
+    grab += 32u;
+    if (grab - 32u >= n) break;
+    if (k >= n) continue;
     const uint32_t i = a.hit_list[k];
     const uint4 meta = a.ps.meta[i];
     const JobRec& job = a.jobs[meta.w];
@@ -532,7 +557,7 @@ void restir_prepare(RestirState& st, uint64_t reservoirs, uint32_t slots, uint32
     st.hit_list.allocate((size_t)slots * 4);
     st.slots = slots;
   }
-  if (!st.hit_count.get()) st.hit_count.allocate(16);
+  if (!st.hit_count.get()) st.hit_count.allocate(32);
   if ((uint64_t)st.next_stamp + chunks >= 0xffffffffull) {
     // stamps would wrap: clear every stored stamp and start again at 1
     for (DeviceBuffer* b : {&st.res_a1, &st.res_b1, &st.hist1}) OLC_CUDA(cudaMemset(b->get(), 0, st.reservoirs * 16));
@@ -575,6 +600,7 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
       hdr, jobs, s, st.pool0.as<float4>(), st.pool1.as<float4>(), st.pool2.as<float4>());
   OLC_LAUNCH_CHECK("k_restir_pool");
   const uint32_t grid = ls.grid_shade;
+  a.cursor = st.hit_count.as<uint32_t>() + 1;
   if (textures)
     k_restir_initial<true><<<resident_grid((const void*)k_restir_initial<true>, 128, 0, grid), 128, 0, stream>>>(a);
   else
@@ -586,6 +612,7 @@ const uint4* restir_run(RestirState& st, const olc_config& cfg, const LaunchShap
   for (uint32_t p = 0; p < passes; ++p) {
     RestirArgs b = a;
     b.pass = p;
+    b.cursor = st.hit_count.as<uint32_t>() + 2 + p;
     b.neighbours = cfg.restir_spatial ? cfg.restir_neighbours : 0u;
     b.in0 = in_a ? st.res_a0.as<uint4>() : st.res_b0.as<uint4>();
     b.in1 = in_a ? st.res_a1.as<uint4>() : st.res_b1.as<uint4>();
