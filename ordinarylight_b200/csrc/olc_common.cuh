@@ -430,7 +430,7 @@ struct Counters {
   uint32_t closest_cursor[OLC_MAX_BOUNCES + 2]; // persistent closest-hit work cursor
   uint32_t shadow_cursor[OLC_MAX_BOUNCES + 2];  // persistent any-hit work cursor
   uint32_t miss_count[OLC_MAX_BOUNCES + 2];     // rays of each bounce that left the scene
-  uint32_t shade_cursor[OLC_MAX_BOUNCES + 2];   // shading work cursor (64-path grabs)
+  uint32_t shade_cursor[OLC_MAX_BOUNCES + 2];   // shading work cursor (32-path grabs)
   uint32_t overflow;
   uint32_t traversal_errors;
   uint32_t nan_samples;

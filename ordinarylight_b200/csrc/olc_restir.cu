@@ -376,14 +376,14 @@ template <bool kTextures>
 __global__ void __launch_bounds__(128, kTextures ? 4 : 8) k_restir_initial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
-  // warps take the hit list in grabs of 64 entries (one atomic per grab),
+  // warps take the hit list 32 entries at a time (one atomic per grab),
   // so blocks whose hits cost more do not hold the launch open
   for (uint32_t grab = 0, grab_end = 0;;) {
     if (grab == grab_end) {
       uint32_t g = 0;
-      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 64u);
+      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 32u);
       grab = __shfl_sync(0xffffffffu, g, 0);
-      grab_end = grab + 64u;
+      grab_end = grab + 32u;
     }
     const uint32_t k = grab + (threadIdx.x & 31u);
     grab += 32u;
@@ -452,14 +452,14 @@ template <bool kTextures>
 __global__ void __launch_bounds__(128, kTextures ? 4 : 8) k_restir_spatial(RestirArgs a) {
   const SceneView& s = a.s;
   const uint32_t n = *a.hit_count;
-  // warps take the hit list in grabs of 64 entries (one atomic per grab),
+  // warps take the hit list 32 entries at a time (one atomic per grab),
   // so blocks whose hits cost more do not hold the launch open
   for (uint32_t grab = 0, grab_end = 0;;) {
     if (grab == grab_end) {
       uint32_t g = 0;
-      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 64u);
+      if ((threadIdx.x & 31u) == 0u) g = atomicAdd(a.cursor, 32u);
       grab = __shfl_sync(0xffffffffu, g, 0);
-      grab_end = grab + 64u;
+      grab_end = grab + 32u;
     }
     const uint32_t k = grab + (threadIdx.x & 31u);
     grab += 32u;

@@ -393,16 +393,16 @@ __global__ void __maxnreg__(ShadeRegisters<kMedia>::kCap) k_shade(ShadeArgs a) {
   const SceneView& s = a.s;
   const uint32_t bounce = a.bounce;
   const uint32_t n = a.cnt->queue_count[bounce];
-  // Warps take the queue in grabs of 64 paths (one atomic per grab), so a
+  // Warps take the queue 32 paths at a time (one atomic per grab), so a
   // block whose paths cost more (media crossings, refractions) does not
   // hold the launch open while others idle.
   uint32_t grab = 0, grab_end = 0;
   while (true) {
     if (grab == grab_end) {
       uint32_t g = 0;
-      if (lane_id() == 0u) g = atomicAdd(&a.cnt->shade_cursor[bounce], 64u);
+      if (lane_id() == 0u) g = atomicAdd(&a.cnt->shade_cursor[bounce], 32u);
       grab = __shfl_sync(0xffffffffu, g, 0);
-      grab_end = grab + 64u;
+      grab_end = grab + 32u;
     }
     const uint32_t base = grab;
     grab += 32u;
