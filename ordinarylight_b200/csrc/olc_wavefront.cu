@@ -914,16 +914,20 @@ __global__ void k_accumulate(const ChunkHeader* __restrict__ hdr, const JobRec* 
   const uint32_t count = hdr->count;
   const uint32_t num_segments = hdr->num_segments;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint4 meta = ps.meta[i];
-    const JobRec& job = jobs[meta.w];
+    // the segment from the chunk's job table (L1-resident), so the paths of
+    // later sample streams, added by their pixel's first-stream path, read
+    // nothing of their own
+    const uint32_t j = segment_of_path(jobs, num_segments, i);
+    const JobRec& job = jobs[j];
     const uint32_t seg_begin = (uint32_t)job.seg_begin;
-    const uint32_t seg_end = meta.w + 1u < num_segments ? (uint32_t)jobs[meta.w + 1u].seg_begin : count;
+    const uint32_t seg_end = j + 1u < num_segments ? (uint32_t)jobs[j + 1u].seg_begin : count;
     const uint32_t seg_count = seg_end - seg_begin;
     uint32_t samples = 1u;
     if (job.seg_first % job.npix == 0ull && seg_count % job.npix == 0u) {
       if (i - seg_begin >= job.npix) continue;   // added with its pixel's first-stream path
       samples = seg_count / job.npix;
     }
+    const uint4 meta = ps.meta[i];
     unsigned long long fr = 0ull, fg = 0ull, fb = 0ull;
     for (uint32_t k = 0; k < samples; ++k) {
       // the path's own emission terms, then its shadow rays' sum
