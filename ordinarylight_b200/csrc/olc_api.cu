@@ -1493,7 +1493,7 @@ void record_run(olc_context* ctx, const RunPlan& plan, const RunBuffers& rb) {
         tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       }
       launch_shade(ctx->ls, jobs, s, *qin, rb.hb, *qout, rb.sq[b & 1u], rb.ps, rb.cnt, b, ctx->capacity, rb.prod,
-                   restir, ch.textures, ch.media, st);
+                   restir, ch.textures, ch.media, b == 0 && !ch.ref_volumes, st);
       tl_mark(ctx, OLC_STAGE_SHADE, b, c);
       // this bounce's shadow rays on the side stream: they read only their
       // queue and add only to the paths' shadow sums, so the later bounces'

@@ -297,6 +297,8 @@ struct ShadeArgs {
   uint32_t capacity;
   ProductPtrs prod;
   const uint4* restir;   // per-path selected light sample (bounce 0), or null
+  uint32_t fresh;        // every path is at its camera vertex with its initial state (throughput 1,
+                         // previous pdf 0, radiance 0), which then is not read back
 };
 
 // One next-event sample from p: an area emitter (alias-table choice, uniform
@@ -419,8 +421,8 @@ __global__ void __maxnreg__(ShadeRegisters<kMedia>::kCap) k_shade(ShadeArgs a) {
       const float4 ot = a.qin.origin_tmin[i];
       const float4 dr = a.qin.dir_root[i];
       const float4 hit = a.hits.tuv_slot[i];
-      const float4 tp4 = a.ps.throughput[path];
-      const float4 rad4 = a.ps.radiance[path];
+      const float4 tp4 = a.fresh ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : a.ps.throughput[path];
+      const float4 rad4 = a.fresh ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.ps.radiance[path];
       const uint4 meta = a.ps.meta[path];
       const JobRec& job = a.jobs[meta.w];
       const SceneRec& sc = s.scenes[job.scene];
@@ -1132,7 +1134,7 @@ uint32_t resident_grid(const void* fn, uint32_t block, size_t smem, uint32_t max
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
-                  bool textures, bool media, cudaStream_t stream) {
+                  bool textures, bool media, bool fresh, cudaStream_t stream) {
   ShadeArgs a;
   a.jobs = jobs;
   a.s = s;
@@ -1146,6 +1148,7 @@ void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s,
   a.capacity = capacity;
   a.prod = prod;
   a.restir = restir;
+  a.fresh = fresh ? 1u : 0u;
   auto launch = [&](auto kernel) {
     kernel<<<resident_grid((const void*)kernel, ls.trace_block, 0, ls.grid_shade), ls.trace_block, 0, stream>>>(a);
   };

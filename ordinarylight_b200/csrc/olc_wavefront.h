@@ -98,10 +98,13 @@ void launch_trace_closest(const LaunchShape& ls, const SceneView& s, const RayQu
                           cudaStream_t stream);
 void launch_trace_shadow(const LaunchShape& ls, const SceneView& s, const ShadowQueue& sq, const PathState& ps,
                          Counters* cnt, uint32_t bounce, cudaStream_t stream);
+// fresh: every path of the queue is at its camera vertex with the initial
+// state that camera-ray generation wrote (bounce 0 without the reference
+// volume pass), so shading does not read it back.
 void launch_shade(const LaunchShape& ls, const JobRec* jobs, const SceneView& s, const RayQueue& qin,
                   const HitBuf& hits, const RayQueue& qout, const ShadowQueue& sq, const PathState& ps,
                   Counters* cnt, uint32_t bounce, uint32_t capacity, const ProductPtrs& prod, const uint4* restir,
-                  bool textures, bool media, cudaStream_t stream);
+                  bool textures, bool media, bool fresh, cudaStream_t stream);
 // Reorder the bounce's ray queue `in` into `out` by origin cell and direction
 // bin (keys: one word per queue slot; bins: sort_bins_bytes() of scratch).
 void launch_sort_rays(const LaunchShape& ls, const SceneView& s, const RayQueue& in, const RayQueue& out,
